@@ -1,0 +1,524 @@
+// batch.cu -- Part 2 of gravcuda.h: every sink group of a step evaluated
+// by persistent kernels from length-sorted work queues, on index lists into
+// device-resident point and cell tables.
+//
+// Mixed precision (none of this exists in the reference, whose lists carry
+// absolute FP32 copies, nln/mac.c:1421-1561):
+//   * each sink is held as an FP32 offset from its group's FP64 centre;
+//   * each source record is re-centred on the same FP64 centre (with its
+//     periodic image shift) as it is staged, so the inner loops subtract
+//     two small FP32 numbers;
+//   * partial sums of one staged tile are plain FP32, folded into a
+//     compensated (hi, lo) accumulator per tile;
+//   * work-item partials are combined per group in FP64, in a fixed order.
+// Work decomposition: a work item is (group, kind, range of its list);
+// long lists are split so that small problems still fill the GPU; every
+// warp pulls items (costliest first) from its kind's queue until it is
+// empty.  One warp owns one item: lane = sink, 32 sources per staged tile,
+// double-buffered TMA bulk copies (one per lane, one record each) signalled
+// on a per-warp mbarrier.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "common.cuh"
+#include "gravcuda.h"
+#include "interact.cuh"
+
+namespace {
+
+enum { KP = 0, KQ = 1, KH = 2 };
+constexpr int TILE = 32;
+
+struct Item {
+    int32_t group;
+    int32_t slot;      // partial-result slot (creation order: grouped by group)
+    int64_t begin, end;
+};
+
+struct DevProblem {
+    const float4 *points;
+    const nln_qcell *qcells;
+    const nln_hcell *hcells;
+    const nln_group *groups;
+    const uint32_t *list[3];   // idx | shift << 27
+    int64_t ntab[3];           // table sizes for bounds checks
+    const Item *items[3];
+    int nitems[3];
+    int *counters;             // 3 queue heads
+    float4 *part;              // nslots x 32 lanes x 2 (hi, lo)
+    const int64_t *gslot;      // ngroups + 1: slots of group g
+    float4 *out;               // nbodies
+    int64_t ngroups;
+    float eps2;
+    float qsh;
+    double box;
+    unsigned *err;
+};
+
+template <int KIND>
+struct KindOf {
+    static constexpr int rec_bytes = KIND == KP ? 16 : (KIND == KQ ? 64 : 128);
+    static constexpr int order = KIND == KP ? 0 : (KIND == KQ ? 2 : 4);
+};
+
+__device__ __forceinline__ void decode_shift(uint32_t code, double box, double &sx, double &sy,
+                                             double &sz) {
+    sx = ((int)(code / 9) - 1) * box;
+    sy = ((int)(code / 3 % 3) - 1) * box;
+    sz = ((int)(code % 3) - 1) * box;
+}
+
+// Convert this lane's raw record (just landed by TMA) in place into the
+// staged form of interact.cuh, re-centred on the group centre c.
+template <int KIND>
+__device__ __forceinline__ void convert(unsigned char *slot, uint32_t code, const double *c,
+                                        double box) {
+    double sx, sy, sz;
+    decode_shift(code, box, sx, sy, sz);
+    float *o = reinterpret_cast<float *>(slot);
+    if (KIND == KP) {
+        float4 p = *reinterpret_cast<const float4 *>(slot);
+        o[0] = (float)((double)p.x + sx - c[0]);
+        o[1] = (float)((double)p.y + sy - c[1]);
+        o[2] = (float)((double)p.z + sz - c[2]);
+        o[3] = p.w;
+    } else if (KIND == KQ) {
+        const nln_qcell q = *reinterpret_cast<const nln_qcell *>(slot);
+        o[0] = (float)(q.cen[0] + sx - c[0]);
+        o[1] = (float)(q.cen[1] + sy - c[1]);
+        o[2] = (float)(q.cen[2] + sz - c[2]);
+        o[3] = q.mass;
+        float q2[5] = {q.qxx, q.qxy, q.qyy, q.qxz, q.qyz};
+        stage_quad(o, q.R, q2);
+    } else {
+        const nln_hcell h = *reinterpret_cast<const nln_hcell *>(slot);
+        o[0] = (float)(h.cen[0] + sx - c[0]);
+        o[1] = (float)(h.cen[1] + sy - c[1]);
+        o[2] = (float)(h.cen[2] + sz - c[2]);
+        o[3] = h.mass;
+        stage_quad(o, h.R, h.q2);
+        stage_hexa(o, h.R, h.q3, h.q4);
+    }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(256) k_batch(DevProblem P) {
+    constexpr int RB = KindOf<KIND>::rec_bytes;
+    constexpr int ORDER = KindOf<KIND>::order;
+    constexpr int STRIDE = RB / 4;  // floats per staged slot
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    unsigned char *wbuf = smem + (size_t)wib * (2 * TILE * RB + 16);
+    auto buf = [&](uint32_t seq) { return wbuf + (seq & 1) * (TILE * RB); };
+    uint64_t *bar = reinterpret_cast<uint64_t *>(wbuf + 2 * TILE * RB);
+    if (lane == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+
+    const uint32_t *list = P.list[KIND];
+    const int64_t ntab = P.ntab[KIND];
+    const unsigned char *table =
+        KIND == KP ? reinterpret_cast<const unsigned char *>(P.points)
+                   : (KIND == KQ ? reinterpret_cast<const unsigned char *>(P.qcells)
+                                 : reinterpret_cast<const unsigned char *>(P.hcells));
+    uint32_t tseq = 0;  // tiles consumed by this warp: buffer tseq&1, parity (tseq>>1)&1
+    bool alive = true;
+
+    while (alive) {
+        int it = 0;
+        if (lane == 0)
+            it = atomicAdd(&P.counters[KIND], 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= P.nitems[KIND])
+            break;
+        const Item item = P.items[KIND][it];
+        const nln_group G = P.groups[item.group];
+        const double c[3] = {G.cen[0], G.cen[1], G.cen[2]};
+        // this lane's sink, as an FP32 offset from the group centre
+        float ux = 0.f, uy = 0.f, uz = 0.f;
+        if (lane < G.count) {
+            float4 s = P.points[G.first + lane];
+            ux = (float)((double)s.x - c[0]);
+            uy = (float)((double)s.y - c[1]);
+            uz = (float)((double)s.z - c[2]);
+        }
+        float hi[4] = {0.f, 0.f, 0.f, 0.f}, lo[4] = {0.f, 0.f, 0.f, 0.f};
+        const int64_t nent = item.end - item.begin;
+        const int ntile = (int)((nent + TILE - 1) / TILE);
+
+        // entry of this lane in tile t (prefetched one tile ahead)
+        auto fetch = [&](int t) -> uint32_t {
+            int64_t k = item.begin + (int64_t)t * TILE + lane;
+            return (t < ntile && k < item.end) ? __ldg(list + k) : 0xffffffffu;
+        };
+        auto issue = [&](int t, uint32_t ent, uint32_t seq) {
+            const int nt = (int)min((int64_t)TILE, nent - (int64_t)t * TILE);
+            uint64_t *b = &bar[seq & 1];
+            if (lane == 0)
+                mbar_arrive_expect_tx(b, (uint32_t)(nt * RB));
+            __syncwarp();
+            if (lane < nt) {
+                uint32_t idx = ent & NLN_IDX_MASK;
+                if (idx >= (uint32_t)ntab) {  // never expected: keep the transaction count whole
+                    atomicOr(P.err, GC_DEV_BAD_INDEX);
+                    idx = 0;
+                }
+                tma_bulk_g2s(buf(seq) + lane * RB, table + (size_t)idx * RB, RB, b);
+            }
+        };
+        uint32_t ent_cur = fetch(0);
+        uint32_t ent_next = fetch(1);
+        if (ntile > 0)
+            issue(0, ent_cur, tseq);
+        for (int t = 0; t < ntile; t++, tseq++) {
+            if (t + 1 < ntile)
+                issue(t + 1, ent_next, tseq + 1);
+            const uint32_t code_cur = ent_cur >> NLN_IDX_BITS;
+            ent_cur = ent_next;
+            ent_next = fetch(t + 2);
+            const int nt = (int)min((int64_t)TILE, nent - (int64_t)t * TILE);
+            bool ok = mbar_wait_bounded(&bar[tseq & 1], (tseq >> 1) & 1, P.err);
+            if (!__all_sync(0xffffffffu, ok)) {
+                alive = false;
+                break;
+            }
+            unsigned char *bt = buf(tseq);
+            if (lane < nt)
+                convert<KIND>(bt + lane * RB, code_cur, c, P.box);
+            __syncwarp();
+            Acc4 a{0.f, 0.f, 0.f, 0.f};
+            const float *rec = reinterpret_cast<const float *>(bt);
+            if (nt == TILE) {
+#pragma unroll 4
+                for (int r = 0; r < TILE; r++)
+                    interact<ORDER, SOFT_PLUMMER>(rec + r * STRIDE, ux, uy, uz, P.eps2, P.qsh, a);
+            } else {
+                for (int r = 0; r < nt; r++)
+                    interact<ORDER, SOFT_PLUMMER>(rec + r * STRIDE, ux, uy, uz, P.eps2, P.qsh, a);
+            }
+            comp_add(hi[0], lo[0], a.ax);
+            comp_add(hi[1], lo[1], a.ay);
+            comp_add(hi[2], lo[2], a.az);
+            comp_add(hi[3], lo[3], a.phi);
+            __syncwarp();  // every lane is done with bt before it is refilled
+        }
+        if (!alive)
+            break;
+        float4 *dst = P.part + ((size_t)item.slot * 32 + lane) * 2;
+        dst[0] = make_float4(hi[0], hi[1], hi[2], hi[3]);
+        dst[1] = make_float4(lo[0], lo[1], lo[2], lo[3]);
+    }
+}
+
+// Per group, in slot order: sum the partials of its work items in FP64 and
+// write (ax, ay, az, phi) of each sink, coalesced.
+__global__ void k_reduce(DevProblem P) {
+    const int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (g >= P.ngroups)
+        return;
+    const nln_group G = P.groups[g];
+    double s[4] = {0, 0, 0, 0};
+    for (int64_t k = P.gslot[g]; k < P.gslot[g + 1]; k++) {
+        const float4 *src = P.part + ((size_t)k * 32 + lane) * 2;
+        float4 h = src[0], l = src[1];
+        s[0] += (double)h.x + (double)l.x;
+        s[1] += (double)h.y + (double)l.y;
+        s[2] += (double)h.z + (double)l.z;
+        s[3] += (double)h.w + (double)l.w;
+    }
+    if (lane < G.count)
+        P.out[G.first + lane] = make_float4((float)s[0], (float)s[1], (float)s[2], (float)s[3]);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ plan
+struct grav_plan {
+    grav_problem hp{};      // sizes and parameters (host pointers cleared)
+    grav_tuning tune{};
+    DevProblem dp{};
+    std::vector<void *> allocs;
+    int64_t counts[4] = {0, 0, 0, 0};
+    int nsm = 148;
+    int launches = 0;
+    int64_t nslots = 0;
+};
+
+namespace {
+
+template <typename T>
+int dev_copy(grav_plan *pl, const T *src, size_t n, T **dst) {
+    *dst = nullptr;
+    if (n == 0)
+        return 0;
+    GC_CHECK(cudaMalloc((void **)dst, n * sizeof(T)));
+    pl->allocs.push_back(*dst);
+    if (src)
+        GC_CHECK(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+grav_tuning default_tuning(const grav_problem *p, int nsm) {
+    grav_tuning t;
+    t.warps_per_block = 8;
+    t.blocks_per_sm = 2;
+    // split lists so that the item count is at least ~8 per resident warp
+    const int64_t warps = (int64_t)nsm * t.blocks_per_sm * t.warps_per_block;
+    int64_t ng = std::max<int64_t>(p->ngroups, 1);
+    int64_t per = std::max<int64_t>(1, (8 * warps + ng - 1) / ng);
+    auto chunk = [&](int64_t total, int64_t lo, int64_t hi) {
+        int64_t avg = std::max<int64_t>(1, total / ng);
+        int64_t c = std::max<int64_t>(lo, avg / per);
+        c = (c + TILE - 1) / TILE * TILE;
+        return (int)std::min<int64_t>(hi, c);
+    };
+    t.chunk_p = chunk(p->pptr ? p->pptr[p->ngroups] * 16 : 0, 128, 1 << 20);
+    t.chunk_q = chunk(p->qptr ? p->qptr[p->ngroups] : 0, 64, 1 << 20);
+    t.chunk_h = chunk(p->hptr ? p->hptr[p->ngroups] : 0, 32, 1 << 20);
+    return t;
+}
+
+}  // namespace
+
+extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning *tuning,
+                                       grav_plan **plan_out) {
+    *plan_out = nullptr;
+    if (!hp || hp->nbodies <= 0 || hp->ngroups <= 0 || !hp->points || !hp->groups ||
+        !hp->pptr || !hp->plist)
+        return gc::set_status(-1, "grav_groups_upload_CUDA: incomplete problem");
+    if (hp->nbodies + hp->ncells >= (int64_t)NLN_IDX_MASK)
+        return gc::set_status(-1, "grav_groups_upload_CUDA: point table exceeds 27-bit indices");
+    grav_plan *pl = new grav_plan();
+    cudaDeviceGetAttribute(&pl->nsm, cudaDevAttrMultiProcessorCount, 0);
+    pl->hp = *hp;
+    pl->tune = tuning ? *tuning : default_tuning(hp, pl->nsm);
+    const int64_t ng = hp->ngroups, nb = hp->nbodies, np = hp->nbodies + hp->ncells;
+
+    // expand point runs into per-record entries; validate everything we index
+    std::vector<int64_t> eptr(ng + 1, 0);
+    for (int64_t g = 0; g < ng; g++) {
+        int64_t n = 0;
+        for (int64_t k = hp->pptr[g]; k < hp->pptr[g + 1]; k++) n += hp->plist[k].len;
+        eptr[g + 1] = eptr[g] + n;
+        const nln_group &G = hp->groups[g];
+        if (G.count < 1 || G.count > 32 || G.first < 0 || G.first + G.count > nb) {
+            delete pl;
+            return gc::set_status(-1, "group %lld: %d sinks at %lld (1..32 sinks inside the bodies)",
+                                  (long long)g, G.count, (long long)G.first);
+        }
+    }
+    std::vector<uint32_t> pent(eptr[ng]);
+    for (int64_t g = 0; g < ng; g++) {
+        int64_t o = eptr[g];
+        for (int64_t k = hp->pptr[g]; k < hp->pptr[g + 1]; k++) {
+            const nln_pseg s = hp->plist[k];
+            if ((int64_t)s.base + s.len > np || s.shift > 26) {
+                delete pl;
+                return gc::set_status(-1, "point run %lld outside the table", (long long)k);
+            }
+            for (uint32_t j = 0; j < s.len; j++)
+                pent[o++] = (s.base + j) | ((uint32_t)s.shift << NLN_IDX_BITS);
+        }
+    }
+    auto check_cells = [&](const int64_t *ptr, const uint32_t *lst) -> bool {
+        if (!ptr)
+            return true;
+        for (int64_t k = 0; k < ptr[ng]; k++)
+            if ((int64_t)(lst[k] & NLN_IDX_MASK) >= hp->ncells || (lst[k] >> NLN_IDX_BITS) > 26)
+                return false;
+        return true;
+    };
+    if (!check_cells(hp->qptr, hp->qlist) || !check_cells(hp->hptr, hp->hlist) ||
+        (hp->qptr && hp->qptr[ng] && !hp->qcells) || (hp->hptr && hp->hptr[ng] && !hp->hcells)) {
+        delete pl;
+        return gc::set_status(-1, "cell list entry outside the cell table");
+    }
+
+    // work items, created group by group (slot order), then sorted per kind by cost
+    std::vector<Item> items[3];
+    std::vector<int64_t> gslot(ng + 1, 0);
+    const int64_t *ptrs[3] = {eptr.data(), hp->qptr, hp->hptr};
+    const int chunk[3] = {pl->tune.chunk_p, pl->tune.chunk_q, pl->tune.chunk_h};
+    int32_t slot = 0;
+    for (int64_t g = 0; g < ng; g++) {
+        for (int k = 0; k < 3; k++) {
+            if (!ptrs[k])
+                continue;
+            for (int64_t b = ptrs[k][g]; b < ptrs[k][g + 1]; b += chunk[k])
+                items[k].push_back(Item{(int32_t)g, slot++, b, std::min(ptrs[k][g + 1], b + chunk[k])});
+        }
+        gslot[g + 1] = slot;
+    }
+    pl->nslots = slot;
+    for (int k = 0; k < 3; k++)
+        std::stable_sort(items[k].begin(), items[k].end(), [](const Item &a, const Item &b) {
+            return (a.end - a.begin) > (b.end - b.begin);
+        });
+
+    // interaction counts (sinks x sources)
+    for (int64_t g = 0; g < ng; g++) {
+        const int64_t c = hp->groups[g].count;
+        for (int64_t k = hp->pptr[g]; k < hp->pptr[g + 1]; k++)
+            pl->counts[hp->plist[k].base < (uint32_t)nb ? 0 : 1] += c * hp->plist[k].len;
+        if (hp->qptr)
+            pl->counts[2] += c * (hp->qptr[g + 1] - hp->qptr[g]);
+        if (hp->hptr)
+            pl->counts[3] += c * (hp->hptr[g + 1] - hp->hptr[g]);
+    }
+
+    DevProblem &d = pl->dp;
+    int rc = 0;
+    float4 *pts = nullptr;
+    rc |= dev_copy(pl, reinterpret_cast<const float4 *>(hp->points), (size_t)np, &pts);
+    d.points = pts;
+    nln_qcell *qc = nullptr;
+    nln_hcell *hc = nullptr;
+    if (hp->qptr && hp->qptr[ng])
+        rc |= dev_copy(pl, hp->qcells, (size_t)hp->ncells, &qc);
+    if (hp->hptr && hp->hptr[ng])
+        rc |= dev_copy(pl, hp->hcells, (size_t)hp->ncells, &hc);
+    d.qcells = qc;
+    d.hcells = hc;
+    nln_group *gr = nullptr;
+    rc |= dev_copy(pl, hp->groups, (size_t)ng, &gr);
+    d.groups = gr;
+    uint32_t *l0 = nullptr, *l1 = nullptr, *l2 = nullptr;
+    rc |= dev_copy(pl, pent.data(), pent.size(), &l0);
+    if (hp->qptr)
+        rc |= dev_copy(pl, hp->qlist, (size_t)hp->qptr[ng], &l1);
+    if (hp->hptr)
+        rc |= dev_copy(pl, hp->hlist, (size_t)hp->hptr[ng], &l2);
+    d.list[0] = l0;
+    d.list[1] = l1;
+    d.list[2] = l2;
+    d.ntab[0] = np;
+    d.ntab[1] = d.ntab[2] = hp->ncells;
+    for (int k = 0; k < 3; k++) {
+        Item *it = nullptr;
+        rc |= dev_copy(pl, items[k].data(), items[k].size(), &it);
+        d.items[k] = it;
+        d.nitems[k] = (int)items[k].size();
+    }
+    int *ctr = nullptr;
+    rc |= dev_copy<int>(pl, nullptr, 4, &ctr);
+    d.counters = ctr;
+    float4 *part = nullptr;
+    rc |= dev_copy<float4>(pl, nullptr, (size_t)std::max<int64_t>(1, pl->nslots) * 64, &part);
+    d.part = part;
+    int64_t *gs = nullptr;
+    rc |= dev_copy(pl, gslot.data(), gslot.size(), &gs);
+    d.gslot = gs;
+    float4 *out = nullptr;
+    rc |= dev_copy<float4>(pl, nullptr, (size_t)nb, &out);
+    d.out = out;
+    unsigned *err = nullptr;
+    rc |= dev_copy<unsigned>(pl, nullptr, 1, &err);
+    d.err = err;
+    if (rc) {
+        grav_plan_free(pl);
+        return rc;
+    }
+    cudaMemset(err, 0, sizeof(unsigned));
+    d.ngroups = ng;
+    d.eps2 = (float)hp->eps2;
+    d.qsh = 0.5f * (hp->quad_phi_sign == 0.0f ? 1.0f : hp->quad_phi_sign);
+    d.box = hp->box;
+    pl->hp.points = nullptr;
+    pl->hp.qcells = nullptr;
+    pl->hp.hcells = nullptr;
+    pl->hp.groups = nullptr;
+    pl->hp.pptr = pl->hp.qptr = pl->hp.hptr = nullptr;
+    pl->hp.plist = nullptr;
+    pl->hp.qlist = pl->hp.hlist = nullptr;
+    *plan_out = pl;
+    return 0;
+}
+
+namespace {
+template <int KIND>
+int launch_kind(grav_plan *pl, cudaStream_t st) {
+    if (pl->dp.nitems[KIND] == 0)
+        return 0;
+    const int wpb = pl->tune.warps_per_block;
+    const size_t smem = (size_t)wpb * (2 * TILE * KindOf<KIND>::rec_bytes + 16);
+    GC_CHECK(cudaFuncSetAttribute(k_batch<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    int blocks = pl->tune.blocks_per_sm * pl->nsm;
+    blocks = std::min(blocks, (pl->dp.nitems[KIND] + wpb - 1) / wpb);
+    k_batch<KIND><<<blocks, wpb * 32, smem, st>>>(pl->dp);
+    GC_CHECK(cudaGetLastError());
+    pl->launches++;
+    return 0;
+}
+}  // namespace
+
+extern "C" int grav_groups_eval_CUDA(grav_plan *pl, void *stream) {
+    if (!pl)
+        return gc::set_status(-1, "grav_groups_eval_CUDA: no plan");
+    cudaStream_t st = (cudaStream_t)stream;
+    pl->launches = 0;
+    GC_CHECK(cudaMemsetAsync(pl->dp.counters, 0, 4 * sizeof(int), st));
+    if (int rc = launch_kind<KH>(pl, st))
+        return rc;
+    if (int rc = launch_kind<KQ>(pl, st))
+        return rc;
+    if (int rc = launch_kind<KP>(pl, st))
+        return rc;
+    const int wpb = 8;
+    k_reduce<<<(unsigned)((pl->dp.ngroups + wpb - 1) / wpb), wpb * 32, 0, st>>>(pl->dp);
+    GC_CHECK(cudaGetLastError());
+    pl->launches++;
+    return 0;
+}
+
+extern "C" int grav_groups_download_CUDA(grav_plan *pl, float *acc_phi) {
+    if (!pl || !acc_phi)
+        return gc::set_status(-1, "grav_groups_download_CUDA: bad arguments");
+    GC_CHECK(cudaMemcpy(acc_phi, pl->dp.out, (size_t)pl->hp.nbodies * sizeof(float4),
+                        cudaMemcpyDeviceToHost));
+    unsigned h = 0;
+    GC_CHECK(cudaMemcpy(&h, pl->dp.err, sizeof(h), cudaMemcpyDeviceToHost));
+    if (h) {
+        cudaMemset(pl->dp.err, 0, sizeof(unsigned));
+        return gc::set_status(-2, "batched kernels: device error word 0x%x", h);
+    }
+    return 0;
+}
+
+extern "C" float *grav_plan_output(grav_plan *pl) {
+    return pl ? reinterpret_cast<float *>(pl->dp.out) : nullptr;
+}
+
+extern "C" void grav_plan_counts(const grav_plan *pl, int64_t out[4]) {
+    for (int k = 0; k < 4; k++) out[k] = pl ? pl->counts[k] : 0;
+}
+
+extern "C" int grav_plan_launches(const grav_plan *pl) { return pl ? pl->launches : 0; }
+
+extern "C" void grav_plan_free(grav_plan *pl) {
+    if (!pl)
+        return;
+    for (void *p : pl->allocs) cudaFree(p);
+    delete pl;
+}
+
+extern "C" int grav_groups_CUDA(const grav_problem *hp, float *acc_phi) {
+    grav_plan *pl = nullptr;
+    if (int rc = grav_groups_upload_CUDA(hp, nullptr, &pl))
+        return rc;
+    int rc = grav_groups_eval_CUDA(pl, nullptr);
+    if (!rc)
+        rc = grav_groups_download_CUDA(pl, acc_phi);
+    grav_plan_free(pl);
+    return rc;
+}

@@ -1,0 +1,760 @@
+// nlnhost.cpp -- host tree build, FP64 moments, AREL critical radii, group MAC
+// walk and list packing (the producer side of the gravcuda.h boundary).
+//
+// Algorithms restated from the reference (file:line in lanl/ahotsph-2hot-apps):
+//   moments and their normalisation   nln/cofm.c:96-231, 398-420, 486-562
+//   AREL critical radii               nln/cofm.c:276-565, rcrit_poly/rtnewt 577-624
+//   MAC acceptance order m -> q -> h  nln/mac.c:1785-1805 (DLRcritMAC)
+//   leaf expansion to bodies          nln/mac.c:1817-1832
+//   completeness invariant            nln/mac.c:734-735
+//   image offsets                     nln/mac.c:91-111
+// The oct-tree itself comes from the absent 2hot libtree; this is a fresh
+// implementation (Morton keys, level-synchronous split).  The walk is a
+// group walk: every sink group (a tree cell with <= group_max bodies) keeps
+// one list, and the MAC distance is reduced by the group radius so that
+// every sink of the group satisfies the reference's per-sink test.
+#include "nlnhost.h"
+
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <parallel/algorithm>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err;
+
+struct Cell {
+    int64_t first;
+    int32_t count;
+    int32_t child;   // first child cell, -1 for a leaf
+    int32_t nchild;
+    int32_t level;
+    double gc[3];    // geometric cube centre
+    double side;     // cube side
+    double cen[3];   // expansion centre: centre of mass
+    double mass, bmax, B2, B4, B6;
+    double rc_m, rc_q, rc_h;
+};
+
+inline uint64_t spread3(uint32_t v) {
+    uint64_t x = v & 0x1fffff;
+    x = (x | x << 32) & 0x1f00000000ffffULL;
+    x = (x | x << 16) & 0x1f0000ff0000ffULL;
+    x = (x | x << 8) & 0x100f00f00f00f00fULL;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ULL;
+    x = (x | x << 2) & 0x1249249249249249ULL;
+    return x;
+}
+
+constexpr int KEY_LEVELS = 21;
+
+// Newton iteration on a polynomial sum_k a[k] r^k, started at x1 and stopped
+// when the step is below xacc; returns x1 when it does not converge in 30
+// steps (the behaviour of rtnewt, nln/cofm.c:602-624, with rcrit_poly's
+// Horner evaluation, nln/cofm.c:577-596).
+double newton_root(const double *a, int n, double x1, double xacc) {
+    double r = x1;
+    for (int it = 0; it < 30; it++) {
+        double p = a[n], dp = 0.0;
+        for (int k = n; k > 0; k--) {
+            dp = dp * r + p;
+            p = p * r + a[k - 1];
+        }
+        if (!std::isfinite(p) || !std::isfinite(dp) || dp == 0.0)
+            return x1;
+        double dx = p / dp;
+        r -= dx;
+        if (std::fabs(dx) < xacc)
+            return r;
+    }
+    return x1;
+}
+
+}  // namespace
+
+struct nln_tree {
+    nln_params p{};
+    int64_t n = 0;
+    double origin[3] = {0, 0, 0};
+    double side = 0;
+    std::vector<int64_t> order;
+    std::vector<float> spos;   // xyz in tree order
+    std::vector<float> smass;
+    std::vector<Cell> cells;
+    std::vector<float> points;  // float4
+    std::vector<nln_qcell> qc;
+    std::vector<nln_hcell> hc;
+    std::vector<nln_group> groups;
+    
+    std::vector<int64_t> lptr[3];
+    std::vector<nln_pseg> plist;
+    std::vector<uint32_t> qlist, hlist;
+    std::vector<int64_t> aptr[3];
+    std::vector<float> adata[3];
+    int64_t counts[4] = {0, 0, 0, 0};
+};
+
+extern "C" const char *nln_last_error(void) { return g_err.c_str(); }
+
+static int nthreads_of(const nln_params &p) {
+    return p.nthreads > 0 ? p.nthreads : omp_get_max_threads();
+}
+
+// ---------------------------------------------------------------- build
+static void build_cells(nln_tree *t, const std::vector<uint64_t> &keys) {
+    const int leaf_max = t->p.leaf_max;
+    Cell root{};
+    root.first = 0;
+    root.count = (int32_t)t->n;
+    root.child = -1;
+    root.level = 0;
+    for (int d = 0; d < 3; d++) root.gc[d] = t->origin[d] + 0.5 * t->side;
+    root.side = t->side;
+    t->cells.push_back(root);
+    std::vector<int32_t> frontier{0};
+    while (!frontier.empty()) {
+        const int64_t nf = (int64_t)frontier.size();
+        std::vector<int32_t> nkids(nf, 0);
+        std::vector<int64_t> bounds(nf * 9, 0);
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int64_t f = 0; f < nf; f++) {
+            const Cell &c = t->cells[frontier[f]];
+            if (c.count <= leaf_max || c.level >= KEY_LEVELS)
+                continue;
+            const int shift = 3 * (KEY_LEVELS - 1 - c.level);
+            int64_t lo = c.first, hi = c.first + c.count;
+            bounds[f * 9] = lo;
+            int nk = 0;
+            for (int o = 0; o < 8; o++) {
+                // first key whose octant digit exceeds o
+                int64_t a = lo, b = hi;
+                while (a < b) {
+                    int64_t mid = (a + b) / 2;
+                    if ((int)((keys[mid] >> shift) & 7) <= o)
+                        a = mid + 1;
+                    else
+                        b = mid;
+                }
+                bounds[f * 9 + o + 1] = a;
+                if (a > lo)
+                    nk++;
+                lo = a;
+            }
+            nkids[f] = nk;
+        }
+        std::vector<int64_t> off(nf + 1, 0);
+        for (int64_t f = 0; f < nf; f++) off[f + 1] = off[f] + nkids[f];
+        const int64_t base = (int64_t)t->cells.size();
+        t->cells.resize(base + off[nf]);
+        std::vector<int32_t> next(off[nf]);
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int64_t f = 0; f < nf; f++) {
+            if (!nkids[f])
+                continue;
+            Cell &c = t->cells[frontier[f]];
+            c.child = (int32_t)(base + off[f]);
+            c.nchild = nkids[f];
+            int k = 0;
+            for (int o = 0; o < 8; o++) {
+                int64_t lo = bounds[f * 9 + o], hi = bounds[f * 9 + o + 1];
+                if (hi <= lo)
+                    continue;
+                Cell d{};
+                d.first = lo;
+                d.count = (int32_t)(hi - lo);
+                d.child = -1;
+                d.level = c.level + 1;
+                d.side = 0.5 * c.side;
+                d.gc[0] = c.gc[0] + ((o >> 2) & 1 ? 0.25 : -0.25) * c.side;
+                d.gc[1] = c.gc[1] + ((o >> 1) & 1 ? 0.25 : -0.25) * c.side;
+                d.gc[2] = c.gc[2] + ((o >> 0) & 1 ? 0.25 : -0.25) * c.side;
+                t->cells[base + off[f] + k] = d;
+                next[off[f] + k] = (int32_t)(base + off[f] + k);
+                k++;
+            }
+        }
+        frontier.swap(next);
+    }
+}
+
+// FP64 moments about the centre of mass, directly from the bodies of each
+// cell, then the traceless R^-l normalisation of nln/cofm.c:398-420,486-562.
+static void compute_moments(nln_tree *t) {
+    const int64_t nc = (int64_t)t->cells.size();
+    t->qc.assign(nc, nln_qcell{});
+    t->hc.assign(nc, nln_hcell{});
+    t->points.resize((size_t)(t->n + nc) * 4);
+    for (int64_t i = 0; i < t->n; i++) {
+        for (int d = 0; d < 3; d++) t->points[4 * i + d] = t->spos[3 * i + d];
+        t->points[4 * i + 3] = t->smass[i];
+    }
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t ci = 0; ci < nc; ci++) {
+        Cell &c = t->cells[ci];
+        const float *P = t->spos.data() + 3 * c.first;
+        const float *M = t->smass.data() + c.first;
+        double m = 0, s[3] = {0, 0, 0};
+        for (int32_t k = 0; k < c.count; k++) {
+            m += M[k];
+            for (int d = 0; d < 3; d++) s[d] += M[k] * ((double)P[3 * k + d] - c.gc[d]);
+        }
+        for (int d = 0; d < 3; d++) c.cen[d] = c.gc[d] + (m > 0 ? s[d] / m : 0.0);
+        c.mass = m;
+        // raw moments about cen
+        double x2 = 0, xy = 0, xz = 0, y2 = 0, yz = 0, z2 = 0;
+        double x3 = 0, x2y = 0, x2z = 0, xy2 = 0, xyz = 0, xz2 = 0, y3 = 0, y2z = 0, yz2 = 0,
+               z3 = 0;
+        double x4 = 0, x3y = 0, x3z = 0, x2y2 = 0, x2yz = 0, x2z2 = 0, xy3 = 0, xy2z = 0,
+               xyz2 = 0, xz3 = 0, y4 = 0, y3z = 0, y2z2 = 0, yz3 = 0, z4 = 0;
+        double r2s = 0, r4s = 0, r6s = 0, bmax2 = 0;
+        for (int32_t k = 0; k < c.count; k++) {
+            const double w = M[k];
+            const double x = (double)P[3 * k] - c.cen[0];
+            const double y = (double)P[3 * k + 1] - c.cen[1];
+            const double z = (double)P[3 * k + 2] - c.cen[2];
+            const double xx = x * x, yy = y * y, zz = z * z, r2 = xx + yy + zz;
+            bmax2 = std::max(bmax2, r2);
+            r2s += w * r2;
+            r4s += w * r2 * r2;
+            r6s += w * r2 * r2 * r2;
+            x2 += w * xx; xy += w * x * y; xz += w * x * z;
+            y2 += w * yy; yz += w * y * z; z2 += w * zz;
+            x3 += w * xx * x; x2y += w * xx * y; x2z += w * xx * z;
+            xy2 += w * x * yy; xyz += w * x * y * z; xz2 += w * x * zz;
+            y3 += w * yy * y; y2z += w * yy * z; yz2 += w * y * zz; z3 += w * zz * z;
+            x4 += w * xx * xx; x3y += w * xx * x * y; x3z += w * xx * x * z;
+            x2y2 += w * xx * yy; x2yz += w * xx * y * z; x2z2 += w * xx * zz;
+            xy3 += w * x * yy * y; xy2z += w * x * yy * z; xyz2 += w * x * y * zz;
+            xz3 += w * x * zz * z; y4 += w * yy * yy; y3z += w * yy * y * z;
+            y2z2 += w * yy * zz; yz3 += w * y * zz * z; z4 += w * zz * zz;
+        }
+        c.bmax = std::sqrt(bmax2);
+        c.B2 = r2s;
+        c.B4 = r4s;
+        c.B6 = r6s;
+        const double ri = c.bmax > 0 ? 1.0 / c.bmax : 0.0;
+        // point-table monopole of the cell
+        float *pt = &t->points[4 * (t->n + ci)];
+        for (int d = 0; d < 3; d++) pt[d] = (float)c.cen[d];
+        pt[3] = (float)m;
+        // quadrupole, nln/cofm.c:398-420
+        double tq = (x2 + y2 + z2) / 3.0;
+        double q2[5] = {(x2 - tq) * ri * ri, xy * ri * ri, (y2 - tq) * ri * ri, xz * ri * ri,
+                        yz * ri * ri};
+        // octupole, nln/cofm.c:507-522
+        double tx = (x3 + xy2 + xz2) / 5.0, ty = (x2y + y3 + yz2) / 5.0,
+               tz = (x2z + y2z + z3) / 5.0;
+        double r3 = ri * ri * ri;
+        double q3[7] = {(x3 - 3.0 * tx) * r3, (x2y - ty) * r3, (xy2 - tx) * r3,
+                        (y3 - 3.0 * ty) * r3, (x2z - tz) * r3, xyz * r3,
+                        (y2z - tz) * r3};
+        // hexadecapole, nln/cofm.c:523-558
+        double txx = (x4 + x2y2 + x2z2) / 7.0, txy = (x3y + xy3 + xyz2) / 7.0,
+               txz = (x3z + xy2z + xz3) / 7.0, tyy = (x2y2 + y4 + y2z2) / 7.0,
+               tyz = (x2yz + y3z + yz3) / 7.0, tzz = (x2z2 + y2z2 + z4) / 7.0;
+        double tt = 0.1 * (txx + tyy + tzz);
+        double r4 = r3 * ri;
+        double q4[9] = {(x4 - 6.0 * (txx - tt)) * r4, (x3y - 3.0 * txy) * r4,
+                        (x2y2 - (txx + tyy - 2.0 * tt)) * r4, (xy3 - 3.0 * txy) * r4,
+                        (y4 - 6.0 * (tyy - tt)) * r4, (x3z - 3.0 * txz) * r4,
+                        (x2yz - tyz) * r4, (xy2z - txz) * r4, (y3z - 3.0 * tyz) * r4};
+        nln_qcell &q = t->qc[ci];
+        nln_hcell &h = t->hc[ci];
+        for (int d = 0; d < 3; d++) q.cen[d] = h.cen[d] = c.cen[d];
+        q.mass = h.mass = (float)m;
+        q.R = h.R = (float)c.bmax;
+        q.qxx = (float)q2[0];
+        q.qxy = (float)q2[1];
+        q.qyy = (float)q2[2];
+        q.qxz = (float)q2[3];
+        q.qyz = (float)q2[4];
+        for (int k = 0; k < 5; k++) h.q2[k] = (float)q2[k];
+        for (int k = 0; k < 7; k++) h.q3[k] = (float)q3[k];
+        for (int k = 0; k < 9; k++) h.q4[k] = (float)q4[k];
+    }
+}
+
+// AREL critical radii, nln/cofm.c:276-565 (ptol = tol: stol_max and
+// ptol_boost at their defaults).  A relative tolerance of 0 switches that
+// criterion off (the reference would divide by zero, cofm.c:322-335).
+static void compute_rcrit(nln_tree *t) {
+    const double ptol = t->p.tol, rel = t->p.rel_tol, rel0 = t->p.rel_tol0;
+    const int p2 = t->p.p2cut, p4 = t->p.p4cut;
+    const int64_t nc = (int64_t)t->cells.size();
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t ci = 0; ci < nc; ci++) {
+        Cell &c = t->cells[ci];
+        c.rc_m = c.rc_q = c.rc_h = 0.0;
+        if (c.B2 <= 0.0 || c.mass <= 0.0 || c.bmax <= 0.0)
+            continue;  // coincident bodies: every expansion is exact
+        const double b = c.bmax, m = c.mass, B2 = c.B2;
+        const double B3 = B2 * std::sqrt(B2 / m);  // lower bound, cofm.c:314
+        double a[10];
+        // monopole
+        double bh = 0.5 * b;
+        double rmax = bh + std::sqrt(bh * bh + std::sqrt(3.0 * B2 / ptol));
+        a[0] = 2 * B3; a[1] = -3 * B2; a[2] = 0; a[3] = ptol * b * b; a[4] = -2 * ptol * b;
+        a[5] = ptol;
+        double r_abs = newton_root(a, 5, rmax, 0.01 * rmax) + 0.01 * rmax;
+        double r_rel0 = 0.0, r_rel = INFINITY;
+        if (rel0 > 0) {
+            rmax = b + std::sqrt(3.0 / rel0 * B2 / m);
+            a[0] = 2 * B3; a[1] = -3 * B2 + rel0 * b * b * m; a[2] = -2 * rel0 * b * m;
+            a[3] = rel0 * m;
+            r_rel0 = newton_root(a, 3, rmax, 0.01 * rmax) + 0.01 * rmax;
+        }
+        if (rel > 0) {
+            rmax = b + std::sqrt(3.0 / rel * B2 / m);
+            a[0] = 2 * B3; a[1] = -3 * B2 + rel * b * b * m; a[2] = -2 * rel * b * m;
+            a[3] = rel * m;
+            r_rel = newton_root(a, 3, rmax, 0.01 * rmax) + 0.01 * rmax;
+        }
+        c.rc_m = std::max(std::min(r_abs, r_rel), r_rel0);
+        const double m_abs = r_abs, m_rel0 = r_rel0, m_rel = r_rel;
+        // quadrupole, cofm.c:442-485
+        if (p2 && c.count >= p2) {
+            const double B3q = b * B2, B4 = c.B4;  // upper bound, cofm.c:433
+            a[0] = 3 * B4; a[1] = -4 * B3q; a[2] = 0; a[3] = 0; a[4] = ptol * b * b;
+            a[5] = -2 * ptol * b; a[6] = ptol;
+            r_abs = newton_root(a, 6, m_abs, 0.01 * m_abs) + 0.01 * m_abs;
+            r_rel0 = 0.0;
+            r_rel = INFINITY;
+            if (rel0 > 0) {
+                a[0] = 3 * B4; a[1] = -4 * B3q; a[2] = rel0 * b * b * m; a[3] = -2 * rel0 * b * m;
+                a[4] = rel0 * m;
+                r_rel0 = newton_root(a, 4, m_rel0, 0.01 * m_rel0) + 0.01 * m_rel0;
+            }
+            if (rel > 0 && std::isfinite(m_rel)) {
+                a[0] = 3 * B4; a[1] = -4 * B3q; a[2] = rel * b * b * m; a[3] = -2 * rel * b * m;
+                a[4] = rel * m;
+                r_rel = newton_root(a, 4, m_rel, 0.01 * m_rel) + 0.01 * m_rel;
+            }
+            c.rc_q = std::max(std::min(r_abs, r_rel), r_rel0);
+        }
+        // order 4, cofm.c:489-505
+        if (p4 && c.count >= p4) {
+            const double B5 = b * c.B4, B6 = c.B6;
+            std::fill(a, a + 10, 0.0);
+            a[0] = 5 * B6; a[1] = -6 * B5; a[6] = ptol * b * b; a[7] = -2 * ptol * b; a[8] = ptol;
+            r_abs = newton_root(a, 8, m_abs, 0.001 * m_abs) + 0.001 * m_abs;
+            r_rel0 = 0.0;
+            r_rel = INFINITY;
+            if (rel0 > 0) {
+                std::fill(a, a + 10, 0.0);
+                a[0] = 5 * B6; a[1] = -6 * B5; a[4] = rel0 * b * b * m; a[5] = -2 * rel0 * b * m;
+                a[6] = rel0 * m;
+                r_rel0 = newton_root(a, 6, m_rel0, 0.001 * m_rel0) + 0.001 * m_rel0;
+            }
+            if (rel > 0 && std::isfinite(m_rel)) {
+                std::fill(a, a + 10, 0.0);
+                a[0] = 5 * B6; a[1] = -6 * B5; a[4] = rel * b * b * m; a[5] = -2 * rel * b * m;
+                a[6] = rel * m;
+                r_rel = newton_root(a, 6, m_rel, 0.001 * m_rel) + 0.001 * m_rel;
+            }
+            c.rc_h = std::max(std::min(r_abs, r_rel), r_rel0);
+        }
+    }
+}
+
+// Sink groups: the largest cells with <= group_max bodies, then consecutive
+// sibling cells merged while the merged group still holds <= group_max
+// bodies (siblings are adjacent in key order, so a merged group is still one
+// contiguous run of sinks inside its parent's cube).
+static void collect_groups(nln_tree *t) {
+    const int gmax = t->p.group_max;
+    struct Run {
+        int64_t first;
+        int32_t count;
+    };
+    std::vector<Run> runs;
+    std::vector<int32_t> stack{0};
+    while (!stack.empty()) {
+        int32_t ci = stack.back();
+        stack.pop_back();
+        const Cell &c = t->cells[ci];
+        if (c.count <= gmax || c.child < 0) {
+            runs.push_back(Run{c.first, c.count});
+            continue;
+        }
+        // children of c that are small enough: merge adjacent ones greedily
+        std::vector<Run> merged;
+        std::vector<int32_t> big;
+        for (int k = 0; k < c.nchild; k++) {
+            const Cell &d = t->cells[c.child + k];
+            if (d.count > gmax && d.child >= 0) {
+                big.push_back(c.child + k);
+                continue;
+            }
+            if (!merged.empty() && merged.back().first + merged.back().count == d.first &&
+                merged.back().count + d.count <= gmax)
+                merged.back().count += d.count;
+            else
+                merged.push_back(Run{d.first, d.count});
+        }
+        runs.insert(runs.end(), merged.begin(), merged.end());
+        for (auto it = big.rbegin(); it != big.rend(); ++it) stack.push_back(*it);
+    }
+    std::sort(runs.begin(), runs.end(), [](const Run &a, const Run &b) { return a.first < b.first; });
+    t->groups.resize(runs.size());
+#pragma omp parallel for schedule(static)
+    for (size_t g = 0; g < runs.size(); g++) {
+        nln_group &G = t->groups[g];
+        const float *P = t->spos.data() + 3 * runs[g].first;
+        const float *M = t->smass.data() + runs[g].first;
+        double m = 0, s[3] = {0, 0, 0};
+        for (int32_t k = 0; k < runs[g].count; k++) {
+            m += M[k];
+            for (int d = 0; d < 3; d++) s[d] += M[k] * (double)P[3 * k + d];
+        }
+        double r2max = 0;
+        for (int d = 0; d < 3; d++) G.cen[d] = m > 0 ? s[d] / m : (double)P[d];
+        for (int32_t k = 0; k < runs[g].count; k++) {
+            double r2 = 0;
+            for (int d = 0; d < 3; d++) {
+                double x = (double)P[3 * k + d] - G.cen[d];
+                r2 += x * x;
+            }
+            r2max = std::max(r2max, r2);
+        }
+        G.first = runs[g].first;
+        G.count = runs[g].count;
+        G.radius = (float)(std::sqrt(r2max) * (1.0 + 1e-6));
+    }
+}
+
+extern "C" nln_tree *nln_tree_build(const float *pos, int stride, const float *mass, int mstride,
+                                    int64_t n, const nln_params *p) {
+    if (!pos || !mass || !p || n <= 0 || stride < 3 || mstride < 1) {
+        g_err = "nln_tree_build: bad arguments";
+        return nullptr;
+    }
+    if (p->leaf_max < 1 || p->leaf_max > 65535 || p->group_max < 1 || p->group_max > 64 ||
+        p->tol <= 0.0 || p->p2cut < 0 || p->p4cut < 0) {
+        g_err = "nln_tree_build: bad parameters (leaf_max 1..65535, group_max 1..64, tol > 0)";
+        return nullptr;
+    }
+    if (n + 1 >= (int64_t)NLN_IDX_MASK) {
+        g_err = "nln_tree_build: too many bodies for 27-bit list indices";
+        return nullptr;
+    }
+    nln_tree *t = new nln_tree();
+    t->p = *p;
+    t->n = n;
+    const int nth = nthreads_of(*p);
+    omp_set_num_threads(nth);
+    // bounding cube
+    if (p->box > 0) {
+        for (int64_t i = 0; i < n; i++)
+            for (int d = 0; d < 3; d++) {
+                float x = pos[i * stride + d];
+                if (!(x >= 0.0f && (double)x < p->box)) {
+                    g_err = "nln_tree_build: periodic body outside [0, box)";
+                    delete t;
+                    return nullptr;
+                }
+            }
+        t->side = p->box;
+    } else {
+        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int64_t i = 0; i < n; i++)
+            for (int d = 0; d < 3; d++) {
+                double x = pos[i * stride + d];
+                if (!std::isfinite(x)) {
+                    g_err = "nln_tree_build: non-finite position";
+                    delete t;
+                    return nullptr;
+                }
+                lo[d] = std::min(lo[d], x);
+                hi[d] = std::max(hi[d], x);
+            }
+        double ext = 0;
+        for (int d = 0; d < 3; d++) ext = std::max(ext, hi[d] - lo[d]);
+        ext = ext > 0 ? ext * (1.0 + 1e-5) : 1.0;
+        for (int d = 0; d < 3; d++) t->origin[d] = 0.5 * (lo[d] + hi[d]) - 0.5 * ext;
+        t->side = ext;
+    }
+    // keys + sort
+    struct KI {
+        uint64_t k;
+        int64_t i;
+    };
+    std::vector<KI> ki(n);
+    const double scale = (double)(1u << KEY_LEVELS) / t->side;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) {
+        uint32_t c[3];
+        for (int d = 0; d < 3; d++) {
+            double u = ((double)pos[i * stride + d] - t->origin[d]) * scale;
+            int64_t v = (int64_t)std::floor(u);
+            v = std::min<int64_t>(std::max<int64_t>(v, 0), (1 << KEY_LEVELS) - 1);
+            c[d] = (uint32_t)v;
+        }
+        ki[i].k = spread3(c[0]) << 2 | spread3(c[1]) << 1 | spread3(c[2]);
+        ki[i].i = i;
+    }
+    __gnu_parallel::sort(ki.begin(), ki.end(), [](const KI &a, const KI &b) {
+        return a.k < b.k || (a.k == b.k && a.i < b.i);
+    });
+    std::vector<uint64_t> keys(n);
+    t->order.resize(n);
+    t->spos.resize(3 * n);
+    t->smass.resize(n);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) {
+        keys[i] = ki[i].k;
+        int64_t j = ki[i].i;
+        t->order[i] = j;
+        for (int d = 0; d < 3; d++) t->spos[3 * i + d] = pos[j * stride + d];
+        t->smass[i] = mass[j * mstride];
+    }
+    build_cells(t, keys);
+    compute_moments(t);
+    compute_rcrit(t);
+    collect_groups(t);
+    return t;
+}
+
+extern "C" void nln_tree_free(nln_tree *t) { delete t; }
+
+// ---------------------------------------------------------------- walk
+namespace {
+
+struct GroupLists {
+    std::vector<nln_pseg> p;
+    std::vector<uint32_t> q, h;
+    int64_t nb = 0, nm = 0;
+};
+
+inline uint16_t shift_code(const int s[3]) {
+    return (uint16_t)((s[0] + 1) * 9 + (s[1] + 1) * 3 + (s[2] + 1));
+}
+
+}  // namespace
+
+static void walk_group(const nln_tree *t, const nln_group &G, GroupLists &L,
+                       std::vector<int32_t> &stack) {
+    const double box = t->p.box;
+    const int p2 = t->p.p2cut, p4 = t->p.p4cut;
+    int64_t covered = 0;
+    stack.clear();
+    stack.push_back(0);
+    while (!stack.empty()) {
+        const int32_t ci = stack.back();
+        stack.pop_back();
+        const Cell &c = t->cells[ci];
+        double y[3];
+        int s[3] = {0, 0, 0};
+        for (int d = 0; d < 3; d++) {
+            y[d] = c.cen[d] - G.cen[d];
+            if (box > 0) {
+                s[d] = -(int)std::nearbyint(y[d] / box);
+                y[d] += s[d] * box;
+            }
+        }
+        const double dist = std::sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
+        // Periodic: the cell is taken whole in the image nearest the group
+        // centre.  Every sink-body displacement it implies must stay inside
+        // the domain of the Ewald correction, |y_k| <= NLN_EWALD_REACH * box,
+        // where the correction is smooth; otherwise the cell is opened.
+        bool inside = true;
+        if (box > 0) {
+            double ym = std::max(std::fabs(y[0]), std::max(std::fabs(y[1]), std::fabs(y[2])));
+            inside = ym + c.bmax + G.radius <= NLN_EWALD_REACH * box;
+        }
+        const double dd = dist - G.radius;
+        const uint16_t sc = shift_code(s);
+        if (inside && c.count > 0) {
+            if (dd > c.rc_m + c.bmax) {
+                L.p.push_back(nln_pseg{(uint32_t)(t->n + ci), 1, sc});
+                L.nm++;
+                covered += c.count;
+                continue;
+            }
+            if (p2 && c.count >= p2 && dd > c.rc_q + c.bmax) {
+                L.q.push_back((uint32_t)ci | ((uint32_t)sc << NLN_IDX_BITS));
+                covered += c.count;
+                continue;
+            }
+            if (p4 && c.count >= p4 && dd > c.rc_h + c.bmax) {
+                L.h.push_back((uint32_t)ci | ((uint32_t)sc << NLN_IDX_BITS));
+                covered += c.count;
+                continue;
+            }
+        }
+        if (c.child >= 0) {
+            for (int k = c.nchild - 1; k >= 0; k--) stack.push_back(c.child + k);
+            continue;
+        }
+        // leaf: expand to bodies (nln/mac.c:1817-1832)
+        if (inside || box <= 0) {
+            L.p.push_back(nln_pseg{(uint32_t)c.first, (uint16_t)c.count, sc});
+        } else {
+            // a leaf straddling the group's half-box: each body its own image
+            for (int32_t k = 0; k < c.count; k++) {
+                const float *x = &t->spos[3 * (c.first + k)];
+                int sb[3];
+                for (int d = 0; d < 3; d++) sb[d] = -(int)std::nearbyint((x[d] - G.cen[d]) / box);
+                uint16_t scb = shift_code(sb);
+                if (!L.p.empty() && L.p.back().shift == scb &&
+                    L.p.back().base + L.p.back().len == (uint32_t)(c.first + k) &&
+                    L.p.back().len < 65535 && L.p.back().base < (uint32_t)t->n)
+                    L.p.back().len++;
+                else
+                    L.p.push_back(nln_pseg{(uint32_t)(c.first + k), 1, scb});
+            }
+        }
+        L.nb += c.count;
+        covered += c.count;
+    }
+    if (covered != t->n) {
+        std::fprintf(stderr, "nln_tree_walk: group at %lld covers %lld of %lld bodies\n",
+                     (long long)G.first, (long long)covered, (long long)t->n);
+        std::abort();
+    }
+}
+
+static void emit_aosoa(nln_tree *t, const std::vector<GroupLists> &GL) {
+    const int64_t ng = (int64_t)t->groups.size();
+    const int SZ[3] = {4, 13, 29};
+    const double box = t->p.box;
+    for (int kind = 0; kind < 3; kind++) {
+        std::vector<int64_t> &ptr = t->aptr[kind];
+        ptr.assign(ng + 1, 0);
+        for (int64_t g = 0; g < ng; g++) {
+            int64_t nrec = 0;
+            if (kind == 0)
+                for (const nln_pseg &s : GL[g].p) nrec += s.len;
+            else
+                nrec = (int64_t)(kind == 1 ? GL[g].q.size() : GL[g].h.size());
+            ptr[g + 1] = ptr[g] + (nrec + 7) / 8;
+        }
+        t->adata[kind].assign((size_t)ptr[ng] * SZ[kind] * 8, 0.0f);
+    }
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t g = 0; g < ng; g++) {
+        // M list: bodies and monopole cells, [m, x, y, z]
+        {
+            float *f = t->adata[0].data() + (size_t)t->aptr[0][g] * 4 * 8;
+            int64_t r = 0;
+            for (const nln_pseg &s : GL[g].p) {
+                int sh[3] = {(int)s.shift / 9 - 1, (int)(s.shift / 3) % 3 - 1, (int)s.shift % 3 - 1};
+                for (uint32_t k = 0; k < s.len; k++, r++) {
+                    const float *pt = &t->points[4 * ((size_t)s.base + k)];
+                    float *blk = f + (r / 8) * 4 * 8;
+                    int l = (int)(r % 8);
+                    blk[0 * 8 + l] = pt[3];
+                    for (int d = 0; d < 3; d++)
+                        blk[(1 + d) * 8 + l] = (float)((double)pt[d] + sh[d] * box);
+                }
+            }
+        }
+        for (int kind = 1; kind < 3; kind++) {
+            const std::vector<uint32_t> &lst = kind == 1 ? GL[g].q : GL[g].h;
+            const int sz = SZ[kind];
+            float *f = t->adata[kind].data() + (size_t)t->aptr[kind][g] * sz * 8;
+            for (size_t r = 0; r < lst.size(); r++) {
+                uint32_t ci = lst[r] & NLN_IDX_MASK, sc = lst[r] >> NLN_IDX_BITS;
+                int sh[3] = {(int)sc / 9 - 1, (int)(sc / 3) % 3 - 1, (int)sc % 3 - 1};
+                const nln_hcell &h = t->hc[ci];
+                float *blk = f + (r / 8) * sz * 8;
+                int l = (int)(r % 8);
+                blk[0 * 8 + l] = h.mass;
+                for (int d = 0; d < 3; d++) blk[(1 + d) * 8 + l] = (float)(h.cen[d] + sh[d] * box);
+                blk[4 * 8 + l] = h.R;
+                for (int k = 0; k < 5; k++) blk[(8 + k) * 8 + l] = h.q2[k];
+                if (kind == 2) {
+                    for (int k = 0; k < 7; k++) blk[(13 + k) * 8 + l] = h.q3[k];
+                    for (int k = 0; k < 9; k++) blk[(20 + k) * 8 + l] = h.q4[k];
+                }
+            }
+        }
+    }
+}
+
+extern "C" int nln_tree_walk(nln_tree *t) {
+    if (!t)
+        return -1;
+    omp_set_num_threads(nthreads_of(t->p));
+    const int64_t ng = (int64_t)t->groups.size();
+    std::vector<GroupLists> GL(ng);
+#pragma omp parallel
+    {
+        std::vector<int32_t> stack;
+        stack.reserve(1024);
+#pragma omp for schedule(dynamic, 8)
+        for (int64_t g = 0; g < ng; g++) walk_group(t, t->groups[g], GL[g], stack);
+    }
+    for (int k = 0; k < 3; k++) t->lptr[k].assign(ng + 1, 0);
+    int64_t cnt[4] = {0, 0, 0, 0};
+    for (int64_t g = 0; g < ng; g++) {
+        t->lptr[0][g + 1] = t->lptr[0][g] + (int64_t)GL[g].p.size();
+        t->lptr[1][g + 1] = t->lptr[1][g] + (int64_t)GL[g].q.size();
+        t->lptr[2][g + 1] = t->lptr[2][g] + (int64_t)GL[g].h.size();
+        const int64_t gc = t->groups[g].count;
+        cnt[0] += gc * GL[g].nb;
+        cnt[1] += gc * GL[g].nm;
+        cnt[2] += gc * (int64_t)GL[g].q.size();
+        cnt[3] += gc * (int64_t)GL[g].h.size();
+    }
+    std::memcpy(t->counts, cnt, sizeof(cnt));
+    t->plist.resize(t->lptr[0][ng]);
+    t->qlist.resize(t->lptr[1][ng]);
+    t->hlist.resize(t->lptr[2][ng]);
+#pragma omp parallel for schedule(static)
+    for (int64_t g = 0; g < ng; g++) {
+        std::copy(GL[g].p.begin(), GL[g].p.end(), t->plist.begin() + t->lptr[0][g]);
+        std::copy(GL[g].q.begin(), GL[g].q.end(), t->qlist.begin() + t->lptr[1][g]);
+        std::copy(GL[g].h.begin(), GL[g].h.end(), t->hlist.begin() + t->lptr[2][g]);
+    }
+    if (t->p.emit_aosoa)
+        emit_aosoa(t, GL);
+    return 0;
+}
+
+// ---------------------------------------------------------------- accessors
+extern "C" int64_t nln_nbodies(const nln_tree *t) { return t->n; }
+extern "C" int64_t nln_ncells(const nln_tree *t) { return (int64_t)t->cells.size(); }
+extern "C" int64_t nln_ngroups(const nln_tree *t) { return (int64_t)t->groups.size(); }
+extern "C" const int64_t *nln_order(const nln_tree *t) { return t->order.data(); }
+extern "C" const float *nln_points(const nln_tree *t) { return t->points.data(); }
+extern "C" const nln_qcell *nln_qcells(const nln_tree *t) { return t->qc.data(); }
+extern "C" const nln_hcell *nln_hcells(const nln_tree *t) { return t->hc.data(); }
+extern "C" const nln_group *nln_groups(const nln_tree *t) { return t->groups.data(); }
+extern "C" const float *nln_sorted_pos(const nln_tree *t) { return t->spos.data(); }
+
+extern "C" const int64_t *nln_list_ptr(const nln_tree *t, int kind) {
+    return (kind >= 0 && kind < 3 && !t->lptr[kind].empty()) ? t->lptr[kind].data() : nullptr;
+}
+extern "C" const void *nln_list_data(const nln_tree *t, int kind) {
+    if (kind == 0)
+        return t->plist.data();
+    if (kind == 1)
+        return t->qlist.data();
+    if (kind == 2)
+        return t->hlist.data();
+    return nullptr;
+}
+extern "C" int64_t nln_list_len(const nln_tree *t, int kind) {
+    if (kind == 0)
+        return (int64_t)t->plist.size();
+    if (kind == 1)
+        return (int64_t)t->qlist.size();
+    if (kind == 2)
+        return (int64_t)t->hlist.size();
+    return -1;
+}
+extern "C" void nln_counts(const nln_tree *t, int64_t out[4]) {
+    std::memcpy(out, t->counts, sizeof(t->counts));
+}
+extern "C" const int64_t *nln_aosoa_ptr(const nln_tree *t, int kind) {
+    return (kind >= 0 && kind < 3 && !t->aptr[kind].empty()) ? t->aptr[kind].data() : nullptr;
+}
+extern "C" const float *nln_aosoa_data(const nln_tree *t, int kind) {
+    return (kind >= 0 && kind < 3 && !t->adata[kind].empty()) ? t->adata[kind].data() : nullptr;
+}

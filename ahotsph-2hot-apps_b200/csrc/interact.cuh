@@ -1,0 +1,206 @@
+// interact.cuh -- one sink against one staged source record, FP32.
+//
+// The arithmetic is the reference's multipole recurrence
+// (do_gravph_avx8, nln/do_grav_avx8.c:1779-1904; pH, nln/pgrav.cu:49-213):
+// with d = sink - source and the normalised traceless moments q_l / R^l,
+// order l contributes
+//     eq  = t_l * (q_l contracted with d^(l-1)),   t_l = -(2l-1)!! R^l / r^(2l+1)
+//     phi += c_l eq.d,          c_l = 1/2, 1/3, 1/4
+//     a   += d (2l+1) c_l eq.d / r^2 - eq
+// The constant -(2l-1)!! R^l is folded into the moments once per source when
+// a tile is staged (stage_* below), so the inner loop only multiplies by
+// powers of 1/r.  Staged record layouts (floats, 16-byte aligned):
+//   P (points, 4):      x y z m
+//   Q (quadrupole, 12): x y z m | Qxx Qxy Qyy Qxz Qyz Qzz | - -
+//   H (order 4, 32):    x y z m | Qxx Qxy Qyy Qxz Qyz Qzz | O[7] Osum1 Osum2 |
+//                       X[9] Xsum | - - -
+// with Q = -3 R^2 q2, O = -15 R^3 q3, X = -105 R^4 q4 and the sums
+// Qzz = -(Qxx+Qyy), Osum1 = Oxxx+Oxyy, Osum2 = Oxxy+Oyyy, Xsum = Xxyyy+Xxxxy.
+#pragma once
+
+#include "common.cuh"
+
+constexpr int REC_P = 4, REC_Q = 12, REC_H = 32;
+
+struct Acc4 {
+    float ax, ay, az, phi;
+};
+
+// Softening laws of the monopole term.
+enum Soft { SOFT_PLUMMER = 0, SOFT_NONE = 1, SOFT_MASKED = 2, SOFT_K1 = 3 };
+
+// Staging: raw fields -> folded record.  q2[5], q3[7], q4[9] in the
+// reference order (qxx qxy qyy qxz qyz; qxxx qxxy qxyy qyyy qxxz qxyz qyyz;
+// qxxxx qxxxy qxxyy qxyyy qyyyy qxxxz qxxyz qxyyz qyyyz).
+__device__ __forceinline__ void stage_quad(float *o, float R, const float *q2) {
+    const float c2 = -3.0f * R * R;
+    float Qxx = c2 * q2[0], Qxy = c2 * q2[1], Qyy = c2 * q2[2], Qxz = c2 * q2[3],
+          Qyz = c2 * q2[4];
+    o[4] = Qxx;
+    o[5] = Qxy;
+    o[6] = Qyy;
+    o[7] = Qxz;
+    o[8] = Qyz;
+    o[9] = -(Qxx + Qyy);
+    o[10] = 0.0f;
+    o[11] = 0.0f;
+}
+
+__device__ __forceinline__ void stage_hexa(float *o, float R, const float *q3, const float *q4) {
+    const float c3 = -15.0f * R * R * R;
+    const float c4 = -105.0f * R * R * R * R;
+    float O[7], X[9];
+#pragma unroll
+    for (int k = 0; k < 7; k++) O[k] = c3 * q3[k];
+#pragma unroll
+    for (int k = 0; k < 9; k++) X[k] = c4 * q4[k];
+#pragma unroll
+    for (int k = 0; k < 7; k++) o[12 + k] = O[k];
+    o[19] = O[0] + O[2];  // Oxxx + Oxyy
+    o[20] = O[1] + O[3];  // Oxxy + Oyyy
+#pragma unroll
+    for (int k = 0; k < 9; k++) o[21 + k] = X[k];
+    o[30] = X[3] + X[1];  // Xxyyy + Xxxxy
+    o[31] = 0.0f;
+}
+
+// Monopole term.  Returns ri (1/r) and ri2 for the higher orders.
+template <int SOFT>
+__device__ __forceinline__ void mono(float x, float y, float z, float m, float e, Acc4 &a,
+                                     float &ri, float &ri2) {
+    if (SOFT == SOFT_PLUMMER) {
+        // nln/do_grav_avx8.c:2181-2210, e = eps^2
+        float r2 = fmaf(x, x, fmaf(y, y, fmaf(z, z, e)));
+        ri = rsqrt_fast(r2);
+        ri2 = ri * ri;
+        float mri = m * ri;
+        float mri3 = mri * ri2;
+        a.phi -= mri;
+        a.ax = fmaf(-x, mri3, a.ax);
+        a.ay = fmaf(-y, mri3, a.ay);
+        a.az = fmaf(-z, mri3, a.az);
+    } else if (SOFT == SOFT_NONE) {
+        float r2 = fmaf(x, x, fmaf(y, y, z * z));
+        ri = rsqrt_fast(r2);
+        ri2 = ri * ri;
+        float mri = m * ri;
+        float mri3 = mri * ri2;
+        a.phi -= mri;
+        a.ax = fmaf(-x, mri3, a.ax);
+        a.ay = fmaf(-y, mri3, a.ay);
+        a.az = fmaf(-z, mri3, a.az);
+    } else if (SOFT == SOFT_MASKED) {
+        // do_grav_avx8: pairs closer than e contribute nothing (nln/do_grav_avx8.c:978-990)
+        float r2 = fmaf(x, x, fmaf(y, y, z * z));
+        ri = (r2 >= e * e) ? rsqrt_fast(r2) : 0.0f;
+        ri2 = ri * ri;
+        float mri = m * ri;
+        float mri3 = mri * ri2;
+        a.phi -= mri;
+        a.ax = fmaf(-x, mri3, a.ax);
+        a.ay = fmaf(-y, mri3, a.ay);
+        a.az = fmaf(-z, mri3, a.az);
+    } else {
+        // Dehnen K1 inside r < eps, e = 1/eps (nln/do_grav_avx8.c:1013-1045, nln/pgrav.cu:441-461)
+        float r2 = fmaf(x, x, fmaf(y, y, z * z));
+        float pf, af;
+        if (r2 * e * e < 1.0f) {
+            float u2 = fmaf(r2, e * e, -1.0f);
+            pf = fmaf(fmaf(fmaf(-45.0f / 32.0f, u2, 3.0f / 8.0f), u2, -0.5f), u2, 1.0f) * e;
+            af = fmaf(fmaf(135.0f / 16.0f, u2, -1.5f), u2, 1.0f) * e * e * e;
+            ri = 0.0f;
+        } else {
+            ri = rsqrt_fast(r2);
+            pf = ri;
+            af = ri * ri * ri;
+        }
+        ri2 = ri * ri;
+        a.phi = fmaf(-m, pf, a.phi);
+        float maf = m * af;
+        a.ax = fmaf(-x, maf, a.ax);
+        a.ay = fmaf(-y, maf, a.ay);
+        a.az = fmaf(-z, maf, a.az);
+    }
+}
+
+// Quadrupole term; qsh = quadrupole potential sign times 1/2.
+__device__ __forceinline__ void quad(float x, float y, float z, const float *__restrict__ r,
+                                     float ri, float ri2, float qsh, Acc4 &a, float &ri5) {
+    const float4 q0 = *reinterpret_cast<const float4 *>(r + 4);  // Qxx Qxy Qyy Qxz
+    const float2 q1 = *reinterpret_cast<const float2 *>(r + 8);  // Qyz Qzz
+    float Qx = fmaf(q0.x, x, fmaf(q0.y, y, q0.w * z));
+    float Qy = fmaf(q0.y, x, fmaf(q0.z, y, q1.x * z));
+    float Qz = fmaf(q0.w, x, fmaf(q1.x, y, q1.y * z));
+    float dQd = fmaf(x, Qx, fmaf(y, Qy, z * Qz));
+    float ri3 = ri * ri2;
+    ri5 = ri3 * ri2;
+    float eqd = ri5 * dQd;                  // eq . d
+    a.phi = fmaf(qsh, eqd, a.phi);
+    float k = 2.5f * eqd * ri2;             // 5 * (1/2) eq.d / r^2
+    a.ax = fmaf(x, k, fmaf(-ri5, Qx, a.ax));
+    a.ay = fmaf(y, k, fmaf(-ri5, Qy, a.ay));
+    a.az = fmaf(z, k, fmaf(-ri5, Qz, a.az));
+}
+
+// Octupole + hexadecapole terms (nln/do_grav_avx8.c:1853-1898).
+__device__ __forceinline__ void hexa(float x, float y, float z, const float *__restrict__ r,
+                                     float ri2, float ri5, Acc4 &a) {
+    const float4 o0 = *reinterpret_cast<const float4 *>(r + 12);  // Oxxx Oxxy Oxyy Oyyy
+    const float4 o1 = *reinterpret_cast<const float4 *>(r + 16);  // Oxxz Oxyz Oyyz S1
+    const float4 o2 = *reinterpret_cast<const float4 *>(r + 20);  // S2 Xxxxx Xxxxy Xxxyy
+    const float4 x0 = *reinterpret_cast<const float4 *>(r + 24);  // Xxyyy Xyyyy Xxxxz Xxxyz
+    const float4 x1 = *reinterpret_cast<const float4 *>(r + 28);  // Xxyyz Xyyyz XS -
+    const float third = 1.0f / 3.0f;
+    float xx = 0.5f * x * x, yy = 0.5f * y * y, zz = 0.5f * z * z;
+    float xy = x * y, xz = x * z, yz = y * z;
+    float xxx = x * fmaf(xx, third, -zz);
+    float xxz = z * fmaf(zz, -third, xx);
+    float yyy = y * fmaf(yy, third, -zz);
+    float yyz = z * fmaf(zz, -third, yy);
+    xx -= zz;
+    yy -= zz;
+    // octupole
+    float e0 = fmaf(o0.x, xx, fmaf(o0.z, yy, fmaf(o0.y, xy, fmaf(o1.x, xz, o1.y * yz))));
+    float e1 = fmaf(o0.z, xy, fmaf(o0.y, xx, fmaf(o0.w, yy, fmaf(o1.z, yz, o1.y * xz))));
+    float e2 = fmaf(-o1.w, xz, fmaf(-o2.x, yz, fmaf(o1.x, xx, fmaf(o1.z, yy, o1.y * xy))));
+    float ri7 = ri5 * ri2;
+    float eqd = ri7 * fmaf(x, e0, fmaf(y, e1, z * e2));
+    a.phi = fmaf(third, eqd, a.phi);
+    float k = (7.0f / 3.0f) * eqd * ri2;
+    a.ax = fmaf(x, k, fmaf(-ri7, e0, a.ax));
+    a.ay = fmaf(y, k, fmaf(-ri7, e1, a.ay));
+    a.az = fmaf(z, k, fmaf(-ri7, e2, a.az));
+    // hexadecapole
+    float xxy = y * xx, xyy = x * yy, xyz = xy * z;
+    // X order: xxxx(o2.y) xxxy(o2.z) xxyy(o2.w) xyyy(x0.x) yyyy(x0.y) xxxz(x0.z) xxyz(x0.w)
+    //          xyyz(x1.x) yyyz(x1.y), XS = xyyy + xxxy (x1.z)
+    float h0 = fmaf(o2.y, xxx, fmaf(x0.x, yyy, fmaf(o2.z, xxy, fmaf(x0.z, xxz,
+               fmaf(o2.w, xyy, fmaf(x0.w, xyz, x1.x * yyz))))));
+    float h1 = fmaf(x0.x, xyy, fmaf(o2.z, xxx, fmaf(x0.y, yyy, fmaf(x1.y, yyz,
+               fmaf(o2.w, xxy, fmaf(x0.w, xxz, x1.x * xyz))))));
+    float h2 = fmaf(-o2.y, xxz, fmaf(-x1.z, xyz, fmaf(-x0.y, yyz, fmaf(x0.z, xxx,
+               fmaf(x1.y, yyy, fmaf(-o2.w, xxz + yyz, fmaf(x0.w, xxy, x1.x * xyy)))))));
+    float ri9 = ri7 * ri2;
+    float hqd = ri9 * fmaf(x, h0, fmaf(y, h1, z * h2));
+    a.phi = fmaf(0.25f, hqd, a.phi);
+    float kh = 2.25f * hqd * ri2;
+    a.ax = fmaf(x, kh, fmaf(-ri9, h0, a.ax));
+    a.ay = fmaf(y, kh, fmaf(-ri9, h1, a.ay));
+    a.az = fmaf(z, kh, fmaf(-ri9, h2, a.az));
+}
+
+// One staged record of order ORDER (0, 2, 4) against a sink at (sx, sy, sz).
+template <int ORDER, int SOFT>
+__device__ __forceinline__ void interact(const float *__restrict__ r, float sx, float sy,
+                                         float sz, float e, float qsh, Acc4 &a) {
+    const float4 p = *reinterpret_cast<const float4 *>(r);
+    float x = sx - p.x, y = sy - p.y, z = sz - p.z;
+    float ri, ri2;
+    mono<SOFT>(x, y, z, p.w, e, a, ri, ri2);
+    if (ORDER >= 2) {
+        float ri5;
+        quad(x, y, z, r, ri, ri2, qsh, a, ri5);
+        if (ORDER >= 4)
+            hexa(x, y, z, r, ri2, ri5, a);
+    }
+}

@@ -1,0 +1,91 @@
+"""In-tree build of the native libraries (no JIT cache: the .so files live next
+to this file so they travel with the repository snapshot).
+
+* ``lib/libnlnhost.so``  host tree / moments / MAC walk / list packing (g++, OpenMP)
+* ``lib/libgravcuda.so`` the gravcuda.h C ABI and its sm_100a kernels (nvcc)
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)                 # the ahotsph-2hot-apps_b200 directory
+REPO = os.path.dirname(ROOT)
+CSRC = os.path.join(ROOT, "csrc")
+INCLUDE = os.path.join(REPO, "include")
+LIBDIR = os.path.join(PKG, "lib")
+HOST_SO = os.path.join(LIBDIR, "libnlnhost.so")
+CUDA_SO = os.path.join(LIBDIR, "libgravcuda.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _cxx():
+    # the image exports CXX=/opt/gcc/bin/g++, a wrapper without OpenMP
+    return "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+
+
+def _nvcc():
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _newer(target, sources):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources)
+
+
+def _run(cmd):
+    print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+
+
+def host_sources():
+    d = os.path.join(CSRC, "host")
+    return sorted(os.path.join(d, f) for f in os.listdir(d) if f.endswith(".cpp"))
+
+
+def cuda_sources():
+    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+
+
+def cuda_headers():
+    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h")))
+
+
+def build_host(force=False):
+    os.makedirs(LIBDIR, exist_ok=True)
+    srcs = host_sources()
+    deps = srcs + [os.path.join(INCLUDE, "nlnhost.h")]
+    if force or _newer(HOST_SO, deps):
+        _run([_cxx(), "-O3", "-mavx2", "-mfma", "-fPIC", "-fopenmp", "-std=c++17", "-shared",
+              "-I", INCLUDE, "-o", HOST_SO] + srcs)
+    return HOST_SO
+
+
+def build_cuda(force=False, verbose_ptxas=False):
+    os.makedirs(LIBDIR, exist_ok=True)
+    srcs = cuda_sources()
+    deps = srcs + cuda_headers() + [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE)]
+    if force or _newer(CUDA_SO, deps):
+        cmd = [_nvcc()] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-shared",
+                                  "-Xcompiler", "-fPIC", "-ccbin", _cxx(),
+                                  "-I", INCLUDE, "-I", CSRC, "-o", CUDA_SO]
+        if verbose_ptxas:
+            cmd += ["-Xptxas", "-v"]
+        _run(cmd + srcs + ["-lcudart"])
+    return CUDA_SO
+
+
+def build_all(force=False):
+    build_host(force)
+    build_cuda(force)
+
+
+if __name__ == "__main__":
+    build_all(force="--force" in sys.argv)

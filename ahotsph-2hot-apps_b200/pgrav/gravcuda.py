@@ -1,0 +1,263 @@
+"""ctypes binding of libgravcuda.so (include/gravcuda.h).
+
+The library is the product's only compute path: nothing here falls back to
+the CPU.  Loading it on a machine without a GPU works (tests check the
+exported symbols there); calling a compute entry point needs a CUDA device.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import _build
+from .host import GROUP_DTYPE, HCELL_DTYPE, PSEG_DTYPE, QCELL_DTYPE
+
+_lib = None
+
+# every entry point declared in include/gravcuda.h
+EXPORTS = [
+    "CUDA_Init", "CUDA_Finalize", "vecwidthCUDA", "qallocCUDA", "WalkInitSrcCUDA",
+    "WalkTerminateSrcCUDA", "WalkInitSinkCUDA", "WalkTerminateSinkCUDA", "grav_mn_CUDA",
+    "grav_mns_CUDA", "grav_mnss_CUDA", "grav_qns_CUDA", "grav_qnss_CUDA",
+    "gravcuda_set_error_mode", "gravcuda_status", "gravcuda_status_string",
+    "gravcuda_clear_status", "grav_mn_status_CUDA", "gravcuda_peek_accumulators",
+    "grav_groups_upload_CUDA", "grav_groups_eval_CUDA", "grav_groups_download_CUDA",
+    "grav_plan_output", "grav_plan_counts", "grav_plan_launches", "grav_plan_free",
+    "grav_groups_CUDA",
+]
+
+
+class GravError(RuntimeError):
+    pass
+
+
+class Segment(ctypes.Structure):
+    _fields_ = [("base", ctypes.c_uint), ("length", ctypes.c_uint)]
+
+
+class Problem(ctypes.Structure):
+    _fields_ = [("nbodies", ctypes.c_int64), ("ncells", ctypes.c_int64),
+                ("ngroups", ctypes.c_int64), ("points", ctypes.c_void_p),
+                ("qcells", ctypes.c_void_p), ("hcells", ctypes.c_void_p),
+                ("groups", ctypes.c_void_p), ("pptr", ctypes.c_void_p),
+                ("qptr", ctypes.c_void_p), ("hptr", ctypes.c_void_p),
+                ("plist", ctypes.c_void_p), ("qlist", ctypes.c_void_p),
+                ("hlist", ctypes.c_void_p), ("eps2", ctypes.c_double), ("box", ctypes.c_double),
+                ("quad_phi_sign", ctypes.c_float), ("ewald", ctypes.c_int)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("warps_per_block", ctypes.c_int), ("chunk_p", ctypes.c_int),
+                ("chunk_q", ctypes.c_int), ("chunk_h", ctypes.c_int),
+                ("blocks_per_sm", ctypes.c_int)]
+
+
+def lib(record_errors=True):
+    """Load libgravcuda.so (building it when absent).  With record_errors the
+    library returns error codes instead of aborting (gravcuda_set_error_mode(1))."""
+    global _lib
+    if _lib is None:
+        path = _build.CUDA_SO
+        if not os.path.exists(path):
+            _build.build_cuda()
+        L = ctypes.CDLL(path)
+        vp, i32, i64, f32, f64 = (ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_float,
+                                  ctypes.c_double)
+        cs = ctypes.c_char_p
+        sig = {
+            "CUDA_Init": ([vp], None), "CUDA_Finalize": ([], None), "vecwidthCUDA": ([], i32),
+            "qallocCUDA": ([vp], i32), "WalkInitSrcCUDA": ([vp, i32, i64], None),
+            "WalkTerminateSrcCUDA": ([], None), "WalkInitSinkCUDA": ([vp, i32, i64], None),
+            "WalkTerminateSinkCUDA": ([vp, i32, i64], None),
+            "grav_mn_CUDA": ([cs, vp, vp, i32, i32, vp, i32, i32, f32, vp, i32], None),
+            "grav_mns_CUDA": ([cs, i32, i32, vp, i32, i32, f32, f32, vp, i32], None),
+            "grav_mnss_CUDA": ([cs, i32, i32, vp, vp, i32, vp, i32, i32, vp, f32, f32, vp, i32],
+                               None),
+            "grav_qns_CUDA": ([cs, i32, i32, vp, i32, i32], None),
+            "grav_qnss_CUDA": ([cs, i32, i32, vp, vp, i32, i32], None),
+            "gravcuda_set_error_mode": ([i32], None), "gravcuda_status": ([], i32),
+            "gravcuda_status_string": ([], cs), "gravcuda_clear_status": ([], None),
+            "grav_mn_status_CUDA": ([cs, vp, i32, i32, vp, i32, i32, f32, i32], i32),
+            "gravcuda_peek_accumulators": ([vp, i64, i64], i32),
+            "grav_groups_upload_CUDA": ([vp, vp, vp], i32),
+            "grav_groups_eval_CUDA": ([vp, vp], i32),
+            "grav_groups_download_CUDA": ([vp, vp], i32),
+            "grav_plan_output": ([vp], vp), "grav_plan_counts": ([vp, vp], None),
+            "grav_plan_launches": ([vp], i32), "grav_plan_free": ([vp], None),
+            "grav_groups_CUDA": ([vp, vp], i32),
+        }
+        for name, (args, res) in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    if record_errors:
+        _lib.gravcuda_set_error_mode(1)
+    return _lib
+
+
+def check(rc=None):
+    """Raise GravError when the library recorded an error."""
+    L = lib()
+    st = L.gravcuda_status() if rc is None else rc
+    if st:
+        msg = L.gravcuda_status_string().decode()
+        L.gravcuda_clear_status()
+        raise GravError(f"gravcuda status {st}: {msg}")
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+class Plan:
+    """A device-resident batched problem (grav_groups_upload_CUDA)."""
+
+    def __init__(self, tree, eps2, quad_phi_sign=1.0, ewald=False, tuning=None):
+        self.tree = tree
+        self._keep = []
+
+        def keep(a, dtype=None):
+            a = np.ascontiguousarray(a if dtype is None else a.astype(dtype, copy=False))
+            self._keep.append(a)
+            return a
+
+        t = tree
+        pts = keep(t.points, np.float32)
+        groups = keep(t.groups)
+        has_q = len(t.qlist) > 0
+        has_h = len(t.hlist) > 0
+        prob = Problem()
+        prob.nbodies, prob.ncells, prob.ngroups = t.n, t.ncells, t.ngroups
+        prob.points = pts.ctypes.data
+        prob.qcells = keep(t.qcells).ctypes.data if has_q else None
+        prob.hcells = keep(t.hcells).ctypes.data if has_h else None
+        prob.groups = groups.ctypes.data
+        prob.pptr = keep(t.ptr[0]).ctypes.data
+        prob.qptr = keep(t.ptr[1]).ctypes.data
+        prob.hptr = keep(t.ptr[2]).ctypes.data
+        prob.plist = keep(t.plist).ctypes.data if len(t.plist) else keep(np.zeros(1, PSEG_DTYPE)).ctypes.data
+        prob.qlist = keep(t.qlist).ctypes.data if has_q else keep(np.zeros(1, np.uint32)).ctypes.data
+        prob.hlist = keep(t.hlist).ctypes.data if has_h else keep(np.zeros(1, np.uint32)).ctypes.data
+        prob.eps2 = float(eps2)
+        prob.box = float(t.box)
+        prob.quad_phi_sign = float(quad_phi_sign)
+        prob.ewald = int(bool(ewald))
+        self.problem = prob
+        h = ctypes.c_void_p()
+        tun = None
+        if tuning is not None:
+            tun = Tuning(*tuning) if not isinstance(tuning, Tuning) else tuning
+        L = lib()
+        check(L.grav_groups_upload_CUDA(ctypes.byref(prob),
+                                        ctypes.byref(tun) if tun is not None else None,
+                                        ctypes.byref(h)))
+        self._h = h
+        self.n = t.n
+
+    def eval(self, stream=None):
+        check(lib().grav_groups_eval_CUDA(self._h, stream))
+
+    def download(self):
+        out = np.empty((self.n, 4), dtype=np.float32)
+        check(lib().grav_groups_download_CUDA(self._h, out.ctypes.data))
+        return out
+
+    def output_ptr(self):
+        return lib().grav_plan_output(self._h)
+
+    def counts(self):
+        c = (ctypes.c_int64 * 4)()
+        lib().grav_plan_counts(self._h, c)
+        return np.array(list(c), dtype=np.int64)
+
+    def launches(self):
+        return lib().grav_plan_launches(self._h)
+
+    def free(self):
+        if getattr(self, "_h", None):
+            lib().grav_plan_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def groups_eval(tree, eps2, quad_phi_sign=1.0):
+    """One-call end-to-end form (grav_groups_CUDA): returns (n, 4) float32
+    (ax, ay, az, phi) in tree order."""
+    plan = Plan(tree, eps2, quad_phi_sign)
+    plan.eval()
+    out = plan.download()
+    plan.free()
+    return out
+
+
+# ---------------------------------------------------------------- drop-in API
+BODY_STRIDE = 14  # floats per reference body record (nln/physics.h:33-44)
+
+
+def body_table(pos, mass):
+    """A reference-layout body table (mass, pos[3], vel[3], acc[3], phi, nterms, ident)."""
+    n = len(pos)
+    bt = np.zeros((n, BODY_STRIDE), dtype=np.float32)
+    bt[:, 0] = mass
+    bt[:, 1:4] = pos
+    return bt
+
+
+class DropIn:
+    """The reference call sequence of nln/mac.c on the drop-in entry points:
+    WalkInitSinkCUDA, any number of grav_*_CUDA calls, WalkTerminateSinkCUDA."""
+
+    def __init__(self, btab):
+        self.btab = np.ascontiguousarray(btab, dtype=np.float32)
+        assert self.btab.shape[1] == BODY_STRIDE
+        L = lib()
+        L.CUDA_Init(None)
+        check()
+        L.WalkInitSinkCUDA(self.btab.ctypes.data, BODY_STRIDE, len(self.btab))
+        check()
+
+    def slot(self):
+        L = lib()
+        inuse = ctypes.c_int()
+        while True:
+            q = L.qallocCUDA(ctypes.byref(inuse))
+            check()
+            if q >= 0:
+                return q
+
+    def mn(self, routine, first, count, f, source_n, sz, e):
+        """grav_mn_CUDA on sinks [first, first+count) with list f."""
+        L = lib()
+        p = self.btab.ctypes.data + 4 * BODY_STRIDE * first
+        f = np.ascontiguousarray(f, dtype=np.float32)
+        L.grav_mn_CUDA(routine.encode(), p, None, count, BODY_STRIDE, f.ctypes.data, source_n, sz,
+                       float(e), None, self.slot())
+        check()
+
+    def mnss(self, sink_base, m, ss_index, ss_seg, seg, source_base, source_n, mmass, e):
+        L = lib()
+        ss_index = np.ascontiguousarray(ss_index, np.uint16)
+        ss_seg = np.ascontiguousarray(ss_seg, np.uint32).reshape(-1, 2)
+        seg = np.ascontiguousarray(seg, np.uint32).reshape(-1, 2)
+        source_n = np.ascontiguousarray(source_n, np.int32)
+        L.grav_mnss_CUDA(b"pMM_mnss_sK1", sink_base, m, ss_index.ctypes.data, ss_seg.ctypes.data,
+                         len(ss_seg), seg.ctypes.data, len(seg), source_base, source_n.ctypes.data,
+                         float(mmass), float(e), None, self.slot())
+        check()
+
+    def peek(self):
+        out = np.empty((len(self.btab), 4), dtype=np.float32)
+        check(lib().gravcuda_peek_accumulators(out.ctypes.data, 0, len(self.btab)))
+        return out
+
+    def terminate(self):
+        L = lib()
+        L.WalkTerminateSinkCUDA(self.btab.ctypes.data, BODY_STRIDE, len(self.btab))
+        check()
+        return self.btab[:, 7:11].copy()

@@ -1,0 +1,209 @@
+/*
+ * gravcuda.h -- the C ABI of libgravcuda.so, the B200 (sm_100a) drop-in for
+ * the CUDA entry points that nln/mac.c and nln/main.c call through the
+ * reference's nln/gravcuda.h (declarations at nln/gravcuda.h:13-69).
+ *
+ * Part 1 keeps every reference entry point with its name, arguments and
+ * meaning.  Part 2 adds status-returning variants, the Plummer-softened
+ * list kernels the reference only has on the CPU, and the batched
+ * index-list path (all sink groups of a step in one persistent launch,
+ * mixed precision, Ewald correction).
+ *
+ * Conventions kept from the reference:
+ *   - sinks are bodies of the table registered by WalkInitSinkCUDA, read at
+ *     float offsets 1..3 of each record of `stride` floats (body.pos,
+ *     nln/physics.h:33-44); results are ADDED to offsets 7..10 (acc, phi)
+ *     at WalkTerminateSinkCUDA, unscaled by G (nln/mac.c:273-276 scales);
+ *   - lists are the reference AoSoA 8-lane blocks (nln/mac.c:117-153),
+ *     source_n a multiple of 8, zero-mass padding lanes;
+ *   - list kernels accumulate d = sink - source with the monopole potential
+ *     -m/r, and the quadrupole potential sign of the CPU kernel they stand
+ *     in for (-1 for the quadrupole kernels, nln/do_grav_avx8.c:2150,940;
+ *     +1 for the order-4 kernels, nln/do_grav_avx8.c:1846,638).
+ * Errors: by default an error prints a message and aborts, as the
+ * reference's Error() does (nln/pgrav.cu:1047-1052); gravcuda_set_error_mode(1)
+ * makes every entry point record the error and return instead
+ * (gravcuda_status() reads it).
+ */
+#ifndef GRAVCUDA_H
+#define GRAVCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "nlnlists.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The reference's body-run type (nln/segment.h:16-19). */
+#ifndef SEGMENT_DEFINED
+#define SEGMENT_DEFINED
+typedef struct {
+    unsigned int base;
+    unsigned int length;
+} segment;
+#endif
+
+/* ================================================================ Part 1 */
+
+/* Select device 0 and report it (nln/cuda.cu:13-47; caller passes NULL, nln/main.c:228). */
+void CUDA_Init(void *device_prop);
+/* Release every library resource (declared but never defined in the reference, nln/gravcuda.h:15). */
+void CUDA_Finalize(void);
+/* Sinks handled per thread by the list kernels (nln/pgrav.cu:1022). */
+int vecwidthCUDA(void);
+/* A free queue slot 0..31 or -1; *inuse receives the busy count (nln/pgrav.cu:814-853,1024). */
+int qallocCUDA(int *inuse);
+
+/*
+ * Cell table for grav_qns_CUDA: ncells records of `stride` floats in the
+ * hexacell layout of nln/physics.h:140-157 (mass 0, pos 1..3, bmax 5,
+ * quadrupole 15..19).  The reference copied wrong fields here
+ * (nln/pgrav.cu:890-904); this maps the hexacell fields as named.
+ * Replaces nln/pgrav.cu:878-913.
+ */
+void WalkInitSrcCUDA(float *qtab, int stride, int64_t nobj);
+/* Free the cell table; safe when never initialised (called unconditionally, nln/main.c:953). */
+void WalkTerminateSrcCUDA(void);
+/* Copy sink positions (floats 1..3 of each record) to the device, zero the accumulators (nln/pgrav.cu:915-967). */
+void WalkInitSinkCUDA(float *btab, int stride, int64_t nobj);
+/* Wait for all queued work, ADD (ax, ay, az, phi) into floats 7..10 of each record (nln/pgrav.cu:969-1020). */
+void WalkTerminateSinkCUDA(float *btab, int stride, int64_t nobj);
+
+/*
+ * n sinks starting at p (a pointer into the registered sink table; sink
+ * index (p - btab)/stride) against the AoSoA list f of source_n sources of
+ * sz floats each, on queue slot q (nln/pgrav.cu:1026-1087).  accp is
+ * ignored (results accumulate on the device).  routine:
+ *   "pM"     monopole, no softening              (CUDA pM,  nln/pgrav.cu:370-410)
+ *   "pQ"     quadrupole, no softening            (do_gravq_avx8, nln/do_grav_avx8.c:881-950)
+ *   "pH"     order 4, no softening               (do_gravh_avx8, nln/do_grav_avx8.c:572-696)
+ *   "pM_sK1" monopole, Dehnen K1, e = 1/eps      (CUDA pM_sK1, nln/pgrav.cu:412-468)
+ *   "pMp"    monopole, Plummer, e = eps^2        (do_gravp_avx8,  nln/do_grav_avx8.c:2163-2216)
+ *   "pQp"    quadrupole, Plummer, e = eps^2      (do_gravpq_avx8, nln/do_grav_avx8.c:2090-2160)
+ *   "pHp"    order 4, Plummer, e = eps^2         (do_gravph_avx8, nln/do_grav_avx8.c:1779-1904)
+ *   "pMs"    monopole, contributions with r < e dropped (do_grav_avx8, nln/do_grav_avx8.c:953-1006)
+ * The list is copied before return, so the caller may reuse f at once.
+ */
+void grav_mn_CUDA(const char *routine, const float *p, float *accp, const int n, const int stride,
+                  const float *f, const int source_n, const int sz, const float e, int *ncut,
+                  int q);
+/*
+ * m sinks from body `base` against seg_n body runs of the sink table, all
+ * of mass mmass, K1 softening with e = 1/eps; routine "pMM_sK1"
+ * (nln/pgrav.cu:575-637, 1089-1147).
+ */
+void grav_mns_CUDA(const char *routine, const int base, const int m, const segment *seg,
+                   const int seg_n, const int source_n, const float mmass, float e, int *ncut,
+                   int q);
+/*
+ * Batched body-run p-p, many sink groups in one launch: sink i of
+ * [sink_base, sink_base+m) belongs to group ss_index[i]; group g owns body
+ * runs seg[ss_seg[g].base .. +ss_seg[g].length), offsets relative to
+ * source_base, source_n[g] bodies in all; routine "pMM_mnss_sK1"
+ * (nln/pgrav.cu:713-790, 1202-1295).  A group whose runs do not add up to
+ * source_n[g] is an error (the reference printed it, nln/pgrav.cu:779-789).
+ */
+void grav_mnss_CUDA(const char *routine, const int sink_base, const int m,
+                    const uint16_t *ss_index, const segment *ss_seg, const int ss_len,
+                    const segment *seg, const int seg_len, const int source_base,
+                    const int *source_n, const float mmass, float e, int *ncut, int q);
+/*
+ * m sinks from `base` against the cells source_list[0..source_n) of the
+ * table registered by WalkInitSrcCUDA, quadrupole, no softening; routine
+ * "pQQ1" (nln/pgrav.cu:498-572, 1149-1200; the reference kernel was dead and
+ * read the wrong bound and fields; this one reads the list as named).
+ */
+void grav_qns_CUDA(const char *routine, const int base, const int m, const int *source_list,
+                   const int source_n, int q);
+/*
+ * Sink i of [base, base+m) against the run seg[i] of the packed QSZ AoSoA
+ * buffer source (source_n records), quadrupole, no softening; routine
+ * "pQ1_qnss" (nln/pgrav.cu:293-368, 1297-1358).
+ */
+void grav_qnss_CUDA(const char *routine, const int base, const int m, const segment *seg,
+                    const float *source, const int source_n, int q);
+
+/* ================================================================ Part 2 */
+
+/* Error reporting: mode 0 = print and abort (reference behaviour), 1 = record and return. */
+void gravcuda_set_error_mode(int mode);
+/* Last recorded status (0 = success) and its message; gravcuda_clear_status() resets both. */
+int gravcuda_status(void);
+const char *gravcuda_status_string(void);
+void gravcuda_clear_status(void);
+
+/* grav_mn_CUDA returning the status instead of aborting. */
+int grav_mn_status_CUDA(const char *routine, const float *p, const int n, const int stride,
+                        const float *f, const int source_n, const int sz, const float e, int q);
+
+/* Synchronise the queue and copy the device accumulators (4 floats per sink) to out, without clearing. */
+int gravcuda_peek_accumulators(float *out, int64_t first, int64_t count);
+
+/*
+ * ---- batched index-list evaluation ----
+ * A step's problem: bodies in tree order and cell monopoles in one point
+ * table, quadrupole and order-4 cell tables, sink groups, and per-group
+ * CSR index lists into those tables, as built by nlnhost.h.  All pointers
+ * are host pointers for grav_groups_upload_CUDA and device pointers for
+ * grav_groups_eval_dev_CUDA.
+ */
+typedef struct grav_problem {
+    int64_t nbodies;            /* bodies = sinks, tree order */
+    int64_t ncells;
+    int64_t ngroups;
+    const float *points;        /* (nbodies + ncells) x float4 (x, y, z, m) */
+    const nln_qcell *qcells;    /* ncells records, or NULL when no quadrupole lists */
+    const nln_hcell *hcells;    /* ncells records, or NULL when no order-4 lists */
+    const nln_group *groups;    /* ngroups records */
+    const int64_t *pptr, *qptr, *hptr;  /* ngroups + 1 each */
+    const nln_pseg *plist;
+    const uint32_t *qlist, *hlist;
+    double eps2;                /* Plummer softening eps^2 (all interactions) */
+    double box;                 /* periodic cube side; 0 = isolated */
+    float quad_phi_sign;        /* +1 physical; -1 reproduces do_gravpq's potential */
+    int ewald;                  /* periodic only: 1 = add the Ewald correction */
+} grav_problem;
+
+typedef struct grav_plan grav_plan;
+
+/* Tile shapes of the batched kernels (the autotuner's search space). */
+typedef struct grav_tuning {
+    int warps_per_block;        /* 4, 8 or 16 */
+    int chunk_p;                /* max point records per work item (split long lists) */
+    int chunk_q;                /* max quadrupole cells per work item */
+    int chunk_h;                /* max order-4 cells per work item */
+    int blocks_per_sm;          /* persistent grid = blocks_per_sm x SM count */
+} grav_tuning;
+
+/*
+ * Copy a problem to the device and build its work queue (items sorted by
+ * cost, longest first).  tuning may be NULL for defaults.  The plan owns
+ * device copies of every table and its scratch; free with grav_plan_free.
+ */
+int grav_groups_upload_CUDA(const grav_problem *host_problem, const grav_tuning *tuning,
+                            grav_plan **plan);
+/* Evaluate on a stream (cudaStream_t passed as void*; NULL = legacy default). */
+int grav_groups_eval_CUDA(grav_plan *plan, void *stream);
+/* Copy (ax, ay, az, phi) per body, tree order, float4, to host memory (synchronising). */
+int grav_groups_download_CUDA(grav_plan *plan, float *acc_phi);
+/* Device pointer of the plan's output (nbodies x float4), for callers that keep results resident. */
+float *grav_plan_output(grav_plan *plan);
+/* Interaction counts of the plan: body-body, monopole, quadrupole, order-4 (over all sinks). */
+void grav_plan_counts(const grav_plan *plan, int64_t out[4]);
+/* Kernel launches per evaluation. */
+int grav_plan_launches(const grav_plan *plan);
+void grav_plan_free(grav_plan *plan);
+
+/*
+ * One-call end-to-end form: upload, evaluate, download, free.  acc_phi:
+ * host, nbodies x 4 floats, tree order.
+ */
+int grav_groups_CUDA(const grav_problem *host_problem, float *acc_phi);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,101 @@
+/*
+ * nlnhost.h -- host-side tree build, moments, MAC walk and list packing that
+ * feed the interaction-list kernels of gravcuda.h.
+ *
+ * This is the caller side of the drop-in boundary: it stands in for the
+ * pieces of 2HOT that produce interaction lists, all of which stay on the
+ * host as plain C/C++:
+ *   - key sort + oct-tree build   (libtree BuildTree, not vendored; used at nln/main.c:900-914)
+ *   - FP64 moments, normalisation (nln/cofm.c:96-231 CofmFromDaugh, 247-574 CellFromCofm)
+ *   - AREL critical radii         (nln/cofm.c:276-565, rcrit_poly/rtnewt 577-624)
+ *   - MAC walk + list appends     (nln/mac.c:1774-1844 DLRcritMAC, append macros 1421-1561)
+ *   - periodic image offsets      (nln/mac.c:91-111 SetGravOffset)
+ * Lists are emitted in two forms from one walk: the reference AoSoA 8-lane
+ * blocks (Mvec/Qvec/Hvec of nln/mac.c:117-153) for grav_mn_CUDA and the
+ * reference CPU kernels, and index lists into device-resident cell and point
+ * tables for the batched kernels (grav_groups_CUDA).
+ */
+#ifndef NLNHOST_H
+#define NLNHOST_H
+
+#include <stdint.h>
+
+#include "nlnlists.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct nln_params {
+    int leaf_max;     /* bodies per leaf cell (1..65535); reference leaf_max_n, main.c:541 */
+    int group_max;    /* sinks per sink group (1..64) */
+    int p2cut;        /* quad_ncut: cells with >= p2cut bodies carry quadrupoles (0: none) */
+    int p4cut;        /* hexa_ncut: cells with >= p4cut bodies carry order-4 moments (0: none) */
+    double tol;       /* errtol, absolute acceleration tolerance (mac_s.tol) */
+    double rel_tol;   /* frac_tol  (0: relative criterion off) */
+    double rel_tol0;  /* frac_tol0 (0: floor criterion off) */
+    double box;       /* periodic cube side L with bodies in [0,L)^3; 0 = isolated */
+    int nthreads;     /* host threads (0: all) */
+    int emit_aosoa;   /* 1: also pack the reference AoSoA lists */
+} nln_params;
+
+typedef struct nln_tree nln_tree;
+
+/*
+ * Sort bodies into key order, build the oct-tree, compute FP64 moments and
+ * critical radii.  pos: xyz of body i at pos[i*stride + 0..2] (floats),
+ * mass at mass[i*mstride].  Returns NULL on bad arguments (message via
+ * nln_last_error()).
+ */
+nln_tree *nln_tree_build(const float *pos, int stride, const float *mass, int mstride, int64_t n,
+                         const nln_params *p);
+void nln_tree_free(nln_tree *t);
+const char *nln_last_error(void);
+
+/* Walk every sink group against the source tree and build its lists. */
+int nln_tree_walk(nln_tree *t);
+
+/* Sizes. */
+int64_t nln_nbodies(const nln_tree *t);
+int64_t nln_ncells(const nln_tree *t);
+int64_t nln_ngroups(const nln_tree *t);
+
+/*
+ * Array accessors (owned by the tree, valid until nln_tree_free).
+ * order:  tree position -> original body index
+ * points: float4 (x, y, z, m): bodies [0, n) then cell monopoles [n, n+ncells)
+ */
+const int64_t *nln_order(const nln_tree *t);
+const float *nln_points(const nln_tree *t);
+const nln_qcell *nln_qcells(const nln_tree *t);
+const nln_hcell *nln_hcells(const nln_tree *t);
+const nln_group *nln_groups(const nln_tree *t);
+
+/* CSR lists per group: entries [ptr[g], ptr[g+1]). kind 0 = P segments, 1 = Q, 2 = H. */
+const int64_t *nln_list_ptr(const nln_tree *t, int kind);
+const void *nln_list_data(const nln_tree *t, int kind);
+int64_t nln_list_len(const nln_tree *t, int kind);
+
+/*
+ * Interaction counts over all sinks: [0] body-body, [1] monopole cells,
+ * [2] quadrupole cells, [3] order-4 cells.
+ */
+void nln_counts(const nln_tree *t, int64_t out[4]);
+
+/*
+ * Reference AoSoA lists (when emit_aosoa): per group and kind (0 = M with
+ * MSZ 4, 1 = Q with QSZ 13, 2 = H with HSZ 29) a run of 8-lane blocks.
+ * blk_ptr has ngroups+1 entries; data has blk_ptr[ngroups]*sz*8 floats.
+ * Positions are absolute (centre + image shift), moments as in the cell
+ * tables, dipole fields zero.
+ */
+const int64_t *nln_aosoa_ptr(const nln_tree *t, int kind);
+const float *nln_aosoa_data(const nln_tree *t, int kind);
+
+/* Body positions in tree order (xyz floats), the sink positions the lists were built for. */
+const float *nln_sorted_pos(const nln_tree *t);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,58 @@
+/*
+ * nlnlists.h -- record layouts shared by the host list builder (nlnhost.h)
+ * and the batched device kernels (gravcuda.h).
+ *
+ * The reference packs each list as copies of cell fields into 8-lane AoSoA
+ * blocks (nln/mac.c:117-153).  At N = 2^24 per-group copies do not fit, so
+ * the batched path instead keeps one table of cells and one table of points
+ * resident on the device and hands the kernels index lists into them.
+ */
+#ifndef NLNLISTS_H
+#define NLNLISTS_H
+
+#include <stdint.h>
+
+/* Cell record layouts of the device tables (little-endian, 16-byte multiples). */
+typedef struct nln_qcell {      /* 64 bytes */
+    double cen[3];              /* FP64 expansion centre (centre of mass) */
+    float mass, R;              /* R = bmax normalises the moments */
+    float qxx, qxy, qyy, qxz, qyz;
+    float pad[3];
+} nln_qcell;
+
+typedef struct nln_hcell {      /* 128 bytes */
+    double cen[3];
+    float mass, R;
+    float q2[5];                /* qxx qxy qyy qxz qyz              / R^2 */
+    float q3[7];                /* qxxx qxxy qxyy qyyy qxxz qxyz qyyz / R^3 */
+    float q4[9];                /* qxxxx qxxxy qxxyy qxyyy qyyyy qxxxz qxxyz qxyyz qyyyz / R^4 */
+    float pad[3];
+} nln_hcell;
+
+/* One run of point-table records with one periodic image shift. */
+typedef struct nln_pseg {
+    uint32_t base;              /* first record in the point table */
+    uint16_t len;               /* records in the run */
+    uint16_t shift;             /* image code (sx+1)*9+(sy+1)*3+(sz+1); 13 = none */
+} nln_pseg;
+
+/*
+ * Periodic boxes: a source is used whole in the image nearest the sink
+ * group's centre, and every sink-source displacement stays inside
+ * |y_k| <= NLN_EWALD_REACH * box, the domain of the Ewald correction table.
+ */
+#define NLN_EWALD_REACH 0.75
+
+/* Index-list entries for quad/order-4 cells: cell index | shift << 27. */
+#define NLN_SHIFT_NONE 13u
+#define NLN_IDX_BITS 27
+#define NLN_IDX_MASK ((1u << NLN_IDX_BITS) - 1u)
+
+typedef struct nln_group {      /* 40 bytes */
+    double cen[3];              /* FP64 group centre (centre of mass of its sinks) */
+    int64_t first;              /* first sink, in tree order */
+    int32_t count;              /* sinks */
+    float radius;               /* max sink distance from cen */
+} nln_group;
+
+#endif

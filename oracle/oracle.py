@@ -1,0 +1,181 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes access to the parity checkers.
+
+* ``liboracle``   -- this repository's CPU restatement (oracle/grav_oracle.c)
+* ``libnlnref``   -- the reference's own AVX kernels compiled unmodified from
+                     nln/do_grav_avx8.c and nln/pgrav_vec.c (oracle/Makefile)
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import
+this module, as the checker; the product path never does.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libnlnref.so")
+
+# list kinds (shared numbering with grav_oracle.c / ref_harness.c)
+MONO_PLUMMER, QUAD_PLUMMER, HEXA_PLUMMER = 0, 1, 2
+MONO_MASKED, MONO_K1, QUAD_COM, HEXA_COM, MONO_BARE = 3, 4, 5, 6, 7
+QUAD_PLUMMER_P = 8
+KIND_SZ = {0: 4, 1: 13, 2: 29, 3: 4, 4: 4, 5: 13, 6: 29, 7: 4, 8: 13}
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+
+_orc = None
+_ref = None
+
+
+def build():
+    """Compile the restatement (and the reference kernels when the reference tree is present)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def orc():
+    global _orc
+    if _orc is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        lib = ctypes.CDLL(ORACLE_SO)
+        lib.orc_list_eval.argtypes = [ctypes.c_int, _f32p, ctypes.c_long, ctypes.c_int, _f32p,
+                                      ctypes.c_float, _f64p]
+        lib.orc_list_eval.restype = ctypes.c_int
+        lib.orc_mxn_eval.argtypes = [ctypes.c_int, _f32p, _f32p, ctypes.c_int, ctypes.c_int, _f32p,
+                                     ctypes.c_long, ctypes.c_int, ctypes.c_float]
+        lib.orc_segments_k1.argtypes = [_f32p, ctypes.c_int, ctypes.c_float, _u32p, ctypes.c_int,
+                                        _f32p, ctypes.c_float, _f64p]
+        lib.orc_segments_k1.restype = ctypes.c_long
+        lib.orc_direct.argtypes = [_f64p, _f64p, ctypes.c_long, ctypes.c_double, _i64p,
+                                   ctypes.c_long, _f64p, _f64p]
+        lib.orc_ewald.argtypes = [_f64p, ctypes.c_double, _f64p, _f64p]
+        lib.orc_ewald_batch.argtypes = [_f64p, ctypes.c_long, ctypes.c_double, _f64p, _f64p]
+        lib.orc_direct_ewald.argtypes = [_f64p, _f64p, ctypes.c_long, ctypes.c_double,
+                                         ctypes.c_double, _i64p, ctypes.c_long, _f64p, _f64p]
+        lib.orc_groups_eval.argtypes = [ctypes.c_int, _f32p, ctypes.c_int, _i64p, _i64p, _i64p,
+                                        _i32p, ctypes.c_long, _f32p, ctypes.c_float, _f64p]
+        _orc = lib
+    return _orc
+
+
+def ref_available():
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        lib = ctypes.CDLL(REF_SO)
+        lib.ref_list_eval.argtypes = [ctypes.c_int, _f32p, ctypes.c_long, ctypes.c_int, _f32p,
+                                      ctypes.c_float, _f32p]
+        lib.ref_list_eval.restype = ctypes.c_int
+        lib.ref_groups_eval.argtypes = [ctypes.c_int, _f32p, ctypes.c_int, _i64p, _i64p, _i64p,
+                                        _i32p, ctypes.c_long, _f32p, ctypes.c_float, _f32p,
+                                        ctypes.c_int]
+        lib.ref_pinteract.argtypes = [ctypes.c_int, _f32p, _f32p, ctypes.c_int, ctypes.c_int,
+                                      _f32p, ctypes.c_long]
+        lib.ref_segments_k1.argtypes = [_f32p, ctypes.c_int, ctypes.c_float, _u32p, ctypes.c_int,
+                                        ctypes.c_long, _f32p, ctypes.c_float, _f32p]
+        lib.ref_segments_k1.restype = ctypes.c_long
+        _ref = lib
+    return _ref
+
+
+def aligned_f32(n, align=64):
+    """A zeroed float32 array whose data pointer is `align`-byte aligned (the
+    reference AVX kernels load 32-byte vectors)."""
+    buf = np.zeros(n + align // 4, dtype=np.float32)
+    off = (-buf.ctypes.data % align) // 4
+    return buf[off:off + n]
+
+
+def pack_aosoa(fields):
+    """(nsrc, sz) records -> the reference 8-lane AoSoA layout, zero-padded
+    to a multiple of 8 sources (mac.c:606-612 pads with zero-mass lanes)."""
+    fields = np.asarray(fields, dtype=np.float32)
+    n, sz = fields.shape
+    nblk = (n + 7) // 8
+    pad = np.zeros((nblk * 8, sz), dtype=np.float32)
+    pad[:n] = fields
+    out = aligned_f32(nblk * 8 * sz)
+    out[:] = pad.reshape(nblk, 8, sz).transpose(0, 2, 1).ravel()
+    return out, nblk
+
+
+def list_eval(kind, f, nblk, pos0, e):
+    out = np.zeros(4, dtype=np.float64)
+    orc().orc_list_eval(kind, f, nblk, KIND_SZ[kind], np.ascontiguousarray(pos0, np.float32),
+                        float(e), out)
+    return out
+
+
+def ref_list_eval(kind, f, nblk, pos0, e):
+    out = np.zeros(4, dtype=np.float32)
+    ref().ref_list_eval(kind, f, nblk, KIND_SZ[kind], np.ascontiguousarray(pos0, np.float32),
+                        float(e), out)
+    return out
+
+
+def direct(pos, mass, eps2, sinks=None):
+    """FP64 direct sum (self included, Plummer eps2); returns (acc[nsink,3], phi[nsink])."""
+    pos = np.ascontiguousarray(pos, np.float64)
+    mass = np.ascontiguousarray(mass, np.float64)
+    n = len(mass)
+    sinks = np.arange(n, dtype=np.int64) if sinks is None else np.ascontiguousarray(sinks, np.int64)
+    acc = np.zeros((len(sinks), 3))
+    phi = np.zeros(len(sinks))
+    orc().orc_direct(pos, mass, n, float(eps2), sinks, len(sinks), acc, phi)
+    return acc, phi
+
+
+def ewald(x, L):
+    x = np.ascontiguousarray(np.atleast_2d(x), np.float64)
+    f = np.zeros_like(x)
+    phi = np.zeros(len(x))
+    orc().orc_ewald_batch(x, len(x), float(L), f, phi)
+    return f, phi
+
+
+def direct_ewald(pos, mass, L, eps2, sinks):
+    pos = np.ascontiguousarray(pos, np.float64)
+    mass = np.ascontiguousarray(mass, np.float64)
+    sinks = np.ascontiguousarray(sinks, np.int64)
+    acc = np.zeros((len(sinks), 3))
+    phi = np.zeros(len(sinks))
+    orc().orc_direct_ewald(pos, mass, len(mass), float(L), float(eps2), sinks, len(sinks), acc, phi)
+    return acc, phi
+
+
+def tree_eval(tree, eps2, quad_kind=QUAD_PLUMMER_P, hexa_kind=HEXA_PLUMMER, mono_kind=MONO_PLUMMER,
+              reference=False):
+    """Evaluate a host tree's AoSoA lists (built with emit_aosoa) for every
+    sink: (n, 4) (ax, ay, az, phi) in tree order.  reference=True runs the
+    compiled reference AVX kernels (FP32) instead of the restatement."""
+    n = tree.n
+    sf = np.ascontiguousarray(tree.groups["first"]).astype(np.int64)
+    sc = np.ascontiguousarray(tree.groups["count"]).astype(np.int32)
+    pos = np.ascontiguousarray(tree.sorted_pos.ravel(), np.float32)
+    out = np.zeros((n, 4), np.float32 if reference else np.float64)
+    if reference and quad_kind == QUAD_PLUMMER_P:
+        raise ValueError("the reference quadrupole kernels use the -1 potential sign")
+    for k, kind in ((0, mono_kind), (1, quad_kind), (2, hexa_kind)):
+        ptr, data = tree.aosoa[k]
+        if ptr[-1] == 0:
+            continue
+        d = aligned_f32(len(data))
+        d[:] = data
+        bf = np.ascontiguousarray(ptr[:-1])
+        bc = np.ascontiguousarray(np.diff(ptr))
+        if reference:
+            ref().ref_groups_eval(kind, d, KIND_SZ[kind], bf, bc, sf, sc, len(sf), pos, eps2,
+                                  out.ravel(), 0 or os.cpu_count())
+        else:
+            orc().orc_groups_eval(kind, d, KIND_SZ[kind], bf, bc, sf, sc, len(sf), pos, eps2,
+                                  out.ravel())
+    return out
