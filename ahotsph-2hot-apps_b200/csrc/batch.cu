@@ -17,6 +17,8 @@
 // empty.  One warp owns one item: lane = sink, 32 sources per staged tile,
 // double-buffered TMA bulk copies (one per lane, one record each) signalled
 // on a per-warp mbarrier.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <string.h>
@@ -64,6 +66,18 @@ template <int KIND>
 struct KindOf {
     static constexpr int rec_bytes = KIND == KP ? 16 : (KIND == KQ ? 64 : 128);
     static constexpr int order = KIND == KP ? 0 : (KIND == KQ ? 2 : 4);
+    // pipeline depth: short per-record work needs more copies in flight
+    static constexpr int stages = KIND == KP ? 4 : (KIND == KQ ? 3 : 2);
+    // one TMA row gather brings 4 records; each lands 128-byte aligned
+    static constexpr int group_bytes = 4 * rec_bytes < 128 ? 128 : 4 * rec_bytes;
+    static constexpr int stage_bytes = (TILE / 4) * group_bytes;
+    // per-warp shared memory: stages of 32 records, mbarriers, image codes
+    static constexpr int warp_bytes =
+        (stages * stage_bytes + stages * 8 + stages * TILE * 4 + 127) / 128 * 128;
+    // byte offset of record r inside a stage
+    static __device__ __forceinline__ int rec_off(int r) {
+        return (r >> 2) * group_bytes + (r & 3) * rec_bytes;
+    }
 };
 
 __device__ __forceinline__ void decode_shift(uint32_t code, double box, double &sx, double &sy,
@@ -107,30 +121,29 @@ __device__ __forceinline__ void convert(unsigned char *slot, uint32_t code, cons
 }
 
 template <int KIND>
-__global__ void __launch_bounds__(256) k_batch(DevProblem P) {
-    constexpr int RB = KindOf<KIND>::rec_bytes;
-    constexpr int ORDER = KindOf<KIND>::order;
-    constexpr int STRIDE = RB / 4;  // floats per staged slot
+__global__ void __launch_bounds__(256) k_batch(const __grid_constant__ CUtensorMap tmap,
+                                               DevProblem P) {
+    using K = KindOf<KIND>;
+    constexpr int RB = K::rec_bytes;
+    constexpr int ORDER = K::order;
+    constexpr int NST = K::stages;
     extern __shared__ __align__(128) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    unsigned char *wbuf = smem + (size_t)wib * (2 * TILE * RB + 16);
-    auto buf = [&](uint32_t seq) { return wbuf + (seq & 1) * (TILE * RB); };
-    uint64_t *bar = reinterpret_cast<uint64_t *>(wbuf + 2 * TILE * RB);
+    unsigned char *wbuf = smem + (size_t)wib * K::warp_bytes;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(wbuf + NST * K::stage_bytes);
+    uint32_t *codes = reinterpret_cast<uint32_t *>(bar + NST);  // [NST][TILE] image codes
     if (lane == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int s = 0; s < NST; s++) mbar_init(&bar[s], 1);
         fence_mbar_init();
     }
     __syncwarp();
 
     const uint32_t *list = P.list[KIND];
-    const int64_t ntab = P.ntab[KIND];
-    const unsigned char *table =
-        KIND == KP ? reinterpret_cast<const unsigned char *>(P.points)
-                   : (KIND == KQ ? reinterpret_cast<const unsigned char *>(P.qcells)
-                                 : reinterpret_cast<const unsigned char *>(P.hcells));
-    uint32_t tseq = 0;  // tiles consumed by this warp: buffer tseq&1, parity (tseq>>1)&1
+    const uint32_t ntab = (uint32_t)P.ntab[KIND];
+    // tiles issued (and later consumed, in the same order) by this warp:
+    // tile seq uses stage seq % NST with mbarrier parity (seq / NST) & 1
+    uint32_t tseq = 0;
     bool alive = true;
 
     while (alive) {
@@ -155,62 +168,81 @@ __global__ void __launch_bounds__(256) k_batch(DevProblem P) {
         const int64_t nent = item.end - item.begin;
         const int ntile = (int)((nent + TILE - 1) / TILE);
 
-        // entry of this lane in tile t (prefetched one tile ahead)
         auto fetch = [&](int t) -> uint32_t {
             int64_t k = item.begin + (int64_t)t * TILE + lane;
-            return (t < ntile && k < item.end) ? __ldg(list + k) : 0xffffffffu;
+            return (t < ntile && k < item.end) ? __ldg(list + k) : 0u;
         };
+        // Start tile t (sequence number seq): each lane holds one entry; the
+        // row indices are gathered to lane 0, which issues one TMA row
+        // gather per 4 records.  Unused rows of a short tile repeat row 0.
         auto issue = [&](int t, uint32_t ent, uint32_t seq) {
             const int nt = (int)min((int64_t)TILE, nent - (int64_t)t * TILE);
-            uint64_t *b = &bar[seq & 1];
+            const int ng4 = (nt + 3) >> 2;
+            const uint32_t st = seq % NST;
+            uint32_t idx = ent & NLN_IDX_MASK;
+            if (lane < nt && idx >= ntab) {  // never expected: the host validated every entry
+                atomicOr(P.err, GC_DEV_BAD_INDEX);
+                idx = 0;
+            }
+            if (lane >= nt)
+                idx = 0;
+            codes[st * TILE + lane] = ent >> NLN_IDX_BITS;
             if (lane == 0)
-                mbar_arrive_expect_tx(b, (uint32_t)(nt * RB));
-            __syncwarp();
-            if (lane < nt) {
-                uint32_t idx = ent & NLN_IDX_MASK;
-                if (idx >= (uint32_t)ntab) {  // never expected: keep the transaction count whole
-                    atomicOr(P.err, GC_DEV_BAD_INDEX);
-                    idx = 0;
-                }
-                tma_bulk_g2s(buf(seq) + lane * RB, table + (size_t)idx * RB, RB, b);
+                mbar_arrive_expect_tx(&bar[st], (uint32_t)(ng4 * 4 * RB));
+            unsigned char *dst = wbuf + st * K::stage_bytes;
+#pragma unroll
+            for (int g = 0; g < TILE / 4; g++) {
+                const int r0 = __shfl_sync(0xffffffffu, (int)idx, 4 * g);
+                const int r1 = __shfl_sync(0xffffffffu, (int)idx, 4 * g + 1);
+                const int r2 = __shfl_sync(0xffffffffu, (int)idx, 4 * g + 2);
+                const int r3 = __shfl_sync(0xffffffffu, (int)idx, 4 * g + 3);
+                if (lane == 0 && g < ng4)
+                    tma_gather4(dst + g * K::group_bytes, &tmap, r0, r1, r2, r3, &bar[st]);
             }
         };
-        uint32_t ent_cur = fetch(0);
-        uint32_t ent_next = fetch(1);
-        if (ntile > 0)
-            issue(0, ent_cur, tseq);
-        for (int t = 0; t < ntile; t++, tseq++) {
-            if (t + 1 < ntile)
-                issue(t + 1, ent_next, tseq + 1);
-            const uint32_t code_cur = ent_cur >> NLN_IDX_BITS;
-            ent_cur = ent_next;
-            ent_next = fetch(t + 2);
+#pragma unroll
+        for (int p = 0; p < NST - 1; p++)
+            if (p < ntile)
+                issue(p, fetch(p), tseq + p);
+        uint32_t ent_next = fetch(NST - 1);
+        for (int t = 0; t < ntile; t++) {
+            const uint32_t seq = tseq + t;
+            if (t + NST - 1 < ntile)
+                issue(t + NST - 1, ent_next, seq + NST - 1);
+            ent_next = fetch(t + NST);
             const int nt = (int)min((int64_t)TILE, nent - (int64_t)t * TILE);
-            bool ok = mbar_wait_bounded(&bar[tseq & 1], (tseq >> 1) & 1, P.err);
+            const uint32_t st = seq % NST;
+            bool ok = mbar_wait_bounded(&bar[st], (seq / NST) & 1, P.err);
             if (!__all_sync(0xffffffffu, ok)) {
+                // give the copies still in flight a bounded chance to land
+                for (int u = t + 1; u < ntile && u < t + NST; u++)
+                    mbar_wait_bounded(&bar[(tseq + u) % NST], ((tseq + u) / NST) & 1, P.err,
+                                      1u << 10);
                 alive = false;
                 break;
             }
-            unsigned char *bt = buf(tseq);
+            unsigned char *bt = wbuf + st * K::stage_bytes;
             if (lane < nt)
-                convert<KIND>(bt + lane * RB, code_cur, c, P.box);
+                convert<KIND>(bt + K::rec_off(lane), codes[st * TILE + lane], c, P.box);
             __syncwarp();
             Acc4 a{0.f, 0.f, 0.f, 0.f};
-            const float *rec = reinterpret_cast<const float *>(bt);
             if (nt == TILE) {
 #pragma unroll 4
                 for (int r = 0; r < TILE; r++)
-                    interact<ORDER, SOFT_PLUMMER>(rec + r * STRIDE, ux, uy, uz, P.eps2, P.qsh, a);
+                    interact<ORDER, SOFT_PLUMMER>(reinterpret_cast<const float *>(bt + K::rec_off(r)),
+                                                  ux, uy, uz, P.eps2, P.qsh, a);
             } else {
                 for (int r = 0; r < nt; r++)
-                    interact<ORDER, SOFT_PLUMMER>(rec + r * STRIDE, ux, uy, uz, P.eps2, P.qsh, a);
+                    interact<ORDER, SOFT_PLUMMER>(reinterpret_cast<const float *>(bt + K::rec_off(r)),
+                                                  ux, uy, uz, P.eps2, P.qsh, a);
             }
             comp_add(hi[0], lo[0], a.ax);
             comp_add(hi[1], lo[1], a.ay);
             comp_add(hi[2], lo[2], a.az);
             comp_add(hi[3], lo[3], a.phi);
-            __syncwarp();  // every lane is done with bt before it is refilled
+            __syncwarp();  // every lane is done with this stage before it is refilled
         }
+        tseq += ntile;
         if (!alive)
             break;
         float4 *dst = P.part + ((size_t)item.slot * 32 + lane) * 2;
@@ -252,9 +284,37 @@ struct grav_plan {
     int nsm = 148;
     int launches = 0;
     int64_t nslots = 0;
+    CUtensorMap tmap[3];    // row-gather views of the point, quadrupole and order-4 tables
 };
 
 namespace {
+
+// A 2-D tensor map over `rows` records of `row_bytes` (a multiple of 16),
+// box = one full record (one row high, as the row gather requires).
+int encode_rows(CUtensorMap *m, const void *base, uint64_t rows, uint32_t row_bytes) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        GC_CHECK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (!fn || q != cudaDriverEntryPointSuccess)
+            return gc::set_status(-1, "cuTensorMapEncodeTiled unavailable");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const uint32_t w = row_bytes / 4;
+    cuuint64_t dims[2] = {w, rows};
+    cuuint64_t strides[1] = {row_bytes};
+    cuuint32_t box[2] = {w, 1};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(base), dims,
+                        strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return gc::set_status(-1, "cuTensorMapEncodeTiled failed (%d) for %llu rows of %u bytes",
+                              (int)r, (unsigned long long)rows, row_bytes);
+    return 0;
+}
 
 template <typename T>
 int dev_copy(grav_plan *pl, const T *src, size_t n, T **dst) {
@@ -268,24 +328,27 @@ int dev_copy(grav_plan *pl, const T *src, size_t n, T **dst) {
     return 0;
 }
 
-grav_tuning default_tuning(const grav_problem *p, int nsm) {
+// Defaults: 8 warps per block, as many resident blocks as registers and
+// shared memory allow (blocks_per_sm = 0), list chunks sized automatically
+// (chunk_* = 0) from the totals once the lists are known.
+grav_tuning default_tuning() {
     grav_tuning t;
     t.warps_per_block = 8;
-    t.blocks_per_sm = 2;
-    // split lists so that the item count is at least ~8 per resident warp
-    const int64_t warps = (int64_t)nsm * t.blocks_per_sm * t.warps_per_block;
-    int64_t ng = std::max<int64_t>(p->ngroups, 1);
-    int64_t per = std::max<int64_t>(1, (8 * warps + ng - 1) / ng);
-    auto chunk = [&](int64_t total, int64_t lo, int64_t hi) {
-        int64_t avg = std::max<int64_t>(1, total / ng);
-        int64_t c = std::max<int64_t>(lo, avg / per);
-        c = (c + TILE - 1) / TILE * TILE;
-        return (int)std::min<int64_t>(hi, c);
-    };
-    t.chunk_p = chunk(p->pptr ? p->pptr[p->ngroups] * 16 : 0, 128, 1 << 20);
-    t.chunk_q = chunk(p->qptr ? p->qptr[p->ngroups] : 0, 64, 1 << 20);
-    t.chunk_h = chunk(p->hptr ? p->hptr[p->ngroups] : 0, 32, 1 << 20);
+    t.blocks_per_sm = 0;
+    t.chunk_p = t.chunk_q = t.chunk_h = 0;
     return t;
+}
+
+// Split lists so that there are at least ~8 work items per resident warp
+// (about 148 SMs x 32 warps), in whole tiles, no shorter than `lo`.
+int auto_chunk(int64_t total, int64_t ngroups, int nsm, int64_t lo) {
+    const int64_t warps = (int64_t)nsm * 32;
+    int64_t ng = std::max<int64_t>(ngroups, 1);
+    int64_t per = std::max<int64_t>(1, (8 * warps + ng - 1) / ng);
+    int64_t avg = std::max<int64_t>(1, total / ng);
+    int64_t c = std::max<int64_t>(lo, avg / per);
+    c = (c + TILE - 1) / TILE * TILE;
+    return (int)std::min<int64_t>(1 << 24, c);
 }
 
 }  // namespace
@@ -301,7 +364,7 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
     grav_plan *pl = new grav_plan();
     cudaDeviceGetAttribute(&pl->nsm, cudaDevAttrMultiProcessorCount, 0);
     pl->hp = *hp;
-    pl->tune = tuning ? *tuning : default_tuning(hp, pl->nsm);
+    pl->tune = tuning ? *tuning : default_tuning();
     const int64_t ng = hp->ngroups, nb = hp->nbodies, np = hp->nbodies + hp->ncells;
 
     // expand point runs into per-record entries; validate everything we index
@@ -343,6 +406,15 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
         delete pl;
         return gc::set_status(-1, "cell list entry outside the cell table");
     }
+
+    if (pl->tune.warps_per_block < 1 || pl->tune.warps_per_block > 8)
+        pl->tune.warps_per_block = 8;
+    if (pl->tune.chunk_p <= 0)
+        pl->tune.chunk_p = auto_chunk(eptr[ng], ng, pl->nsm, 128);
+    if (pl->tune.chunk_q <= 0)
+        pl->tune.chunk_q = auto_chunk(hp->qptr ? hp->qptr[ng] : 0, ng, pl->nsm, 64);
+    if (pl->tune.chunk_h <= 0)
+        pl->tune.chunk_h = auto_chunk(hp->hptr ? hp->hptr[ng] : 0, ng, pl->nsm, 32);
 
     // work items, created group by group (slot order), then sorted per kind by cost
     std::vector<Item> items[3];
@@ -429,6 +501,16 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
         return rc;
     }
     cudaMemset(err, 0, sizeof(unsigned));
+    memset(pl->tmap, 0, sizeof(pl->tmap));
+    rc |= encode_rows(&pl->tmap[KP], d.points, (uint64_t)np, 16);
+    if (d.qcells)
+        rc |= encode_rows(&pl->tmap[KQ], d.qcells, (uint64_t)hp->ncells, sizeof(nln_qcell));
+    if (d.hcells)
+        rc |= encode_rows(&pl->tmap[KH], d.hcells, (uint64_t)hp->ncells, sizeof(nln_hcell));
+    if (rc) {
+        grav_plan_free(pl);
+        return rc;
+    }
     d.ngroups = ng;
     d.eps2 = (float)hp->eps2;
     d.qsh = 0.5f * (hp->quad_phi_sign == 0.0f ? 1.0f : hp->quad_phi_sign);
@@ -450,12 +532,15 @@ int launch_kind(grav_plan *pl, cudaStream_t st) {
     if (pl->dp.nitems[KIND] == 0)
         return 0;
     const int wpb = pl->tune.warps_per_block;
-    const size_t smem = (size_t)wpb * (2 * TILE * KindOf<KIND>::rec_bytes + 16);
+    const size_t smem = (size_t)wpb * KindOf<KIND>::warp_bytes;
     GC_CHECK(cudaFuncSetAttribute(k_batch<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem));
-    int blocks = pl->tune.blocks_per_sm * pl->nsm;
+    int fit = 0;
+    GC_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_batch<KIND>, wpb * 32, smem));
+    int per_sm = pl->tune.blocks_per_sm > 0 ? std::min(pl->tune.blocks_per_sm, fit) : fit;
+    int blocks = std::max(1, per_sm) * pl->nsm;
     blocks = std::min(blocks, (pl->dp.nitems[KIND] + wpb - 1) / wpb);
-    k_batch<KIND><<<blocks, wpb * 32, smem, st>>>(pl->dp);
+    k_batch<KIND><<<blocks, wpb * 32, smem, st>>>(pl->tmap[KIND], pl->dp);
     GC_CHECK(cudaGetLastError());
     pl->launches++;
     return 0;

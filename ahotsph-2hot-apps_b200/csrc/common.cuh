@@ -67,23 +67,39 @@ __device__ __forceinline__ void tma_bulk_g2s(void *dst, const void *src, uint32_
         : "memory");
 }
 
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+// try_wait with a suspend-time hint: a warp whose data has not landed is
+// suspended (up to hint_ns) until the phase completes instead of spinning
+// through issue slots the other warps need.
+// TMA row gather (sm_100a): four rows of a 2-D tensor map, each one box
+// (one row high, the full row wide), selected by row index, land back to
+// back at dst (128-byte aligned).  No multicast.
+__device__ __forceinline__ void tma_gather4(void *dst, const void *tmap, int r0, int r1, int r2,
+                                            int r3, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(dst)),
+        "l"(tmap), "r"(0), "r"(r0), "r"(r1), "r"(r2), "r"(r3), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity,
+                                              uint32_t hint_ns = 20000) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
         : "memory");
     return ok != 0;
 }
 
-// Bounded wait: gives up after `limit` polls (each try_wait itself blocks
-// for a hardware-defined interval), sets GC_DEV_WAIT_TIMEOUT and returns
-// false, so a lost transaction ends the kernel instead of hanging the GPU.
+// Bounded wait: gives up after `limit` polls (each suspends for at most the
+// hint), sets GC_DEV_WAIT_TIMEOUT and returns false, so a lost transaction
+// ends the kernel within about a second instead of hanging the GPU.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
-                                                  unsigned *err, uint32_t limit = 1u << 22) {
+                                                  unsigned *err, uint32_t limit = 1u << 16) {
     for (uint32_t i = 0; i < limit; i++)
         if (mbar_try_wait(bar, parity))
             return true;

@@ -78,7 +78,10 @@ struct RecOf {
 
 // Fold source s of a raw AoSoA tile (sz fields x 8 lanes per block) into a
 // staged record.  Zero-mass padding lanes (nln/mac.c:606-612) are moved far
-// away so they add exactly zero even without softening.
+// away so they add exactly zero even without softening; 1e8 keeps every
+// power of the displacement used by the order-4 terms (up to the 4th) finite.
+constexpr float kFarAway = 1.0e8f;
+
 template <int ORDER>
 __device__ void stage_aosoa(float *o, const float *raw, int sz, int s) {
     const float *blk = raw + (s >> 3) * sz * 8;
@@ -86,7 +89,7 @@ __device__ void stage_aosoa(float *o, const float *raw, int sz, int s) {
     float m = blk[l];
     float x = blk[8 + l], y = blk[16 + l], z = blk[24 + l];
     if (m == 0.0f) {
-        x = y = z = 1.0e18f;
+        x = y = z = kFarAway;
     }
     o[0] = x;
     o[1] = y;
@@ -160,12 +163,16 @@ __global__ void __launch_bounds__(128) k_list(const float *__restrict__ pos, flo
     }
 
     bool ok = true;
+    int failed_at = -1;
     for (int t = 0; t < ntile; t++) {
         if (tid == 0 && t + 1 < ntile)
             issue(t + 1);
         ok = mbar_wait_bounded(&bar[t & 1], (t >> 1) & 1, err);
-        if (!__syncthreads_and(ok))
+        if (!__syncthreads_and(ok)) {
+            ok = false;
+            failed_at = t;
             break;
+        }
         const float *rt = (t & 1) ? raw1 : raw0;
         const int nsrc = min(TBLK, c1 - (c0 + t * TBLK)) * 8;
         for (int s = tid; s < nsrc; s += blockDim.x) stage_aosoa<ORDER>(rec + s * REC, rt, sz, s);
@@ -178,9 +185,10 @@ __global__ void __launch_bounds__(128) k_list(const float *__restrict__ pos, flo
         __syncthreads();
     }
     if (!ok) {
-        // drain: wait (bounded) for any copy still in flight before exit
-        if (tid == 0 && ntile > 1)
-            mbar_wait_bounded(&bar[1], 0, err, 1u << 16);
+        // drain: wait (bounded) for the next tile's copy, if one was issued
+        const int t1 = failed_at + 1;
+        if (tid == 0 && t1 < ntile)
+            mbar_wait_bounded(&bar[t1 & 1], (t1 >> 1) & 1, err, 1u << 16);
         return;
     }
 #pragma unroll
@@ -257,7 +265,7 @@ __global__ void k_quad_runs(const float *__restrict__ pos, float4 *accp, int m,
         rec[2] = __ldg(blk + 24 + l);
         rec[3] = mm;
         if (mm == 0.0f)
-            rec[0] = rec[1] = rec[2] = 1.0e18f;
+            rec[0] = rec[1] = rec[2] = kFarAway;
         float q2[5];
         for (int t = 0; t < 5; t++) q2[t] = __ldg(blk + (8 + t) * 8 + l);
         stage_quad(rec, __ldg(blk + 32 + l), q2);

@@ -63,7 +63,7 @@ def grf_box(n1d, seed=123, slope=-2.5, rms_disp=0.25, total_mass=1.0):
     disp = np.empty((n1d, n1d, n1d, 3), dtype=np.float64)
     for d, K in enumerate((KX, KY, KZ)):
         # psi_k = i k / k^2 delta_k  (so that div psi = -delta)
-        disp[..., d] = np.fft.irfftn(1j * K / k2 * delta_k, s=(n1d, n1d, n1d))
+        disp[..., d] = np.fft.irfftn(1j * K / k2 * delta_k, s=(n1d, n1d, n1d), axes=(0, 1, 2))
     del delta_k
     rms = np.sqrt(np.mean(np.sum(disp * disp, axis=-1)))
     disp *= rms_disp * spacing / rms
