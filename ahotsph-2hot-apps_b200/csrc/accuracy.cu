@@ -1,0 +1,179 @@
+// accuracy.cu -- FP64 direct sums at sample sinks: the reference every
+// reported force error is measured against.
+//
+// Isolated: a_i = sum_j m_j d/(r^2+eps2)^1.5, phi_i = -sum_j m_j/(r^2+eps2)^0.5
+// with d = x_j - x_i, self included (the scalar do_grav of nln/grav.c:46-79
+// summed in FP64).  Periodic: the Ewald-summed direct sum of
+// nln/grav_n2.c:97-196 (EwaldForces) with the nearest-image Newtonian term
+// Plummer-softened like the tree's: for each pair the nearest-image term
+// plus C(y), the smooth remainder of ewald() (nln/ewald.c:13-64), taken from
+// an FP64 table over |y_k| <= L/2 by a third-order Taylor expansion about
+// the nearest node; a pair at zero separation contributes only the constant
+// pi/(alpha^2 L^3) that ewald() returns for x = 0.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "gravcuda.h"
+#define NLN_EWALD_NO_EXPORT
+#include "host/ewald_table.cpp"
+
+namespace {
+
+constexpr double kDirectReach = 0.5;  // min-image displacements
+constexpr int kDirectN = 64;
+
+struct Tab64 {
+    const double *t;
+    int n;
+    double h, inv_h;
+};
+
+// C and grad C at y from the FP64 table (positive octant, cubic symmetry)
+__device__ void ew64(const Tab64 &E, double yx, double yy, double yz, double &C, double *G) {
+    const double sx = yx < 0 ? -1.0 : 1.0, sy = yy < 0 ? -1.0 : 1.0, sz = yz < 0 ? -1.0 : 1.0;
+    const double ax = fabs(yx), ay = fabs(yy), az = fabs(yz);
+    const int nm = E.n - 1;
+    const int i = min((int)rint(ax * E.inv_h), nm), j = min((int)rint(ay * E.inv_h), nm),
+              k = min((int)rint(az * E.inv_h), nm);
+    const double dx = ax - i * E.h, dy = ay - j * E.h, dz = az - k * E.h;
+    const double *t = E.t + (((size_t)i * E.n + j) * E.n + k) * 20;
+    const double *G0 = t + 1, *H = t + 4, *T = t + 10;
+    const double Hd0 = H[0] * dx + H[1] * dy + H[2] * dz;
+    const double Hd1 = H[1] * dx + H[3] * dy + H[4] * dz;
+    const double Hd2 = H[2] * dx + H[4] * dy + H[5] * dz;
+    const double xx = dx * dx, xy = 2 * dx * dy, xz = 2 * dx * dz, yyv = dy * dy,
+                 yzv = 2 * dy * dz, zz = dz * dz;
+    const double T0 = T[0] * xx + T[1] * xy + T[2] * xz + T[3] * yyv + T[4] * yzv + T[5] * zz;
+    const double T1 = T[1] * xx + T[3] * xy + T[4] * xz + T[6] * yyv + T[7] * yzv + T[8] * zz;
+    const double T2 = T[2] * xx + T[4] * xy + T[5] * xz + T[7] * yyv + T[8] * yzv + T[9] * zz;
+    C = t[0] + G0[0] * dx + G0[1] * dy + G0[2] * dz + 0.5 * (Hd0 * dx + Hd1 * dy + Hd2 * dz) +
+        (T0 * dx + T1 * dy + T2 * dz) / 6.0;
+    G[0] = sx * (G0[0] + Hd0 + 0.5 * T0);
+    G[1] = sy * (G0[1] + Hd1 + 0.5 * T1);
+    G[2] = sz * (G0[2] + Hd2 + 0.5 * T2);
+}
+
+__global__ void __launch_bounds__(256) k_direct64(const float4 *__restrict__ pts, int64_t n,
+                                                  const int64_t *__restrict__ sinks, double eps2,
+                                                  double box, Tab64 E, double phi0, double *out) {
+    const int64_t i = sinks[blockIdx.x];
+    const float4 s = pts[i];
+    const double xi = s.x, yi = s.y, zi = s.z;
+    double ax = 0, ay = 0, az = 0, ph = 0;
+    for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
+        const float4 p = pts[j];
+        const double m = p.w;
+        if (j == i) {
+            if (eps2 > 0)
+                ph -= m / sqrt(eps2);
+            if (box > 0)
+                ph += m * phi0;
+            continue;
+        }
+        double dx = (double)p.x - xi, dy = (double)p.y - yi, dz = (double)p.z - zi;
+        if (box > 0) {
+            dx -= box * rint(dx / box);
+            dy -= box * rint(dy / box);
+            dz -= box * rint(dz / box);
+        }
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (box > 0 && r2 == 0.0) {
+            ph += m * phi0;
+            if (eps2 > 0)
+                ph -= m / sqrt(eps2);
+            continue;
+        }
+        const double rs2 = r2 + eps2;
+        if (rs2 == 0.0)
+            continue;
+        const double ri = 1.0 / sqrt(rs2);
+        const double mri = m * ri, mri3 = mri * ri * ri;
+        ph -= mri;
+        ax += dx * mri3;
+        ay += dy * mri3;
+        az += dz * mri3;
+        if (box > 0) {
+            double C, G[3];
+            ew64(E, dx, dy, dz, C, G);
+            ph += m * C;
+            ax += m * G[0];
+            ay += m * G[1];
+            az += m * G[2];
+        }
+    }
+    __shared__ double red[4][256];
+    red[0][threadIdx.x] = ax;
+    red[1][threadIdx.x] = ay;
+    red[2][threadIdx.x] = az;
+    red[3][threadIdx.x] = ph;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int q = 0; q < 4; q++) red[q][threadIdx.x] += red[q][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 4; q++) out[4 * blockIdx.x + q] = red[q][0];
+}
+
+}  // namespace
+
+extern "C" int grav_direct_fp64_CUDA(const float *points, int64_t n, const int64_t *sinks,
+                                     int64_t nsink, double eps2, double box, double *out) {
+    if (!points || n <= 0 || !sinks || nsink <= 0 || !out || eps2 < 0 || box < 0)
+        return gc::set_status(-1, "grav_direct_fp64_CUDA: bad arguments");
+    for (int64_t k = 0; k < nsink; k++)
+        if (sinks[k] < 0 || sinks[k] >= n)
+            return gc::set_status(-1, "grav_direct_fp64_CUDA: sink %lld outside the bodies",
+                                  (long long)sinks[k]);
+    std::vector<void *> alloc;
+    auto cleanup = [&]() {
+        for (void *p : alloc) cudaFree(p);
+    };
+    float4 *d_pts = nullptr;
+    int64_t *d_s = nullptr;
+    double *d_out = nullptr, *d_tab = nullptr;
+    cudaError_t e = cudaMalloc(&d_pts, n * sizeof(float4));
+    if (e == cudaSuccess) alloc.push_back(d_pts), e = cudaMalloc(&d_s, nsink * sizeof(int64_t));
+    if (e == cudaSuccess) alloc.push_back(d_s), e = cudaMalloc(&d_out, nsink * 4 * sizeof(double));
+    if (e == cudaSuccess) alloc.push_back(d_out);
+    if (e != cudaSuccess) {
+        cleanup();
+        return gc::cuda_status(e, "grav_direct_fp64_CUDA allocation");
+    }
+    Tab64 E{nullptr, kDirectN, 0, 0};
+    double phi0 = 0;
+    if (box > 0) {
+        std::vector<double> t((size_t)kDirectN * kDirectN * kDirectN * NLN_EWALD_NQ);
+        ewald_table(box, kDirectN, kDirectReach, t.data());
+        e = cudaMalloc(&d_tab, t.size() * sizeof(double));
+        if (e == cudaSuccess)
+            alloc.push_back(d_tab),
+                e = cudaMemcpy(d_tab, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cleanup();
+            return gc::cuda_status(e, "grav_direct_fp64_CUDA table");
+        }
+        E.t = d_tab;
+        E.h = kDirectReach * box / (kDirectN - 1);
+        E.inv_h = 1.0 / E.h;
+        const double alpha = 2.0 / box;
+        phi0 = M_PI / (alpha * alpha * box * box * box);
+    }
+    e = cudaMemcpy(d_pts, points, n * sizeof(float4), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(d_s, sinks, nsink * sizeof(int64_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_direct64<<<(unsigned)nsink, 256>>>(d_pts, n, d_s, eps2, box, E, phi0, d_out);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpy(out, d_out, nsink * 4 * sizeof(double), cudaMemcpyDeviceToHost);
+    cleanup();
+    if (e != cudaSuccess)
+        return gc::cuda_status(e, "grav_direct_fp64_CUDA");
+    return 0;
+}

@@ -14,9 +14,10 @@
 // Work decomposition: a work item is (group, kind, range of its list);
 // long lists are split so that small problems still fill the GPU; every
 // warp pulls items (costliest first) from its kind's queue until it is
-// empty.  One warp owns one item: lane = sink, 32 sources per staged tile,
-// double-buffered TMA bulk copies (one per lane, one record each) signalled
-// on a per-warp mbarrier.
+// empty.  One warp owns one item: lane = sink, 32 sources per staged tile;
+// tiles are staged by TMA row gathers (cp.async.bulk.tensor tile::gather4
+// over a 2-D tensor map of the table, one instruction per 4 records, issued
+// by one lane) into a 2-4 stage ring signalled by per-warp mbarriers.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -24,11 +25,15 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
 #include "common.cuh"
 #include "gravcuda.h"
+#include "ewald.cuh"
+#define NLN_EWALD_NO_EXPORT
+#include "host/ewald_table.cpp"
 #include "interact.cuh"
 
 namespace {
@@ -60,6 +65,12 @@ struct DevProblem {
     float qsh;
     double box;
     unsigned *err;
+    // periodic correction
+    const int64_t *lptr[3];    // per-group list offsets (P expanded, Q, H)
+    int ewald;
+    EwTab ew;
+    float ew_self;             // C(0) - pi/(alpha^2 L^3): the self term ewald() leaves out
+    float ew_trace;            // trace of the Hessian of C: -4 pi / L^3
 };
 
 template <int KIND>
@@ -251,9 +262,77 @@ __global__ void __launch_bounds__(256) k_batch(const __grid_constant__ CUtensorM
     }
 }
 
-// Per group, in slot order: sum the partials of its work items in FP64 and
-// write (ax, ay, az, phi) of each sink, coalesced.
-__global__ void k_reduce(DevProblem P) {
+// Periodic correction moments of group g: every list entry at its centre
+// (bodies and monopole cells as points, quadrupole and order-4 cells with
+// their traceless second moment folded in), lanes striding the lists.
+__device__ void ewald_moments(const DevProblem &P, int64_t g, const double *c, int lane,
+                              float *M) {
+#pragma unroll
+    for (int q = 0; q < 20; q++) M[q] = 0.f;
+    float o[20];
+    for (int64_t k = P.lptr[0][g] + lane; k < P.lptr[0][g + 1]; k += 32) {
+        const uint32_t ent = P.list[0][k];
+        double sx, sy, sz;
+        decode_shift(ent >> NLN_IDX_BITS, P.box, sx, sy, sz);
+        const float4 p = P.points[ent & NLN_IDX_MASK];
+        ew_lookup(P.ew, (float)((double)p.x + sx - c[0]), (float)((double)p.y + sy - c[1]),
+                  (float)((double)p.z + sz - c[2]), o);
+#pragma unroll
+        for (int q = 0; q < 20; q++) M[q] = fmaf(p.w, o[q], M[q]);
+    }
+    for (int kind = 1; kind < 3; kind++) {
+        if (!P.list[kind])
+            continue;
+        for (int64_t k = P.lptr[kind][g] + lane; k < P.lptr[kind][g + 1]; k += 32) {
+            const uint32_t ent = P.list[kind][k];
+            const uint32_t ci = ent & NLN_IDX_MASK;
+            double sx, sy, sz;
+            decode_shift(ent >> NLN_IDX_BITS, P.box, sx, sy, sz);
+            double cx, cy, cz;
+            float m, R, B2, q2[5];
+            if (kind == 1) {
+                const nln_qcell &q = P.qcells[ci];
+                cx = q.cen[0]; cy = q.cen[1]; cz = q.cen[2];
+                m = q.mass; R = q.R; B2 = q.B2;
+                q2[0] = q.qxx; q2[1] = q.qxy; q2[2] = q.qyy; q2[3] = q.qxz; q2[4] = q.qyz;
+            } else {
+                const nln_hcell &h = P.hcells[ci];
+                cx = h.cen[0]; cy = h.cen[1]; cz = h.cen[2];
+                m = h.mass; R = h.R; B2 = h.B2;
+#pragma unroll
+                for (int t = 0; t < 5; t++) q2[t] = h.q2[t];
+            }
+            ew_lookup(P.ew, (float)(cx + sx - c[0]), (float)(cy + sy - c[1]),
+                      (float)(cz + sz - c[2]), o);
+#pragma unroll
+            for (int q = 0; q < 20; q++) M[q] = fmaf(m, o[q], M[q]);
+            // second moment sum m xi xi = Q + B2/3 I, Q = R^2 q2 traceless:
+            // phi += 1/2 Q:ddC + B2/6 tr ddC ;  grad += 1/2 dddC[Q]
+            const float R2 = R * R;
+            const float Q[6] = {R2 * q2[0], R2 * q2[1], R2 * q2[3], R2 * q2[2], R2 * q2[4],
+                                -R2 * (q2[0] + q2[2])};
+            const float *H = o + 4;
+            M[0] += 0.5f * (Q[0] * H[0] + 2.f * Q[1] * H[1] + 2.f * Q[2] * H[2] + Q[3] * H[3] +
+                            2.f * Q[4] * H[4] + Q[5] * H[5]) +
+                    (B2 / 6.f) * P.ew_trace;
+            float v[3];
+            t_q(o + 10, Q, v);
+            M[1] += 0.5f * v[0];
+            M[2] += 0.5f * v[1];
+            M[3] += 0.5f * v[2];
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 20; q++) {
+        float x = M[q];
+        for (int d = 16; d > 0; d >>= 1) x += __shfl_xor_sync(0xffffffffu, x, d);
+        M[q] = x;
+    }
+}
+
+// Per group, in slot order: sum the partials of its work items in FP64,
+// add the periodic correction, and write (ax, ay, az, phi) of each sink.
+__global__ void k_finish(DevProblem P) {
     const int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (g >= P.ngroups)
@@ -267,6 +346,21 @@ __global__ void k_reduce(DevProblem P) {
         s[1] += (double)h.y + (double)l.y;
         s[2] += (double)h.z + (double)l.z;
         s[3] += (double)h.w + (double)l.w;
+    }
+    if (P.ewald) {
+        const double c[3] = {G.cen[0], G.cen[1], G.cen[2]};
+        float M[20];
+        ewald_moments(P, g, c, lane, M);
+        if (lane < G.count) {
+            const float4 p = P.points[G.first + lane];
+            float phi, ax, ay, az;
+            ew_apply(M, (float)((double)p.x - c[0]), (float)((double)p.y - c[1]),
+                     (float)((double)p.z - c[2]), phi, ax, ay, az);
+            s[0] += ax;
+            s[1] += ay;
+            s[2] += az;
+            s[3] += phi - p.w * P.ew_self;
+        }
     }
     if (lane < G.count)
         P.out[G.first + lane] = make_float4((float)s[0], (float)s[1], (float)s[2], (float)s[3]);
@@ -285,6 +379,8 @@ struct grav_plan {
     int launches = 0;
     int64_t nslots = 0;
     CUtensorMap tmap[3];    // row-gather views of the point, quadrupole and order-4 tables
+    int timing = 0;         // record events around each kernel of an evaluation
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace {
@@ -336,6 +432,7 @@ grav_tuning default_tuning() {
     t.warps_per_block = 8;
     t.blocks_per_sm = 0;
     t.chunk_p = t.chunk_q = t.chunk_h = 0;
+    t.ewald_n = 0;
     return t;
 }
 
@@ -367,41 +464,35 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
     pl->tune = tuning ? *tuning : default_tuning();
     const int64_t ng = hp->ngroups, nb = hp->nbodies, np = hp->nbodies + hp->ncells;
 
-    // expand point runs into per-record entries; validate everything we index
-    std::vector<int64_t> eptr(ng + 1, 0);
+    // validate everything the kernels will index
+    int bad_group = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad_group)
     for (int64_t g = 0; g < ng; g++) {
-        int64_t n = 0;
-        for (int64_t k = hp->pptr[g]; k < hp->pptr[g + 1]; k++) n += hp->plist[k].len;
-        eptr[g + 1] = eptr[g] + n;
         const nln_group &G = hp->groups[g];
-        if (G.count < 1 || G.count > 32 || G.first < 0 || G.first + G.count > nb) {
-            delete pl;
-            return gc::set_status(-1, "group %lld: %d sinks at %lld (1..32 sinks inside the bodies)",
-                                  (long long)g, G.count, (long long)G.first);
-        }
+        if (G.count < 1 || G.count > 32 || G.first < 0 || G.first + G.count > nb)
+            bad_group |= 1;
+        if (hp->pptr[g + 1] < hp->pptr[g] || (hp->qptr && hp->qptr[g + 1] < hp->qptr[g]) ||
+            (hp->hptr && hp->hptr[g + 1] < hp->hptr[g]))
+            bad_group |= 1;
     }
-    std::vector<uint32_t> pent(eptr[ng]);
-    for (int64_t g = 0; g < ng; g++) {
-        int64_t o = eptr[g];
-        for (int64_t k = hp->pptr[g]; k < hp->pptr[g + 1]; k++) {
-            const nln_pseg s = hp->plist[k];
-            if ((int64_t)s.base + s.len > np || s.shift > 26) {
-                delete pl;
-                return gc::set_status(-1, "point run %lld outside the table", (long long)k);
-            }
-            for (uint32_t j = 0; j < s.len; j++)
-                pent[o++] = (s.base + j) | ((uint32_t)s.shift << NLN_IDX_BITS);
-        }
+    if (bad_group) {
+        delete pl;
+        return gc::set_status(-1, "a group has 0 or more than 32 sinks, lies outside the bodies, "
+                                  "or has decreasing list offsets");
     }
-    auto check_cells = [&](const int64_t *ptr, const uint32_t *lst) -> bool {
+    auto check_list = [&](const int64_t *ptr, const uint32_t *lst, int64_t ntab) -> bool {
         if (!ptr)
             return true;
+        int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
         for (int64_t k = 0; k < ptr[ng]; k++)
-            if ((int64_t)(lst[k] & NLN_IDX_MASK) >= hp->ncells || (lst[k] >> NLN_IDX_BITS) > 26)
-                return false;
-        return true;
+            if ((int64_t)(lst[k] & NLN_IDX_MASK) >= ntab || (lst[k] >> NLN_IDX_BITS) > 26)
+                bad |= 1;
+        return !bad;
     };
-    if (!check_cells(hp->qptr, hp->qlist) || !check_cells(hp->hptr, hp->hlist) ||
+    const int64_t *eptr = hp->pptr;
+    if (!check_list(hp->pptr, hp->plist, np) || !check_list(hp->qptr, hp->qlist, hp->ncells) ||
+        !check_list(hp->hptr, hp->hlist, hp->ncells) ||
         (hp->qptr && hp->qptr[ng] && !hp->qcells) || (hp->hptr && hp->hptr[ng] && !hp->hcells)) {
         delete pl;
         return gc::set_status(-1, "cell list entry outside the cell table");
@@ -419,7 +510,7 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
     // work items, created group by group (slot order), then sorted per kind by cost
     std::vector<Item> items[3];
     std::vector<int64_t> gslot(ng + 1, 0);
-    const int64_t *ptrs[3] = {eptr.data(), hp->qptr, hp->hptr};
+    const int64_t *ptrs[3] = {eptr, hp->qptr, hp->hptr};
     const int chunk[3] = {pl->tune.chunk_p, pl->tune.chunk_q, pl->tune.chunk_h};
     int32_t slot = 0;
     for (int64_t g = 0; g < ng; g++) {
@@ -438,10 +529,21 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
         });
 
     // interaction counts (sinks x sources)
+    int64_t cb = 0, cm = 0;
+#pragma omp parallel for schedule(static) reduction(+ : cb, cm)
     for (int64_t g = 0; g < ng; g++) {
         const int64_t c = hp->groups[g].count;
-        for (int64_t k = hp->pptr[g]; k < hp->pptr[g + 1]; k++)
-            pl->counts[hp->plist[k].base < (uint32_t)nb ? 0 : 1] += c * hp->plist[k].len;
+        for (int64_t k = hp->pptr[g]; k < hp->pptr[g + 1]; k++) {
+            if ((hp->plist[k] & NLN_IDX_MASK) < (uint32_t)nb)
+                cb += c;
+            else
+                cm += c;
+        }
+    }
+    pl->counts[0] = cb;
+    pl->counts[1] = cm;
+    for (int64_t g = 0; g < ng; g++) {
+        const int64_t c = hp->groups[g].count;
         if (hp->qptr)
             pl->counts[2] += c * (hp->qptr[g + 1] - hp->qptr[g]);
         if (hp->hptr)
@@ -465,7 +567,7 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
     rc |= dev_copy(pl, hp->groups, (size_t)ng, &gr);
     d.groups = gr;
     uint32_t *l0 = nullptr, *l1 = nullptr, *l2 = nullptr;
-    rc |= dev_copy(pl, pent.data(), pent.size(), &l0);
+    rc |= dev_copy(pl, hp->plist, (size_t)hp->pptr[ng], &l0);
     if (hp->qptr)
         rc |= dev_copy(pl, hp->qlist, (size_t)hp->qptr[ng], &l1);
     if (hp->hptr)
@@ -490,6 +592,46 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
     int64_t *gs = nullptr;
     rc |= dev_copy(pl, gslot.data(), gslot.size(), &gs);
     d.gslot = gs;
+    int64_t *lp0 = nullptr, *lp1 = nullptr, *lp2 = nullptr;
+    rc |= dev_copy(pl, eptr, (size_t)ng + 1, &lp0);
+    if (hp->qptr)
+        rc |= dev_copy(pl, hp->qptr, (size_t)ng + 1, &lp1);
+    if (hp->hptr)
+        rc |= dev_copy(pl, hp->hptr, (size_t)ng + 1, &lp2);
+    d.lptr[0] = lp0;
+    d.lptr[1] = lp1;
+    d.lptr[2] = lp2;
+    d.ewald = 0;
+    if (hp->box > 0 && hp->ewald) {
+        // FP64 table on the host, FP32 copy on the device
+        const int n = pl->tune.ewald_n > 1 ? pl->tune.ewald_n : 64;
+        // the table depends only on (box, n): build it once per process
+        static std::mutex cache_mu;
+        static double cache_box = 0;
+        static int cache_n = 0;
+        static std::vector<double> t64;
+        {
+            std::lock_guard<std::mutex> lk(cache_mu);
+            if (cache_box != hp->box || cache_n != n) {
+                t64.assign((size_t)n * n * n * NLN_EWALD_NQ, 0.0);
+                if (ewald_table(hp->box, n, NLN_EWALD_REACH, t64.data())) {
+                    grav_plan_free(pl);
+                    return gc::set_status(-1, "Ewald table build failed");
+                }
+                cache_box = hp->box;
+                cache_n = n;
+            }
+        }
+        std::vector<float> t32(t64.begin(), t64.end());
+        float *tab = nullptr;
+        rc |= dev_copy(pl, t32.data(), t32.size(), &tab);
+        const double h = NLN_EWALD_REACH * hp->box / (n - 1);
+        d.ew = EwTab{tab, n, (float)h, (float)(1.0 / h)};
+        const double alpha = 2.0 / hp->box;
+        d.ew_self = (float)(t64[0] - M_PI / (alpha * alpha * hp->box * hp->box * hp->box));
+        d.ew_trace = (float)(-4.0 * M_PI / (hp->box * hp->box * hp->box));
+        d.ewald = 1;
+    }
     float4 *out = nullptr;
     rc |= dev_copy<float4>(pl, nullptr, (size_t)nb, &out);
     d.out = out;
@@ -552,17 +694,47 @@ extern "C" int grav_groups_eval_CUDA(grav_plan *pl, void *stream) {
         return gc::set_status(-1, "grav_groups_eval_CUDA: no plan");
     cudaStream_t st = (cudaStream_t)stream;
     pl->launches = 0;
+    auto mark = [&](int k) -> int {
+        if (pl->timing)
+            GC_CHECK(cudaEventRecord(pl->ev[k], st));
+        return 0;
+    };
     GC_CHECK(cudaMemsetAsync(pl->dp.counters, 0, 4 * sizeof(int), st));
+    if (int rc = mark(0))
+        return rc;
     if (int rc = launch_kind<KH>(pl, st))
+        return rc;
+    if (int rc = mark(1))
         return rc;
     if (int rc = launch_kind<KQ>(pl, st))
         return rc;
+    if (int rc = mark(2))
+        return rc;
     if (int rc = launch_kind<KP>(pl, st))
         return rc;
+    if (int rc = mark(3))
+        return rc;
     const int wpb = 8;
-    k_reduce<<<(unsigned)((pl->dp.ngroups + wpb - 1) / wpb), wpb * 32, 0, st>>>(pl->dp);
+    k_finish<<<(unsigned)((pl->dp.ngroups + wpb - 1) / wpb), wpb * 32, 0, st>>>(pl->dp);
     GC_CHECK(cudaGetLastError());
     pl->launches++;
+    return mark(4);
+}
+
+extern "C" int grav_plan_set_timing(grav_plan *pl, int on) {
+    if (!pl)
+        return gc::set_status(-1, "grav_plan_set_timing: no plan");
+    if (on && !pl->ev[0])
+        for (int k = 0; k < 5; k++) GC_CHECK(cudaEventCreate(&pl->ev[k]));
+    pl->timing = on ? 1 : 0;
+    return 0;
+}
+
+extern "C" int grav_plan_kernel_ms(grav_plan *pl, float ms[4]) {
+    if (!pl || !pl->timing)
+        return gc::set_status(-1, "grav_plan_kernel_ms: timing is off");
+    GC_CHECK(cudaEventSynchronize(pl->ev[4]));
+    for (int k = 0; k < 4; k++) GC_CHECK(cudaEventElapsedTime(&ms[k], pl->ev[k], pl->ev[k + 1]));
     return 0;
 }
 
@@ -594,6 +766,9 @@ extern "C" void grav_plan_free(grav_plan *pl) {
     if (!pl)
         return;
     for (void *p : pl->allocs) cudaFree(p);
+    for (cudaEvent_t e : pl->ev)
+        if (e)
+            cudaEventDestroy(e);
     delete pl;
 }
 

@@ -93,7 +93,7 @@ struct nln_tree {
     std::vector<nln_group> groups;
     
     std::vector<int64_t> lptr[3];
-    std::vector<nln_pseg> plist;
+    std::vector<uint32_t> plist;
     std::vector<uint32_t> qlist, hlist;
     std::vector<int64_t> aptr[3];
     std::vector<float> adata[3];
@@ -269,6 +269,7 @@ static void compute_moments(nln_tree *t) {
         for (int d = 0; d < 3; d++) q.cen[d] = h.cen[d] = c.cen[d];
         q.mass = h.mass = (float)m;
         q.R = h.R = (float)c.bmax;
+        q.B2 = h.B2 = (float)c.B2;
         q.qxx = (float)q2[0];
         q.qxy = (float)q2[1];
         q.qyy = (float)q2[2];
@@ -526,7 +527,7 @@ extern "C" void nln_tree_free(nln_tree *t) { delete t; }
 namespace {
 
 struct GroupLists {
-    std::vector<nln_pseg> p;
+    std::vector<uint32_t> p;   // point-table record | image << 27
     std::vector<uint32_t> q, h;
     int64_t nb = 0, nm = 0;
 };
@@ -571,7 +572,7 @@ static void walk_group(const nln_tree *t, const nln_group &G, GroupLists &L,
         const uint16_t sc = shift_code(s);
         if (inside && c.count > 0) {
             if (dd > c.rc_m + c.bmax) {
-                L.p.push_back(nln_pseg{(uint32_t)(t->n + ci), 1, sc});
+                L.p.push_back((uint32_t)(t->n + ci) | ((uint32_t)sc << NLN_IDX_BITS));
                 L.nm++;
                 covered += c.count;
                 continue;
@@ -593,20 +594,15 @@ static void walk_group(const nln_tree *t, const nln_group &G, GroupLists &L,
         }
         // leaf: expand to bodies (nln/mac.c:1817-1832)
         if (inside || box <= 0) {
-            L.p.push_back(nln_pseg{(uint32_t)c.first, (uint16_t)c.count, sc});
+            for (int32_t k = 0; k < c.count; k++)
+                L.p.push_back((uint32_t)(c.first + k) | ((uint32_t)sc << NLN_IDX_BITS));
         } else {
-            // a leaf straddling the group's half-box: each body its own image
+            // a leaf reaching out of the correction's domain: each body its own image
             for (int32_t k = 0; k < c.count; k++) {
                 const float *x = &t->spos[3 * (c.first + k)];
                 int sb[3];
                 for (int d = 0; d < 3; d++) sb[d] = -(int)std::nearbyint((x[d] - G.cen[d]) / box);
-                uint16_t scb = shift_code(sb);
-                if (!L.p.empty() && L.p.back().shift == scb &&
-                    L.p.back().base + L.p.back().len == (uint32_t)(c.first + k) &&
-                    L.p.back().len < 65535 && L.p.back().base < (uint32_t)t->n)
-                    L.p.back().len++;
-                else
-                    L.p.push_back(nln_pseg{(uint32_t)(c.first + k), 1, scb});
+                L.p.push_back((uint32_t)(c.first + k) | ((uint32_t)shift_code(sb) << NLN_IDX_BITS));
             }
         }
         L.nb += c.count;
@@ -628,10 +624,8 @@ static void emit_aosoa(nln_tree *t, const std::vector<GroupLists> &GL) {
         ptr.assign(ng + 1, 0);
         for (int64_t g = 0; g < ng; g++) {
             int64_t nrec = 0;
-            if (kind == 0)
-                for (const nln_pseg &s : GL[g].p) nrec += s.len;
-            else
-                nrec = (int64_t)(kind == 1 ? GL[g].q.size() : GL[g].h.size());
+            nrec = (int64_t)(kind == 0 ? GL[g].p.size()
+                                       : (kind == 1 ? GL[g].q.size() : GL[g].h.size()));
             ptr[g + 1] = ptr[g] + (nrec + 7) / 8;
         }
         t->adata[kind].assign((size_t)ptr[ng] * SZ[kind] * 8, 0.0f);
@@ -642,16 +636,16 @@ static void emit_aosoa(nln_tree *t, const std::vector<GroupLists> &GL) {
         {
             float *f = t->adata[0].data() + (size_t)t->aptr[0][g] * 4 * 8;
             int64_t r = 0;
-            for (const nln_pseg &s : GL[g].p) {
-                int sh[3] = {(int)s.shift / 9 - 1, (int)(s.shift / 3) % 3 - 1, (int)s.shift % 3 - 1};
-                for (uint32_t k = 0; k < s.len; k++, r++) {
-                    const float *pt = &t->points[4 * ((size_t)s.base + k)];
-                    float *blk = f + (r / 8) * 4 * 8;
-                    int l = (int)(r % 8);
-                    blk[0 * 8 + l] = pt[3];
-                    for (int d = 0; d < 3; d++)
-                        blk[(1 + d) * 8 + l] = (float)((double)pt[d] + sh[d] * box);
-                }
+            for (const uint32_t e : GL[g].p) {
+                const uint32_t sc = e >> NLN_IDX_BITS;
+                int sh[3] = {(int)sc / 9 - 1, (int)(sc / 3) % 3 - 1, (int)sc % 3 - 1};
+                const float *pt = &t->points[4 * (size_t)(e & NLN_IDX_MASK)];
+                float *blk = f + (r / 8) * 4 * 8;
+                int l = (int)(r % 8);
+                blk[0 * 8 + l] = pt[3];
+                for (int d = 0; d < 3; d++)
+                    blk[(1 + d) * 8 + l] = (float)((double)pt[d] + sh[d] * box);
+                r++;
             }
         }
         for (int kind = 1; kind < 3; kind++) {
@@ -757,4 +751,56 @@ extern "C" const int64_t *nln_aosoa_ptr(const nln_tree *t, int kind) {
 }
 extern "C" const float *nln_aosoa_data(const nln_tree *t, int kind) {
     return (kind >= 0 && kind < 3 && !t->adata[kind].empty()) ? t->adata[kind].data() : nullptr;
+}
+
+// Reference AoSoA blocks (nln/mac.c:117-153) for a subset of groups, packed
+// from the index lists: kind 0 = M (bodies and monopole cells, MSZ 4), 1 = Q
+// (QSZ 13), 2 = H (HSZ 29).  With data == NULL only blk_ptr (ngsel + 1
+// entries) is filled; the return value is the total block count.
+extern "C" int64_t nln_aosoa_subset(const nln_tree *t, const int64_t *gids, int64_t ngsel,
+                                    int kind, int64_t *blk_ptr, float *data) {
+    if (!t || kind < 0 || kind > 2 || t->lptr[kind].empty())
+        return -1;
+    static const int SZ[3] = {4, 13, 29};
+    const int sz = SZ[kind];
+    const std::vector<uint32_t> &lst = kind == 0 ? t->plist : (kind == 1 ? t->qlist : t->hlist);
+    const int64_t *ptr = t->lptr[kind].data();
+    blk_ptr[0] = 0;
+    for (int64_t s = 0; s < ngsel; s++) {
+        const int64_t g = gids[s];
+        blk_ptr[s + 1] = blk_ptr[s] + (ptr[g + 1] - ptr[g] + 7) / 8;
+    }
+    if (!data)
+        return blk_ptr[ngsel];
+    const double box = t->p.box;
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int64_t s = 0; s < ngsel; s++) {
+        const int64_t g = gids[s];
+        float *f = data + (size_t)blk_ptr[s] * sz * 8;
+        std::fill(f, f + (size_t)(blk_ptr[s + 1] - blk_ptr[s]) * sz * 8, 0.0f);
+        for (int64_t r = 0; r < ptr[g + 1] - ptr[g]; r++) {
+            const uint32_t e = lst[ptr[g] + r];
+            const uint32_t idx = e & NLN_IDX_MASK, sc = e >> NLN_IDX_BITS;
+            const int sh[3] = {(int)sc / 9 - 1, (int)(sc / 3) % 3 - 1, (int)sc % 3 - 1};
+            float *blk = f + (r / 8) * sz * 8;
+            const int l = (int)(r % 8);
+            if (kind == 0) {
+                const float *pt = &t->points[4 * (size_t)idx];
+                blk[l] = pt[3];
+                for (int d = 0; d < 3; d++)
+                    blk[(1 + d) * 8 + l] = (float)((double)pt[d] + sh[d] * box);
+            } else {
+                const nln_hcell &h = t->hc[idx];
+                blk[l] = h.mass;
+                for (int d = 0; d < 3; d++) blk[(1 + d) * 8 + l] = (float)(h.cen[d] + sh[d] * box);
+                blk[4 * 8 + l] = h.R;
+                for (int k = 0; k < 5; k++) blk[(8 + k) * 8 + l] = h.q2[k];
+                if (kind == 2) {
+                    for (int k = 0; k < 7; k++) blk[(13 + k) * 8 + l] = h.q3[k];
+                    for (int k = 0; k < 9; k++) blk[(20 + k) * 8 + l] = h.q4[k];
+                }
+            }
+        }
+    }
+    return blk_ptr[ngsel];
 }

@@ -74,11 +74,11 @@ def build_cuda(force=False, verbose_ptxas=False):
     deps = srcs + cuda_headers() + [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE)]
     if force or _newer(CUDA_SO, deps):
         cmd = [_nvcc()] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-shared",
-                                  "-Xcompiler", "-fPIC", "-ccbin", _cxx(),
+                                  "-Xcompiler", "-fPIC,-fopenmp", "-ccbin", _cxx(),
                                   "-I", INCLUDE, "-I", CSRC, "-o", CUDA_SO]
         if verbose_ptxas:
             cmd += ["-Xptxas", "-v"]
-        _run(cmd + srcs + ["-lcudart"])
+        _run(cmd + srcs + ["-lcudart", "-lgomp"])
     return CUDA_SO
 
 

@@ -10,7 +10,7 @@ import os
 import numpy as np
 
 from . import _build
-from .host import GROUP_DTYPE, HCELL_DTYPE, PSEG_DTYPE, QCELL_DTYPE
+from .host import GROUP_DTYPE, HCELL_DTYPE, QCELL_DTYPE  # noqa: F401
 
 _lib = None
 
@@ -23,7 +23,7 @@ EXPORTS = [
     "gravcuda_clear_status", "grav_mn_status_CUDA", "gravcuda_peek_accumulators",
     "grav_groups_upload_CUDA", "grav_groups_eval_CUDA", "grav_groups_download_CUDA",
     "grav_plan_output", "grav_plan_counts", "grav_plan_launches", "grav_plan_free",
-    "grav_groups_CUDA",
+    "grav_groups_CUDA", "grav_direct_fp64_CUDA", "grav_plan_set_timing", "grav_plan_kernel_ms",
 ]
 
 
@@ -49,7 +49,7 @@ class Problem(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("warps_per_block", ctypes.c_int), ("chunk_p", ctypes.c_int),
                 ("chunk_q", ctypes.c_int), ("chunk_h", ctypes.c_int),
-                ("blocks_per_sm", ctypes.c_int)]
+                ("blocks_per_sm", ctypes.c_int), ("ewald_n", ctypes.c_int)]
 
 
 def lib(record_errors=True):
@@ -85,6 +85,8 @@ def lib(record_errors=True):
             "grav_plan_output": ([vp], vp), "grav_plan_counts": ([vp, vp], None),
             "grav_plan_launches": ([vp], i32), "grav_plan_free": ([vp], None),
             "grav_groups_CUDA": ([vp, vp], i32),
+            "grav_direct_fp64_CUDA": ([vp, i64, vp, i64, f64, f64, vp], i32),
+            "grav_plan_set_timing": ([vp, i32], i32), "grav_plan_kernel_ms": ([vp, vp], i32),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -136,7 +138,7 @@ class Plan:
         prob.pptr = keep(t.ptr[0]).ctypes.data
         prob.qptr = keep(t.ptr[1]).ctypes.data
         prob.hptr = keep(t.ptr[2]).ctypes.data
-        prob.plist = keep(t.plist).ctypes.data if len(t.plist) else keep(np.zeros(1, PSEG_DTYPE)).ctypes.data
+        prob.plist = keep(t.plist).ctypes.data if len(t.plist) else keep(np.zeros(1, np.uint32)).ctypes.data
         prob.qlist = keep(t.qlist).ctypes.data if has_q else keep(np.zeros(1, np.uint32)).ctypes.data
         prob.hlist = keep(t.hlist).ctypes.data if has_h else keep(np.zeros(1, np.uint32)).ctypes.data
         prob.eps2 = float(eps2)
@@ -173,6 +175,15 @@ class Plan:
 
     def launches(self):
         return lib().grav_plan_launches(self._h)
+
+    def set_timing(self, on=True):
+        check(lib().grav_plan_set_timing(self._h, int(bool(on))))
+
+    def kernel_ms(self):
+        """Per-kernel milliseconds of the last evaluation: order-4, quadrupole, point, finish."""
+        ms = (ctypes.c_float * 4)()
+        check(lib().grav_plan_kernel_ms(self._h, ms))
+        return dict(zip(("hexa", "quad", "point", "finish"), list(ms)))
 
     def free(self):
         if getattr(self, "_h", None):
@@ -261,3 +272,66 @@ class DropIn:
         L.WalkTerminateSinkCUDA(self.btab.ctypes.data, BODY_STRIDE, len(self.btab))
         check()
         return self.btab[:, 7:11].copy()
+
+
+def direct_fp64(points, sinks, eps2, box=0.0):
+    """FP64 direct sum on the GPU at sample sinks (grav_direct_fp64_CUDA):
+    (nsink, 4) doubles (ax, ay, az, phi); Ewald-summed when box > 0."""
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 4)
+    sinks = np.ascontiguousarray(sinks, np.int64)
+    out = np.zeros((len(sinks), 4), np.float64)
+    check(lib().grav_direct_fp64_CUDA(pts.ctypes.data, len(pts), sinks.ctypes.data, len(sinks),
+                                      float(eps2), float(box), out.ctypes.data))
+    return out
+
+
+class PinnedProblem:
+    """A tree's tables and lists copied into page-locked host memory, as the
+    host side of an end-to-end grav_groups_CUDA call reads them."""
+
+    def __init__(self, tree):
+        import torch
+        self._keep = []
+        self.h2d_bytes = 0
+
+        def pin(a):
+            a = np.ascontiguousarray(a)
+            buf = torch.empty(max(1, a.nbytes), dtype=torch.uint8, pin_memory=True)
+            v = buf.numpy()[:a.nbytes].view(a.dtype).reshape(a.shape)
+            v[...] = a
+            self._keep.append(buf)
+            self.h2d_bytes += a.nbytes
+            return v
+
+        t = tree
+        p = Problem()
+        p.nbodies, p.ncells, p.ngroups = t.n, t.ncells, t.ngroups
+        p.points = pin(t.points).ctypes.data
+        has_q, has_h = len(t.qlist) > 0, len(t.hlist) > 0
+        p.qcells = pin(t.qcells).ctypes.data if has_q else None
+        p.hcells = pin(t.hcells).ctypes.data if has_h else None
+        p.groups = pin(t.groups).ctypes.data
+        p.pptr = pin(t.ptr[0]).ctypes.data
+        p.qptr = pin(t.ptr[1]).ctypes.data
+        p.hptr = pin(t.ptr[2]).ctypes.data
+        p.plist = pin(t.plist if len(t.plist) else np.zeros(1, np.uint32)).ctypes.data
+        p.qlist = pin(t.qlist if has_q else np.zeros(1, np.uint32)).ctypes.data
+        p.hlist = pin(t.hlist if has_h else np.zeros(1, np.uint32)).ctypes.data
+        p.quad_phi_sign = 1.0
+        self.problem = p
+        buf = torch.empty(t.n * 16, dtype=torch.uint8, pin_memory=True)
+        self._keep.append(buf)
+        self.out = buf.numpy().view(np.float32).reshape(t.n, 4)
+
+
+def pinned_problem(tree):
+    return PinnedProblem(tree)
+
+
+def groups_eval_problem(pp, eps2, box, ewald=False):
+    """grav_groups_CUDA on a PinnedProblem: upload, evaluate, download, free."""
+    pp.problem.eps2 = float(eps2)
+    pp.problem.box = float(box)
+    pp.problem.ewald = int(bool(ewald))
+    check(lib().grav_groups_CUDA(ctypes.byref(pp.problem), pp.out.ctypes.data))
+    return pp.out

@@ -10,13 +10,12 @@ from . import _build
 _lib = None
 
 QCELL_DTYPE = np.dtype([("cen", "<f8", 3), ("mass", "<f4"), ("R", "<f4"), ("q2", "<f4", 5),
-                        ("pad", "<f4", 3)])
+                        ("B2", "<f4"), ("pad", "<f4", 2)])
 HCELL_DTYPE = np.dtype([("cen", "<f8", 3), ("mass", "<f4"), ("R", "<f4"), ("q2", "<f4", 5),
-                        ("q3", "<f4", 7), ("q4", "<f4", 9), ("pad", "<f4", 3)])
-PSEG_DTYPE = np.dtype([("base", "<u4"), ("len", "<u2"), ("shift", "<u2")])
+                        ("q3", "<f4", 7), ("q4", "<f4", 9), ("B2", "<f4"), ("pad", "<f4", 2)])
 GROUP_DTYPE = np.dtype([("cen", "<f8", 3), ("first", "<i8"), ("count", "<i4"), ("radius", "<f4")])
 assert QCELL_DTYPE.itemsize == 64 and HCELL_DTYPE.itemsize == 128
-assert PSEG_DTYPE.itemsize == 8 and GROUP_DTYPE.itemsize == 40
+assert GROUP_DTYPE.itemsize == 40
 
 SHIFT_NONE = 13
 IDX_BITS = 27
@@ -59,16 +58,36 @@ def lib():
         L.nln_list_len.argtypes = [vp, ctypes.c_int]
         L.nln_list_len.restype = ctypes.c_int64
         L.nln_counts.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.nln_aosoa_subset.argtypes = [vp, vp, ctypes.c_int64, ctypes.c_int, vp, vp]
+        L.nln_aosoa_subset.restype = ctypes.c_int64
         _lib = L
     return _lib
 
 
-def _view(ptr, dtype, count):
+class _Handle:
+    """Owns one nln_tree; freed when the last array viewing its memory goes."""
+
+    def __init__(self, h):
+        self.h = h
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().nln_tree_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def _view(ptr, dtype, count, owner=None):
+    """A zero-copy array over library memory; the buffer keeps `owner` (the
+    tree's handle) alive as long as the array exists."""
     if count == 0 or not ptr:
         return np.zeros(0, dtype=dtype)
     dt = np.dtype(dtype)
     buf = (ctypes.c_char * (dt.itemsize * count)).from_address(ptr)
-    return np.frombuffer(buf, dtype=dt, count=count).copy()
+    buf._owner = owner
+    return np.frombuffer(buf, dtype=dt, count=count)
 
 
 class Tree:
@@ -91,16 +110,17 @@ class Tree:
         if not h:
             raise ValueError(L.nln_last_error().decode())
         self._h = h
+        self._owner = _Handle(h)
         self.n = L.nln_nbodies(h)
         self.ncells = L.nln_ncells(h)
         self.box = float(box)
-        self.order = _view(L.nln_order(h), np.int64, self.n)
-        self.sorted_pos = _view(L.nln_sorted_pos(h), np.float32, 3 * self.n).reshape(-1, 3)
-        self.points = _view(L.nln_points(h), np.float32, 4 * (self.n + self.ncells)).reshape(-1, 4)
-        self.qcells = _view(L.nln_qcells(h), QCELL_DTYPE, self.ncells)
-        self.hcells = _view(L.nln_hcells(h), HCELL_DTYPE, self.ncells)
+        self.order = _view(L.nln_order(h), np.int64, self.n, self._owner)
+        self.sorted_pos = _view(L.nln_sorted_pos(h), np.float32, 3 * self.n, self._owner).reshape(-1, 3)
+        self.points = _view(L.nln_points(h), np.float32, 4 * (self.n + self.ncells), self._owner).reshape(-1, 4)
+        self.qcells = _view(L.nln_qcells(h), QCELL_DTYPE, self.ncells, self._owner)
+        self.hcells = _view(L.nln_hcells(h), HCELL_DTYPE, self.ncells, self._owner)
         self.ngroups = L.nln_ngroups(h)
-        self.groups = _view(L.nln_groups(h), GROUP_DTYPE, self.ngroups)
+        self.groups = _view(L.nln_groups(h), GROUP_DTYPE, self.ngroups, self._owner)
         if walk:
             self.walk()
 
@@ -109,10 +129,10 @@ class Tree:
         if L.nln_tree_walk(self._h) != 0:
             raise RuntimeError("walk failed")
         ng = self.ngroups
-        self.ptr = [_view(L.nln_list_ptr(self._h, k), np.int64, ng + 1) for k in range(3)]
-        self.plist = _view(L.nln_list_data(self._h, 0), PSEG_DTYPE, L.nln_list_len(self._h, 0))
-        self.qlist = _view(L.nln_list_data(self._h, 1), np.uint32, L.nln_list_len(self._h, 1))
-        self.hlist = _view(L.nln_list_data(self._h, 2), np.uint32, L.nln_list_len(self._h, 2))
+        self.ptr = [_view(L.nln_list_ptr(self._h, k), np.int64, ng + 1, self._owner) for k in range(3)]
+        self.plist = _view(L.nln_list_data(self._h, 0), np.uint32, L.nln_list_len(self._h, 0), self._owner)
+        self.qlist = _view(L.nln_list_data(self._h, 1), np.uint32, L.nln_list_len(self._h, 1), self._owner)
+        self.hlist = _view(L.nln_list_data(self._h, 2), np.uint32, L.nln_list_len(self._h, 2), self._owner)
         c = (ctypes.c_int64 * 4)()
         L.nln_counts(self._h, c)
         self.counts = np.array(list(c), dtype=np.int64)
@@ -120,9 +140,26 @@ class Tree:
         if self.params.emit_aosoa:
             self.aosoa = []
             for k, sz in enumerate((4, 13, 29)):
-                ptr = _view(L.nln_aosoa_ptr(self._h, k), np.int64, ng + 1)
-                data = _view(L.nln_aosoa_data(self._h, k), np.float32, int(ptr[-1]) * sz * 8)
+                ptr = _view(L.nln_aosoa_ptr(self._h, k), np.int64, ng + 1, self._owner)
+                data = _view(L.nln_aosoa_data(self._h, k), np.float32, int(ptr[-1]) * sz * 8, self._owner)
                 self.aosoa.append((ptr, data))
+
+    def aosoa_subset(self, gids, kind):
+        """Reference AoSoA blocks (kind 0 = M, 1 = Q, 2 = H) for groups gids:
+        (blk_ptr[len(gids)+1], data) with data 64-byte aligned."""
+        sz = (4, 13, 29)[kind]
+        gids = np.ascontiguousarray(gids, np.int64)
+        ptr = np.zeros(len(gids) + 1, np.int64)
+        L = lib()
+        nblk = L.nln_aosoa_subset(self._h, gids.ctypes.data, len(gids), kind, ptr.ctypes.data, None)
+        if nblk < 0:
+            raise ValueError("no lists of that kind")
+        buf = np.zeros(nblk * sz * 8 + 16, np.float32)
+        off = (-buf.ctypes.data % 64) // 4
+        data = buf[off:off + nblk * sz * 8]
+        L.nln_aosoa_subset(self._h, gids.ctypes.data, len(gids), kind, ptr.ctypes.data,
+                           data.ctypes.data)
+        return ptr, data
 
     @property
     def interactions(self):
@@ -130,12 +167,6 @@ class Tree:
         return self.counts
 
     def close(self):
-        if getattr(self, "_h", None):
-            lib().nln_tree_free(self._h)
-            self._h = None
-
-    def __del__(self):
-        try:
-            self.close()
-        except Exception:
-            pass
+        """Drop this object's reference; the library memory is freed once no
+        array viewing it remains."""
+        self._owner = None

@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark of the 2HOT tree-gravity force evaluation on B200.
+
+One step = one force evaluation (every sink group of the step through the
+batched kernels) of a seeded synthetic particle set.  The default workload
+is the periodic 256^3 box: N = 2^24 particles on a grid displaced by a
+Gaussian random field with P(k) ~ k^-2.5 (rms 0.5 grid spacing), Plummer
+softening 1/50 of the spacing, order-4 moments plus the Ewald correction,
+force error measured against an FP64 Ewald-summed direct sum on 8192 sinks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload box256|box128|plummer64k]
+
+Under torchrun (N > 1) every rank evaluates its own replica of the workload
+(the force evaluation does not shard across GPUs here): value is the sum of
+interactions over ranks divided by the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+for _p in (REPO, os.path.join(REPO, "ahotsph-2hot-apps_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "tree-gravity interactions/s (one force evaluation per step)"
+UNIT = "interactions/s"
+# algorithmic flops per interaction: 23 for body-body and monopole cells
+# (reference count 26-27, nln/grav.c:56-75), 66 quadrupole
+# (nln/do_grav_avx8.c:378), 217 order 4 (nln/do_grav_avx8.c:45)
+FLOPS = np.array([23, 23, 66, 217], np.float64)
+
+WORKLOADS = {
+    # N = 2^24 periodic box, order 4 + Ewald (the metric's N)
+    "box256": dict(kind="box", n1d=256, rms_disp=0.5, p2cut=7, p4cut=20, ewald=True,
+                   tol=2e-4, sample=8192),
+    # 128^3 periodic box, order 4 + Ewald
+    "box128": dict(kind="box", n1d=128, rms_disp=0.25, p2cut=7, p4cut=20, ewald=True,
+                   tol=2e-4, sample=4096),
+    # Plummer sphere N = 65536, order 2
+    "plummer64k": dict(kind="plummer", n=65536, eps=0.01, p2cut=7, p4cut=0, ewald=False,
+                       tol=2e-5, sample=8192),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_problem(w, seed=123):
+    from pgrav import ics
+    if w["kind"] == "box":
+        pos, m = ics.grf_box(w["n1d"], seed=seed, slope=-2.5, rms_disp=w["rms_disp"])
+        eps = 1.0 / w["n1d"] / 50.0
+        return pos, m, eps * eps, 1.0
+    pos, m = ics.plummer(w["n"], seed=seed)
+    return pos, m, w["eps"] ** 2, 0.0
+
+
+def build_tree(w, pos, m, box, tol, nthreads=0):
+    from pgrav import host
+    return host.Tree(pos, m, leaf_max=16, group_max=32, p2cut=w["p2cut"], p4cut=w["p4cut"],
+                     tol=tol, box=box, nthreads=nthreads)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5], f[6], f[7], f[8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [r[0] for r in rows]
+        reasons = set()
+        for r in rows:
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                                "sw_power_cap"), r[2:]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": rows[0][1],
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def measured_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        return json.load(open(path)), "measured"
+    return {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def cpu_reference_rate(tree, eps2, seconds=15.0, nthreads=None, seed=0, max_groups=4096):
+    """The reference's own AVX kernels (nln/do_grav_avx8.c compiled from the
+    reference source into oracle/_ref) over the same lists, for a random
+    sample of groups, all host threads: (interactions/s, seconds, threads, sample)."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    nthreads = nthreads or os.cpu_count()
+    rng = np.random.default_rng(seed)
+    gids = np.sort(rng.choice(tree.ngroups, min(max_groups, tree.ngroups), replace=False))
+    sf = np.ascontiguousarray(tree.groups["first"][gids]).astype(np.int64)
+    sc = np.ascontiguousarray(tree.groups["count"][gids]).astype(np.int32)
+    pos = np.ascontiguousarray(tree.sorted_pos.ravel(), np.float32)
+    out = np.zeros((tree.n, 4), np.float32)
+    lists = []
+    inter = 0
+    for kind, refkind in ((0, O.MONO_PLUMMER), (1, O.QUAD_PLUMMER), (2, O.HEXA_PLUMMER)):
+        ptr = tree.ptr[kind]
+        if ptr[-1] == 0:
+            continue
+        bp, data = tree.aosoa_subset(gids, kind)
+        lists.append((refkind, O.KIND_SZ[refkind], data, np.ascontiguousarray(bp[:-1]),
+                      np.ascontiguousarray(np.diff(bp))))
+        inter += int(((ptr[gids + 1] - ptr[gids]) * tree.groups["count"][gids]).sum())
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        for refkind, sz, data, bf, bc in lists:
+            O.ref().ref_groups_eval(refkind, data, sz, bf, bc, sf, sc, len(gids), pos, eps2,
+                                    out.ravel(), nthreads)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el > seconds or reps >= 1000:
+            break
+    return (inter * reps / el, el, nthreads,
+            f"{len(gids)} random sink groups ({int(sc.sum())} sinks, {inter} interactions) "
+            f"x {reps} passes; Newtonian list terms only (the reference applies its periodic "
+            f"correction separately)")
+
+
+def run_reference(args, w, rank, world):
+    """--impl reference: the reference's CPU kernels on the host cores."""
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libnlnref.so (the reference AVX kernels) is not built"}))
+        return 0
+    pos, m, eps2, box = make_problem(w)
+    tree = build_tree(w, pos, m, box, args.tol or w["tol"])
+    rates = []
+    for _ in range(args.warmup):
+        cpu_reference_rate(tree, eps2, seconds=1.0)
+    per_step = max(2.0, 60.0 / max(1, args.steps))
+    info = None
+    for _ in range(args.steps):
+        info = cpu_reference_rate(tree, eps2, seconds=per_step)
+        rates.append(info[0])
+    value = float(np.mean(rates))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": float(tree.counts.sum() / value * 1e3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)", "config": config_of(args, w, tree, box),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": info[2],
+                             "kind": "reference", "sample": info[3]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def tree_input_bytes(tree):
+    """Bytes one evaluation reads: point and cell tables plus the index lists."""
+    return (tree.points.nbytes + tree.qcells.nbytes + tree.hcells.nbytes + tree.plist.nbytes +
+            tree.qlist.nbytes + tree.hlist.nbytes)
+
+
+def config_of(args, w, tree, box):
+    c = {"workload": args.workload, "n_bodies": int(tree.n), "groups": int(tree.ngroups),
+         "mac_tol": args.tol or w["tol"], "order": 4 if w["p4cut"] else 2,
+         "periodic": bool(box > 0), "ewald": bool(w["ewald"]),
+         "interactions_per_sink": [round(float(x) / tree.n, 1) for x in tree.counts],
+         "l2": "inputs larger than L2 (no flush)" if tree_input_bytes(tree) >= 126e6 else
+               "L2 flushed between steps (256 MB overwrite outside the step events)"}
+    return c
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="box256", choices=list(WORKLOADS))
+    ap.add_argument("--tol", type=float, default=0.0)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, w, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900),
+                                device_id=torch.device("cuda", local))
+    from pgrav import gravcuda as gc
+
+    # ---- setup (untimed): ICs, host tree + walk, device plan
+    t0 = time.perf_counter()
+    pos, m, eps2, box = make_problem(w)
+    t1 = time.perf_counter()
+    tree = build_tree(w, pos, m, box, args.tol or w["tol"])
+    t2 = time.perf_counter()
+    plan = gc.Plan(tree, eps2, ewald=w["ewald"] and box > 0)
+    plan.set_timing(True)
+    t3 = time.perf_counter()
+    log(f"[bench] ics {t1 - t0:.1f}s tree+walk {t2 - t1:.1f}s upload {t3 - t2:.1f}s "
+        f"groups {tree.ngroups} counts/sink {np.round(tree.counts / tree.n, 1)}")
+    stream = torch.cuda.Stream()
+    for _ in range(max(3, args.warmup)):
+        plan.eval(stream.cuda_stream)
+    torch.cuda.synchronize()
+
+    # ---- timed region: one event pair per step; when the step's inputs fit
+    # in L2 (126 MB), a 256 MB buffer is overwritten between steps, outside
+    # the events, so every step starts cold
+    flush = tree_input_bytes(tree) < 126e6
+    scratch = torch.empty(64 << 20, dtype=torch.float32, device="cuda") if flush else None
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            for a, b in evs:
+                if flush:
+                    scratch.zero_()
+                a.record(stream)
+                plan.eval(stream.cuda_stream)
+                b.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+    kms = plan.kernel_ms()
+    clocks = clk.summary()
+    ms_t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    counts = plan.counts().astype(np.float64)
+    inter = float(counts.sum())
+    value = inter * world / (ms_max * 1e-3)
+
+    # ---- roofline of the dominant kernel (FP32 CUDA-core pipe)
+    peaks, peak_src = measured_peaks()
+    sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s
+    kflops = {"hexa": counts[3] * FLOPS[3], "quad": counts[2] * FLOPS[2],
+              "point": (counts[0] + counts[1]) * FLOPS[0]}
+    dom = max(("hexa", "quad", "point"), key=lambda k: kms[k])
+    achieved = kflops[dom] / (kms[dom] * 1e-3) / 1e12
+    total_tflops = float((counts * FLOPS).sum() / (ms * 1e-3) / 1e12)
+    roofline = {"bound": "fp32", "kernel": f"k_batch<{dom}>", "achieved": achieved,
+                "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                "traffic": None,
+                "peak_source": (f"148 SMs x 128 FP32 lanes x 2 x {sm_mhz:.0f} MHz "
+                                f"(sm_max_mhz of {peak_src} MEASURED_PEAKS.json; it holds no "
+                                f"FP32 CUDA-core figure)"),
+                "kernel_ms": {k: round(v, 4) for k, v in kms.items()},
+                "step_tflops": total_tflops, "step_frac": total_tflops / fp32_peak}
+
+    # ---- accuracy against the FP64 direct sum (untimed)
+    acc = None
+    if not args.no_accuracy and rank == 0:
+        out = plan.download()
+        rng = np.random.default_rng(7)
+        samp = np.sort(rng.choice(tree.n, min(w["sample"], tree.n), replace=False))
+        ref = gc.direct_fp64(tree.points[:tree.n], samp, eps2, box=box)
+        e = np.linalg.norm(out[samp, :3] - ref[:, :3], axis=1) / np.linalg.norm(ref[:, :3], axis=1)
+        pe = np.abs(out[samp, 3] - ref[:, 3]) / np.abs(ref[:, 3])
+        acc = {"rms_rel_force_err": float(np.sqrt(np.mean(e * e))),
+               "max_rel_force_err": float(e.max()),
+               "rms_rel_phi_err": float(np.sqrt(np.mean(pe * pe))),
+               "sinks": int(len(samp)),
+               "oracle": "FP64 direct sum" + (" with Ewald images" if box > 0 else "")}
+
+    # ---- end to end through the C ABI with host buffers (pinned)
+    e2e = None
+    if args.e2e_steps > 0:
+        host = gc.pinned_problem(tree)
+        out = host.out
+        torch.cuda.synchronize()
+        walls = []
+        for _ in range(args.e2e_steps):
+            ta = time.perf_counter()
+            gc.groups_eval_problem(host, eps2, box, ewald=w["ewald"] and box > 0)
+            torch.cuda.synchronize()
+            walls.append(time.perf_counter() - ta)
+        e2e_s = float(np.median(walls))
+        e2e = {"value": inter * world / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(host.h2d_bytes), "d2h_bytes_per_step": int(out.nbytes),
+               "ms_per_step": e2e_s * 1e3, "steps": args.e2e_steps,
+               "timing": "wall clock around grav_groups_CUDA (upload, evaluate, download)"}
+
+    cpu = None
+    if rank == 0 and args.cpu_seconds > 0:
+        info = cpu_reference_rate(tree, eps2, seconds=args.cpu_seconds)
+        if info:
+            cpu = {"value": info[0], "unit": UNIT, "cores": info[2], "kind": "reference",
+                   "sample": info[3]}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_max,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 (FP64 centres, compensated sums)", "data": "synthetic (seeded)",
+                "config": config_of(args, w, tree, box), "gpu_launches": plan.launches() * args.steps,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+                "accuracy": acc,
+                "host_setup_s": {"ics": t1 - t0, "tree_walk": t2 - t1, "upload": t3 - t2}}
+        print(json.dumps(line))
+    plan.free()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -159,8 +159,7 @@ typedef struct grav_problem {
     const nln_hcell *hcells;    /* ncells records, or NULL when no order-4 lists */
     const nln_group *groups;    /* ngroups records */
     const int64_t *pptr, *qptr, *hptr;  /* ngroups + 1 each */
-    const nln_pseg *plist;
-    const uint32_t *qlist, *hlist;
+    const uint32_t *plist, *qlist, *hlist;  /* entries: index | image << 27 (nlnlists.h) */
     double eps2;                /* Plummer softening eps^2 (all interactions) */
     double box;                 /* periodic cube side; 0 = isolated */
     float quad_phi_sign;        /* +1 physical; -1 reproduces do_gravpq's potential */
@@ -175,7 +174,8 @@ typedef struct grav_tuning {
     int chunk_p;                /* max point records per work item (split long lists) */
     int chunk_q;                /* max quadrupole cells per work item */
     int chunk_h;                /* max order-4 cells per work item */
-    int blocks_per_sm;          /* persistent grid = blocks_per_sm x SM count */
+    int blocks_per_sm;          /* persistent grid = blocks_per_sm x SM count (0: as many as fit) */
+    int ewald_n;                /* Ewald table nodes per axis (0: 64) */
 } grav_tuning;
 
 /*
@@ -195,6 +195,10 @@ float *grav_plan_output(grav_plan *plan);
 void grav_plan_counts(const grav_plan *plan, int64_t out[4]);
 /* Kernel launches per evaluation. */
 int grav_plan_launches(const grav_plan *plan);
+/* Record CUDA events around each kernel of every evaluation (on its stream). */
+int grav_plan_set_timing(grav_plan *plan, int on);
+/* Milliseconds of the last evaluation's kernels: order-4, quadrupole, point, finish (synchronising). */
+int grav_plan_kernel_ms(grav_plan *plan, float ms[4]);
 void grav_plan_free(grav_plan *plan);
 
 /*
@@ -202,6 +206,18 @@ void grav_plan_free(grav_plan *plan);
  * host, nbodies x 4 floats, tree order.
  */
 int grav_groups_CUDA(const grav_problem *host_problem, float *acc_phi);
+
+/*
+ * FP64 direct sum at nsink sample sinks, the accuracy reference of every
+ * reported force error.  Isolated (box = 0): Plummer-softened sum over all
+ * bodies, self included.  Periodic (box > 0): the Ewald-summed direct sum of
+ * EwaldForces (nln/grav_n2.c:97-196, pair term ewald() of nln/ewald.c:13-64)
+ * with the nearest-image Newtonian term softened by eps2.  points: host
+ * (x, y, z, m) float4 per body; sinks: host indices; out: host, 4 doubles
+ * (ax, ay, az, phi) per sample; G not applied.
+ */
+int grav_direct_fp64_CUDA(const float *points, int64_t n, const int64_t *sinks, int64_t nsink,
+                          double eps2, double box, double *out);
 
 #ifdef __cplusplus
 }

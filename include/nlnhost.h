@@ -71,7 +71,7 @@ const nln_qcell *nln_qcells(const nln_tree *t);
 const nln_hcell *nln_hcells(const nln_tree *t);
 const nln_group *nln_groups(const nln_tree *t);
 
-/* CSR lists per group: entries [ptr[g], ptr[g+1]). kind 0 = P segments, 1 = Q, 2 = H. */
+/* CSR lists per group: uint32 entries [ptr[g], ptr[g+1]); kind 0 = points, 1 = Q, 2 = H. */
 const int64_t *nln_list_ptr(const nln_tree *t, int kind);
 const void *nln_list_data(const nln_tree *t, int kind);
 int64_t nln_list_len(const nln_tree *t, int kind);
@@ -92,8 +92,27 @@ void nln_counts(const nln_tree *t, int64_t out[4]);
 const int64_t *nln_aosoa_ptr(const nln_tree *t, int kind);
 const float *nln_aosoa_data(const nln_tree *t, int kind);
 
+/*
+ * The same AoSoA blocks for a subset of groups gids[0..ngsel), packed from
+ * the index lists (so emit_aosoa is not needed).  With data == NULL only
+ * blk_ptr (ngsel + 1 entries) is filled; returns the total block count.
+ */
+int64_t nln_aosoa_subset(const nln_tree *t, const int64_t *gids, int64_t ngsel, int kind,
+                         int64_t *blk_ptr, float *data);
+
 /* Body positions in tree order (xyz floats), the sink positions the lists were built for. */
 const float *nln_sorted_pos(const nln_tree *t);
+
+/*
+ * The periodic correction C(y) = Phi_Ewald(y) + 1/|y| and its first three
+ * derivatives (NLN_EWALD_NQ doubles, layout of nlnlists.h) at one
+ * displacement y = source - sink in a cube of side L, from the Ewald sum of
+ * nln/ewald.c:13-64 (same alpha = 2/L and k-space cut), differentiated
+ * analytically.  Its gradient plus y/|y|^3 is ewald()'s force.
+ */
+void nln_ewald_eval(double L, const double *y, double *out);
+/* The same on an n^3 grid over [0, reach*L]^3 (node (i,j,k) at (i,j,k)*reach*L/(n-1)). */
+int nln_ewald_table(double L, int n, double reach, double *out);
 
 #ifdef __cplusplus
 }

@@ -17,7 +17,8 @@ typedef struct nln_qcell {      /* 64 bytes */
     double cen[3];              /* FP64 expansion centre (centre of mass) */
     float mass, R;              /* R = bmax normalises the moments */
     float qxx, qxy, qyy, qxz, qyz;
-    float pad[3];
+    float B2;                   /* sum m |x - cen|^2 (the trace the quadrupole drops) */
+    float pad[2];
 } nln_qcell;
 
 typedef struct nln_hcell {      /* 128 bytes */
@@ -26,24 +27,34 @@ typedef struct nln_hcell {      /* 128 bytes */
     float q2[5];                /* qxx qxy qyy qxz qyz              / R^2 */
     float q3[7];                /* qxxx qxxy qxyy qyyy qxxz qxyz qyyz / R^3 */
     float q4[9];                /* qxxxx qxxxy qxxyy qxyyy qyyyy qxxxz qxxyz qxyyz qyyyz / R^4 */
-    float pad[3];
+    float B2;                   /* sum m |x - cen|^2 */
+    float pad[2];
 } nln_hcell;
 
-/* One run of point-table records with one periodic image shift. */
-typedef struct nln_pseg {
-    uint32_t base;              /* first record in the point table */
-    uint16_t len;               /* records in the run */
-    uint16_t shift;             /* image code (sx+1)*9+(sy+1)*3+(sz+1); 13 = none */
-} nln_pseg;
 
 /*
  * Periodic boxes: a source is used whole in the image nearest the sink
  * group's centre, and every sink-source displacement stays inside
  * |y_k| <= NLN_EWALD_REACH * box, the domain of the Ewald correction table.
  */
-#define NLN_EWALD_REACH 0.75
+#define NLN_EWALD_REACH 0.625
 
-/* Index-list entries for quad/order-4 cells: cell index | shift << 27. */
+/*
+ * Ewald correction table: per node, NLN_EWALD_NQ values of
+ * C(y) = Phi_Ewald(y) + 1/|y| and its derivatives, in the order
+ *   C | dC/dx dC/dy dC/dz | xx xy xz yy yz zz | xxx xxy xxz xyy xyz xzz yyy yyz yzz zzz
+ * on an n^3 grid over the positive octant [0, NLN_EWALD_REACH * L]^3
+ * (the cubic lattice makes C even in each coordinate).
+ */
+#define NLN_EWALD_NQ 20
+
+/*
+ * List entries (points, quadrupole and order-4 cells alike): the record
+ * index in its table | image code << 27, where the image code is
+ * (sx+1)*9 + (sy+1)*3 + (sz+1) for the periodic shift (sx, sy, sz) in box
+ * units; 13 = no shift.  Point-table records below the body count are
+ * bodies, the rest cell monopoles.
+ */
 #define NLN_SHIFT_NONE 13u
 #define NLN_IDX_BITS 27
 #define NLN_IDX_MASK ((1u << NLN_IDX_BITS) - 1u)

@@ -1,0 +1,132 @@
+"""The Ewald restatement (oracle/grav_oracle.c orc_ewald, after nln/ewald.c)
+and the FP64 correction table (csrc/host/ewald_table.cpp), on the CPU."""
+import ctypes
+import itertools
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+# The potential at a lattice site of a simple cubic lattice of unit masses
+# in a neutralising background, self term removed: lim_{r->0} (phi + 1/r)
+# = 2.8372974794806 / L  (the Ewald constant of the simple cubic lattice,
+# e.g. Nijboer & De Wette, Physica 23 (1957) 309).
+SC_CONSTANT = 2.837297479480620
+
+
+@pytest.fixture(scope="module")
+def host():
+    from pgrav import host as H
+    L = H.lib()
+    L.nln_ewald_eval.argtypes = [ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
+    L.nln_ewald_table.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_void_p]
+    L.nln_ewald_table.restype = ctypes.c_int
+    return L
+
+
+def ev(host, y, L=1.0):
+    o = np.zeros(20)
+    y = np.ascontiguousarray(y, np.float64)
+    host.nln_ewald_eval(L, y.ctypes.data, o.ctypes.data)
+    return o
+
+
+def test_restatement_periodic_and_odd():
+    rng = np.random.default_rng(0)
+    x = rng.uniform(-0.5, 0.5, (20, 3))
+    f, p = O.ewald(x, 1.0)
+    for k in range(3):
+        xs = x.copy()
+        xs[:, k] += 1.0
+        f2, p2 = O.ewald(xs, 1.0)
+        assert np.abs(f2 - f).max() < 1e-9 and np.abs(p2 - p).max() < 1e-9
+    fm, pm = O.ewald(-x, 1.0)
+    assert np.abs(fm + f).max() < 1e-12 and np.abs(pm - p).max() < 1e-12
+
+
+def test_restatement_x0_rule():
+    f, p = O.ewald(np.zeros(3), 1.0)
+    assert np.all(f == 0) and p[0] == pytest.approx(np.pi / 4)  # pi/(alpha^2 L^3), alpha = 2/L
+
+
+def test_restatement_lattice_constant():
+    # phi(x) + 1/|x| -> SC constant as x -> 0 (the quadratic term is -(2 pi/3) x^2)
+    x = np.array([[1e-3, 0.0, 0.0]])
+    f, p = O.ewald(x, 1.0)
+    assert p[0] + 1e3 + 2 * np.pi / 3 * 1e-6 == pytest.approx(SC_CONSTANT, abs=1e-8)
+
+
+def test_force_is_gradient_of_potential():
+    y = np.array([[0.17, -0.22, 0.31]])
+    h = 1e-6
+    f, _ = O.ewald(y, 1.0)
+    for k in range(3):
+        e = np.zeros((1, 3))
+        e[0, k] = h
+        _, pp = O.ewald(y + e, 1.0)
+        _, pm = O.ewald(y - e, 1.0)
+        assert (pp[0] - pm[0]) / (2 * h) == pytest.approx(f[0, k], rel=1e-7)
+
+
+def test_table_matches_restatement(host):
+    rng = np.random.default_rng(1)
+    for L in (1.0, 3.0):
+        for y in rng.uniform(-0.6 * L, 0.6 * L, (40, 3)):
+            o = ev(host, y, L)
+            f, p = O.ewald(y, L)
+            r = np.linalg.norm(y)
+            assert o[0] == pytest.approx(p[0] + 1.0 / r, rel=1e-9, abs=1e-10 / L)
+            assert np.abs(o[1:4] - (f[0] - y / r ** 3)).max() < 1e-10 / L ** 2
+
+
+def test_table_constant_and_laplacian(host):
+    o = ev(host, np.zeros(3))
+    assert o[0] == pytest.approx(SC_CONSTANT, abs=1e-12)
+    assert np.abs(o[1:4]).max() < 1e-14
+    y = np.array([0.3, 0.1, -0.2])
+    o = ev(host, y, 2.0)
+    assert o[4] + o[7] + o[9] == pytest.approx(-4 * np.pi / 8.0, rel=1e-10)  # -4 pi / L^3
+
+
+def test_table_derivatives_by_differences(host):
+    y = np.array([0.21, -0.13, 0.33])
+    h = 1e-5
+    o = ev(host, y)
+    H = np.array([[o[4], o[5], o[6]], [o[5], o[7], o[8]], [o[6], o[8], o[9]]])
+    T = np.zeros((3, 3, 3))
+    idx = [(0, 0, 0), (0, 0, 1), (0, 0, 2), (0, 1, 1), (0, 1, 2), (0, 2, 2), (1, 1, 1),
+           (1, 1, 2), (1, 2, 2), (2, 2, 2)]
+    for v, ijk in zip(o[10:20], idx):
+        for p in set(itertools.permutations(ijk)):
+            T[p] = v
+    for k in range(3):
+        e = np.zeros(3)
+        e[k] = h
+        op, om = ev(host, y + e), ev(host, y - e)
+        assert np.abs((op[1:4] - om[1:4]) / (2 * h) - H[:, k]).max() < 1e-7
+        Hp = np.array([[op[4], op[5], op[6]], [op[5], op[7], op[8]], [op[6], op[8], op[9]]])
+        Hm = np.array([[om[4], om[5], om[6]], [om[5], om[7], om[8]], [om[6], om[8], om[9]]])
+        assert np.abs((Hp - Hm) / (2 * h) - T[:, :, k]).max() < 1e-5
+
+
+def test_table_grid(host):
+    n, L, reach = 5, 2.0, 0.625
+    tab = np.zeros(n ** 3 * 20)
+    assert host.nln_ewald_table(L, n, reach, tab.ctypes.data) == 0
+    tab = tab.reshape(n, n, n, 20)
+    h = reach * L / (n - 1)
+    assert np.allclose(tab[1, 2, 3], ev(host, np.array([1, 2, 3]) * h, L), rtol=1e-13, atol=1e-13)
+
+
+def test_direct_ewald_oracle_softening_limit():
+    """With eps2 -> 0 the softened periodic oracle tends to the plain EwaldForces sum."""
+    rng = np.random.default_rng(2)
+    pos = rng.uniform(0, 1, (40, 3))
+    m = rng.uniform(0.5, 1.5, 40) / 40
+    a0, p0 = O.direct_ewald(pos, m, 1.0, 0.0, np.arange(5))
+    a1, _ = O.direct_ewald(pos, m, 1.0, 1e-14, np.arange(5))
+    assert np.abs(a1 - a0).max() < 1e-6 * np.abs(a0).max()
+    # momentum: sum_i m_i a_i over all sinks vanishes
+    a, _ = O.direct_ewald(pos, m, 1.0, 0.0, np.arange(40))
+    assert np.abs((m[:, None] * a).sum(0)).max() < 1e-10
