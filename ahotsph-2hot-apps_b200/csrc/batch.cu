@@ -61,6 +61,7 @@ struct DevProblem {
     const int64_t *gslot;      // ngroups + 1: slots of group g
     float4 *out;               // nbodies
     int64_t ngroups;
+    int64_t ncells;
     float eps2;
     float qsh;
     double box;
@@ -262,23 +263,64 @@ __global__ void __launch_bounds__(256) k_batch(const __grid_constant__ CUtensorM
     }
 }
 
-// Periodic correction moments of group g: every list entry at its centre
-// (bodies and monopole cells as points, quadrupole and order-4 cells with
-// their traceless second moment folded in), lanes striding the lists.
-__device__ void ewald_moments(const DevProblem &P, int64_t g, const double *c, int lane,
-                              float *M) {
+// One list entry's part of the correction moments, accumulated in FP64
+// (the terms are O(1) per unit mass and cancel to a small net field, so an
+// FP32 sum over thousands of entries would lose the answer).  o = C and its
+// derivatives at the entry centre, m its mass; a cell adds its second moment
+// sum m xi xi = Q + B2/3 I (Q = R^2 q2, traceless):
+//   C += 1/2 Q:ddC + B2/6 tr ddC,   dC += 1/2 dddC[Q]   (tr ddC is constant).
+__device__ __forceinline__ void ew_accumulate(double *M, const float *o, float m, bool cell,
+                                              float R, const float *q2, float B2, float trace) {
+    float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
+    if (cell) {
+        const float R2 = R * R;
+        const float Q[6] = {R2 * q2[0], R2 * q2[1], R2 * q2[3], R2 * q2[2], R2 * q2[4],
+                            -R2 * (q2[0] + q2[2])};
+        const float *H = o + 4;
+        c0 = 0.5f * (Q[0] * H[0] + 2.f * Q[1] * H[1] + 2.f * Q[2] * H[2] + Q[3] * H[3] +
+                     2.f * Q[4] * H[4] + Q[5] * H[5]) +
+             (B2 / 6.f) * trace;
+        float v[3];
+        t_q(o + 10, Q, v);
+        c1 = 0.5f * v[0];
+        c2 = 0.5f * v[1];
+        c3 = 0.5f * v[2];
+    }
+    M[0] += (double)fmaf(m, o[0], c0);
+    M[1] += (double)fmaf(m, o[1], c1);
+    M[2] += (double)fmaf(m, o[2], c2);
+    M[3] += (double)fmaf(m, o[3], c3);
 #pragma unroll
-    for (int q = 0; q < 20; q++) M[q] = 0.f;
+    for (int q = 4; q < 20; q++) M[q] += (double)(m * o[q]);
+}
+
+// Periodic correction moments of group g: every list entry at its centre
+// (bodies as points; monopole, quadrupole and order-4 cells with their
+// second moment folded in), lanes striding the lists, FP64 sums.
+__device__ void ewald_moments(const DevProblem &P, int64_t g, const double *c, int lane,
+                              double *M) {
+#pragma unroll
+    for (int q = 0; q < 20; q++) M[q] = 0.0;
     float o[20];
+    const uint32_t nb = (uint32_t)P.ntab[0] - (uint32_t)P.ncells;
+    const float zero5[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
     for (int64_t k = P.lptr[0][g] + lane; k < P.lptr[0][g + 1]; k += 32) {
         const uint32_t ent = P.list[0][k];
+        const uint32_t idx = ent & NLN_IDX_MASK;
         double sx, sy, sz;
         decode_shift(ent >> NLN_IDX_BITS, P.box, sx, sy, sz);
-        const float4 p = P.points[ent & NLN_IDX_MASK];
+        const float4 p = P.points[idx];
         ew_lookup(P.ew, (float)((double)p.x + sx - c[0]), (float)((double)p.y + sy - c[1]),
                   (float)((double)p.z + sz - c[2]), o);
-#pragma unroll
-        for (int q = 0; q < 20; q++) M[q] = fmaf(p.w, o[q], M[q]);
+        if (idx >= nb) {
+            // a cell taken as a monopole by the Newtonian sum: the correction
+            // still needs its second moment (it varies on the scale of the box)
+            const nln_qcell &q = P.qcells[idx - nb];
+            const float q2[5] = {q.qxx, q.qxy, q.qyy, q.qxz, q.qyz};
+            ew_accumulate(M, o, p.w, true, q.R, q2, q.B2, P.ew_trace);
+        } else {
+            ew_accumulate(M, o, p.w, false, 0.f, zero5, 0.f, P.ew_trace);
+        }
     }
     for (int kind = 1; kind < 3; kind++) {
         if (!P.list[kind])
@@ -304,27 +346,12 @@ __device__ void ewald_moments(const DevProblem &P, int64_t g, const double *c, i
             }
             ew_lookup(P.ew, (float)(cx + sx - c[0]), (float)(cy + sy - c[1]),
                       (float)(cz + sz - c[2]), o);
-#pragma unroll
-            for (int q = 0; q < 20; q++) M[q] = fmaf(m, o[q], M[q]);
-            // second moment sum m xi xi = Q + B2/3 I, Q = R^2 q2 traceless:
-            // phi += 1/2 Q:ddC + B2/6 tr ddC ;  grad += 1/2 dddC[Q]
-            const float R2 = R * R;
-            const float Q[6] = {R2 * q2[0], R2 * q2[1], R2 * q2[3], R2 * q2[2], R2 * q2[4],
-                                -R2 * (q2[0] + q2[2])};
-            const float *H = o + 4;
-            M[0] += 0.5f * (Q[0] * H[0] + 2.f * Q[1] * H[1] + 2.f * Q[2] * H[2] + Q[3] * H[3] +
-                            2.f * Q[4] * H[4] + Q[5] * H[5]) +
-                    (B2 / 6.f) * P.ew_trace;
-            float v[3];
-            t_q(o + 10, Q, v);
-            M[1] += 0.5f * v[0];
-            M[2] += 0.5f * v[1];
-            M[3] += 0.5f * v[2];
+            ew_accumulate(M, o, m, true, R, q2, B2, P.ew_trace);
         }
     }
 #pragma unroll
     for (int q = 0; q < 20; q++) {
-        float x = M[q];
+        double x = M[q];
         for (int d = 16; d > 0; d >>= 1) x += __shfl_xor_sync(0xffffffffu, x, d);
         M[q] = x;
     }
@@ -349,17 +376,17 @@ __global__ void k_finish(DevProblem P) {
     }
     if (P.ewald) {
         const double c[3] = {G.cen[0], G.cen[1], G.cen[2]};
-        float M[20];
+        double M[20];
         ewald_moments(P, g, c, lane, M);
         if (lane < G.count) {
             const float4 p = P.points[G.first + lane];
-            float phi, ax, ay, az;
-            ew_apply(M, (float)((double)p.x - c[0]), (float)((double)p.y - c[1]),
-                     (float)((double)p.z - c[2]), phi, ax, ay, az);
+            double phi, ax, ay, az;
+            ew_apply(M, (double)p.x - c[0], (double)p.y - c[1], (double)p.z - c[2], phi, ax, ay,
+                     az);
             s[0] += ax;
             s[1] += ay;
             s[2] += az;
-            s[3] += phi - p.w * P.ew_self;
+            s[3] += phi - (double)p.w * P.ew_self;
         }
     }
     if (lane < G.count)
@@ -557,7 +584,12 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
     d.points = pts;
     nln_qcell *qc = nullptr;
     nln_hcell *hc = nullptr;
-    if (hp->qptr && hp->qptr[ng])
+    const bool want_ewald = hp->box > 0 && hp->ewald;
+    if (want_ewald && !hp->qcells && hp->ncells > 0) {
+        grav_plan_free(pl);
+        return gc::set_status(-1, "the Ewald correction needs the quadrupole cell table");
+    }
+    if ((hp->qptr && hp->qptr[ng]) || (want_ewald && hp->ncells > 0))
         rc |= dev_copy(pl, hp->qcells, (size_t)hp->ncells, &qc);
     if (hp->hptr && hp->hptr[ng])
         rc |= dev_copy(pl, hp->hcells, (size_t)hp->ncells, &hc);
@@ -654,6 +686,7 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
         return rc;
     }
     d.ngroups = ng;
+    d.ncells = hp->ncells;
     d.eps2 = (float)hp->eps2;
     d.qsh = 0.5f * (hp->quad_phi_sign == 0.0f ? 1.0f : hp->quad_phi_sign);
     d.box = hp->box;

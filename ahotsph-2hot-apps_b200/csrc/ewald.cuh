@@ -108,17 +108,21 @@ __device__ __forceinline__ void ew_lookup(const EwTab &E, float yx, float yy, fl
     o[19] = sz * T0[9];
 }
 
-// Evaluate a group's correction moments M (20) at sink offset u: (phi, a).
-__device__ __forceinline__ void ew_apply(const float *M, float ux, float uy, float uz,
-                                         float &phi, float &axx, float &ayy, float &azz) {
-    const float *M1 = M + 1, *M2 = M + 4, *M3 = M + 10;
-    float Mu[3], Tuu[3];
-    h_d(M2, ux, uy, uz, Mu);
-    t_dd(M3, ux, uy, uz, Tuu);
-    phi = M[0] - (M1[0] * ux + M1[1] * uy + M1[2] * uz) +
-          0.5f * (Mu[0] * ux + Mu[1] * uy + Mu[2] * uz) -
-          (1.f / 6.f) * (Tuu[0] * ux + Tuu[1] * uy + Tuu[2] * uz);
-    axx = M1[0] - Mu[0] + 0.5f * Tuu[0];
-    ayy = M1[1] - Mu[1] + 0.5f * Tuu[1];
-    azz = M1[2] - Mu[2] + 0.5f * Tuu[2];
+// Evaluate a group's correction moments M (20, FP64) at sink offset u: (phi, a).
+__device__ __forceinline__ void ew_apply(const double *M, double ux, double uy, double uz,
+                                         double &phi, double &axx, double &ayy, double &azz) {
+    const double *M1 = M + 1, *H = M + 4, *T = M + 10;
+    const double Mu0 = H[0] * ux + H[1] * uy + H[2] * uz;
+    const double Mu1 = H[1] * ux + H[3] * uy + H[4] * uz;
+    const double Mu2 = H[2] * ux + H[4] * uy + H[5] * uz;
+    const double xx = ux * ux, xy = 2 * ux * uy, xz = 2 * ux * uz, yy = uy * uy,
+                 yz = 2 * uy * uz, zz = uz * uz;
+    const double T0 = T[0] * xx + T[1] * xy + T[2] * xz + T[3] * yy + T[4] * yz + T[5] * zz;
+    const double T1 = T[1] * xx + T[3] * xy + T[4] * xz + T[6] * yy + T[7] * yz + T[8] * zz;
+    const double T2 = T[2] * xx + T[4] * xy + T[5] * xz + T[7] * yy + T[8] * yz + T[9] * zz;
+    phi = M[0] - (M1[0] * ux + M1[1] * uy + M1[2] * uz) + 0.5 * (Mu0 * ux + Mu1 * uy + Mu2 * uz) -
+          (T0 * ux + T1 * uy + T2 * uz) / 6.0;
+    axx = M1[0] - Mu0 + 0.5 * T0;
+    ayy = M1[1] - Mu1 + 0.5 * T1;
+    azz = M1[2] - Mu2 + 0.5 * T2;
 }

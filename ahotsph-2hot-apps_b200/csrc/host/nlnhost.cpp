@@ -567,6 +567,21 @@ static void walk_group(const nln_tree *t, const nln_group &G, GroupLists &L,
         if (box > 0) {
             double ym = std::max(std::fabs(y[0]), std::max(std::fabs(y[1]), std::fabs(y[2])));
             inside = ym + c.bmax + G.radius <= NLN_EWALD_REACH * box;
+            // The correction takes a cell at its centre with its quadrupole;
+            // keep cells small against their distance to the correction's
+            // nearest singularity (the sink's own image at a lattice vector).
+            if (inside && t->p.ewald_theta > 0) {
+                double D2 = INFINITY;
+                for (int a = -1; a <= 1; a++)
+                    for (int b = -1; b <= 1; b++)
+                        for (int e = -1; e <= 1; e++) {
+                            if (!a && !b && !e)
+                                continue;
+                            const double dx = y[0] - a * box, dy = y[1] - b * box, dz = y[2] - e * box;
+                            D2 = std::min(D2, dx * dx + dy * dy + dz * dz);
+                        }
+                inside = c.bmax + G.radius <= t->p.ewald_theta * std::sqrt(D2);
+            }
         }
         const double dd = dist - G.radius;
         const uint16_t sc = shift_code(s);
@@ -803,4 +818,12 @@ extern "C" int64_t nln_aosoa_subset(const nln_tree *t, const int64_t *gids, int6
         }
     }
     return blk_ptr[ngsel];
+}
+
+// Body range of every cell (tree order): bodies [first[c], first[c] + count[c]).
+extern "C" void nln_cell_ranges(const nln_tree *t, int64_t *first, int32_t *count) {
+    for (size_t c = 0; c < t->cells.size(); c++) {
+        first[c] = t->cells[c].first;
+        count[c] = t->cells[c].count;
+    }
 }

@@ -132,7 +132,7 @@ class Plan:
         prob = Problem()
         prob.nbodies, prob.ncells, prob.ngroups = t.n, t.ncells, t.ngroups
         prob.points = pts.ctypes.data
-        prob.qcells = keep(t.qcells).ctypes.data if has_q else None
+        prob.qcells = keep(t.qcells).ctypes.data if len(t.qcells) else None
         prob.hcells = keep(t.hcells).ctypes.data if has_h else None
         prob.groups = groups.ctypes.data
         prob.pptr = keep(t.ptr[0]).ctypes.data
@@ -308,7 +308,7 @@ class PinnedProblem:
         p.nbodies, p.ncells, p.ngroups = t.n, t.ncells, t.ngroups
         p.points = pin(t.points).ctypes.data
         has_q, has_h = len(t.qlist) > 0, len(t.hlist) > 0
-        p.qcells = pin(t.qcells).ctypes.data if has_q else None
+        p.qcells = pin(t.qcells).ctypes.data if len(t.qcells) else None
         p.hcells = pin(t.hcells).ctypes.data if has_h else None
         p.groups = pin(t.groups).ctypes.data
         p.pptr = pin(t.ptr[0]).ctypes.data

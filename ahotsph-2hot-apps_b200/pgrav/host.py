@@ -27,7 +27,8 @@ class Params(ctypes.Structure):
                 ("p2cut", ctypes.c_int), ("p4cut", ctypes.c_int),
                 ("tol", ctypes.c_double), ("rel_tol", ctypes.c_double),
                 ("rel_tol0", ctypes.c_double), ("box", ctypes.c_double),
-                ("nthreads", ctypes.c_int), ("emit_aosoa", ctypes.c_int)]
+                ("nthreads", ctypes.c_int), ("emit_aosoa", ctypes.c_int),
+                ("ewald_theta", ctypes.c_double)]
 
 
 def lib():
@@ -60,6 +61,7 @@ def lib():
         L.nln_counts.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.nln_aosoa_subset.argtypes = [vp, vp, ctypes.c_int64, ctypes.c_int, vp, vp]
         L.nln_aosoa_subset.restype = ctypes.c_int64
+        L.nln_cell_ranges.argtypes = [vp, vp, vp]
         _lib = L
     return _lib
 
@@ -99,11 +101,12 @@ class Tree:
     """
 
     def __init__(self, pos, mass, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-3,
-                 rel_tol=0.0, rel_tol0=0.0, box=0.0, nthreads=0, emit_aosoa=False, walk=True):
+                 rel_tol=0.0, rel_tol0=0.0, box=0.0, nthreads=0, emit_aosoa=False, walk=True,
+                 ewald_theta=0.0):
         pos = np.ascontiguousarray(pos, dtype=np.float32).reshape(-1, 3)
         mass = np.ascontiguousarray(np.broadcast_to(np.asarray(mass, np.float32), (len(pos),)))
         self.params = Params(leaf_max, group_max, p2cut, p4cut, tol, rel_tol, rel_tol0, box,
-                             nthreads, int(bool(emit_aosoa)))
+                             nthreads, int(bool(emit_aosoa)), ewald_theta)
         L = lib()
         h = L.nln_tree_build(pos.ctypes.data, 3, mass.ctypes.data, 1, len(pos),
                              ctypes.byref(self.params))
@@ -143,6 +146,13 @@ class Tree:
                 ptr = _view(L.nln_aosoa_ptr(self._h, k), np.int64, ng + 1, self._owner)
                 data = _view(L.nln_aosoa_data(self._h, k), np.float32, int(ptr[-1]) * sz * 8, self._owner)
                 self.aosoa.append((ptr, data))
+
+    def cell_ranges(self):
+        """(first, count) body range of every cell, tree order."""
+        first = np.zeros(self.ncells, np.int64)
+        count = np.zeros(self.ncells, np.int32)
+        lib().nln_cell_ranges(self._h, first.ctypes.data, count.ctypes.data)
+        return first, count
 
     def aosoa_subset(self, gids, kind):
         """Reference AoSoA blocks (kind 0 = M, 1 = Q, 2 = H) for groups gids:

@@ -37,6 +37,8 @@ typedef struct nln_params {
     double box;       /* periodic cube side L with bodies in [0,L)^3; 0 = isolated */
     int nthreads;     /* host threads (0: all) */
     int emit_aosoa;   /* 1: also pack the reference AoSoA lists */
+    double ewald_theta; /* periodic: accepted cells keep bmax + group radius <= ewald_theta x
+                           distance to the nearest other image of the sink (0: off) */
 } nln_params;
 
 typedef struct nln_tree nln_tree;
@@ -99,6 +101,9 @@ const float *nln_aosoa_data(const nln_tree *t, int kind);
  */
 int64_t nln_aosoa_subset(const nln_tree *t, const int64_t *gids, int64_t ngsel, int kind,
                          int64_t *blk_ptr, float *data);
+
+/* Body range of every cell: bodies [first[c], first[c] + count[c]) in tree order. */
+void nln_cell_ranges(const nln_tree *t, int64_t *first, int32_t *count);
 
 /* Body positions in tree order (xyz floats), the sink positions the lists were built for. */
 const float *nln_sorted_pos(const nln_tree *t);
