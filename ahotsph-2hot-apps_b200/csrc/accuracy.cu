@@ -7,7 +7,7 @@
 // nln/grav_n2.c:97-196 (EwaldForces) with the nearest-image Newtonian term
 // Plummer-softened like the tree's: for each pair the nearest-image term
 // plus C(y), the smooth remainder of ewald() (nln/ewald.c:13-64), taken from
-// an FP64 table over |y_k| <= L/2 by a third-order Taylor expansion about
+// an FP64 table over |y_k| <= L/2 by a fifth-order Taylor expansion about
 // the nearest node; a pair at zero separation contributes only the constant
 // pi/(alpha^2 L^3) that ewald() returns for x = 0.
 #include <cuda_runtime.h>
@@ -31,29 +31,52 @@ struct Tab64 {
     double h, inv_h;
 };
 
-// C and grad C at y from the FP64 table (positive octant, cubic symmetry)
+// C and grad C at y from the FP64 table (positive octant, cubic symmetry):
+// fifth-order Taylor expansion about the nearest node, C = sum_{|b| <= 5}
+// V[b] d^b / b!, dC/dy_i = sum_{|b| <= 4} V[e_i + b] d^b / b!  (multi-index
+// layout of nlnlists.h: order n at n(n+1)(n+2)/6, (ax, ay, az) at offset
+// (ay+az)(ay+az+1)/2 + az).
+__host__ __device__ constexpr int mi(int ax, int ay, int az) {
+    return (ax + ay + az) * (ax + ay + az + 1) * (ax + ay + az + 2) / 6 +
+           (ay + az) * (ay + az + 1) / 2 + az;
+}
+
 __device__ void ew64(const Tab64 &E, double yx, double yy, double yz, double &C, double *G) {
     const double sx = yx < 0 ? -1.0 : 1.0, sy = yy < 0 ? -1.0 : 1.0, sz = yz < 0 ? -1.0 : 1.0;
     const double ax = fabs(yx), ay = fabs(yy), az = fabs(yz);
     const int nm = E.n - 1;
     const int i = min((int)rint(ax * E.inv_h), nm), j = min((int)rint(ay * E.inv_h), nm),
               k = min((int)rint(az * E.inv_h), nm);
-    const double dx = ax - i * E.h, dy = ay - j * E.h, dz = az - k * E.h;
-    const double *t = E.t + (((size_t)i * E.n + j) * E.n + k) * 20;
-    const double *G0 = t + 1, *H = t + 4, *T = t + 10;
-    const double Hd0 = H[0] * dx + H[1] * dy + H[2] * dz;
-    const double Hd1 = H[1] * dx + H[3] * dy + H[4] * dz;
-    const double Hd2 = H[2] * dx + H[4] * dy + H[5] * dz;
-    const double xx = dx * dx, xy = 2 * dx * dy, xz = 2 * dx * dz, yyv = dy * dy,
-                 yzv = 2 * dy * dz, zz = dz * dz;
-    const double T0 = T[0] * xx + T[1] * xy + T[2] * xz + T[3] * yyv + T[4] * yzv + T[5] * zz;
-    const double T1 = T[1] * xx + T[3] * xy + T[4] * xz + T[6] * yyv + T[7] * yzv + T[8] * zz;
-    const double T2 = T[2] * xx + T[4] * xy + T[5] * xz + T[7] * yyv + T[8] * yzv + T[9] * zz;
-    C = t[0] + G0[0] * dx + G0[1] * dy + G0[2] * dz + 0.5 * (Hd0 * dx + Hd1 * dy + Hd2 * dz) +
-        (T0 * dx + T1 * dy + T2 * dz) / 6.0;
-    G[0] = sx * (G0[0] + Hd0 + 0.5 * T0);
-    G[1] = sy * (G0[1] + Hd1 + 0.5 * T1);
-    G[2] = sz * (G0[2] + Hd2 + 0.5 * T2);
+    const double d[3] = {ax - i * E.h, ay - j * E.h, az - k * E.h};
+    const double *t = E.t + (((size_t)i * E.n + j) * E.n + k) * NLN_EWALD_NQ;
+    double p[3][6];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        p[a][0] = 1.0;
+#pragma unroll
+        for (int q = 1; q < 6; q++) p[a][q] = p[a][q - 1] * d[a] / q;
+    }
+    double c = 0, g0 = 0, g1 = 0, g2 = 0;
+#pragma unroll
+    for (int b0 = 0; b0 <= 5; b0++)
+#pragma unroll
+        for (int b1 = 0; b1 <= 5; b1++)
+#pragma unroll
+            for (int b2 = 0; b2 <= 5; b2++) {
+                if (b0 + b1 + b2 > 5)
+                    continue;
+                const double w = p[0][b0] * p[1][b1] * p[2][b2];
+                c += t[mi(b0, b1, b2)] * w;
+                if (b0 + b1 + b2 <= 4) {
+                    g0 += t[mi(b0 + 1, b1, b2)] * w;
+                    g1 += t[mi(b0, b1 + 1, b2)] * w;
+                    g2 += t[mi(b0, b1, b2 + 1)] * w;
+                }
+            }
+    C = c;
+    G[0] = sx * g0;
+    G[1] = sy * g1;
+    G[2] = sz * g2;
 }
 
 __global__ void __launch_bounds__(256) k_direct64(const float4 *__restrict__ pts, int64_t n,

@@ -67,7 +67,8 @@ struct DevProblem {
     double box;
     unsigned *err;
     // periodic correction
-    const int64_t *lptr[3];    // per-group list offsets (P expanded, Q, H)
+    const int64_t *cptr;       // per-group offsets of the correction list
+    const uint32_t *clist;     // correction list: point-table record | image << 27
     int ewald;
     EwTab ew;
     float ew_self;             // C(0) - pi/(alpha^2 L^3): the self term ewald() leaves out
@@ -263,98 +264,44 @@ __global__ void __launch_bounds__(256) k_batch(const __grid_constant__ CUtensorM
     }
 }
 
-// One list entry's part of the correction moments, accumulated in FP64
-// (the terms are O(1) per unit mass and cancel to a small net field, so an
-// FP32 sum over thousands of entries would lose the answer).  o = C and its
-// derivatives at the entry centre, m its mass; a cell adds its second moment
-// sum m xi xi = Q + B2/3 I (Q = R^2 q2, traceless):
-//   C += 1/2 Q:ddC + B2/6 tr ddC,   dC += 1/2 dddC[Q]   (tr ddC is constant).
-__device__ __forceinline__ void ew_accumulate(double *M, const float *o, float m, bool cell,
-                                              float R, const float *q2, float B2, float trace) {
-    float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
-    if (cell) {
-        const float R2 = R * R;
-        const float Q[6] = {R2 * q2[0], R2 * q2[1], R2 * q2[3], R2 * q2[2], R2 * q2[4],
-                            -R2 * (q2[0] + q2[2])};
-        const float *H = o + 4;
-        c0 = 0.5f * (Q[0] * H[0] + 2.f * Q[1] * H[1] + 2.f * Q[2] * H[2] + Q[3] * H[3] +
-                     2.f * Q[4] * H[4] + Q[5] * H[5]) +
-             (B2 / 6.f) * trace;
-        float v[3];
-        t_q(o + 10, Q, v);
-        c1 = 0.5f * v[0];
-        c2 = 0.5f * v[1];
-        c3 = 0.5f * v[2];
-    }
-    M[0] += (double)fmaf(m, o[0], c0);
-    M[1] += (double)fmaf(m, o[1], c1);
-    M[2] += (double)fmaf(m, o[2], c2);
-    M[3] += (double)fmaf(m, o[3], c3);
-#pragma unroll
-    for (int q = 4; q < 20; q++) M[q] += (double)(m * o[q]);
-}
-
-// Periodic correction moments of group g: every list entry at its centre
-// (bodies as points; monopole, quadrupole and order-4 cells with their
-// second moment folded in), lanes striding the lists, FP64 sums.
-__device__ void ewald_moments(const DevProblem &P, int64_t g, const double *c, int lane,
-                              double *M) {
-#pragma unroll
-    for (int q = 0; q < 20; q++) M[q] = 0.0;
-    float o[20];
+// Periodic correction moments of group g (ewald.cuh) over its correction
+// list, lanes striding it.  Bodies count as masses; a cell adds its
+// traceless second to fourth moments (the list's cells include coarse
+// ones standing for whole subtrees, and cells a tenth of the box wide near
+// the half-box, where C varies on the scale of the cell), and its
+// second-moment trace B2/3 against the constant Laplacian of C.
+__device__ __forceinline__ void ewald_moments(const DevProblem &P, int64_t g, const double *c,
+                                              int lane, EwMoments &M) {
+    M.zero();
+    float o[ew::kNQ4], f5[21];
     const uint32_t nb = (uint32_t)P.ntab[0] - (uint32_t)P.ncells;
-    const float zero5[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-    for (int64_t k = P.lptr[0][g] + lane; k < P.lptr[0][g + 1]; k += 32) {
-        const uint32_t ent = P.list[0][k];
+    for (int64_t k = P.cptr[g] + lane; k < P.cptr[g + 1]; k += 32) {
+        const uint32_t ent = P.clist[k];
         const uint32_t idx = ent & NLN_IDX_MASK;
         double sx, sy, sz;
         decode_shift(ent >> NLN_IDX_BITS, P.box, sx, sy, sz);
-        const float4 p = P.points[idx];
-        ew_lookup(P.ew, (float)((double)p.x + sx - c[0]), (float)((double)p.y + sy - c[1]),
-                  (float)((double)p.z + sz - c[2]), o);
-        if (idx >= nb) {
-            // a cell taken as a monopole by the Newtonian sum: the correction
-            // still needs its second moment (it varies on the scale of the box)
-            const nln_qcell &q = P.qcells[idx - nb];
-            const float q2[5] = {q.qxx, q.qxy, q.qyy, q.qxz, q.qyz};
-            ew_accumulate(M, o, p.w, true, q.R, q2, q.B2, P.ew_trace);
+        if (idx < nb) {
+            const float4 p = P.points[idx];
+            ew_lookup<false>(P.ew, (float)((double)p.x + sx - c[0]),
+                             (float)((double)p.y + sy - c[1]), (float)((double)p.z + sz - c[2]),
+                             o, nullptr);
+            ew_add_mass(M, p.w, o);
         } else {
-            ew_accumulate(M, o, p.w, false, 0.f, zero5, 0.f, P.ew_trace);
+            const nln_hcell &h = P.hcells[idx - nb];
+            ew_lookup<true>(P.ew, (float)(h.cen[0] + sx - c[0]), (float)(h.cen[1] + sy - c[1]),
+                            (float)(h.cen[2] + sz - c[2]), o, f5);
+            ew_add_mass(M, h.mass, o);
+            float S[15];
+            ew_quad(h.R, h.q2, S);
+            ew_fold<2, 3>(M, S, o, f5);
+            ew_oct(h.R, h.q3, S);
+            ew_fold<3, 2>(M, S, o, f5);
+            ew_hex(h.R, h.q4, S);
+            ew_fold<4, 1>(M, S, o, f5);
+            M.add(0, h.B2 * (1.f / 6.f) * P.ew_trace);
         }
     }
-    for (int kind = 1; kind < 3; kind++) {
-        if (!P.list[kind])
-            continue;
-        for (int64_t k = P.lptr[kind][g] + lane; k < P.lptr[kind][g + 1]; k += 32) {
-            const uint32_t ent = P.list[kind][k];
-            const uint32_t ci = ent & NLN_IDX_MASK;
-            double sx, sy, sz;
-            decode_shift(ent >> NLN_IDX_BITS, P.box, sx, sy, sz);
-            double cx, cy, cz;
-            float m, R, B2, q2[5];
-            if (kind == 1) {
-                const nln_qcell &q = P.qcells[ci];
-                cx = q.cen[0]; cy = q.cen[1]; cz = q.cen[2];
-                m = q.mass; R = q.R; B2 = q.B2;
-                q2[0] = q.qxx; q2[1] = q.qxy; q2[2] = q.qyy; q2[3] = q.qxz; q2[4] = q.qyz;
-            } else {
-                const nln_hcell &h = P.hcells[ci];
-                cx = h.cen[0]; cy = h.cen[1]; cz = h.cen[2];
-                m = h.mass; R = h.R; B2 = h.B2;
-#pragma unroll
-                for (int t = 0; t < 5; t++) q2[t] = h.q2[t];
-            }
-            ew_lookup(P.ew, (float)(cx + sx - c[0]), (float)(cy + sy - c[1]),
-                      (float)(cz + sz - c[2]), o);
-            ew_accumulate(M, o, m, true, R, q2, B2, P.ew_trace);
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < 20; q++) {
-        double x = M[q];
-        for (int d = 16; d > 0; d >>= 1) x += __shfl_xor_sync(0xffffffffu, x, d);
-        M[q] = x;
-    }
+    M.warp_sum();
 }
 
 // Per group, in slot order: sum the partials of its work items in FP64,
@@ -376,7 +323,7 @@ __global__ void k_finish(DevProblem P) {
     }
     if (P.ewald) {
         const double c[3] = {G.cen[0], G.cen[1], G.cen[2]};
-        double M[20];
+        EwMoments M;
         ewald_moments(P, g, c, lane, M);
         if (lane < G.count) {
             const float4 p = P.points[G.first + lane];
@@ -524,6 +471,24 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
         delete pl;
         return gc::set_status(-1, "cell list entry outside the cell table");
     }
+    const bool want_ewald = hp->box > 0 && hp->ewald;
+    if (want_ewald) {
+        if (!hp->cptr || !hp->clist || (hp->ncells > 0 && !hp->hcells)) {
+            delete pl;
+            return gc::set_status(-1, "the Ewald correction needs the correction list and the "
+                                      "order-4 cell table");
+        }
+        int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+        for (int64_t g = 0; g < ng; g++)
+            if (hp->cptr[g + 1] < hp->cptr[g])
+                bad |= 1;
+        if (bad || hp->cptr[0] != 0 || !check_list(hp->cptr, hp->clist, np)) {
+            delete pl;
+            return gc::set_status(-1, "bad correction list (decreasing offsets or entry outside "
+                                      "the point table)");
+        }
+    }
 
     if (pl->tune.warps_per_block < 1 || pl->tune.warps_per_block > 8)
         pl->tune.warps_per_block = 8;
@@ -584,14 +549,9 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
     d.points = pts;
     nln_qcell *qc = nullptr;
     nln_hcell *hc = nullptr;
-    const bool want_ewald = hp->box > 0 && hp->ewald;
-    if (want_ewald && !hp->qcells && hp->ncells > 0) {
-        grav_plan_free(pl);
-        return gc::set_status(-1, "the Ewald correction needs the quadrupole cell table");
-    }
-    if ((hp->qptr && hp->qptr[ng]) || (want_ewald && hp->ncells > 0))
+    if (hp->qptr && hp->qptr[ng])
         rc |= dev_copy(pl, hp->qcells, (size_t)hp->ncells, &qc);
-    if (hp->hptr && hp->hptr[ng])
+    if ((hp->hptr && hp->hptr[ng]) || (want_ewald && hp->ncells > 0))
         rc |= dev_copy(pl, hp->hcells, (size_t)hp->ncells, &hc);
     d.qcells = qc;
     d.hcells = hc;
@@ -624,19 +584,20 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
     int64_t *gs = nullptr;
     rc |= dev_copy(pl, gslot.data(), gslot.size(), &gs);
     d.gslot = gs;
-    int64_t *lp0 = nullptr, *lp1 = nullptr, *lp2 = nullptr;
-    rc |= dev_copy(pl, eptr, (size_t)ng + 1, &lp0);
-    if (hp->qptr)
-        rc |= dev_copy(pl, hp->qptr, (size_t)ng + 1, &lp1);
-    if (hp->hptr)
-        rc |= dev_copy(pl, hp->hptr, (size_t)ng + 1, &lp2);
-    d.lptr[0] = lp0;
-    d.lptr[1] = lp1;
-    d.lptr[2] = lp2;
+    d.cptr = nullptr;
+    d.clist = nullptr;
+    if (want_ewald) {
+        int64_t *cp = nullptr;
+        uint32_t *cl = nullptr;
+        rc |= dev_copy(pl, hp->cptr, (size_t)ng + 1, &cp);
+        rc |= dev_copy(pl, hp->clist, (size_t)std::max<int64_t>(1, hp->cptr[ng]), &cl);
+        d.cptr = cp;
+        d.clist = cl;
+    }
     d.ewald = 0;
-    if (hp->box > 0 && hp->ewald) {
+    if (want_ewald) {
         // FP64 table on the host, FP32 copy on the device
-        const int n = pl->tune.ewald_n > 1 ? pl->tune.ewald_n : 64;
+        const int n = pl->tune.ewald_n > 1 ? pl->tune.ewald_n : 32;
         // the table depends only on (box, n): build it once per process
         static std::mutex cache_mu;
         static double cache_box = 0;

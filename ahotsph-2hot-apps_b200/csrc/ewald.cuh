@@ -3,61 +3,71 @@
 // C(y) = Phi_Ewald(y) + 1/|y| (nln/ewald.c:13-64 minus the nearest-image
 // Newtonian term) is smooth inside |y_k| < NLN_EWALD_REACH * L, so a sink
 // group collects, over its list, the moments
-//     M0 = sum m C(y_j),  M1 = sum m dC(y_j),  M2 = sum m ddC(y_j),  M3 = sum m dddC(y_j)
-// at its centre (y_j = source centre - group centre, in the list's image)
-// and each sink at offset u takes the Taylor expansion
-//     phi_i = M0 - u.M1 + 1/2 u.M2.u - 1/6 M3[uuu],   a_i = M1 - M2 u + 1/2 M3[uu].
-// Values at y come from an FP64-built table of C and its first three
-// derivatives on the positive octant (cubic symmetry), by a third-order
+//     M_s[alpha] = sum_j sum_k sum_{|beta| = k} S_k,j[beta] D^(alpha+beta) C(y_j) / beta!,
+// |alpha| = s = 0..4, at its centre (y_j = source centre - group centre, in
+// the list's image; S_0 = m, S_1 = 0 about the centre of mass, S_2..S_4 the
+// source's traceless second to fourth moments; their traces only meet the
+// constant Laplacian of C).  A sink at offset u then takes the Taylor
+// expansion
+//     phi = sum_{|beta| <= 4} M[beta] (-u)^beta / beta!,
+//     a_i = sum_{|beta| <= 3} M[e_i + beta] (-u)^beta / beta!.
+// Values at y come from an FP64-built table of C and its first five
+// derivatives on the positive octant (cubic symmetry), by a fourth-order
 // Taylor expansion about the nearest node, in FP32.
-// Component order (nlnlists.h): C | x y z | xx xy xz yy yz zz |
-//                                xxx xxy xxz xyy xyz xzz yyy yyz yzz zzz
+//
+// Multi-index layout (nlnlists.h): order n starts at n(n+1)(n+2)/6 and
+// (ax, ay, az) sits at offset (ay+az)(ay+az+1)/2 + az within it.
 #pragma once
 
 #include "common.cuh"
 
+namespace ew {
+
+constexpr int kNode = 56;  // floats per table node: orders 0..5
+constexpr int kNQ4 = 35;   // components of orders 0..4
+
+__host__ __device__ constexpr int base(int n) { return n * (n + 1) * (n + 2) / 6; }
+__host__ __device__ constexpr int idx(int ax, int ay, int az) {
+    return base(ax + ay + az) + (ay + az) * (ay + az + 1) / 2 + az;
+}
+__host__ __device__ constexpr float ifact(int k) {
+    return k == 0 ? 1.f : k == 1 ? 1.f : k == 2 ? 0.5f : k == 3 ? 1.f / 6.f : k == 4 ? 1.f / 24.f
+                                                                                 : 1.f / 120.f;
+}
+
+}  // namespace ew
+
 struct EwTab {
-    const float *t;   // n^3 x NLN_EWALD_NQ
+    const float *t;   // n^3 nodes x ew::kNode
     int n;
     float h, inv_h;
 };
 
-// v = T[d, d] (vector) for symmetric T in the 10-component order
-__device__ __forceinline__ void t_dd(const float *T, float dx, float dy, float dz, float *v) {
-    const float xx = dx * dx, xy = 2.f * dx * dy, xz = 2.f * dx * dz, yy = dy * dy,
-                yz = 2.f * dy * dz, zz = dz * dz;
-    v[0] = T[0] * xx + T[1] * xy + T[2] * xz + T[3] * yy + T[4] * yz + T[5] * zz;
-    v[1] = T[1] * xx + T[3] * xy + T[4] * xz + T[6] * yy + T[7] * yz + T[8] * zz;
-    v[2] = T[2] * xx + T[4] * xy + T[5] * xz + T[7] * yy + T[8] * yz + T[9] * zz;
+// d^beta / beta! for |beta| <= 4 (35 values, multi-index layout)
+__device__ __forceinline__ void ew_monomials(float dx, float dy, float dz, float *mono) {
+    float px[5], py[5], pz[5];
+    px[0] = py[0] = pz[0] = 1.f;
+#pragma unroll
+    for (int k = 1; k < 5; k++) {
+        px[k] = px[k - 1] * dx * (1.f / k);
+        py[k] = py[k - 1] * dy * (1.f / k);
+        pz[k] = pz[k - 1] * dz * (1.f / k);
+    }
+#pragma unroll
+    for (int bx = 0; bx <= 4; bx++)
+#pragma unroll
+        for (int by = 0; by <= 4; by++)
+#pragma unroll
+            for (int bz = 0; bz <= 4; bz++)
+                if (bx + by + bz <= 4)
+                    mono[ew::idx(bx, by, bz)] = px[bx] * py[by] * pz[bz];
 }
 
-// v = T[Q] (vector) for symmetric 3x3 Q given as xx xy xz yy yz zz
-__device__ __forceinline__ void t_q(const float *T, const float *Q, float *v) {
-    v[0] = T[0] * Q[0] + 2.f * T[1] * Q[1] + 2.f * T[2] * Q[2] + T[3] * Q[3] + 2.f * T[4] * Q[4] + T[5] * Q[5];
-    v[1] = T[1] * Q[0] + 2.f * T[3] * Q[1] + 2.f * T[4] * Q[2] + T[6] * Q[3] + 2.f * T[7] * Q[4] + T[8] * Q[5];
-    v[2] = T[2] * Q[0] + 2.f * T[4] * Q[1] + 2.f * T[5] * Q[2] + T[7] * Q[3] + 2.f * T[8] * Q[4] + T[9] * Q[5];
-}
-
-// M = T d (symmetric matrix xx xy xz yy yz zz)
-__device__ __forceinline__ void t_d(const float *T, float dx, float dy, float dz, float *M) {
-    M[0] = T[0] * dx + T[1] * dy + T[2] * dz;
-    M[1] = T[1] * dx + T[3] * dy + T[4] * dz;
-    M[2] = T[2] * dx + T[4] * dy + T[5] * dz;
-    M[3] = T[3] * dx + T[6] * dy + T[7] * dz;
-    M[4] = T[4] * dx + T[7] * dy + T[8] * dz;
-    M[5] = T[5] * dx + T[8] * dy + T[9] * dz;
-}
-
-// w = H d
-__device__ __forceinline__ void h_d(const float *H, float dx, float dy, float dz, float *w) {
-    w[0] = H[0] * dx + H[1] * dy + H[2] * dz;
-    w[1] = H[1] * dx + H[3] * dy + H[4] * dz;
-    w[2] = H[2] * dx + H[4] * dy + H[5] * dz;
-}
-
-// C and its derivatives at y (20 floats, component order above).
-__device__ __forceinline__ void ew_lookup(const EwTab &E, float yx, float yy, float yz,
-                                          float *o) {
+// C and its derivatives of orders 0..4 at y (35 floats, multi-index layout);
+// with WANT5 also the fifth derivatives at the nearest node (21 floats, f5).
+template <bool WANT5>
+__device__ __forceinline__ void ew_lookup(const EwTab &E, float yx, float yy, float yz, float *o,
+                                          float *f5) {
     const float sx = yx < 0.f ? -1.f : 1.f, sy = yy < 0.f ? -1.f : 1.f, sz = yz < 0.f ? -1.f : 1.f;
     const float ax = fabsf(yx), ay = fabsf(yy), az = fabsf(yz);
     const int nm = E.n - 1;
@@ -65,64 +75,207 @@ __device__ __forceinline__ void ew_lookup(const EwTab &E, float yx, float yy, fl
     const int j = min(__float2int_rn(ay * E.inv_h), nm);
     const int k = min(__float2int_rn(az * E.inv_h), nm);
     const float dx = ax - i * E.h, dy = ay - j * E.h, dz = az - k * E.h;
-    const float4 *p = reinterpret_cast<const float4 *>(E.t + (((size_t)i * E.n + j) * E.n + k) * 20);
-    float t[20];
+    const float4 *p =
+        reinterpret_cast<const float4 *>(E.t + (((size_t)i * E.n + j) * E.n + k) * ew::kNode);
+    float V[WANT5 ? 56 : 36];
 #pragma unroll
-    for (int q = 0; q < 5; q++) {
-        float4 v = __ldg(p + q);
-        t[4 * q] = v.x;
-        t[4 * q + 1] = v.y;
-        t[4 * q + 2] = v.z;
-        t[4 * q + 3] = v.w;
+    for (int q = 0; q < (WANT5 ? 14 : 9); q++) {
+        const float4 v = __ldg(p + q);
+        V[4 * q] = v.x;
+        V[4 * q + 1] = v.y;
+        V[4 * q + 2] = v.z;
+        V[4 * q + 3] = v.w;
     }
-    const float *G0 = t + 1, *H0 = t + 4, *T0 = t + 10;
-    float Tdd[3], Td[6], Hd[3];
-    t_dd(T0, dx, dy, dz, Tdd);
-    t_d(T0, dx, dy, dz, Td);
-    h_d(H0, dx, dy, dz, Hd);
-    // C
-    o[0] = t[0] + G0[0] * dx + G0[1] * dy + G0[2] * dz +
-           0.5f * (Hd[0] * dx + Hd[1] * dy + Hd[2] * dz) +
-           (1.f / 6.f) * (Tdd[0] * dx + Tdd[1] * dy + Tdd[2] * dz);
-    // gradient
-    o[1] = sx * (G0[0] + Hd[0] + 0.5f * Tdd[0]);
-    o[2] = sy * (G0[1] + Hd[1] + 0.5f * Tdd[1]);
-    o[3] = sz * (G0[2] + Hd[2] + 0.5f * Tdd[2]);
-    // Hessian
-    o[4] = H0[0] + Td[0];
-    o[5] = sx * sy * (H0[1] + Td[1]);
-    o[6] = sx * sz * (H0[2] + Td[2]);
-    o[7] = H0[3] + Td[3];
-    o[8] = sy * sz * (H0[4] + Td[4]);
-    o[9] = H0[5] + Td[5];
-    // third derivatives: component xyz picks up sx^nx sy^ny sz^nz
-    o[10] = sx * T0[0];
-    o[11] = sy * T0[1];
-    o[12] = sz * T0[2];
-    o[13] = sx * T0[3];
-    o[14] = sx * sy * sz * T0[4];
-    o[15] = sx * T0[5];
-    o[16] = sy * T0[6];
-    o[17] = sz * T0[7];
-    o[18] = sy * T0[8];
-    o[19] = sz * T0[9];
+    float mono[35];
+    ew_monomials(dx, dy, dz, mono);
+    // o[alpha] = sum_{|beta| <= 4 - |alpha|} V[alpha + beta] d^beta / beta!, then the octant
+    // sign.  Every loop has constant bounds (guards fold after unrolling), so
+    // the arrays stay in registers.
+#pragma unroll
+    for (int a0 = 0; a0 <= 4; a0++)
+#pragma unroll
+        for (int a1 = 0; a1 <= 4; a1++)
+#pragma unroll
+            for (int a2 = 0; a2 <= 4; a2++) {
+                if (a0 + a1 + a2 > 4)
+                    continue;
+                float acc = 0.f;
+#pragma unroll
+                for (int b0 = 0; b0 <= 4; b0++)
+#pragma unroll
+                    for (int b1 = 0; b1 <= 4; b1++)
+#pragma unroll
+                        for (int b2 = 0; b2 <= 4; b2++)
+                            if (a0 + a1 + a2 + b0 + b1 + b2 <= 4)
+                                acc = fmaf(V[ew::idx(a0 + b0, a1 + b1, a2 + b2)],
+                                           mono[ew::idx(b0, b1, b2)], acc);
+                const float sg = ((a0 & 1) ? sx : 1.f) * ((a1 & 1) ? sy : 1.f) * ((a2 & 1) ? sz : 1.f);
+                o[ew::idx(a0, a1, a2)] = sg * acc;
+            }
+    if (WANT5) {
+#pragma unroll
+        for (int a0 = 0; a0 <= 5; a0++)
+#pragma unroll
+            for (int a1 = 0; a1 <= 5; a1++) {
+                if (a0 + a1 > 5)
+                    continue;
+                const int a2 = 5 - a0 - a1;
+                const float sg = ((a0 & 1) ? sx : 1.f) * ((a1 & 1) ? sy : 1.f) * ((a2 & 1) ? sz : 1.f);
+                f5[ew::idx(a0, a1, a2) - ew::base(5)] = sg * V[ew::idx(a0, a1, a2)];
+            }
+    }
 }
 
-// Evaluate a group's correction moments M (20, FP64) at sink offset u: (phi, a).
-__device__ __forceinline__ void ew_apply(const double *M, double ux, double uy, double uz,
+// Group correction moments: orders 0..2 in FP64 (the net field is a small
+// difference of O(1)-per-mass terms summed over thousands of entries), the
+// u^2 and u^3 terms (orders 3, 4) in FP32.
+struct EwMoments {
+    double lo[10];
+    float hi[25];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int q = 0; q < 10; q++) lo[q] = 0.0;
+#pragma unroll
+        for (int q = 0; q < 25; q++) hi[q] = 0.f;
+    }
+    __device__ __forceinline__ void add(int q, float v) {
+        if (q < 10)
+            lo[q] += (double)v;
+        else
+            hi[q - 10] += v;
+    }
+    __device__ __forceinline__ double get(int q) const { return q < 10 ? lo[q] : (double)hi[q - 10]; }
+    __device__ __forceinline__ void warp_sum() {
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+#pragma unroll
+            for (int q = 0; q < 10; q++) lo[q] += __shfl_xor_sync(0xffffffffu, lo[q], d);
+#pragma unroll
+            for (int q = 0; q < 25; q++) hi[q] += __shfl_xor_sync(0xffffffffu, hi[q], d);
+        }
+    }
+};
+
+// M_s[alpha] += sum_{|beta| = K} S[beta] D[alpha + beta] / beta!  for s = 0..SMAX,
+// D = o (orders <= 4) and f5 (order 5); S in the multi-index layout of order K.
+template <int K, int SMAX>
+__device__ __forceinline__ void ew_fold(EwMoments &M, const float *S, const float *o, const float *f5) {
+#pragma unroll
+    for (int a0 = 0; a0 <= SMAX; a0++)
+#pragma unroll
+        for (int a1 = 0; a1 <= SMAX; a1++)
+#pragma unroll
+            for (int a2 = 0; a2 <= SMAX; a2++) {
+                if (a0 + a1 + a2 > SMAX)
+                    continue;
+                float acc = 0.f;
+#pragma unroll
+                for (int b0 = 0; b0 <= K; b0++)
+#pragma unroll
+                    for (int b1 = 0; b1 <= K; b1++) {
+                        if (b0 + b1 > K)
+                            continue;
+                        const int b2 = K - b0 - b1;
+                        const int q = ew::idx(a0 + b0, a1 + b1, a2 + b2);
+                        const float D = q < ew::kNQ4 ? o[q] : f5[q - ew::kNQ4];
+                        acc = fmaf(S[ew::idx(b0, b1, b2) - ew::base(K)] *
+                                       (ew::ifact(b0) * ew::ifact(b1) * ew::ifact(b2)),
+                                   D, acc);
+                    }
+                M.add(ew::idx(a0, a1, a2), acc);
+            }
+}
+
+// A source of mass m at the looked-up point: M_s += m D^alpha C.
+__device__ __forceinline__ void ew_add_mass(EwMoments &M, float m, const float *o) {
+#pragma unroll
+    for (int q = 0; q < ew::kNQ4; q++) M.add(q, m * o[q]);
+}
+
+// Traceless second moment (multi-index layout xx xy xz yy yz zz) from the
+// normalised quadrupole q2 = (xx, xy, yy, xz, yz) / R^2 of the cell tables.
+__device__ __forceinline__ void ew_quad(float R, const float *q2, float *S2) {
+    const float R2 = R * R;
+    S2[0] = R2 * q2[0];
+    S2[1] = R2 * q2[1];
+    S2[2] = R2 * q2[3];
+    S2[3] = R2 * q2[2];
+    S2[4] = R2 * q2[4];
+    S2[5] = -R2 * (q2[0] + q2[2]);
+}
+
+// Traceless third moment (10 components) from q3 = (xxx, xxy, xyy, yyy, xxz, xyz, yyz) / R^3.
+__device__ __forceinline__ void ew_oct(float R, const float *q3, float *S3) {
+    const float R3 = R * R * R;
+    const float xxx = R3 * q3[0], xxy = R3 * q3[1], xyy = R3 * q3[2], yyy = R3 * q3[3],
+                xxz = R3 * q3[4], xyz = R3 * q3[5], yyz = R3 * q3[6];
+    S3[ew::idx(3, 0, 0) - 10] = xxx;
+    S3[ew::idx(2, 1, 0) - 10] = xxy;
+    S3[ew::idx(2, 0, 1) - 10] = xxz;
+    S3[ew::idx(1, 2, 0) - 10] = xyy;
+    S3[ew::idx(1, 1, 1) - 10] = xyz;
+    S3[ew::idx(1, 0, 2) - 10] = -(xxx + xyy);
+    S3[ew::idx(0, 3, 0) - 10] = yyy;
+    S3[ew::idx(0, 2, 1) - 10] = yyz;
+    S3[ew::idx(0, 1, 2) - 10] = -(xxy + yyy);
+    S3[ew::idx(0, 0, 3) - 10] = -(xxz + yyz);
+}
+
+// Traceless fourth moment (15 components) from
+// q4 = (xxxx, xxxy, xxyy, xyyy, yyyy, xxxz, xxyz, xyyz, yyyz) / R^4.
+__device__ __forceinline__ void ew_hex(float R, const float *q4, float *S4) {
+    const float R2 = R * R, R4 = R2 * R2;
+    const float xxxx = R4 * q4[0], xxxy = R4 * q4[1], xxyy = R4 * q4[2], xyyy = R4 * q4[3],
+                yyyy = R4 * q4[4], xxxz = R4 * q4[5], xxyz = R4 * q4[6], xyyz = R4 * q4[7],
+                yyyz = R4 * q4[8];
+    const float xxzz = -(xxxx + xxyy), yyzz = -(xxyy + yyyy);
+    S4[ew::idx(4, 0, 0) - 20] = xxxx;
+    S4[ew::idx(3, 1, 0) - 20] = xxxy;
+    S4[ew::idx(3, 0, 1) - 20] = xxxz;
+    S4[ew::idx(2, 2, 0) - 20] = xxyy;
+    S4[ew::idx(2, 1, 1) - 20] = xxyz;
+    S4[ew::idx(2, 0, 2) - 20] = xxzz;
+    S4[ew::idx(1, 3, 0) - 20] = xyyy;
+    S4[ew::idx(1, 2, 1) - 20] = xyyz;
+    S4[ew::idx(1, 1, 2) - 20] = -(xxxy + xyyy);
+    S4[ew::idx(1, 0, 3) - 20] = -(xxxz + xyyz);
+    S4[ew::idx(0, 4, 0) - 20] = yyyy;
+    S4[ew::idx(0, 3, 1) - 20] = yyyz;
+    S4[ew::idx(0, 2, 2) - 20] = yyzz;
+    S4[ew::idx(0, 1, 3) - 20] = -(xxyz + yyyz);
+    S4[ew::idx(0, 0, 4) - 20] = -(xxzz + yyzz);
+}
+
+// Evaluate the group's correction moments at sink offset u: (phi, a), FP64.
+__device__ __forceinline__ void ew_apply(const EwMoments &M, double ux, double uy, double uz,
                                          double &phi, double &axx, double &ayy, double &azz) {
-    const double *M1 = M + 1, *H = M + 4, *T = M + 10;
-    const double Mu0 = H[0] * ux + H[1] * uy + H[2] * uz;
-    const double Mu1 = H[1] * ux + H[3] * uy + H[4] * uz;
-    const double Mu2 = H[2] * ux + H[4] * uy + H[5] * uz;
-    const double xx = ux * ux, xy = 2 * ux * uy, xz = 2 * ux * uz, yy = uy * uy,
-                 yz = 2 * uy * uz, zz = uz * uz;
-    const double T0 = T[0] * xx + T[1] * xy + T[2] * xz + T[3] * yy + T[4] * yz + T[5] * zz;
-    const double T1 = T[1] * xx + T[3] * xy + T[4] * xz + T[6] * yy + T[7] * yz + T[8] * zz;
-    const double T2 = T[2] * xx + T[4] * xy + T[5] * xz + T[7] * yy + T[8] * yz + T[9] * zz;
-    phi = M[0] - (M1[0] * ux + M1[1] * uy + M1[2] * uz) + 0.5 * (Mu0 * ux + Mu1 * uy + Mu2 * uz) -
-          (T0 * ux + T1 * uy + T2 * uz) / 6.0;
-    axx = M1[0] - Mu0 + 0.5 * T0;
-    ayy = M1[1] - Mu1 + 0.5 * T1;
-    azz = M1[2] - Mu2 + 0.5 * T2;
+    double px[5], py[5], pz[5];
+    px[0] = py[0] = pz[0] = 1.0;
+#pragma unroll
+    for (int k = 1; k < 5; k++) {
+        px[k] = px[k - 1] * (-ux) / k;
+        py[k] = py[k - 1] * (-uy) / k;
+        pz[k] = pz[k - 1] * (-uz) / k;
+    }
+    double p = 0.0, a[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int b0 = 0; b0 <= 4; b0++)
+#pragma unroll
+        for (int b1 = 0; b1 <= 4; b1++)
+#pragma unroll
+            for (int b2 = 0; b2 <= 4; b2++) {
+                if (b0 + b1 + b2 > 4)
+                    continue;
+                const double w = px[b0] * py[b1] * pz[b2];
+                p += M.get(ew::idx(b0, b1, b2)) * w;
+                if (b0 + b1 + b2 <= 3) {
+                    a[0] += M.get(ew::idx(b0 + 1, b1, b2)) * w;
+                    a[1] += M.get(ew::idx(b0, b1 + 1, b2)) * w;
+                    a[2] += M.get(ew::idx(b0, b1, b2 + 1)) * w;
+                }
+            }
+    phi = p;
+    axx = a[0];
+    ayy = a[1];
+    azz = a[2];
 }

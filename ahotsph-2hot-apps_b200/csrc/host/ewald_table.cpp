@@ -1,5 +1,5 @@
 // ewald_table.cpp -- FP64 table of the periodic correction to the Newtonian
-// potential, with its first three derivatives, for the batched kernels'
+// potential, with its first five derivatives, for the batched kernels'
 // Ewald term and for the FP64 direct-sum measurement.
 //
 // The periodic Green's function is the Ewald sum of nln/ewald.c:13-64
@@ -9,11 +9,20 @@
 //                - sum_{h != 0} exp(-pi^2 h^2/(alpha L)^2) cos(2 pi h.y/L) / (pi L h^2)
 // and its gradient is the force of ewald() on the sink.  The table holds
 //   C(y) = Phi_per(y) + 1/|y|      (the n = 0 term becomes erf(alpha r)/r)
-// which is smooth in |y_k| < L.  Every derivative is analytic: radial
-// terms through g'/r, (g'' - g'/r)/r^2 and (g''' - 3g''/r + 3g'/r^2)/r^3,
-// plane waves through powers of k; near r = 0 the n = 0 term is summed as a
-// power series in (alpha r)^2.  Real-space images are kept while
-// erfc(alpha r) > 1e-17 (r < 3L), the same k-space cut as ewald().
+// which is smooth in |y_k| < L.
+//
+// Every derivative is analytic.  A radial g(r) differentiates through
+// D^k g, D = (1/r) d/dr: the derivative with multi-index alpha (|alpha| = n)
+// is the sum over partial pairings of its n indices, a pairing with p
+// pairs contributing D^(n-p) g times the product of the paired deltas and
+// of x over the unpaired indices.  For erfc(alpha r)/r the D^k follow the
+// recurrence B_0 = erfc(alpha r)/r,
+//   B_k = ((2k-1) B_(k-1) + (2 alpha^2)^k exp(-alpha^2 r^2) / (alpha sqrt(pi))) / r^2,
+// with D^k (erfc(alpha r)/r) = (-1)^k B_k; near r = 0 the n = 0 term
+// erf(alpha r)/r is summed as a power series in q = r^2 (D = 2 d/dq).
+// Plane waves differentiate through powers of k.  Real-space images are
+// kept while erfc(alpha r) > 1e-17 (r < 3L), the same k-space cut as
+// ewald().
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -25,90 +34,107 @@
 
 namespace {
 
+constexpr int kMaxOrder = 5;
+
+// Component layout (nlnlists.h): order n starts at n(n+1)(n+2)/6 and lists
+// the multi-indices (ax, ay, az), ax + ay + az = n, with the sorted index
+// tuples in lexicographic order, i.e. at offset (n-ax)(n-ax+1)/2 + az.
+int comp_base(int n) { return n * (n + 1) * (n + 2) / 6; }
+int comp_off(int n, int ax, int az) { return (n - ax) * (n - ax + 1) / 2 + az; }
+
+// D^k g for k = 0..kMaxOrder at radius r
 struct Rad {
-    double g, gr, a2, a3;  // g, g'/r, (g''-g'/r)/r^2, (g'''-3g''/r+3g'/r^2)/r^3
+    double d[kMaxOrder + 1];
 };
 
 // g(r) = -erfc(alpha r)/r
 Rad rad_erfc(double r, double alpha) {
-    const double c = 2.0 * alpha / std::sqrt(M_PI);
-    const double E = std::erfc(alpha * r);
-    const double ex = std::exp(-alpha * alpha * r * r);
-    const double E1 = -c * ex;
-    const double E2 = c * 2.0 * alpha * alpha * r * ex;
-    const double E3 = c * 2.0 * alpha * alpha * (1.0 - 2.0 * alpha * alpha * r * r) * ex;
-    const double r2 = r * r, r3 = r2 * r, r4 = r3 * r;
-    double f = E / r;
-    double f1 = E1 / r - E / r2;
-    double f2 = E2 / r - 2.0 * E1 / r2 + 2.0 * E / r3;
-    double f3 = E3 / r - 3.0 * E2 / r2 + 6.0 * E1 / r3 - 6.0 * E / r4;
-    f = -f; f1 = -f1; f2 = -f2; f3 = -f3;
+    const double r2 = r * r;
+    const double ex = std::exp(-alpha * alpha * r2) / (alpha * std::sqrt(M_PI));
+    double B = std::erfc(alpha * r) / r, p = 1.0;
     Rad o;
-    o.g = f;
-    o.gr = f1 / r;
-    o.a2 = (f2 - f1 / r) / r2;
-    o.a3 = (f3 - 3.0 * f2 / r + 3.0 * f1 / r2) / r3;
+    o.d[0] = -B;
+    for (int k = 1; k <= kMaxOrder; k++) {
+        p *= 2.0 * alpha * alpha;
+        B = ((2 * k - 1) * B + p * ex) / r2;
+        o.d[k] = (k & 1) ? B : -B;  // -(-1)^k B_k
+    }
     return o;
 }
 
 // g(r) = erf(alpha r)/r = c P(q), q = r^2, c = 2 alpha/sqrt(pi),
-// P(q) = sum_n (-1)^n alpha^(2n) q^n / (n! (2n+1)); then g'/r = 2cP',
-// a2 = 4cP'', a3 = 8cP''' (all regular at r = 0).
+// P(q) = sum_n (-1)^n alpha^(2n) q^n / (n! (2n+1)); D^k g = 2^k c P^(k)(q)
+// (all regular at r = 0).
 Rad rad_erf_series(double r, double alpha) {
     const double c = 2.0 * alpha / std::sqrt(M_PI);
     const double q = r * r, a2 = alpha * alpha;
-    double P = 0, P1 = 0, P2 = 0, P3 = 0;
+    double P[kMaxOrder + 1] = {};
     double coef = 1.0;  // (-1)^n alpha^(2n) / n!
     for (int n = 0; n < 40; n++) {
         const double pn = coef / (2 * n + 1);
-        P += pn * std::pow(q, n);
-        if (n >= 1) P1 += pn * n * std::pow(q, n - 1);
-        if (n >= 2) P2 += pn * n * (n - 1) * std::pow(q, n - 2);
-        if (n >= 3) P3 += pn * n * (n - 1) * (n - 2) * std::pow(q, n - 3);
+        // k-th derivative of q^n: n!/(n-k)! q^(n-k)
+        double f = 1.0;
+        for (int k = 0; k <= kMaxOrder && k <= n; k++) {
+            P[k] += pn * f * std::pow(q, n - k);
+            f *= (n - k);
+        }
         coef *= -a2 / (n + 1);
-        if (std::fabs(coef) * std::pow(q + 1e-300, n) < 1e-30 && n > 8)
+        if (std::fabs(coef) * std::pow(q + 1e-300, n) < 1e-30 && n > 10)
             break;
     }
     Rad o;
-    o.g = c * P;
-    o.gr = 2.0 * c * P1;
-    o.a2 = 4.0 * c * P2;
-    o.a3 = 8.0 * c * P3;
+    double s = c;
+    for (int k = 0; k <= kMaxOrder; k++, s *= 2.0) o.d[k] = s * P[k];
     return o;
 }
 
-// g(r) = erf(alpha r)/r = 1/r - erfc(alpha r)/r, directly (alpha r >= 1)
+// g(r) = erf(alpha r)/r = 1/r - erfc(alpha r)/r, directly (alpha r >= 1);
+// D^k (1/r) = (-1)^k (2k-1)!! / r^(2k+1)
 Rad rad_erf_direct(double r, double alpha) {
-    Rad e = rad_erfc(r, alpha);  // -erfc/r
-    const double r2 = r * r, r3 = r2 * r;
-    // 1/r: g = 1/r, g' = -1/r^2, g'' = 2/r^3, g''' = -6/r^4
-    Rad o;
-    o.g = 1.0 / r + e.g;
-    o.gr = -1.0 / r3 + e.gr;
-    o.a2 = 3.0 / (r2 * r3) + e.a2;
-    o.a3 = -15.0 / (r3 * r2 * r2) + e.a3;
+    Rad o = rad_erfc(r, alpha);
+    const double r2 = r * r;
+    double v = 1.0 / r;
+    for (int k = 0; k <= kMaxOrder; k++) {
+        o.d[k] += v;
+        v *= -(2 * k + 1) / r2;
+    }
     return o;
 }
 
-// accumulate a radial term at displacement x into the 20 outputs
+// Sum over partial pairings of the index list I[0..n): for each set of
+// disjoint pairs, delta products times x over the unpaired indices times
+// D^(n - pairs) g.  n <= 5, so a plain recursion is enough.
+double pair_sum(const int *I, int n, const double x[3], const Rad &R, unsigned used, int pairs) {
+    int first = -1;
+    for (int a = 0; a < n; a++)
+        if (!(used & (1u << a))) {
+            first = a;
+            break;
+        }
+    if (first < 0)
+        return R.d[n - pairs];
+    // `first` stays unpaired ...
+    double s = x[I[first]] * pair_sum(I, n, x, R, used | (1u << first), pairs);
+    // ... or pairs with a later free index of the same axis
+    for (int b = first + 1; b < n; b++)
+        if (!(used & (1u << b)) && I[b] == I[first])
+            s += pair_sum(I, n, x, R, used | (1u << first) | (1u << b), pairs + 1);
+    return s;
+}
+
+// accumulate a radial term at displacement x into all NLN_EWALD_NQ outputs
 void add_radial(const Rad &R, const double x[3], double *o) {
-    o[0] += R.g;
-    for (int i = 0; i < 3; i++) o[1 + i] += R.gr * x[i];
-    static const int H[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
-    for (int k = 0; k < 6; k++) {
-        int i = H[k][0], j = H[k][1];
-        o[4 + k] += R.a2 * x[i] * x[j] + (i == j ? R.gr : 0.0);
-    }
-    static const int T[10][3] = {{0, 0, 0}, {0, 0, 1}, {0, 0, 2}, {0, 1, 1}, {0, 1, 2},
-                                 {0, 2, 2}, {1, 1, 1}, {1, 1, 2}, {1, 2, 2}, {2, 2, 2}};
-    for (int k = 0; k < 10; k++) {
-        int i = T[k][0], j = T[k][1], l = T[k][2];
-        double d = 0.0;
-        if (j == l) d += x[i];
-        if (i == l) d += x[j];
-        if (i == j) d += x[l];
-        o[10 + k] += R.a3 * x[i] * x[j] * x[l] + R.a2 * d;
-    }
+    for (int n = 0; n <= kMaxOrder; n++)
+        for (int ax = n; ax >= 0; ax--)
+            for (int ay = n - ax; ay >= 0; ay--) {
+                const int az = n - ax - ay;
+                int I[kMaxOrder];
+                int k = 0;
+                for (int a = 0; a < ax; a++) I[k++] = 0;
+                for (int a = 0; a < ay; a++) I[k++] = 1;
+                for (int a = 0; a < az; a++) I[k++] = 2;
+                o[comp_base(n) + comp_off(n, ax, az)] += pair_sum(I, n, x, R, 0u, 0);
+            }
 }
 
 void ewald_eval(double L, const double *y, double *o) {
@@ -133,7 +159,8 @@ void ewald_eval(double L, const double *y, double *o) {
                     continue;
                 add_radial(rad_erfc(r, alpha), x, o);
             }
-    // k space: -A cos(k.y), A = exp(-pi^2 h^2/(alpha L)^2)/(pi L h^2), k = 2 pi h / L
+    // k space: -A cos(k.y), A = exp(-pi^2 h^2/(alpha L)^2)/(pi L h^2), k = 2 pi h / L;
+    // the n-th derivative is -A k^alpha times cos, -sin, -cos, sin, ... at n = 0, 1, 2, 3
     for (int i = -4; i <= 4; i++)
         for (int j = -4; j <= 4; j++)
             for (int k = -4; k <= 4; k++) {
@@ -145,15 +172,15 @@ void ewald_eval(double L, const double *y, double *o) {
                 const double kv[3] = {2 * M_PI * i / L, 2 * M_PI * j / L, 2 * M_PI * k / L};
                 const double ph = kv[0] * y[0] + kv[1] * y[1] + kv[2] * y[2];
                 const double cs = std::cos(ph), sn = std::sin(ph);
-                o[0] -= A * cs;
-                for (int a = 0; a < 3; a++) o[1 + a] += A * kv[a] * sn;
-                static const int H[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
-                for (int m = 0; m < 6; m++) o[4 + m] += A * kv[H[m][0]] * kv[H[m][1]] * cs;
-                static const int T[10][3] = {{0, 0, 0}, {0, 0, 1}, {0, 0, 2}, {0, 1, 1},
-                                             {0, 1, 2}, {0, 2, 2}, {1, 1, 1}, {1, 1, 2},
-                                             {1, 2, 2}, {2, 2, 2}};
-                for (int m = 0; m < 10; m++)
-                    o[10 + m] -= A * kv[T[m][0]] * kv[T[m][1]] * kv[T[m][2]] * sn;
+                const double trig[4] = {cs, -sn, -cs, sn};
+                for (int n = 0; n <= kMaxOrder; n++)
+                    for (int ax = n; ax >= 0; ax--)
+                        for (int ay = n - ax; ay >= 0; ay--) {
+                            const int az = n - ax - ay;
+                            const double kp = std::pow(kv[0], ax) * std::pow(kv[1], ay) *
+                                              std::pow(kv[2], az);
+                            o[comp_base(n) + comp_off(n, ax, az)] -= A * kp * trig[n & 3];
+                        }
             }
 }
 

@@ -92,9 +92,10 @@ struct nln_tree {
     std::vector<nln_hcell> hc;
     std::vector<nln_group> groups;
     
-    std::vector<int64_t> lptr[3];
+    std::vector<int64_t> lptr[4];
     std::vector<uint32_t> plist;
     std::vector<uint32_t> qlist, hlist;
+    std::vector<uint32_t> clist;  // periodic correction list
     std::vector<int64_t> aptr[3];
     std::vector<float> adata[3];
     int64_t counts[4] = {0, 0, 0, 0};
@@ -529,6 +530,7 @@ namespace {
 struct GroupLists {
     std::vector<uint32_t> p;   // point-table record | image << 27
     std::vector<uint32_t> q, h;
+    std::vector<uint32_t> c;   // periodic correction: point-table record | image << 27
     int64_t nb = 0, nm = 0;
 };
 
@@ -538,16 +540,48 @@ inline uint16_t shift_code(const int s[3]) {
 
 }  // namespace
 
+// Distance from y to the nearest nonzero lattice vector of the periodic cube.
+static double lattice_gap(const double y[3], double box) {
+    double D2 = INFINITY;
+    for (int a = -1; a <= 1; a++)
+        for (int b = -1; b <= 1; b++)
+            for (int e = -1; e <= 1; e++) {
+                if (!a && !b && !e)
+                    continue;
+                const double dx = y[0] - a * box, dy = y[1] - b * box, dz = y[2] - e * box;
+                D2 = std::min(D2, dx * dx + dy * dy + dz * dz);
+            }
+    return std::sqrt(D2);
+}
+
+// The walk of one sink group (nln/mac.c:1703-1840 semantics: a cell is
+// taken at the lowest order whose critical radius it clears, else opened;
+// a leaf that cannot be taken expands to its bodies).
+//
+// Periodic boxes also get the group's correction list.  The correction
+// needs every source in the same image as its Newtonian entry, but only
+// near the half-box does that image depend on the walk: a cell whose
+// bodies all lie strictly inside the group centre's minimum-image cube
+// (|y|_inf + bmax < L/2) has every descendant entry in that same image.
+// Such a cell enters the correction list whole, in place of its subtree's
+// entries, once bmax + group radius <= ewald_theta x its distance to the
+// correction's nearest singularity (the group's own image at a lattice
+// vector); everywhere else the correction list repeats the Newtonian
+// entries.  Stack entries carry that "covered" flag in bit 0.
 static void walk_group(const nln_tree *t, const nln_group &G, GroupLists &L,
                        std::vector<int32_t> &stack) {
     const double box = t->p.box;
+    const double theta = t->p.ewald_theta;
     const int p2 = t->p.p2cut, p4 = t->p.p4cut;
+    const uint32_t nb = (uint32_t)t->n;
     int64_t covered = 0;
     stack.clear();
     stack.push_back(0);
     while (!stack.empty()) {
-        const int32_t ci = stack.back();
+        const int32_t top = stack.back();
         stack.pop_back();
+        const int32_t ci = top >> 1;
+        bool ccov = (top & 1) != 0;
         const Cell &c = t->cells[ci];
         double y[3];
         int s[3] = {0, 0, 0};
@@ -564,61 +598,56 @@ static void walk_group(const nln_tree *t, const nln_group &G, GroupLists &L,
         // the domain of the Ewald correction, |y_k| <= NLN_EWALD_REACH * box,
         // where the correction is smooth; otherwise the cell is opened.
         bool inside = true;
+        const uint16_t sc = shift_code(s);
         if (box > 0) {
-            double ym = std::max(std::fabs(y[0]), std::max(std::fabs(y[1]), std::fabs(y[2])));
+            const double ym = std::max(std::fabs(y[0]), std::max(std::fabs(y[1]), std::fabs(y[2])));
             inside = ym + c.bmax + G.radius <= NLN_EWALD_REACH * box;
-            // The correction takes a cell at its centre with its quadrupole;
-            // keep cells small against their distance to the correction's
-            // nearest singularity (the sink's own image at a lattice vector).
-            if (inside && t->p.ewald_theta > 0) {
-                double D2 = INFINITY;
-                for (int a = -1; a <= 1; a++)
-                    for (int b = -1; b <= 1; b++)
-                        for (int e = -1; e <= 1; e++) {
-                            if (!a && !b && !e)
-                                continue;
-                            const double dx = y[0] - a * box, dy = y[1] - b * box, dz = y[2] - e * box;
-                            D2 = std::min(D2, dx * dx + dy * dy + dz * dz);
-                        }
-                inside = c.bmax + G.radius <= t->p.ewald_theta * std::sqrt(D2);
+            if (!ccov && theta > 0 && c.count > 0 && ym + c.bmax < 0.5 * box * (1.0 - 1e-9) &&
+                c.bmax + G.radius <= theta * lattice_gap(y, box)) {
+                L.c.push_back((nb + (uint32_t)ci) | ((uint32_t)sc << NLN_IDX_BITS));
+                ccov = true;
             }
         }
+        const bool emit_c = box > 0 && !ccov;
         const double dd = dist - G.radius;
-        const uint16_t sc = shift_code(s);
         if (inside && c.count > 0) {
-            if (dd > c.rc_m + c.bmax) {
-                L.p.push_back((uint32_t)(t->n + ci) | ((uint32_t)sc << NLN_IDX_BITS));
-                L.nm++;
-                covered += c.count;
-                continue;
-            }
-            if (p2 && c.count >= p2 && dd > c.rc_q + c.bmax) {
-                L.q.push_back((uint32_t)ci | ((uint32_t)sc << NLN_IDX_BITS));
-                covered += c.count;
-                continue;
-            }
-            if (p4 && c.count >= p4 && dd > c.rc_h + c.bmax) {
-                L.h.push_back((uint32_t)ci | ((uint32_t)sc << NLN_IDX_BITS));
+            const bool take = dd > c.rc_m + c.bmax || (p2 && c.count >= p2 && dd > c.rc_q + c.bmax) ||
+                              (p4 && c.count >= p4 && dd > c.rc_h + c.bmax);
+            if (take) {
+                if (dd > c.rc_m + c.bmax) {
+                    L.p.push_back((nb + (uint32_t)ci) | ((uint32_t)sc << NLN_IDX_BITS));
+                    L.nm++;
+                } else if (p2 && c.count >= p2 && dd > c.rc_q + c.bmax) {
+                    L.q.push_back((uint32_t)ci | ((uint32_t)sc << NLN_IDX_BITS));
+                } else {
+                    L.h.push_back((uint32_t)ci | ((uint32_t)sc << NLN_IDX_BITS));
+                }
+                if (emit_c)
+                    L.c.push_back((nb + (uint32_t)ci) | ((uint32_t)sc << NLN_IDX_BITS));
                 covered += c.count;
                 continue;
             }
         }
         if (c.child >= 0) {
-            for (int k = c.nchild - 1; k >= 0; k--) stack.push_back(c.child + k);
+            for (int k = c.nchild - 1; k >= 0; k--)
+                stack.push_back(((c.child + k) << 1) | (ccov ? 1 : 0));
             continue;
         }
         // leaf: expand to bodies (nln/mac.c:1817-1832)
-        if (inside || box <= 0) {
-            for (int32_t k = 0; k < c.count; k++)
-                L.p.push_back((uint32_t)(c.first + k) | ((uint32_t)sc << NLN_IDX_BITS));
-        } else {
-            // a leaf reaching out of the correction's domain: each body its own image
-            for (int32_t k = 0; k < c.count; k++) {
+        for (int32_t k = 0; k < c.count; k++) {
+            uint32_t e;
+            if (inside || box <= 0) {
+                e = (uint32_t)(c.first + k) | ((uint32_t)sc << NLN_IDX_BITS);
+            } else {
+                // a leaf reaching out of the correction's domain: each body its own image
                 const float *x = &t->spos[3 * (c.first + k)];
                 int sb[3];
                 for (int d = 0; d < 3; d++) sb[d] = -(int)std::nearbyint((x[d] - G.cen[d]) / box);
-                L.p.push_back((uint32_t)(c.first + k) | ((uint32_t)shift_code(sb) << NLN_IDX_BITS));
+                e = (uint32_t)(c.first + k) | ((uint32_t)shift_code(sb) << NLN_IDX_BITS);
             }
+            L.p.push_back(e);
+            if (emit_c)
+                L.c.push_back(e);
         }
         L.nb += c.count;
         covered += c.count;
@@ -629,6 +658,7 @@ static void walk_group(const nln_tree *t, const nln_group &G, GroupLists &L,
         std::abort();
     }
 }
+
 
 static void emit_aosoa(nln_tree *t, const std::vector<GroupLists> &GL) {
     const int64_t ng = (int64_t)t->groups.size();
@@ -699,12 +729,13 @@ extern "C" int nln_tree_walk(nln_tree *t) {
 #pragma omp for schedule(dynamic, 8)
         for (int64_t g = 0; g < ng; g++) walk_group(t, t->groups[g], GL[g], stack);
     }
-    for (int k = 0; k < 3; k++) t->lptr[k].assign(ng + 1, 0);
+    for (int k = 0; k < 4; k++) t->lptr[k].assign(ng + 1, 0);
     int64_t cnt[4] = {0, 0, 0, 0};
     for (int64_t g = 0; g < ng; g++) {
         t->lptr[0][g + 1] = t->lptr[0][g] + (int64_t)GL[g].p.size();
         t->lptr[1][g + 1] = t->lptr[1][g] + (int64_t)GL[g].q.size();
         t->lptr[2][g + 1] = t->lptr[2][g] + (int64_t)GL[g].h.size();
+        t->lptr[3][g + 1] = t->lptr[3][g] + (int64_t)GL[g].c.size();
         const int64_t gc = t->groups[g].count;
         cnt[0] += gc * GL[g].nb;
         cnt[1] += gc * GL[g].nm;
@@ -715,11 +746,13 @@ extern "C" int nln_tree_walk(nln_tree *t) {
     t->plist.resize(t->lptr[0][ng]);
     t->qlist.resize(t->lptr[1][ng]);
     t->hlist.resize(t->lptr[2][ng]);
+    t->clist.resize(t->lptr[3][ng]);
 #pragma omp parallel for schedule(static)
     for (int64_t g = 0; g < ng; g++) {
         std::copy(GL[g].p.begin(), GL[g].p.end(), t->plist.begin() + t->lptr[0][g]);
         std::copy(GL[g].q.begin(), GL[g].q.end(), t->qlist.begin() + t->lptr[1][g]);
         std::copy(GL[g].h.begin(), GL[g].h.end(), t->hlist.begin() + t->lptr[2][g]);
+        std::copy(GL[g].c.begin(), GL[g].c.end(), t->clist.begin() + t->lptr[3][g]);
     }
     if (t->p.emit_aosoa)
         emit_aosoa(t, GL);
@@ -738,7 +771,7 @@ extern "C" const nln_group *nln_groups(const nln_tree *t) { return t->groups.dat
 extern "C" const float *nln_sorted_pos(const nln_tree *t) { return t->spos.data(); }
 
 extern "C" const int64_t *nln_list_ptr(const nln_tree *t, int kind) {
-    return (kind >= 0 && kind < 3 && !t->lptr[kind].empty()) ? t->lptr[kind].data() : nullptr;
+    return (kind >= 0 && kind < 4 && !t->lptr[kind].empty()) ? t->lptr[kind].data() : nullptr;
 }
 extern "C" const void *nln_list_data(const nln_tree *t, int kind) {
     if (kind == 0)
@@ -747,6 +780,8 @@ extern "C" const void *nln_list_data(const nln_tree *t, int kind) {
         return t->qlist.data();
     if (kind == 2)
         return t->hlist.data();
+    if (kind == 3)
+        return t->clist.data();
     return nullptr;
 }
 extern "C" int64_t nln_list_len(const nln_tree *t, int kind) {
@@ -756,6 +791,8 @@ extern "C" int64_t nln_list_len(const nln_tree *t, int kind) {
         return (int64_t)t->qlist.size();
     if (kind == 2)
         return (int64_t)t->hlist.size();
+    if (kind == 3)
+        return (int64_t)t->clist.size();
     return -1;
 }
 extern "C" void nln_counts(const nln_tree *t, int64_t out[4]) {

@@ -43,7 +43,8 @@ class Problem(ctypes.Structure):
                 ("qptr", ctypes.c_void_p), ("hptr", ctypes.c_void_p),
                 ("plist", ctypes.c_void_p), ("qlist", ctypes.c_void_p),
                 ("hlist", ctypes.c_void_p), ("eps2", ctypes.c_double), ("box", ctypes.c_double),
-                ("quad_phi_sign", ctypes.c_float), ("ewald", ctypes.c_int)]
+                ("quad_phi_sign", ctypes.c_float), ("ewald", ctypes.c_int),
+                ("cptr", ctypes.c_void_p), ("clist", ctypes.c_void_p)]
 
 
 class Tuning(ctypes.Structure):
@@ -133,7 +134,7 @@ class Plan:
         prob.nbodies, prob.ncells, prob.ngroups = t.n, t.ncells, t.ngroups
         prob.points = pts.ctypes.data
         prob.qcells = keep(t.qcells).ctypes.data if len(t.qcells) else None
-        prob.hcells = keep(t.hcells).ctypes.data if has_h else None
+        prob.hcells = keep(t.hcells).ctypes.data if (has_h or ewald) and len(t.hcells) else None
         prob.groups = groups.ctypes.data
         prob.pptr = keep(t.ptr[0]).ctypes.data
         prob.qptr = keep(t.ptr[1]).ctypes.data
@@ -145,6 +146,9 @@ class Plan:
         prob.box = float(t.box)
         prob.quad_phi_sign = float(quad_phi_sign)
         prob.ewald = int(bool(ewald))
+        if ewald:
+            prob.cptr = keep(t.ptr[3]).ctypes.data
+            prob.clist = keep(t.clist).ctypes.data if len(t.clist) else keep(np.zeros(1, np.uint32)).ctypes.data
         self.problem = prob
         h = ctypes.c_void_p()
         tun = None
@@ -308,8 +312,9 @@ class PinnedProblem:
         p.nbodies, p.ncells, p.ngroups = t.n, t.ncells, t.ngroups
         p.points = pin(t.points).ctypes.data
         has_q, has_h = len(t.qlist) > 0, len(t.hlist) > 0
-        p.qcells = pin(t.qcells).ctypes.data if len(t.qcells) else None
-        p.hcells = pin(t.hcells).ctypes.data if has_h else None
+        periodic = t.box > 0
+        p.qcells = pin(t.qcells).ctypes.data if has_q else None
+        p.hcells = pin(t.hcells).ctypes.data if (has_h or periodic) and len(t.hcells) else None
         p.groups = pin(t.groups).ctypes.data
         p.pptr = pin(t.ptr[0]).ctypes.data
         p.qptr = pin(t.ptr[1]).ctypes.data
@@ -317,6 +322,9 @@ class PinnedProblem:
         p.plist = pin(t.plist if len(t.plist) else np.zeros(1, np.uint32)).ctypes.data
         p.qlist = pin(t.qlist if has_q else np.zeros(1, np.uint32)).ctypes.data
         p.hlist = pin(t.hlist if has_h else np.zeros(1, np.uint32)).ctypes.data
+        if periodic:
+            p.cptr = pin(t.ptr[3]).ctypes.data
+            p.clist = pin(t.clist if len(t.clist) else np.zeros(1, np.uint32)).ctypes.data
         p.quad_phi_sign = 1.0
         self.problem = p
         buf = torch.empty(t.n * 16, dtype=torch.uint8, pin_memory=True)

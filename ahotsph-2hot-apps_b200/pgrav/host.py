@@ -97,12 +97,17 @@ class Tree:
 
     Bodies are stored in key (tree) order; ``order[i]`` is the original
     index of tree body ``i``.  Lists are index lists into ``points`` (float4
-    bodies then cell monopoles), ``qcells`` and ``hcells``.
+    bodies then cell monopoles), ``qcells`` and ``hcells``.  Periodic trees
+    (box > 0) also carry ``clist``/``ptr[3]``, the Ewald correction list:
+    ``ewald_theta`` is its opening angle (a cell wholly inside a group's
+    minimum-image cube stands for its subtree once bmax + group radius <=
+    ewald_theta x its distance to the group's nearest lattice image; 0 makes
+    the list repeat the Newtonian entries).
     """
 
     def __init__(self, pos, mass, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-3,
                  rel_tol=0.0, rel_tol0=0.0, box=0.0, nthreads=0, emit_aosoa=False, walk=True,
-                 ewald_theta=0.0):
+                 ewald_theta=0.2):
         pos = np.ascontiguousarray(pos, dtype=np.float32).reshape(-1, 3)
         mass = np.ascontiguousarray(np.broadcast_to(np.asarray(mass, np.float32), (len(pos),)))
         self.params = Params(leaf_max, group_max, p2cut, p4cut, tol, rel_tol, rel_tol0, box,
@@ -132,10 +137,12 @@ class Tree:
         if L.nln_tree_walk(self._h) != 0:
             raise RuntimeError("walk failed")
         ng = self.ngroups
-        self.ptr = [_view(L.nln_list_ptr(self._h, k), np.int64, ng + 1, self._owner) for k in range(3)]
+        self.ptr = [_view(L.nln_list_ptr(self._h, k), np.int64, ng + 1, self._owner) for k in range(4)]
         self.plist = _view(L.nln_list_data(self._h, 0), np.uint32, L.nln_list_len(self._h, 0), self._owner)
         self.qlist = _view(L.nln_list_data(self._h, 1), np.uint32, L.nln_list_len(self._h, 1), self._owner)
         self.hlist = _view(L.nln_list_data(self._h, 2), np.uint32, L.nln_list_len(self._h, 2), self._owner)
+        # periodic correction list (bodies and cells as n + cell index); empty when isolated
+        self.clist = _view(L.nln_list_data(self._h, 3), np.uint32, L.nln_list_len(self._h, 3), self._owner)
         c = (ctypes.c_int64 * 4)()
         L.nln_counts(self._h, c)
         self.counts = np.array(list(c), dtype=np.int64)

@@ -156,7 +156,8 @@ typedef struct grav_problem {
     int64_t ngroups;
     const float *points;        /* (nbodies + ncells) x float4 (x, y, z, m) */
     const nln_qcell *qcells;    /* ncells records, or NULL when no quadrupole lists */
-    const nln_hcell *hcells;    /* ncells records, or NULL when no order-4 lists */
+    const nln_hcell *hcells;    /* ncells records, or NULL when no order-4 lists (required
+                                   with ewald: the correction uses every cell's moments) */
     const nln_group *groups;    /* ngroups records */
     const int64_t *pptr, *qptr, *hptr;  /* ngroups + 1 each */
     const uint32_t *plist, *qlist, *hlist;  /* entries: index | image << 27 (nlnlists.h) */
@@ -164,6 +165,9 @@ typedef struct grav_problem {
     double box;                 /* periodic cube side; 0 = isolated */
     float quad_phi_sign;        /* +1 physical; -1 reproduces do_gravpq's potential */
     int ewald;                  /* periodic only: 1 = add the Ewald correction */
+    const int64_t *cptr;        /* ewald: ngroups + 1 offsets of the correction list */
+    const uint32_t *clist;      /* ewald: point-table records | image << 27; cells enter as
+                                   nbodies + cell index and take the order-4 table's moments */
 } grav_problem;
 
 typedef struct grav_plan grav_plan;
@@ -175,7 +179,7 @@ typedef struct grav_tuning {
     int chunk_q;                /* max quadrupole cells per work item */
     int chunk_h;                /* max order-4 cells per work item */
     int blocks_per_sm;          /* persistent grid = blocks_per_sm x SM count (0: as many as fit) */
-    int ewald_n;                /* Ewald table nodes per axis (0: 64) */
+    int ewald_n;                /* Ewald table nodes per axis (0: 32) */
 } grav_tuning;
 
 /*

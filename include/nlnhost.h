@@ -37,8 +37,11 @@ typedef struct nln_params {
     double box;       /* periodic cube side L with bodies in [0,L)^3; 0 = isolated */
     int nthreads;     /* host threads (0: all) */
     int emit_aosoa;   /* 1: also pack the reference AoSoA lists */
-    double ewald_theta; /* periodic: accepted cells keep bmax + group radius <= ewald_theta x
-                           distance to the nearest other image of the sink (0: off) */
+    double ewald_theta; /* periodic: opening angle of the correction list -- a cell wholly
+                           inside the group's minimum-image cube stands for its subtree there
+                           once bmax + group radius <= ewald_theta x its distance to the
+                           nearest other lattice image of the group centre (0: the correction
+                           list repeats the Newtonian entries) */
 } nln_params;
 
 typedef struct nln_tree nln_tree;
@@ -73,7 +76,11 @@ const nln_qcell *nln_qcells(const nln_tree *t);
 const nln_hcell *nln_hcells(const nln_tree *t);
 const nln_group *nln_groups(const nln_tree *t);
 
-/* CSR lists per group: uint32 entries [ptr[g], ptr[g+1]); kind 0 = points, 1 = Q, 2 = H. */
+/*
+ * CSR lists per group: uint32 entries [ptr[g], ptr[g+1]); kind 0 = points,
+ * 1 = Q, 2 = H, 3 = the periodic correction list (point-table records:
+ * bodies, and cells as n + cell index, whose moments are the order-4 table's).
+ */
 const int64_t *nln_list_ptr(const nln_tree *t, int kind);
 const void *nln_list_data(const nln_tree *t, int kind);
 int64_t nln_list_len(const nln_tree *t, int kind);
@@ -109,7 +116,7 @@ void nln_cell_ranges(const nln_tree *t, int64_t *first, int32_t *count);
 const float *nln_sorted_pos(const nln_tree *t);
 
 /*
- * The periodic correction C(y) = Phi_Ewald(y) + 1/|y| and its first three
+ * The periodic correction C(y) = Phi_Ewald(y) + 1/|y| and its first five
  * derivatives (NLN_EWALD_NQ doubles, layout of nlnlists.h) at one
  * displacement y = source - sink in a cube of side L, from the Ewald sum of
  * nln/ewald.c:13-64 (same alpha = 2/L and k-space cut), differentiated

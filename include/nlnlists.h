@@ -41,12 +41,16 @@ typedef struct nln_hcell {      /* 128 bytes */
 
 /*
  * Ewald correction table: per node, NLN_EWALD_NQ values of
- * C(y) = Phi_Ewald(y) + 1/|y| and its derivatives, in the order
- *   C | dC/dx dC/dy dC/dz | xx xy xz yy yz zz | xxx xxy xxz xyy xyz xzz yyy yyz yzz zzz
+ * C(y) = Phi_Ewald(y) + 1/|y| and its derivatives of orders 0..5, in the order
+ *   C | dC/dx dC/dy dC/dz | xx xy xz yy yz zz | xxx xxy xxz xyy xyz xzz yyy yyz yzz zzz |
+ *   xxxx xxxy ... zzzz (15) | xxxxx xxxxy ... zzzzz (21)
+ * (order n starts at n(n+1)(n+2)/6; its components are the sorted index
+ * tuples i <= j <= ... in lexicographic order, multi-index (ax, ay, az) at
+ * offset (n-ax)(n-ax+1)/2 + az)
  * on an n^3 grid over the positive octant [0, NLN_EWALD_REACH * L]^3
  * (the cubic lattice makes C even in each coordinate).
  */
-#define NLN_EWALD_NQ 20
+#define NLN_EWALD_NQ 56
 
 /*
  * List entries (points, quadrupole and order-4 cells alike): the record

@@ -25,8 +25,23 @@ def host():
     return L
 
 
+NQ = 56   # C, 3 first, 6 second, 10 third, 15 fourth, 21 fifth derivatives
+IDX3 = [(0, 0, 0), (0, 0, 1), (0, 0, 2), (0, 1, 1), (0, 1, 2), (0, 2, 2), (1, 1, 1),
+        (1, 1, 2), (1, 2, 2), (2, 2, 2)]
+IDX4 = list(itertools.combinations_with_replacement(range(3), 4))
+IDX5 = list(itertools.combinations_with_replacement(range(3), 5))
+
+
+def full(vals, idx, rank):
+    T = np.zeros((3,) * rank)
+    for v, ijk in zip(vals, idx):
+        for p in set(itertools.permutations(ijk)):
+            T[p] = v
+    return T
+
+
 def ev(host, y, L=1.0):
-    o = np.zeros(20)
+    o = np.zeros(NQ)
     y = np.ascontiguousarray(y, np.float64)
     host.nln_ewald_eval(L, y.ctypes.data, o.ctypes.data)
     return o
@@ -94,12 +109,8 @@ def test_table_derivatives_by_differences(host):
     h = 1e-5
     o = ev(host, y)
     H = np.array([[o[4], o[5], o[6]], [o[5], o[7], o[8]], [o[6], o[8], o[9]]])
-    T = np.zeros((3, 3, 3))
-    idx = [(0, 0, 0), (0, 0, 1), (0, 0, 2), (0, 1, 1), (0, 1, 2), (0, 2, 2), (1, 1, 1),
-           (1, 1, 2), (1, 2, 2), (2, 2, 2)]
-    for v, ijk in zip(o[10:20], idx):
-        for p in set(itertools.permutations(ijk)):
-            T[p] = v
+    T = full(o[10:20], IDX3, 3)
+    X = full(o[20:35], IDX4, 4)
     for k in range(3):
         e = np.zeros(3)
         e[k] = h
@@ -108,13 +119,37 @@ def test_table_derivatives_by_differences(host):
         Hp = np.array([[op[4], op[5], op[6]], [op[5], op[7], op[8]], [op[6], op[8], op[9]]])
         Hm = np.array([[om[4], om[5], om[6]], [om[5], om[7], om[8]], [om[6], om[8], om[9]]])
         assert np.abs((Hp - Hm) / (2 * h) - T[:, :, k]).max() < 1e-5
+        Tp, Tm = full(op[10:20], IDX3, 3), full(om[10:20], IDX3, 3)
+        assert np.abs((Tp - Tm) / (2 * h) - X[:, :, :, k]).max() < 1e-4 * np.abs(X).max()
+
+
+def test_high_derivatives_by_differences_and_traceless(host):
+    # both branches of the n = 0 term (series for alpha r < 1, closed form
+    # beyond), and Laplace: the traces of the third to fifth derivatives
+    # vanish because the Laplacian of C is the constant -4 pi / L^3
+    for y in (np.array([0.01, -0.02, 0.005]), np.array([0.4, 0.35, -0.3]),
+              np.array([0.55, -0.1, 0.6])):
+        o = ev(host, y)
+        T, X, F = full(o[10:20], IDX3, 3), full(o[20:35], IDX4, 4), full(o[35:56], IDX5, 5)
+        assert np.abs(np.einsum('iik->k', T)).max() < 1e-9 * np.abs(T).max()
+        assert np.abs(np.einsum('iikl->kl', X)).max() < 1e-9 * np.abs(X).max()
+        assert np.abs(np.einsum('iiklm->klm', F)).max() < 1e-9 * np.abs(F).max()
+        h = 1e-5
+        for k in range(3):
+            e = np.zeros(3)
+            e[k] = h
+            op, om = ev(host, y + e), ev(host, y - e)
+            Tp, Tm = full(op[10:20], IDX3, 3), full(om[10:20], IDX3, 3)
+            assert np.abs((Tp - Tm) / (2 * h) - X[..., k]).max() < 1e-4 * np.abs(X).max()
+            Xp, Xm = full(op[20:35], IDX4, 4), full(om[20:35], IDX4, 4)
+            assert np.abs((Xp - Xm) / (2 * h) - F[..., k]).max() < 1e-4 * np.abs(F).max()
 
 
 def test_table_grid(host):
     n, L, reach = 5, 2.0, 0.625
-    tab = np.zeros(n ** 3 * 20)
+    tab = np.zeros(n ** 3 * NQ)
     assert host.nln_ewald_table(L, n, reach, tab.ctypes.data) == 0
-    tab = tab.reshape(n, n, n, 20)
+    tab = tab.reshape(n, n, n, NQ)
     h = reach * L / (n - 1)
     assert np.allclose(tab[1, 2, 3], ev(host, np.array([1, 2, 3]) * h, L), rtol=1e-13, atol=1e-13)
 
