@@ -776,3 +776,201 @@ extern "C" int grav_groups_CUDA(const grav_problem *hp, float *acc_phi) {
     grav_plan_free(pl);
     return rc;
 }
+
+// ------------------------------------------------------------ no-allocation evaluation
+//
+// grav_groups_eval_dev_CUDA runs the batched kernels above on a problem that
+// is already on the device, with every byte of scratch taken from this one
+// file-scope array: queue counters and the error word, one work item per
+// (group, list kind), a checked copy of the groups, the slot offsets and
+// the per-item partial sums.  Its address is looked up once per device.
+static __device__ __align__(256) unsigned char g_dev_scratch[GRAV_DEV_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+
+struct DevScratch {
+    int *counters;      // 4 queue heads: must be 0 when the kernels start
+    unsigned *err;      // device error word: must be 0 when the kernels start
+    Item *items[3];
+    nln_group *groups;  // checked copy of the caller's groups
+    int64_t *gslot;
+    float4 *part;
+};
+
+size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+
+// Scratch bytes for ng groups with nk list kinds.
+size_t dev_scratch_bytes(int64_t ng, int nk) {
+    return 256 + 3 * round256((size_t)ng * sizeof(Item)) + round256((size_t)ng * sizeof(nln_group)) +
+           round256((size_t)(ng + 1) * sizeof(int64_t)) + (size_t)nk * ng * 64 * sizeof(float4);
+}
+
+// Once per device, with that device current: the scratch's address and the
+// kernels' shared-memory attribute.
+int dev_scratch_base(void **out) {
+    static std::mutex mu;
+    static void *base[kMaxDevices] = {};
+    int dev = 0;
+    GC_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices)
+        return gc::set_status(-1, "grav_groups_eval_dev_CUDA: device %d beyond %d", dev, kMaxDevices);
+    std::lock_guard<std::mutex> lk(mu);
+    if (!base[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_dev_scratch);
+        if (e != cudaSuccess || !p)
+            return gc::cuda_status(e, "grav_groups_eval_dev_CUDA: cudaGetSymbolAddress of the scratch");
+        GC_CHECK(cudaFuncSetAttribute(k_batch<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      8 * KindOf<KP>::warp_bytes));
+        GC_CHECK(cudaFuncSetAttribute(k_batch<KQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      8 * KindOf<KQ>::warp_bytes));
+        GC_CHECK(cudaFuncSetAttribute(k_batch<KH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      8 * KindOf<KH>::warp_bytes));
+        base[dev] = p;
+    }
+    *out = base[dev];
+    return 0;
+}
+
+// One thread per group: check the group and its list offsets, copy it, and
+// write its work items (slot nk*g + kind rank) and slot offset.  A group
+// that fails the checks flags GC_DEV_BAD_INDEX and becomes one sink (body
+// 0) with empty lists, so no kernel leaves the tables.
+__global__ void k_dev_setup(const nln_group *__restrict__ groups, const int64_t *p0,
+                            const int64_t *p1, const int64_t *p2, int64_t ng, int64_t nbodies,
+                            int nk, DevScratch S) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g == 0)
+        S.gslot[ng] = (int64_t)nk * ng;
+    if (g >= ng)
+        return;
+    nln_group G = groups[g];
+    const int64_t *ptr[3] = {p0, p1, p2};
+    bool ok = G.count >= 1 && G.count <= 32 && G.first >= 0 && G.first + G.count <= nbodies;
+    for (int k = 0; k < 3; k++)
+        if (ptr[k] && (ptr[k][g] < 0 || ptr[k][g + 1] < ptr[k][g]))
+            ok = false;
+    if (!ok) {
+        atomicOr(S.err, GC_DEV_BAD_INDEX);
+        G.first = 0;
+        G.count = 1;
+    }
+    S.groups[g] = G;
+    int rank = 0;
+    for (int k = 0; k < 3; k++) {
+        if (!ptr[k])
+            continue;
+        const int64_t b = ok ? ptr[k][g] : 0, e = ok ? ptr[k][g + 1] : 0;
+        S.items[k][g] = Item{(int32_t)g, (int32_t)((int64_t)nk * g + rank), b, e};
+        rank++;
+    }
+    S.gslot[g] = (int64_t)nk * g;
+}
+
+}  // namespace
+
+extern "C" int grav_groups_eval_dev_CUDA(const grav_problem *dp, float *acc_phi, void *stream) {
+    if (!dp || !acc_phi || dp->nbodies <= 0 || dp->ngroups <= 0 || !dp->points || !dp->groups ||
+        !dp->pptr || !dp->plist)
+        return gc::set_status(-1, "grav_groups_eval_dev_CUDA: incomplete problem");
+    if (dp->box > 0 && dp->ewald)
+        return gc::set_status(-1, "grav_groups_eval_dev_CUDA: no Ewald correction here (its table "
+                                  "is a per-plan allocation); use grav_groups_upload_CUDA");
+    if (dp->nbodies + dp->ncells >= (int64_t)NLN_IDX_MASK)
+        return gc::set_status(-1, "grav_groups_eval_dev_CUDA: point table exceeds 27-bit indices");
+    if ((dp->qptr && (!dp->qlist || !dp->qcells)) || (dp->hptr && (!dp->hlist || !dp->hcells)))
+        return gc::set_status(-1, "grav_groups_eval_dev_CUDA: a cell list without its table");
+    auto misaligned = [](const void *p) { return ((uintptr_t)p & 15u) != 0; };
+    if (misaligned(dp->points) || misaligned(dp->qcells) || misaligned(dp->hcells) ||
+        misaligned(acc_phi))
+        return gc::set_status(-1, "grav_groups_eval_dev_CUDA: tables and output must be "
+                                  "16-byte aligned");
+    const int64_t ng = dp->ngroups, np = dp->nbodies + dp->ncells;
+    const int nk = 1 + (dp->qptr ? 1 : 0) + (dp->hptr ? 1 : 0);
+    const size_t need = dev_scratch_bytes(ng, nk);
+    if (need > (size_t)GRAV_DEV_SCRATCH_BYTES) {
+        int64_t fit = 0;
+        while (dev_scratch_bytes(fit + 1, nk) <= (size_t)GRAV_DEV_SCRATCH_BYTES) fit += 1;
+        return gc::set_status(-1, "grav_groups_eval_dev_CUDA: %lld groups need %zu bytes of "
+                                  "scratch; the static scratch holds %zu (at most %lld groups with "
+                                  "%d list kinds)",
+                              (long long)ng, need, (size_t)GRAV_DEV_SCRATCH_BYTES, (long long)fit, nk);
+    }
+    void *basev = nullptr;
+    if (int rc = dev_scratch_base(&basev))
+        return rc;
+    unsigned char *base = static_cast<unsigned char *>(basev);
+    DevScratch S{};
+    size_t off = 0;
+    S.counters = reinterpret_cast<int *>(base);
+    S.err = reinterpret_cast<unsigned *>(base + 4 * sizeof(int));
+    off = 256;
+    for (int k = 0; k < 3; k++) {
+        S.items[k] = reinterpret_cast<Item *>(base + off);
+        off += round256((size_t)ng * sizeof(Item));
+    }
+    S.groups = reinterpret_cast<nln_group *>(base + off);
+    off += round256((size_t)ng * sizeof(nln_group));
+    S.gslot = reinterpret_cast<int64_t *>(base + off);
+    off += round256((size_t)(ng + 1) * sizeof(int64_t));
+    S.part = reinterpret_cast<float4 *>(base + off);
+
+    // a plan on the stack: device pointers only, nothing owned
+    grav_plan pl;
+    cudaDeviceGetAttribute(&pl.nsm, cudaDevAttrMultiProcessorCount, 0);
+    pl.tune = default_tuning();
+    DevProblem &d = pl.dp;
+    d.points = reinterpret_cast<const float4 *>(dp->points);
+    d.qcells = dp->qptr ? dp->qcells : nullptr;
+    d.hcells = dp->hptr ? dp->hcells : nullptr;
+    d.groups = S.groups;
+    const int64_t *ptrs[3] = {dp->pptr, dp->qptr, dp->hptr};
+    const uint32_t *lists[3] = {dp->plist, dp->qlist, dp->hlist};
+    for (int k = 0; k < 3; k++) {
+        d.list[k] = ptrs[k] ? lists[k] : nullptr;
+        d.items[k] = ptrs[k] ? S.items[k] : nullptr;
+        d.nitems[k] = ptrs[k] ? (int)ng : 0;
+    }
+    d.ntab[0] = np;
+    d.ntab[1] = d.ntab[2] = dp->ncells;
+    d.counters = S.counters;
+    d.part = S.part;
+    d.gslot = S.gslot;
+    d.out = reinterpret_cast<float4 *>(acc_phi);
+    d.ngroups = ng;
+    d.ncells = dp->ncells;
+    d.eps2 = (float)dp->eps2;
+    d.qsh = 0.5f * (dp->quad_phi_sign == 0.0f ? 1.0f : dp->quad_phi_sign);
+    d.box = dp->box;
+    d.err = S.err;
+    d.cptr = nullptr;
+    d.clist = nullptr;
+    d.ewald = 0;
+    memset(pl.tmap, 0, sizeof(pl.tmap));
+    int rc = encode_rows(&pl.tmap[KP], d.points, (uint64_t)np, 16);
+    if (!rc && d.qcells)
+        rc = encode_rows(&pl.tmap[KQ], d.qcells, (uint64_t)dp->ncells, sizeof(nln_qcell));
+    if (!rc && d.hcells)
+        rc = encode_rows(&pl.tmap[KH], d.hcells, (uint64_t)dp->ncells, sizeof(nln_hcell));
+    if (rc)
+        return rc;
+
+    cudaStream_t st = (cudaStream_t)stream;
+    GC_CHECK(cudaMemsetAsync(base, 0, 256, st));  // queue counters and error word
+    k_dev_setup<<<(unsigned)((ng + 255) / 256), 256, 0, st>>>(dp->groups, dp->pptr, dp->qptr,
+                                                               dp->hptr, ng, dp->nbodies, nk, S);
+    GC_CHECK(cudaGetLastError());
+    if ((rc = launch_kind<KH>(&pl, st)) || (rc = launch_kind<KQ>(&pl, st)) ||
+        (rc = launch_kind<KP>(&pl, st)))
+        return rc;
+    k_finish<<<(unsigned)((ng + 7) / 8), 256, 0, st>>>(pl.dp);
+    GC_CHECK(cudaGetLastError());
+    unsigned h = 0;
+    GC_CHECK(cudaMemcpyAsync(&h, S.err, sizeof(h), cudaMemcpyDeviceToHost, st));
+    GC_CHECK(cudaStreamSynchronize(st));
+    if (h)
+        return gc::set_status(-2, "grav_groups_eval_dev_CUDA: device error word 0x%x", h);
+    return 0;
+}

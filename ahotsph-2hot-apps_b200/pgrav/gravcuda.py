@@ -24,6 +24,7 @@ EXPORTS = [
     "grav_groups_upload_CUDA", "grav_groups_eval_CUDA", "grav_groups_download_CUDA",
     "grav_plan_output", "grav_plan_counts", "grav_plan_launches", "grav_plan_free",
     "grav_groups_CUDA", "grav_direct_fp64_CUDA", "grav_plan_set_timing", "grav_plan_kernel_ms",
+    "grav_groups_eval_dev_CUDA",
 ]
 
 
@@ -88,6 +89,7 @@ def lib(record_errors=True):
             "grav_groups_CUDA": ([vp, vp], i32),
             "grav_direct_fp64_CUDA": ([vp, i64, vp, i64, f64, f64, vp], i32),
             "grav_plan_set_timing": ([vp, i32], i32), "grav_plan_kernel_ms": ([vp, vp], i32),
+            "grav_groups_eval_dev_CUDA": ([vp, vp, vp], i32),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)

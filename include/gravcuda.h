@@ -223,6 +223,43 @@ int grav_groups_CUDA(const grav_problem *host_problem, float *acc_phi);
 int grav_direct_fp64_CUDA(const float *points, int64_t n, const int64_t *sinks, int64_t nsink,
                           double eps2, double box, double *out);
 
+/*
+ * ---- evaluation without allocation (no counterpart in the reference) ----
+ * grav_groups_eval_dev_CUDA evaluates a problem whose tables and lists are
+ * already in device memory (every grav_problem pointer a device pointer,
+ * 16-byte aligned tables; acc_phi: device, nbodies x float4, tree order)
+ * and allocates no device memory at all: no cudaMalloc/cudaFree and no
+ * allocating library call.  It is for callers that cannot allocate on the
+ * device: a code whose memory is owned by another allocator's pool (a
+ * framework caching allocator holding the device, where an outside
+ * cudaMalloc can fail or fragment the pool), and a time-step loop on a
+ * stream it must not stall, where cudaFree would synchronise the whole
+ * device.
+ *
+ * All scratch -- queue counters, error word, work items, a checked copy of
+ * the groups, slot offsets and the per-item partial sums -- lives in one
+ * file-scope device array of GRAV_DEV_SCRATCH_BYTES (16 MiB), enough for
+ * about 5,200 groups with three list kinds (about 100,000 bodies at 20 per
+ * group); larger problems are rejected with an error naming the limit.  The
+ * queue counters and the error word must be zero when the kernels start:
+ * every call zeroes them on its stream first, and writes every work item,
+ * group copy, slot offset and partial sum it reads, so the scratch's earlier
+ * contents never matter.  One work item per group and list kind (no list
+ * splitting, no cost sort); isolated problems, or periodic ones without the
+ * Ewald correction (ewald must be 0: its table is a per-plan allocation).
+ *
+ * The scratch is one per device, so calls that overlap on a device (other
+ * host threads, other streams) race on it and must be serialised by the
+ * caller.  The first call on each device (with that device current) looks
+ * up the scratch's address with cudaGetSymbolAddress and sets kernel
+ * attributes; make it before any stream capture.  The call enqueues on
+ * `stream` (cudaStream_t as void*; NULL = legacy default), synchronises it
+ * to read the error word, and returns 0, -1 for a rejected problem, or -2
+ * when a kernel flagged an error (a bad group or list entry, a lost copy).
+ */
+#define GRAV_DEV_SCRATCH_BYTES (16u << 20)
+int grav_groups_eval_dev_CUDA(const grav_problem *device_problem, float *acc_phi, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
