@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <parallel/algorithm>
 #include <string>
 #include <vector>
@@ -78,6 +79,25 @@ double newton_root(const double *a, int n, double x1, double xacc) {
 
 }  // namespace
 
+// A list array left uninitialised at allocation (its pages are committed as
+// the walk writes them) and released explicitly.
+struct ListBuf {
+    std::unique_ptr<uint32_t[]> p;
+    size_t n = 0;
+    void alloc(size_t count) {
+        p.reset(count ? new uint32_t[count] : nullptr);
+        n = count;
+    }
+    void release() {
+        p.reset();
+        n = 0;
+    }
+    uint32_t *data() { return p.get(); }
+    const uint32_t *data() const { return p.get(); }
+    size_t size() const { return n; }
+    uint32_t operator[](size_t i) const { return p[i]; }
+};
+
 struct nln_tree {
     nln_params p{};
     int64_t n = 0;
@@ -93,9 +113,9 @@ struct nln_tree {
     std::vector<nln_group> groups;
     
     std::vector<int64_t> lptr[4];
-    std::vector<uint32_t> plist;
-    std::vector<uint32_t> qlist, hlist;
-    std::vector<uint32_t> clist;  // periodic correction list
+    ListBuf plist;
+    ListBuf qlist, hlist;
+    ListBuf clist;  // periodic correction list
     std::vector<int64_t> aptr[3];
     std::vector<float> adata[3];
     int64_t counts[4] = {0, 0, 0, 0};
@@ -721,38 +741,78 @@ extern "C" int nln_tree_walk(nln_tree *t) {
         return -1;
     omp_set_num_threads(nthreads_of(t->p));
     const int64_t ng = (int64_t)t->groups.size();
-    std::vector<GroupLists> GL(ng);
-#pragma omp parallel
-    {
-        std::vector<int32_t> stack;
-        stack.reserve(1024);
-#pragma omp for schedule(dynamic, 8)
-        for (int64_t g = 0; g < ng; g++) walk_group(t, t->groups[g], GL[g], stack);
-    }
+    // Groups are walked in chunks.  Each chunk's lists are packed into one
+    // exact-size segment per kind, and its per-group vectors are reused by
+    // the next chunk, so the host holds about one copy of the lists (plus
+    // one segment while they are joined), not per-group vectors and the
+    // final arrays at once.  The AoSoA emitter needs every group's vectors:
+    // then there is a single chunk.
+    const int64_t chunk = t->p.emit_aosoa ? std::max<int64_t>(ng, 1) : 16384;
+    std::vector<GroupLists> GL((size_t)std::min<int64_t>(ng, chunk));
+    struct Segment {
+        ListBuf part[4];
+    };
+    std::vector<Segment> segs;
     for (int k = 0; k < 4; k++) t->lptr[k].assign(ng + 1, 0);
     int64_t cnt[4] = {0, 0, 0, 0};
-    for (int64_t g = 0; g < ng; g++) {
-        t->lptr[0][g + 1] = t->lptr[0][g] + (int64_t)GL[g].p.size();
-        t->lptr[1][g + 1] = t->lptr[1][g] + (int64_t)GL[g].q.size();
-        t->lptr[2][g + 1] = t->lptr[2][g] + (int64_t)GL[g].h.size();
-        t->lptr[3][g + 1] = t->lptr[3][g] + (int64_t)GL[g].c.size();
-        const int64_t gc = t->groups[g].count;
-        cnt[0] += gc * GL[g].nb;
-        cnt[1] += gc * GL[g].nm;
-        cnt[2] += gc * (int64_t)GL[g].q.size();
-        cnt[3] += gc * (int64_t)GL[g].h.size();
+    for (int64_t c0 = 0; c0 < ng; c0 += chunk) {
+        const int64_t c1 = std::min(ng, c0 + chunk);
+#pragma omp parallel
+        {
+            std::vector<int32_t> stack;
+            stack.reserve(1024);
+#pragma omp for schedule(dynamic, 8)
+            for (int64_t g = c0; g < c1; g++) {
+                GroupLists &L = GL[g - c0];
+                L.p.clear();
+                L.q.clear();
+                L.h.clear();
+                L.c.clear();
+                L.nb = L.nm = 0;
+                walk_group(t, t->groups[g], L, stack);
+            }
+        }
+        for (int64_t g = c0; g < c1; g++) {
+            const GroupLists &L = GL[g - c0];
+            t->lptr[0][g + 1] = t->lptr[0][g] + (int64_t)L.p.size();
+            t->lptr[1][g + 1] = t->lptr[1][g] + (int64_t)L.q.size();
+            t->lptr[2][g + 1] = t->lptr[2][g] + (int64_t)L.h.size();
+            t->lptr[3][g + 1] = t->lptr[3][g] + (int64_t)L.c.size();
+            const int64_t gc = t->groups[g].count;
+            cnt[0] += gc * L.nb;
+            cnt[1] += gc * L.nm;
+            cnt[2] += gc * (int64_t)L.q.size();
+            cnt[3] += gc * (int64_t)L.h.size();
+        }
+        Segment S;
+        for (int k = 0; k < 4; k++) S.part[k].alloc((size_t)(t->lptr[k][c1] - t->lptr[k][c0]));
+#pragma omp parallel for schedule(static)
+        for (int64_t g = c0; g < c1; g++) {
+            const GroupLists &L = GL[g - c0];
+            const std::vector<uint32_t> *src[4] = {&L.p, &L.q, &L.h, &L.c};
+            for (int k = 0; k < 4; k++)
+                std::copy(src[k]->begin(), src[k]->end(),
+                          S.part[k].data() + (t->lptr[k][g] - t->lptr[k][c0]));
+        }
+        segs.push_back(std::move(S));
     }
     std::memcpy(t->counts, cnt, sizeof(cnt));
-    t->plist.resize(t->lptr[0][ng]);
-    t->qlist.resize(t->lptr[1][ng]);
-    t->hlist.resize(t->lptr[2][ng]);
-    t->clist.resize(t->lptr[3][ng]);
+    ListBuf *dst[4] = {&t->plist, &t->qlist, &t->hlist, &t->clist};
+    for (int k = 0; k < 4; k++) {
+        dst[k]->alloc((size_t)t->lptr[k][ng]);
+        size_t off = 0;
+        for (Segment &S : segs) {
+            const size_t n = S.part[k].size();
+            uint32_t *d = dst[k]->data() + off;
+            const uint32_t *sp = S.part[k].data();
 #pragma omp parallel for schedule(static)
-    for (int64_t g = 0; g < ng; g++) {
-        std::copy(GL[g].p.begin(), GL[g].p.end(), t->plist.begin() + t->lptr[0][g]);
-        std::copy(GL[g].q.begin(), GL[g].q.end(), t->qlist.begin() + t->lptr[1][g]);
-        std::copy(GL[g].h.begin(), GL[g].h.end(), t->hlist.begin() + t->lptr[2][g]);
-        std::copy(GL[g].c.begin(), GL[g].c.end(), t->clist.begin() + t->lptr[3][g]);
+            for (int64_t b = 0; b < (int64_t)((n + 65535) / 65536); b++) {
+                const size_t lo = (size_t)b * 65536, hi = std::min(n, lo + 65536);
+                std::memcpy(d + lo, sp + lo, (hi - lo) * sizeof(uint32_t));
+            }
+            off += n;
+            S.part[k].release();
+        }
     }
     if (t->p.emit_aosoa)
         emit_aosoa(t, GL);
@@ -815,7 +875,7 @@ extern "C" int64_t nln_aosoa_subset(const nln_tree *t, const int64_t *gids, int6
         return -1;
     static const int SZ[3] = {4, 13, 29};
     const int sz = SZ[kind];
-    const std::vector<uint32_t> &lst = kind == 0 ? t->plist : (kind == 1 ? t->qlist : t->hlist);
+    const ListBuf &lst = kind == 0 ? t->plist : (kind == 1 ? t->qlist : t->hlist);
     const int64_t *ptr = t->lptr[kind].data();
     blk_ptr[0] = 0;
     for (int64_t s = 0; s < ngsel; s++) {

@@ -1,0 +1,61 @@
+"""Host walk invariants (csrc/host/nlnhost.cpp): the chunked list assembly
+equals the single-chunk one, and every group's correction list covers each
+body exactly once, in the image its Newtonian entries use."""
+import numpy as np
+
+
+def _decode(e, n):
+    idx = e & ((1 << 27) - 1)
+    sc = e >> 27
+    return idx, np.stack([sc // 9 - 1, (sc // 3) % 3 - 1, sc % 3 - 1], -1)
+
+
+def test_chunked_walk_equals_single_chunk():
+    from pgrav import host, ics
+    pos, m = ics.grf_box(64, seed=3, rms_disp=0.3)
+    # 64^3 bodies in groups of <= 32 gives more than one 16384-group chunk;
+    # emit_aosoa forces a single chunk
+    a = host.Tree(pos, m, tol=3e-4, box=1.0, group_max=16)
+    b = host.Tree(pos, m, tol=3e-4, box=1.0, group_max=16, emit_aosoa=True)
+    assert a.ngroups > 16384
+    for k in range(4):
+        assert np.array_equal(a.ptr[k], b.ptr[k])
+    for x, y in ((a.plist, b.plist), (a.qlist, b.qlist), (a.hlist, b.hlist), (a.clist, b.clist)):
+        assert np.array_equal(x, y)
+    assert np.array_equal(a.counts, b.counts)
+
+
+def test_correction_list_covers_bodies_once_in_newtonian_image():
+    from pgrav import host, ics
+    pos, m = ics.grf_box(24, seed=5, rms_disp=0.3)
+    t = host.Tree(pos, m, tol=1e-4, box=1.0, ewald_theta=0.2)
+    cf, cc = t.cell_ranges()
+    n = t.n
+
+    def bodies_with_shift(lst, ptr, g, kind):
+        out = np.full((n, 3), 99, np.int64)
+        hit = np.zeros(n, np.int64)
+        idx, sh = _decode(lst[ptr[g]:ptr[g + 1]].astype(np.int64), n)
+        for i, s in zip(idx, sh):
+            if kind in (0, 3) and i < n:
+                rng = np.array([i])
+            else:
+                c = i - n if kind in (0, 3) else i
+                rng = np.arange(cf[c], cf[c] + cc[c])
+            hit[rng] += 1
+            out[rng] = s
+        return hit, out
+
+    rng = np.random.default_rng(0)
+    for g in rng.choice(t.ngroups, 12, replace=False):
+        hits_n = np.zeros(n, np.int64)
+        img_n = np.full((n, 3), 99, np.int64)
+        for kind, lst in ((0, t.plist), (1, t.qlist), (2, t.hlist)):
+            h, o = bodies_with_shift(lst, t.ptr[kind], g, kind)
+            hits_n += h
+            img_n[h > 0] = o[h > 0]
+        hc, img_c = bodies_with_shift(t.clist, t.ptr[3], g, 3)
+        assert np.all(hits_n == 1) and np.all(hc == 1)
+        assert np.array_equal(img_n, img_c)
+        # coarse cells make the correction list shorter than the Newtonian lists
+        assert t.ptr[3][g + 1] - t.ptr[3][g] <= sum(t.ptr[k][g + 1] - t.ptr[k][g] for k in range(3))
