@@ -343,6 +343,9 @@ __global__ void k_finish(DevProblem P) {
 }  // namespace
 
 // ------------------------------------------------------------ plan
+struct grav_step_state;  // time-step state (step.cuh)
+void step_state_free(grav_step_state *S);
+
 struct grav_plan {
     grav_problem hp{};      // sizes and parameters (host pointers cleared)
     grav_tuning tune{};
@@ -355,6 +358,7 @@ struct grav_plan {
     CUtensorMap tmap[3];    // row-gather views of the point, quadrupole and order-4 tables
     int timing = 0;         // record events around each kernel of an evaluation
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    grav_step_state *step = nullptr;  // tree links, refit scratch and the step graph
 };
 
 namespace {
@@ -759,6 +763,8 @@ extern "C" int grav_plan_launches(const grav_plan *pl) { return pl ? pl->launche
 extern "C" void grav_plan_free(grav_plan *pl) {
     if (!pl)
         return;
+    if (pl->step)
+        step_state_free(pl->step);
     for (void *p : pl->allocs) cudaFree(p);
     for (cudaEvent_t e : pl->ev)
         if (e)
@@ -974,3 +980,5 @@ extern "C" int grav_groups_eval_dev_CUDA(const grav_problem *dp, float *acc_phi,
         return gc::set_status(-2, "grav_groups_eval_dev_CUDA: device error word 0x%x", h);
     return 0;
 }
+
+#include "step.cuh"

@@ -924,3 +924,21 @@ extern "C" void nln_cell_ranges(const nln_tree *t, int64_t *first, int32_t *coun
         count[c] = t->cells[c].count;
     }
 }
+
+extern "C" void nln_cell_links(const nln_tree *t, int32_t *child, int32_t *nchild,
+                               int32_t *level) {
+    for (size_t c = 0; c < t->cells.size(); c++) {
+        child[c] = t->cells[c].child;
+        nchild[c] = t->cells[c].nchild;
+        level[c] = t->cells[c].level;
+    }
+}
+
+extern "C" int nln_tree_refit(nln_tree *t, const float *pos) {
+    if (!t || !pos)
+        return -1;
+    omp_set_num_threads(nthreads_of(t->p));
+    std::memcpy(t->spos.data(), pos, sizeof(float) * 3 * (size_t)t->n);
+    compute_moments(t);
+    return 0;
+}

@@ -24,7 +24,8 @@ EXPORTS = [
     "grav_groups_upload_CUDA", "grav_groups_eval_CUDA", "grav_groups_download_CUDA",
     "grav_plan_output", "grav_plan_counts", "grav_plan_launches", "grav_plan_free",
     "grav_groups_CUDA", "grav_direct_fp64_CUDA", "grav_plan_set_timing", "grav_plan_kernel_ms",
-    "grav_groups_eval_dev_CUDA",
+    "grav_groups_eval_dev_CUDA", "grav_plan_set_tree_CUDA", "grav_plan_refit_CUDA",
+    "grav_plan_bodies", "grav_plan_integrate_CUDA", "grav_plan_step_CUDA",
 ]
 
 
@@ -90,6 +91,10 @@ def lib(record_errors=True):
             "grav_direct_fp64_CUDA": ([vp, i64, vp, i64, f64, f64, vp], i32),
             "grav_plan_set_timing": ([vp, i32], i32), "grav_plan_kernel_ms": ([vp, vp], i32),
             "grav_groups_eval_dev_CUDA": ([vp, vp, vp], i32),
+            "grav_plan_set_tree_CUDA": ([vp, vp, vp, vp, vp, vp], i32),
+            "grav_plan_refit_CUDA": ([vp, vp], i32), "grav_plan_bodies": ([vp], vp),
+            "grav_plan_integrate_CUDA": ([vp, vp, vp, vp, vp], i32),
+            "grav_plan_step_CUDA": ([vp, vp, vp, vp, vp, i32], i32),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -173,6 +178,30 @@ class Plan:
 
     def output_ptr(self):
         return lib().grav_plan_output(self._h)
+
+    def bodies_ptr(self):
+        """Device pointer of the body table (x, y, z, m float4, tree order)."""
+        return lib().grav_plan_bodies(self._h)
+
+    def set_tree(self, tree=None):
+        """Give the plan its tree's links so that it can refit on the device."""
+        t = tree or self.tree
+        first, count = t.cell_ranges()
+        child, nchild, level = t.cell_links()
+        self._links = (first, count, child, nchild, level)
+        check(lib().grav_plan_set_tree_CUDA(self._h, first.ctypes.data, count.ctypes.data,
+                                            child.ctypes.data, nchild.ctypes.data,
+                                            level.ctypes.data))
+
+    def refit(self, stream=None):
+        check(lib().grav_plan_refit_CUDA(self._h, stream))
+
+    def integrate(self, vel_ptr, params_ptr, energy_ptr, stream=None):
+        check(lib().grav_plan_integrate_CUDA(self._h, vel_ptr, params_ptr, energy_ptr, stream))
+
+    def step(self, vel_ptr, params_ptr, energy_ptr, stream=None, graph=False):
+        check(lib().grav_plan_step_CUDA(self._h, vel_ptr, params_ptr, energy_ptr, stream,
+                                        int(bool(graph))))
 
     def counts(self):
         c = (ctypes.c_int64 * 4)()

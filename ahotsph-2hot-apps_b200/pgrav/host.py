@@ -62,6 +62,9 @@ def lib():
         L.nln_aosoa_subset.argtypes = [vp, vp, ctypes.c_int64, ctypes.c_int, vp, vp]
         L.nln_aosoa_subset.restype = ctypes.c_int64
         L.nln_cell_ranges.argtypes = [vp, vp, vp]
+        L.nln_cell_links.argtypes = [vp, vp, vp, vp]
+        L.nln_tree_refit.argtypes = [vp, vp]
+        L.nln_tree_refit.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -160,6 +163,25 @@ class Tree:
         count = np.zeros(self.ncells, np.int32)
         lib().nln_cell_ranges(self._h, first.ctypes.data, count.ctypes.data)
         return first, count
+
+    def cell_links(self):
+        """(child, nchild, level) of every cell: first child (-1 for a leaf),
+        child count (children are consecutive) and depth (root 0)."""
+        child = np.zeros(self.ncells, np.int32)
+        nchild = np.zeros(self.ncells, np.int32)
+        level = np.zeros(self.ncells, np.int32)
+        lib().nln_cell_links(self._h, child.ctypes.data, nchild.ctypes.data, level.ctypes.data)
+        return child, nchild, level
+
+    def refit(self, pos_tree_order):
+        """Recompute every cell's moments (and the point, quadrupole and
+        order-4 tables, in place) for new body positions in tree order; the
+        tree, the critical radii and the lists are kept."""
+        p = np.ascontiguousarray(pos_tree_order, np.float32).reshape(-1, 3)
+        if len(p) != self.n:
+            raise ValueError("refit needs one position per body")
+        if lib().nln_tree_refit(self._h, p.ctypes.data) != 0:
+            raise RuntimeError("refit failed")
 
     def aosoa_subset(self, gids, kind):
         """Reference AoSoA blocks (kind 0 = M, 1 = Q, 2 = H) for groups gids:

@@ -1,0 +1,138 @@
+"""Time stepping on the device: the KDK integrator of nln/integrate.c:16-59
+(Integrate) around the batched force evaluation.
+
+The host builds the tree and the interaction lists every ``rebuild``
+steps.  Between rebuilds every step runs on the GPU as evaluate, integrate
+(kick by dtv, drift by dt) and refit of the cell tables, optionally replayed
+from one captured CUDA graph (grav_plan_step_CUDA).  Velocities lag the
+positions by half a step after the first kick (dtv = dt/2 once, then dt),
+and the energies of each step are those of Integrate: KE of the velocity
+synchronised to the positions' time, PE = 1/2 sum m phi (G = 1).
+"""
+import numpy as np
+
+from . import gravcuda as gc
+from . import host
+
+
+def _rt():
+    from cuda.bindings import runtime as rt
+    return rt
+
+
+def memcpy_d2h(dst_array, src_ptr):
+    rt = _rt()
+    err, = rt.cudaMemcpy(dst_array.ctypes.data, src_ptr, dst_array.nbytes,
+                         rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)
+    if int(err) != 0:
+        raise gc.GravError(f"cudaMemcpy D2H failed: {err}")
+    return dst_array
+
+
+def memcpy_h2d(dst_ptr, src_array):
+    rt = _rt()
+    src = np.ascontiguousarray(src_array)
+    err, = rt.cudaMemcpy(dst_ptr, src.ctypes.data, src.nbytes,
+                         rt.cudaMemcpyKind.cudaMemcpyHostToDevice)
+    if int(err) != 0:
+        raise gc.GravError(f"cudaMemcpy H2D failed: {err}")
+
+
+class Stepper:
+    """KDK steps of a particle set with the batched evaluation.
+
+    pos, vel: (n, 3); mass: (n,); eps2 Plummer softening; box > 0 makes the
+    run periodic (with the Ewald correction unless ewald=False).  tree_kw
+    goes to host.Tree (tol, leaf_max, ...).  graph=True replays each step
+    from a CUDA graph captured on the first step after every rebuild.
+    """
+
+    def __init__(self, pos, vel, mass, eps2, box=0.0, ewald=None, rebuild=8, graph=True,
+                 tree_kw=None):
+        import torch
+        self.torch = torch
+        self.pos = np.array(pos, np.float32).reshape(-1, 3)
+        self.vel = np.array(vel, np.float32).reshape(-1, 3)
+        self.mass = np.asarray(mass, np.float32)
+        self.n = len(self.pos)
+        self.eps2 = float(eps2)
+        self.box = float(box)
+        self.ewald = (self.box > 0) if ewald is None else bool(ewald)
+        self.rebuild = max(1, int(rebuild))
+        self.graph = bool(graph)
+        self.tree_kw = dict(tree_kw or {})
+        self.tpos = 0.0
+        self.tvel = 0.0
+        self.nsteps = 0
+        self.history = []
+        self.stream = torch.cuda.Stream()
+        dev = torch.device("cuda")
+        self.params = torch.zeros(3, dtype=torch.float64, device=dev)
+        self.energy = torch.zeros(2, dtype=torch.float64, device=dev)
+        self.dvel = None
+        self.plan = None
+        self.tree = None
+        self._build()
+
+    # -- host rebuild: tree and lists from the current positions
+    def _build(self):
+        torch = self.torch
+        if self.plan is not None:
+            self._pull()
+            self.plan.free()
+            self.plan = None
+        if self.box > 0:
+            self.pos = np.mod(self.pos, np.float32(self.box)).astype(np.float32)
+            self.pos[self.pos >= self.box] = 0.0
+        self.tree = host.Tree(self.pos, self.mass, box=self.box, **self.tree_kw)
+        self.plan = gc.Plan(self.tree, self.eps2, ewald=self.ewald)
+        self.plan.set_tree(self.tree)
+        v = np.zeros((self.n, 4), np.float32)
+        v[:, :3] = self.vel[self.tree.order]
+        self.dvel = torch.from_numpy(v).to("cuda")
+
+    # -- device state back to host arrays in the original body order
+    def _pull(self):
+        self.torch.cuda.synchronize()
+        body = memcpy_d2h(np.empty((self.n, 4), np.float32), self.plan.bodies_ptr())
+        order = self.tree.order
+        self.pos[order] = body[:, :3]
+        self.vel[order] = self.dvel.cpu().numpy()[:, :3]
+
+    def state(self):
+        """(pos, vel) in the original order, current."""
+        self._pull()
+        return self.pos.copy(), self.vel.copy()
+
+    def step(self, dt):
+        torch = self.torch
+        if self.nsteps > 0 and self.nsteps % self.rebuild == 0:
+            self._build()
+        dtv = 0.5 * dt if self.nsteps == 0 else dt
+        dtsync = self.tpos - self.tvel
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(self.stream):
+            self.params.copy_(torch.tensor([dt, dtv, dtsync], dtype=torch.float64))
+            e0.record(self.stream)
+            self.plan.step(self.dvel.data_ptr(), self.params.data_ptr(), self.energy.data_ptr(),
+                           self.stream.cuda_stream, graph=self.graph)
+            e1.record(self.stream)
+        self.stream.synchronize()
+        ke, pe = self.energy.cpu().numpy()
+        rec = {"t": self.tpos, "ke": 0.5 * float(ke), "pe": 0.5 * float(pe),
+               "ms": e0.elapsed_time(e1), "graph": self.graph}
+        rec["e"] = rec["ke"] + rec["pe"]
+        self.history.append(rec)
+        self.tpos += dt
+        self.tvel += dtv
+        self.nsteps += 1
+        return rec
+
+    def run(self, nsteps, dt):
+        return [self.step(dt) for _ in range(nsteps)]
+
+    def free(self):
+        if self.plan is not None:
+            self.plan.free()
+            self.plan = None

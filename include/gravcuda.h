@@ -224,6 +224,41 @@ int grav_direct_fp64_CUDA(const float *points, int64_t n, const int64_t *sinks, 
                           double eps2, double box, double *out);
 
 /*
+ * ---- the time step on the device ----
+ * Between host rebuilds of the tree and lists, bodies move on the device
+ * and the plan's cell tables are refitted from them.
+ *
+ * grav_plan_set_tree_CUDA: the tree's links (host arrays over the plan's
+ * ncells cells, as nlnhost.h's nln_cell_ranges and nln_cell_links give them:
+ * body range, first child or -1, child count, depth).
+ * grav_plan_refit_CUDA: recompute every cell record (monopole, quadrupole,
+ * order-4) from the plan's current body positions, deepest cells first
+ * (leaves from their bodies in FP64, parents by parallel-axis shifts of
+ * their children, as nln/cofm.c mpole_add); lists and sink groups are kept.
+ * grav_plan_bodies: device pointer of the body table (x, y, z, m float4,
+ * tree order), which the integrator updates in place.
+ * grav_plan_integrate_CUDA: Integrate() of nln/integrate.c:16-59 on the
+ * last evaluation's (acc, phi): params (device, 3 doubles) = {dt, dtv,
+ * dtsync = tpos - tvel}; for each body ke += m |v + dtsync a|^2, pe += m phi
+ * (added into energy, device, 2 doubles), then v += dtv a, x += dt v.
+ * vel: device, float4 (vx, vy, vz, unused) per body, tree order.
+ * grav_plan_step_CUDA: one step = zero energy, evaluate, integrate, refit.
+ * With use_graph the step is captured once into a CUDA graph on `stream`
+ * (a created stream, not the legacy default) and replayed by later calls
+ * with the same pointers; params and energy are read and written through
+ * their device pointers, so update params between launches.
+ */
+int grav_plan_set_tree_CUDA(grav_plan *plan, const int64_t *cell_first, const int32_t *cell_count,
+                            const int32_t *cell_child, const int32_t *cell_nchild,
+                            const int32_t *cell_level);
+int grav_plan_refit_CUDA(grav_plan *plan, void *stream);
+float *grav_plan_bodies(grav_plan *plan);
+int grav_plan_integrate_CUDA(grav_plan *plan, float *vel, const double *params, double *energy,
+                             void *stream);
+int grav_plan_step_CUDA(grav_plan *plan, float *vel, const double *params, double *energy,
+                        void *stream, int use_graph);
+
+/*
  * ---- evaluation without allocation (no counterpart in the reference) ----
  * grav_groups_eval_dev_CUDA evaluates a problem whose tables and lists are
  * already in device memory (every grav_problem pointer a device pointer,

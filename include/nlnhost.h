@@ -112,6 +112,21 @@ int64_t nln_aosoa_subset(const nln_tree *t, const int64_t *gids, int64_t ngsel, 
 /* Body range of every cell: bodies [first[c], first[c] + count[c]) in tree order. */
 void nln_cell_ranges(const nln_tree *t, int64_t *first, int32_t *count);
 
+/*
+ * Tree links of every cell: first child (-1 for a leaf), number of children
+ * (children are consecutive cells) and depth (root 0).  Children always
+ * follow their parent in the cell array.
+ */
+void nln_cell_links(const nln_tree *t, int32_t *child, int32_t *nchild, int32_t *level);
+
+/*
+ * Refit: new body positions (tree order, xyz floats) with the same tree and
+ * lists; every cell's centre of mass, moments and bmax (and the point,
+ * quadrupole and order-4 tables) are recomputed from the bodies in FP64.
+ * Critical radii and lists are kept.  Returns 0, or -1 for bad arguments.
+ */
+int nln_tree_refit(nln_tree *t, const float *pos);
+
 /* Body positions in tree order (xyz floats), the sink positions the lists were built for. */
 const float *nln_sorted_pos(const nln_tree *t);
 

@@ -1,0 +1,155 @@
+"""GPU: the device time step (csrc/step.cuh) -- refit of the cell tables
+against the host refit (nln_tree_refit), the integrator against
+nln/integrate.c's formulas, graph replay against eager launches, and energy
+conservation over KDK steps."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mods():
+    import torch
+    from pgrav import gravcuda, host, ics, step
+    return torch, gravcuda, host, ics, step
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)
+
+
+def test_refit_in_place_keeps_forces(mods):
+    torch, gc, host, ics, _ = mods
+    pos, m = ics.plummer(20000, seed=21)
+    t = host.Tree(pos, m, tol=1e-4, p2cut=7, p4cut=20)
+    plan = gc.Plan(t, 1e-4)
+    plan.set_tree(t)
+    plan.eval()
+    f0 = plan.download()
+    plan.refit()
+    plan.eval()
+    f1 = plan.download()
+    plan.free()
+    # R differs (a parent's bmax is a bound) but kernels see R^l q_l
+    assert _rel(f1[:, :3], f0[:, :3]).max() < 2e-6
+    assert np.abs(f1[:, 3] - f0[:, 3]).max() < 2e-6 * np.abs(f0[:, 3]).max()
+
+
+@pytest.mark.parametrize("box", [0.0, 1.0])
+def test_device_refit_matches_host_refit(mods, box):
+    torch, gc, host, ics, step = mods
+    if box:
+        pos, m = ics.grf_box(24, seed=22, rms_disp=0.3)
+        eps2 = (1.0 / 24 / 50) ** 2
+    else:
+        pos, m = ics.plummer(20000, seed=22)
+        eps2 = 1e-4
+    t = host.Tree(pos, m, tol=1e-4, p2cut=7, p4cut=20, box=box)
+    plan = gc.Plan(t, eps2, ewald=box > 0)
+    plan.set_tree(t)
+    # move every body a little, on the device and in the host tree
+    rng = np.random.default_rng(3)
+    moved = t.sorted_pos + rng.normal(0, 1e-3, t.sorted_pos.shape).astype(np.float32)
+    body = np.concatenate([moved, t.points[:t.n, 3:4]], 1).astype(np.float32)
+    step.memcpy_h2d(plan.bodies_ptr(), body)
+    plan.refit()
+    plan.eval()
+    got = plan.download()
+    plan.free()
+    t.refit(moved)
+    ref_plan = gc.Plan(t, eps2, ewald=box > 0)
+    ref_plan.eval()
+    ref = ref_plan.download()
+    ref_plan.free()
+    e = _rel(got[:, :3], ref[:, :3])
+    assert np.sqrt(np.mean(e * e)) < 1e-6 and e.max() < 2e-5, (np.sqrt(np.mean(e * e)), e.max())
+    assert np.abs(got[:, 3] - ref[:, 3]).max() < 1e-5 * np.abs(ref[:, 3]).max()
+
+
+def test_integrate_matches_formula(mods):
+    torch, gc, host, ics, step = mods
+    pos, m = ics.plummer(5000, seed=23)
+    t = host.Tree(pos, m, tol=1e-4)
+    plan = gc.Plan(t, 1e-4)
+    plan.set_tree(t)
+    plan.eval()
+    f = plan.download()
+    rng = np.random.default_rng(4)
+    v = rng.normal(0, 0.3, (t.n, 4)).astype(np.float32)
+    v[:, 3] = 0
+    dvel = torch.from_numpy(v.copy()).cuda()
+    dt, dtv, dtsync = 1e-3, 1e-3, 5e-4
+    params = torch.tensor([dt, dtv, dtsync], dtype=torch.float64, device="cuda")
+    energy = torch.zeros(2, dtype=torch.float64, device="cuda")
+    plan.integrate(dvel.data_ptr(), params.data_ptr(), energy.data_ptr())
+    torch.cuda.synchronize()
+    body = step.memcpy_d2h(np.empty((t.n, 4), np.float32), plan.bodies_ptr())
+    plan.free()
+    x0 = t.points[:t.n, :3].astype(np.float64)
+    mm = t.points[:t.n, 3].astype(np.float64)
+    a = f[:, :3].astype(np.float64)
+    vc = v[:, :3] + dtsync * a
+    v1 = (v[:, :3] + dtv * a).astype(np.float32)
+    x1 = (x0 + dt * v1.astype(np.float64)).astype(np.float32)
+    # FP64 arithmetic rounded to FP32 (a fused multiply-add may round once less)
+    np.testing.assert_allclose(dvel.cpu().numpy()[:, :3], v1, rtol=2e-7, atol=1e-9)
+    np.testing.assert_allclose(body[:, :3], x1, rtol=2e-7, atol=1e-9)
+    ke, pe = energy.cpu().numpy()
+    assert ke == pytest.approx(float((mm[:, None] * vc * vc).sum()), rel=1e-10)
+    assert pe == pytest.approx(float((mm * f[:, 3]).sum()), rel=1e-9)
+
+
+def test_graph_replay_equals_eager(mods):
+    torch, gc, host, ics, step = mods
+    pos, m = ics.plummer(8000, seed=24)
+    vel = np.zeros_like(pos)
+    runs = []
+    for graph in (False, True):
+        s = step.Stepper(pos, vel, m, 1e-4, rebuild=100, graph=graph, tree_kw=dict(tol=1e-4))
+        s.run(3, 1e-3)
+        p, v = s.state()
+        runs.append((p, v, [h["e"] for h in s.history]))
+        s.free()
+    assert np.array_equal(runs[0][0], runs[1][0]) and np.array_equal(runs[0][1], runs[1][1])
+    # energies are FP64 atomic sums: equal up to summation order
+    np.testing.assert_allclose(runs[0][2], runs[1][2], rtol=1e-12)
+
+
+def test_kdk_energy_conservation_plummer(mods):
+    torch, gc, host, ics, step = mods
+    n = 16384
+    pos, m = ics.plummer(n, seed=25)
+    # isotropic velocities at half the local circular speed: a bound, moving system
+    r = np.linalg.norm(pos, axis=1)
+    vc = np.sqrt(r * r / (1 + r * r) ** 1.5)
+    rng = np.random.default_rng(5)
+    d = rng.normal(size=pos.shape)
+    vel = (0.5 * vc / np.linalg.norm(d, axis=1))[:, None] * d
+    s = step.Stepper(pos, vel, m, 0.01 ** 2, rebuild=10, graph=True,
+                     tree_kw=dict(tol=1e-5, p2cut=7, p4cut=20))
+    s.run(40, 2e-3)
+    e = np.array([h["e"] for h in s.history])
+    s.free()
+    assert np.all(np.isfinite(e))
+    assert np.abs(e - e[0]).max() < 2e-4 * abs(e[0]), (e[0], np.abs(e - e[0]).max())
+
+
+def test_kdk_periodic_box_runs_and_wraps(mods):
+    torch, gc, host, ics, step = mods
+    n1 = 16
+    pos, m = ics.grf_box(n1, seed=26, rms_disp=0.3)
+    rng = np.random.default_rng(6)
+    vel = rng.normal(0, 0.05, pos.shape)
+    s = step.Stepper(pos, vel, m, (1.0 / n1 / 50) ** 2, box=1.0, rebuild=3, graph=True,
+                     tree_kw=dict(tol=1e-5, p2cut=7, p4cut=20))
+    s.run(7, 1e-2)
+    p, v = s.state()
+    e = np.array([h["e"] for h in s.history])
+    s.free()
+    assert np.all(np.isfinite(e)) and np.all(np.isfinite(p))
+    # rebuilds wrapped every body back into the box; since the last rebuild
+    # bodies moved by at most a few v dt
+    assert p.min() > -0.05 and p.max() < 1.05
