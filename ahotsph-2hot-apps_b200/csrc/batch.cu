@@ -345,6 +345,8 @@ __global__ void k_finish(DevProblem P) {
 // ------------------------------------------------------------ plan
 struct grav_step_state;  // time-step state (step.cuh)
 void step_state_free(grav_step_state *S);
+struct grav_adjoint_state;  // adjoint scratch (adjoint.cuh)
+void adjoint_state_free(grav_adjoint_state *A);
 
 struct grav_plan {
     grav_problem hp{};      // sizes and parameters (host pointers cleared)
@@ -359,6 +361,7 @@ struct grav_plan {
     int timing = 0;         // record events around each kernel of an evaluation
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     grav_step_state *step = nullptr;  // tree links, refit scratch and the step graph
+    grav_adjoint_state *adj = nullptr;  // adjoint scratch
 };
 
 namespace {
@@ -765,6 +768,8 @@ extern "C" void grav_plan_free(grav_plan *pl) {
         return;
     if (pl->step)
         step_state_free(pl->step);
+    if (pl->adj)
+        adjoint_state_free(pl->adj);
     for (void *p : pl->allocs) cudaFree(p);
     for (cudaEvent_t e : pl->ev)
         if (e)
@@ -982,3 +987,4 @@ extern "C" int grav_groups_eval_dev_CUDA(const grav_problem *dp, float *acc_phi,
 }
 
 #include "step.cuh"
+#include "adjoint.cuh"

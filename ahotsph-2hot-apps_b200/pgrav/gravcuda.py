@@ -26,6 +26,7 @@ EXPORTS = [
     "grav_groups_CUDA", "grav_direct_fp64_CUDA", "grav_plan_set_timing", "grav_plan_kernel_ms",
     "grav_groups_eval_dev_CUDA", "grav_plan_set_tree_CUDA", "grav_plan_refit_CUDA",
     "grav_plan_bodies", "grav_plan_integrate_CUDA", "grav_plan_step_CUDA",
+    "grav_plan_adjoint_CUDA",
 ]
 
 
@@ -95,6 +96,7 @@ def lib(record_errors=True):
             "grav_plan_refit_CUDA": ([vp, vp], i32), "grav_plan_bodies": ([vp], vp),
             "grav_plan_integrate_CUDA": ([vp, vp, vp, vp, vp], i32),
             "grav_plan_step_CUDA": ([vp, vp, vp, vp, vp, i32], i32),
+            "grav_plan_adjoint_CUDA": ([vp, vp, vp, vp], i32),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -198,6 +200,11 @@ class Plan:
 
     def integrate(self, vel_ptr, params_ptr, energy_ptr, stream=None):
         check(lib().grav_plan_integrate_CUDA(self._h, vel_ptr, params_ptr, energy_ptr, stream))
+
+    def adjoint(self, wu_ptr, grad_ptr, stream=None):
+        """dL/d(x, m) per body (device float4, tree order) for L = sum w.a + u phi
+        (wu: device float4 (w, u) per body, tree order)."""
+        check(lib().grav_plan_adjoint_CUDA(self._h, wu_ptr, grad_ptr, stream))
 
     def step(self, vel_ptr, params_ptr, energy_ptr, stream=None, graph=False):
         check(lib().grav_plan_step_CUDA(self._h, vel_ptr, params_ptr, energy_ptr, stream,

@@ -259,6 +259,21 @@ int grav_plan_step_CUDA(grav_plan *plan, float *vel, const double *params, doubl
                         void *stream, int use_graph);
 
 /*
+ * ---- adjoint (no counterpart in the reference) ----
+ * For a loss L = sum_i w_i . a_i + u_i phi_i on the plan's last evaluation,
+ * dL/dx and dL/dm of every body with the lists held fixed: the pair terms'
+ * tidal-tensor-vector products on the sink and source sides, the mass and
+ * quadrupole-moment adjoints of every listed cell, then the moments'
+ * chain rule to the cell's bodies (centre of mass, second moment).  wu:
+ * device float4 (wx, wy, wz, u) per body, tree order; grad: device float4
+ * (dL/dx, dL/dy, dL/dz, dL/dm) per body, tree order.  Needs the tree links
+ * (grav_plan_set_tree_CUDA); isolated problems with monopole and
+ * quadrupole lists and quad_phi_sign = +1 (no order-4 cells, no periodic
+ * images).  Enqueued on `stream`.
+ */
+int grav_plan_adjoint_CUDA(grav_plan *plan, const float *wu, float *grad, void *stream);
+
+/*
  * ---- evaluation without allocation (no counterpart in the reference) ----
  * grav_groups_eval_dev_CUDA evaluates a problem whose tables and lists are
  * already in device memory (every grav_problem pointer a device pointer,
