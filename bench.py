@@ -175,6 +175,108 @@ def cpu_reference_rate(tree, eps2, seconds=15.0, nthreads=None, seed=0, max_grou
             f"correction separately)")
 
 
+def dropin_rate(tree, eps2, max_groups=2048, seed=1, max_bytes=1 << 30):
+    """The plain FP32 drop-in path (gravcuda.h Part 1 as nln/mac.c drives it:
+    WalkInitSinkCUDA, one grav_mn_CUDA per group and list kind on the
+    reference AoSoA lists with absolute FP32 coordinates, then
+    WalkTerminateSinkCUDA) over a random sample of the same groups; wall
+    clock, Newtonian list terms: (interactions/s, seconds, sample)."""
+    from pgrav import gravcuda as gc
+    rng = np.random.default_rng(seed)
+    per_group = sum(float(tree.ptr[k][-1]) / tree.ngroups * sz * 4 for k, sz in ((0, 4), (1, 13), (2, 29)))
+    ng = int(max(16, min(max_groups, tree.ngroups, max_bytes / max(per_group, 1.0))))
+    gids = np.sort(rng.choice(tree.ngroups, ng, replace=False))
+    packs = []
+    inter = 0
+    for kind, routine, sz in ((0, "pMp", 4), (1, "pQp", 13), (2, "pHp", 29)):
+        ptr = tree.ptr[kind]
+        if ptr[-1] == 0:
+            continue
+        bp, data = tree.aosoa_subset(gids, kind)
+        packs.append((routine, sz, bp, data))
+        inter += int(((ptr[gids + 1] - ptr[gids]) * tree.groups["count"][gids]).sum())
+    bt = gc.body_table(tree.sorted_pos, tree.points[:tree.n, 3])
+    first = tree.groups["first"][gids].astype(np.int64)
+    count = tree.groups["count"][gids].astype(np.int64)
+    import torch
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    d = gc.DropIn(bt)
+    for routine, sz, bp, data in packs:
+        for s in range(ng):
+            b0, b1 = int(bp[s]), int(bp[s + 1])
+            if b1 > b0:
+                d.mn(routine, int(first[s]), int(count[s]), data[b0 * sz * 8:b1 * sz * 8],
+                     (b1 - b0) * 8, sz, eps2)
+    d.terminate()
+    el = time.perf_counter() - t0
+    return (inter / el, el, f"{ng} random sink groups ({int(count.sum())} sinks, {inter} "
+            f"interactions), one grav_mn_CUDA per group and kind (pMp/pQp/pHp)")
+
+
+def kdk_run(w, pos, m, eps2, box, tol, nsteps, dt, rebuild):
+    """configs[4]'s time-stepping leg: nsteps KDK steps (Integrate of
+    nln/integrate.c) from rest, graph-captured device steps between host
+    rebuilds; energies per step."""
+    from pgrav import step as S
+    st = S.Stepper(pos, np.zeros_like(pos), m, eps2, box=box, ewald=w["ewald"] and box > 0,
+                   rebuild=rebuild, graph=True,
+                   tree_kw=dict(leaf_max=16, group_max=32, p2cut=w["p2cut"], p4cut=w["p4cut"],
+                                tol=tol))
+    t0 = time.perf_counter()
+    st.run(nsteps, dt)
+    wall = time.perf_counter() - t0
+    h = st.history
+    st.free()
+    e = np.array([r["e"] for r in h])
+    pe = np.array([r["pe"] for r in h])
+    ms = np.array([r["ms"] for r in h])
+    steady = ms[[k for k in range(len(ms)) if k % rebuild != 0]] if len(ms) > 1 else ms
+    return {"steps": nsteps, "dt": dt, "rebuild_every": rebuild, "graph": True,
+            "device_ms_per_step_median": float(np.median(steady)),
+            "device_ms_first_step_after_rebuild_median": float(np.median(ms[::rebuild])),
+            "wall_s": wall, "energy_first": float(e[0]), "energy_last": float(e[-1]),
+            "max_abs_energy_change_over_abs_pe0": float(np.abs(e - e[0]).max() / abs(pe[0])),
+            "ke_last": float(h[-1]["ke"]), "pe_first": float(pe[0]), "pe_last": float(pe[-1])}
+
+
+def adjoint_timing(reps=5):
+    """configs[3]'s cost ratio: Plummer N = 2^20 (order 2), forward
+    evaluation against grav_plan_adjoint_CUDA on the same lists, CUDA events."""
+    import torch
+    from pgrav import gravcuda as gc, host, ics
+    n = 1 << 20
+    pos, m = ics.plummer(n, seed=123)
+    tol = 1e-5
+    t = host.Tree(pos, m, leaf_max=16, group_max=32, p2cut=7, p4cut=0, tol=tol)
+    plan = gc.Plan(t, 0.01 ** 2)
+    plan.set_tree(t)
+    rng = np.random.default_rng(0)
+    wu = torch.from_numpy(rng.normal(size=(n, 4)).astype(np.float32)).cuda()
+    grad = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    st = torch.cuda.Stream()
+    for _ in range(3):
+        plan.eval(st.cuda_stream)
+        plan.adjoint(wu.data_ptr(), grad.data_ptr(), st.cuda_stream)
+    res = {}
+    for name, fn in (("forward", lambda: plan.eval(st.cuda_stream)),
+                     ("adjoint", lambda: plan.adjoint(wu.data_ptr(), grad.data_ptr(), st.cuda_stream))):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(st)
+        for _ in range(reps):
+            fn()
+        b.record(st)
+        torch.cuda.synchronize()
+        res[name] = a.elapsed_time(b) / reps
+    c = plan.counts()
+    plan.free()
+    return {"workload": "Plummer N=2^20, order 2, eps 0.01, tol 1e-5", "n_bodies": n,
+            "interactions_per_sink": [round(float(x) / n, 1) for x in c],
+            "forward_ms": res["forward"], "adjoint_ms": res["adjoint"],
+            "adjoint_over_forward": res["adjoint"] / res["forward"]}
+
+
 def run_reference(args, w, rank, world):
     """--impl reference: the reference's CPU kernels on the host cores."""
     if rank != 0:
@@ -235,6 +337,14 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--dropin-groups", type=int, default=0,
+                    help="also time the plain FP32 drop-in path on this many sample groups")
+    ap.add_argument("--kdk-steps", type=int, default=0,
+                    help="also run this many graph-captured KDK steps (energy drift)")
+    ap.add_argument("--kdk-dt", type=float, default=0.01)
+    ap.add_argument("--kdk-rebuild", type=int, default=8)
+    ap.add_argument("--adjoint", action="store_true",
+                    help="also time the adjoint against the forward (Plummer 2^20, order 2)")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -340,6 +450,7 @@ def main():
 
     # ---- end to end through the C ABI with host buffers (pinned)
     e2e = None
+    host = out = None
     if args.e2e_steps > 0:
         host = gc.pinned_problem(tree)
         out = host.out
@@ -356,6 +467,16 @@ def main():
                "ms_per_step": e2e_s * 1e3, "steps": args.e2e_steps,
                "timing": "wall clock around grav_groups_CUDA (upload, evaluate, download)"}
 
+    dropin = None
+    if rank == 0 and args.dropin_groups > 0:
+        rate, el, sample = dropin_rate(tree, eps2, max_groups=args.dropin_groups)
+        newt_ms = kms["hexa"] + kms["quad"] + kms["point"]
+        batched = inter / (newt_ms * 1e-3)
+        dropin = {"value": rate, "unit": UNIT, "seconds": el, "sample": sample,
+                  "batched_newtonian_value": batched,
+                  "batched_over_dropin": batched / rate,
+                  "note": "batched: the three list kernels' event time (no Ewald) over all groups"}
+
     cpu = None
     if rank == 0 and args.cpu_seconds > 0:
         info = cpu_reference_rate(tree, eps2, seconds=args.cpu_seconds)
@@ -363,15 +484,33 @@ def main():
             cpu = {"value": info[0], "unit": UNIT, "cores": info[2], "kind": "reference",
                    "sample": info[3]}
 
+    cfg = config_of(args, w, tree, box)
+    kdk = None
+    if args.kdk_steps > 0:
+        # the time-stepping leg builds its own trees: release this step's
+        # host lists and pinned copies first
+        host = out = tree = None
+        import gc as pygc
+        pygc.collect()
+        kdk = kdk_run(w, pos, m, eps2, box, args.tol or w["tol"], args.kdk_steps, args.kdk_dt,
+                      args.kdk_rebuild)
+    adj = adjoint_timing() if args.adjoint and rank == 0 else None
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_max,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32 (FP64 centres, compensated sums)", "data": "synthetic (seeded)",
-                "config": config_of(args, w, tree, box), "gpu_launches": launches * args.steps,
+                "config": cfg, "gpu_launches": launches * args.steps,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
                 "accuracy": acc,
                 "host_setup_s": {"ics": t1 - t0, "tree_walk": t2 - t1, "upload": t3 - t2}}
+        if dropin:
+            line["dropin"] = dropin
+        if kdk:
+            line["kdk"] = kdk
+        if adj:
+            line["adjoint"] = adj
         print(json.dumps(line))
     if world > 1:
         dist.barrier()
