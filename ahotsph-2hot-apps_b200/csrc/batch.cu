@@ -345,6 +345,7 @@ __global__ void k_finish(DevProblem P) {
 // ------------------------------------------------------------ plan
 struct grav_step_state;  // time-step state (step.cuh)
 void step_state_free(grav_step_state *S);
+void step_graph_reset(grav_step_state *S);
 struct grav_adjoint_state;  // adjoint scratch (adjoint.cuh)
 void adjoint_state_free(grav_adjoint_state *A);
 
@@ -360,6 +361,7 @@ struct grav_plan {
     CUtensorMap tmap[3];    // row-gather views of the point, quadrupole and order-4 tables
     int timing = 0;         // record events around each kernel of an evaluation
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    std::vector<int64_t> lists_ptr[3];  // host copies of the P, Q, H list offsets (queue rebuilds)
     grav_step_state *step = nullptr;  // tree links, refit scratch and the step graph
     grav_adjoint_state *adj = nullptr;  // adjoint scratch
 };
@@ -427,6 +429,30 @@ int auto_chunk(int64_t total, int64_t ngroups, int nsm, int64_t lo) {
     int64_t c = std::max<int64_t>(lo, avg / per);
     c = (c + TILE - 1) / TILE * TILE;
     return (int)std::min<int64_t>(1 << 24, c);
+}
+
+// Work items of a plan from its kept list offsets and tuning: created group
+// by group (slot order), then sorted per kind by cost, longest first.
+int64_t make_queue(const grav_plan *pl, std::vector<Item> items[3], std::vector<int64_t> &gslot) {
+    const int64_t ng = pl->hp.ngroups;
+    const int chunk[3] = {pl->tune.chunk_p, pl->tune.chunk_q, pl->tune.chunk_h};
+    gslot.assign(ng + 1, 0);
+    int32_t slot = 0;
+    for (int64_t g = 0; g < ng; g++) {
+        for (int k = 0; k < 3; k++) {
+            if (pl->lists_ptr[k].empty())
+                continue;
+            const int64_t *ptr = pl->lists_ptr[k].data();
+            for (int64_t b = ptr[g]; b < ptr[g + 1]; b += chunk[k])
+                items[k].push_back(Item{(int32_t)g, slot++, b, std::min(ptr[g + 1], b + chunk[k])});
+        }
+        gslot[g + 1] = slot;
+    }
+    for (int k = 0; k < 3; k++)
+        std::stable_sort(items[k].begin(), items[k].end(), [](const Item &a, const Item &b) {
+            return (a.end - a.begin) > (b.end - b.begin);
+        });
+    return slot;
 }
 
 }  // namespace
@@ -508,24 +534,12 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
 
     // work items, created group by group (slot order), then sorted per kind by cost
     std::vector<Item> items[3];
-    std::vector<int64_t> gslot(ng + 1, 0);
+    std::vector<int64_t> gslot;
     const int64_t *ptrs[3] = {eptr, hp->qptr, hp->hptr};
-    const int chunk[3] = {pl->tune.chunk_p, pl->tune.chunk_q, pl->tune.chunk_h};
-    int32_t slot = 0;
-    for (int64_t g = 0; g < ng; g++) {
-        for (int k = 0; k < 3; k++) {
-            if (!ptrs[k])
-                continue;
-            for (int64_t b = ptrs[k][g]; b < ptrs[k][g + 1]; b += chunk[k])
-                items[k].push_back(Item{(int32_t)g, slot++, b, std::min(ptrs[k][g + 1], b + chunk[k])});
-        }
-        gslot[g + 1] = slot;
-    }
-    pl->nslots = slot;
     for (int k = 0; k < 3; k++)
-        std::stable_sort(items[k].begin(), items[k].end(), [](const Item &a, const Item &b) {
-            return (a.end - a.begin) > (b.end - b.begin);
-        });
+        if (ptrs[k])
+            pl->lists_ptr[k].assign(ptrs[k], ptrs[k] + ng + 1);
+    pl->nslots = make_queue(pl, items, gslot);
 
     // interaction counts (sinks x sources)
     int64_t cb = 0, cm = 0;
@@ -720,6 +734,67 @@ extern "C" int grav_groups_eval_CUDA(grav_plan *pl, void *stream) {
     GC_CHECK(cudaGetLastError());
     pl->launches++;
     return mark(4);
+}
+
+extern "C" int grav_plan_retune_CUDA(grav_plan *pl, const grav_tuning *tuning) {
+    if (!pl || !tuning)
+        return gc::set_status(-1, "grav_plan_retune_CUDA: bad arguments");
+    const int64_t ng = pl->hp.ngroups;
+    grav_tuning t = *tuning;
+    if (t.warps_per_block < 1 || t.warps_per_block > 8)
+        t.warps_per_block = 8;
+    const int64_t tot[3] = {pl->lists_ptr[0].empty() ? 0 : pl->lists_ptr[0][ng],
+                            pl->lists_ptr[1].empty() ? 0 : pl->lists_ptr[1][ng],
+                            pl->lists_ptr[2].empty() ? 0 : pl->lists_ptr[2][ng]};
+    if (t.chunk_p <= 0)
+        t.chunk_p = auto_chunk(tot[0], ng, pl->nsm, 128);
+    if (t.chunk_q <= 0)
+        t.chunk_q = auto_chunk(tot[1], ng, pl->nsm, 64);
+    if (t.chunk_h <= 0)
+        t.chunk_h = auto_chunk(tot[2], ng, pl->nsm, 32);
+    t.ewald_n = pl->tune.ewald_n;  // the correction table is not rebuilt
+    pl->tune = t;
+    std::vector<Item> items[3];
+    std::vector<int64_t> gslot;
+    pl->nslots = make_queue(pl, items, gslot);
+    // replace the queue's device buffers
+    GC_CHECK(cudaDeviceSynchronize());
+    auto drop = [&](const void *p) {
+        if (!p)
+            return;
+        auto it = std::find(pl->allocs.begin(), pl->allocs.end(), p);
+        if (it != pl->allocs.end()) {
+            cudaFree(*it);
+            pl->allocs.erase(it);
+        }
+    };
+    DevProblem &d = pl->dp;
+    for (int k = 0; k < 3; k++) drop(d.items[k]);
+    drop(d.part);
+    drop(d.gslot);
+    int rc = 0;
+    for (int k = 0; k < 3; k++) {
+        Item *it = nullptr;
+        rc |= dev_copy(pl, items[k].data(), items[k].size(), &it);
+        d.items[k] = it;
+        d.nitems[k] = (int)items[k].size();
+    }
+    float4 *part = nullptr;
+    rc |= dev_copy<float4>(pl, nullptr, (size_t)std::max<int64_t>(1, pl->nslots) * 64, &part);
+    d.part = part;
+    int64_t *gs = nullptr;
+    rc |= dev_copy(pl, gslot.data(), gslot.size(), &gs);
+    d.gslot = gs;
+    if (pl->step)
+        step_graph_reset(pl->step);  // a captured step holds the old queue
+    return rc;
+}
+
+extern "C" int grav_plan_get_tuning(const grav_plan *pl, grav_tuning *out) {
+    if (!pl || !out)
+        return gc::set_status(-1, "grav_plan_get_tuning: bad arguments");
+    *out = pl->tune;
+    return 0;
 }
 
 extern "C" int grav_plan_set_timing(grav_plan *pl, int on) {

@@ -119,6 +119,7 @@ struct nln_tree {
     std::vector<int64_t> aptr[3];
     std::vector<float> adata[3];
     int64_t counts[4] = {0, 0, 0, 0};
+    int merged = 0;  // a batch of trees (nln_tree_merge): several roots, no re-walk
 };
 
 extern "C" const char *nln_last_error(void) { return g_err.c_str(); }
@@ -739,6 +740,10 @@ static void emit_aosoa(nln_tree *t, const std::vector<GroupLists> &GL) {
 extern "C" int nln_tree_walk(nln_tree *t) {
     if (!t)
         return -1;
+    if (t->merged) {
+        g_err = "nln_tree_walk: a merged batch keeps its members' lists";
+        return -1;
+    }
     omp_set_num_threads(nthreads_of(t->p));
     const int64_t ng = (int64_t)t->groups.size();
     // Groups are walked in chunks.  Each chunk's lists are packed into one
@@ -923,6 +928,99 @@ extern "C" void nln_cell_ranges(const nln_tree *t, int64_t *first, int32_t *coun
         first[c] = t->cells[c].first;
         count[c] = t->cells[c].count;
     }
+}
+
+extern "C" nln_tree *nln_tree_merge(nln_tree *const *trees, int ntrees) {
+    if (!trees || ntrees < 1) {
+        g_err = "nln_tree_merge: no trees";
+        return nullptr;
+    }
+    int64_t nb = 0, nc = 0, ng = 0, nl[3] = {0, 0, 0};
+    std::vector<int64_t> bo(ntrees), co(ntrees), go(ntrees), lo[3];
+    for (int k = 0; k < 3; k++) lo[k].resize(ntrees);
+    for (int i = 0; i < ntrees; i++) {
+        const nln_tree *t = trees[i];
+        if (!t || t->p.box > 0 || t->lptr[0].empty() || t->merged) {
+            g_err = "nln_tree_merge: every member must be an isolated, walked tree";
+            return nullptr;
+        }
+        bo[i] = nb;
+        co[i] = nc;
+        go[i] = ng;
+        for (int k = 0; k < 3; k++) {
+            lo[k][i] = nl[k];
+            nl[k] += t->lptr[k].back();
+        }
+        nb += t->n;
+        nc += (int64_t)t->cells.size();
+        ng += (int64_t)t->groups.size();
+    }
+    if (nb + nc >= (int64_t)NLN_IDX_MASK) {
+        g_err = "nln_tree_merge: bodies plus cells exceed 27-bit list indices";
+        return nullptr;
+    }
+    nln_tree *m = new nln_tree();
+    m->p = trees[0]->p;
+    m->merged = 1;
+    m->n = nb;
+    m->order.resize(nb);
+    m->spos.resize(3 * nb);
+    m->smass.resize(nb);
+    m->cells.resize(nc);
+    m->points.resize(4 * (nb + nc));
+    m->qc.resize(nc);
+    m->hc.resize(nc);
+    m->groups.resize(ng);
+    for (int k = 0; k < 4; k++) m->lptr[k].assign(ng + 1, 0);
+    m->plist.alloc(nl[0]);
+    m->qlist.alloc(nl[1]);
+    m->hlist.alloc(nl[2]);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int i = 0; i < ntrees; i++) {
+        const nln_tree *t = trees[i];
+        const int64_t b0 = bo[i], c0 = co[i], g0 = go[i];
+        for (int64_t j = 0; j < t->n; j++) {
+            m->order[b0 + j] = b0 + t->order[j];
+            for (int d = 0; d < 3; d++) m->spos[3 * (b0 + j) + d] = t->spos[3 * j + d];
+            m->smass[b0 + j] = t->smass[j];
+            for (int d = 0; d < 4; d++) m->points[4 * (b0 + j) + d] = t->points[4 * j + d];
+        }
+        const int64_t tc = (int64_t)t->cells.size();
+        for (int64_t c = 0; c < tc; c++) {
+            Cell cc = t->cells[c];
+            cc.first += b0;
+            if (cc.child >= 0)
+                cc.child += (int32_t)c0;
+            m->cells[c0 + c] = cc;
+            for (int d = 0; d < 4; d++)
+                m->points[4 * (nb + c0 + c) + d] = t->points[4 * (t->n + c) + d];
+            m->qc[c0 + c] = t->qc[c];
+            m->hc[c0 + c] = t->hc[c];
+        }
+        for (size_t g = 0; g < t->groups.size(); g++) {
+            nln_group G = t->groups[g];
+            G.first += b0;
+            m->groups[g0 + g] = G;
+            for (int k = 0; k < 3; k++) m->lptr[k][g0 + g + 1] = lo[k][i] + t->lptr[k][g + 1];
+        }
+        const uint32_t tn = (uint32_t)t->n;
+        for (int64_t e = 0; e < t->lptr[0].back(); e++) {
+            const uint32_t v = t->plist[e], idx = v & NLN_IDX_MASK, hi = v & ~NLN_IDX_MASK;
+            const uint32_t r = idx < tn ? (uint32_t)b0 + idx : (uint32_t)(nb + c0) + (idx - tn);
+            m->plist.data()[lo[0][i] + e] = r | hi;
+        }
+        const ListBuf *src[2] = {&t->qlist, &t->hlist};
+        ListBuf *dst[2] = {&m->qlist, &m->hlist};
+        for (int k = 0; k < 2; k++)
+            for (int64_t e = 0; e < t->lptr[k + 1].back(); e++) {
+                const uint32_t v = (*src[k])[e];
+                dst[k]->data()[lo[k + 1][i] + e] = ((v & NLN_IDX_MASK) + (uint32_t)c0) |
+                                                    (v & ~NLN_IDX_MASK);
+            }
+    }
+    for (int i = 0; i < ntrees; i++)
+        for (int k = 0; k < 4; k++) m->counts[k] += trees[i]->counts[k];
+    return m;
 }
 
 extern "C" void nln_cell_links(const nln_tree *t, int32_t *child, int32_t *nchild,

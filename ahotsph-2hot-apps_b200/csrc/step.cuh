@@ -345,6 +345,15 @@ int step_enqueue(grav_plan *pl, float *vel, const double *params, double *energy
 
 void step_state_free(grav_step_state *S) { delete S; }
 
+void step_graph_reset(grav_step_state *S) {
+    if (S->exec)
+        cudaGraphExecDestroy(S->exec);
+    if (S->graph)
+        cudaGraphDestroy(S->graph);
+    S->exec = nullptr;
+    S->graph = nullptr;
+}
+
 extern "C" int grav_plan_set_tree_CUDA(grav_plan *pl, const int64_t *cell_first,
                                        const int32_t *cell_count, const int32_t *cell_child,
                                        const int32_t *cell_nchild, const int32_t *cell_level) {

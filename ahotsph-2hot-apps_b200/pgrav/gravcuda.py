@@ -26,7 +26,7 @@ EXPORTS = [
     "grav_groups_CUDA", "grav_direct_fp64_CUDA", "grav_plan_set_timing", "grav_plan_kernel_ms",
     "grav_groups_eval_dev_CUDA", "grav_plan_set_tree_CUDA", "grav_plan_refit_CUDA",
     "grav_plan_bodies", "grav_plan_integrate_CUDA", "grav_plan_step_CUDA",
-    "grav_plan_adjoint_CUDA",
+    "grav_plan_adjoint_CUDA", "grav_plan_retune_CUDA", "grav_plan_get_tuning",
 ]
 
 
@@ -97,6 +97,7 @@ def lib(record_errors=True):
             "grav_plan_integrate_CUDA": ([vp, vp, vp, vp, vp], i32),
             "grav_plan_step_CUDA": ([vp, vp, vp, vp, vp, i32], i32),
             "grav_plan_adjoint_CUDA": ([vp, vp, vp, vp], i32),
+            "grav_plan_retune_CUDA": ([vp, vp], i32), "grav_plan_get_tuning": ([vp, vp], i32),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -200,6 +201,16 @@ class Plan:
 
     def integrate(self, vel_ptr, params_ptr, energy_ptr, stream=None):
         check(lib().grav_plan_integrate_CUDA(self._h, vel_ptr, params_ptr, energy_ptr, stream))
+
+    def retune(self, tuning):
+        """New tile shapes (a Tuning or a tuple of its fields); rebuilds the queue only."""
+        tun = Tuning(*tuning) if not isinstance(tuning, Tuning) else tuning
+        check(lib().grav_plan_retune_CUDA(self._h, ctypes.byref(tun)))
+
+    def tuning(self):
+        t = Tuning()
+        check(lib().grav_plan_get_tuning(self._h, ctypes.byref(t)))
+        return t
 
     def adjoint(self, wu_ptr, grad_ptr, stream=None):
         """dL/d(x, m) per body (device float4, tree order) for L = sum w.a + u phi

@@ -64,6 +64,8 @@ def lib():
         L.nln_cell_ranges.argtypes = [vp, vp, vp]
         L.nln_cell_links.argtypes = [vp, vp, vp, vp]
         L.nln_tree_refit.argtypes = [vp, vp]
+        L.nln_tree_merge.argtypes = [vp, ctypes.c_int]
+        L.nln_tree_merge.restype = vp
         L.nln_tree_refit.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -120,6 +122,12 @@ class Tree:
                              ctypes.byref(self.params))
         if not h:
             raise ValueError(L.nln_last_error().decode())
+        self._attach(h, box)
+        if walk:
+            self.walk()
+
+    def _attach(self, h, box):
+        L = lib()
         self._h = h
         self._owner = _Handle(h)
         self.n = L.nln_nbodies(h)
@@ -132,13 +140,33 @@ class Tree:
         self.hcells = _view(L.nln_hcells(h), HCELL_DTYPE, self.ncells, self._owner)
         self.ngroups = L.nln_ngroups(h)
         self.groups = _view(L.nln_groups(h), GROUP_DTYPE, self.ngroups, self._owner)
-        if walk:
-            self.walk()
+
+    @classmethod
+    def merge(cls, trees):
+        """A batch of independent isolated trees as one (nln_tree_merge): the
+        members' bodies one after another, then their cells; lists renumbered
+        so each still refers only to its own member."""
+        L = lib()
+        hs = (ctypes.c_void_p * len(trees))(*[t._h for t in trees])
+        h = L.nln_tree_merge(hs, len(trees))
+        if not h:
+            raise ValueError(L.nln_last_error().decode())
+        self = cls.__new__(cls)
+        self.params = trees[0].params
+        self._merged = True
+        self._attach(h, 0.0)
+        self._views()
+        self.body_offsets = np.concatenate([[0], np.cumsum([t.n for t in trees])])
+        return self
 
     def walk(self):
         L = lib()
         if L.nln_tree_walk(self._h) != 0:
             raise RuntimeError("walk failed")
+        self._views()
+
+    def _views(self):
+        L = lib()
         ng = self.ngroups
         self.ptr = [_view(L.nln_list_ptr(self._h, k), np.int64, ng + 1, self._owner) for k in range(4)]
         self.plist = _view(L.nln_list_data(self._h, 0), np.uint32, L.nln_list_len(self._h, 0), self._owner)
@@ -150,7 +178,7 @@ class Tree:
         L.nln_counts(self._h, c)
         self.counts = np.array(list(c), dtype=np.int64)
         self.aosoa = None
-        if self.params.emit_aosoa:
+        if self.params.emit_aosoa and not getattr(self, "_merged", False):
             self.aosoa = []
             for k, sz in enumerate((4, 13, 29)):
                 ptr = _view(L.nln_aosoa_ptr(self._h, k), np.int64, ng + 1, self._owner)

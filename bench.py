@@ -48,6 +48,10 @@ WORKLOADS = {
     # Plummer sphere N = 65536, order 2
     "plummer64k": dict(kind="plummer", n=65536, eps=0.01, p2cut=7, p4cut=0, ewald=False,
                        tol=2e-5, sample=8192),
+    # 1024 independent isolated systems, N log-uniform in [512, 65536],
+    # half Plummer half Hernquist (a = 1), eps = 0.01 a, order 4, one launch per kind
+    "batch1024": dict(kind="batch", nsys=1024, nmin=512, nmax=65536, eps=0.01, p2cut=7,
+                      p4cut=20, ewald=False, tol=1e-5, sample=2048),
 }
 
 
@@ -57,6 +61,14 @@ def log(*a):
 
 def make_problem(w, seed=123):
     from pgrav import ics
+    if w["kind"] == "batch":
+        rng = np.random.default_rng(seed)
+        ns = np.floor(np.exp(rng.uniform(np.log(w["nmin"]), np.log(w["nmax"]), w["nsys"])))
+        systems = []
+        for k, n in enumerate(ns.astype(int)):
+            gen = ics.plummer if k % 2 == 0 else ics.hernquist
+            systems.append(gen(int(n), seed=seed + 1 + k))
+        return systems, None, w["eps"] ** 2, 0.0
     if w["kind"] == "box":
         pos, m = ics.grf_box(w["n1d"], seed=seed, slope=-2.5, rms_disp=w["rms_disp"])
         eps = 1.0 / w["n1d"] / 50.0
@@ -67,6 +79,16 @@ def make_problem(w, seed=123):
 
 def build_tree(w, pos, m, box, tol, nthreads=0):
     from pgrav import host
+    if w["kind"] == "batch":
+        # members built in parallel (one host thread each), then merged
+        from concurrent.futures import ThreadPoolExecutor
+        kw = dict(leaf_max=16, group_max=32, p2cut=w["p2cut"], p4cut=w["p4cut"], tol=tol,
+                  nthreads=1)
+        with ThreadPoolExecutor(max_workers=os.cpu_count()) as ex:
+            members = list(ex.map(lambda s: host.Tree(s[0], s[1], **kw), pos))
+        t = host.Tree.merge(members)
+        del members
+        return t
     return host.Tree(pos, m, leaf_max=16, group_max=32, p2cut=w["p2cut"], p4cut=w["p4cut"],
                      tol=tol, box=box, nthreads=nthreads)
 
@@ -318,6 +340,7 @@ def tree_input_bytes(tree):
 
 def config_of(args, w, tree, box):
     c = {"workload": args.workload, "n_bodies": int(tree.n), "groups": int(tree.ngroups),
+         **({"systems": int(len(tree.body_offsets) - 1)} if hasattr(tree, "body_offsets") else {}),
          "mac_tol": args.tol or w["tol"], "order": 4 if w["p4cut"] else 2,
          "periodic": bool(box > 0), "ewald": bool(w["ewald"]),
          "interactions_per_sink": [round(float(x) / tree.n, 1) for x in tree.counts],
@@ -343,6 +366,8 @@ def main():
                     help="also run this many graph-captured KDK steps (energy drift)")
     ap.add_argument("--kdk-dt", type=float, default=0.01)
     ap.add_argument("--kdk-rebuild", type=int, default=8)
+    ap.add_argument("--autotune", action="store_true",
+                    help="pick the tile shapes with the autotuner first (always for batch1024)")
     ap.add_argument("--adjoint", action="store_true",
                     help="also time the adjoint against the forward (Plummer 2^20, order 2)")
     args = ap.parse_args()
@@ -373,6 +398,18 @@ def main():
     t3 = time.perf_counter()
     log(f"[bench] ics {t1 - t0:.1f}s tree+walk {t2 - t1:.1f}s upload {t3 - t2:.1f}s "
         f"groups {tree.ngroups} counts/sink {np.round(tree.counts / tree.n, 1)}")
+    tuning = None
+    if args.autotune or w["kind"] == "batch":
+        from pgrav import autotune as AT
+        ta = time.perf_counter()
+        best, trials = AT.autotune(plan)
+        tuning = {"chosen": {"warps_per_block": best.warps_per_block,
+                             "blocks_per_sm": best.blocks_per_sm,
+                             "chunks": [best.chunk_p, best.chunk_q, best.chunk_h]},
+                  "trials": len(trials), "search_s": time.perf_counter() - ta,
+                  "best_ms": min(t["ms"] for t in trials),
+                  "auto_ms": trials[0]["ms"]}
+        plan.set_timing(True)
     stream = torch.cuda.Stream()
     for _ in range(max(3, args.warmup)):
         plan.eval(stream.cuda_stream)
@@ -433,19 +470,54 @@ def main():
     if not args.no_accuracy and rank == 0:
         out = plan.download()
         rng = np.random.default_rng(7)
-        samp = np.sort(rng.choice(tree.n, min(w["sample"], tree.n), replace=False))
-        ref = gc.direct_fp64(tree.points[:tree.n], samp, eps2, box=box)
-        e = np.linalg.norm(out[samp, :3] - ref[:, :3], axis=1) / np.linalg.norm(ref[:, :3], axis=1)
+        if w["kind"] == "batch":
+            # each system's own FP64 direct sum, on sinks of 8 random systems
+            offs = tree.body_offsets
+            pick = rng.choice(len(offs) - 1, 8, replace=False)
+            got, refs = [], []
+            for sidx in pick:
+                lo, hi = int(offs[sidx]), int(offs[sidx + 1])
+                ss = np.sort(rng.choice(hi - lo, min(hi - lo, w["sample"] // 8), replace=False))
+                refs.append(gc.direct_fp64(tree.points[lo:hi], ss, eps2))
+                got.append(out[lo + ss])
+            ref = np.concatenate(refs)
+            gotv = np.concatenate(got)
+            samp = None
+        else:
+            samp = np.sort(rng.choice(tree.n, min(w["sample"], tree.n), replace=False))
+            ref = gc.direct_fp64(tree.points[:tree.n], samp, eps2, box=box)
+            gotv = out[samp]
+        e = np.linalg.norm(gotv[:, :3] - ref[:, :3], axis=1) / np.linalg.norm(ref[:, :3], axis=1)
         # potential: rms error over rms potential (a periodic potential can pass through zero)
-        pe = np.sqrt(np.mean((out[samp, 3] - ref[:, 3]) ** 2) / np.mean(ref[:, 3] ** 2))
+        pe = np.sqrt(np.mean((gotv[:, 3] - ref[:, 3]) ** 2) / np.mean(ref[:, 3] ** 2))
         acc = {"rms_rel_force_err": float(np.sqrt(np.mean(e * e))),
                "max_rel_force_err": float(e.max()),
                "p99_rel_force_err": float(np.quantile(e, 0.99)),
                "rms_phi_err_over_rms_phi": float(pe),
-               "sinks": int(len(samp)),
+               "sinks": int(len(ref)),
                "target_rms": 1e-4, "meets_target": bool(np.sqrt(np.mean(e * e)) <= 1e-4),
                "oracle": "FP64 direct sum" + (" with Ewald images" if box > 0 else "")}
     launches = plan.launches()
+    batch_kdk = None
+    if w["kind"] == "batch" and rank == 0:
+        # the graph-captured KDK step of the batch (evaluate, integrate, refit)
+        plan.set_tree(tree)
+        vel = torch.zeros((tree.n, 4), dtype=torch.float32, device="cuda")
+        prm = torch.tensor([1e-3, 5e-4, 0.0], dtype=torch.float64, device="cuda")
+        en = torch.zeros(2, dtype=torch.float64, device="cuda")
+        with torch.cuda.stream(stream):
+            plan.step(vel.data_ptr(), prm.data_ptr(), en.data_ptr(), stream.cuda_stream, graph=True)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(args.steps):
+                plan.step(vel.data_ptr(), prm.data_ptr(), en.data_ptr(), stream.cuda_stream,
+                          graph=True)
+            b.record(stream)
+        torch.cuda.synchronize()
+        batch_kdk = {"graph_step_ms": a.elapsed_time(b) / args.steps, "steps": args.steps,
+                     "step": "evaluate + integrate + refit, one CUDA graph launch",
+                     "systems": int(len(tree.body_offsets) - 1)}
     plan.free()   # the end-to-end leg uploads its own copy
 
     # ---- end to end through the C ABI with host buffers (pinned)
@@ -507,6 +579,10 @@ def main():
                 "host_setup_s": {"ics": t1 - t0, "tree_walk": t2 - t1, "upload": t3 - t2}}
         if dropin:
             line["dropin"] = dropin
+        if tuning:
+            line["tuning"] = tuning
+        if batch_kdk:
+            line["batch_kdk"] = batch_kdk
         if kdk:
             line["kdk"] = kdk
         if adj:

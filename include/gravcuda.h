@@ -199,6 +199,15 @@ float *grav_plan_output(grav_plan *plan);
 void grav_plan_counts(const grav_plan *plan, int64_t out[4]);
 /* Kernel launches per evaluation. */
 int grav_plan_launches(const grav_plan *plan);
+/*
+ * Rebuild a plan's work queue for new tile shapes (warps per block, blocks
+ * per SM, list chunks; a chunk <= 0 is chosen automatically) without
+ * re-uploading its tables: the autotuner's step.  Synchronises the device;
+ * a captured step graph is dropped and recaptured on its next call.
+ * grav_plan_get_tuning returns the shapes in use (automatic chunks resolved).
+ */
+int grav_plan_retune_CUDA(grav_plan *plan, const grav_tuning *tuning);
+int grav_plan_get_tuning(const grav_plan *plan, grav_tuning *out);
 /* Record CUDA events around each kernel of every evaluation (on its stream). */
 int grav_plan_set_timing(grav_plan *plan, int on);
 /* Milliseconds of the last evaluation's kernels: order-4, quadrupole, point, finish (synchronising). */

@@ -113,6 +113,20 @@ int64_t nln_aosoa_subset(const nln_tree *t, const int64_t *gids, int64_t ngsel, 
 void nln_cell_ranges(const nln_tree *t, int64_t *first, int32_t *count);
 
 /*
+ * A batch of independent systems as one tree-like object: the members'
+ * bodies one after another (member i's at the sum of the earlier members'
+ * counts, in each member's tree order), then all their cells; groups,
+ * lists, cell links and interaction counts are renumbered so that every
+ * list still refers only to its own member.  Members must be isolated and
+ * walked; they are not modified and may be freed afterwards.  Every
+ * accessor works on the result (nln_order maps into the concatenation of
+ * the members' original bodies); nln_tree_walk refuses it.  Free with
+ * nln_tree_free.  NULL (see nln_last_error) on bad members or when bodies
+ * plus cells exceed 27-bit list indices.
+ */
+nln_tree *nln_tree_merge(nln_tree *const *trees, int ntrees);
+
+/*
  * Tree links of every cell: first child (-1 for a leaf), number of children
  * (children are consecutive cells) and depth (root 0).  Children always
  * follow their parent in the cell array.

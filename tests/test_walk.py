@@ -59,3 +59,38 @@ def test_correction_list_covers_bodies_once_in_newtonian_image():
         assert np.array_equal(img_n, img_c)
         # coarse cells make the correction list shorter than the Newtonian lists
         assert t.ptr[3][g + 1] - t.ptr[3][g] <= sum(t.ptr[k][g + 1] - t.ptr[k][g] for k in range(3))
+
+
+def test_merge_renumbers_members():
+    from pgrav import host, ics
+    trees = []
+    for k, n in enumerate((700, 1500, 333)):
+        pos, m = (ics.plummer if k % 2 == 0 else ics.hernquist)(n, seed=40 + k)
+        trees.append(host.Tree(pos, m, tol=1e-3, p2cut=7, p4cut=20))
+    b = host.Tree.merge(trees)
+    assert b.n == sum(t.n for t in trees) and b.ncells == sum(t.ncells for t in trees)
+    assert b.ngroups == sum(t.ngroups for t in trees)
+    assert list(b.body_offsets) == [0, 700, 2200, 2533]
+    assert (b.counts == sum(t.counts for t in trees)).all()
+    bo = co = go = 0
+    for t in trees:
+        assert np.array_equal(b.points[bo:bo + t.n], t.points[:t.n])
+        assert np.array_equal(b.points[b.n + co:b.n + co + t.ncells], t.points[t.n:])
+        assert np.array_equal(b.order[bo:bo + t.n], bo + t.order)
+        assert np.array_equal(b.groups["first"][go:go + t.ngroups], bo + t.groups["first"])
+        for g in range(t.ngroups):
+            e = t.plist[t.ptr[0][g]:t.ptr[0][g + 1]] & ((1 << 27) - 1)
+            want = np.where(e < t.n, bo + e, b.n + co + (e - t.n))
+            got = b.plist[b.ptr[0][go + g]:b.ptr[0][go + g + 1]] & ((1 << 27) - 1)
+            assert np.array_equal(got, want)
+            for k, lst, blst in ((1, t.qlist, b.qlist), (2, t.hlist, b.hlist)):
+                e = lst[t.ptr[k][g]:t.ptr[k][g + 1]] & ((1 << 27) - 1)
+                got = blst[b.ptr[k][go + g]:b.ptr[k][go + g + 1]] & ((1 << 27) - 1)
+                assert np.array_equal(got, co + e)
+        ch, nc, lv = t.cell_links()
+        bch, bnc, blv = b.cell_links()
+        assert np.array_equal(bch[co:co + t.ncells], np.where(ch >= 0, ch + co, -1))
+        assert np.array_equal(blv[co:co + t.ncells], lv)
+        bo += t.n
+        co += t.ncells
+        go += t.ngroups
