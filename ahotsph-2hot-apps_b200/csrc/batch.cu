@@ -264,6 +264,97 @@ __global__ void __launch_bounds__(256) k_batch(const __grid_constant__ CUtensorM
     }
 }
 
+// Point records (bodies and cell monopoles, 16 B each) are staged without
+// TMA: every lane loads its own record with a plain read-only load, one tile
+// ahead of use (the list entry two tiles ahead), re-centres it in registers
+// and writes it to the warp's shared tile; the row-gather path costs more
+// than it saves for records this small.
+__global__ void __launch_bounds__(256) k_points(DevProblem P) {
+    __shared__ __align__(16) float4 stile[8][TILE];
+    const int lane = threadIdx.x & 31;
+    float4 *tile = stile[threadIdx.x >> 5];
+    const uint32_t *list = P.list[KP];
+    const uint32_t ntab = (uint32_t)P.ntab[KP];
+    const bool periodic = P.box > 0;
+    while (true) {
+        int it = 0;
+        if (lane == 0)
+            it = atomicAdd(&P.counters[KP], 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= P.nitems[KP])
+            break;
+        const Item item = P.items[KP][it];
+        const nln_group G = P.groups[item.group];
+        const double c[3] = {G.cen[0], G.cen[1], G.cen[2]};
+        float ux = 0.f, uy = 0.f, uz = 0.f;
+        if (lane < G.count) {
+            float4 sk = P.points[G.first + lane];
+            ux = (float)((double)sk.x - c[0]);
+            uy = (float)((double)sk.y - c[1]);
+            uz = (float)((double)sk.z - c[2]);
+        }
+        float hi[4] = {0.f, 0.f, 0.f, 0.f}, lo[4] = {0.f, 0.f, 0.f, 0.f};
+        const int64_t nent = item.end - item.begin;
+        const int ntile = (int)((nent + TILE - 1) / TILE);
+        constexpr uint32_t kNone = 0xffffffffu;  // no entry in this lane
+        auto entry = [&](int t) -> uint32_t {
+            const int64_t k = item.begin + (int64_t)t * TILE + lane;
+            return (t < ntile && k < item.end) ? __ldg(list + k) : kNone;
+        };
+        auto record = [&](uint32_t e) -> float4 {
+            if (e == kNone)
+                return make_float4(0.f, 0.f, 0.f, 0.f);
+            uint32_t idx = e & NLN_IDX_MASK;
+            if (idx >= ntab) {  // never expected: the host validated every entry
+                atomicOr(P.err, GC_DEV_BAD_INDEX);
+                idx = 0;
+            }
+            return __ldg(P.points + idx);
+        };
+        uint32_t e_cur = entry(0);
+        float4 r_cur = record(e_cur);
+        uint32_t e_nxt = entry(1);
+        for (int t = 0; t < ntile; t++) {
+            const float4 r_nxt = record(e_nxt);  // consumed next tile
+            const uint32_t e_nn = entry(t + 2);
+            const int nt = (int)min((int64_t)TILE, nent - (int64_t)t * TILE);
+            float4 st = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (e_cur != kNone) {
+                double sx = 0.0, sy = 0.0, sz = 0.0;
+                if (periodic)
+                    decode_shift(e_cur >> NLN_IDX_BITS, P.box, sx, sy, sz);
+                st = make_float4((float)((double)r_cur.x + sx - c[0]),
+                                 (float)((double)r_cur.y + sy - c[1]),
+                                 (float)((double)r_cur.z + sz - c[2]), r_cur.w);
+            }
+            __syncwarp();  // the previous tile is no longer read
+            tile[lane] = st;
+            __syncwarp();
+            Acc4 a{0.f, 0.f, 0.f, 0.f};
+            if (nt == TILE) {
+#pragma unroll 8
+                for (int r = 0; r < TILE; r++)
+                    interact<0, SOFT_PLUMMER>(reinterpret_cast<const float *>(tile + r), ux, uy,
+                                              uz, P.eps2, P.qsh, a);
+            } else {
+                for (int r = 0; r < nt; r++)
+                    interact<0, SOFT_PLUMMER>(reinterpret_cast<const float *>(tile + r), ux, uy,
+                                              uz, P.eps2, P.qsh, a);
+            }
+            comp_add(hi[0], lo[0], a.ax);
+            comp_add(hi[1], lo[1], a.ay);
+            comp_add(hi[2], lo[2], a.az);
+            comp_add(hi[3], lo[3], a.phi);
+            e_cur = e_nxt;
+            r_cur = r_nxt;
+            e_nxt = e_nn;
+        }
+        float4 *dst = P.part + ((size_t)item.slot * 32 + lane) * 2;
+        dst[0] = make_float4(hi[0], hi[1], hi[2], hi[3]);
+        dst[1] = make_float4(lo[0], lo[1], lo[2], lo[3]);
+    }
+}
+
 // Periodic correction moments of group g (ewald.cuh) over its correction
 // list, lanes striding it.  Bodies count as masses; a cell adds its
 // traceless second to fourth moments (the list's cells include coarse
@@ -689,6 +780,17 @@ int launch_kind(grav_plan *pl, cudaStream_t st) {
     if (pl->dp.nitems[KIND] == 0)
         return 0;
     const int wpb = pl->tune.warps_per_block;
+    if (KIND == KP) {
+        int fit = 0;
+        GC_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_points, 256, 0));
+        int per_sm = pl->tune.blocks_per_sm > 0 ? std::min(pl->tune.blocks_per_sm, fit) : fit;
+        int blocks = std::max(1, per_sm) * pl->nsm;
+        blocks = std::min(blocks, (pl->dp.nitems[KP] + 7) / 8);
+        k_points<<<blocks, 256, 0, st>>>(pl->dp);
+        GC_CHECK(cudaGetLastError());
+        pl->launches++;
+        return 0;
+    }
     const size_t smem = (size_t)wpb * KindOf<KIND>::warp_bytes;
     GC_CHECK(cudaFuncSetAttribute(k_batch<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem));

@@ -81,6 +81,7 @@ class Stepper:
             self._pull()
             self.plan.free()
             self.plan = None
+            self.tree = None  # release the old lists before the new walk
         if self.box > 0:
             self.pos = np.mod(self.pos, np.float32(self.box)).astype(np.float32)
             self.pos[self.pos >= self.box] = 0.0

@@ -560,10 +560,13 @@ def main():
     kdk = None
     if args.kdk_steps > 0:
         # the time-stepping leg builds its own trees: release this step's
-        # host lists and pinned copies first
+        # host lists and pinned copies (and torch's cache of pinned blocks) first
         host = out = tree = None
         import gc as pygc
         pygc.collect()
+        empty_host = getattr(torch._C, "_host_emptyCache", None)
+        if empty_host:
+            empty_host()
         kdk = kdk_run(w, pos, m, eps2, box, args.tol or w["tol"], args.kdk_steps, args.kdk_dt,
                       args.kdk_rebuild)
     adj = adjoint_timing() if args.adjoint and rank == 0 else None
