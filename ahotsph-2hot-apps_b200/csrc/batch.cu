@@ -100,9 +100,12 @@ __device__ __forceinline__ void decode_shift(uint32_t code, double box, double &
     sz = ((int)(code % 3) - 1) * box;
 }
 
-// Convert this lane's raw record (just landed by TMA) in place into the
-// staged form of interact.cuh, re-centred on the group centre c.
-template <int KIND>
+// Convert this lane's record (just landed by TMA) in place into the staged
+// form of interact.cuh, re-centred on the group centre c.  STAGED: the cell
+// tables are pre-staged (k_stage_cells) and only the 16-byte header (FP64
+// centre -> FP32 offset, mass) is rewritten; otherwise the raw nln_qcell /
+// nln_hcell record is scaled here.
+template <int KIND, bool STAGED>
 __device__ __forceinline__ void convert(unsigned char *slot, uint32_t code, const double *c,
                                         double box) {
     double sx, sy, sz;
@@ -114,6 +117,12 @@ __device__ __forceinline__ void convert(unsigned char *slot, uint32_t code, cons
         o[1] = (float)((double)p.y + sy - c[1]);
         o[2] = (float)((double)p.z + sz - c[2]);
         o[3] = p.w;
+    } else if (STAGED) {
+        const double *d = reinterpret_cast<const double *>(slot);
+        const double cx = d[0], cy = d[1], cz = d[5];
+        const float m = o[KIND == KQ ? 12 : 31];
+        *reinterpret_cast<float4 *>(slot) =
+            make_float4((float)(cx + sx - c[0]), (float)(cy + sy - c[1]), (float)(cz + sz - c[2]), m);
     } else if (KIND == KQ) {
         const nln_qcell q = *reinterpret_cast<const nln_qcell *>(slot);
         o[0] = (float)(q.cen[0] + sx - c[0]);
@@ -133,7 +142,47 @@ __device__ __forceinline__ void convert(unsigned char *slot, uint32_t code, cons
     }
 }
 
-template <int KIND>
+// Pre-staged cell tables: the staged moments of interact.cuh at their
+// offsets, with the FP64 centre and the mass in the slots the inner loops
+// never read (centre x, y in floats 0-3 and z in floats 10-11; mass in
+// float 12 (quadrupole, 16 floats) or 31 (order 4, 32 floats)), so that a
+// tile's convert only rewrites the header.
+__global__ void k_stage_cells(const nln_qcell *__restrict__ qc, const nln_hcell *__restrict__ hc,
+                              int64_t n, float4 *__restrict__ qs, float4 *__restrict__ hs) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n)
+        return;
+    if (qs) {
+        const nln_qcell q = qc[c];
+        float o[16];
+#pragma unroll
+        for (int k = 0; k < 16; k++) o[k] = 0.f;
+        const float q2[5] = {q.qxx, q.qxy, q.qyy, q.qxz, q.qyz};
+        stage_quad(o, q.R, q2);
+        memcpy(&o[0], &q.cen[0], 8);
+        memcpy(&o[2], &q.cen[1], 8);
+        memcpy(&o[10], &q.cen[2], 8);
+        o[12] = q.mass;
+#pragma unroll
+        for (int k = 0; k < 4; k++) qs[c * 4 + k] = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+    }
+    if (hs) {
+        const nln_hcell h = hc[c];
+        float o[32];
+#pragma unroll
+        for (int k = 0; k < 32; k++) o[k] = 0.f;
+        stage_quad(o, h.R, h.q2);
+        stage_hexa(o, h.R, h.q3, h.q4);
+        memcpy(&o[0], &h.cen[0], 8);
+        memcpy(&o[2], &h.cen[1], 8);
+        memcpy(&o[10], &h.cen[2], 8);
+        o[31] = h.mass;
+#pragma unroll
+        for (int k = 0; k < 8; k++) hs[c * 8 + k] = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+    }
+}
+
+template <int KIND, bool STAGED>
 __global__ void __launch_bounds__(256) k_batch(const __grid_constant__ CUtensorMap tmap,
                                                DevProblem P) {
     using K = KindOf<KIND>;
@@ -236,7 +285,7 @@ __global__ void __launch_bounds__(256) k_batch(const __grid_constant__ CUtensorM
             }
             unsigned char *bt = wbuf + st * K::stage_bytes;
             if (lane < nt)
-                convert<KIND>(bt + K::rec_off(lane), codes[st * TILE + lane], c, P.box);
+                convert<KIND, STAGED>(bt + K::rec_off(lane), codes[st * TILE + lane], c, P.box);
             __syncwarp();
             Acc4 a{0.f, 0.f, 0.f, 0.f};
             if (nt == TILE) {
@@ -453,6 +502,8 @@ struct grav_plan {
     int timing = 0;         // record events around each kernel of an evaluation
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     std::vector<int64_t> lists_ptr[3];  // host copies of the P, Q, H list offsets (queue rebuilds)
+    bool staged = false;                // the Q/H tensor maps view pre-staged tables
+    float4 *qstage = nullptr, *hstage = nullptr;  // pre-staged cell tables (k_stage_cells)
     grav_step_state *step = nullptr;  // tree links, refit scratch and the step graph
     grav_adjoint_state *adj = nullptr;  // adjoint scratch
 };
@@ -749,11 +800,26 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
     }
     cudaMemset(err, 0, sizeof(unsigned));
     memset(pl->tmap, 0, sizeof(pl->tmap));
+    // pre-staged copies of the cell tables the Q and H lists gather from
+    if (d.qcells && hp->qptr && hp->qptr[ng])
+        rc |= dev_copy<float4>(pl, nullptr, (size_t)hp->ncells * 4, &pl->qstage);
+    if (d.hcells && hp->hptr && hp->hptr[ng])
+        rc |= dev_copy<float4>(pl, nullptr, (size_t)hp->ncells * 8, &pl->hstage);
+    if (!rc && (pl->qstage || pl->hstage)) {
+        k_stage_cells<<<(unsigned)((hp->ncells + 127) / 128), 128>>>(d.qcells, d.hcells, hp->ncells,
+                                                                       pl->qstage, pl->hstage);
+        const cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) {
+            grav_plan_free(pl);
+            return gc::cuda_status(e, "grav_groups_upload_CUDA: staging the cell tables");
+        }
+        pl->staged = true;
+    }
     rc |= encode_rows(&pl->tmap[KP], d.points, (uint64_t)np, 16);
-    if (d.qcells)
-        rc |= encode_rows(&pl->tmap[KQ], d.qcells, (uint64_t)hp->ncells, sizeof(nln_qcell));
-    if (d.hcells)
-        rc |= encode_rows(&pl->tmap[KH], d.hcells, (uint64_t)hp->ncells, sizeof(nln_hcell));
+    if (pl->qstage)
+        rc |= encode_rows(&pl->tmap[KQ], pl->qstage, (uint64_t)hp->ncells, sizeof(nln_qcell));
+    if (pl->hstage)
+        rc |= encode_rows(&pl->tmap[KH], pl->hstage, (uint64_t)hp->ncells, sizeof(nln_hcell));
     if (rc) {
         grav_plan_free(pl);
         return rc;
@@ -792,14 +858,14 @@ int launch_kind(grav_plan *pl, cudaStream_t st) {
         return 0;
     }
     const size_t smem = (size_t)wpb * KindOf<KIND>::warp_bytes;
-    GC_CHECK(cudaFuncSetAttribute(k_batch<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
+    auto kern = pl->staged ? k_batch<KIND, true> : k_batch<KIND, false>;
+    GC_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int fit = 0;
-    GC_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_batch<KIND>, wpb * 32, smem));
+    GC_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, kern, wpb * 32, smem));
     int per_sm = pl->tune.blocks_per_sm > 0 ? std::min(pl->tune.blocks_per_sm, fit) : fit;
     int blocks = std::max(1, per_sm) * pl->nsm;
     blocks = std::min(blocks, (pl->dp.nitems[KIND] + wpb - 1) / wpb);
-    k_batch<KIND><<<blocks, wpb * 32, smem, st>>>(pl->tmap[KIND], pl->dp);
+    kern<<<blocks, wpb * 32, smem, st>>>(pl->tmap[KIND], pl->dp);
     GC_CHECK(cudaGetLastError());
     pl->launches++;
     return 0;
@@ -1010,11 +1076,11 @@ int dev_scratch_base(void **out) {
         cudaError_t e = cudaGetSymbolAddress(&p, g_dev_scratch);
         if (e != cudaSuccess || !p)
             return gc::cuda_status(e, "grav_groups_eval_dev_CUDA: cudaGetSymbolAddress of the scratch");
-        GC_CHECK(cudaFuncSetAttribute(k_batch<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        GC_CHECK(cudaFuncSetAttribute(k_batch<KP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       8 * KindOf<KP>::warp_bytes));
-        GC_CHECK(cudaFuncSetAttribute(k_batch<KQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        GC_CHECK(cudaFuncSetAttribute(k_batch<KQ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       8 * KindOf<KQ>::warp_bytes));
-        GC_CHECK(cudaFuncSetAttribute(k_batch<KH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        GC_CHECK(cudaFuncSetAttribute(k_batch<KH, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       8 * KindOf<KH>::warp_bytes));
         base[dev] = p;
     }

@@ -317,6 +317,9 @@ int refit_enqueue(grav_plan *pl, cudaStream_t st) {
     k_refit_tables<<<(unsigned)((S->ncells + 127) / 128), 128, 0, st>>>(
         S->raw, S->ncells, pl->hp.nbodies, const_cast<float4 *>(pl->dp.points),
         const_cast<nln_qcell *>(pl->dp.qcells), const_cast<nln_hcell *>(pl->dp.hcells));
+    if (pl->qstage || pl->hstage)
+        k_stage_cells<<<(unsigned)((S->ncells + 127) / 128), 128, 0, st>>>(
+            pl->dp.qcells, pl->dp.hcells, S->ncells, pl->qstage, pl->hstage);
     GC_CHECK(cudaGetLastError());
     return 0;
 }
