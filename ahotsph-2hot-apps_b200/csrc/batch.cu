@@ -897,7 +897,9 @@ extern "C" int grav_groups_eval_CUDA(grav_plan *pl, void *stream) {
         return rc;
     if (int rc = mark(3))
         return rc;
-    const int wpb = 8;
+    // two warps per block: at ~160 registers a thread, small blocks let more
+    // warps stay resident, which this latency-bound kernel needs
+    const int wpb = 2;
     k_finish<<<(unsigned)((pl->dp.ngroups + wpb - 1) / wpb), wpb * 32, 0, st>>>(pl->dp);
     GC_CHECK(cudaGetLastError());
     pl->launches++;
