@@ -36,6 +36,10 @@ UNIT = "interactions/s"
 # (reference count 26-27, nln/grav.c:56-75), 66 quadrupole
 # (nln/do_grav_avx8.c:378), 217 order 4 (nln/do_grav_avx8.c:45)
 FLOPS = np.array([23, 23, 66, 217], np.float64)
+# DRAM bytes (read + write) per interaction of each list kernel, from the ncu
+# capture of the 128^3 case (profiles/k_batch_box128_full.md); a launch's
+# traffic is this times its interactions (traffic grows with list entries)
+DRAM_BYTES_PER_INTERACTION = {"hexa": 0.2007, "quad": 0.192, "point": 0.167}
 
 WORKLOADS = {
     # N = 2^24 periodic box, order 4 + Ewald (the metric's N)
@@ -458,7 +462,11 @@ def main():
     total_tflops = float((counts * FLOPS).sum() / (ms * 1e-3) / 1e12)
     roofline = {"bound": "fp32", "kernel": f"k_batch<{dom}>", "achieved": achieved,
                 "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                "traffic": None,
+                "traffic": float(DRAM_BYTES_PER_INTERACTION[dom] * (
+                    counts[3] if dom == "hexa" else counts[2] if dom == "quad" else counts[0] + counts[1])),
+                "traffic_note": "bytes per launch: ncu dram bytes per interaction of the 128^3 "
+                                "capture (profiles/k_batch_box128_full.md) times this launch's "
+                                "interactions",
                 "peak_source": (f"148 SMs x 128 FP32 lanes x 2 x {sm_mhz:.0f} MHz "
                                 f"(sm_max_mhz of {peak_src} MEASURED_PEAKS.json; it holds no "
                                 f"FP32 CUDA-core figure)"),
