@@ -317,14 +317,21 @@ __global__ void __launch_bounds__(256) k_batch(const __grid_constant__ CUtensorM
 // TMA: every lane loads its own record with a plain read-only load, one tile
 // ahead of use (the list entry two tiles ahead), re-centres it in registers
 // and writes it to the warp's shared tile; the row-gather path costs more
-// than it saves for records this small.
+// than it saves for records this small.  The tile is laid out in record
+// pairs, field by field (pair j: npx0 npx1 npy0 npy1 | npz0 npz1 m0 m1, with
+// np the negated offset), so that each 16-byte shared read yields two ready
+// operand pairs for the paired FP32 instructions of mono2_plummer.
 __global__ void __launch_bounds__(256) k_points(DevProblem P) {
-    __shared__ __align__(16) float4 stile[8][TILE];
+    __shared__ __align__(16) float stile[8][TILE * 4];
     const int lane = threadIdx.x & 31;
-    float4 *tile = stile[threadIdx.x >> 5];
+    float *tile = stile[threadIdx.x >> 5];
+    const float4 *tile4 = reinterpret_cast<const float4 *>(tile);
+    // this lane's record slot in the pair layout
+    float *mine = tile + (lane >> 1) * 8 + (lane & 1);
     const uint32_t *list = P.list[KP];
     const uint32_t ntab = (uint32_t)P.ntab[KP];
     const bool periodic = P.box > 0;
+    const float2 e2 = make_float2(P.eps2, P.eps2);
     while (true) {
         int it = 0;
         if (lane == 0)
@@ -342,6 +349,7 @@ __global__ void __launch_bounds__(256) k_points(DevProblem P) {
             uy = (float)((double)sk.y - c[1]);
             uz = (float)((double)sk.z - c[2]);
         }
+        const float2 sx = make_float2(ux, ux), sy = make_float2(uy, uy), sz = make_float2(uz, uz);
         float hi[4] = {0.f, 0.f, 0.f, 0.f}, lo[4] = {0.f, 0.f, 0.f, 0.f};
         const int64_t nent = item.end - item.begin;
         const int ntile = (int)((nent + TILE - 1) / TILE);
@@ -367,33 +375,43 @@ __global__ void __launch_bounds__(256) k_points(DevProblem P) {
             const float4 r_nxt = record(e_nxt);  // consumed next tile
             const uint32_t e_nn = entry(t + 2);
             const int nt = (int)min((int64_t)TILE, nent - (int64_t)t * TILE);
-            float4 st = make_float4(0.f, 0.f, 0.f, 0.f);
+            // an absent record: massless and far from every sink
+            float npx = -1.0e3f, npy = -1.0e3f, npz = -1.0e3f, m = 0.f;
             if (e_cur != kNone) {
-                double sx = 0.0, sy = 0.0, sz = 0.0;
+                double sxs = 0.0, sys = 0.0, szs = 0.0;
                 if (periodic)
-                    decode_shift(e_cur >> NLN_IDX_BITS, P.box, sx, sy, sz);
-                st = make_float4((float)((double)r_cur.x + sx - c[0]),
-                                 (float)((double)r_cur.y + sy - c[1]),
-                                 (float)((double)r_cur.z + sz - c[2]), r_cur.w);
+                    decode_shift(e_cur >> NLN_IDX_BITS, P.box, sxs, sys, szs);
+                npx = (float)(c[0] - ((double)r_cur.x + sxs));
+                npy = (float)(c[1] - ((double)r_cur.y + sys));
+                npz = (float)(c[2] - ((double)r_cur.z + szs));
+                m = r_cur.w;
             }
             __syncwarp();  // the previous tile is no longer read
-            tile[lane] = st;
+            mine[0] = npx;
+            mine[2] = npy;
+            mine[4] = npz;
+            mine[6] = m;
             __syncwarp();
-            Acc4 a{0.f, 0.f, 0.f, 0.f};
+            Acc2 a2{make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f),
+                    make_float2(0.f, 0.f)};
             if (nt == TILE) {
 #pragma unroll 8
-                for (int r = 0; r < TILE; r++)
-                    interact<0, SOFT_PLUMMER>(reinterpret_cast<const float *>(tile + r), ux, uy,
-                                              uz, P.eps2, P.qsh, a);
+                for (int j = 0; j < TILE / 2; j++) {
+                    const float4 A = tile4[2 * j], B = tile4[2 * j + 1];
+                    mono2_plummer(make_float2(A.x, A.y), make_float2(A.z, A.w),
+                                  make_float2(B.x, B.y), make_float2(B.z, B.w), sx, sy, sz, e2, a2);
+                }
             } else {
-                for (int r = 0; r < nt; r++)
-                    interact<0, SOFT_PLUMMER>(reinterpret_cast<const float *>(tile + r), ux, uy,
-                                              uz, P.eps2, P.qsh, a);
+                for (int j = 0; j < (nt + 1) / 2; j++) {
+                    const float4 A = tile4[2 * j], B = tile4[2 * j + 1];
+                    mono2_plummer(make_float2(A.x, A.y), make_float2(A.z, A.w),
+                                  make_float2(B.x, B.y), make_float2(B.z, B.w), sx, sy, sz, e2, a2);
+                }
             }
-            comp_add(hi[0], lo[0], a.ax);
-            comp_add(hi[1], lo[1], a.ay);
-            comp_add(hi[2], lo[2], a.az);
-            comp_add(hi[3], lo[3], a.phi);
+            comp_add(hi[0], lo[0], -(a2.nax.x + a2.nax.y));
+            comp_add(hi[1], lo[1], -(a2.nay.x + a2.nay.y));
+            comp_add(hi[2], lo[2], -(a2.naz.x + a2.naz.y));
+            comp_add(hi[3], lo[3], -(a2.nphi.x + a2.nphi.y));
             e_cur = e_nxt;
             r_cur = r_nxt;
             e_nxt = e_nn;

@@ -204,3 +204,28 @@ __device__ __forceinline__ void interact(const float *__restrict__ r, float sx, 
             hexa(x, y, z, r, ri2, ri5, a);
     }
 }
+
+// Two point records against one sink with Blackwell's paired FP32
+// instructions (fma/add/mul .f32x2): the .x halves belong to one record,
+// the .y halves to the other.  The records are staged as negated offsets,
+// np = -(source - group centre), so d = s + np needs no negation; the
+// accumulators hold +m/r and +d m/r^3 (the caller negates once per tile).
+// Same Plummer arithmetic as mono<SOFT_PLUMMER>, element by element.
+struct Acc2 {
+    float2 nax, nay, naz, nphi;
+};
+
+__device__ __forceinline__ void mono2_plummer(float2 npx, float2 npy, float2 npz, float2 m,
+                                              float2 sx, float2 sy, float2 sz, float2 e2,
+                                              Acc2 &acc) {
+    const float2 dx = __fadd2_rn(sx, npx), dy = __fadd2_rn(sy, npy), dz = __fadd2_rn(sz, npz);
+    const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, e2)));
+    const float2 ri = make_float2(rsqrt_fast(r2.x), rsqrt_fast(r2.y));
+    const float2 ri2 = __fmul2_rn(ri, ri);
+    const float2 mri = __fmul2_rn(m, ri);
+    const float2 mri3 = __fmul2_rn(mri, ri2);
+    acc.nphi = __fadd2_rn(acc.nphi, mri);
+    acc.nax = __ffma2_rn(dx, mri3, acc.nax);
+    acc.nay = __ffma2_rn(dy, mri3, acc.nay);
+    acc.naz = __ffma2_rn(dz, mri3, acc.naz);
+}
