@@ -142,6 +142,53 @@ __device__ __forceinline__ void convert(unsigned char *slot, uint32_t code, cons
     }
 }
 
+// Device-side check of an uploaded list, one warp per work item (or per
+// group for the correction list): every entry's index inside its table and
+// its image code in 0..26.  For the point list it also counts body and cell
+// entries, weighted by the group's sinks.  acc: [0] error flag, [1] body
+// interactions, [2] monopole-cell interactions.
+__global__ void k_check_lists(const uint32_t *__restrict__ list, const Item *__restrict__ items,
+                              int nitems, const int64_t *__restrict__ gptr, int64_t ngroups,
+                              const nln_group *__restrict__ groups, uint32_t ntab, uint32_t nb,
+                              int count_bodies, unsigned long long *acc) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nwork = items ? nitems : ngroups;
+    for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nwork;
+         w += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        int64_t b, e;
+        int32_t g;
+        if (items) {
+            const Item it = items[w];
+            b = it.begin;
+            e = it.end;
+            g = it.group;
+        } else {
+            b = gptr[w];
+            e = gptr[w + 1];
+            g = (int32_t)w;
+        }
+        unsigned bad = 0;
+        long long nbody = 0;
+        for (int64_t k = b + lane; k < e; k += 32) {
+            const uint32_t v = list[k];
+            const uint32_t idx = v & NLN_IDX_MASK;
+            bad |= (idx >= ntab || (v >> NLN_IDX_BITS) > 26u) ? 1u : 0u;
+            nbody += idx < nb ? 1 : 0;
+        }
+        bad = __reduce_or_sync(0xffffffffu, bad);
+        for (int d = 16; d > 0; d >>= 1) nbody += __shfl_xor_sync(0xffffffffu, nbody, d);
+        if (lane == 0) {
+            if (bad)
+                atomicOr(&acc[0], 1ull);
+            if (count_bodies) {
+                const long long c = groups[g].count;
+                atomicAdd(&acc[1], (unsigned long long)(nbody * c));
+                atomicAdd(&acc[2], (unsigned long long)((e - b - nbody) * c));
+            }
+        }
+    }
+}
+
 // Pre-staged cell tables: the staged moments of interact.cuh at their
 // offsets, with the FP64 centre and the mass in the slots the inner loops
 // never read (centre x, y in floats 0-3 and z in floats 10-11; mass in
@@ -241,14 +288,15 @@ __global__ void __launch_bounds__(256) k_batch(const __grid_constant__ CUtensorM
             const int nt = (int)min((int64_t)TILE, nent - (int64_t)t * TILE);
             const int ng4 = (nt + 3) >> 2;
             const uint32_t st = seq % NST;
-            uint32_t idx = ent & NLN_IDX_MASK;
-            if (lane < nt && idx >= ntab) {  // never expected: the host validated every entry
+            uint32_t idx = ent & NLN_IDX_MASK, code = ent >> NLN_IDX_BITS;
+            if (lane < nt && (idx >= ntab || code > 26u)) {  // never expected: checked at upload
                 atomicOr(P.err, GC_DEV_BAD_INDEX);
                 idx = 0;
+                code = NLN_SHIFT_NONE;
             }
             if (lane >= nt)
                 idx = 0;
-            codes[st * TILE + lane] = ent >> NLN_IDX_BITS;
+            codes[st * TILE + lane] = code;
             if (lane == 0)
                 mbar_arrive_expect_tx(&bar[st], (uint32_t)(ng4 * 4 * RB));
             unsigned char *dst = wbuf + st * K::stage_bytes;
@@ -358,13 +406,14 @@ __global__ void __launch_bounds__(256) k_points(DevProblem P) {
             const int64_t k = item.begin + (int64_t)t * TILE + lane;
             return (t < ntile && k < item.end) ? __ldg(list + k) : kNone;
         };
-        auto record = [&](uint32_t e) -> float4 {
+        auto record = [&](uint32_t &e) -> float4 {
             if (e == kNone)
                 return make_float4(0.f, 0.f, 0.f, 0.f);
             uint32_t idx = e & NLN_IDX_MASK;
-            if (idx >= ntab) {  // never expected: the host validated every entry
+            if (idx >= ntab || (e >> NLN_IDX_BITS) > 26u) {  // never expected: checked at upload
                 atomicOr(P.err, GC_DEV_BAD_INDEX);
                 idx = 0;
+                e = NLN_SHIFT_NONE << NLN_IDX_BITS;
             }
             return __ldg(P.points + idx);
         };
@@ -436,6 +485,10 @@ __device__ __forceinline__ void ewald_moments(const DevProblem &P, int64_t g, co
     for (int64_t k = P.cptr[g] + lane; k < P.cptr[g + 1]; k += 32) {
         const uint32_t ent = P.clist[k];
         const uint32_t idx = ent & NLN_IDX_MASK;
+        if (idx >= (uint32_t)P.ntab[0] || (ent >> NLN_IDX_BITS) > 26u) {  // never expected
+            atomicOr(P.err, GC_DEV_BAD_INDEX);
+            continue;
+        }
         double sx, sy, sz;
         decode_shift(ent >> NLN_IDX_BITS, P.box, sx, sy, sz);
         if (idx < nb) {
@@ -615,6 +668,17 @@ int64_t make_queue(const grav_plan *pl, std::vector<Item> items[3], std::vector<
     return slot;
 }
 
+// The device address of page-locked host memory (lists read in place over
+// PCIe), or null when `p` is not page-locked host memory.
+const uint32_t *mapped_host(const uint32_t *p) {
+    cudaPointerAttributes a{};
+    if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? static_cast<const uint32_t *>(a.devicePointer) : nullptr;
+}
+
 }  // namespace
 
 extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning *tuning,
@@ -647,22 +711,12 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
         return gc::set_status(-1, "a group has 0 or more than 32 sinks, lies outside the bodies, "
                                   "or has decreasing list offsets");
     }
-    auto check_list = [&](const int64_t *ptr, const uint32_t *lst, int64_t ntab) -> bool {
-        if (!ptr)
-            return true;
-        int bad = 0;
-#pragma omp parallel for schedule(static) reduction(| : bad)
-        for (int64_t k = 0; k < ptr[ng]; k++)
-            if ((int64_t)(lst[k] & NLN_IDX_MASK) >= ntab || (lst[k] >> NLN_IDX_BITS) > 26)
-                bad |= 1;
-        return !bad;
-    };
+    // Every list entry is checked on the device after the upload (k_check_lists):
+    // a host pass over tens of gigabytes of lists would dominate an end-to-end call.
     const int64_t *eptr = hp->pptr;
-    if (!check_list(hp->pptr, hp->plist, np) || !check_list(hp->qptr, hp->qlist, hp->ncells) ||
-        !check_list(hp->hptr, hp->hlist, hp->ncells) ||
-        (hp->qptr && hp->qptr[ng] && !hp->qcells) || (hp->hptr && hp->hptr[ng] && !hp->hcells)) {
+    if ((hp->qptr && hp->qptr[ng] && !hp->qcells) || (hp->hptr && hp->hptr[ng] && !hp->hcells)) {
         delete pl;
-        return gc::set_status(-1, "cell list entry outside the cell table");
+        return gc::set_status(-1, "a cell list without its cell table");
     }
     const bool want_ewald = hp->box > 0 && hp->ewald;
     if (want_ewald) {
@@ -676,10 +730,9 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
         for (int64_t g = 0; g < ng; g++)
             if (hp->cptr[g + 1] < hp->cptr[g])
                 bad |= 1;
-        if (bad || hp->cptr[0] != 0 || !check_list(hp->cptr, hp->clist, np)) {
+        if (bad || hp->cptr[0] != 0) {
             delete pl;
-            return gc::set_status(-1, "bad correction list (decreasing offsets or entry outside "
-                                      "the point table)");
+            return gc::set_status(-1, "bad correction list offsets");
         }
     }
 
@@ -701,20 +754,8 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
             pl->lists_ptr[k].assign(ptrs[k], ptrs[k] + ng + 1);
     pl->nslots = make_queue(pl, items, gslot);
 
-    // interaction counts (sinks x sources)
-    int64_t cb = 0, cm = 0;
-#pragma omp parallel for schedule(static) reduction(+ : cb, cm)
-    for (int64_t g = 0; g < ng; g++) {
-        const int64_t c = hp->groups[g].count;
-        for (int64_t k = hp->pptr[g]; k < hp->pptr[g + 1]; k++) {
-            if ((hp->plist[k] & NLN_IDX_MASK) < (uint32_t)nb)
-                cb += c;
-            else
-                cm += c;
-        }
-    }
-    pl->counts[0] = cb;
-    pl->counts[1] = cm;
+    // interaction counts (sinks x sources); the point list's split into
+    // bodies and cell monopoles is counted on the device (k_check_lists)
     for (int64_t g = 0; g < ng; g++) {
         const int64_t c = hp->groups[g].count;
         if (hp->qptr)
@@ -740,11 +781,26 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
     rc |= dev_copy(pl, hp->groups, (size_t)ng, &gr);
     d.groups = gr;
     uint32_t *l0 = nullptr, *l1 = nullptr, *l2 = nullptr;
-    rc |= dev_copy(pl, hp->plist, (size_t)hp->pptr[ng], &l0);
-    if (hp->qptr)
-        rc |= dev_copy(pl, hp->qlist, (size_t)hp->qptr[ng], &l1);
-    if (hp->hptr)
-        rc |= dev_copy(pl, hp->hlist, (size_t)hp->hptr[ng], &l2);
+    if (hp->lists_in_host) {
+        // the kernels read the lists in place from page-locked host memory
+        const uint32_t *m0 = mapped_host(hp->plist);
+        const uint32_t *m1 = hp->qptr ? mapped_host(hp->qlist) : nullptr;
+        const uint32_t *m2 = hp->hptr ? mapped_host(hp->hlist) : nullptr;
+        if (!m0 || (hp->qptr && !m1) || (hp->hptr && !m2)) {
+            grav_plan_free(pl);
+            return gc::set_status(-1, "grav_groups_upload_CUDA: lists_in_host needs the lists in "
+                                      "page-locked host memory (cudaHostAlloc)");
+        }
+        l0 = const_cast<uint32_t *>(m0);
+        l1 = const_cast<uint32_t *>(m1);
+        l2 = const_cast<uint32_t *>(m2);
+    } else {
+        rc |= dev_copy(pl, hp->plist, (size_t)hp->pptr[ng], &l0);
+        if (hp->qptr)
+            rc |= dev_copy(pl, hp->qlist, (size_t)hp->qptr[ng], &l1);
+        if (hp->hptr)
+            rc |= dev_copy(pl, hp->hlist, (size_t)hp->hptr[ng], &l2);
+    }
     d.list[0] = l0;
     d.list[1] = l1;
     d.list[2] = l2;
@@ -771,7 +827,16 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
         int64_t *cp = nullptr;
         uint32_t *cl = nullptr;
         rc |= dev_copy(pl, hp->cptr, (size_t)ng + 1, &cp);
-        rc |= dev_copy(pl, hp->clist, (size_t)std::max<int64_t>(1, hp->cptr[ng]), &cl);
+        if (hp->lists_in_host) {
+            cl = const_cast<uint32_t *>(mapped_host(hp->clist));
+            if (!cl) {
+                grav_plan_free(pl);
+                return gc::set_status(-1, "grav_groups_upload_CUDA: lists_in_host needs the "
+                                          "correction list in page-locked host memory");
+            }
+        } else {
+            rc |= dev_copy(pl, hp->clist, (size_t)std::max<int64_t>(1, hp->cptr[ng]), &cl);
+        }
         d.cptr = cp;
         d.clist = cl;
     }
@@ -817,6 +882,45 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
         return rc;
     }
     cudaMemset(err, 0, sizeof(unsigned));
+    if (hp->lists_in_host) {
+        // entries are checked by the kernels as they read them (bad ones set
+        // the error word); the point list's body/cell split is not counted
+        int64_t tot = 0;
+        for (int64_t g = 0; g < ng; g++) tot += (int64_t)hp->groups[g].count * (hp->pptr[g + 1] - hp->pptr[g]);
+        pl->counts[0] = tot;
+        pl->counts[1] = 0;
+    } else {
+        // check every list entry on the device and count the point list's split
+        unsigned long long *acc = nullptr;
+        rc |= dev_copy<unsigned long long>(pl, nullptr, 3, &acc);
+        if (rc) {
+            grav_plan_free(pl);
+            return rc;
+        }
+        cudaMemset(acc, 0, 3 * sizeof(unsigned long long));
+        const unsigned blocks = (unsigned)pl->nsm * 8;
+        const uint32_t ntabs[3] = {(uint32_t)np, (uint32_t)hp->ncells, (uint32_t)hp->ncells};
+        for (int k = 0; k < 3; k++)
+            if (d.nitems[k] > 0)
+                k_check_lists<<<blocks, 256>>>(d.list[k], d.items[k], d.nitems[k], nullptr, 0,
+                                                d.groups, ntabs[k], (uint32_t)nb, k == KP, acc);
+        if (d.cptr)
+            k_check_lists<<<blocks, 256>>>(d.clist, nullptr, 0, d.cptr, ng, d.groups, (uint32_t)np,
+                                            (uint32_t)nb, 0, acc);
+        unsigned long long h[3] = {0, 0, 0};
+        const cudaError_t e = cudaMemcpy(h, acc, sizeof(h), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) {
+            grav_plan_free(pl);
+            return gc::cuda_status(e, "grav_groups_upload_CUDA: list check");
+        }
+        if (h[0]) {
+            grav_plan_free(pl);
+            return gc::set_status(-1, "a list entry lies outside its table or has an image code "
+                                      "beyond 26");
+        }
+        pl->counts[0] = (int64_t)h[1];
+        pl->counts[1] = (int64_t)h[2];
+    }
     memset(pl->tmap, 0, sizeof(pl->tmap));
     // pre-staged copies of the cell tables the Q and H lists gather from
     if (d.qcells && hp->qptr && hp->qptr[ng])

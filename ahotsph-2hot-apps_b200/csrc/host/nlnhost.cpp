@@ -303,11 +303,12 @@ static void compute_moments(nln_tree *t) {
     }
 }
 
-// AREL critical radii, nln/cofm.c:276-565 (ptol = tol: stol_max and
-// ptol_boost at their defaults).  A relative tolerance of 0 switches that
+// AREL critical radii, nln/cofm.c:276-565 (stol_max at its default;
+// ptol = tol / (1 + ptol_boost bmax / bmax0), bmax0 half the root cube).  A relative tolerance of 0 switches that
 // criterion off (the reference would divide by zero, cofm.c:322-335).
 static void compute_rcrit(nln_tree *t) {
-    const double ptol = t->p.tol, rel = t->p.rel_tol, rel0 = t->p.rel_tol0;
+    const double rel = t->p.rel_tol, rel0 = t->p.rel_tol0;
+    const double boost = t->p.ptol_boost, bmax0 = 0.5 * t->side;  // mac->bmax0 = r0, cofm.c:66
     const int p2 = t->p.p2cut, p4 = t->p.p4cut;
     const int64_t nc = (int64_t)t->cells.size();
 #pragma omp parallel for schedule(dynamic, 256)
@@ -317,6 +318,8 @@ static void compute_rcrit(nln_tree *t) {
         if (c.B2 <= 0.0 || c.mass <= 0.0 || c.bmax <= 0.0)
             continue;  // coincident bodies: every expansion is exact
         const double b = c.bmax, m = c.mass, B2 = c.B2;
+        // larger cells get a tighter tolerance with ptol_boost (cofm.c:302)
+        const double ptol = t->p.tol / (1.0 + (boost > 0 && bmax0 > 0 ? boost * b / bmax0 : 0.0));
         const double B3 = B2 * std::sqrt(B2 / m);  // lower bound, cofm.c:314
         double a[10];
         // monopole

@@ -47,7 +47,8 @@ class Problem(ctypes.Structure):
                 ("plist", ctypes.c_void_p), ("qlist", ctypes.c_void_p),
                 ("hlist", ctypes.c_void_p), ("eps2", ctypes.c_double), ("box", ctypes.c_double),
                 ("quad_phi_sign", ctypes.c_float), ("ewald", ctypes.c_int),
-                ("cptr", ctypes.c_void_p), ("clist", ctypes.c_void_p)]
+                ("cptr", ctypes.c_void_p), ("clist", ctypes.c_void_p),
+                ("lists_in_host", ctypes.c_int)]
 
 
 class Tuning(ctypes.Structure):
@@ -342,7 +343,7 @@ class PinnedProblem:
     """A tree's tables and lists copied into page-locked host memory, as the
     host side of an end-to-end grav_groups_CUDA call reads them."""
 
-    def __init__(self, tree):
+    def __init__(self, tree, lists_in_host=False):
         import torch
         self._keep = []
         self.h2d_bytes = 0
@@ -375,14 +376,15 @@ class PinnedProblem:
             p.cptr = pin(t.ptr[3]).ctypes.data
             p.clist = pin(t.clist if len(t.clist) else np.zeros(1, np.uint32)).ctypes.data
         p.quad_phi_sign = 1.0
+        p.lists_in_host = int(bool(lists_in_host))
         self.problem = p
         buf = torch.empty(t.n * 16, dtype=torch.uint8, pin_memory=True)
         self._keep.append(buf)
         self.out = buf.numpy().view(np.float32).reshape(t.n, 4)
 
 
-def pinned_problem(tree):
-    return PinnedProblem(tree)
+def pinned_problem(tree, lists_in_host=False):
+    return PinnedProblem(tree, lists_in_host)
 
 
 def groups_eval_problem(pp, eps2, box, ewald=False):

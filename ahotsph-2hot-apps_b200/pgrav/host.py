@@ -28,7 +28,7 @@ class Params(ctypes.Structure):
                 ("tol", ctypes.c_double), ("rel_tol", ctypes.c_double),
                 ("rel_tol0", ctypes.c_double), ("box", ctypes.c_double),
                 ("nthreads", ctypes.c_int), ("emit_aosoa", ctypes.c_int),
-                ("ewald_theta", ctypes.c_double)]
+                ("ewald_theta", ctypes.c_double), ("ptol_boost", ctypes.c_double)]
 
 
 def lib():
@@ -112,11 +112,11 @@ class Tree:
 
     def __init__(self, pos, mass, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-3,
                  rel_tol=0.0, rel_tol0=0.0, box=0.0, nthreads=0, emit_aosoa=False, walk=True,
-                 ewald_theta=0.2):
+                 ewald_theta=0.2, ptol_boost=0.0):
         pos = np.ascontiguousarray(pos, dtype=np.float32).reshape(-1, 3)
         mass = np.ascontiguousarray(np.broadcast_to(np.asarray(mass, np.float32), (len(pos),)))
         self.params = Params(leaf_max, group_max, p2cut, p4cut, tol, rel_tol, rel_tol0, box,
-                             nthreads, int(bool(emit_aosoa)), ewald_theta)
+                             nthreads, int(bool(emit_aosoa)), ewald_theta, ptol_boost)
         L = lib()
         h = L.nln_tree_build(pos.ctypes.data, 3, mass.ctypes.data, 1, len(pos),
                              ctypes.byref(self.params))

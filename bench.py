@@ -362,6 +362,8 @@ def main():
     ap.add_argument("--workload", default="box256", choices=list(WORKLOADS))
     ap.add_argument("--tol", type=float, default=0.0)
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-copy-lists", action="store_true",
+                    help="end-to-end leg: copy the lists at upload instead of reading them in place")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--dropin-groups", type=int, default=0,
@@ -532,7 +534,7 @@ def main():
     e2e = None
     host = out = None
     if args.e2e_steps > 0:
-        host = gc.pinned_problem(tree)
+        host = gc.pinned_problem(tree, lists_in_host=not args.e2e_copy_lists)
         out = host.out
         torch.cuda.synchronize()
         walls = []
@@ -545,7 +547,10 @@ def main():
         e2e = {"value": inter * world / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(host.h2d_bytes), "d2h_bytes_per_step": int(out.nbytes),
                "ms_per_step": e2e_s * 1e3, "steps": args.e2e_steps,
-               "timing": "wall clock around grav_groups_CUDA (upload, evaluate, download)"}
+               "timing": "wall clock around grav_groups_CUDA (upload, evaluate, download)",
+               "lists": ("copied to the device at upload" if args.e2e_copy_lists else
+                         "read by the kernels in place from page-locked host memory over PCIe "
+                         "(every step; tables copied at upload)")}
 
     dropin = None
     if rank == 0 and args.dropin_groups > 0:

@@ -168,6 +168,13 @@ typedef struct grav_problem {
     const int64_t *cptr;        /* ewald: ngroups + 1 offsets of the correction list */
     const uint32_t *clist;      /* ewald: point-table records | image << 27; cells enter as
                                    nbodies + cell index and take the order-4 table's moments */
+    int lists_in_host;          /* 1: the lists are page-locked host memory (cudaHostAlloc) that
+                                   the kernels read in place over PCIe, overlapping the transfer
+                                   with the evaluation; their entries are then checked as they
+                                   are read (a bad one sets the device error word) and the
+                                   point list's interactions are counted as bodies.  The plan
+                                   reads them at every evaluation: keep them alive and unchanged
+                                   until grav_plan_free.  0: copied to the device at upload. */
 } grav_problem;
 
 typedef struct grav_plan grav_plan;

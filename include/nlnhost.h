@@ -42,6 +42,8 @@ typedef struct nln_params {
                            once bmax + group radius <= ewald_theta x its distance to the
                            nearest other lattice image of the group centre (0: the correction
                            list repeats the Newtonian entries) */
+    double ptol_boost;  /* ptol_boost: cell tolerance tol / (1 + ptol_boost bmax / bmax0),
+                           bmax0 half the root cube (nln/cofm.c:302; 0: off) */
 } nln_params;
 
 typedef struct nln_tree nln_tree;

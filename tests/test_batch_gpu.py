@@ -92,3 +92,38 @@ def test_batched_repeatable(gc):
     plan.eval()
     b = plan.download()
     assert np.array_equal(a, b)  # deterministic: fixed per-group summation order
+
+
+def test_upload_refuses_bad_entries(gc):
+    """Every list entry is checked on the device at upload: an index past its
+    table, or an image code past 26, fails the upload with a status."""
+    t = make_tree("plummer", 5000, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-4)
+    for kind, bad in ((0, t.n + t.ncells + 5), (2, t.ncells + 1), (0, 5 | (27 << 27))):
+        lst = {0: t.plist, 1: t.qlist, 2: t.hlist}[kind]
+        keep = int(lst[3])
+        lst[3] = bad
+        try:
+            with pytest.raises(gc.GravError, match="outside its table|image code"):
+                gc.Plan(t, 1e-4)
+        finally:
+            lst[3] = keep
+    p = gc.Plan(t, 1e-4)   # intact lists still upload
+    p.free()
+
+
+def test_lists_read_in_place_from_host_memory(gc):
+    """lists_in_host: the kernels read page-locked lists over PCIe; the
+    results are those of the copied lists, bit for bit."""
+    t = make_tree("box", 24 ** 3, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-4)
+    eps2 = (1.0 / 24 / 50) ** 2
+    outs = []
+    for in_host in (False, True):
+        pp = gc.pinned_problem(t, lists_in_host=in_host)
+        outs.append(gc.groups_eval_problem(pp, eps2, 1.0, ewald=True).copy())
+    assert np.array_equal(outs[0], outs[1])
+    # pageable lists are refused in that mode
+    prob = gc.pinned_problem(t, lists_in_host=True).problem
+    prob.plist = t.plist.ctypes.data
+    with pytest.raises(gc.GravError, match="page-locked"):
+        gc.check(gc.lib().grav_groups_CUDA(__import__("ctypes").byref(prob),
+                                           np.empty((t.n, 4), np.float32).ctypes.data))
