@@ -25,6 +25,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <mutex>
 #include <numeric>
 #include <vector>
@@ -60,7 +61,8 @@ struct DevProblem {
     float4 *part;              // nslots x 32 lanes x 2 (hi, lo)
     const int64_t *gslot;      // ngroups + 1: slots of group g
     float4 *out;               // nbodies
-    int64_t ngroups;
+    int64_t ngroups;           // k_finish covers groups gbegin .. ngroups-1
+    int64_t gbegin;
     int64_t ncells;
     float eps2;
     float qsh;
@@ -289,7 +291,8 @@ __global__ void __launch_bounds__(256) k_batch(const __grid_constant__ CUtensorM
             const int ng4 = (nt + 3) >> 2;
             const uint32_t st = seq % NST;
             uint32_t idx = ent & NLN_IDX_MASK, code = ent >> NLN_IDX_BITS;
-            if (lane < nt && (idx >= ntab || code > 26u)) {  // never expected: checked at upload
+            // entries are checked at upload, except in the pipelined end-to-end call
+            if (lane < nt && (idx >= ntab || code > 26u)) {
                 atomicOr(P.err, GC_DEV_BAD_INDEX);
                 idx = 0;
                 code = NLN_SHIFT_NONE;
@@ -410,7 +413,8 @@ __global__ void __launch_bounds__(256) k_points(DevProblem P) {
             if (e == kNone)
                 return make_float4(0.f, 0.f, 0.f, 0.f);
             uint32_t idx = e & NLN_IDX_MASK;
-            if (idx >= ntab || (e >> NLN_IDX_BITS) > 26u) {  // never expected: checked at upload
+            // entries are checked at upload, except in the pipelined end-to-end call
+            if (idx >= ntab || (e >> NLN_IDX_BITS) > 26u) {
                 atomicOr(P.err, GC_DEV_BAD_INDEX);
                 idx = 0;
                 e = NLN_SHIFT_NONE << NLN_IDX_BITS;
@@ -485,7 +489,7 @@ __device__ __forceinline__ void ewald_moments(const DevProblem &P, int64_t g, co
     for (int64_t k = P.cptr[g] + lane; k < P.cptr[g + 1]; k += 32) {
         const uint32_t ent = P.clist[k];
         const uint32_t idx = ent & NLN_IDX_MASK;
-        if (idx >= (uint32_t)P.ntab[0] || (ent >> NLN_IDX_BITS) > 26u) {  // never expected
+        if (idx >= (uint32_t)P.ntab[0] || (ent >> NLN_IDX_BITS) > 26u) {  // as in k_batch
             atomicOr(P.err, GC_DEV_BAD_INDEX);
             continue;
         }
@@ -518,7 +522,7 @@ __device__ __forceinline__ void ewald_moments(const DevProblem &P, int64_t g, co
 // Per group, in slot order: sum the partials of its work items in FP64,
 // add the periodic correction, and write (ax, ay, az, phi) of each sink.
 __global__ void k_finish(DevProblem P) {
-    const int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int64_t g = P.gbegin + (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (g >= P.ngroups)
         return;
@@ -577,6 +581,12 @@ struct grav_plan {
     float4 *qstage = nullptr, *hstage = nullptr;  // pre-staged cell tables (k_stage_cells)
     grav_step_state *step = nullptr;  // tree links, refit scratch and the step graph
     grav_adjoint_state *adj = nullptr;  // adjoint scratch
+    // Group ranges of the work queue: items are sorted by cost within each
+    // range, and chunk_item[k][c] is the first item of kind k in range c.
+    // One range [0, ngroups) except in the pipelined end-to-end call.
+    std::vector<int64_t> chunk_group;
+    std::vector<int> chunk_item[3];
+    cudaMemPool_t pool = nullptr;  // device buffers from this pool (the end-to-end call)
 };
 
 namespace {
@@ -613,7 +623,16 @@ int dev_copy(grav_plan *pl, const T *src, size_t n, T **dst) {
     *dst = nullptr;
     if (n == 0)
         return 0;
-    GC_CHECK(cudaMalloc((void **)dst, n * sizeof(T)));
+    if (pl->pool) {
+        if (cudaMallocFromPoolAsync((void **)dst, n * sizeof(T), pl->pool, 0) != cudaSuccess) {
+            // the pool's reserved but unused memory may be what is missing
+            cudaGetLastError();
+            cudaStreamSynchronize(0);
+            cudaMemPoolTrimTo(pl->pool, 0);
+            GC_CHECK(cudaMallocFromPoolAsync((void **)dst, n * sizeof(T), pl->pool, 0));
+        }
+    } else
+        GC_CHECK(cudaMalloc((void **)dst, n * sizeof(T)));
     pl->allocs.push_back(*dst);
     if (src)
         GC_CHECK(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
@@ -645,27 +664,64 @@ int auto_chunk(int64_t total, int64_t ngroups, int nsm, int64_t lo) {
 }
 
 // Work items of a plan from its kept list offsets and tuning: created group
-// by group (slot order), then sorted per kind by cost, longest first.
-int64_t make_queue(const grav_plan *pl, std::vector<Item> items[3], std::vector<int64_t> &gslot) {
+// by group (slot order: a group's point items, then quadrupole, then order 4),
+// then ordered per kind by cost, longest first, within each of the plan's
+// group ranges (chunk_group; the whole set when empty).  Every item but a
+// group's last of a kind is a full chunk, so the order is the full chunks in
+// creation order, then the remainders by length (both stable).
+int64_t make_queue(grav_plan *pl, std::vector<Item> items[3], std::vector<int64_t> &gslot) {
     const int64_t ng = pl->hp.ngroups;
-    const int chunk[3] = {pl->tune.chunk_p, pl->tune.chunk_q, pl->tune.chunk_h};
+    const int64_t chunk[3] = {pl->tune.chunk_p, pl->tune.chunk_q, pl->tune.chunk_h};
+    if (pl->chunk_group.size() < 2)
+        pl->chunk_group = {0, ng};
+    const int nc = (int)pl->chunk_group.size() - 1;
+    const int64_t *ptr[3];
+    for (int k = 0; k < 3; k++) ptr[k] = pl->lists_ptr[k].empty() ? nullptr : pl->lists_ptr[k].data();
+    // items per group and kind, then their first index and slot by prefix sums
+    std::vector<int64_t> first[3];
+    for (int k = 0; k < 3; k++) first[k].assign(ng + 1, 0);
     gslot.assign(ng + 1, 0);
-    int32_t slot = 0;
+#pragma omp parallel for schedule(static)
     for (int64_t g = 0; g < ng; g++) {
+        int64_t all = 0;
         for (int k = 0; k < 3; k++) {
-            if (pl->lists_ptr[k].empty())
-                continue;
-            const int64_t *ptr = pl->lists_ptr[k].data();
-            for (int64_t b = ptr[g]; b < ptr[g + 1]; b += chunk[k])
-                items[k].push_back(Item{(int32_t)g, slot++, b, std::min(ptr[g + 1], b + chunk[k])});
+            const int64_t n = ptr[k] ? (ptr[k][g + 1] - ptr[k][g] + chunk[k] - 1) / chunk[k] : 0;
+            first[k][g + 1] = n;
+            all += n;
         }
-        gslot[g + 1] = slot;
+        gslot[g + 1] = all;
     }
-    for (int k = 0; k < 3; k++)
-        std::stable_sort(items[k].begin(), items[k].end(), [](const Item &a, const Item &b) {
-            return (a.end - a.begin) > (b.end - b.begin);
+    for (int64_t g = 0; g < ng; g++) {
+        for (int k = 0; k < 3; k++) first[k][g + 1] += first[k][g];
+        gslot[g + 1] += gslot[g];
+    }
+    for (int k = 0; k < 3; k++) items[k].resize((size_t)first[k][ng]);
+#pragma omp parallel for schedule(static)
+    for (int64_t g = 0; g < ng; g++) {
+        int32_t slot = (int32_t)gslot[g];
+        for (int k = 0; k < 3; k++) {
+            if (!ptr[k])
+                continue;
+            Item *out = items[k].data() + first[k][g];
+            for (int64_t b = ptr[k][g]; b < ptr[k][g + 1]; b += chunk[k])
+                *out++ = Item{(int32_t)g, slot++, b, std::min(ptr[k][g + 1], b + chunk[k])};
+        }
+    }
+    for (int k = 0; k < 3; k++) {
+        pl->chunk_item[k].resize(nc + 1);
+        for (int c = 0; c <= nc; c++) pl->chunk_item[k][c] = (int)first[k][pl->chunk_group[c]];
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int task = 0; task < 3 * nc; task++) {
+        const int k = task % 3, c = task / 3;
+        auto b = items[k].begin() + pl->chunk_item[k][c], e = items[k].begin() + pl->chunk_item[k][c + 1];
+        const int64_t full = chunk[k];
+        auto mid = std::stable_partition(b, e, [full](const Item &x) { return x.end - x.begin == full; });
+        std::stable_sort(mid, e, [](const Item &x, const Item &y) {
+            return (x.end - x.begin) > (y.end - y.begin);
         });
-    return slot;
+    }
+    return gslot[ng];
 }
 
 // The device address of page-locked host memory (lists read in place over
@@ -681,9 +737,52 @@ const uint32_t *mapped_host(const uint32_t *p) {
 
 }  // namespace
 
-extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning *tuning,
-                                       grav_plan **plan_out) {
+namespace {
+// The upload.  With nchunks > 0 (the pipelined end-to-end call) the list
+// buffers are allocated but not filled: the caller copies each group range's
+// lists while the kernels evaluate the previous range, and the kernels'
+// own index checks stand in for the upload-time list check.
+thread_local double t_phase[5];  // grav_groups_CUDA_phases
+
+// The end-to-end call's device buffers come from a pool that keeps freed
+// memory reserved (until grav_groups_release_CUDA): mapping and unmapping
+// tens of gigabytes in every call costs as much as the evaluation's tail.
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool = nullptr;
+int g_pool_device = -1;
+
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+int e2e_pool(cudaMemPool_t *out) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    int dev = 0;
+    GC_CHECK(cudaGetDevice(&dev));
+    if (g_pool && g_pool_device != dev) {
+        cudaMemPoolDestroy(g_pool);
+        g_pool = nullptr;
+    }
+    if (!g_pool) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        GC_CHECK(cudaMemPoolCreate(&g_pool, &props));
+        uint64_t keep = UINT64_MAX;
+        GC_CHECK(cudaMemPoolSetAttribute(g_pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        g_pool_device = dev;
+    }
+    *out = g_pool;
+    return 0;
+}
+
+int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **plan_out,
+                int nchunks) {
     *plan_out = nullptr;
+    const double t_start = now_s();
     if (!hp || hp->nbodies <= 0 || hp->ngroups <= 0 || !hp->points || !hp->groups ||
         !hp->pptr || !hp->plist)
         return gc::set_status(-1, "grav_groups_upload_CUDA: incomplete problem");
@@ -694,6 +793,17 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
     pl->hp = *hp;
     pl->tune = tuning ? *tuning : default_tuning();
     const int64_t ng = hp->ngroups, nb = hp->nbodies, np = hp->nbodies + hp->ncells;
+    const bool deferred = nchunks > 0;
+    if (deferred && hp->lists_in_host) {
+        delete pl;
+        return gc::set_status(-1, "upload: deferred lists and lists_in_host exclude each other");
+    }
+    if (deferred) {
+        if (int e = e2e_pool(&pl->pool)) {
+            delete pl;
+            return e;
+        }
+    }
 
     // validate everything the kernels will index
     int bad_group = 0;
@@ -706,15 +816,19 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
             (hp->hptr && hp->hptr[g + 1] < hp->hptr[g]))
             bad_group |= 1;
     }
+    if (hp->pptr[0] != 0 || (hp->qptr && hp->qptr[0] != 0) || (hp->hptr && hp->hptr[0] != 0))
+        bad_group |= 1;
     if (bad_group) {
         delete pl;
         return gc::set_status(-1, "a group has 0 or more than 32 sinks, lies outside the bodies, "
-                                  "or has decreasing list offsets");
+                                  "or has list offsets that decrease or do not start at 0");
     }
-    // Every list entry is checked on the device after the upload (k_check_lists):
-    // a host pass over tens of gigabytes of lists would dominate an end-to-end call.
+    // Every list entry is checked on the device: after the upload (k_check_lists),
+    // or by the kernels as they read it (deferred lists, lists_in_host).  A host
+    // pass over tens of gigabytes of lists would dominate an end-to-end call.
     const int64_t *eptr = hp->pptr;
-    if ((hp->qptr && hp->qptr[ng] && !hp->qcells) || (hp->hptr && hp->hptr[ng] && !hp->hcells)) {
+    if ((hp->qptr && hp->qptr[ng] && (!hp->qcells || hp->ncells <= 0)) ||
+        (hp->hptr && hp->hptr[ng] && (!hp->hcells || hp->ncells <= 0))) {
         delete pl;
         return gc::set_status(-1, "a cell list without its cell table");
     }
@@ -752,6 +866,37 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
     for (int k = 0; k < 3; k++)
         if (ptrs[k])
             pl->lists_ptr[k].assign(ptrs[k], ptrs[k] + ng + 1);
+    if (deferred) {
+        // group ranges holding about equal list bytes
+        auto bytes_to = [&](int64_t g) {
+            int64_t b = eptr[g];
+            if (hp->qptr)
+                b += hp->qptr[g];
+            if (hp->hptr)
+                b += hp->hptr[g];
+            if (want_ewald)
+                b += hp->cptr[g];
+            return b;
+        };
+        const int64_t total = std::max<int64_t>(1, bytes_to(ng));
+        pl->chunk_group.assign(1, 0);
+        int64_t g = 0;
+        for (int c = 1; c < nchunks; c++) {
+            const int64_t want = total * c / nchunks;
+            int64_t lo = g, hi = ng;  // first group whose prefix reaches `want`
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) / 2;
+                if (bytes_to(mid) < want)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            g = lo;
+            if (g > pl->chunk_group.back() && g < ng)
+                pl->chunk_group.push_back(g);
+        }
+        pl->chunk_group.push_back(ng);
+    }
     pl->nslots = make_queue(pl, items, gslot);
 
     // interaction counts (sinks x sources); the point list's split into
@@ -764,6 +909,8 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
             pl->counts[3] += c * (hp->hptr[g + 1] - hp->hptr[g]);
     }
 
+    t_phase[0] = now_s() - t_start;
+    const double t_dev = now_s();
     DevProblem &d = pl->dp;
     int rc = 0;
     float4 *pts = nullptr;
@@ -780,8 +927,26 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
     nln_group *gr = nullptr;
     rc |= dev_copy(pl, hp->groups, (size_t)ng, &gr);
     d.groups = gr;
-    uint32_t *l0 = nullptr, *l1 = nullptr, *l2 = nullptr;
-    if (hp->lists_in_host) {
+    uint32_t *l0 = nullptr, *l1 = nullptr, *l2 = nullptr, *all_clist = nullptr;
+    if (deferred) {
+        // one buffer for the four lists, filled range by range by the caller
+        const size_t n[4] = {(size_t)hp->pptr[ng], hp->qptr ? (size_t)hp->qptr[ng] : 0,
+                             hp->hptr ? (size_t)hp->hptr[ng] : 0,
+                             want_ewald ? (size_t)std::max<int64_t>(1, hp->cptr[ng]) : 0};
+        size_t off[4], words = 0;
+        for (int k = 0; k < 4; k++) {
+            off[k] = words;
+            words += (n[k] + 63) / 64 * 64;
+        }
+        uint32_t *all = nullptr;
+        rc |= dev_copy<uint32_t>(pl, nullptr, words, &all);
+        if (all) {
+            l0 = n[0] ? all + off[0] : nullptr;
+            l1 = n[1] ? all + off[1] : nullptr;
+            l2 = n[2] ? all + off[2] : nullptr;
+            all_clist = n[3] ? all + off[3] : nullptr;
+        }
+    } else if (hp->lists_in_host) {
         // the kernels read the lists in place from page-locked host memory
         const uint32_t *m0 = mapped_host(hp->plist);
         const uint32_t *m1 = hp->qptr ? mapped_host(hp->qlist) : nullptr;
@@ -812,8 +977,8 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
         d.items[k] = it;
         d.nitems[k] = (int)items[k].size();
     }
-    int *ctr = nullptr;
-    rc |= dev_copy<int>(pl, nullptr, 4, &ctr);
+    int *ctr = nullptr;  // 4 queue heads per group range
+    rc |= dev_copy<int>(pl, nullptr, 4 * (pl->chunk_group.size() - 1), &ctr);
     d.counters = ctr;
     float4 *part = nullptr;
     rc |= dev_copy<float4>(pl, nullptr, (size_t)std::max<int64_t>(1, pl->nslots) * 64, &part);
@@ -834,6 +999,8 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
                 return gc::set_status(-1, "grav_groups_upload_CUDA: lists_in_host needs the "
                                           "correction list in page-locked host memory");
             }
+        } else if (deferred) {
+            cl = all_clist;
         } else {
             rc |= dev_copy(pl, hp->clist, (size_t)std::max<int64_t>(1, hp->cptr[ng]), &cl);
         }
@@ -882,7 +1049,7 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
         return rc;
     }
     cudaMemset(err, 0, sizeof(unsigned));
-    if (hp->lists_in_host) {
+    if (hp->lists_in_host || deferred) {
         // entries are checked by the kernels as they read them (bad ones set
         // the error word); the point list's body/cell split is not counted
         int64_t tot = 0;
@@ -958,14 +1125,30 @@ extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning
     pl->hp.pptr = pl->hp.qptr = pl->hp.hptr = nullptr;
     pl->hp.plist = nullptr;
     pl->hp.qlist = pl->hp.hlist = nullptr;
+    if (pl->pool) {
+        // buffers allocated in stream order on the default stream: complete
+        // before other streams use them
+        const cudaError_t e = cudaStreamSynchronize(0);
+        if (e != cudaSuccess) {
+            grav_plan_free(pl);
+            return gc::cuda_status(e, "upload: pool allocations");
+        }
+    }
     *plan_out = pl;
+    t_phase[1] = now_s() - t_dev;
     return 0;
+}
+}  // namespace
+
+extern "C" int grav_groups_upload_CUDA(const grav_problem *hp, const grav_tuning *tuning,
+                                       grav_plan **plan_out) {
+    return upload_impl(hp, tuning, plan_out, 0);
 }
 
 namespace {
 template <int KIND>
-int launch_kind(grav_plan *pl, cudaStream_t st) {
-    if (pl->dp.nitems[KIND] == 0)
+int launch_kind(grav_plan *pl, const DevProblem &dp, cudaStream_t st) {
+    if (dp.nitems[KIND] == 0)
         return 0;
     const int wpb = pl->tune.warps_per_block;
     if (KIND == KP) {
@@ -973,8 +1156,8 @@ int launch_kind(grav_plan *pl, cudaStream_t st) {
         GC_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_points, 256, 0));
         int per_sm = pl->tune.blocks_per_sm > 0 ? std::min(pl->tune.blocks_per_sm, fit) : fit;
         int blocks = std::max(1, per_sm) * pl->nsm;
-        blocks = std::min(blocks, (pl->dp.nitems[KP] + 7) / 8);
-        k_points<<<blocks, 256, 0, st>>>(pl->dp);
+        blocks = std::min(blocks, (dp.nitems[KP] + 7) / 8);
+        k_points<<<blocks, 256, 0, st>>>(dp);
         GC_CHECK(cudaGetLastError());
         pl->launches++;
         return 0;
@@ -986,8 +1169,21 @@ int launch_kind(grav_plan *pl, cudaStream_t st) {
     GC_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, kern, wpb * 32, smem));
     int per_sm = pl->tune.blocks_per_sm > 0 ? std::min(pl->tune.blocks_per_sm, fit) : fit;
     int blocks = std::max(1, per_sm) * pl->nsm;
-    blocks = std::min(blocks, (pl->dp.nitems[KIND] + wpb - 1) / wpb);
-    kern<<<blocks, wpb * 32, smem, st>>>(pl->tmap[KIND], pl->dp);
+    blocks = std::min(blocks, (dp.nitems[KIND] + wpb - 1) / wpb);
+    kern<<<blocks, wpb * 32, smem, st>>>(pl->tmap[KIND], dp);
+    GC_CHECK(cudaGetLastError());
+    pl->launches++;
+    return 0;
+}
+
+// Two warps per block: at ~160 registers a thread, small blocks let more
+// warps stay resident, which this latency-bound kernel needs.
+int launch_finish(grav_plan *pl, const DevProblem &dp, cudaStream_t st) {
+    const int wpb = 2;
+    const int64_t n = dp.ngroups - dp.gbegin;
+    if (n <= 0)
+        return 0;
+    k_finish<<<(unsigned)((n + wpb - 1) / wpb), wpb * 32, 0, st>>>(dp);
     GC_CHECK(cudaGetLastError());
     pl->launches++;
     return 0;
@@ -1007,24 +1203,20 @@ extern "C" int grav_groups_eval_CUDA(grav_plan *pl, void *stream) {
     GC_CHECK(cudaMemsetAsync(pl->dp.counters, 0, 4 * sizeof(int), st));
     if (int rc = mark(0))
         return rc;
-    if (int rc = launch_kind<KH>(pl, st))
+    if (int rc = launch_kind<KH>(pl, pl->dp, st))
         return rc;
     if (int rc = mark(1))
         return rc;
-    if (int rc = launch_kind<KQ>(pl, st))
+    if (int rc = launch_kind<KQ>(pl, pl->dp, st))
         return rc;
     if (int rc = mark(2))
         return rc;
-    if (int rc = launch_kind<KP>(pl, st))
+    if (int rc = launch_kind<KP>(pl, pl->dp, st))
         return rc;
     if (int rc = mark(3))
         return rc;
-    // two warps per block: at ~160 registers a thread, small blocks let more
-    // warps stay resident, which this latency-bound kernel needs
-    const int wpb = 2;
-    k_finish<<<(unsigned)((pl->dp.ngroups + wpb - 1) / wpb), wpb * 32, 0, st>>>(pl->dp);
-    GC_CHECK(cudaGetLastError());
-    pl->launches++;
+    if (int rc = launch_finish(pl, pl->dp, st))
+        return rc;
     return mark(4);
 }
 
@@ -1056,7 +1248,10 @@ extern "C" int grav_plan_retune_CUDA(grav_plan *pl, const grav_tuning *tuning) {
             return;
         auto it = std::find(pl->allocs.begin(), pl->allocs.end(), p);
         if (it != pl->allocs.end()) {
-            cudaFree(*it);
+            if (pl->pool)
+                cudaFreeAsync(*it, 0);
+            else
+                cudaFree(*it);
             pl->allocs.erase(it);
         }
     };
@@ -1137,22 +1332,155 @@ extern "C" void grav_plan_free(grav_plan *pl) {
         step_state_free(pl->step);
     if (pl->adj)
         adjoint_state_free(pl->adj);
-    for (void *p : pl->allocs) cudaFree(p);
+    for (void *p : pl->allocs) {
+        if (pl->pool)
+            cudaFreeAsync(p, 0);  // back to the pool, reserved for the next call
+        else
+            cudaFree(p);
+    }
     for (cudaEvent_t e : pl->ev)
         if (e)
             cudaEventDestroy(e);
     delete pl;
 }
 
+namespace {
+// Group ranges of the pipelined end-to-end call: about 128 MiB of lists
+// each, at most 32; GRAV_E2E_CHUNKS overrides the count.
+int e2e_chunks(const grav_problem *hp) {
+    if (const char *e = getenv("GRAV_E2E_CHUNKS"))
+        return std::max(1, std::min(64, atoi(e)));
+    const int64_t ng = hp->ngroups;
+    int64_t n = hp->pptr[ng] + (hp->qptr ? hp->qptr[ng] : 0) + (hp->hptr ? hp->hptr[ng] : 0) +
+                (hp->box > 0 && hp->ewald && hp->cptr ? hp->cptr[ng] : 0);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(32, n * 4 / (128ll << 20)));
+}
+
+// Copy group range c's slice of every list on `cs`, then make `st` wait for it.
+int copy_range(grav_plan *pl, const grav_problem *hp, size_t c, cudaStream_t cs, cudaStream_t st,
+               cudaEvent_t ev) {
+    const int64_t g0 = pl->chunk_group[c], g1 = pl->chunk_group[c + 1];
+    const DevProblem &d = pl->dp;
+    const int64_t *ptr[4] = {hp->pptr, hp->qptr, hp->hptr, d.clist ? hp->cptr : nullptr};
+    const uint32_t *src[4] = {hp->plist, hp->qlist, hp->hlist, hp->clist};
+    const uint32_t *dst[4] = {d.list[0], d.list[1], d.list[2], d.clist};
+    for (int k = 0; k < 4; k++) {
+        if (!ptr[k] || !dst[k] || ptr[k][g1] <= ptr[k][g0])
+            continue;
+        GC_CHECK(cudaMemcpyAsync(const_cast<uint32_t *>(dst[k]) + ptr[k][g0], src[k] + ptr[k][g0],
+                                 (size_t)(ptr[k][g1] - ptr[k][g0]) * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice, cs));
+    }
+    GC_CHECK(cudaEventRecord(ev, cs));
+    GC_CHECK(cudaStreamWaitEvent(st, ev, 0));
+    return 0;
+}
+
+// Evaluate group range c: its work items, then its groups' finish pass.
+int eval_range(grav_plan *pl, size_t c, cudaStream_t st) {
+    DevProblem dp = pl->dp;
+    for (int k = 0; k < 3; k++) {
+        const int b = pl->chunk_item[k][c], e = pl->chunk_item[k][c + 1];
+        dp.items[k] = pl->dp.items[k] ? pl->dp.items[k] + b : nullptr;
+        dp.nitems[k] = e - b;
+    }
+    dp.counters = pl->dp.counters + 4 * c;
+    dp.gbegin = pl->chunk_group[c];
+    dp.ngroups = pl->chunk_group[c + 1];
+    int rc = launch_kind<KH>(pl, dp, st);
+    if (!rc)
+        rc = launch_kind<KQ>(pl, dp, st);
+    if (!rc)
+        rc = launch_kind<KP>(pl, dp, st);
+    if (!rc)
+        rc = launch_finish(pl, dp, st);
+    return rc;
+}
+}  // namespace
+
+// The end-to-end call: upload the tables, then copy the lists range by range
+// on a copy stream while the kernels evaluate the ranges already copied, and
+// download.  Lists in page-locked host memory overlap best; pageable lists
+// still overlap each copy with the previous range's kernels.
 extern "C" int grav_groups_CUDA(const grav_problem *hp, float *acc_phi) {
+    if (!hp || hp->ngroups <= 0 || !hp->pptr || !acc_phi)
+        return gc::set_status(-1, "grav_groups_CUDA: incomplete problem");
     grav_plan *pl = nullptr;
-    if (int rc = grav_groups_upload_CUDA(hp, nullptr, &pl))
+    if (hp->lists_in_host) {
+        if (int rc = grav_groups_upload_CUDA(hp, nullptr, &pl))
+            return rc;
+        double t0 = now_s();
+        int rc = grav_groups_eval_CUDA(pl, nullptr);
+        const cudaError_t e = rc ? cudaSuccess : cudaDeviceSynchronize();
+        if (e != cudaSuccess)
+            rc = gc::cuda_status(e, "grav_groups_CUDA: evaluation");
+        t_phase[2] = now_s() - t0;
+        t0 = now_s();
+        if (!rc)
+            rc = grav_groups_download_CUDA(pl, acc_phi);
+        t_phase[3] = now_s() - t0;
+        t0 = now_s();
+        grav_plan_free(pl);
+        t_phase[4] = now_s() - t0;
         return rc;
-    int rc = grav_groups_eval_CUDA(pl, nullptr);
+    }
+    if (int rc = upload_impl(hp, nullptr, &pl, e2e_chunks(hp)))
+        return rc;
+    const size_t nc = pl->chunk_group.size() - 1;
+    double t0 = now_s();
+    auto chk = [](cudaError_t e, const char *what) {
+        return e == cudaSuccess ? 0 : gc::cuda_status(e, what);
+    };
+    cudaStream_t cs = nullptr, st = nullptr;
+    std::vector<cudaEvent_t> ev(nc, nullptr);
+    int rc = 0;
+    cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    for (size_t c = 0; c < nc && e == cudaSuccess; c++)
+        e = cudaEventCreateWithFlags(&ev[c], cudaEventDisableTiming);
+    rc = chk(e, "grav_groups_CUDA: streams");
+    if (!rc)
+        rc = chk(cudaMemsetAsync(pl->dp.counters, 0, 4 * nc * sizeof(int), st),
+                 "grav_groups_CUDA: queue heads");
+    pl->launches = 0;
+    for (size_t c = 0; c < nc && !rc; c++) {
+        rc = copy_range(pl, hp, c, cs, st, ev[c]);
+        if (!rc)
+            rc = eval_range(pl, c, st);
+    }
+    if (!rc)
+        rc = chk(cudaStreamSynchronize(st), "grav_groups_CUDA: evaluation");
+    t_phase[2] = now_s() - t0;
+    t0 = now_s();
     if (!rc)
         rc = grav_groups_download_CUDA(pl, acc_phi);
+    t_phase[3] = now_s() - t0;
+    t0 = now_s();
+    if (cs)
+        cudaStreamSynchronize(cs);
+    for (cudaEvent_t x : ev)
+        if (x)
+            cudaEventDestroy(x);
+    if (cs)
+        cudaStreamDestroy(cs);
+    if (st)
+        cudaStreamDestroy(st);
     grav_plan_free(pl);
+    t_phase[4] = now_s() - t0;
     return rc;
+}
+
+extern "C" void grav_groups_release_CUDA(void) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (g_pool) {
+        cudaDeviceSynchronize();
+        cudaMemPoolTrimTo(g_pool, 0);
+    }
+}
+
+extern "C" void grav_groups_CUDA_phases(double seconds[5]) {
+    for (int k = 0; k < 5; k++) seconds[k] = t_phase[k];
 }
 
 // ------------------------------------------------------------ no-allocation evaluation
@@ -1340,8 +1668,8 @@ extern "C" int grav_groups_eval_dev_CUDA(const grav_problem *dp, float *acc_phi,
     k_dev_setup<<<(unsigned)((ng + 255) / 256), 256, 0, st>>>(dp->groups, dp->pptr, dp->qptr,
                                                                dp->hptr, ng, dp->nbodies, nk, S);
     GC_CHECK(cudaGetLastError());
-    if ((rc = launch_kind<KH>(&pl, st)) || (rc = launch_kind<KQ>(&pl, st)) ||
-        (rc = launch_kind<KP>(&pl, st)))
+    if ((rc = launch_kind<KH>(&pl, pl.dp, st)) || (rc = launch_kind<KQ>(&pl, pl.dp, st)) ||
+        (rc = launch_kind<KP>(&pl, pl.dp, st)))
         return rc;
     k_finish<<<(unsigned)((ng + 7) / 8), 256, 0, st>>>(pl.dp);
     GC_CHECK(cudaGetLastError());

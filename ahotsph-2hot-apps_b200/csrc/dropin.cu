@@ -468,6 +468,7 @@ extern "C" void CUDA_Init(void *device_prop) {
 }
 
 extern "C" void CUDA_Finalize(void) {
+    grav_groups_release_CUDA();
     if (!S.init)
         return;
     for (int i = 0; i < NQ; i++) {

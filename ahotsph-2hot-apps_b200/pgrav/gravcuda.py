@@ -27,6 +27,7 @@ EXPORTS = [
     "grav_groups_eval_dev_CUDA", "grav_plan_set_tree_CUDA", "grav_plan_refit_CUDA",
     "grav_plan_bodies", "grav_plan_integrate_CUDA", "grav_plan_step_CUDA",
     "grav_plan_adjoint_CUDA", "grav_plan_retune_CUDA", "grav_plan_get_tuning",
+    "grav_groups_CUDA_phases", "grav_groups_release_CUDA",
 ]
 
 
@@ -89,7 +90,8 @@ def lib(record_errors=True):
             "grav_groups_download_CUDA": ([vp, vp], i32),
             "grav_plan_output": ([vp], vp), "grav_plan_counts": ([vp, vp], None),
             "grav_plan_launches": ([vp], i32), "grav_plan_free": ([vp], None),
-            "grav_groups_CUDA": ([vp, vp], i32),
+            "grav_groups_CUDA": ([vp, vp], i32), "grav_groups_CUDA_phases": ([vp], None),
+            "grav_groups_release_CUDA": ([], None),
             "grav_direct_fp64_CUDA": ([vp, i64, vp, i64, f64, f64, vp], i32),
             "grav_plan_set_timing": ([vp, i32], i32), "grav_plan_kernel_ms": ([vp, vp], i32),
             "grav_groups_eval_dev_CUDA": ([vp, vp, vp], i32),
@@ -369,9 +371,10 @@ class PinnedProblem:
         p.pptr = pin(t.ptr[0]).ctypes.data
         p.qptr = pin(t.ptr[1]).ctypes.data
         p.hptr = pin(t.ptr[2]).ctypes.data
-        p.plist = pin(t.plist if len(t.plist) else np.zeros(1, np.uint32)).ctypes.data
-        p.qlist = pin(t.qlist if has_q else np.zeros(1, np.uint32)).ctypes.data
-        p.hlist = pin(t.hlist if has_h else np.zeros(1, np.uint32)).ctypes.data
+        self.lists = [pin(t.plist if len(t.plist) else np.zeros(1, np.uint32)),
+                      pin(t.qlist if has_q else np.zeros(1, np.uint32)),
+                      pin(t.hlist if has_h else np.zeros(1, np.uint32))]
+        p.plist, p.qlist, p.hlist = (a.ctypes.data for a in self.lists)
         if periodic:
             p.cptr = pin(t.ptr[3]).ctypes.data
             p.clist = pin(t.clist if len(t.clist) else np.zeros(1, np.uint32)).ctypes.data
@@ -394,3 +397,12 @@ def groups_eval_problem(pp, eps2, box, ewald=False):
     pp.problem.ewald = int(bool(ewald))
     check(lib().grav_groups_CUDA(ctypes.byref(pp.problem), pp.out.ctypes.data))
     return pp.out
+
+
+def groups_phases():
+    """Seconds of the phases of this thread's last grav_groups_CUDA call:
+    host checks and queue, allocation and table upload, list copies with
+    the overlapped evaluation, download, release."""
+    out = np.zeros(5, np.float64)
+    lib().grav_groups_CUDA_phases(out.ctypes.data)
+    return dict(zip(("host", "upload", "copy_eval", "download", "release"), out.tolist()))

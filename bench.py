@@ -361,9 +361,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="box256", choices=list(WORKLOADS))
     ap.add_argument("--tol", type=float, default=0.0)
-    ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--e2e-copy-lists", action="store_true",
-                    help="end-to-end leg: copy the lists at upload instead of reading them in place")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-lists-in-host", action="store_true",
+                    help="end-to-end leg: the kernels read the lists in place from page-locked "
+                         "host memory instead of the pipelined copy")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--dropin-groups", type=int, default=0,
@@ -534,23 +535,30 @@ def main():
     e2e = None
     host = out = None
     if args.e2e_steps > 0:
-        host = gc.pinned_problem(tree, lists_in_host=not args.e2e_copy_lists)
+        host = gc.pinned_problem(tree, lists_in_host=args.e2e_lists_in_host)
         out = host.out
         torch.cuda.synchronize()
-        walls = []
+        gc.groups_eval_problem(host, eps2, box, ewald=w["ewald"] and box > 0)  # warm-up
+        walls, phases = [], []
         for _ in range(args.e2e_steps):
             ta = time.perf_counter()
             gc.groups_eval_problem(host, eps2, box, ewald=w["ewald"] and box > 0)
             torch.cuda.synchronize()
             walls.append(time.perf_counter() - ta)
+            phases.append(gc.groups_phases())
         e2e_s = float(np.median(walls))
+        mid = int(np.argsort(walls)[len(walls) // 2])
         e2e = {"value": inter * world / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(host.h2d_bytes), "d2h_bytes_per_step": int(out.nbytes),
                "ms_per_step": e2e_s * 1e3, "steps": args.e2e_steps,
                "timing": "wall clock around grav_groups_CUDA (upload, evaluate, download)",
-               "lists": ("copied to the device at upload" if args.e2e_copy_lists else
-                         "read by the kernels in place from page-locked host memory over PCIe "
-                         "(every step; tables copied at upload)")}
+               "walls_s": walls, "phases_s": phases[mid],
+               "lists": ("read by the kernels in place from page-locked host memory over PCIe "
+                         "(every step; tables copied at upload)" if args.e2e_lists_in_host else
+                         "copied from page-locked host memory group range by group range on a "
+                         "copy stream, overlapped with the evaluation of the ranges already "
+                         "copied (every step)")}
+        gc.lib().grav_groups_release_CUDA()  # the end-to-end call's kept list buffer
 
     dropin = None
     if rank == 0 and args.dropin_groups > 0:

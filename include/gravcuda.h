@@ -223,9 +223,28 @@ void grav_plan_free(grav_plan *plan);
 
 /*
  * One-call end-to-end form: upload, evaluate, download, free.  acc_phi:
- * host, nbodies x 4 floats, tree order.
+ * host, nbodies x 4 floats, tree order.  Unless lists_in_host is set, the
+ * lists are copied group range by group range (about 128 MiB each, at most
+ * 32 ranges; the environment variable GRAV_E2E_CHUNKS sets the count) on a
+ * copy stream while the kernels evaluate the ranges already copied; list
+ * entries are then checked by the kernels as they read them, and a bad one
+ * fails the call with status -2 after the evaluation.  Lists in page-locked
+ * host memory overlap best.  The call's device buffers come from a memory
+ * pool that keeps freed memory reserved for the next call, until
+ * grav_groups_release_CUDA or CUDA_Finalize.
  */
 int grav_groups_CUDA(const grav_problem *host_problem, float *acc_phi);
+
+/* Return the memory grav_groups_CUDA keeps reserved between calls. */
+void grav_groups_release_CUDA(void);
+
+/*
+ * Wall-clock seconds of the phases of this thread's last grav_groups_CUDA
+ * call: [0] host checks and work queue, [1] device allocation and table
+ * upload, [2] list copies overlapped with the evaluation, [3] download,
+ * [4] release of the device buffers.
+ */
+void grav_groups_CUDA_phases(double seconds[5]);
 
 /*
  * FP64 direct sum at nsink sample sinks, the accuracy reference of every

@@ -127,3 +127,58 @@ def test_lists_read_in_place_from_host_memory(gc):
     with pytest.raises(gc.GravError, match="page-locked"):
         gc.check(gc.lib().grav_groups_CUDA(__import__("ctypes").byref(prob),
                                            np.empty((t.n, 4), np.float32).ctypes.data))
+
+
+@pytest.mark.parametrize("chunks", ["1", "3", "7"])
+def test_pipelined_end_to_end_matches_plan(gc, chunks, monkeypatch):
+    """grav_groups_CUDA copies the lists group range by group range on a copy
+    stream while the kernels evaluate the ranges already copied: the results
+    are those of a plan that uploaded everything first, bit for bit."""
+    t = make_tree("box", 24 ** 3, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-4)
+    eps2 = (1.0 / 24 / 50) ** 2
+    plan = gc.Plan(t, eps2, ewald=True)
+    plan.eval()
+    ref = plan.download()
+    plan.free()
+    monkeypatch.setenv("GRAV_E2E_CHUNKS", chunks)
+    pp = gc.pinned_problem(t, lists_in_host=False)
+    got = gc.groups_eval_problem(pp, eps2, 1.0, ewald=True).copy()
+    assert np.array_equal(got, ref)
+
+
+def test_pipelined_end_to_end_reports_bad_entries(gc, monkeypatch):
+    """Without an upload-time list check, the kernels' own index checks flag
+    an entry past its table and the call fails with a status."""
+    t = make_tree("plummer", 5000, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-4)
+    monkeypatch.setenv("GRAV_E2E_CHUNKS", "3")
+    for kind, bad in ((0, t.n + t.ncells + 5), (2, t.ncells + 1), (1, 7 | (27 << 27))):
+        pp = gc.pinned_problem(t, lists_in_host=False)
+        lst = pp.lists[kind]
+        lst[len(lst) // 2] = bad
+        with pytest.raises(gc.GravError, match="device error word"):
+            gc.groups_eval_problem(pp, 1e-4, 0.0)
+        gc.lib().gravcuda_clear_status()
+    pp = gc.pinned_problem(t, lists_in_host=False)
+    gc.groups_eval_problem(pp, 1e-4, 0.0)   # intact lists still evaluate
+
+
+def test_end_to_end_list_buffer_grows_and_releases(gc, monkeypatch):
+    """The memory kept between end-to-end calls serves a smaller problem,
+    grows for a larger one, and is allocated again after
+    grav_groups_release_CUDA."""
+    monkeypatch.setenv("GRAV_E2E_CHUNKS", "2")
+    small = make_tree("plummer", 3000, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-4)
+    large = make_tree("plummer", 12000, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-4)
+    refs = {}
+    for t in (small, large):
+        plan = gc.Plan(t, 1e-4)
+        plan.eval()
+        refs[id(t)] = plan.download()
+        plan.free()
+    for t in (small, large, small):
+        got = gc.groups_eval_problem(gc.pinned_problem(t), 1e-4, 0.0)
+        assert np.array_equal(got, refs[id(t)])
+    gc.lib().grav_groups_release_CUDA()
+    got = gc.groups_eval_problem(gc.pinned_problem(large), 1e-4, 0.0)
+    assert np.array_equal(got, refs[id(large)])
+    gc.lib().grav_groups_release_CUDA()
