@@ -144,6 +144,83 @@ __device__ __forceinline__ void convert(unsigned char *slot, uint32_t code, cons
     }
 }
 
+// Unpack the run-packed lists (format in nlnlists.h) of groups g0..g1-1,
+// one warp per group.  Per 32-word block: a warp scan of the words' entry
+// counts places each word's entries (an entry word stands for itself, a run
+// word for the n entries after the word before it); then the warp writes
+// the block's entries 32 consecutive ones at a time, each lane finding the
+// word its entry comes from by a binary search over the scan.  Stores stay
+// inside the group's plain range [ptr[g], ptr[g+1]); a group that does not
+// fill it exactly, a run word that starts a group or follows a run word, or
+// a run that would carry into the image code sets GC_DEV_BAD_RUNS.
+__global__ void k_unpack(const uint32_t *__restrict__ z, const int64_t *__restrict__ zptr,
+                         const int64_t *__restrict__ ptr, int64_t g0, int64_t g1,
+                         uint32_t *__restrict__ out, unsigned *err) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t g = g0 + (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < g1;
+         g += nwarps) {
+        const int64_t zb = zptr[g], ze = zptr[g + 1], oe = ptr[g + 1];
+        int64_t pos = ptr[g];
+        uint32_t prev = 0;  // last word of the previous block
+        bool have_prev = false, bad = false;
+        for (int64_t b = zb; b < ze; b += 32) {
+            const bool valid = b + lane < ze;
+            const uint32_t w = valid ? z[b + lane] : 0u;
+            const bool run = valid && (w >> NLN_IDX_BITS) == NLN_RUN_CODE;
+            uint32_t before = __shfl_up_sync(FULL, w, 1);
+            bool before_ok = true;
+            if (lane == 0) {
+                before = prev;
+                before_ok = have_prev;
+            }
+            uint32_t cnt = !valid ? 0u : (run ? (w & NLN_IDX_MASK) : 1u);
+            if (run && (!before_ok || (before >> NLN_IDX_BITS) == NLN_RUN_CODE || cnt == 0 ||
+                        (before & NLN_IDX_MASK) + cnt > NLN_IDX_MASK)) {
+                bad = true;
+                cnt = 0;
+            }
+            const uint32_t first = run ? before + 1u : w;  // entry j of this word: first + j
+            // block totals stay below 2^32: at most 32 words of 2^27 - 1
+            uint32_t inc = cnt;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(FULL, inc, o);
+                if (lane >= o)
+                    inc += v;
+            }
+            const uint32_t total = __shfl_sync(FULL, inc, 31);
+            if (pos + (int64_t)total > oe)
+                bad = true;
+            const int64_t room = oe - pos;
+            const uint32_t lim = room <= 0 ? 0u : (room < (int64_t)total ? (uint32_t)room : total);
+            for (uint32_t j0 = 0; j0 < lim; j0 += 32) {
+                const uint32_t j = j0 + lane;
+                // owner = number of words whose entries all lie before j
+                int owner = 0;
+#pragma unroll
+                for (int step = 16; step >= 1; step >>= 1) {
+                    const uint32_t v = __shfl_sync(FULL, inc, owner + step - 1);
+                    if (v <= j)
+                        owner += step;
+                }
+                owner = min(owner, 31);
+                const uint32_t f = __shfl_sync(FULL, first, owner);
+                const uint32_t s0 = __shfl_sync(FULL, inc - cnt, owner);
+                if (j < lim)
+                    out[pos + j] = f + (j - s0);
+            }
+            pos += total;
+            prev = __shfl_sync(FULL, w, 31);
+            have_prev = true;
+        }
+        if (pos != oe)
+            bad = true;
+        if (__any_sync(FULL, bad) && lane == 0)
+            atomicOr(err, GC_DEV_BAD_RUNS);
+    }
+}
+
 // Device-side check of an uploaded list, one warp per work item (or per
 // group for the correction list): every entry's index inside its table and
 // its image code in 0..26.  For the point list it also counts body and cell
@@ -587,6 +664,11 @@ struct grav_plan {
     std::vector<int64_t> chunk_group;
     std::vector<int> chunk_item[3];
     cudaMemPool_t pool = nullptr;  // device buffers from this pool (the end-to-end call)
+    // run-packed lists of the end-to-end call (P, Q, H, correction): device
+    // words, their offsets and the plain offsets they unpack to
+    uint32_t *zdev[4] = {nullptr, nullptr, nullptr, nullptr};
+    const int64_t *zptr_dev[4] = {nullptr, nullptr, nullptr, nullptr};
+    const int64_t *lptr_dev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace {
@@ -784,7 +866,7 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
     *plan_out = nullptr;
     const double t_start = now_s();
     if (!hp || hp->nbodies <= 0 || hp->ngroups <= 0 || !hp->points || !hp->groups ||
-        !hp->pptr || !hp->plist)
+        !hp->pptr || (!hp->plist && !(nchunks > 0 && hp->zlist[0])))
         return gc::set_status(-1, "grav_groups_upload_CUDA: incomplete problem");
     if (hp->nbodies + hp->ncells >= (int64_t)NLN_IDX_MASK)
         return gc::set_status(-1, "grav_groups_upload_CUDA: point table exceeds 27-bit indices");
@@ -834,7 +916,8 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
     }
     const bool want_ewald = hp->box > 0 && hp->ewald;
     if (want_ewald) {
-        if (!hp->cptr || !hp->clist || (hp->ncells > 0 && !hp->hcells)) {
+        if (!hp->cptr || (!hp->clist && !(deferred && hp->zlist[3])) ||
+            (hp->ncells > 0 && !hp->hcells)) {
             delete pl;
             return gc::set_status(-1, "the Ewald correction needs the correction list and the "
                                       "order-4 cell table");
@@ -847,6 +930,32 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
         if (bad || hp->cptr[0] != 0) {
             delete pl;
             return gc::set_status(-1, "bad correction list offsets");
+        }
+    }
+    // run-packed lists (the end-to-end call): offsets from 0, never decreasing
+    const int64_t *plain_ptr[4] = {hp->pptr, hp->qptr, hp->hptr, want_ewald ? hp->cptr : nullptr};
+    bool packed[4] = {false, false, false, false};
+    if (deferred) {
+        for (int k = 0; k < 4; k++) {
+            if (!hp->zlist[k] || !plain_ptr[k] || plain_ptr[k][ng] == 0)
+                continue;
+            const int64_t *z = hp->zptr[k];
+            int bad = !z || z[0] != 0;
+            if (!bad) {
+#pragma omp parallel for schedule(static) reduction(| : bad)
+                for (int64_t g = 0; g < ng; g++)
+                    if (z[g + 1] < z[g])
+                        bad |= 1;
+            }
+            if (bad) {
+                delete pl;
+                return gc::set_status(-1, "bad run-packed list offsets (kind %d)", k);
+            }
+            packed[k] = true;
+        }
+        if (!hp->plist && !packed[0]) {
+            delete pl;
+            return gc::set_status(-1, "grav_groups_CUDA: no point list");
         }
     }
 
@@ -878,11 +987,16 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
                 b += hp->cptr[g];
             return b;
         };
+        // The first range's copy is not overlapped: split it further into
+        // 1/8, 1/8, 1/4 and 1/2 of an equal share.
         const int64_t total = std::max<int64_t>(1, bytes_to(ng));
+        std::vector<int64_t> wants;
+        if (nchunks > 1)
+            for (int d : {8, 4, 2}) wants.push_back(total / ((int64_t)nchunks * d));
+        for (int c = 1; c < nchunks; c++) wants.push_back(total * c / nchunks);
         pl->chunk_group.assign(1, 0);
         int64_t g = 0;
-        for (int c = 1; c < nchunks; c++) {
-            const int64_t want = total * c / nchunks;
+        for (const int64_t want : wants) {
             int64_t lo = g, hi = ng;  // first group whose prefix reaches `want`
             while (lo < hi) {
                 const int64_t mid = (lo + hi) / 2;
@@ -945,6 +1059,19 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
             l1 = n[1] ? all + off[1] : nullptr;
             l2 = n[2] ? all + off[2] : nullptr;
             all_clist = n[3] ? all + off[3] : nullptr;
+        }
+        // packed kinds: device words (filled range by range) and both offset arrays
+        for (int k = 0; k < 4; k++) {
+            if (!packed[k])
+                continue;
+            uint32_t *zw = nullptr;
+            int64_t *zp = nullptr, *lp = nullptr;
+            rc |= dev_copy<uint32_t>(pl, nullptr, (size_t)std::max<int64_t>(1, hp->zptr[k][ng]), &zw);
+            rc |= dev_copy(pl, hp->zptr[k], (size_t)ng + 1, &zp);
+            rc |= dev_copy(pl, plain_ptr[k], (size_t)ng + 1, &lp);
+            pl->zdev[k] = zw;
+            pl->zptr_dev[k] = zp;
+            pl->lptr_dev[k] = lp;
         }
     } else if (hp->lists_in_host) {
         // the kernels read the lists in place from page-locked host memory
@@ -1345,15 +1472,22 @@ extern "C" void grav_plan_free(grav_plan *pl) {
 }
 
 namespace {
-// Group ranges of the pipelined end-to-end call: about 128 MiB of lists
-// each, at most 32; GRAV_E2E_CHUNKS overrides the count.
+// Group ranges of the pipelined end-to-end call: one per 2 GiB of list
+// words copied (packed words where a kind is run-packed), at most 16, the
+// first one split further; GRAV_E2E_CHUNKS overrides the count.
 int e2e_chunks(const grav_problem *hp) {
     if (const char *e = getenv("GRAV_E2E_CHUNKS"))
         return std::max(1, std::min(64, atoi(e)));
     const int64_t ng = hp->ngroups;
-    int64_t n = hp->pptr[ng] + (hp->qptr ? hp->qptr[ng] : 0) + (hp->hptr ? hp->hptr[ng] : 0) +
-                (hp->box > 0 && hp->ewald && hp->cptr ? hp->cptr[ng] : 0);
-    return (int)std::max<int64_t>(1, std::min<int64_t>(32, n * 4 / (128ll << 20)));
+    const int64_t *plain[4] = {hp->pptr, hp->qptr, hp->hptr,
+                               hp->box > 0 && hp->ewald ? hp->cptr : nullptr};
+    int64_t words = 0;
+    for (int k = 0; k < 4; k++) {
+        if (!plain[k])
+            continue;
+        words += (hp->zlist[k] && hp->zptr[k]) ? hp->zptr[k][ng] : plain[k][ng];
+    }
+    return (int)std::max<int64_t>(1, std::min<int64_t>(16, (words * 4 + (2ll << 30) - 1) >> 31));
 }
 
 // Copy group range c's slice of every list on `cs`, then make `st` wait for it.
@@ -1365,6 +1499,11 @@ int copy_range(grav_plan *pl, const grav_problem *hp, size_t c, cudaStream_t cs,
     const uint32_t *src[4] = {hp->plist, hp->qlist, hp->hlist, hp->clist};
     const uint32_t *dst[4] = {d.list[0], d.list[1], d.list[2], d.clist};
     for (int k = 0; k < 4; k++) {
+        if (pl->zdev[k]) {  // run-packed: copy the words, k_unpack fills dst
+            ptr[k] = hp->zptr[k];
+            src[k] = hp->zlist[k];
+            dst[k] = pl->zdev[k];
+        }
         if (!ptr[k] || !dst[k] || ptr[k][g1] <= ptr[k][g0])
             continue;
         GC_CHECK(cudaMemcpyAsync(const_cast<uint32_t *>(dst[k]) + ptr[k][g0], src[k] + ptr[k][g0],
@@ -1387,6 +1526,18 @@ int eval_range(grav_plan *pl, size_t c, cudaStream_t st) {
     dp.counters = pl->dp.counters + 4 * c;
     dp.gbegin = pl->chunk_group[c];
     dp.ngroups = pl->chunk_group[c + 1];
+    for (int k = 0; k < 4; k++) {
+        if (!pl->zdev[k])
+            continue;
+        uint32_t *dst = const_cast<uint32_t *>(k < 3 ? pl->dp.list[k] : pl->dp.clist);
+        const int64_t n = dp.ngroups - dp.gbegin;
+        const unsigned blocks = (unsigned)std::max<int64_t>(
+            1, std::min<int64_t>((n + 7) / 8, (int64_t)pl->nsm * 16));
+        k_unpack<<<blocks, 256, 0, st>>>(pl->zdev[k], pl->zptr_dev[k], pl->lptr_dev[k], dp.gbegin,
+                                         dp.ngroups, dst, pl->dp.err);
+        GC_CHECK(cudaGetLastError());
+        pl->launches++;
+    }
     int rc = launch_kind<KH>(pl, dp, st);
     if (!rc)
         rc = launch_kind<KQ>(pl, dp, st);
@@ -1431,6 +1582,8 @@ extern "C" int grav_groups_CUDA(const grav_problem *hp, float *acc_phi) {
     auto chk = [](cudaError_t e, const char *what) {
         return e == cudaSuccess ? 0 : gc::cuda_status(e, what);
     };
+    // one copy stream and one compute stream (ranges alternating over two
+    // compute streams measured no faster: their kernels compete for the SMs)
     cudaStream_t cs = nullptr, st = nullptr;
     std::vector<cudaEvent_t> ev(nc, nullptr);
     int rc = 0;
@@ -1459,6 +1612,8 @@ extern "C" int grav_groups_CUDA(const grav_problem *hp, float *acc_phi) {
     t0 = now_s();
     if (cs)
         cudaStreamSynchronize(cs);
+    if (st)
+        cudaStreamSynchronize(st);
     for (cudaEvent_t x : ev)
         if (x)
             cudaEventDestroy(x);

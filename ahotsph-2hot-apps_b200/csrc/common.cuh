@@ -28,6 +28,7 @@ enum : unsigned {
     GC_DEV_WAIT_TIMEOUT = 1u,   // an mbarrier wait gave up
     GC_DEV_BAD_INDEX = 2u,      // a list entry pointed outside its table
     GC_DEV_BAD_COUNT = 4u,      // a body-run checksum did not match
+    GC_DEV_BAD_RUNS = 8u,       // a run-packed list did not unpack to its group's length
 };
 
 // ------------------------------------------------------------ PTX helpers

@@ -116,6 +116,8 @@ struct nln_tree {
     ListBuf plist;
     ListBuf qlist, hlist;
     ListBuf clist;  // periodic correction list
+    std::vector<int64_t> zptr[4];  // run-packed lists (nln_tree_pack)
+    ListBuf zlist[4];
     std::vector<int64_t> aptr[3];
     std::vector<float> adata[3];
     int64_t counts[4] = {0, 0, 0, 0};
@@ -805,6 +807,10 @@ extern "C" int nln_tree_walk(nln_tree *t) {
         segs.push_back(std::move(S));
     }
     std::memcpy(t->counts, cnt, sizeof(cnt));
+    for (int k = 0; k < 4; k++) {  // packed forms of earlier lists are stale
+        t->zptr[k].clear();
+        t->zlist[k].release();
+    }
     ListBuf *dst[4] = {&t->plist, &t->qlist, &t->hlist, &t->clist};
     for (int k = 0; k < 4; k++) {
         dst[k]->alloc((size_t)t->lptr[k][ng]);
@@ -871,6 +877,73 @@ extern "C" const int64_t *nln_aosoa_ptr(const nln_tree *t, int kind) {
 }
 extern "C" const float *nln_aosoa_data(const nln_tree *t, int kind) {
     return (kind >= 0 && kind < 3 && !t->adata[kind].empty()) ? t->adata[kind].data() : nullptr;
+}
+
+// ---------------------------------------------------------------- run packing
+// Words of one group's packed list; with out != nullptr they are written.
+// A run shorter than 3 entries stays as plain entries (a run word saves
+// nothing there).
+static int64_t pack_group(const uint32_t *e, int64_t n, uint32_t *out) {
+    int64_t w = 0, i = 0;
+    while (i < n) {
+        const uint32_t v = e[i];
+        int64_t j = i + 1;
+        while (j < n && e[j] == v + (uint32_t)(j - i) && (e[j] >> NLN_IDX_BITS) == (v >> NLN_IDX_BITS) &&
+               (uint64_t)(j - i) < (uint64_t)NLN_IDX_MASK)
+            j++;
+        const int64_t len = j - i;
+        if (len >= 3) {
+            if (out) {
+                out[w] = v;
+                out[w + 1] = (NLN_RUN_CODE << NLN_IDX_BITS) | (uint32_t)(len - 1);
+            }
+            w += 2;
+        } else {
+            for (int64_t k = 0; k < len; k++)
+                if (out)
+                    out[w + k] = e[i + k];
+            w += len;
+        }
+        i = j;
+    }
+    return w;
+}
+
+extern "C" int nln_tree_pack(nln_tree *t) {
+    const int64_t ng = (int64_t)t->groups.size();
+    if (ng == 0 || t->lptr[0].empty()) {
+        g_err = "nln_tree_pack: no lists (walk the tree first)";
+        return -1;
+    }
+    const ListBuf *src[4] = {&t->plist, &t->qlist, &t->hlist, &t->clist};
+    for (int k = 0; k < 4; k++) {
+        t->zptr[k].clear();
+        t->zlist[k].release();
+        if (t->lptr[k].empty())
+            continue;
+        const int64_t *ptr = t->lptr[k].data();
+        const uint32_t *e = src[k]->data();
+        std::vector<int64_t> &z = t->zptr[k];
+        z.assign(ng + 1, 0);
+#pragma omp parallel for schedule(dynamic, 1024)
+        for (int64_t g = 0; g < ng; g++) z[g + 1] = pack_group(e + ptr[g], ptr[g + 1] - ptr[g], nullptr);
+        for (int64_t g = 0; g < ng; g++) z[g + 1] += z[g];
+        t->zlist[k].alloc((size_t)z[ng]);
+        uint32_t *out = t->zlist[k].data();
+#pragma omp parallel for schedule(dynamic, 1024)
+        for (int64_t g = 0; g < ng; g++) pack_group(e + ptr[g], ptr[g + 1] - ptr[g], out + z[g]);
+    }
+    return 0;
+}
+
+extern "C" const int64_t *nln_packed_ptr(const nln_tree *t, int kind) {
+    return (kind >= 0 && kind < 4 && !t->zptr[kind].empty()) ? t->zptr[kind].data() : nullptr;
+}
+extern "C" const uint32_t *nln_packed_data(const nln_tree *t, int kind) {
+    return (kind >= 0 && kind < 4) ? t->zlist[kind].data() : nullptr;
+}
+extern "C" int64_t nln_packed_len(const nln_tree *t, int kind) {
+    return (kind >= 0 && kind < 4 && !t->zptr[kind].empty()) ? (int64_t)t->zlist[kind].size() : -1;
 }
 
 // Reference AoSoA blocks (nln/mac.c:117-153) for a subset of groups, packed

@@ -49,7 +49,8 @@ class Problem(ctypes.Structure):
                 ("hlist", ctypes.c_void_p), ("eps2", ctypes.c_double), ("box", ctypes.c_double),
                 ("quad_phi_sign", ctypes.c_float), ("ewald", ctypes.c_int),
                 ("cptr", ctypes.c_void_p), ("clist", ctypes.c_void_p),
-                ("lists_in_host", ctypes.c_int)]
+                ("lists_in_host", ctypes.c_int),
+                ("zptr", ctypes.c_void_p * 4), ("zlist", ctypes.c_void_p * 4)]
 
 
 class Tuning(ctypes.Structure):
@@ -343,9 +344,12 @@ def direct_fp64(points, sinks, eps2, box=0.0):
 
 class PinnedProblem:
     """A tree's tables and lists copied into page-locked host memory, as the
-    host side of an end-to-end grav_groups_CUDA call reads them."""
+    host side of an end-to-end grav_groups_CUDA call reads them.  With
+    packed, the run-packed lists (tree.pack()) stand in for the plain ones;
+    `lists` holds the pinned point, quadrupole and order-4 lists (packed
+    words when packed)."""
 
-    def __init__(self, tree, lists_in_host=False):
+    def __init__(self, tree, lists_in_host=False, packed=False):
         import torch
         self._keep = []
         self.h2d_bytes = 0
@@ -371,13 +375,29 @@ class PinnedProblem:
         p.pptr = pin(t.ptr[0]).ctypes.data
         p.qptr = pin(t.ptr[1]).ctypes.data
         p.hptr = pin(t.ptr[2]).ctypes.data
-        self.lists = [pin(t.plist if len(t.plist) else np.zeros(1, np.uint32)),
-                      pin(t.qlist if has_q else np.zeros(1, np.uint32)),
-                      pin(t.hlist if has_h else np.zeros(1, np.uint32))]
-        p.plist, p.qlist, p.hlist = (a.ctypes.data for a in self.lists)
         if periodic:
             p.cptr = pin(t.ptr[3]).ctypes.data
-            p.clist = pin(t.clist if len(t.clist) else np.zeros(1, np.uint32)).ctypes.data
+        if packed:
+            if lists_in_host:
+                raise ValueError("packed lists are for the copied form")
+            if not hasattr(t, "zlist"):
+                t.pack()
+            self.lists = []
+            for k in range(4):
+                if len(t.zlist[k]) == 0:
+                    self.lists.append(None)
+                    continue
+                p.zptr[k] = pin(t.zptr[k]).ctypes.data
+                self.lists.append(pin(t.zlist[k]))
+                p.zlist[k] = self.lists[-1].ctypes.data
+            self.lists = self.lists[:3]
+        else:
+            self.lists = [pin(t.plist if len(t.plist) else np.zeros(1, np.uint32)),
+                          pin(t.qlist if has_q else np.zeros(1, np.uint32)),
+                          pin(t.hlist if has_h else np.zeros(1, np.uint32))]
+            p.plist, p.qlist, p.hlist = (a.ctypes.data for a in self.lists)
+            if periodic:
+                p.clist = pin(t.clist if len(t.clist) else np.zeros(1, np.uint32)).ctypes.data
         p.quad_phi_sign = 1.0
         p.lists_in_host = int(bool(lists_in_host))
         self.problem = p
@@ -386,8 +406,8 @@ class PinnedProblem:
         self.out = buf.numpy().view(np.float32).reshape(t.n, 4)
 
 
-def pinned_problem(tree, lists_in_host=False):
-    return PinnedProblem(tree, lists_in_host)
+def pinned_problem(tree, lists_in_host=False, packed=False):
+    return PinnedProblem(tree, lists_in_host, packed)
 
 
 def groups_eval_problem(pp, eps2, box, ewald=False):

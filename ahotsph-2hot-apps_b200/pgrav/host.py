@@ -67,6 +67,13 @@ def lib():
         L.nln_tree_merge.argtypes = [vp, ctypes.c_int]
         L.nln_tree_merge.restype = vp
         L.nln_tree_refit.restype = ctypes.c_int
+        L.nln_tree_pack.argtypes = [vp]
+        L.nln_tree_pack.restype = ctypes.c_int
+        for name in ("nln_packed_ptr", "nln_packed_data"):
+            getattr(L, name).argtypes = [vp, ctypes.c_int]
+            getattr(L, name).restype = vp
+        L.nln_packed_len.argtypes = [vp, ctypes.c_int]
+        L.nln_packed_len.restype = ctypes.c_int64
         _lib = L
     return _lib
 
@@ -184,6 +191,26 @@ class Tree:
                 ptr = _view(L.nln_aosoa_ptr(self._h, k), np.int64, ng + 1, self._owner)
                 data = _view(L.nln_aosoa_data(self._h, k), np.float32, int(ptr[-1]) * sz * 8, self._owner)
                 self.aosoa.append((ptr, data))
+
+    def pack(self):
+        """Run-pack the lists (nln_tree_pack; format in nlnlists.h).  Sets
+        zptr[k] (ngroups + 1 word offsets) and zlist[k] (the words) for
+        k = 0 P, 1 Q, 2 H, 3 correction (empty arrays for a kind without
+        lists) and returns self."""
+        L = lib()
+        if L.nln_tree_pack(self._h) != 0:
+            raise RuntimeError(L.nln_last_error().decode())
+        ng = self.ngroups
+        self.zptr, self.zlist = [], []
+        for k in range(4):
+            n = L.nln_packed_len(self._h, k)
+            if n < 0:
+                self.zptr.append(np.zeros(0, np.int64))
+                self.zlist.append(np.zeros(0, np.uint32))
+                continue
+            self.zptr.append(_view(L.nln_packed_ptr(self._h, k), np.int64, ng + 1, self._owner))
+            self.zlist.append(_view(L.nln_packed_data(self._h, k), np.uint32, n, self._owner))
+        return self
 
     def cell_ranges(self):
         """(first, count) body range of every cell, tree order."""

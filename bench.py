@@ -362,6 +362,8 @@ def main():
     ap.add_argument("--workload", default="box256", choices=list(WORKLOADS))
     ap.add_argument("--tol", type=float, default=0.0)
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-plain-lists", action="store_true",
+                    help="end-to-end leg: copy the plain lists instead of the run-packed ones")
     ap.add_argument("--e2e-lists-in-host", action="store_true",
                     help="end-to-end leg: the kernels read the lists in place from page-locked "
                          "host memory instead of the pipelined copy")
@@ -534,8 +536,14 @@ def main():
     # ---- end to end through the C ABI with host buffers (pinned)
     e2e = None
     host = out = None
+    pack_s = None
     if args.e2e_steps > 0:
-        host = gc.pinned_problem(tree, lists_in_host=args.e2e_lists_in_host)
+        packed = not (args.e2e_plain_lists or args.e2e_lists_in_host)
+        if packed:
+            tp = time.perf_counter()
+            tree.pack()   # list building: the walk's lists in run-packed form
+            pack_s = time.perf_counter() - tp
+        host = gc.pinned_problem(tree, lists_in_host=args.e2e_lists_in_host, packed=packed)
         out = host.out
         torch.cuda.synchronize()
         gc.groups_eval_problem(host, eps2, box, ewald=w["ewald"] and box > 0)  # warm-up
@@ -555,9 +563,11 @@ def main():
                "walls_s": walls, "phases_s": phases[mid],
                "lists": ("read by the kernels in place from page-locked host memory over PCIe "
                          "(every step; tables copied at upload)" if args.e2e_lists_in_host else
+                         ("run-packed (nln_tree_pack), " if packed else "plain, ") +
                          "copied from page-locked host memory group range by group range on a "
                          "copy stream, overlapped with the evaluation of the ranges already "
-                         "copied (every step)")}
+                         "copied (every step)" + ("; unpacked on the device" if packed else "")),
+               "host_pack_s": pack_s}
         gc.lib().grav_groups_release_CUDA()  # the end-to-end call's kept list buffer
 
     dropin = None

@@ -175,6 +175,13 @@ typedef struct grav_problem {
                                    point list's interactions are counted as bodies.  The plan
                                    reads them at every evaluation: keep them alive and unchanged
                                    until grav_plan_free.  0: copied to the device at upload. */
+    /* Run-packed lists (nlnlists.h), read by grav_groups_CUDA only: when zlist[k] is set
+       (k = 0 P, 1 Q, 2 H, 3 correction) the call copies these ngroups + 1 word offsets and
+       words instead of the plain list, which it then does not read (may be NULL), and unpacks
+       them on the device; the plain offsets (pptr, qptr, hptr, cptr) are still required.  A
+       group that does not unpack to its plain length fails the call with status -2. */
+    const int64_t *zptr[4];
+    const uint32_t *zlist[4];
 } grav_problem;
 
 typedef struct grav_plan grav_plan;
@@ -224,12 +231,16 @@ void grav_plan_free(grav_plan *plan);
 /*
  * One-call end-to-end form: upload, evaluate, download, free.  acc_phi:
  * host, nbodies x 4 floats, tree order.  Unless lists_in_host is set, the
- * lists are copied group range by group range (about 128 MiB each, at most
- * 32 ranges; the environment variable GRAV_E2E_CHUNKS sets the count) on a
- * copy stream while the kernels evaluate the ranges already copied; list
- * entries are then checked by the kernels as they read them, and a bad one
- * fails the call with status -2 after the evaluation.  Lists in page-locked
- * host memory overlap best.  The call's device buffers come from a memory
+ * lists are copied group range by group range (one per 2 GiB of words
+ * copied, at most 16, the first split in four; the environment variable
+ * GRAV_E2E_CHUNKS sets the count) on a copy stream while the kernels
+ * evaluate the ranges already copied.  Run-packed lists (zptr/zlist) are
+ * copied as packed words and unpacked on the device before each range's
+ * kernels: about 4x fewer bytes over the host link.  List entries are
+ * checked by the kernels as they read them, and a bad one (or a packed
+ * group of the wrong length) fails the call with status -2 after the
+ * evaluation.  Lists in page-locked host memory overlap best.  The call's
+ * device buffers come from a memory
  * pool that keeps freed memory reserved for the next call, until
  * grav_groups_release_CUDA or CUDA_Finalize.
  */

@@ -147,6 +147,18 @@ int nln_tree_refit(nln_tree *t, const float *pos);
 const float *nln_sorted_pos(const nln_tree *t);
 
 /*
+ * Run-pack the walked lists (format in nlnlists.h) of every kind (0 P,
+ * 1 Q, 2 H, 3 correction), group by group in parallel, and keep them beside
+ * the plain lists.  Returns 0, or -1 when the tree has no lists.
+ * nln_packed_ptr: ngroups + 1 word offsets per group (NULL before packing);
+ * nln_packed_data / nln_packed_len: the words.
+ */
+int nln_tree_pack(nln_tree *t);
+const int64_t *nln_packed_ptr(const nln_tree *t, int kind);
+const uint32_t *nln_packed_data(const nln_tree *t, int kind);
+int64_t nln_packed_len(const nln_tree *t, int kind);
+
+/*
  * The periodic correction C(y) = Phi_Ewald(y) + 1/|y| and its first five
  * derivatives (NLN_EWALD_NQ doubles, layout of nlnlists.h) at one
  * displacement y = source - sink in a cube of side L, from the Ewald sum of

@@ -33,6 +33,32 @@ _orc = None
 _ref = None
 
 
+def unpack_runs(zptr, zlist):
+    """Plain list offsets and entries of a run-packed list (format of
+    include/nlnlists.h), decoded on the CPU: an entry word is itself, a run
+    word (image code 31, count n) stands for the n entries after the entry
+    word before it, index + 1 .. + n, same image code."""
+    w = np.asarray(zlist, np.uint32)
+    zptr = np.asarray(zptr, np.int64)
+    is_run = (w >> np.uint32(27)) == 31
+    cnt = np.where(is_run, w & np.uint32((1 << 27) - 1), 1).astype(np.int64)
+    first = np.zeros(len(w), bool)
+    first[zptr[:-1][zptr[:-1] < len(w)]] = True
+    assert not np.any(is_run & first), "a run word starts a group"
+    assert not np.any(is_run[1:] & is_run[:-1]), "a run word follows a run word"
+    end = np.cumsum(cnt)
+    start = end - cnt
+    out = np.empty(int(end[-1]) if len(w) else 0, np.uint32)
+    out[start[~is_run]] = w[~is_run]
+    ri = np.nonzero(is_run)[0]
+    if len(ri):
+        rc = cnt[ri]
+        off = np.arange(rc.sum()) - np.repeat(np.cumsum(rc) - rc, rc) + 1
+        out[np.repeat(start[ri], rc) + off - 1] = np.repeat(w[ri - 1], rc) + off.astype(np.uint32)
+    ptr = np.concatenate([[0], end])[zptr]
+    return ptr, out
+
+
 def build():
     """Compile the restatement (and the reference kernels when the reference tree is present)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)

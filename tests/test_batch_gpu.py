@@ -182,3 +182,56 @@ def test_end_to_end_list_buffer_grows_and_releases(gc, monkeypatch):
     got = gc.groups_eval_problem(gc.pinned_problem(large), 1e-4, 0.0)
     assert np.array_equal(got, refs[id(large)])
     gc.lib().grav_groups_release_CUDA()
+
+
+@pytest.mark.parametrize("chunks", ["1", "3", "7"])
+@pytest.mark.parametrize("kind", ["box", "plummer"])
+def test_run_packed_end_to_end_matches_plan(gc, chunks, kind, monkeypatch):
+    """grav_groups_CUDA given run-packed lists (nln_tree_pack) copies the
+    packed words and unpacks them on the device (k_unpack) before each
+    range's kernels: the results are the plain-list plan's, bit for bit."""
+    if kind == "box":
+        t = make_tree("box", 24 ** 3, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-4)
+        eps2, box, ewald = (1.0 / 24 / 50) ** 2, 1.0, True
+    else:
+        t = make_tree("plummer", 8000, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-4)
+        eps2, box, ewald = 1e-4, 0.0, False
+    plan = gc.Plan(t, eps2, ewald=ewald)
+    plan.eval()
+    ref = plan.download()
+    plan.free()
+    monkeypatch.setenv("GRAV_E2E_CHUNKS", chunks)
+    pp = gc.pinned_problem(t, packed=True)
+    assert pp.problem.plist is None
+    assert pp.h2d_bytes < t.plist.nbytes + t.qlist.nbytes + t.hlist.nbytes + t.clist.nbytes
+    got = gc.groups_eval_problem(pp, eps2, box, ewald=ewald).copy()
+    assert np.array_equal(got, ref)
+    gc.lib().grav_groups_release_CUDA()
+
+
+def test_run_packed_end_to_end_reports_malformed_runs(gc, monkeypatch):
+    """A packed group that unpacks longer or shorter than its plain range, a
+    run word at a group's start and a run word after a run word each fail
+    the call with the device error word; the device writes stay inside each
+    group's range."""
+    t = make_tree("plummer", 6000, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-4)
+    t.pack()
+    monkeypatch.setenv("GRAV_E2E_CHUNKS", "2")
+    z, zp = t.zlist[0], t.zptr[0]
+    runs = np.nonzero((z >> 27) == 31)[0]
+    r = int(runs[len(runs) // 2])
+    g = int(np.searchsorted(zp, r, side="right") - 1)
+    edits = [
+        (r, z[r] + 1),                      # one entry too many
+        (r, z[r] - 1 if (z[r] & 0x7FFFFFF) > 1 else z[r] + 2),   # too few / too many
+        (int(zp[g]), (31 << 27) | 1),       # run word starts the group
+        (r + 1 if r + 1 < zp[g + 1] else r - 1, (31 << 27) | 1),  # run next to a run
+    ]
+    for pos, val in edits:
+        pp = gc.pinned_problem(t, packed=True)
+        pp.lists[0][pos] = val
+        with pytest.raises(gc.GravError, match="device error word"):
+            gc.groups_eval_problem(pp, 1e-4, 0.0)
+        gc.lib().gravcuda_clear_status()
+    gc.groups_eval_problem(gc.pinned_problem(t, packed=True), 1e-4, 0.0)
+    gc.lib().grav_groups_release_CUDA()

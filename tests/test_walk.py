@@ -94,3 +94,46 @@ def test_merge_renumbers_members():
         bo += t.n
         co += t.ncells
         go += t.ngroups
+
+
+def test_run_packed_lists_unpack_to_the_plain_lists():
+    """nln_tree_pack: every kind of list (points, quadrupole, order 4,
+    correction) of an isolated and a periodic tree unpacks, with the CPU
+    decoder, to exactly the plain list and offsets; runs never cross a group
+    or an image-code change, and the point list packs several-fold."""
+    from pgrav import host, ics
+    from oracle import oracle as O
+    pos, m = ics.plummer(6000, seed=8)
+    iso = host.Tree(pos, m, tol=1e-4, p2cut=7, p4cut=20).pack()
+    pos, m = ics.grf_box(20, seed=9, rms_disp=0.3)
+    per = host.Tree(pos, m, tol=1e-4, box=1.0, p2cut=7, p4cut=20).pack()
+    for t in (iso, per):
+        plain = (t.plist, t.qlist, t.hlist, t.clist)
+        for k in range(4):
+            if len(t.ptr[k]) == 0:
+                assert len(t.zlist[k]) == 0
+                continue
+            ptr, lst = O.unpack_runs(t.zptr[k], t.zlist[k])
+            assert np.array_equal(ptr, t.ptr[k]), k
+            assert np.array_equal(lst, plain[k]), k
+            assert len(t.zlist[k]) <= len(plain[k])
+        assert len(t.zlist[0]) * 3 < len(t.plist)
+    # groups with empty lists of a kind keep zero words
+    q = np.diff(per.ptr[1]) == 0
+    assert np.array_equal(np.diff(per.zptr[1])[q], np.zeros(q.sum(), np.int64))
+
+
+def test_unpack_rejects_malformed_runs():
+    """The CPU decoder (the device unpacker's checker) refuses a run word at
+    a group's start and a run word after a run word."""
+    import pytest
+    from oracle import oracle as O
+    run = lambda n: (31 << 27) | n
+    e = (13 << 27) | 100
+    ptr, lst = O.unpack_runs([0, 3], np.array([e, run(4), e + 20], np.uint32))
+    assert ptr.tolist() == [0, 6]
+    assert lst.tolist() == [e, e + 1, e + 2, e + 3, e + 4, e + 20]
+    with pytest.raises(AssertionError, match="starts a group"):
+        O.unpack_runs([0, 1, 3], np.array([e, run(2), e], np.uint32))
+    with pytest.raises(AssertionError, match="follows a run word"):
+        O.unpack_runs([0, 3], np.array([e, run(2), run(1)], np.uint32))
