@@ -64,42 +64,28 @@ __device__ __forceinline__ void stage_hexa(float *o, float R, const float *q3, c
     o[31] = 0.0f;
 }
 
-// Monopole term.  Returns ri (1/r) and ri2 for the higher orders.
+// Monopole term: its potential pm and radial coefficient kr (the term adds
+// pm to phi and d * kr to the acceleration), and ri = 1/r, ri2 for the
+// higher orders.
 template <int SOFT>
-__device__ __forceinline__ void mono(float x, float y, float z, float m, float e, Acc4 &a,
-                                     float &ri, float &ri2) {
-    if (SOFT == SOFT_PLUMMER) {
+__device__ __forceinline__ void mono_terms(float x, float y, float z, float m, float e, float &pm,
+                                           float &kr, float &ri, float &ri2) {
+    if (SOFT == SOFT_PLUMMER || SOFT == SOFT_NONE) {
         // nln/do_grav_avx8.c:2181-2210, e = eps^2
-        float r2 = fmaf(x, x, fmaf(y, y, fmaf(z, z, e)));
+        float r2 = fmaf(x, x, fmaf(y, y, SOFT == SOFT_PLUMMER ? fmaf(z, z, e) : z * z));
         ri = rsqrt_fast(r2);
         ri2 = ri * ri;
         float mri = m * ri;
-        float mri3 = mri * ri2;
-        a.phi -= mri;
-        a.ax = fmaf(-x, mri3, a.ax);
-        a.ay = fmaf(-y, mri3, a.ay);
-        a.az = fmaf(-z, mri3, a.az);
-    } else if (SOFT == SOFT_NONE) {
-        float r2 = fmaf(x, x, fmaf(y, y, z * z));
-        ri = rsqrt_fast(r2);
-        ri2 = ri * ri;
-        float mri = m * ri;
-        float mri3 = mri * ri2;
-        a.phi -= mri;
-        a.ax = fmaf(-x, mri3, a.ax);
-        a.ay = fmaf(-y, mri3, a.ay);
-        a.az = fmaf(-z, mri3, a.az);
+        pm = -mri;
+        kr = -mri * ri2;
     } else if (SOFT == SOFT_MASKED) {
         // do_grav_avx8: pairs closer than e contribute nothing (nln/do_grav_avx8.c:978-990)
         float r2 = fmaf(x, x, fmaf(y, y, z * z));
         ri = (r2 >= e * e) ? rsqrt_fast(r2) : 0.0f;
         ri2 = ri * ri;
         float mri = m * ri;
-        float mri3 = mri * ri2;
-        a.phi -= mri;
-        a.ax = fmaf(-x, mri3, a.ax);
-        a.ay = fmaf(-y, mri3, a.ay);
-        a.az = fmaf(-z, mri3, a.az);
+        pm = -mri;
+        kr = -mri * ri2;
     } else {
         // Dehnen K1 inside r < eps, e = 1/eps (nln/do_grav_avx8.c:1013-1045, nln/pgrav.cu:441-461)
         float r2 = fmaf(x, x, fmaf(y, y, z * z));
@@ -115,36 +101,37 @@ __device__ __forceinline__ void mono(float x, float y, float z, float m, float e
             af = ri * ri * ri;
         }
         ri2 = ri * ri;
-        a.phi = fmaf(-m, pf, a.phi);
-        float maf = m * af;
-        a.ax = fmaf(-x, maf, a.ax);
-        a.ay = fmaf(-y, maf, a.ay);
-        a.az = fmaf(-z, maf, a.az);
+        pm = -m * pf;
+        kr = -m * af;
     }
 }
 
-// Quadrupole term; qsh = quadrupole potential sign times 1/2.
-__device__ __forceinline__ void quad(float x, float y, float z, const float *__restrict__ r,
-                                     float ri, float ri2, float qsh, Acc4 &a, float &ri5) {
-    const float4 q0 = *reinterpret_cast<const float4 *>(r + 4);  // Qxx Qxy Qyy Qxz
-    const float2 q1 = *reinterpret_cast<const float2 *>(r + 8);  // Qyz Qzz
-    float Qx = fmaf(q0.x, x, fmaf(q0.y, y, q0.w * z));
-    float Qy = fmaf(q0.y, x, fmaf(q0.z, y, q1.x * z));
-    float Qz = fmaf(q0.w, x, fmaf(q1.x, y, q1.y * z));
-    float dQd = fmaf(x, Qx, fmaf(y, Qy, z * Qz));
-    float ri3 = ri * ri2;
-    ri5 = ri3 * ri2;
-    float eqd = ri5 * dQd;                  // eq . d
-    a.phi = fmaf(qsh, eqd, a.phi);
-    float k = 2.5f * eqd * ri2;             // 5 * (1/2) eq.d / r^2
-    a.ax = fmaf(x, k, fmaf(-ri5, Qx, a.ax));
-    a.ay = fmaf(y, k, fmaf(-ri5, Qy, a.ay));
-    a.az = fmaf(z, k, fmaf(-ri5, Qz, a.az));
+template <int SOFT>
+__device__ __forceinline__ void mono(float x, float y, float z, float m, float e, Acc4 &a,
+                                     float &ri, float &ri2) {
+    float pm, kr;
+    mono_terms<SOFT>(x, y, z, m, e, pm, kr, ri, ri2);
+    a.phi += pm;
+    a.ax = fmaf(x, kr, a.ax);
+    a.ay = fmaf(y, kr, a.ay);
+    a.az = fmaf(z, kr, a.az);
 }
 
-// Octupole + hexadecapole terms (nln/do_grav_avx8.c:1853-1898).
-__device__ __forceinline__ void hexa(float x, float y, float z, const float *__restrict__ r,
-                                     float ri2, float ri5, Acc4 &a) {
+// Quadrupole contraction: Q.d and d.Q.d.
+__device__ __forceinline__ void quad_vec(float x, float y, float z, const float *__restrict__ r,
+                                         float &Qx, float &Qy, float &Qz, float &dQd) {
+    const float4 q0 = *reinterpret_cast<const float4 *>(r + 4);  // Qxx Qxy Qyy Qxz
+    const float2 q1 = *reinterpret_cast<const float2 *>(r + 8);  // Qyz Qzz
+    Qx = fmaf(q0.x, x, fmaf(q0.y, y, q0.w * z));
+    Qy = fmaf(q0.y, x, fmaf(q0.z, y, q1.x * z));
+    Qz = fmaf(q0.w, x, fmaf(q1.x, y, q1.y * z));
+    dQd = fmaf(x, Qx, fmaf(y, Qy, z * Qz));
+}
+
+// Octupole and hexadecapole contractions with d^2 and d^3 (e, h) and their
+// products with d (nln/do_grav_avx8.c:1853-1898), traceless moments.
+__device__ __forceinline__ void hexa_vec(float x, float y, float z, const float *__restrict__ r,
+                                         float e[3], float &d3, float h[3], float &d4) {
     const float4 o0 = *reinterpret_cast<const float4 *>(r + 12);  // Oxxx Oxxy Oxyy Oyyy
     const float4 o1 = *reinterpret_cast<const float4 *>(r + 16);  // Oxxz Oxyz Oyyz S1
     const float4 o2 = *reinterpret_cast<const float4 *>(r + 20);  // S2 Xxxxx Xxxxy Xxxyy
@@ -159,50 +146,63 @@ __device__ __forceinline__ void hexa(float x, float y, float z, const float *__r
     float yyz = z * fmaf(zz, -third, yy);
     xx -= zz;
     yy -= zz;
-    // octupole
-    float e0 = fmaf(o0.x, xx, fmaf(o0.z, yy, fmaf(o0.y, xy, fmaf(o1.x, xz, o1.y * yz))));
-    float e1 = fmaf(o0.z, xy, fmaf(o0.y, xx, fmaf(o0.w, yy, fmaf(o1.z, yz, o1.y * xz))));
-    float e2 = fmaf(-o1.w, xz, fmaf(-o2.x, yz, fmaf(o1.x, xx, fmaf(o1.z, yy, o1.y * xy))));
-    float ri7 = ri5 * ri2;
-    float eqd = ri7 * fmaf(x, e0, fmaf(y, e1, z * e2));
-    a.phi = fmaf(third, eqd, a.phi);
-    float k = (7.0f / 3.0f) * eqd * ri2;
-    a.ax = fmaf(x, k, fmaf(-ri7, e0, a.ax));
-    a.ay = fmaf(y, k, fmaf(-ri7, e1, a.ay));
-    a.az = fmaf(z, k, fmaf(-ri7, e2, a.az));
-    // hexadecapole
+    e[0] = fmaf(o0.x, xx, fmaf(o0.z, yy, fmaf(o0.y, xy, fmaf(o1.x, xz, o1.y * yz))));
+    e[1] = fmaf(o0.z, xy, fmaf(o0.y, xx, fmaf(o0.w, yy, fmaf(o1.z, yz, o1.y * xz))));
+    e[2] = fmaf(-o1.w, xz, fmaf(-o2.x, yz, fmaf(o1.x, xx, fmaf(o1.z, yy, o1.y * xy))));
+    d3 = fmaf(x, e[0], fmaf(y, e[1], z * e[2]));
     float xxy = y * xx, xyy = x * yy, xyz = xy * z;
     // X order: xxxx(o2.y) xxxy(o2.z) xxyy(o2.w) xyyy(x0.x) yyyy(x0.y) xxxz(x0.z) xxyz(x0.w)
     //          xyyz(x1.x) yyyz(x1.y), XS = xyyy + xxxy (x1.z)
-    float h0 = fmaf(o2.y, xxx, fmaf(x0.x, yyy, fmaf(o2.z, xxy, fmaf(x0.z, xxz,
-               fmaf(o2.w, xyy, fmaf(x0.w, xyz, x1.x * yyz))))));
-    float h1 = fmaf(x0.x, xyy, fmaf(o2.z, xxx, fmaf(x0.y, yyy, fmaf(x1.y, yyz,
-               fmaf(o2.w, xxy, fmaf(x0.w, xxz, x1.x * xyz))))));
-    float h2 = fmaf(-o2.y, xxz, fmaf(-x1.z, xyz, fmaf(-x0.y, yyz, fmaf(x0.z, xxx,
-               fmaf(x1.y, yyy, fmaf(-o2.w, xxz + yyz, fmaf(x0.w, xxy, x1.x * xyy)))))));
-    float ri9 = ri7 * ri2;
-    float hqd = ri9 * fmaf(x, h0, fmaf(y, h1, z * h2));
-    a.phi = fmaf(0.25f, hqd, a.phi);
-    float kh = 2.25f * hqd * ri2;
-    a.ax = fmaf(x, kh, fmaf(-ri9, h0, a.ax));
-    a.ay = fmaf(y, kh, fmaf(-ri9, h1, a.ay));
-    a.az = fmaf(z, kh, fmaf(-ri9, h2, a.az));
+    h[0] = fmaf(o2.y, xxx, fmaf(x0.x, yyy, fmaf(o2.z, xxy, fmaf(x0.z, xxz,
+           fmaf(o2.w, xyy, fmaf(x0.w, xyz, x1.x * yyz))))));
+    h[1] = fmaf(x0.x, xyy, fmaf(o2.z, xxx, fmaf(x0.y, yyy, fmaf(x1.y, yyz,
+           fmaf(o2.w, xxy, fmaf(x0.w, xxz, x1.x * xyz))))));
+    h[2] = fmaf(-o2.y, xxz, fmaf(-x1.z, xyz, fmaf(-x0.y, yyz, fmaf(x0.z, xxx,
+           fmaf(x1.y, yyy, fmaf(-o2.w, xxz + yyz, fmaf(x0.w, xxy, x1.x * xyy)))))));
+    d4 = fmaf(x, h[0], fmaf(y, h[1], z * h[2]));
 }
 
 // One staged record of order ORDER (0, 2, 4) against a sink at (sx, sy, sz).
+// The orders' terms are summed before they reach the accumulators: with
+// eq_l = r^-(2l+1) (moment contracted with d^(l-1)),
+//     phi += pm + qsh eq_2.d + eq_3.d/3 + eq_4.d/4
+//     a   += d (kr + r^-2 (5 qsh' eq_2.d + 7/3 eq_3.d + 9/4 eq_4.d)) - (eq_2 + eq_3 + eq_4)
+// (qsh' = 1/2: the acceleration does not take the potential's sign
+// convention) and eq_2 + eq_3 + eq_4 = r^-5 (Q.d + r^-2 (e + r^-2 h)).
 template <int ORDER, int SOFT>
 __device__ __forceinline__ void interact(const float *__restrict__ r, float sx, float sy,
                                          float sz, float e, float qsh, Acc4 &a) {
     const float4 p = *reinterpret_cast<const float4 *>(r);
     float x = sx - p.x, y = sy - p.y, z = sz - p.z;
     float ri, ri2;
-    mono<SOFT>(x, y, z, p.w, e, a, ri, ri2);
-    if (ORDER >= 2) {
-        float ri5;
-        quad(x, y, z, r, ri, ri2, qsh, a, ri5);
-        if (ORDER >= 4)
-            hexa(x, y, z, r, ri2, ri5, a);
+    if (ORDER == 0) {
+        mono<SOFT>(x, y, z, p.w, e, a, ri, ri2);
+        return;
     }
+    float pm, kr;
+    mono_terms<SOFT>(x, y, z, p.w, e, pm, kr, ri, ri2);
+    float Qx, Qy, Qz, dQd;
+    quad_vec(x, y, z, r, Qx, Qy, Qz, dQd);
+    const float ri5 = ri * ri2 * ri2;
+    const float eqd2 = ri5 * dQd;
+    float tx = Qx, ty = Qy, tz = Qz, K;
+    if (ORDER >= 4) {
+        float ev[3], hv[3], d3, d4;
+        hexa_vec(x, y, z, r, ev, d3, hv, d4);
+        const float ri7 = ri5 * ri2, ri9 = ri7 * ri2;
+        const float eqd3 = ri7 * d3, eqd4 = ri9 * d4;
+        a.phi = fmaf(0.25f, eqd4, fmaf(1.0f / 3.0f, eqd3, fmaf(qsh, eqd2, a.phi + pm)));
+        K = fmaf(ri2, fmaf(2.25f, eqd4, fmaf(7.0f / 3.0f, eqd3, 2.5f * eqd2)), kr);
+        tx = fmaf(ri2, fmaf(ri2, hv[0], ev[0]), Qx);
+        ty = fmaf(ri2, fmaf(ri2, hv[1], ev[1]), Qy);
+        tz = fmaf(ri2, fmaf(ri2, hv[2], ev[2]), Qz);
+    } else {
+        a.phi = fmaf(qsh, eqd2, a.phi + pm);
+        K = fmaf(2.5f * ri2, eqd2, kr);
+    }
+    a.ax = fmaf(x, K, fmaf(-ri5, tx, a.ax));
+    a.ay = fmaf(y, K, fmaf(-ri5, ty, a.ay));
+    a.az = fmaf(z, K, fmaf(-ri5, tz, a.az));
 }
 
 // Two point records against one sink with Blackwell's paired FP32
