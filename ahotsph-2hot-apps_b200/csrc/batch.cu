@@ -77,18 +77,26 @@ struct DevProblem {
     float ew_trace;            // trace of the Hessian of C: -4 pi / L^3
 };
 
-template <int KIND>
+template <int KIND, bool PAIRED = false>
 struct KindOf {
     static constexpr int rec_bytes = KIND == KP ? 16 : (KIND == KQ ? 64 : 128);
     static constexpr int order = KIND == KP ? 0 : (KIND == KQ ? 2 : 4);
-    // pipeline depth: short per-record work needs more copies in flight
-    static constexpr int stages = KIND == KP ? 4 : (KIND == KQ ? 3 : 2);
+    // pipeline depth: short per-record work needs more copies in flight; the
+    // paired order-4 path frees its one stage as soon as the tile is
+    // re-laid into the pair buffer, so the next copy overlaps the compute
+    static constexpr int stages = PAIRED ? 1 : (KIND == KP ? 4 : (KIND == KQ ? 3 : 2));
     // one TMA row gather brings 4 records; each lands 128-byte aligned
     static constexpr int group_bytes = 4 * rec_bytes < 128 ? 128 : 4 * rec_bytes;
     static constexpr int stage_bytes = (TILE / 4) * group_bytes;
-    // per-warp shared memory: stages of 32 records, mbarriers, image codes
+    // paired order-4 tile: 16 record pairs of 32 interleaved fields, one pair
+    // every 68 floats (16-byte aligned; the re-lay's 8-byte stores of a
+    // half-warp hit distinct banks)
+    static constexpr int pair_stride = 68;
+    static constexpr int pair_bytes = PAIRED ? (TILE / 2) * pair_stride * 4 : 0;
+    // per-warp shared memory: stages of 32 records, the pair buffer,
+    // mbarriers, image codes
     static constexpr int warp_bytes =
-        (stages * stage_bytes + stages * 8 + stages * TILE * 4 + 127) / 128 * 128;
+        (stages * stage_bytes + pair_bytes + stages * 8 + stages * TILE * 4 + 127) / 128 * 128;
     // byte offset of record r inside a stage
     static __device__ __forceinline__ int rec_off(int r) {
         return (r >> 2) * group_bytes + (r & 3) * rec_bytes;
@@ -308,10 +316,77 @@ __global__ void k_stage_cells(const nln_qcell *__restrict__ qc, const nln_hcell 
     }
 }
 
+// Re-lay this lane's pre-staged order-4 record (just landed by TMA at its
+// stage slot) into the pair-interleaved tile of hexa2_plummer: header
+// re-centred on the group centre c in the record's image, the octupole and
+// four hexadecapole fields negated as that layout wants.  A lane past the
+// tile's end writes a massless, momentless record far away, which adds
+// exactly zero.  Lanes 2p and 2p+1 write pair p: one shuffle per field pair.
+__device__ __forceinline__ void relay_pairs(const unsigned char *stage, uint32_t code, bool valid,
+                                            const double *c, double box, float *pbuf, int lane) {
+    using K = KindOf<KH, true>;
+    float g[32];
+    if (valid) {
+        const float4 *src = reinterpret_cast<const float4 *>(stage + K::rec_off(lane));
+        float f[32];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const float4 v = src[k];
+            f[4 * k] = v.x;
+            f[4 * k + 1] = v.y;
+            f[4 * k + 2] = v.z;
+            f[4 * k + 3] = v.w;
+        }
+        double sx, sy, sz;
+        decode_shift(code, box, sx, sy, sz);
+        const double cx = __hiloint2double(__float_as_int(f[1]), __float_as_int(f[0]));
+        const double cy = __hiloint2double(__float_as_int(f[3]), __float_as_int(f[2]));
+        const double cz = __hiloint2double(__float_as_int(f[11]), __float_as_int(f[10]));
+        g[0] = (float)(cx + sx - c[0]);
+        g[1] = (float)(cy + sy - c[1]);
+        g[2] = (float)(cz + sz - c[2]);
+        g[3] = f[31];
+#pragma unroll
+        for (int k = 4; k < 10; k++) g[k] = f[k];
+        g[10] = -f[21];
+        g[11] = -f[25];
+#pragma unroll
+        for (int k = 12; k < 19; k++) g[k] = -f[k];
+        g[19] = f[19];
+        g[20] = f[20];
+#pragma unroll
+        for (int k = 21; k < 30; k++) g[k] = f[k];
+        g[30] = -f[30];
+        g[31] = -f[23];
+    } else {
+#pragma unroll
+        for (int k = 0; k < 32; k++) g[k] = k < 3 ? 1.0e3f : 0.f;
+    }
+    const int s = lane & 1;
+    float *dst = pbuf + (lane >> 1) * K::pair_stride + 2 * s;
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const float send = s ? g[2 * q] : g[2 * q + 1];
+        const float recv = __shfl_xor_sync(0xffffffffu, send, 1);
+        *reinterpret_cast<float2 *>(dst + 4 * q) =
+            s ? make_float2(recv, g[2 * q + 1]) : make_float2(g[2 * q], recv);
+    }
+}
+
+#ifndef GRAV_H2_UNROLL
+#define GRAV_H2_UNROLL 1
+#endif
+#ifndef GRAV_H2_MINB
+#define GRAV_H2_MINB 3
+#endif
+constexpr int kH2Unroll = GRAV_H2_UNROLL;
 template <int KIND, bool STAGED>
-__global__ void __launch_bounds__(256) k_batch(const __grid_constant__ CUtensorMap tmap,
+__global__ void __launch_bounds__(256, KIND == KH ? (STAGED ? GRAV_H2_MINB : 3) : 0) k_batch(const __grid_constant__ CUtensorMap tmap,
                                                DevProblem P) {
-    using K = KindOf<KIND>;
+    // staged order-4 tables run the paired (f32x2) interaction on a
+    // pair-interleaved copy of each tile
+    constexpr bool PAIRED = KIND == KH && STAGED;
+    using K = KindOf<KIND, PAIRED>;
     constexpr int RB = K::rec_bytes;
     constexpr int ORDER = K::order;
     constexpr int NST = K::stages;
@@ -319,7 +394,8 @@ __global__ void __launch_bounds__(256) k_batch(const __grid_constant__ CUtensorM
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     unsigned char *wbuf = smem + (size_t)wib * K::warp_bytes;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(wbuf + NST * K::stage_bytes);
+    float *pbuf = reinterpret_cast<float *>(wbuf + NST * K::stage_bytes);  // paired path
+    uint64_t *bar = reinterpret_cast<uint64_t *>(wbuf + NST * K::stage_bytes + K::pair_bytes);
     uint32_t *codes = reinterpret_cast<uint32_t *>(bar + NST);  // [NST][TILE] image codes
     if (lane == 0) {
         for (int s = 0; s < NST; s++) mbar_init(&bar[s], 1);
@@ -390,16 +466,20 @@ __global__ void __launch_bounds__(256) k_batch(const __grid_constant__ CUtensorM
                     tma_gather4(dst + g * K::group_bytes, &tmap, r0, r1, r2, r3, &bar[st]);
             }
         };
+        // tiles in flight ahead of the one being computed
+        constexpr int AHEAD = PAIRED ? 1 : NST - 1;
 #pragma unroll
-        for (int p = 0; p < NST - 1; p++)
+        for (int p = 0; p < AHEAD; p++)
             if (p < ntile)
                 issue(p, fetch(p), tseq + p);
-        uint32_t ent_next = fetch(NST - 1);
+        uint32_t ent_next = fetch(AHEAD);
         for (int t = 0; t < ntile; t++) {
             const uint32_t seq = tseq + t;
-            if (t + NST - 1 < ntile)
-                issue(t + NST - 1, ent_next, seq + NST - 1);
-            ent_next = fetch(t + NST);
+            if (!PAIRED) {
+                if (t + NST - 1 < ntile)
+                    issue(t + NST - 1, ent_next, seq + NST - 1);
+                ent_next = fetch(t + NST);
+            }
             const int nt = (int)min((int64_t)TILE, nent - (int64_t)t * TILE);
             const uint32_t st = seq % NST;
             bool ok = mbar_wait_bounded(&bar[st], (seq / NST) & 1, P.err);
@@ -412,10 +492,33 @@ __global__ void __launch_bounds__(256) k_batch(const __grid_constant__ CUtensorM
                 break;
             }
             unsigned char *bt = wbuf + st * K::stage_bytes;
+            Acc4 a{0.f, 0.f, 0.f, 0.f};
+            if (PAIRED) {
+                relay_pairs(bt, codes[st * TILE + lane], lane < nt, c, P.box, pbuf, lane);
+                __syncwarp();  // the stage is free: start the next copy, then compute
+                if (t + 1 < ntile)
+                    issue(t + 1, ent_next, seq + 1);
+                ent_next = fetch(t + 2);
+                const float2 nsx = splat2(-ux), nsy = splat2(-uy), nsz = splat2(-uz);
+                const float2 e2 = splat2(P.eps2), nqsh = splat2(-P.qsh);
+                Acc2h A{splat2(0.f), splat2(0.f), splat2(0.f), splat2(0.f)};
+                const int npair = (nt + 1) >> 1;
+                if (npair == TILE / 2) {
+#pragma unroll kH2Unroll
+                    for (int q = 0; q < TILE / 2; q++)
+                        hexa2_plummer(pbuf + q * K::pair_stride, nsx, nsy, nsz, e2, nqsh, A);
+                } else {
+                    for (int q = 0; q < npair; q++)
+                        hexa2_plummer(pbuf + q * K::pair_stride, nsx, nsy, nsz, e2, nqsh, A);
+                }
+                a.ax = A.ax.x + A.ax.y;
+                a.ay = A.ay.x + A.ay.y;
+                a.az = A.az.x + A.az.y;
+                a.phi = -(A.nphi.x + A.nphi.y);
+            } else {
             if (lane < nt)
                 convert<KIND, STAGED>(bt + K::rec_off(lane), codes[st * TILE + lane], c, P.box);
             __syncwarp();
-            Acc4 a{0.f, 0.f, 0.f, 0.f};
             if (nt == TILE) {
 #pragma unroll 4
                 for (int r = 0; r < TILE; r++)
@@ -425,6 +528,7 @@ __global__ void __launch_bounds__(256) k_batch(const __grid_constant__ CUtensorM
                 for (int r = 0; r < nt; r++)
                     interact<ORDER, SOFT_PLUMMER>(reinterpret_cast<const float *>(bt + K::rec_off(r)),
                                                   ux, uy, uz, P.eps2, P.qsh, a);
+            }
             }
             comp_add(hi[0], lo[0], a.ax);
             comp_add(hi[1], lo[1], a.ay);
@@ -1289,7 +1393,8 @@ int launch_kind(grav_plan *pl, const DevProblem &dp, cudaStream_t st) {
         pl->launches++;
         return 0;
     }
-    const size_t smem = (size_t)wpb * KindOf<KIND>::warp_bytes;
+    const size_t smem = (size_t)wpb * (pl->staged ? KindOf<KIND, KIND == KH>::warp_bytes
+                                                  : KindOf<KIND>::warp_bytes);
     auto kern = pl->staged ? k_batch<KIND, true> : k_batch<KIND, false>;
     GC_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int fit = 0;

@@ -229,3 +229,113 @@ __device__ __forceinline__ void mono2_plummer(float2 npx, float2 npy, float2 npz
     acc.nay = __ffma2_rn(dy, mri3, acc.nay);
     acc.naz = __ffma2_rn(dz, mri3, acc.naz);
 }
+
+// Two order-4 records against one sink with the paired FP32 instructions,
+// on a pair-interleaved tile: field f of records a (.x) and b (.y) sits at
+// floats 2f, 2f+1 of the pair.  Fields: 0-2 position (group-centred), 3
+// mass, 4-9 Q as in the staged record, 10 -Xxxxx, 11 -Xyyyy, 12-18 -O (the
+// octupole negated), 19-20 the octupole sums (not negated), 21-29 X, 30 -XS,
+// 31 -Xxxyy.  Working in v = source - sink = -d with those signs folded in
+// leaves no negation in the loop:
+//   e'(v) = -O:vv (so v.e' = d.e), h(v) = -h(d), U = Q.v + r^-2 (e' + r^-2 h),
+//   a   = v (m/r^3 - r^-2 (5/2 eq_2.d + 7/3 eq_3.d + 9/4 eq_4.d)) + r^-5 U,
+//   -phi = m/r - qsh eq_2.d - eq_3.d/3 - eq_4.d/4   (accumulated negated),
+// the terms of interact<4, SOFT_PLUMMER> in another order, element by element.
+struct Acc2h {
+    float2 ax, ay, az, nphi;
+};
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 splat2(float a) { return make_float2(a, a); }
+
+__device__ __forceinline__ void hexa2_plummer(const float *__restrict__ pr, float2 nsx, float2 nsy,
+                                              float2 nsz, float2 eps2, float2 nqsh, Acc2h &A) {
+    const float4 *q = reinterpret_cast<const float4 *>(pr);
+    float4 w = q[0];
+    const float2 vx = __fadd2_rn(f2(w.x, w.y), nsx);
+    const float2 vy = __fadd2_rn(f2(w.z, w.w), nsy);
+    w = q[1];
+    const float2 vz = __fadd2_rn(f2(w.x, w.y), nsz);
+    const float2 m = f2(w.z, w.w);
+    // monopole
+    const float2 r2 = __ffma2_rn(vx, vx, __ffma2_rn(vy, vy, __ffma2_rn(vz, vz, eps2)));
+    const float2 ri = f2(rsqrt_fast(r2.x), rsqrt_fast(r2.y));
+    const float2 ri2 = __fmul2_rn(ri, ri);
+    const float2 mri3 = __fmul2_rn(__fmul2_rn(m, ri), ri2);
+    A.nphi = __ffma2_rn(m, ri, A.nphi);
+    // quadrupole
+    w = q[2];
+    const float2 Qxx = f2(w.x, w.y), Qxy = f2(w.z, w.w);
+    w = q[3];
+    const float2 Qyy = f2(w.x, w.y), Qxz = f2(w.z, w.w);
+    w = q[4];
+    const float2 Qyz = f2(w.x, w.y), Qzz = f2(w.z, w.w);
+    float2 Ux = __ffma2_rn(Qxx, vx, __ffma2_rn(Qxy, vy, __fmul2_rn(Qxz, vz)));
+    float2 Uy = __ffma2_rn(Qxy, vx, __ffma2_rn(Qyy, vy, __fmul2_rn(Qyz, vz)));
+    float2 Uz = __ffma2_rn(Qxz, vx, __ffma2_rn(Qyz, vy, __fmul2_rn(Qzz, vz)));
+    const float2 vQv = __ffma2_rn(vx, Ux, __ffma2_rn(vy, Uy, __fmul2_rn(vz, Uz)));
+    const float2 ri5 = __fmul2_rn(__fmul2_rn(ri, ri2), ri2);
+    const float2 eqd2 = __fmul2_rn(ri5, vQv);
+    // monomials of v (hexa_vec's, with -zz in place of zz)
+    const float2 third = splat2(1.0f / 3.0f);
+    float2 xx = __fmul2_rn(__fmul2_rn(splat2(0.5f), vx), vx);
+    float2 yy = __fmul2_rn(__fmul2_rn(splat2(0.5f), vy), vy);
+    const float2 nzz = __fmul2_rn(__fmul2_rn(splat2(-0.5f), vz), vz);
+    const float2 xy = __fmul2_rn(vx, vy), xz = __fmul2_rn(vx, vz), yz = __fmul2_rn(vy, vz);
+    const float2 xxx = __fmul2_rn(vx, __ffma2_rn(xx, third, nzz));
+    const float2 xxz = __fmul2_rn(vz, __ffma2_rn(nzz, third, xx));
+    const float2 yyy = __fmul2_rn(vy, __ffma2_rn(yy, third, nzz));
+    const float2 yyz = __fmul2_rn(vz, __ffma2_rn(nzz, third, yy));
+    xx = __fadd2_rn(xx, nzz);
+    yy = __fadd2_rn(yy, nzz);
+    // octupole (negated moments): e' and d3 = v.e'
+    w = q[6];
+    const float2 O0 = f2(w.x, w.y), O1 = f2(w.z, w.w);  // Oxxx Oxxy
+    w = q[7];
+    const float2 O2 = f2(w.x, w.y), O3 = f2(w.z, w.w);  // Oxyy Oyyy
+    w = q[8];
+    const float2 O4 = f2(w.x, w.y), O5 = f2(w.z, w.w);  // Oxxz Oxyz
+    w = q[9];
+    const float2 O6 = f2(w.x, w.y), S1 = f2(w.z, w.w);  // Oyyz, Oxxx+Oxyy
+    w = q[10];
+    const float2 S2 = f2(w.x, w.y), X0 = f2(w.z, w.w);  // Oxxy+Oyyy, Xxxxx
+    const float2 e0 = __ffma2_rn(O0, xx, __ffma2_rn(O2, yy, __ffma2_rn(O1, xy, __ffma2_rn(O4, xz, __fmul2_rn(O5, yz)))));
+    const float2 e1 = __ffma2_rn(O2, xy, __ffma2_rn(O1, xx, __ffma2_rn(O3, yy, __ffma2_rn(O6, yz, __fmul2_rn(O5, xz)))));
+    const float2 e2 = __ffma2_rn(S1, xz, __ffma2_rn(S2, yz, __ffma2_rn(O4, xx, __ffma2_rn(O6, yy, __fmul2_rn(O5, xy)))));
+    const float2 d3 = __ffma2_rn(vx, e0, __ffma2_rn(vy, e1, __fmul2_rn(vz, e2)));
+    // hexadecapole: h(v) and d4 = v.h
+    w = q[11];
+    const float2 X1 = f2(w.x, w.y), X2 = f2(w.z, w.w);  // Xxxxy Xxxyy
+    w = q[12];
+    const float2 X3 = f2(w.x, w.y), X4 = f2(w.z, w.w);  // Xxyyy Xyyyy
+    w = q[13];
+    const float2 X5 = f2(w.x, w.y), X6 = f2(w.z, w.w);  // Xxxxz Xxxyz
+    w = q[14];
+    const float2 X7 = f2(w.x, w.y), X8 = f2(w.z, w.w);  // Xxyyz Xyyyz
+    w = q[15];
+    const float2 nXS = f2(w.x, w.y), nX2 = f2(w.z, w.w);
+    w = q[5];
+    const float2 nX0 = f2(w.x, w.y), nX4 = f2(w.z, w.w);
+    const float2 xxy = __fmul2_rn(vy, xx), xyy = __fmul2_rn(vx, yy), xyz = __fmul2_rn(xy, vz);
+    const float2 h0 = __ffma2_rn(X0, xxx, __ffma2_rn(X3, yyy, __ffma2_rn(X1, xxy, __ffma2_rn(X5, xxz,
+                      __ffma2_rn(X2, xyy, __ffma2_rn(X6, xyz, __fmul2_rn(X7, yyz)))))));
+    const float2 h1 = __ffma2_rn(X3, xyy, __ffma2_rn(X1, xxx, __ffma2_rn(X4, yyy, __ffma2_rn(X8, yyz,
+                      __ffma2_rn(X2, xxy, __ffma2_rn(X6, xxz, __fmul2_rn(X7, xyz)))))));
+    const float2 h2 = __ffma2_rn(nX0, xxz, __ffma2_rn(nXS, xyz, __ffma2_rn(nX4, yyz, __ffma2_rn(X5, xxx,
+                      __ffma2_rn(X8, yyy, __ffma2_rn(nX2, __fadd2_rn(xxz, yyz), __ffma2_rn(X6, xxy,
+                      __fmul2_rn(X7, xyy))))))));
+    const float2 d4 = __ffma2_rn(vx, h0, __ffma2_rn(vy, h1, __fmul2_rn(vz, h2)));
+    // sums of the orders
+    const float2 ri7 = __fmul2_rn(ri5, ri2), ri9 = __fmul2_rn(ri7, ri2);
+    const float2 eqd3 = __fmul2_rn(ri7, d3), eqd4 = __fmul2_rn(ri9, d4);
+    A.nphi = __ffma2_rn(splat2(-0.25f), eqd4,
+             __ffma2_rn(splat2(-1.0f / 3.0f), eqd3, __ffma2_rn(nqsh, eqd2, A.nphi)));
+    const float2 Kn = __ffma2_rn(ri2, __ffma2_rn(splat2(-2.25f), eqd4,
+                      __ffma2_rn(splat2(-7.0f / 3.0f), eqd3, __fmul2_rn(splat2(-2.5f), eqd2))), mri3);
+    Ux = __ffma2_rn(ri2, __ffma2_rn(ri2, h0, e0), Ux);
+    Uy = __ffma2_rn(ri2, __ffma2_rn(ri2, h1, e1), Uy);
+    Uz = __ffma2_rn(ri2, __ffma2_rn(ri2, h2, e2), Uz);
+    A.ax = __ffma2_rn(vx, Kn, __ffma2_rn(ri5, Ux, A.ax));
+    A.ay = __ffma2_rn(vy, Kn, __ffma2_rn(ri5, Uy, A.ay));
+    A.az = __ffma2_rn(vz, Kn, __ffma2_rn(ri5, Uz, A.az));
+}

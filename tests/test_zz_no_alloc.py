@@ -3,10 +3,12 @@ memory (its scratch is a static device array), against the plan path
 (grav_groups_upload_CUDA + grav_groups_eval_CUDA) on the same problem.
 
 With lists left unsplit the plan path also runs one work item per group
-and list kind and sums the same partials in the same order, so the two
-agree bit for bit.  Two calls in a row check that nothing carries over in
-the scratch between calls.  This file sorts last so that the GPU case also
-runs after every other GPU test in one process."""
+and list kind and sums the partials in the same order; its order-4 kernel
+evaluates records in pairs with the terms in another order, so the two
+agree to FP32 rounding (relative force differences below 1e-5), and the
+two calls in a row agree bit for bit, which checks that nothing carries
+over in the scratch between calls.  This file sorts last so that the GPU
+case also runs after every other GPU test in one process."""
 import ctypes
 
 import numpy as np
@@ -68,8 +70,17 @@ def test_dev_entry_matches_plan_on_two_calls():
     p.plist, p.qlist, p.hlist = on_device(t.plist), on_device(t.qlist), on_device(t.hlist)
     p.eps2, p.box, p.quad_phi_sign, p.ewald = eps2, 0.0, 1.0, 0
     out = torch.empty((t.n, 4), dtype=torch.float32, device=dev)
+    first = None
     for call in range(2):
         out.fill_(float("nan"))
         gc.check(gc.lib().grav_groups_eval_dev_CUDA(ctypes.byref(p), out.data_ptr(), None))
         got = out.cpu().numpy()
-        assert np.array_equal(got, ref), f"call {call}: max diff {np.abs(got - ref).max()}"
+        assert np.all(np.isfinite(got)), f"call {call}"
+        ra = np.linalg.norm(got[:, :3] - ref[:, :3], axis=1) / np.linalg.norm(ref[:, :3], axis=1)
+        rp = np.abs(got[:, 3] - ref[:, 3]) / np.abs(ref[:, 3])
+        assert ra.max() < 1e-5 and np.sqrt(np.mean(ra * ra)) < 2e-6, (call, ra.max())
+        assert rp.max() < 1e-5, (call, rp.max())
+        if first is None:
+            first = got.copy()
+        else:
+            assert np.array_equal(got, first), "the second call differs from the first"
