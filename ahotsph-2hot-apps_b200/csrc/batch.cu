@@ -48,6 +48,13 @@ struct Item {
     int64_t begin, end;
 };
 
+// One group's correction moments as k_ewald_side stores them (EwMoments).
+struct EwStored {
+    double lo[10];
+    float hi[25];
+    float pad[3];
+};
+
 struct DevProblem {
     const float4 *points;
     const nln_qcell *qcells;
@@ -75,6 +82,7 @@ struct DevProblem {
     EwTab ew;
     float ew_self;             // C(0) - pi/(alpha^2 L^3): the self term ewald() leaves out
     float ew_trace;            // trace of the Hessian of C: -4 pi / L^3
+    EwStored *ewm;             // per-group moments from k_ewald_side, or null: k_finish computes them
 };
 
 template <int KIND, bool PAIRED = false>
@@ -700,6 +708,33 @@ __device__ __forceinline__ void ewald_moments(const DevProblem &P, int64_t g, co
     M.warp_sum();
 }
 
+// The correction moments of groups gbegin..ngroups-1, stored per group for
+// k_finish: one warp per group from a queue (counter 3), run on a side
+// stream beside the list kernels, which it does not depend on.
+__global__ void __launch_bounds__(64) k_ewald_side(DevProblem P) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int it = 0;
+        if (lane == 0)
+            it = atomicAdd(&P.counters[3], 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        const int64_t g = P.gbegin + it;
+        if (g >= P.ngroups)
+            break;
+        const nln_group G = P.groups[g];
+        const double c[3] = {G.cen[0], G.cen[1], G.cen[2]};
+        EwMoments M;
+        ewald_moments(P, g, c, lane, M);
+        if (lane == 0) {
+            EwStored &E = P.ewm[g];
+#pragma unroll
+            for (int q = 0; q < 10; q++) E.lo[q] = M.lo[q];
+#pragma unroll
+            for (int q = 0; q < 25; q++) E.hi[q] = M.hi[q];
+        }
+    }
+}
+
 // Per group, in slot order: sum the partials of its work items in FP64,
 // add the periodic correction, and write (ax, ay, az, phi) of each sink.
 __global__ void k_finish(DevProblem P) {
@@ -720,7 +755,15 @@ __global__ void k_finish(DevProblem P) {
     if (P.ewald) {
         const double c[3] = {G.cen[0], G.cen[1], G.cen[2]};
         EwMoments M;
-        ewald_moments(P, g, c, lane, M);
+        if (P.ewm) {
+            const EwStored &E = P.ewm[g];
+#pragma unroll
+            for (int q = 0; q < 10; q++) M.lo[q] = E.lo[q];
+#pragma unroll
+            for (int q = 0; q < 25; q++) M.hi[q] = E.hi[q];
+        } else {
+            ewald_moments(P, g, c, lane, M);
+        }
         if (lane < G.count) {
             const float4 p = P.points[G.first + lane];
             double phi, ax, ay, az;
@@ -762,6 +805,11 @@ struct grav_plan {
     float4 *qstage = nullptr, *hstage = nullptr;  // pre-staged cell tables (k_stage_cells)
     grav_step_state *step = nullptr;  // tree links, refit scratch and the step graph
     grav_adjoint_state *adj = nullptr;  // adjoint scratch
+    // periodic: the side stream of k_ewald_side, its fork/join events and
+    // the per-group moments it stores
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    EwStored *ewm = nullptr;
     // Group ranges of the work queue: items are sorted by cost within each
     // range, and chunk_item[k][c] is the first item of kind k in range c.
     // One range [0, ngroups) except in the pipelined end-to-end call.
@@ -834,6 +882,7 @@ grav_tuning default_tuning() {
     t.blocks_per_sm = 0;
     t.chunk_p = t.chunk_q = t.chunk_h = 0;
     t.ewald_n = 0;
+    t.ewald_side = 0;
     return t;
 }
 
@@ -1268,6 +1317,14 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
         d.ew_self = (float)(t64[0] - M_PI / (alpha * alpha * hp->box * hp->box * hp->box));
         d.ew_trace = (float)(-4.0 * M_PI / (hp->box * hp->box * hp->box));
         d.ewald = 1;
+        rc |= dev_copy<EwStored>(pl, nullptr, (size_t)ng, &pl->ewm);
+        cudaError_t e = cudaStreamCreateWithFlags(&pl->side, cudaStreamNonBlocking);
+        if (e == cudaSuccess)
+            e = cudaEventCreateWithFlags(&pl->fork, cudaEventDisableTiming);
+        if (e == cudaSuccess)
+            e = cudaEventCreateWithFlags(&pl->join, cudaEventDisableTiming);
+        if (e != cudaSuccess)
+            rc |= gc::cuda_status(e, "upload: side stream");
     }
     float4 *out = nullptr;
     rc |= dev_copy<float4>(pl, nullptr, (size_t)nb, &out);
@@ -1408,6 +1465,42 @@ int launch_kind(grav_plan *pl, const DevProblem &dp, cudaStream_t st) {
     return 0;
 }
 
+// Blocks per SM of k_ewald_side (0: the moments are computed in k_finish).
+// Automatic: 2, the best of 1-6 at 128^3 and 256^3 (one is too few to
+// finish with the list kernels; more take too many of their registers).
+int side_blocks(const grav_plan *pl) {
+    if (!pl->dp.ewald || !pl->side || !pl->ewm || pl->tune.ewald_side < 0)
+        return 0;
+    return pl->tune.ewald_side > 0 ? pl->tune.ewald_side : 2;
+}
+
+// Fork: k_ewald_side over dp's groups on the side stream, after the work
+// already on st; returns whether it forked (join with side_join).
+int side_fork(grav_plan *pl, const DevProblem &dp, cudaStream_t st, bool &forked) {
+    forked = false;
+    const int per_sm = side_blocks(pl);
+    const int64_t n = dp.ngroups - dp.gbegin;
+    if (per_sm <= 0 || n <= 0)
+        return 0;
+    GC_CHECK(cudaEventRecord(pl->fork, st));
+    GC_CHECK(cudaStreamWaitEvent(pl->side, pl->fork, 0));
+    DevProblem d = dp;
+    d.ewm = pl->ewm;
+    const unsigned blocks =
+        (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 1) / 2, (int64_t)per_sm * pl->nsm));
+    k_ewald_side<<<blocks, 64, 0, pl->side>>>(d);
+    GC_CHECK(cudaGetLastError());
+    GC_CHECK(cudaEventRecord(pl->join, pl->side));
+    pl->launches++;
+    forked = true;
+    return 0;
+}
+
+int side_join(grav_plan *pl, cudaStream_t st) {
+    GC_CHECK(cudaStreamWaitEvent(st, pl->join, 0));
+    return 0;
+}
+
 // Two warps per block: at ~160 registers a thread, small blocks let more
 // warps stay resident, which this latency-bound kernel needs.
 int launch_finish(grav_plan *pl, const DevProblem &dp, cudaStream_t st) {
@@ -1435,6 +1528,9 @@ extern "C" int grav_groups_eval_CUDA(grav_plan *pl, void *stream) {
     GC_CHECK(cudaMemsetAsync(pl->dp.counters, 0, 4 * sizeof(int), st));
     if (int rc = mark(0))
         return rc;
+    bool forked = false;
+    if (int rc = side_fork(pl, pl->dp, st, forked))
+        return rc;
     if (int rc = launch_kind<KH>(pl, pl->dp, st))
         return rc;
     if (int rc = mark(1))
@@ -1447,7 +1543,13 @@ extern "C" int grav_groups_eval_CUDA(grav_plan *pl, void *stream) {
         return rc;
     if (int rc = mark(3))
         return rc;
-    if (int rc = launch_finish(pl, pl->dp, st))
+    DevProblem df = pl->dp;
+    if (forked) {
+        if (int rc = side_join(pl, st))
+            return rc;
+        df.ewm = pl->ewm;
+    }
+    if (int rc = launch_finish(pl, df, st))
         return rc;
     return mark(4);
 }
@@ -1573,6 +1675,14 @@ extern "C" void grav_plan_free(grav_plan *pl) {
     for (cudaEvent_t e : pl->ev)
         if (e)
             cudaEventDestroy(e);
+    if (pl->side) {
+        cudaStreamSynchronize(pl->side);
+        cudaStreamDestroy(pl->side);
+    }
+    if (pl->fork)
+        cudaEventDestroy(pl->fork);
+    if (pl->join)
+        cudaEventDestroy(pl->join);
     delete pl;
 }
 
@@ -1643,11 +1753,18 @@ int eval_range(grav_plan *pl, size_t c, cudaStream_t st) {
         GC_CHECK(cudaGetLastError());
         pl->launches++;
     }
-    int rc = launch_kind<KH>(pl, dp, st);
+    bool forked = false;
+    int rc = side_fork(pl, dp, st, forked);
+    if (!rc)
+        rc = launch_kind<KH>(pl, dp, st);
     if (!rc)
         rc = launch_kind<KQ>(pl, dp, st);
     if (!rc)
         rc = launch_kind<KP>(pl, dp, st);
+    if (!rc && forked) {
+        rc = side_join(pl, st);
+        dp.ewm = pl->ewm;
+    }
     if (!rc)
         rc = launch_finish(pl, dp, st);
     return rc;

@@ -56,7 +56,8 @@ class Problem(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("warps_per_block", ctypes.c_int), ("chunk_p", ctypes.c_int),
                 ("chunk_q", ctypes.c_int), ("chunk_h", ctypes.c_int),
-                ("blocks_per_sm", ctypes.c_int), ("ewald_n", ctypes.c_int)]
+                ("blocks_per_sm", ctypes.c_int), ("ewald_n", ctypes.c_int),
+                ("ewald_side", ctypes.c_int)]
 
 
 def lib(record_errors=True):

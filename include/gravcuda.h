@@ -194,6 +194,9 @@ typedef struct grav_tuning {
     int chunk_h;                /* max order-4 cells per work item */
     int blocks_per_sm;          /* persistent grid = blocks_per_sm x SM count (0: as many as fit) */
     int ewald_n;                /* Ewald table nodes per axis (0: 32) */
+    int ewald_side;             /* periodic: the Ewald correction moments run on a side stream
+                                   beside the list kernels with this many 2-warp blocks per SM
+                                   (0: automatic; -1: inside the finish pass, after them) */
 } grav_tuning;
 
 /*

@@ -235,3 +235,20 @@ def test_run_packed_end_to_end_reports_malformed_runs(gc, monkeypatch):
         gc.lib().gravcuda_clear_status()
     gc.groups_eval_problem(gc.pinned_problem(t, packed=True), 1e-4, 0.0)
     gc.lib().grav_groups_release_CUDA()
+
+
+def test_ewald_moments_on_side_stream_match_finish_pass(gc):
+    """The periodic correction's moments computed by k_ewald_side on a side
+    stream, beside the list kernels (the default), give the results of the
+    moments computed inside the finish pass, bit for bit.  (The periodic
+    KDK test of test_step_gpu.py runs the fork and join inside a captured
+    CUDA graph.)"""
+    t = make_tree("box", 20 ** 3, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-4)
+    eps2 = (1.0 / 20 / 50) ** 2
+    outs = []
+    for side in (-1, 0, 3):
+        plan = gc.Plan(t, eps2, ewald=True, tuning=gc.Tuning(8, 0, 0, 0, 0, 0, side))
+        plan.eval()
+        outs.append(plan.download())
+        plan.free()
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
