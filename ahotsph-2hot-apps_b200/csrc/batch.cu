@@ -96,10 +96,11 @@ struct KindOf {
     // one TMA row gather brings 4 records; each lands 128-byte aligned
     static constexpr int group_bytes = 4 * rec_bytes < 128 ? 128 : 4 * rec_bytes;
     static constexpr int stage_bytes = (TILE / 4) * group_bytes;
-    // paired order-4 tile: 16 record pairs of 32 interleaved fields, one pair
-    // every 68 floats (16-byte aligned; the re-lay's 8-byte stores of a
-    // half-warp hit distinct banks)
-    static constexpr int pair_stride = 68;
+    // paired tiles: 16 record pairs of 32 (order 4) or 10 (quadrupole)
+    // interleaved fields, one pair every 68 or 20 floats (16-byte aligned;
+    // the re-lay's 8-byte stores of a half-warp hit distinct banks)
+    static constexpr int pair_fields = KIND == KH ? 32 : 10;
+    static constexpr int pair_stride = KIND == KH ? 68 : 20;
     static constexpr int pair_bytes = PAIRED ? (TILE / 2) * pair_stride * 4 : 0;
     // per-warp shared memory: stages of 32 records, the pair buffer,
     // mbarriers, image codes
@@ -324,21 +325,25 @@ __global__ void k_stage_cells(const nln_qcell *__restrict__ qc, const nln_hcell 
     }
 }
 
-// Re-lay this lane's pre-staged order-4 record (just landed by TMA at its
-// stage slot) into the pair-interleaved tile of hexa2_plummer: header
-// re-centred on the group centre c in the record's image, the octupole and
-// four hexadecapole fields negated as that layout wants.  A lane past the
-// tile's end writes a massless, momentless record far away, which adds
-// exactly zero.  Lanes 2p and 2p+1 write pair p: one shuffle per field pair.
+// Re-lay this lane's pre-staged record (just landed by TMA at its stage
+// slot) into the pair-interleaved tile of quad2_plummer / hexa2_plummer:
+// header re-centred on the group centre c in the record's image; for order
+// 4 the octupole and four hexadecapole fields negated as that layout wants.
+// A lane past the tile's end writes a massless, momentless record far away,
+// which adds exactly zero.  Lanes 2p and 2p+1 write pair p: one shuffle per
+// field pair.
+template <int KIND>
 __device__ __forceinline__ void relay_pairs(const unsigned char *stage, uint32_t code, bool valid,
                                             const double *c, double box, float *pbuf, int lane) {
-    using K = KindOf<KH, true>;
-    float g[32];
+    using K = KindOf<KIND, true>;
+    constexpr int NF = K::pair_fields;
+    constexpr int NR = K::rec_bytes / 4;  // staged record floats
+    float g[NF];
     if (valid) {
         const float4 *src = reinterpret_cast<const float4 *>(stage + K::rec_off(lane));
-        float f[32];
+        float f[NR];
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
+        for (int k = 0; k < NR / 4; k++) {
             const float4 v = src[k];
             f[4 * k] = v.x;
             f[4 * k + 1] = v.y;
@@ -353,27 +358,29 @@ __device__ __forceinline__ void relay_pairs(const unsigned char *stage, uint32_t
         g[0] = (float)(cx + sx - c[0]);
         g[1] = (float)(cy + sy - c[1]);
         g[2] = (float)(cz + sz - c[2]);
-        g[3] = f[31];
+        g[3] = f[KIND == KH ? 31 : 12];
 #pragma unroll
         for (int k = 4; k < 10; k++) g[k] = f[k];
-        g[10] = -f[21];
-        g[11] = -f[25];
+        if (KIND == KH) {
+            g[10] = -f[21];
+            g[11] = -f[25];
 #pragma unroll
-        for (int k = 12; k < 19; k++) g[k] = -f[k];
-        g[19] = f[19];
-        g[20] = f[20];
+            for (int k = 12; k < 19; k++) g[k] = -f[k];
+            g[19] = f[19];
+            g[20] = f[20];
 #pragma unroll
-        for (int k = 21; k < 30; k++) g[k] = f[k];
-        g[30] = -f[30];
-        g[31] = -f[23];
+            for (int k = 21; k < 30; k++) g[k] = f[k];
+            g[30] = -f[30];
+            g[31] = -f[23];
+        }
     } else {
 #pragma unroll
-        for (int k = 0; k < 32; k++) g[k] = k < 3 ? 1.0e3f : 0.f;
+        for (int k = 0; k < NF; k++) g[k] = k < 3 ? 1.0e3f : 0.f;
     }
     const int s = lane & 1;
     float *dst = pbuf + (lane >> 1) * K::pair_stride + 2 * s;
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
+    for (int q = 0; q < NF / 2; q++) {
         const float send = s ? g[2 * q] : g[2 * q + 1];
         const float recv = __shfl_xor_sync(0xffffffffu, send, 1);
         *reinterpret_cast<float2 *>(dst + 4 * q) =
@@ -387,13 +394,25 @@ __device__ __forceinline__ void relay_pairs(const unsigned char *stage, uint32_t
 #ifndef GRAV_H2_MINB
 #define GRAV_H2_MINB 3
 #endif
+#ifndef GRAV_Q2_MINB
+#define GRAV_Q2_MINB 0
+#endif
+#ifndef GRAV_Q2_UNROLL
+#define GRAV_Q2_UNROLL 4
+#endif
+#ifndef GRAV_Q2_PAIRED
+#define GRAV_Q2_PAIRED 1
+#endif
 constexpr int kH2Unroll = GRAV_H2_UNROLL;
+constexpr int kQ2Unroll = GRAV_Q2_UNROLL;
 template <int KIND, bool STAGED>
-__global__ void __launch_bounds__(256, KIND == KH ? (STAGED ? GRAV_H2_MINB : 3) : 0) k_batch(const __grid_constant__ CUtensorMap tmap,
+__global__ void __launch_bounds__(256, KIND == KH ? (STAGED ? GRAV_H2_MINB : 3)
+                                                  : (KIND == KQ && STAGED ? GRAV_Q2_MINB : 0))
+    k_batch(const __grid_constant__ CUtensorMap tmap,
                                                DevProblem P) {
-    // staged order-4 tables run the paired (f32x2) interaction on a
-    // pair-interleaved copy of each tile
-    constexpr bool PAIRED = KIND == KH && STAGED;
+    // staged quadrupole and order-4 tables run the paired (f32x2)
+    // interaction on a pair-interleaved copy of each tile
+    constexpr bool PAIRED = (KIND == KH || (KIND == KQ && GRAV_Q2_PAIRED)) && STAGED;
     using K = KindOf<KIND, PAIRED>;
     constexpr int RB = K::rec_bytes;
     constexpr int ORDER = K::order;
@@ -501,8 +520,8 @@ __global__ void __launch_bounds__(256, KIND == KH ? (STAGED ? GRAV_H2_MINB : 3) 
             }
             unsigned char *bt = wbuf + st * K::stage_bytes;
             Acc4 a{0.f, 0.f, 0.f, 0.f};
-            if (PAIRED) {
-                relay_pairs(bt, codes[st * TILE + lane], lane < nt, c, P.box, pbuf, lane);
+            if constexpr (PAIRED) {
+                relay_pairs<KIND>(bt, codes[st * TILE + lane], lane < nt, c, P.box, pbuf, lane);
                 __syncwarp();  // the stage is free: start the next copy, then compute
                 if (t + 1 < ntile)
                     issue(t + 1, ent_next, seq + 1);
@@ -511,13 +530,18 @@ __global__ void __launch_bounds__(256, KIND == KH ? (STAGED ? GRAV_H2_MINB : 3) 
                 const float2 e2 = splat2(P.eps2), nqsh = splat2(-P.qsh);
                 Acc2h A{splat2(0.f), splat2(0.f), splat2(0.f), splat2(0.f)};
                 const int npair = (nt + 1) >> 1;
+                auto pair = [&](int q) {
+                    if (KIND == KH)
+                        hexa2_plummer(pbuf + q * K::pair_stride, nsx, nsy, nsz, e2, nqsh, A);
+                    else
+                        quad2_plummer(pbuf + q * K::pair_stride, nsx, nsy, nsz, e2, nqsh, A);
+                };
+                constexpr int kUnroll = KIND == KH ? kH2Unroll : kQ2Unroll;
                 if (npair == TILE / 2) {
-#pragma unroll kH2Unroll
-                    for (int q = 0; q < TILE / 2; q++)
-                        hexa2_plummer(pbuf + q * K::pair_stride, nsx, nsy, nsz, e2, nqsh, A);
+#pragma unroll kUnroll
+                    for (int q = 0; q < TILE / 2; q++) pair(q);
                 } else {
-                    for (int q = 0; q < npair; q++)
-                        hexa2_plummer(pbuf + q * K::pair_stride, nsx, nsy, nsz, e2, nqsh, A);
+                    for (int q = 0; q < npair; q++) pair(q);
                 }
                 a.ax = A.ax.x + A.ax.y;
                 a.ay = A.ay.x + A.ay.y;
@@ -810,6 +834,7 @@ struct grav_plan {
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
     EwStored *ewm = nullptr;
+    int64_t ewald_entries = 0;  // correction-list length
     // Group ranges of the work queue: items are sorted by cost within each
     // range, and chunk_item[k][c] is the first item of kind k in range c.
     // One range [0, ngroups) except in the pipelined end-to-end call.
@@ -1318,6 +1343,7 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
         d.ew_trace = (float)(-4.0 * M_PI / (hp->box * hp->box * hp->box));
         d.ewald = 1;
         rc |= dev_copy<EwStored>(pl, nullptr, (size_t)ng, &pl->ewm);
+        pl->ewald_entries = hp->cptr[ng];
         cudaError_t e = cudaStreamCreateWithFlags(&pl->side, cudaStreamNonBlocking);
         if (e == cudaSuccess)
             e = cudaEventCreateWithFlags(&pl->fork, cudaEventDisableTiming);
@@ -1450,7 +1476,8 @@ int launch_kind(grav_plan *pl, const DevProblem &dp, cudaStream_t st) {
         pl->launches++;
         return 0;
     }
-    const size_t smem = (size_t)wpb * (pl->staged ? KindOf<KIND, KIND == KH>::warp_bytes
+    constexpr bool paired = KIND == KH || (KIND == KQ && GRAV_Q2_PAIRED);
+    const size_t smem = (size_t)wpb * (pl->staged ? KindOf<KIND, paired>::warp_bytes
                                                   : KindOf<KIND>::warp_bytes);
     auto kern = pl->staged ? k_batch<KIND, true> : k_batch<KIND, false>;
     GC_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1466,12 +1493,19 @@ int launch_kind(grav_plan *pl, const DevProblem &dp, cudaStream_t st) {
 }
 
 // Blocks per SM of k_ewald_side (0: the moments are computed in k_finish).
-// Automatic: 2, the best of 1-6 at 128^3 and 256^3 (one is too few to
-// finish with the list kernels; more take too many of their registers).
+// Automatic: 2 blocks (the best of 1-6 on the 128^3 and 256^3 boxes) when
+// the correction list is short beside the order-4 lists, else 0.  The side
+// kernel shares the SMs with the list kernels: it pays only while it ends
+// well within them.  Measured on one B200: correction entries at 1.2 % of
+// the order-4 interactions (256^3, MAC 1.5e-6) gain 1.2 %; where the
+// moments take half the order-4 kernel's time (128^3, MAC 1e-4) the side
+// stream loses 8 %.  The threshold below sits between.
 int side_blocks(const grav_plan *pl) {
     if (!pl->dp.ewald || !pl->side || !pl->ewm || pl->tune.ewald_side < 0)
         return 0;
-    return pl->tune.ewald_side > 0 ? pl->tune.ewald_side : 2;
+    if (pl->tune.ewald_side > 0)
+        return pl->tune.ewald_side;
+    return pl->ewald_entries < 0.015 * (double)pl->counts[3] ? 2 : 0;
 }
 
 // Fork: k_ewald_side over dp's groups on the side stream, after the work

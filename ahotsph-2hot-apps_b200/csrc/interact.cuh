@@ -245,6 +245,12 @@ struct Acc2h {
     float2 ax, ay, az, nphi;
 };
 
+// The quadrupole counterpart on a pair-interleaved tile of 10 fields
+// (position, mass, Q as staged): with v = -d and U = Q.v,
+//   a = v (m/r^3 - 5/2 r^-2 eq_2.d) + r^-5 U,  -phi = m/r - qsh eq_2.d.
+__device__ __forceinline__ void quad2_plummer(const float *__restrict__ pr, float2 nsx, float2 nsy,
+                                              float2 nsz, float2 eps2, float2 nqsh, Acc2h &A);
+
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ float2 splat2(float a) { return make_float2(a, a); }
 
@@ -335,6 +341,38 @@ __device__ __forceinline__ void hexa2_plummer(const float *__restrict__ pr, floa
     Ux = __ffma2_rn(ri2, __ffma2_rn(ri2, h0, e0), Ux);
     Uy = __ffma2_rn(ri2, __ffma2_rn(ri2, h1, e1), Uy);
     Uz = __ffma2_rn(ri2, __ffma2_rn(ri2, h2, e2), Uz);
+    A.ax = __ffma2_rn(vx, Kn, __ffma2_rn(ri5, Ux, A.ax));
+    A.ay = __ffma2_rn(vy, Kn, __ffma2_rn(ri5, Uy, A.ay));
+    A.az = __ffma2_rn(vz, Kn, __ffma2_rn(ri5, Uz, A.az));
+}
+
+__device__ __forceinline__ void quad2_plummer(const float *__restrict__ pr, float2 nsx, float2 nsy,
+                                              float2 nsz, float2 eps2, float2 nqsh, Acc2h &A) {
+    const float4 *q = reinterpret_cast<const float4 *>(pr);
+    float4 w = q[0];
+    const float2 vx = __fadd2_rn(f2(w.x, w.y), nsx);
+    const float2 vy = __fadd2_rn(f2(w.z, w.w), nsy);
+    w = q[1];
+    const float2 vz = __fadd2_rn(f2(w.x, w.y), nsz);
+    const float2 m = f2(w.z, w.w);
+    const float2 r2 = __ffma2_rn(vx, vx, __ffma2_rn(vy, vy, __ffma2_rn(vz, vz, eps2)));
+    const float2 ri = f2(rsqrt_fast(r2.x), rsqrt_fast(r2.y));
+    const float2 ri2 = __fmul2_rn(ri, ri);
+    const float2 mri3 = __fmul2_rn(__fmul2_rn(m, ri), ri2);
+    w = q[2];
+    const float2 Qxx = f2(w.x, w.y), Qxy = f2(w.z, w.w);
+    w = q[3];
+    const float2 Qyy = f2(w.x, w.y), Qxz = f2(w.z, w.w);
+    w = q[4];
+    const float2 Qyz = f2(w.x, w.y), Qzz = f2(w.z, w.w);
+    const float2 Ux = __ffma2_rn(Qxx, vx, __ffma2_rn(Qxy, vy, __fmul2_rn(Qxz, vz)));
+    const float2 Uy = __ffma2_rn(Qxy, vx, __ffma2_rn(Qyy, vy, __fmul2_rn(Qyz, vz)));
+    const float2 Uz = __ffma2_rn(Qxz, vx, __ffma2_rn(Qyz, vy, __fmul2_rn(Qzz, vz)));
+    const float2 vQv = __ffma2_rn(vx, Ux, __ffma2_rn(vy, Uy, __fmul2_rn(vz, Uz)));
+    const float2 ri5 = __fmul2_rn(__fmul2_rn(ri, ri2), ri2);
+    const float2 eqd2 = __fmul2_rn(ri5, vQv);
+    A.nphi = __ffma2_rn(nqsh, eqd2, __ffma2_rn(m, ri, A.nphi));
+    const float2 Kn = __ffma2_rn(__fmul2_rn(splat2(-2.5f), ri2), eqd2, mri3);
     A.ax = __ffma2_rn(vx, Kn, __ffma2_rn(ri5, Ux, A.ax));
     A.ay = __ffma2_rn(vy, Kn, __ffma2_rn(ri5, Uy, A.ay));
     A.az = __ffma2_rn(vz, Kn, __ffma2_rn(ri5, Uz, A.az));

@@ -196,7 +196,9 @@ typedef struct grav_tuning {
     int ewald_n;                /* Ewald table nodes per axis (0: 32) */
     int ewald_side;             /* periodic: the Ewald correction moments run on a side stream
                                    beside the list kernels with this many 2-warp blocks per SM
-                                   (0: automatic; -1: inside the finish pass, after them) */
+                                   (-1: inside the finish pass, after them; 0: automatic, 2
+                                   when the correction list is under 1.5 % of the order-4
+                                   interactions, else -1) */
 } grav_tuning;
 
 /*
