@@ -20,17 +20,17 @@
 //     dL/dm_b += Mbar + Xbar.y_b/M + y_b.S2bar.y_b,      S2bar = -3 (Qbar - tr Qbar/3).
 //
 // Work layout: one warp per work item (group, list kind, slice), as the
-// forward's queues.  Lane i holds sink i; a tile's 32 records are staged in
-// shared memory and lane i visits record (i + k) mod 32 at step k, so in
-// every step the 32 lanes touch 32 different records and accumulate their
-// source-side sums into per-record shared slots without conflicts.  Slots
-// are flushed with FP64 atomics once per tile; sink sums once per item.
+// forward's queues.  Each lane holds two sinks as an f32x2 pair and one
+// record of a 32-record tile; records and their running source-side sums
+// pass round the 16 lanes of each half-warp (k_adjoint_points,
+// k_adjoint_quads), so every record meets every sink without shared memory.
+// Record sums are flushed with FP64 atomics once per tile, sink sums once
+// per item.
 #pragma once
 
 namespace {
 
 constexpr int kAdjTile = 32;
-constexpr int kAdjSlot = 11;  // per record: t (3), mass bar, Q bar (6), pad (odd stride)
 
 struct AdjProblem {
     const float4 *points;
@@ -48,148 +48,319 @@ struct AdjProblem {
     unsigned *err;
 };
 
-template <int KIND>
-__global__ void __launch_bounds__(256) k_adjoint(AdjProblem P) {
-    constexpr int REC = KIND == KP ? 4 : 12;
-    __shared__ __align__(16) float srec[8][kAdjTile * REC];
-    __shared__ float sacc[8][kAdjTile * kAdjSlot];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    float *rec = srec[wib];
-    float *acc = sacc[wib];
+// The point-list adjoint (bodies and cell monopoles), systolic.  Lane l
+// holds sinks 2j and 2j+1 (j = l mod 16) as one f32x2 pair, and one record
+// of the tile of 32 in registers (half h = l / 16 takes records 16h..16h+15).
+// At each of 16 steps every lane evaluates its two sinks against the record
+// it holds, adds their source-side terms to the record's running sums, and
+// passes record and sums to the next lane of its half (8 shuffles); after
+// 16 steps every record has met all 32 sinks and its sums are back with
+// their owner lane, which flushes them with FP64 atomics.  No shared memory:
+// per-record shared slots cost 8-12 shared-memory wavefronts per step of
+// 32 interactions and bound that form at 29.6 ms on the N = 2^20 Plummer
+// case (this one: about 22 ms, bound by the FMA pipe).
+__global__ void __launch_bounds__(256) k_adjoint_points(AdjProblem P) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, j = lane & 15;
+    const int next = (lane & 16) | ((j + 1) & 15);  // the lane this one takes its record from
     const uint32_t nb = (uint32_t)P.nbodies;
     while (true) {
         int it = 0;
         if (lane == 0)
-            it = atomicAdd(&P.counters[KIND], 1);
-        it = __shfl_sync(0xffffffffu, it, 0);
-        if (it >= P.nitems[KIND])
+            it = atomicAdd(&P.counters[KP], 1);
+        it = __shfl_sync(FULL, it, 0);
+        if (it >= P.nitems[KP])
             break;
-        const Item item = P.items[KIND][it];
+        const Item item = P.items[KP][it];
         const nln_group G = P.groups[item.group];
         const double c[3] = {G.cen[0], G.cen[1], G.cen[2]};
-        float ux = 0.f, uy = 0.f, uz = 0.f, wx = 0.f, wy = 0.f, wz = 0.f, wu = 0.f;
-        if (lane < G.count) {
-            const float4 s = P.points[G.first + lane];
-            ux = (float)((double)s.x - c[0]);
-            uy = (float)((double)s.y - c[1]);
-            uz = (float)((double)s.z - c[2]);
-            const float4 w = P.wu[G.first + lane];
-            wx = w.x;
-            wy = w.y;
-            wz = w.z;
-            wu = w.w;
+        // sinks 2j, 2j+1 as pairs; a missing sink has w = u = 0 and adds nothing
+        float s[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+        float w[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int sk = 2 * j + h;
+            if (sk < G.count) {
+                const float4 p = P.points[G.first + sk];
+                s[h][0] = (float)((double)p.x - c[0]);
+                s[h][1] = (float)((double)p.y - c[1]);
+                s[h][2] = (float)((double)p.z - c[2]);
+                const float4 q = P.wu[G.first + sk];
+                w[h][0] = q.x;
+                w[h][1] = q.y;
+                w[h][2] = q.z;
+                w[h][3] = q.w;
+            }
         }
-        float gx = 0.f, gy = 0.f, gz = 0.f;  // this sink's -sum t
+        const float2 Sx = f2(s[0][0], s[1][0]), Sy = f2(s[0][1], s[1][1]), Sz = f2(s[0][2], s[1][2]);
+        const float2 Wx = f2(w[0][0], w[1][0]), Wy = f2(w[0][1], w[1][1]), Wz = f2(w[0][2], w[1][2]);
+        const float2 U = f2(w[0][3], w[1][3]), NU = f2(-w[0][3], -w[1][3]);
+        const float2 e2 = splat2(P.eps2);
+        float2 Gx = splat2(0.f), Gy = splat2(0.f), Gz = splat2(0.f);  // the sinks' sums of t
+        // records are loaded a tile ahead of use and list entries two tiles
+        // ahead, so a tile's loads overlap the previous tile's 16 steps
+        auto entry = [&](int64_t b) -> uint32_t {
+            return b + lane < item.end ? (P.list[0][b + lane] & NLN_IDX_MASK) : 0xffffffffu;
+        };
+        auto record = [&](uint32_t e) -> float4 {
+            return e != 0xffffffffu ? __ldg(P.points + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+        };
+        uint32_t e_cur = entry(item.begin), e_next = entry(item.begin + kAdjTile);
+        float4 p_cur = record(e_cur);
         for (int64_t b0 = item.begin; b0 < item.end; b0 += kAdjTile) {
             const int nt = (int)min((int64_t)kAdjTile, item.end - b0);
-            uint32_t idx = 0;
+            const float4 p_next = record(e_next);
+            const uint32_t e_after = entry(b0 + 2 * kAdjTile);
+            // this lane's record, negated position relative to the centre
+            const uint32_t idx = e_cur;
+            float nx = -1.0e3f, ny = -1.0e3f, nz = -1.0e3f, m = 0.f;  // massless and far: adds 0
             if (lane < nt) {
-                idx = P.list[KIND][b0 + lane] & NLN_IDX_MASK;
-                float *o = rec + lane * REC;
-                if (KIND == KP) {
-                    const float4 p = P.points[idx];
-                    o[0] = (float)((double)p.x - c[0]);
-                    o[1] = (float)((double)p.y - c[1]);
-                    o[2] = (float)((double)p.z - c[2]);
-                    o[3] = p.w;
-                } else {
-                    const nln_qcell q = P.qcells[idx];
-                    o[0] = (float)(q.cen[0] - c[0]);
-                    o[1] = (float)(q.cen[1] - c[1]);
-                    o[2] = (float)(q.cen[2] - c[2]);
-                    o[3] = q.mass;
-                    const float q2[5] = {q.qxx, q.qxy, q.qyy, q.qxz, q.qyz};
-                    stage_quad(o, q.R, q2);
-                }
+                nx = (float)(c[0] - (double)p_cur.x);
+                ny = (float)(c[1] - (double)p_cur.y);
+                nz = (float)(c[2] - (double)p_cur.z);
+                m = p_cur.w;
             }
-#pragma unroll
-            for (int q = 0; q < kAdjSlot; q++) acc[lane * kAdjSlot + q] = 0.f;
-            __syncwarp();
-            if (lane < G.count) {
-                for (int k = 0; k < kAdjTile; k++) {
-                    const int r = (lane + k) & (kAdjTile - 1);
-                    if (r >= nt)
-                        continue;
-                    const float *s = rec + r * REC;
-                    const float dx = ux - s[0], dy = uy - s[1], dz = uz - s[2], m = s[3];
-                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, P.eps2)));
-                    const float ri = rsqrt_fast(r2), ri2 = ri * ri, ri3 = ri * ri2;
-                    const float wd = fmaf(wx, dx, fmaf(wy, dy, wz * dz));
-                    // monopole: t = m (ri3 w - 3 ri5 (w.d) d) - u m ri3 d
-                    const float ri5 = ri3 * ri2;
-                    const float cd = m * fmaf(-3.f * ri5, wd, -wu * ri3);
-                    float tx = fmaf(m * ri3, wx, cd * dx);
-                    float ty = fmaf(m * ri3, wy, cd * dy);
-                    float tz = fmaf(m * ri3, wz, cd * dz);
-                    float* slot = acc + r * kAdjSlot;
-                    slot[3] += -fmaf(wd, ri3, wu * ri);  // dL/dm
-                    if (KIND == KQ) {
-                        const float Qxx = s[4], Qxy = s[5], Qyy = s[6], Qxz = s[7], Qyz = s[8],
-                                    Qzz = s[9];
-                        const float Qdx = fmaf(Qxx, dx, fmaf(Qxy, dy, Qxz * dz));
-                        const float Qdy = fmaf(Qxy, dx, fmaf(Qyy, dy, Qyz * dz));
-                        const float Qdz = fmaf(Qxz, dx, fmaf(Qyz, dy, Qzz * dz));
-                        const float Qwx = fmaf(Qxx, wx, fmaf(Qxy, wy, Qxz * wz));
-                        const float Qwy = fmaf(Qxy, wx, fmaf(Qyy, wy, Qyz * wz));
-                        const float Qwz = fmaf(Qxz, wx, fmaf(Qyz, wy, Qzz * wz));
-                        const float P2 = fmaf(dx, Qdx, fmaf(dy, Qdy, dz * Qdz));
-                        const float Qdw = fmaf(wx, Qdx, fmaf(wy, Qdy, wz * Qdz));
-                        const float ri7 = ri5 * ri2, ri9 = ri7 * ri2;
-                        const float h = P.qsh;
-                        // H_q w = qsh [2 ri5 Qw - 10 ri7 (d (Qd.w) + Qd (d.w)) - 5 ri7 P2 w + 35 ri9 P2 (d.w) d]
-                        // a_q = -qsh [2 ri5 Qd - 5 ri7 P2 d]
-                        const float kd = h * (-10.f * ri7 * Qdw + 35.f * ri9 * P2 * wd + 5.f * wu * ri7 * P2);
-                        const float kq = h * (-10.f * ri7 * wd - 2.f * wu * ri5);
-                        const float kw = h * (-5.f * ri7 * P2);
-                        const float k2 = h * 2.f * ri5;
-                        tx += fmaf(k2, Qwx, fmaf(kd, dx, fmaf(kq, Qdx, kw * wx)));
-                        ty += fmaf(k2, Qwy, fmaf(kd, dy, fmaf(kq, Qdy, kw * wy)));
-                        tz += fmaf(k2, Qwz, fmaf(kd, dz, fmaf(kq, Qdz, kw * wz)));
-                        // dL/dQ = qsh [(u ri5 + 5 (w.d) ri7) d d^T - ri5 (w d^T + d w^T)]
-                        const float A = h * fmaf(wu, ri5, 5.f * wd * ri7);
-                        const float B = -h * ri5;
-                        slot[4] += fmaf(A * dx, dx, 2.f * B * wx * dx);
-                        slot[5] += fmaf(A * dx, dy, B * fmaf(wx, dy, wy * dx));
-                        slot[6] += fmaf(A * dx, dz, B * fmaf(wx, dz, wz * dx));
-                        slot[7] += fmaf(A * dy, dy, 2.f * B * wy * dy);
-                        slot[8] += fmaf(A * dy, dz, B * fmaf(wy, dz, wz * dy));
-                        slot[9] += fmaf(A * dz, dz, 2.f * B * wz * dz);
-                    }
-                    slot[0] += tx;
-                    slot[1] += ty;
-                    slot[2] += tz;
-                    gx -= tx;
-                    gy -= ty;
-                    gz -= tz;
-                }
+            e_cur = e_next;
+            e_next = e_after;
+            p_cur = p_next;
+            float ax = 0.f, ay = 0.f, az = 0.f, am = 0.f;  // the record's sums of t, w.d/r^3 + u/r
+#pragma unroll 4
+            for (int k = 0; k < 16; k++) {
+                const float2 dx = __fadd2_rn(Sx, splat2(nx)), dy = __fadd2_rn(Sy, splat2(ny));
+                const float2 dz = __fadd2_rn(Sz, splat2(nz)), M = splat2(m);
+                const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, e2)));
+                const float2 ri = f2(rsqrt_fast(r2.x), rsqrt_fast(r2.y));
+                const float2 ri2 = __fmul2_rn(ri, ri);
+                const float2 mr3 = __fmul2_rn(__fmul2_rn(M, ri), ri2);
+                const float2 wd = __ffma2_rn(Wx, dx, __ffma2_rn(Wy, dy, __fmul2_rn(Wz, dz)));
+                // t = m ri3 (w + (-3 ri2 (w.d) - u) d)
+                const float2 in = __ffma2_rn(__fmul2_rn(splat2(-3.f), ri2), wd, NU);
+                const float2 tx = __fmul2_rn(mr3, __ffma2_rn(in, dx, Wx));
+                const float2 ty = __fmul2_rn(mr3, __ffma2_rn(in, dy, Wy));
+                const float2 tz = __fmul2_rn(mr3, __ffma2_rn(in, dz, Wz));
+                const float2 nm = __fmul2_rn(ri, __ffma2_rn(wd, ri2, U));  // -dL/dm = (w.d) ri3 + u ri
+                Gx = __fadd2_rn(Gx, tx);
+                Gy = __fadd2_rn(Gy, ty);
+                Gz = __fadd2_rn(Gz, tz);
+                ax += tx.x + tx.y;
+                ay += ty.x + ty.y;
+                az += tz.x + tz.y;
+                am += nm.x + nm.y;
+                // pass record and sums on: after 16 steps they are home again
+                nx = __shfl_sync(FULL, nx, next);
+                ny = __shfl_sync(FULL, ny, next);
+                nz = __shfl_sync(FULL, nz, next);
+                m = __shfl_sync(FULL, m, next);
+                ax = __shfl_sync(FULL, ax, next);
+                ay = __shfl_sync(FULL, ay, next);
+                az = __shfl_sync(FULL, az, next);
+                am = __shfl_sync(FULL, am, next);
             }
-            __syncwarp();
             if (lane < nt) {
-                const float *slot = acc + lane * kAdjSlot;
-                if (KIND == KP && idx < nb) {
+                if (idx < nb) {
                     double *g = P.gbody + (size_t)idx * 4;
-                    atomicAdd(g + 0, (double)slot[0]);
-                    atomicAdd(g + 1, (double)slot[1]);
-                    atomicAdd(g + 2, (double)slot[2]);
-                    atomicAdd(g + 3, (double)slot[3]);
+                    atomicAdd(g + 0, (double)ax);
+                    atomicAdd(g + 1, (double)ay);
+                    atomicAdd(g + 2, (double)az);
+                    atomicAdd(g + 3, -(double)am);
                 } else {
-                    const uint32_t ci = KIND == KP ? idx - nb : idx;
-                    double *g = P.gcell + (size_t)ci * 10;
-                    atomicAdd(g + 0, (double)slot[3]);
-                    atomicAdd(g + 1, (double)slot[0]);
-                    atomicAdd(g + 2, (double)slot[1]);
-                    atomicAdd(g + 3, (double)slot[2]);
-                    if (KIND == KQ)
-                        for (int q = 0; q < 6; q++) atomicAdd(g + 4 + q, (double)slot[4 + q]);
+                    double *g = P.gcell + (size_t)(idx - nb) * 10;
+                    atomicAdd(g + 0, -(double)am);
+                    atomicAdd(g + 1, (double)ax);
+                    atomicAdd(g + 2, (double)ay);
+                    atomicAdd(g + 3, (double)az);
                 }
             }
-            __syncwarp();  // the staged records are reused by the next tile
         }
-        if (lane < G.count) {
-            double *g = P.gbody + (size_t)(G.first + lane) * 4;
-            atomicAdd(g + 0, (double)gx);
-            atomicAdd(g + 1, (double)gy);
-            atomicAdd(g + 2, (double)gz);
+        // the two halves met different records: add their sink sums
+        float g6[6] = {Gx.x, Gx.y, Gy.x, Gy.y, Gz.x, Gz.y};
+#pragma unroll
+        for (int q = 0; q < 6; q++) g6[q] += __shfl_xor_sync(FULL, g6[q], 16);
+        if (lane < 16) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int sk = 2 * j + h;
+                if (sk < G.count) {
+                    double *g = P.gbody + (size_t)(G.first + sk) * 4;
+                    atomicAdd(g + 0, -(double)g6[h]);
+                    atomicAdd(g + 1, -(double)g6[2 + h]);
+                    atomicAdd(g + 2, -(double)g6[4 + h]);
+                }
+            }
+        }
+    }
+}
+
+#ifndef GRAV_ADJQ_UNROLL
+#define GRAV_ADJQ_UNROLL 2
+#endif
+constexpr int kAdjQUnroll = GRAV_ADJQ_UNROLL;
+
+// The quadrupole-list adjoint, systolic like k_adjoint_points: each record
+// (negated centre offset, mass, the six staged Q components) travels through
+// the 16 lanes of its half with its ten running sums (t, w.d/r^3 + u/r and
+// dL/dQ), 20 shuffles per step of 64 interactions.
+__global__ void __launch_bounds__(256) k_adjoint_quads(AdjProblem P) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, j = lane & 15;
+    const int next = (lane & 16) | ((j + 1) & 15);
+    const float2 h = splat2(P.qsh);
+    while (true) {
+        int it = 0;
+        if (lane == 0)
+            it = atomicAdd(&P.counters[KQ], 1);
+        it = __shfl_sync(FULL, it, 0);
+        if (it >= P.nitems[KQ])
+            break;
+        const Item item = P.items[KQ][it];
+        const nln_group G = P.groups[item.group];
+        const double c[3] = {G.cen[0], G.cen[1], G.cen[2]};
+        float s[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+        float w[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+        for (int hh = 0; hh < 2; hh++) {
+            const int sk = 2 * j + hh;
+            if (sk < G.count) {
+                const float4 p = P.points[G.first + sk];
+                s[hh][0] = (float)((double)p.x - c[0]);
+                s[hh][1] = (float)((double)p.y - c[1]);
+                s[hh][2] = (float)((double)p.z - c[2]);
+                const float4 q = P.wu[G.first + sk];
+                w[hh][0] = q.x;
+                w[hh][1] = q.y;
+                w[hh][2] = q.z;
+                w[hh][3] = q.w;
+            }
+        }
+        const float2 Sx = f2(s[0][0], s[1][0]), Sy = f2(s[0][1], s[1][1]), Sz = f2(s[0][2], s[1][2]);
+        const float2 Wx = f2(w[0][0], w[1][0]), Wy = f2(w[0][1], w[1][1]), Wz = f2(w[0][2], w[1][2]);
+        const float2 U = f2(w[0][3], w[1][3]), NU = f2(-w[0][3], -w[1][3]);
+        const float2 e2 = splat2(P.eps2);
+        float2 Gx = splat2(0.f), Gy = splat2(0.f), Gz = splat2(0.f);
+        auto entry = [&](int64_t b) -> uint32_t {
+            return b + lane < item.end ? (P.list[1][b + lane] & NLN_IDX_MASK) : 0xffffffffu;
+        };
+        uint32_t e_cur = entry(item.begin), e_next = entry(item.begin + kAdjTile);
+        for (int64_t b0 = item.begin; b0 < item.end; b0 += kAdjTile) {
+            const int nt = (int)min((int64_t)kAdjTile, item.end - b0);
+            const uint32_t idx = e_cur;
+            float r[10];  // negated offset, mass, Qxx Qxy Qyy Qxz Qyz Qzz
+#pragma unroll
+            for (int q = 0; q < 10; q++) r[q] = 0.f;
+            r[0] = r[1] = r[2] = -1.0e3f;  // massless, momentless and far: adds 0
+            if (lane < nt) {
+                const nln_qcell q = P.qcells[idx];
+                r[0] = (float)(c[0] - q.cen[0]);
+                r[1] = (float)(c[1] - q.cen[1]);
+                r[2] = (float)(c[2] - q.cen[2]);
+                r[3] = q.mass;
+                const float q2[5] = {q.qxx, q.qxy, q.qyy, q.qxz, q.qyz};
+                float o[12];
+                stage_quad(o, q.R, q2);
+#pragma unroll
+                for (int k = 4; k < 10; k++) r[k] = o[k];
+            }
+            e_cur = e_next;
+            e_next = entry(b0 + 2 * kAdjTile);
+            float a[10];  // the record's sums: t (3), w.d/r^3 + u/r, dL/dQ (xx xy xz yy yz zz)
+#pragma unroll
+            for (int q = 0; q < 10; q++) a[q] = 0.f;
+#pragma unroll kAdjQUnroll
+            for (int k = 0; k < 16; k++) {
+                const float2 dx = __fadd2_rn(Sx, splat2(r[0])), dy = __fadd2_rn(Sy, splat2(r[1]));
+                const float2 dz = __fadd2_rn(Sz, splat2(r[2])), M = splat2(r[3]);
+                const float2 Qxx = splat2(r[4]), Qxy = splat2(r[5]), Qyy = splat2(r[6]);
+                const float2 Qxz = splat2(r[7]), Qyz = splat2(r[8]), Qzz = splat2(r[9]);
+                const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, e2)));
+                const float2 ri = f2(rsqrt_fast(r2.x), rsqrt_fast(r2.y));
+                const float2 ri2 = __fmul2_rn(ri, ri), ri3 = __fmul2_rn(ri, ri2);
+                const float2 ri5 = __fmul2_rn(ri3, ri2), ri7 = __fmul2_rn(ri5, ri2);
+                const float2 ri9 = __fmul2_rn(ri7, ri2);
+                const float2 wd = __ffma2_rn(Wx, dx, __ffma2_rn(Wy, dy, __fmul2_rn(Wz, dz)));
+                // monopole
+                const float2 cd = __fmul2_rn(M, __ffma2_rn(splat2(-3.f), __fmul2_rn(ri5, wd),
+                                                           __fmul2_rn(NU, ri3)));
+                const float2 mr3 = __fmul2_rn(M, ri3);
+                float2 tx = __ffma2_rn(mr3, Wx, __fmul2_rn(cd, dx));
+                float2 ty = __ffma2_rn(mr3, Wy, __fmul2_rn(cd, dy));
+                float2 tz = __ffma2_rn(mr3, Wz, __fmul2_rn(cd, dz));
+                const float2 nm = __ffma2_rn(wd, ri3, __fmul2_rn(U, ri));
+                // quadrupole: H_q w + u a_q, and dL/dQ
+                const float2 Qdx = __ffma2_rn(Qxx, dx, __ffma2_rn(Qxy, dy, __fmul2_rn(Qxz, dz)));
+                const float2 Qdy = __ffma2_rn(Qxy, dx, __ffma2_rn(Qyy, dy, __fmul2_rn(Qyz, dz)));
+                const float2 Qdz = __ffma2_rn(Qxz, dx, __ffma2_rn(Qyz, dy, __fmul2_rn(Qzz, dz)));
+                const float2 Qwx = __ffma2_rn(Qxx, Wx, __ffma2_rn(Qxy, Wy, __fmul2_rn(Qxz, Wz)));
+                const float2 Qwy = __ffma2_rn(Qxy, Wx, __ffma2_rn(Qyy, Wy, __fmul2_rn(Qyz, Wz)));
+                const float2 Qwz = __ffma2_rn(Qxz, Wx, __ffma2_rn(Qyz, Wy, __fmul2_rn(Qzz, Wz)));
+                const float2 P2 = __ffma2_rn(dx, Qdx, __ffma2_rn(dy, Qdy, __fmul2_rn(dz, Qdz)));
+                const float2 Qdw = __ffma2_rn(Wx, Qdx, __ffma2_rn(Wy, Qdy, __fmul2_rn(Wz, Qdz)));
+                // kd = h (-10 ri7 Qdw + 35 ri9 P2 wd + 5 u ri7 P2)
+                const float2 ri7P2 = __fmul2_rn(ri7, P2);
+                const float2 kd = __fmul2_rn(h, __ffma2_rn(splat2(-10.f), __fmul2_rn(ri7, Qdw),
+                                  __ffma2_rn(splat2(35.f), __fmul2_rn(__fmul2_rn(ri9, P2), wd),
+                                             __fmul2_rn(splat2(5.f), __fmul2_rn(U, ri7P2)))));
+                // kq = h (-10 ri7 wd - 2 u ri5), kw = -5 h ri7 P2, k2 = 2 h ri5
+                const float2 kq = __fmul2_rn(h, __ffma2_rn(splat2(-10.f), __fmul2_rn(ri7, wd),
+                                                           __fmul2_rn(splat2(-2.f), __fmul2_rn(U, ri5))));
+                const float2 kw = __fmul2_rn(splat2(-5.f), __fmul2_rn(h, ri7P2));
+                const float2 k2 = __fmul2_rn(splat2(2.f), __fmul2_rn(h, ri5));
+                tx = __fadd2_rn(tx, __ffma2_rn(k2, Qwx, __ffma2_rn(kd, dx, __ffma2_rn(kq, Qdx, __fmul2_rn(kw, Wx)))));
+                ty = __fadd2_rn(ty, __ffma2_rn(k2, Qwy, __ffma2_rn(kd, dy, __ffma2_rn(kq, Qdy, __fmul2_rn(kw, Wy)))));
+                tz = __fadd2_rn(tz, __ffma2_rn(k2, Qwz, __ffma2_rn(kd, dz, __ffma2_rn(kq, Qdz, __fmul2_rn(kw, Wz)))));
+                // dL/dQ = h [(u ri5 + 5 (w.d) ri7) d d^T - ri5 (w d^T + d w^T)]
+                const float2 A = __fmul2_rn(h, __ffma2_rn(U, ri5, __fmul2_rn(splat2(5.f), __fmul2_rn(wd, ri7))));
+                const float2 B = __fmul2_rn(splat2(-1.f), __fmul2_rn(h, ri5));
+                const float2 Adx = __fmul2_rn(A, dx), Ady = __fmul2_rn(A, dy), Adz = __fmul2_rn(A, dz);
+                const float2 B2 = __fmul2_rn(splat2(2.f), B);
+                const float2 gxx = __ffma2_rn(Adx, dx, __fmul2_rn(B2, __fmul2_rn(Wx, dx)));
+                const float2 gxy = __ffma2_rn(Adx, dy, __fmul2_rn(B, __ffma2_rn(Wx, dy, __fmul2_rn(Wy, dx))));
+                const float2 gxz = __ffma2_rn(Adx, dz, __fmul2_rn(B, __ffma2_rn(Wx, dz, __fmul2_rn(Wz, dx))));
+                const float2 gyy = __ffma2_rn(Ady, dy, __fmul2_rn(B2, __fmul2_rn(Wy, dy)));
+                const float2 gyz = __ffma2_rn(Ady, dz, __fmul2_rn(B, __ffma2_rn(Wy, dz, __fmul2_rn(Wz, dy))));
+                const float2 gzz = __ffma2_rn(Adz, dz, __fmul2_rn(B2, __fmul2_rn(Wz, dz)));
+                Gx = __fadd2_rn(Gx, tx);
+                Gy = __fadd2_rn(Gy, ty);
+                Gz = __fadd2_rn(Gz, tz);
+                a[0] += tx.x + tx.y;
+                a[1] += ty.x + ty.y;
+                a[2] += tz.x + tz.y;
+                a[3] += nm.x + nm.y;
+                a[4] += gxx.x + gxx.y;
+                a[5] += gxy.x + gxy.y;
+                a[6] += gxz.x + gxz.y;
+                a[7] += gyy.x + gyy.y;
+                a[8] += gyz.x + gyz.y;
+                a[9] += gzz.x + gzz.y;
+#pragma unroll
+                for (int q = 0; q < 10; q++) {
+                    r[q] = __shfl_sync(FULL, r[q], next);
+                    a[q] = __shfl_sync(FULL, a[q], next);
+                }
+            }
+            if (lane < nt) {
+                double *g = P.gcell + (size_t)idx * 10;
+                atomicAdd(g + 0, -(double)a[3]);
+                atomicAdd(g + 1, (double)a[0]);
+                atomicAdd(g + 2, (double)a[1]);
+                atomicAdd(g + 3, (double)a[2]);
+#pragma unroll
+                for (int q = 0; q < 6; q++) atomicAdd(g + 4 + q, (double)a[4 + q]);
+            }
+        }
+        float g6[6] = {Gx.x, Gx.y, Gy.x, Gy.y, Gz.x, Gz.y};
+#pragma unroll
+        for (int q = 0; q < 6; q++) g6[q] += __shfl_xor_sync(FULL, g6[q], 16);
+        if (lane < 16) {
+#pragma unroll
+            for (int hh = 0; hh < 2; hh++) {
+                const int sk = 2 * j + hh;
+                if (sk < G.count) {
+                    double *g = P.gbody + (size_t)(G.first + sk) * 4;
+                    atomicAdd(g + 0, -(double)g6[hh]);
+                    atomicAdd(g + 1, -(double)g6[2 + hh]);
+                    atomicAdd(g + 2, -(double)g6[4 + hh]);
+                }
+            }
         }
     }
 }
@@ -339,9 +510,9 @@ extern "C" int grav_plan_adjoint_CUDA(grav_plan *pl, const float *wu, float *gra
     P.err = pl->dp.err;
     const unsigned blocks = (unsigned)pl->nsm * 4;
     if (P.nitems[0] > 0)
-        k_adjoint<KP><<<blocks, 256, 0, st>>>(P);
+        k_adjoint_points<<<blocks, 256, 0, st>>>(P);
     if (P.nitems[1] > 0)
-        k_adjoint<KQ><<<blocks, 256, 0, st>>>(P);
+        k_adjoint_quads<<<blocks, 256, 0, st>>>(P);
     GC_CHECK(cudaGetLastError());
     k_adjoint_bodies<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(
         pl->dp.points, A->leaf, A->parent, pl->dp.qcells, A->gcell, A->gbody, nb,

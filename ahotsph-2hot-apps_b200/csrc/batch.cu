@@ -100,7 +100,7 @@ struct KindOf {
     // interleaved fields, one pair every 68 or 20 floats (16-byte aligned;
     // the re-lay's 8-byte stores of a half-warp hit distinct banks)
     static constexpr int pair_fields = KIND == KH ? 32 : 10;
-    static constexpr int pair_stride = KIND == KH ? 68 : 20;
+    static constexpr int pair_stride = pair_fields == 32 ? 68 : 20;
     static constexpr int pair_bytes = PAIRED ? (TILE / 2) * pair_stride * 4 : 0;
     // per-warp shared memory: stages of 32 records, the pair buffer,
     // mbarriers, image codes
