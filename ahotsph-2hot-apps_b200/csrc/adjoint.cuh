@@ -135,17 +135,17 @@ __global__ void __launch_bounds__(256) k_adjoint_points(AdjProblem P) {
                 const float2 wd = __ffma2_rn(Wx, dx, __ffma2_rn(Wy, dy, __fmul2_rn(Wz, dz)));
                 // t = m ri3 (w + (-3 ri2 (w.d) - u) d)
                 const float2 in = __ffma2_rn(__fmul2_rn(splat2(-3.f), ri2), wd, NU);
-                const float2 tx = __fmul2_rn(mr3, __ffma2_rn(in, dx, Wx));
-                const float2 ty = __fmul2_rn(mr3, __ffma2_rn(in, dy, Wy));
-                const float2 tz = __fmul2_rn(mr3, __ffma2_rn(in, dz, Wz));
-                const float2 nm = __fmul2_rn(ri, __ffma2_rn(wd, ri2, U));  // -dL/dm = (w.d) ri3 + u ri
-                Gx = __fadd2_rn(Gx, tx);
-                Gy = __fadd2_rn(Gy, ty);
-                Gz = __fadd2_rn(Gz, tz);
-                ax += tx.x + tx.y;
-                ay += ty.x + ty.y;
-                az += tz.x + tz.y;
-                am += nm.x + nm.y;
+                const float2 ex = __ffma2_rn(in, dx, Wx), ey = __ffma2_rn(in, dy, Wy);
+                const float2 ez = __ffma2_rn(in, dz, Wz);
+                const float2 qm = __ffma2_rn(wd, ri2, U);  // -dL/dm = ri qm = (w.d) ri3 + u ri
+                // t = mr3 e goes into the sinks' sums and the record's sums
+                Gx = __ffma2_rn(mr3, ex, Gx);
+                Gy = __ffma2_rn(mr3, ey, Gy);
+                Gz = __ffma2_rn(mr3, ez, Gz);
+                ax = fmaf(mr3.x, ex.x, fmaf(mr3.y, ex.y, ax));
+                ay = fmaf(mr3.x, ey.x, fmaf(mr3.y, ey.y, ay));
+                az = fmaf(mr3.x, ez.x, fmaf(mr3.y, ez.y, az));
+                am = fmaf(ri.x, qm.x, fmaf(ri.y, qm.y, am));
                 // pass record and sums on: after 16 steps they are home again
                 nx = __shfl_sync(FULL, nx, next);
                 ny = __shfl_sync(FULL, ny, next);
@@ -308,16 +308,21 @@ __global__ void __launch_bounds__(256) k_adjoint_quads(AdjProblem P) {
                 ty = __fadd2_rn(ty, __ffma2_rn(k2, Qwy, __ffma2_rn(kd, dy, __ffma2_rn(kq, Qdy, __fmul2_rn(kw, Wy)))));
                 tz = __fadd2_rn(tz, __ffma2_rn(k2, Qwz, __ffma2_rn(kd, dz, __ffma2_rn(kq, Qdz, __fmul2_rn(kw, Wz)))));
                 // dL/dQ = h [(u ri5 + 5 (w.d) ri7) d d^T - ri5 (w d^T + d w^T)]
+                // with P = A d + B w and Bw = B w: dQ_ij = P_i d_j + Bw_j d_i
                 const float2 A = __fmul2_rn(h, __ffma2_rn(U, ri5, __fmul2_rn(splat2(5.f), __fmul2_rn(wd, ri7))));
                 const float2 B = __fmul2_rn(splat2(-1.f), __fmul2_rn(h, ri5));
-                const float2 Adx = __fmul2_rn(A, dx), Ady = __fmul2_rn(A, dy), Adz = __fmul2_rn(A, dz);
-                const float2 B2 = __fmul2_rn(splat2(2.f), B);
-                const float2 gxx = __ffma2_rn(Adx, dx, __fmul2_rn(B2, __fmul2_rn(Wx, dx)));
-                const float2 gxy = __ffma2_rn(Adx, dy, __fmul2_rn(B, __ffma2_rn(Wx, dy, __fmul2_rn(Wy, dx))));
-                const float2 gxz = __ffma2_rn(Adx, dz, __fmul2_rn(B, __ffma2_rn(Wx, dz, __fmul2_rn(Wz, dx))));
-                const float2 gyy = __ffma2_rn(Ady, dy, __fmul2_rn(B2, __fmul2_rn(Wy, dy)));
-                const float2 gyz = __ffma2_rn(Ady, dz, __fmul2_rn(B, __ffma2_rn(Wy, dz, __fmul2_rn(Wz, dy))));
-                const float2 gzz = __ffma2_rn(Adz, dz, __fmul2_rn(B2, __fmul2_rn(Wz, dz)));
+                const float2 Bwx = __fmul2_rn(B, Wx), Bwy = __fmul2_rn(B, Wy), Bwz = __fmul2_rn(B, Wz);
+                const float2 Px = __ffma2_rn(A, dx, Bwx), Py = __ffma2_rn(A, dy, Bwy);
+                const float2 Pz = __ffma2_rn(A, dz, Bwz);
+                auto dq = [](float acc, float2 p, float2 d1, float2 bw, float2 d2) {
+                    return fmaf(p.x, d1.x, fmaf(p.y, d1.y, fmaf(bw.x, d2.x, fmaf(bw.y, d2.y, acc))));
+                };
+                a[4] = dq(a[4], Px, dx, Bwx, dx);
+                a[5] = dq(a[5], Px, dy, Bwy, dx);
+                a[6] = dq(a[6], Px, dz, Bwz, dx);
+                a[7] = dq(a[7], Py, dy, Bwy, dy);
+                a[8] = dq(a[8], Py, dz, Bwz, dy);
+                a[9] = dq(a[9], Pz, dz, Bwz, dz);
                 Gx = __fadd2_rn(Gx, tx);
                 Gy = __fadd2_rn(Gy, ty);
                 Gz = __fadd2_rn(Gz, tz);
@@ -325,12 +330,6 @@ __global__ void __launch_bounds__(256) k_adjoint_quads(AdjProblem P) {
                 a[1] += ty.x + ty.y;
                 a[2] += tz.x + tz.y;
                 a[3] += nm.x + nm.y;
-                a[4] += gxx.x + gxx.y;
-                a[5] += gxy.x + gxy.y;
-                a[6] += gxz.x + gxz.y;
-                a[7] += gyy.x + gyy.y;
-                a[8] += gyz.x + gyz.y;
-                a[9] += gzz.x + gzz.y;
 #pragma unroll
                 for (int q = 0; q < 10; q++) {
                     r[q] = __shfl_sync(FULL, r[q], next);
