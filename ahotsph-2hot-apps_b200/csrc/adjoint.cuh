@@ -49,8 +49,8 @@ struct AdjProblem {
 };
 
 // The point-list adjoint (bodies and cell monopoles), systolic.  Lane l
-// holds sinks 2j and 2j+1 (j = l mod 16) as one f32x2 pair, and one record
-// of the tile of 32 in registers (half h = l / 16 takes records 16h..16h+15).
+// holds sinks 2j and 2j+1 (j = l mod 16) and one record of the tile of 32
+// in registers (half h = l / 16 takes records 16h..16h+15).
 // At each of 16 steps every lane evaluates its two sinks against the record
 // it holds, adds their source-side terms to the record's running sums, and
 // passes record and sums to the next lane of its half (8 shuffles); after
@@ -58,7 +58,8 @@ struct AdjProblem {
 // their owner lane, which flushes them with FP64 atomics.  No shared memory:
 // per-record shared slots cost 8-12 shared-memory wavefronts per step of
 // 32 interactions and bound that form at 29.6 ms on the N = 2^20 Plummer
-// case (this one: about 22 ms, bound by the FMA pipe).
+// case (this one: about 19 ms).  Plain FP32: the same loop with the two
+// sinks as an f32x2 pair measured 9 % slower.
 __global__ void __launch_bounds__(256) k_adjoint_points(AdjProblem P) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, j = lane & 15;
@@ -126,27 +127,25 @@ __global__ void __launch_bounds__(256) k_adjoint_points(AdjProblem P) {
             float ax = 0.f, ay = 0.f, az = 0.f, am = 0.f;  // the record's sums of t, w.d/r^3 + u/r
 #pragma unroll 4
             for (int k = 0; k < 16; k++) {
-                const float2 dx = __fadd2_rn(Sx, splat2(nx)), dy = __fadd2_rn(Sy, splat2(ny));
-                const float2 dz = __fadd2_rn(Sz, splat2(nz)), M = splat2(m);
-                const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, e2)));
-                const float2 ri = f2(rsqrt_fast(r2.x), rsqrt_fast(r2.y));
-                const float2 ri2 = __fmul2_rn(ri, ri);
-                const float2 mr3 = __fmul2_rn(__fmul2_rn(M, ri), ri2);
-                const float2 wd = __ffma2_rn(Wx, dx, __ffma2_rn(Wy, dy, __fmul2_rn(Wz, dz)));
-                // t = m ri3 (w + (-3 ri2 (w.d) - u) d)
-                const float2 in = __ffma2_rn(__fmul2_rn(splat2(-3.f), ri2), wd, NU);
-                const float2 ex = __ffma2_rn(in, dx, Wx), ey = __ffma2_rn(in, dy, Wy);
-                const float2 ez = __ffma2_rn(in, dz, Wz);
-                const float2 qm = __ffma2_rn(wd, ri2, U);  // -dL/dm = ri qm = (w.d) ri3 + u ri
-                // t = mr3 e goes into the sinks' sums and the record's sums
-                Gx = __ffma2_rn(mr3, ex, Gx);
-                Gy = __ffma2_rn(mr3, ey, Gy);
-                Gz = __ffma2_rn(mr3, ez, Gz);
-                ax = fmaf(mr3.x, ex.x, fmaf(mr3.y, ex.y, ax));
-                ay = fmaf(mr3.x, ey.x, fmaf(mr3.y, ey.y, ay));
-                az = fmaf(mr3.x, ez.x, fmaf(mr3.y, ez.y, az));
-                am = fmaf(ri.x, qm.x, fmaf(ri.y, qm.y, am));
-                // pass record and sums on: after 16 steps they are home again
+#pragma unroll
+                for (int hh = 0; hh < 2; hh++) {
+                    const float sx_ = hh ? Sx.y : Sx.x, sy_ = hh ? Sy.y : Sy.x, sz_ = hh ? Sz.y : Sz.x;
+                    const float wx_ = hh ? Wx.y : Wx.x, wy_ = hh ? Wy.y : Wy.x, wz_ = hh ? Wz.y : Wz.x;
+                    const float u_ = hh ? U.y : U.x;
+                    const float dx = sx_ + nx, dy = sy_ + ny, dz = sz_ + nz;
+                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, e2.x)));
+                    const float ri = rsqrt_fast(r2), ri2 = ri * ri;
+                    const float mr3 = m * ri * ri2;
+                    const float wd = fmaf(wx_, dx, fmaf(wy_, dy, wz_ * dz));
+                    const float in = fmaf(-3.f * ri2, wd, -u_);
+                    const float ex = fmaf(in, dx, wx_), ey = fmaf(in, dy, wy_), ez = fmaf(in, dz, wz_);
+                    const float tx = mr3 * ex, ty = mr3 * ey, tz = mr3 * ez;
+                    if (hh) { Gx.y += tx; Gy.y += ty; Gz.y += tz; } else { Gx.x += tx; Gy.x += ty; Gz.x += tz; }
+                    ax += tx;
+                    ay += ty;
+                    az += tz;
+                    am = fmaf(ri, fmaf(wd, ri2, u_), am);
+                }
                 nx = __shfl_sync(FULL, nx, next);
                 ny = __shfl_sync(FULL, ny, next);
                 nz = __shfl_sync(FULL, nz, next);
@@ -234,7 +233,7 @@ __global__ void __launch_bounds__(256) k_adjoint_quads(AdjProblem P) {
         }
         const float2 Sx = f2(s[0][0], s[1][0]), Sy = f2(s[0][1], s[1][1]), Sz = f2(s[0][2], s[1][2]);
         const float2 Wx = f2(w[0][0], w[1][0]), Wy = f2(w[0][1], w[1][1]), Wz = f2(w[0][2], w[1][2]);
-        const float2 U = f2(w[0][3], w[1][3]), NU = f2(-w[0][3], -w[1][3]);
+        const float2 U = f2(w[0][3], w[1][3]);
         const float2 e2 = splat2(P.eps2);
         float2 Gx = splat2(0.f), Gy = splat2(0.f), Gz = splat2(0.f);
         auto entry = [&](int64_t b) -> uint32_t {
@@ -267,69 +266,64 @@ __global__ void __launch_bounds__(256) k_adjoint_quads(AdjProblem P) {
             for (int q = 0; q < 10; q++) a[q] = 0.f;
 #pragma unroll kAdjQUnroll
             for (int k = 0; k < 16; k++) {
-                const float2 dx = __fadd2_rn(Sx, splat2(r[0])), dy = __fadd2_rn(Sy, splat2(r[1]));
-                const float2 dz = __fadd2_rn(Sz, splat2(r[2])), M = splat2(r[3]);
-                const float2 Qxx = splat2(r[4]), Qxy = splat2(r[5]), Qyy = splat2(r[6]);
-                const float2 Qxz = splat2(r[7]), Qyz = splat2(r[8]), Qzz = splat2(r[9]);
-                const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, e2)));
-                const float2 ri = f2(rsqrt_fast(r2.x), rsqrt_fast(r2.y));
-                const float2 ri2 = __fmul2_rn(ri, ri), ri3 = __fmul2_rn(ri, ri2);
-                const float2 ri5 = __fmul2_rn(ri3, ri2), ri7 = __fmul2_rn(ri5, ri2);
-                const float2 ri9 = __fmul2_rn(ri7, ri2);
-                const float2 wd = __ffma2_rn(Wx, dx, __ffma2_rn(Wy, dy, __fmul2_rn(Wz, dz)));
-                // monopole
-                const float2 cd = __fmul2_rn(M, __ffma2_rn(splat2(-3.f), __fmul2_rn(ri5, wd),
-                                                           __fmul2_rn(NU, ri3)));
-                const float2 mr3 = __fmul2_rn(M, ri3);
-                float2 tx = __ffma2_rn(mr3, Wx, __fmul2_rn(cd, dx));
-                float2 ty = __ffma2_rn(mr3, Wy, __fmul2_rn(cd, dy));
-                float2 tz = __ffma2_rn(mr3, Wz, __fmul2_rn(cd, dz));
-                const float2 nm = __ffma2_rn(wd, ri3, __fmul2_rn(U, ri));
-                // quadrupole: H_q w + u a_q, and dL/dQ
-                const float2 Qdx = __ffma2_rn(Qxx, dx, __ffma2_rn(Qxy, dy, __fmul2_rn(Qxz, dz)));
-                const float2 Qdy = __ffma2_rn(Qxy, dx, __ffma2_rn(Qyy, dy, __fmul2_rn(Qyz, dz)));
-                const float2 Qdz = __ffma2_rn(Qxz, dx, __ffma2_rn(Qyz, dy, __fmul2_rn(Qzz, dz)));
-                const float2 Qwx = __ffma2_rn(Qxx, Wx, __ffma2_rn(Qxy, Wy, __fmul2_rn(Qxz, Wz)));
-                const float2 Qwy = __ffma2_rn(Qxy, Wx, __ffma2_rn(Qyy, Wy, __fmul2_rn(Qyz, Wz)));
-                const float2 Qwz = __ffma2_rn(Qxz, Wx, __ffma2_rn(Qyz, Wy, __fmul2_rn(Qzz, Wz)));
-                const float2 P2 = __ffma2_rn(dx, Qdx, __ffma2_rn(dy, Qdy, __fmul2_rn(dz, Qdz)));
-                const float2 Qdw = __ffma2_rn(Wx, Qdx, __ffma2_rn(Wy, Qdy, __fmul2_rn(Wz, Qdz)));
-                // kd = h (-10 ri7 Qdw + 35 ri9 P2 wd + 5 u ri7 P2)
-                const float2 ri7P2 = __fmul2_rn(ri7, P2);
-                const float2 kd = __fmul2_rn(h, __ffma2_rn(splat2(-10.f), __fmul2_rn(ri7, Qdw),
-                                  __ffma2_rn(splat2(35.f), __fmul2_rn(__fmul2_rn(ri9, P2), wd),
-                                             __fmul2_rn(splat2(5.f), __fmul2_rn(U, ri7P2)))));
-                // kq = h (-10 ri7 wd - 2 u ri5), kw = -5 h ri7 P2, k2 = 2 h ri5
-                const float2 kq = __fmul2_rn(h, __ffma2_rn(splat2(-10.f), __fmul2_rn(ri7, wd),
-                                                           __fmul2_rn(splat2(-2.f), __fmul2_rn(U, ri5))));
-                const float2 kw = __fmul2_rn(splat2(-5.f), __fmul2_rn(h, ri7P2));
-                const float2 k2 = __fmul2_rn(splat2(2.f), __fmul2_rn(h, ri5));
-                tx = __fadd2_rn(tx, __ffma2_rn(k2, Qwx, __ffma2_rn(kd, dx, __ffma2_rn(kq, Qdx, __fmul2_rn(kw, Wx)))));
-                ty = __fadd2_rn(ty, __ffma2_rn(k2, Qwy, __ffma2_rn(kd, dy, __ffma2_rn(kq, Qdy, __fmul2_rn(kw, Wy)))));
-                tz = __fadd2_rn(tz, __ffma2_rn(k2, Qwz, __ffma2_rn(kd, dz, __ffma2_rn(kq, Qdz, __fmul2_rn(kw, Wz)))));
-                // dL/dQ = h [(u ri5 + 5 (w.d) ri7) d d^T - ri5 (w d^T + d w^T)]
-                // with P = A d + B w and Bw = B w: dQ_ij = P_i d_j + Bw_j d_i
-                const float2 A = __fmul2_rn(h, __ffma2_rn(U, ri5, __fmul2_rn(splat2(5.f), __fmul2_rn(wd, ri7))));
-                const float2 B = __fmul2_rn(splat2(-1.f), __fmul2_rn(h, ri5));
-                const float2 Bwx = __fmul2_rn(B, Wx), Bwy = __fmul2_rn(B, Wy), Bwz = __fmul2_rn(B, Wz);
-                const float2 Px = __ffma2_rn(A, dx, Bwx), Py = __ffma2_rn(A, dy, Bwy);
-                const float2 Pz = __ffma2_rn(A, dz, Bwz);
-                auto dq = [](float acc, float2 p, float2 d1, float2 bw, float2 d2) {
-                    return fmaf(p.x, d1.x, fmaf(p.y, d1.y, fmaf(bw.x, d2.x, fmaf(bw.y, d2.y, acc))));
-                };
-                a[4] = dq(a[4], Px, dx, Bwx, dx);
-                a[5] = dq(a[5], Px, dy, Bwy, dx);
-                a[6] = dq(a[6], Px, dz, Bwz, dx);
-                a[7] = dq(a[7], Py, dy, Bwy, dy);
-                a[8] = dq(a[8], Py, dz, Bwz, dy);
-                a[9] = dq(a[9], Pz, dz, Bwz, dz);
-                Gx = __fadd2_rn(Gx, tx);
-                Gy = __fadd2_rn(Gy, ty);
-                Gz = __fadd2_rn(Gz, tz);
-                a[0] += tx.x + tx.y;
-                a[1] += ty.x + ty.y;
-                a[2] += tz.x + tz.y;
-                a[3] += nm.x + nm.y;
+#pragma unroll
+                for (int hh = 0; hh < 2; hh++) {
+                    const float wx = hh ? Wx.y : Wx.x, wy = hh ? Wy.y : Wy.x, wz = hh ? Wz.y : Wz.x;
+                    const float u = hh ? U.y : U.x, hq = h.x;
+                    const float dx = (hh ? Sx.y : Sx.x) + r[0], dy = (hh ? Sy.y : Sy.x) + r[1];
+                    const float dz = (hh ? Sz.y : Sz.x) + r[2], M = r[3];
+                    const float Qxx = r[4], Qxy = r[5], Qyy = r[6], Qxz = r[7], Qyz = r[8], Qzz = r[9];
+                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, e2.x)));
+                    const float ri = rsqrt_fast(r2), ri2 = ri * ri, ri3 = ri * ri2;
+                    const float ri5 = ri3 * ri2, ri7 = ri5 * ri2, ri9 = ri7 * ri2;
+                    const float wd = fmaf(wx, dx, fmaf(wy, dy, wz * dz));
+                    // monopole: t = m ri3 (w + (-3 ri2 (w.d) - u) d)
+                    const float in = fmaf(-3.f * ri2, wd, -u);
+                    const float mr3 = M * ri3;
+                    float tx = mr3 * fmaf(in, dx, wx), ty = mr3 * fmaf(in, dy, wy);
+                    float tz = mr3 * fmaf(in, dz, wz);
+                    // quadrupole: H_q w + u a_q, and dL/dQ
+                    const float Qdx = fmaf(Qxx, dx, fmaf(Qxy, dy, Qxz * dz));
+                    const float Qdy = fmaf(Qxy, dx, fmaf(Qyy, dy, Qyz * dz));
+                    const float Qdz = fmaf(Qxz, dx, fmaf(Qyz, dy, Qzz * dz));
+                    const float Qwx = fmaf(Qxx, wx, fmaf(Qxy, wy, Qxz * wz));
+                    const float Qwy = fmaf(Qxy, wx, fmaf(Qyy, wy, Qyz * wz));
+                    const float Qwz = fmaf(Qxz, wx, fmaf(Qyz, wy, Qzz * wz));
+                    const float P2 = fmaf(dx, Qdx, fmaf(dy, Qdy, dz * Qdz));
+                    const float Qdw = fmaf(wx, Qdx, fmaf(wy, Qdy, wz * Qdz));
+                    const float ri7P2 = ri7 * P2;
+                    const float kd = hq * fmaf(-10.f * ri7, Qdw, fmaf(35.f * ri9 * P2, wd, 5.f * u * ri7P2));
+                    const float kq = hq * fmaf(-10.f * ri7, wd, -2.f * u * ri5);
+                    const float kw = -5.f * hq * ri7P2;
+                    const float k2 = 2.f * hq * ri5;
+                    tx += fmaf(k2, Qwx, fmaf(kd, dx, fmaf(kq, Qdx, kw * wx)));
+                    ty += fmaf(k2, Qwy, fmaf(kd, dy, fmaf(kq, Qdy, kw * wy)));
+                    tz += fmaf(k2, Qwz, fmaf(kd, dz, fmaf(kq, Qdz, kw * wz)));
+                    // dL/dQ = h [(u ri5 + 5 (w.d) ri7) d d^T - ri5 (w d^T + d w^T)]
+                    //       = P_i d_j + Bw_j d_i with P = A d + B w, Bw = B w
+                    const float A = hq * fmaf(u, ri5, 5.f * wd * ri7), B = -hq * ri5;
+                    const float Bwx = B * wx, Bwy = B * wy, Bwz = B * wz;
+                    const float Px = fmaf(A, dx, Bwx), Py = fmaf(A, dy, Bwy), Pz = fmaf(A, dz, Bwz);
+                    if (hh) {
+                        Gx.y += tx;
+                        Gy.y += ty;
+                        Gz.y += tz;
+                    } else {
+                        Gx.x += tx;
+                        Gy.x += ty;
+                        Gz.x += tz;
+                    }
+                    a[0] += tx;
+                    a[1] += ty;
+                    a[2] += tz;
+                    a[3] = fmaf(ri, fmaf(wd, ri2, u), a[3]);  // -dL/dm
+                    a[4] = fmaf(Px, dx, fmaf(Bwx, dx, a[4]));
+                    a[5] = fmaf(Px, dy, fmaf(Bwy, dx, a[5]));
+                    a[6] = fmaf(Px, dz, fmaf(Bwz, dx, a[6]));
+                    a[7] = fmaf(Py, dy, fmaf(Bwy, dy, a[7]));
+                    a[8] = fmaf(Py, dz, fmaf(Bwz, dy, a[8]));
+                    a[9] = fmaf(Pz, dz, fmaf(Bwz, dz, a[9]));
+                }
 #pragma unroll
                 for (int q = 0; q < 10; q++) {
                     r[q] = __shfl_sync(FULL, r[q], next);
