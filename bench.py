@@ -39,7 +39,7 @@ FLOPS = np.array([23, 23, 66, 217], np.float64)
 # DRAM bytes (read + write) per interaction of each list kernel, from the ncu
 # capture of the 128^3 case (profiles/k_batch_box128_full.md); a launch's
 # traffic is this times its interactions (traffic grows with list entries)
-DRAM_BYTES_PER_INTERACTION = {"hexa": 0.2007, "quad": 0.192, "point": 0.167}
+DRAM_BYTES_PER_INTERACTION = {"hexa": 0.2007, "quad": 0.193, "point": 0.164}
 
 WORKLOADS = {
     # N = 2^24 periodic box, order 4 + Ewald (the metric's N)
