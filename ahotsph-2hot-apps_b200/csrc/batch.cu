@@ -878,6 +878,22 @@ int encode_rows(CUtensorMap *m, const void *base, uint64_t rows, uint32_t row_by
 }
 
 template <typename T>
+int dev_copy(grav_plan *pl, const T *src, size_t n, T **dst);
+
+// dev_copy whose copy is asynchronous on the default stream when `async`
+// (the end-to-end call's pool allocations are ordered on that stream).
+template <typename T>
+int dev_copy(grav_plan *pl, bool async, const T *src, size_t n, T **dst) {
+    if (!async || !pl->pool)
+        return dev_copy(pl, src, n, dst);
+    if (int rc = dev_copy<T>(pl, nullptr, n, dst))
+        return rc;
+    if (src && n)
+        GC_CHECK(cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, 0));
+    return 0;
+}
+
+template <typename T>
 int dev_copy(grav_plan *pl, const T *src, size_t n, T **dst) {
     *dst = nullptr;
     if (n == 0)
@@ -1137,6 +1153,26 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
         }
     }
 
+    // The tables go first: in the end-to-end call (pool allocations, stream
+    // ordered) their copies are asynchronous and overlap the work queue's
+    // host build below; the upload's later copies and its final
+    // synchronisation order everything before the kernels start.
+    DevProblem &d = pl->dp;
+    int rc = 0;
+    float4 *pts = nullptr;
+    rc |= dev_copy(pl, deferred, reinterpret_cast<const float4 *>(hp->points), (size_t)np, &pts);
+    d.points = pts;
+    nln_qcell *qc = nullptr;
+    nln_hcell *hc = nullptr;
+    if (hp->qptr && hp->qptr[ng])
+        rc |= dev_copy(pl, deferred, hp->qcells, (size_t)hp->ncells, &qc);
+    if ((hp->hptr && hp->hptr[ng]) || (want_ewald && hp->ncells > 0))
+        rc |= dev_copy(pl, deferred, hp->hcells, (size_t)hp->ncells, &hc);
+    d.qcells = qc;
+    d.hcells = hc;
+    nln_group *gr = nullptr;
+    rc |= dev_copy(pl, deferred, hp->groups, (size_t)ng, &gr);
+    d.groups = gr;
     if (pl->tune.warps_per_block < 1 || pl->tune.warps_per_block > 8)
         pl->tune.warps_per_block = 8;
     if (pl->tune.chunk_p <= 0)
@@ -1203,22 +1239,6 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
 
     t_phase[0] = now_s() - t_start;
     const double t_dev = now_s();
-    DevProblem &d = pl->dp;
-    int rc = 0;
-    float4 *pts = nullptr;
-    rc |= dev_copy(pl, reinterpret_cast<const float4 *>(hp->points), (size_t)np, &pts);
-    d.points = pts;
-    nln_qcell *qc = nullptr;
-    nln_hcell *hc = nullptr;
-    if (hp->qptr && hp->qptr[ng])
-        rc |= dev_copy(pl, hp->qcells, (size_t)hp->ncells, &qc);
-    if ((hp->hptr && hp->hptr[ng]) || (want_ewald && hp->ncells > 0))
-        rc |= dev_copy(pl, hp->hcells, (size_t)hp->ncells, &hc);
-    d.qcells = qc;
-    d.hcells = hc;
-    nln_group *gr = nullptr;
-    rc |= dev_copy(pl, hp->groups, (size_t)ng, &gr);
-    d.groups = gr;
     uint32_t *l0 = nullptr, *l1 = nullptr, *l2 = nullptr, *all_clist = nullptr;
     if (deferred) {
         // one buffer for the four lists, filled range by range by the caller
