@@ -388,6 +388,13 @@ __device__ __forceinline__ void relay_pairs(const unsigned char *stage, uint32_t
     }
 }
 
+// Compile-time shape of the paired kernels, as measured best on a B200
+// (-D to rebuild with others): unroll of the pair loop and minimum resident
+// blocks (register cap) for the order-4 (H2) and quadrupole (Q2) kernels;
+// GRAV_Q2_PAIRED=0 keeps the quadrupole kernel on the scalar loop.  Order 4:
+// unroll 1 with 3 blocks (80 registers) beat unroll 2 at 117 registers;
+// minimum blocks 0 leaves the register count to the compiler (a 1 there
+// lets it grow and cost occupancy).
 #ifndef GRAV_H2_UNROLL
 #define GRAV_H2_UNROLL 1
 #endif
@@ -408,8 +415,7 @@ constexpr int kQ2Unroll = GRAV_Q2_UNROLL;
 template <int KIND, bool STAGED>
 __global__ void __launch_bounds__(256, KIND == KH ? (STAGED ? GRAV_H2_MINB : 3)
                                                   : (KIND == KQ && STAGED ? GRAV_Q2_MINB : 0))
-    k_batch(const __grid_constant__ CUtensorMap tmap,
-                                               DevProblem P) {
+    k_batch(const __grid_constant__ CUtensorMap tmap, DevProblem P) {
     // staged quadrupole and order-4 tables run the paired (f32x2)
     // interaction on a pair-interleaved copy of each tile
     constexpr bool PAIRED = (KIND == KH || (KIND == KQ && GRAV_Q2_PAIRED)) && STAGED;
