@@ -133,6 +133,7 @@ class Plan:
 
     def __init__(self, tree, eps2, quad_phi_sign=1.0, ewald=False, tuning=None):
         self.tree = tree
+        self.ewald = bool(ewald)
         self._keep = []
 
         def keep(a, dtype=None):

@@ -414,7 +414,8 @@ def main():
         best, trials = AT.autotune(plan)
         tuning = {"chosen": {"warps_per_block": best.warps_per_block,
                              "blocks_per_sm": best.blocks_per_sm,
-                             "chunks": [best.chunk_p, best.chunk_q, best.chunk_h]},
+                             "chunks": [best.chunk_p, best.chunk_q, best.chunk_h],
+                             "ewald_side": best.ewald_side},
                   "trials": len(trials), "search_s": time.perf_counter() - ta,
                   "best_ms": min(t["ms"] for t in trials),
                   "auto_ms": trials[0]["ms"]}

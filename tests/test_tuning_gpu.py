@@ -31,6 +31,25 @@ def test_retune_keeps_results_and_autotune_picks_a_shape():
     plan.free()
 
 
+def test_autotune_places_the_ewald_moments_of_a_periodic_plan():
+    """For a periodic plan the autotuner also tries the Ewald moments on the
+    side stream and in the finish pass; whatever it picks, the forces are
+    those of the default shape."""
+    from pgrav import autotune as AT, gravcuda as gc, host, ics
+    pos, m = ics.grf_box(20, seed=52, rms_disp=0.3)
+    t = host.Tree(pos, m, tol=1e-4, box=1.0, p2cut=7, p4cut=20)
+    plan = gc.Plan(t, (1.0 / 20 / 50) ** 2, ewald=True)
+    plan.eval()
+    ref = plan.download()
+    best, trials = AT.autotune(plan, reps=1, shapes=((8, 0), (4, 0)), scales=(0.5, 1.0))
+    assert sorted({tr["ewald_side"] for tr in trials}) == [-1, 0, 2]
+    assert best.ewald_side in (-1, 0, 2)
+    plan.eval()
+    e = _rel(plan.download()[:, :3], ref[:, :3])
+    assert e.max() < 1e-6, e.max()
+    plan.free()
+
+
 def test_merged_batch_equals_members():
     from pgrav import gravcuda as gc, host, ics
     members, outs = [], []
