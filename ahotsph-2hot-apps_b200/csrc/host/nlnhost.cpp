@@ -567,16 +567,17 @@ inline uint16_t shift_code(const int s[3]) {
 }  // namespace
 
 // Distance from y to the nearest nonzero lattice vector of the periodic cube.
+// For y in the minimum-image cube (|y_k| <= L/2) that vector is a single
+// step along one axis: a step along two axes i, j is no nearer since
+// L^2 - 2 L |y_j| >= 0.  So the six axis steps suffice.
 static double lattice_gap(const double y[3], double box) {
     double D2 = INFINITY;
-    for (int a = -1; a <= 1; a++)
-        for (int b = -1; b <= 1; b++)
-            for (int e = -1; e <= 1; e++) {
-                if (!a && !b && !e)
-                    continue;
-                const double dx = y[0] - a * box, dy = y[1] - b * box, dz = y[2] - e * box;
-                D2 = std::min(D2, dx * dx + dy * dy + dz * dz);
-            }
+    for (int k = 0; k < 3; k++)
+        for (int a = -1; a <= 1; a += 2) {
+            const double dx = y[0] - (k == 0 ? a * box : 0.0), dy = y[1] - (k == 1 ? a * box : 0.0),
+                         dz = y[2] - (k == 2 ? a * box : 0.0);
+            D2 = std::min(D2, dx * dx + dy * dy + dz * dz);
+        }
     return std::sqrt(D2);
 }
 
