@@ -1026,12 +1026,13 @@ namespace {
 // own index checks stand in for the upload-time list check.
 thread_local double t_phase[5];  // grav_groups_CUDA_phases
 
-// The end-to-end call's device buffers come from a pool that keeps freed
-// memory reserved (until grav_groups_release_CUDA): mapping and unmapping
-// tens of gigabytes in every call costs as much as the evaluation's tail.
+// The end-to-end call's device buffers come from a pool per device that
+// keeps freed memory reserved (until grav_groups_release_CUDA): mapping and
+// unmapping tens of gigabytes in every call costs as much as the
+// evaluation's tail.
+constexpr int kMaxPoolDevices = 64;
 std::mutex g_pool_mu;
-cudaMemPool_t g_pool = nullptr;
-int g_pool_device = -1;
+cudaMemPool_t g_pool[kMaxPoolDevices] = {};
 
 double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
@@ -1042,22 +1043,19 @@ int e2e_pool(cudaMemPool_t *out) {
     std::lock_guard<std::mutex> lk(g_pool_mu);
     int dev = 0;
     GC_CHECK(cudaGetDevice(&dev));
-    if (g_pool && g_pool_device != dev) {
-        cudaMemPoolDestroy(g_pool);
-        g_pool = nullptr;
-    }
-    if (!g_pool) {
+    if (dev < 0 || dev >= kMaxPoolDevices)
+        return gc::set_status(-1, "grav_groups_CUDA: device %d beyond %d", dev, kMaxPoolDevices);
+    if (!g_pool[dev]) {
         cudaMemPoolProps props{};
         props.allocType = cudaMemAllocationTypePinned;
         props.handleTypes = cudaMemHandleTypeNone;
         props.location.type = cudaMemLocationTypeDevice;
         props.location.id = dev;
-        GC_CHECK(cudaMemPoolCreate(&g_pool, &props));
+        GC_CHECK(cudaMemPoolCreate(&g_pool[dev], &props));
         uint64_t keep = UINT64_MAX;
-        GC_CHECK(cudaMemPoolSetAttribute(g_pool, cudaMemPoolAttrReleaseThreshold, &keep));
-        g_pool_device = dev;
+        GC_CHECK(cudaMemPoolSetAttribute(g_pool[dev], cudaMemPoolAttrReleaseThreshold, &keep));
     }
-    *out = g_pool;
+    *out = g_pool[dev];
     return 0;
 }
 
@@ -1910,9 +1908,14 @@ extern "C" int grav_groups_CUDA(const grav_problem *hp, float *acc_phi) {
 
 extern "C" void grav_groups_release_CUDA(void) {
     std::lock_guard<std::mutex> lk(g_pool_mu);
-    if (g_pool) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    if (dev >= 0 && dev < kMaxPoolDevices && g_pool[dev]) {
         cudaDeviceSynchronize();
-        cudaMemPoolTrimTo(g_pool, 0);
+        cudaMemPoolTrimTo(g_pool[dev], 0);
     }
 }
 

@@ -251,7 +251,7 @@ void grav_plan_free(grav_plan *plan);
  */
 int grav_groups_CUDA(const grav_problem *host_problem, float *acc_phi);
 
-/* Return the memory grav_groups_CUDA keeps reserved between calls. */
+/* Return the memory grav_groups_CUDA keeps reserved between calls on the current device. */
 void grav_groups_release_CUDA(void);
 
 /*
