@@ -369,16 +369,20 @@ def main():
                          "host memory instead of the pipelined copy")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--dropin-groups", type=int, default=0,
-                    help="also time the plain FP32 drop-in path on this many sample groups")
+    ap.add_argument("--dropin-groups", type=int, default=2048,
+                    help="also time the plain FP32 drop-in path on this many sample groups "
+                         "(0: skip)")
     ap.add_argument("--kdk-steps", type=int, default=0,
                     help="also run this many graph-captured KDK steps (energy drift)")
     ap.add_argument("--kdk-dt", type=float, default=0.01)
     ap.add_argument("--kdk-rebuild", type=int, default=8)
     ap.add_argument("--autotune", action="store_true",
                     help="pick the tile shapes with the autotuner first (always for batch1024)")
-    ap.add_argument("--adjoint", action="store_true",
-                    help="also time the adjoint against the forward (Plummer 2^20, order 2)")
+    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
+                    help="skip timing the adjoint against the forward (Plummer 2^20, order 2)")
+    ap.add_argument("--adjoint", dest="adjoint", action="store_true",
+                    help="time the adjoint against the forward (the default)")
+    ap.set_defaults(adjoint=True)
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -572,7 +576,7 @@ def main():
         gc.lib().grav_groups_release_CUDA()  # the end-to-end call's kept list buffer
 
     dropin = None
-    if rank == 0 and args.dropin_groups > 0:
+    if rank == 0 and args.dropin_groups > 0 and w["kind"] != "batch":
         rate, el, sample = dropin_rate(tree, eps2, max_groups=args.dropin_groups)
         newt_ms = kms["hexa"] + kms["quad"] + kms["point"]
         batched = inter / (newt_ms * 1e-3)
