@@ -392,11 +392,12 @@ __device__ __forceinline__ void relay_pairs(const unsigned char *stage, uint32_t
 // (-D to rebuild with others): unroll of the pair loop and minimum resident
 // blocks (register cap) for the order-4 (H2) and quadrupole (Q2) kernels;
 // GRAV_Q2_PAIRED=0 keeps the quadrupole kernel on the scalar loop.  Order 4:
-// unroll 1 with 3 blocks (80 registers) beat unroll 2 at 117 registers;
-// minimum blocks 0 leaves the register count to the compiler (a 1 there
-// lets it grow and cost occupancy).
+// unroll 2 held to 3 blocks (80 registers, a few spilled words) is 0.6 %
+// faster than unroll 1 and beat unroll 2 at its own 117 registers; minimum
+// blocks 0 leaves the register count to the compiler (a 1 there lets it
+// grow and cost occupancy).
 #ifndef GRAV_H2_UNROLL
-#define GRAV_H2_UNROLL 1
+#define GRAV_H2_UNROLL 2
 #endif
 #ifndef GRAV_H2_MINB
 #define GRAV_H2_MINB 3
