@@ -12,6 +12,7 @@
 // pi/(alpha^2 L^3) that ewald() returns for x = 0.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -198,5 +199,78 @@ extern "C" int grav_direct_fp64_CUDA(const float *points, int64_t n, const int64
     cleanup();
     if (e != cudaSuccess)
         return gc::cuda_status(e, "grav_direct_fp64_CUDA");
+    return 0;
+}
+
+// ------------------------------------------------------------ FP32 peak
+//
+// The roofline denominator of the interaction kernels, measured rather than
+// derived: every thread runs kChains independent FMA chains x = x * a + b
+// (a, b runtime values, so nothing folds), one FMA (2 flops) per chain per
+// step, in a grid of blocks_per_sm x SM count blocks of 256 threads.  The
+// chains are independent, so the FMA pipes, not the latency, bound it.
+namespace {
+constexpr int kChains = 8;
+constexpr int kPeakThreads = 256;
+
+__global__ void __launch_bounds__(kPeakThreads) k_fma_peak(float *out, int iters, float a,
+                                                           float b) {
+    float x[kChains];
+#pragma unroll
+    for (int k = 0; k < kChains; k++) x[k] = (float)(threadIdx.x + k) * 1e-3f;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int u = 0; u < 16; u++)
+#pragma unroll
+            for (int k = 0; k < kChains; k++) x[k] = fmaf(x[k], a, b);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < kChains; k++) s += x[k];
+    if (s == -1.2345f)  // never true for these inputs; keeps the chains live
+        out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+}  // namespace
+
+extern "C" int grav_fp32_peak_CUDA(double *tflops) {
+    if (!tflops)
+        return gc::set_status(-1, "grav_fp32_peak_CUDA: bad arguments");
+    int dev = 0, nsm = 0;
+    GC_CHECK(cudaGetDevice(&dev));
+    GC_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int blocks = nsm * 8;  // 2048 threads per SM: 64 warps, 16 per scheduler
+    const int iters = 4096;      // x 16 x 8 FMAs per thread: ~45 ms per launch on a B200
+    float *out = nullptr;
+    GC_CHECK(cudaMalloc(&out, (size_t)blocks * kPeakThreads * sizeof(float)));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess)
+        e = cudaEventCreate(&e1);
+    double best = 0.0;
+    for (int rep = 0; rep < 6 && e == cudaSuccess; rep++) {
+        e = cudaEventRecord(e0, 0);
+        if (e == cudaSuccess) {
+            k_fma_peak<<<blocks, kPeakThreads>>>(out, iters, 0.999f, 1e-4f);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess)
+            e = cudaEventRecord(e1, 0);
+        if (e == cudaSuccess)
+            e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess)
+            e = cudaEventElapsedTime(&ms, e0, e1);
+        const double flops = 2.0 * kChains * 16.0 * iters * (double)blocks * kPeakThreads;
+        if (e == cudaSuccess && rep > 0 && ms > 0.f)  // the first launch warms up
+            best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
+    if (e0)
+        cudaEventDestroy(e0);
+    if (e1)
+        cudaEventDestroy(e1);
+    cudaFree(out);
+    if (e != cudaSuccess)
+        return gc::cuda_status(e, "grav_fp32_peak_CUDA");
+    *tflops = best;
     return 0;
 }

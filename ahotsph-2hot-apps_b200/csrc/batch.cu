@@ -413,7 +413,11 @@ __device__ __forceinline__ void relay_pairs(const unsigned char *stage, uint32_t
 #endif
 constexpr int kH2Unroll = GRAV_H2_UNROLL;
 constexpr int kQ2Unroll = GRAV_Q2_UNROLL;
-template <int KIND, bool STAGED>
+// PLAIN: the plain FP32 form the reference's lists compute in (absolute FP32
+// coordinates, nln/mac.c:1421-1561 copies cell centres as floats): sinks and
+// sources are not re-centred on the group centre and tile sums are added
+// without compensation.  It exists to be compared with the mixed form.
+template <int KIND, bool STAGED, bool PLAIN = false>
 __global__ void __launch_bounds__(256, KIND == KH ? (STAGED ? GRAV_H2_MINB : 3)
                                                   : (KIND == KQ && STAGED ? GRAV_Q2_MINB : 0))
     k_batch(const __grid_constant__ CUtensorMap tmap, DevProblem P) {
@@ -453,7 +457,8 @@ __global__ void __launch_bounds__(256, KIND == KH ? (STAGED ? GRAV_H2_MINB : 3)
             break;
         const Item item = P.items[KIND][it];
         const nln_group G = P.groups[item.group];
-        const double c[3] = {G.cen[0], G.cen[1], G.cen[2]};
+        const double c[3] = {PLAIN ? 0.0 : G.cen[0], PLAIN ? 0.0 : G.cen[1],
+                             PLAIN ? 0.0 : G.cen[2]};
         // this lane's sink, as an FP32 offset from the group centre
         float ux = 0.f, uy = 0.f, uz = 0.f;
         if (lane < G.count) {
@@ -569,10 +574,17 @@ __global__ void __launch_bounds__(256, KIND == KH ? (STAGED ? GRAV_H2_MINB : 3)
                                                   ux, uy, uz, P.eps2, P.qsh, a);
             }
             }
-            comp_add(hi[0], lo[0], a.ax);
-            comp_add(hi[1], lo[1], a.ay);
-            comp_add(hi[2], lo[2], a.az);
-            comp_add(hi[3], lo[3], a.phi);
+            if (PLAIN) {
+                hi[0] += a.ax;
+                hi[1] += a.ay;
+                hi[2] += a.az;
+                hi[3] += a.phi;
+            } else {
+                comp_add(hi[0], lo[0], a.ax);
+                comp_add(hi[1], lo[1], a.ay);
+                comp_add(hi[2], lo[2], a.az);
+                comp_add(hi[3], lo[3], a.phi);
+            }
             __syncwarp();  // every lane is done with this stage before it is refilled
         }
         tseq += ntile;
@@ -592,6 +604,7 @@ __global__ void __launch_bounds__(256, KIND == KH ? (STAGED ? GRAV_H2_MINB : 3)
 // pairs, field by field (pair j: npx0 npx1 npy0 npy1 | npz0 npz1 m0 m1, with
 // np the negated offset), so that each 16-byte shared read yields two ready
 // operand pairs for the paired FP32 instructions of mono2_plummer.
+template <bool PLAIN = false>
 __global__ void __launch_bounds__(256) k_points(DevProblem P) {
     __shared__ __align__(16) float stile[8][TILE * 4];
     const int lane = threadIdx.x & 31;
@@ -612,7 +625,8 @@ __global__ void __launch_bounds__(256) k_points(DevProblem P) {
             break;
         const Item item = P.items[KP][it];
         const nln_group G = P.groups[item.group];
-        const double c[3] = {G.cen[0], G.cen[1], G.cen[2]};
+        const double c[3] = {PLAIN ? 0.0 : G.cen[0], PLAIN ? 0.0 : G.cen[1],
+                             PLAIN ? 0.0 : G.cen[2]};
         float ux = 0.f, uy = 0.f, uz = 0.f;
         if (lane < G.count) {
             float4 sk = P.points[G.first + lane];
@@ -681,10 +695,17 @@ __global__ void __launch_bounds__(256) k_points(DevProblem P) {
                                   make_float2(B.x, B.y), make_float2(B.z, B.w), sx, sy, sz, e2, a2);
                 }
             }
-            comp_add(hi[0], lo[0], -(a2.nax.x + a2.nax.y));
-            comp_add(hi[1], lo[1], -(a2.nay.x + a2.nay.y));
-            comp_add(hi[2], lo[2], -(a2.naz.x + a2.naz.y));
-            comp_add(hi[3], lo[3], -(a2.nphi.x + a2.nphi.y));
+            if (PLAIN) {
+                hi[0] -= a2.nax.x + a2.nax.y;
+                hi[1] -= a2.nay.x + a2.nay.y;
+                hi[2] -= a2.naz.x + a2.naz.y;
+                hi[3] -= a2.nphi.x + a2.nphi.y;
+            } else {
+                comp_add(hi[0], lo[0], -(a2.nax.x + a2.nax.y));
+                comp_add(hi[1], lo[1], -(a2.nay.x + a2.nay.y));
+                comp_add(hi[2], lo[2], -(a2.naz.x + a2.naz.y));
+                comp_add(hi[3], lo[3], -(a2.nphi.x + a2.nphi.y));
+            }
             e_cur = e_nxt;
             r_cur = r_nxt;
             e_nxt = e_nn;
@@ -833,6 +854,7 @@ struct grav_plan {
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     std::vector<int64_t> lists_ptr[3];  // host copies of the P, Q, H list offsets (queue rebuilds)
     bool staged = false;                // the Q/H tensor maps view pre-staged tables
+    bool plain = false;                 // plain FP32 kernels (grav_problem.precision = 1)
     float4 *qstage = nullptr, *hstage = nullptr;  // pre-staged cell tables (k_stage_cells)
     grav_step_state *step = nullptr;  // tree links, refit scratch and the step graph
     grav_adjoint_state *adj = nullptr;  // adjoint scratch
@@ -1069,9 +1091,15 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
         return gc::set_status(-1, "grav_groups_upload_CUDA: incomplete problem");
     if (hp->nbodies + hp->ncells >= (int64_t)NLN_IDX_MASK)
         return gc::set_status(-1, "grav_groups_upload_CUDA: point table exceeds 27-bit indices");
+    if (hp->precision != 0 && hp->precision != 1)
+        return gc::set_status(-1, "grav_groups_upload_CUDA: precision must be 0 (mixed) or 1 "
+                                  "(plain FP32)");
     grav_plan *pl = new grav_plan();
-    cudaDeviceGetAttribute(&pl->nsm, cudaDevAttrMultiProcessorCount, 0);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&pl->nsm, cudaDevAttrMultiProcessorCount, dev);
     pl->hp = *hp;
+    pl->plain = hp->precision == 1;
     pl->tune = tuning ? *tuning : default_tuning();
     const int64_t ng = hp->ngroups, nb = hp->nbodies, np = hp->nbodies + hp->ncells;
     const bool deferred = nchunks > 0;
@@ -1491,12 +1519,13 @@ int launch_kind(grav_plan *pl, const DevProblem &dp, cudaStream_t st) {
         return 0;
     const int wpb = pl->tune.warps_per_block;
     if (KIND == KP) {
+        auto kp = pl->plain ? k_points<true> : k_points<false>;
         int fit = 0;
-        GC_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_points, 256, 0));
+        GC_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, kp, 256, 0));
         int per_sm = pl->tune.blocks_per_sm > 0 ? std::min(pl->tune.blocks_per_sm, fit) : fit;
         int blocks = std::max(1, per_sm) * pl->nsm;
         blocks = std::min(blocks, (dp.nitems[KP] + 7) / 8);
-        k_points<<<blocks, 256, 0, st>>>(dp);
+        kp<<<blocks, 256, 0, st>>>(dp);
         GC_CHECK(cudaGetLastError());
         pl->launches++;
         return 0;
@@ -1504,7 +1533,8 @@ int launch_kind(grav_plan *pl, const DevProblem &dp, cudaStream_t st) {
     constexpr bool paired = KIND == KH || (KIND == KQ && GRAV_Q2_PAIRED);
     const size_t smem = (size_t)wpb * (pl->staged ? KindOf<KIND, paired>::warp_bytes
                                                   : KindOf<KIND>::warp_bytes);
-    auto kern = pl->staged ? k_batch<KIND, true> : k_batch<KIND, false>;
+    auto kern = pl->staged ? (pl->plain ? k_batch<KIND, true, true> : k_batch<KIND, true, false>)
+                           : (pl->plain ? k_batch<KIND, false, true> : k_batch<KIND, false, false>);
     GC_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int fit = 0;
     GC_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, kern, wpb * 32, smem));
@@ -1954,11 +1984,13 @@ size_t dev_scratch_bytes(int64_t ng, int nk) {
            round256((size_t)(ng + 1) * sizeof(int64_t)) + (size_t)nk * ng * 64 * sizeof(float4);
 }
 
-// Once per device, with that device current: the scratch's address and the
-// kernels' shared-memory attribute.
-int dev_scratch_base(void **out) {
+// Once per device, with that device current: the scratch's address, the
+// device's SM count and the shared-memory attribute of the two row-gather
+// kernels this entry launches (point lists run in k_points, which needs none).
+int dev_scratch_base(void **out, int *nsm) {
     static std::mutex mu;
     static void *base[kMaxDevices] = {};
+    static int sms[kMaxDevices] = {};
     int dev = 0;
     GC_CHECK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices)
@@ -1967,17 +1999,25 @@ int dev_scratch_base(void **out) {
     if (!base[dev]) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_dev_scratch);
-        if (e != cudaSuccess || !p)
+        if (e != cudaSuccess)
             return gc::cuda_status(e, "grav_groups_eval_dev_CUDA: cudaGetSymbolAddress of the scratch");
-        GC_CHECK(cudaFuncSetAttribute(k_batch<KP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      8 * KindOf<KP>::warp_bytes));
+        if (!p)
+            return gc::set_status(-1, "grav_groups_eval_dev_CUDA: the scratch has no device address");
+        int n = 0;
+        e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess)
+            return gc::cuda_status(e, "grav_groups_eval_dev_CUDA: SM count");
+        if (n <= 0)
+            return gc::set_status(-1, "grav_groups_eval_dev_CUDA: device %d reports no SMs", dev);
         GC_CHECK(cudaFuncSetAttribute(k_batch<KQ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       8 * KindOf<KQ>::warp_bytes));
         GC_CHECK(cudaFuncSetAttribute(k_batch<KH, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       8 * KindOf<KH>::warp_bytes));
+        sms[dev] = n;
         base[dev] = p;
     }
     *out = base[dev];
+    *nsm = sms[dev];
     return 0;
 }
 
@@ -2046,7 +2086,8 @@ extern "C" int grav_groups_eval_dev_CUDA(const grav_problem *dp, float *acc_phi,
                               (long long)ng, need, (size_t)GRAV_DEV_SCRATCH_BYTES, (long long)fit, nk);
     }
     void *basev = nullptr;
-    if (int rc = dev_scratch_base(&basev))
+    int nsm = 0;
+    if (int rc = dev_scratch_base(&basev, &nsm))
         return rc;
     unsigned char *base = static_cast<unsigned char *>(basev);
     DevScratch S{};
@@ -2066,7 +2107,7 @@ extern "C" int grav_groups_eval_dev_CUDA(const grav_problem *dp, float *acc_phi,
 
     // a plan on the stack: device pointers only, nothing owned
     grav_plan pl;
-    cudaDeviceGetAttribute(&pl.nsm, cudaDevAttrMultiProcessorCount, 0);
+    pl.nsm = nsm;
     pl.tune = default_tuning();
     DevProblem &d = pl.dp;
     d.points = reinterpret_cast<const float4 *>(dp->points);
@@ -2106,17 +2147,31 @@ extern "C" int grav_groups_eval_dev_CUDA(const grav_problem *dp, float *acc_phi,
 
     cudaStream_t st = (cudaStream_t)stream;
     GC_CHECK(cudaMemsetAsync(base, 0, 256, st));  // queue counters and error word
+    // From here on work is queued on the shared scratch: every return waits
+    // for the stream first, so that no call leaves kernels behind that could
+    // still write the scratch when the next call starts.
+    auto finish = [&](int status) {
+        const cudaError_t e = cudaStreamSynchronize(st);
+        if (status)
+            return status;
+        return e == cudaSuccess ? 0 : gc::cuda_status(e, "grav_groups_eval_dev_CUDA: evaluation");
+    };
     k_dev_setup<<<(unsigned)((ng + 255) / 256), 256, 0, st>>>(dp->groups, dp->pptr, dp->qptr,
                                                                dp->hptr, ng, dp->nbodies, nk, S);
-    GC_CHECK(cudaGetLastError());
+    if (cudaError_t e = cudaGetLastError(); e != cudaSuccess)
+        return finish(gc::cuda_status(e, "grav_groups_eval_dev_CUDA: setup launch"));
     if ((rc = launch_kind<KH>(&pl, pl.dp, st)) || (rc = launch_kind<KQ>(&pl, pl.dp, st)) ||
         (rc = launch_kind<KP>(&pl, pl.dp, st)))
-        return rc;
+        return finish(rc);
     k_finish<<<(unsigned)((ng + 7) / 8), 256, 0, st>>>(pl.dp);
-    GC_CHECK(cudaGetLastError());
+    if (cudaError_t e = cudaGetLastError(); e != cudaSuccess)
+        return finish(gc::cuda_status(e, "grav_groups_eval_dev_CUDA: finish launch"));
     unsigned h = 0;
-    GC_CHECK(cudaMemcpyAsync(&h, S.err, sizeof(h), cudaMemcpyDeviceToHost, st));
-    GC_CHECK(cudaStreamSynchronize(st));
+    if (cudaError_t e = cudaMemcpyAsync(&h, S.err, sizeof(h), cudaMemcpyDeviceToHost, st);
+        e != cudaSuccess)
+        return finish(gc::cuda_status(e, "grav_groups_eval_dev_CUDA: reading the error word"));
+    if (int r = finish(0))
+        return r;
     if (h)
         return gc::set_status(-2, "grav_groups_eval_dev_CUDA: device error word 0x%x", h);
     return 0;

@@ -241,6 +241,25 @@ __global__ void k_runs_k1(const float *__restrict__ pos, float4 *accp, int m,
 // against per-sink runs of a packed QSZ AoSoA buffer (pQ1_mnss,
 // nln/pgrav.cu:293-368) or against the cell table by index (pQQ1,
 // nln/pgrav.cu:498-572).  One thread per sink; records staged per thread.
+// The dipole term of do_gravdq_avx8 (nln/do_grav_avx8.c:428-436) and of the
+// CUDA pQ1_mnss / pQQ1 kernels (nln/pgrav.cu:334-344,534-544), for a record
+// whose expansion centre is not its centre of mass: with d = sink - source,
+// t = -R / r^3, eq = t q:  phi += eq.d,  a += 3 d (eq.d) / r^2 - eq.
+__device__ __forceinline__ void dipole_term(float dx, float dy, float dz, float R, float qx,
+                                            float qy, float qz, Acc4 &a) {
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    const float rinv = rsqrtf(r2);
+    const float rinv2 = rinv * rinv;
+    const float t = -R * rinv * rinv2;
+    const float e0 = t * qx, e1 = t * qy, e2 = t * qz;
+    float ed = dx * e0 + dy * e1 + dz * e2;
+    a.phi += ed;
+    ed *= 3.0f * rinv2;
+    a.ax += dx * ed - e0;
+    a.ay += dy * ed - e1;
+    a.az += dz * ed - e2;
+}
+
 __global__ void k_quad_runs(const float *__restrict__ pos, float4 *accp, int m,
                             const segment *__restrict__ seg, const float *__restrict__ src,
                             int nsrc, unsigned *err) {
@@ -268,8 +287,12 @@ __global__ void k_quad_runs(const float *__restrict__ pos, float4 *accp, int m,
             rec[0] = rec[1] = rec[2] = kFarAway;
         float q2[5];
         for (int t = 0; t < 5; t++) q2[t] = __ldg(blk + (8 + t) * 8 + l);
-        stage_quad(rec, __ldg(blk + 32 + l), q2);
+        const float R = __ldg(blk + 32 + l);
+        stage_quad(rec, R, q2);
         interact<2, SOFT_NONE>(rec, sx, sy, sz, 0.0f, -0.5f, a);
+        if (mm != 0.0f)
+            dipole_term(sx - rec[0], sy - rec[1], sz - rec[2], R, __ldg(blk + 40 + l),
+                        __ldg(blk + 48 + l), __ldg(blk + 56 + l), a);
     }
     atomicAdd(&accp[i], make_float4(a.ax, a.ay, a.az, a.phi));
 }
@@ -289,15 +312,18 @@ __global__ void k_quad_index(const float *__restrict__ pos, float4 *accp, int m,
             atomicOr(err, GC_DEV_BAD_INDEX);
             continue;
         }
-        const float *q = qtab + (size_t)c * 10;  // m x y z R qxx qxy qyy qxz qyz
+        const float *q = qtab + (size_t)c * 13;  // m x y z R qxx qxy qyy qxz qyz qx qy qz
         rec[0] = __ldg(q + 1);
         rec[1] = __ldg(q + 2);
         rec[2] = __ldg(q + 3);
         rec[3] = __ldg(q);
         float q2[5];
         for (int t = 0; t < 5; t++) q2[t] = __ldg(q + 5 + t);
-        stage_quad(rec, __ldg(q + 4), q2);
+        const float R = __ldg(q + 4);
+        stage_quad(rec, R, q2);
         interact<2, SOFT_NONE>(rec, sx, sy, sz, 0.0f, -0.5f, a);
+        dipole_term(sx - rec[0], sy - rec[1], sz - rec[2], R, __ldg(q + 10), __ldg(q + 11),
+                    __ldg(q + 12), a);
     }
     atomicAdd(&accp[i], make_float4(a.ax, a.ay, a.az, a.phi));
 }
@@ -524,14 +550,15 @@ extern "C" void WalkInitSrcCUDA(float *qtab, int stride, int64_t nobj) {
         gc::set_status(-1, "WalkInitSrcCUDA: bad table (stride %d floats, need >= 20)", stride);
         return;
     }
-    std::vector<float> h((size_t)nobj * 10);
+    std::vector<float> h((size_t)nobj * 13);
     for (int64_t i = 0; i < nobj; i++) {
         const float *c = qtab + (size_t)i * stride;
-        float *o = &h[(size_t)i * 10];
+        float *o = &h[(size_t)i * 13];
         o[0] = c[0];                                  // mass
         o[1] = c[1]; o[2] = c[2]; o[3] = c[3];        // pos
         o[4] = c[5];                                  // bmax
         for (int k = 0; k < 5; k++) o[5 + k] = c[15 + k];  // qxx qxy qyy qxz qyz
+        for (int k = 0; k < 3; k++) o[10 + k] = c[12 + k];  // qx qy qz
     }
     cudaFree(S.qdev);
     S.qdev = nullptr;

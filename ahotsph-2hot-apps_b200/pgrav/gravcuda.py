@@ -27,7 +27,7 @@ EXPORTS = [
     "grav_groups_eval_dev_CUDA", "grav_plan_set_tree_CUDA", "grav_plan_refit_CUDA",
     "grav_plan_bodies", "grav_plan_integrate_CUDA", "grav_plan_step_CUDA",
     "grav_plan_adjoint_CUDA", "grav_plan_retune_CUDA", "grav_plan_get_tuning",
-    "grav_groups_CUDA_phases", "grav_groups_release_CUDA",
+    "grav_groups_CUDA_phases", "grav_groups_release_CUDA", "grav_fp32_peak_CUDA",
 ]
 
 
@@ -50,7 +50,8 @@ class Problem(ctypes.Structure):
                 ("quad_phi_sign", ctypes.c_float), ("ewald", ctypes.c_int),
                 ("cptr", ctypes.c_void_p), ("clist", ctypes.c_void_p),
                 ("lists_in_host", ctypes.c_int),
-                ("zptr", ctypes.c_void_p * 4), ("zlist", ctypes.c_void_p * 4)]
+                ("zptr", ctypes.c_void_p * 4), ("zlist", ctypes.c_void_p * 4),
+                ("precision", ctypes.c_int)]
 
 
 class Tuning(ctypes.Structure):
@@ -103,6 +104,7 @@ def lib(record_errors=True):
             "grav_plan_step_CUDA": ([vp, vp, vp, vp, vp, i32], i32),
             "grav_plan_adjoint_CUDA": ([vp, vp, vp, vp], i32),
             "grav_plan_retune_CUDA": ([vp, vp], i32), "grav_plan_get_tuning": ([vp, vp], i32),
+            "grav_fp32_peak_CUDA": ([vp], i32),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -131,7 +133,9 @@ def _p(a):
 class Plan:
     """A device-resident batched problem (grav_groups_upload_CUDA)."""
 
-    def __init__(self, tree, eps2, quad_phi_sign=1.0, ewald=False, tuning=None):
+    def __init__(self, tree, eps2, quad_phi_sign=1.0, ewald=False, tuning=None, plain=False):
+        """plain: the plain FP32 kernels (absolute coordinates, plain sums)
+        instead of the mixed-precision ones (grav_problem.precision = 1)."""
         self.tree = tree
         self.ewald = bool(ewald)
         self._keep = []
@@ -162,6 +166,7 @@ class Plan:
         prob.box = float(t.box)
         prob.quad_phi_sign = float(quad_phi_sign)
         prob.ewald = int(bool(ewald))
+        prob.precision = 1 if plain else 0
         if ewald:
             prob.cptr = keep(t.ptr[3]).ctypes.data
             prob.clist = keep(t.clist).ctypes.data if len(t.clist) else keep(np.zeros(1, np.uint32)).ctypes.data
@@ -321,6 +326,31 @@ class DropIn:
                          float(mmass), float(e), None, self.slot())
         check()
 
+    def qnss(self, base, m, seg, source, source_n):
+        """grav_qnss_CUDA ("pQ1_qnss"): sink base+i against the run seg[i]
+        (base, length records) of the QSZ AoSoA buffer `source`."""
+        seg = np.ascontiguousarray(seg, np.uint32).reshape(-1, 2)
+        source = np.ascontiguousarray(source, np.float32)
+        lib().grav_qnss_CUDA(b"pQ1_qnss", base, m, seg.ctypes.data, source.ctypes.data,
+                             int(source_n), self.slot())
+        check()
+
+    def init_src(self, qtab):
+        """WalkInitSrcCUDA: the cell table (ncells x stride floats, hexacell layout)."""
+        self._qtab = np.ascontiguousarray(qtab, np.float32)
+        lib().WalkInitSrcCUDA(self._qtab.ctypes.data, self._qtab.shape[1], len(self._qtab))
+        check()
+
+    def qns(self, base, m, source_list):
+        """grav_qns_CUDA ("pQQ1"): sinks [base, base+m) against cells source_list."""
+        sl = np.ascontiguousarray(source_list, np.int32)
+        lib().grav_qns_CUDA(b"pQQ1", base, m, sl.ctypes.data, len(sl), self.slot())
+        check()
+
+    def terminate_src(self):
+        lib().WalkTerminateSrcCUDA()
+        check()
+
     def peek(self):
         out = np.empty((len(self.btab), 4), dtype=np.float32)
         check(lib().gravcuda_peek_accumulators(out.ctypes.data, 0, len(self.btab)))
@@ -331,6 +361,13 @@ class DropIn:
         L.WalkTerminateSinkCUDA(self.btab.ctypes.data, BODY_STRIDE, len(self.btab))
         check()
         return self.btab[:, 7:11].copy()
+
+
+def fp32_peak():
+    """Measured FP32 CUDA-core peak of the current device, TFLOP/s (grav_fp32_peak_CUDA)."""
+    out = ctypes.c_double()
+    check(lib().grav_fp32_peak_CUDA(ctypes.byref(out)))
+    return out.value
 
 
 def direct_fp64(points, sinks, eps2, box=0.0):

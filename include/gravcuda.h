@@ -59,10 +59,10 @@ int qallocCUDA(int *inuse);
 
 /*
  * Cell table for grav_qns_CUDA: ncells records of `stride` floats in the
- * hexacell layout of nln/physics.h:140-157 (mass 0, pos 1..3, bmax 5,
- * quadrupole 15..19).  The reference copied wrong fields here
- * (nln/pgrav.cu:890-904); this maps the hexacell fields as named.
- * Replaces nln/pgrav.cu:878-913.
+ * hexacell layout of nln/physics.h:140-157 as built with DIPOLE (mass 0,
+ * pos 1..3, bmax 5, dipole 12..14, quadrupole 15..19).  The reference copied
+ * wrong fields here (nln/pgrav.cu:890-904); this maps the hexacell fields as
+ * named.  Replaces nln/pgrav.cu:878-913.
  */
 void WalkInitSrcCUDA(float *qtab, int stride, int64_t nobj);
 /* Free the cell table; safe when never initialised (called unconditionally, nln/main.c:953). */
@@ -112,7 +112,8 @@ void grav_mnss_CUDA(const char *routine, const int sink_base, const int m,
                     const int *source_n, const float mmass, float e, int *ncut, int q);
 /*
  * m sinks from `base` against the cells source_list[0..source_n) of the
- * table registered by WalkInitSrcCUDA, quadrupole, no softening; routine
+ * table registered by WalkInitSrcCUDA: monopole, dipole and quadrupole, no
+ * softening, the quadrupole potential with do_gravdq_avx8's sign; routine
  * "pQQ1" (nln/pgrav.cu:498-572, 1149-1200; the reference kernel was dead and
  * read the wrong bound and fields; this one reads the list as named).
  */
@@ -120,8 +121,10 @@ void grav_qns_CUDA(const char *routine, const int base, const int m, const int *
                    const int source_n, int q);
 /*
  * Sink i of [base, base+m) against the run seg[i] of the packed QSZ AoSoA
- * buffer source (source_n records), quadrupole, no softening; routine
- * "pQ1_qnss" (nln/pgrav.cu:293-368, 1297-1358).
+ * buffer source (source_n records): monopole, dipole (fields 5..7) and
+ * quadrupole, no softening, the arithmetic of do_gravdq_avx8
+ * (nln/do_grav_avx8.c:378-459); routine "pQ1_qnss" (nln/pgrav.cu:293-368,
+ * 1297-1358).
  */
 void grav_qnss_CUDA(const char *routine, const int base, const int m, const segment *seg,
                     const float *source, const int source_n, int q);
@@ -182,6 +185,12 @@ typedef struct grav_problem {
        group that does not unpack to its plain length fails the call with status -2. */
     const int64_t *zptr[4];
     const uint32_t *zlist[4];
+    /* Arithmetic of the list kernels (grav_groups_upload_CUDA and grav_groups_CUDA):
+       0 = mixed (default): sinks and sources as FP32 offsets from each group's FP64
+       centre, compensated tile sums; 1 = plain FP32, the form the reference's lists
+       compute in (absolute FP32 coordinates, nln/mac.c:1421-1561; plain sums), kept
+       for comparison.  grav_groups_eval_dev_CUDA always runs the mixed form. */
+    int precision;
 } grav_problem;
 
 typedef struct grav_plan grav_plan;
@@ -275,6 +284,15 @@ int grav_direct_fp64_CUDA(const float *points, int64_t n, const int64_t *sinks, 
                           double eps2, double box, double *out);
 
 /*
+ * The FP32 CUDA-core peak of the current device, measured: a grid of
+ * independent FMA chains (8 per thread, 2048 threads per SM) timed with CUDA
+ * events, best of five launches after one warm-up, in TFLOP/s (2 flops per
+ * FMA).  The roofline denominator of the interaction kernels; about
+ * 74 TFLOP/s on a B200 at 1965 MHz (148 SMs x 128 lanes x 2 flops x clock).
+ */
+int grav_fp32_peak_CUDA(double *tflops);
+
+/*
  * ---- the time step on the device ----
  * Between host rebuilds of the tree and lists, bodies move on the device
  * and the plan's cell tables are refitted from them.
@@ -352,11 +370,20 @@ int grav_plan_adjoint_CUDA(grav_plan *plan, const float *wu, float *grad, void *
  * The scratch is one per device, so calls that overlap on a device (other
  * host threads, other streams) race on it and must be serialised by the
  * caller.  The first call on each device (with that device current) looks
- * up the scratch's address with cudaGetSymbolAddress and sets kernel
- * attributes; make it before any stream capture.  The call enqueues on
- * `stream` (cudaStream_t as void*; NULL = legacy default), synchronises it
- * to read the error word, and returns 0, -1 for a rejected problem, or -2
- * when a kernel flagged an error (a bad group or list entry, a lost copy).
+ * up the scratch's address with cudaGetSymbolAddress, reads the device's SM
+ * count and sets kernel attributes; make it before any stream capture.  The
+ * call enqueues on `stream` (cudaStream_t as void*; NULL = legacy default)
+ * and waits for that stream before it returns, on success and on every
+ * error after its first enqueue, so no work of a returned call still uses
+ * the scratch.  It returns 0, -1 for a rejected problem, or -2 when a
+ * kernel flagged an error (a bad group, list offset or entry, a lost copy).
+ *
+ * Precondition the call cannot check: grav_problem carries no list lengths,
+ * so the last offset of each list (pptr, qptr, hptr [ngroups]) must not
+ * exceed the number of entries in the matching device list (plist, qlist,
+ * hlist).  The kernels check that offsets start at 0 or above and never
+ * decrease, and that every entry they read lies inside its table, but a
+ * final offset past the end of a list makes them read past that buffer.
  */
 #define GRAV_DEV_SCRATCH_BYTES (16u << 20)
 int grav_groups_eval_dev_CUDA(const grav_problem *device_problem, float *acc_phi, void *stream);

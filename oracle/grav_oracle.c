@@ -43,12 +43,16 @@ enum {
     ORC_QUAD_COM = 5,     /* do_gravq_avx8   nln/do_grav_avx8.c:881-950 (no softening) */
     ORC_HEXA_COM = 6,     /* do_gravh_avx8   nln/do_grav_avx8.c:572-696 (no softening) */
     ORC_MONO_BARE = 7,    /* CUDA pM         nln/pgrav.cu:370-410 (no softening, no mask) */
-    ORC_QUAD_PLUMMER_P = 8 /* do_gravpq_avx8 with the order-4 kernels' quadrupole potential
+    ORC_QUAD_PLUMMER_P = 8, /* do_gravpq_avx8 with the order-4 kernels' quadrupole potential
                               sign (+1, nln/do_grav_avx8.c:1846): the physical potential */
+    ORC_QUAD_DIPOLE = 9   /* do_gravdq_avx8  nln/do_grav_avx8.c:378-459 (no softening, dipole
+                             fields 5..7 about the record's centre; CUDA pQ1_mnss and pQQ1,
+                             nln/pgrav.cu:293-368,498-572, compute the same terms) */
 };
 
 typedef struct {
     double m, x, y, z, R;
+    double qx, qy, qz;
     double qxx, qxy, qyy, qxz, qyz;
     double qxxx, qxxy, qxyy, qyyy, qxxz, qxyz, qyyz;
     double qxxxx, qxxxy, qxxyy, qxyyy, qyyyy, qxxxz, qxxyz, qxyyz, qyyyz;
@@ -80,7 +84,7 @@ static void k1_inside(double r2, double eps_inv, double *phi, double *a) {
  * order-4 CPU kernels +1 (nln/do_grav_avx8.c:1846,638).
  */
 static void orc_interact(const orc_src *s, int order, double px, double py, double pz,
-                         double eps2, double qsign, double *acc, double *phi) {
+                         double eps2, double qsign, int dipole, double *acc, double *phi) {
     double x = px - s->x, y = py - s->y, z = pz - s->z;
     double r2 = x * x + y * y + z * z + eps2;
     double rinv = -1.0 / sqrt(r2);
@@ -96,6 +100,18 @@ static void orc_interact(const orc_src *s, int order, double px, double py, doub
     if (order < 2)
         return;
     double R = s->R;
+    if (dipole) {
+        /* do_gravdq_avx8 (nln/do_grav_avx8.c:428-436): t_1 = t R,
+         * eq = t_1 q, phi += eq.d, a += d 3 rinv2 eq.d - eq */
+        double td = t * R;
+        double e0 = td * s->qx, e1 = td * s->qy, e2 = td * s->qz;
+        double ed = x * e0 + y * e1 + z * e2;
+        *phi += ed;
+        ed *= 3.0 * rinv2;
+        acc[0] += x * ed - e0;
+        acc[1] += y * ed - e1;
+        acc[2] += z * ed - e2;
+    }
     t *= 3.0 * rinv2 * R * R;
     double eq0 = t * (s->qxx * x + s->qxy * y + s->qxz * z);
     double eq1 = t * (s->qyy * y + s->qxy * x + s->qyz * z);
@@ -151,6 +167,9 @@ static void load_lane(const float *f, long b, int sz, int l, orc_src *s) {
     s->y = FLD(2);
     s->z = FLD(3);
     s->R = FLD(4);
+    s->qx = FLD(5);
+    s->qy = FLD(6);
+    s->qz = FLD(7);
     s->qxx = FLD(8);
     s->qxy = FLD(9);
     s->qyy = FLD(10);
@@ -195,8 +214,10 @@ int orc_list_eval(int kind, const float *f, long nblk, int sz, const float *pos0
     case ORC_QUAD_COM: order = 2; qsign = -1.0; break;
     case ORC_HEXA_COM: order = 4; qsign = 1.0; break;
     case ORC_QUAD_PLUMMER_P: eps2 = e; order = 2; qsign = 1.0; break;
+    case ORC_QUAD_DIPOLE: order = 2; qsign = -1.0; break;
     default: break;
     }
+    const int dipole = kind == ORC_QUAD_DIPOLE;
     for (long b = 0; b < nblk; b++) {
         for (int l = 0; l < NL; l++) {
             orc_src s;
@@ -206,7 +227,7 @@ int orc_list_eval(int kind, const float *f, long nblk, int sz, const float *pos0
                 double r2 = x * x + y * y + z * z;
                 if (r2 < (double)e * (double)e)
                     continue;
-                orc_interact(&s, 0, px, py, pz, 0.0, 1.0, acc, &phi);
+                orc_interact(&s, 0, px, py, pz, 0.0, 1.0, 0, acc, &phi);
             } else if (kind == ORC_MONO_K1) {
                 double x = px - s.x, y = py - s.y, z = pz - s.z;
                 double r2 = x * x + y * y + z * z;
@@ -220,10 +241,10 @@ int orc_list_eval(int kind, const float *f, long nblk, int sz, const float *pos0
                     acc[2] += z * s.m * ka;
                     ncut++;
                 } else {
-                    orc_interact(&s, 0, px, py, pz, 0.0, 1.0, acc, &phi);
+                    orc_interact(&s, 0, px, py, pz, 0.0, 1.0, 0, acc, &phi);
                 }
             } else {
-                orc_interact(&s, order, px, py, pz, eps2, qsign, acc, &phi);
+                orc_interact(&s, order, px, py, pz, eps2, qsign, dipole, acc, &phi);
             }
         }
     }
@@ -446,5 +467,266 @@ void orc_groups_eval(int kind, const float *f, int sz, const long *blk_first,
             long i = sink_first[g] + s;
             orc_list_eval(kind, fb, blk_count[g], sz, pos + 3 * i, e, out + 4 * i);
         }
+    }
+}
+
+/*
+ * ---- FP64 evaluation of fixed batched index lists (the adjoint's checker) ----
+ *
+ * The batched lists (include/nlnlists.h): bodies 0..n-1 in tree order, the
+ * point table's records n + c are cell c's monopoles, quadrupole-list
+ * entries are cells.  Isolated trees only (image code 13).  Every cell's
+ * moments are taken in FP64 from its bodies: mass M, centre of mass X and
+ * the traceless Q = -3 (S2 - tr(S2)/3 I), S2 = sum m (x - X)(x - X)^T, so
+ * that a quadrupole cell adds phi += 1/2 rho^-5 d.Q.d and
+ * a += 5/2 rho^-7 (d.Q.d) d - rho^-5 Q d to its monopole term (the physical
+ * quadrupole potential, sign +1, of do_gravpq_avx8's arithmetic,
+ * nln/do_grav_avx8.c:2090-2160 with the order-4 kernels' sign, :1846);
+ * d = sink - source, rho^2 = |d|^2 + eps2.  Order-4 lists are not covered.
+ */
+typedef struct {
+    double M, X[3], Q[6]; /* Q: xx xy xz yy yz zz */
+} orc_mom;
+
+static void cell_moments(const double *x, const double *m, long first, int count, orc_mom *o) {
+    double M = 0, s[3] = {0, 0, 0};
+    for (long b = first; b < first + count; b++) {
+        M += m[b];
+        for (int d = 0; d < 3; d++) s[d] += m[b] * x[3 * b + d];
+    }
+    o->M = M;
+    for (int d = 0; d < 3; d++) o->X[d] = M > 0 ? s[d] / M : 0.0;
+    double S[6] = {0, 0, 0, 0, 0, 0};
+    for (long b = first; b < first + count; b++) {
+        double y0 = x[3 * b] - o->X[0], y1 = x[3 * b + 1] - o->X[1], y2 = x[3 * b + 2] - o->X[2];
+        S[0] += m[b] * y0 * y0; S[1] += m[b] * y0 * y1; S[2] += m[b] * y0 * y2;
+        S[3] += m[b] * y1 * y1; S[4] += m[b] * y1 * y2; S[5] += m[b] * y2 * y2;
+    }
+    double tr = (S[0] + S[3] + S[5]) / 3.0;
+    o->Q[0] = -3.0 * (S[0] - tr); o->Q[1] = -3.0 * S[1]; o->Q[2] = -3.0 * S[2];
+    o->Q[3] = -3.0 * (S[3] - tr); o->Q[4] = -3.0 * S[4]; o->Q[5] = -3.0 * (S[5] - tr);
+}
+
+/* One sink at s against a point (quad = 0) or a quadrupole cell (quad = 1). */
+static void term64(const double *s, const double *X, double M, const double *Q, int quad,
+                   double eps2, double *a, double *phi) {
+    double d0 = s[0] - X[0], d1 = s[1] - X[1], d2 = s[2] - X[2];
+    double rho2 = d0 * d0 + d1 * d1 + d2 * d2 + eps2;
+    double ri = 1.0 / sqrt(rho2), ri2 = ri * ri, ri3 = ri * ri2;
+    *phi -= M * ri;
+    a[0] -= M * d0 * ri3;
+    a[1] -= M * d1 * ri3;
+    a[2] -= M * d2 * ri3;
+    if (!quad)
+        return;
+    double q0 = Q[0] * d0 + Q[1] * d1 + Q[2] * d2;
+    double q1 = Q[1] * d0 + Q[3] * d1 + Q[4] * d2;
+    double q2 = Q[2] * d0 + Q[4] * d1 + Q[5] * d2;
+    double P2 = d0 * q0 + d1 * q1 + d2 * q2;
+    double ri5 = ri3 * ri2, ri7 = ri5 * ri2;
+    *phi += 0.5 * ri5 * P2;
+    a[0] += 2.5 * ri7 * P2 * d0 - ri5 * q0;
+    a[1] += 2.5 * ri7 * P2 * d1 - ri5 * q1;
+    a[2] += 2.5 * ri7 * P2 * d2 - ri5 * q2;
+}
+
+#define ORC_IDX_MASK ((1u << 27) - 1u)
+
+/* (X, M, Q) of point-table record idx (body, or cell monopole) from mom[]. */
+static void point_source(unsigned idx, long n, const double *x, const double *m, const orc_mom *mom,
+                         const double **X, double *M) {
+    if ((long)idx < n) {
+        *X = x + 3 * (long)idx;
+        *M = m[idx];
+    } else {
+        *X = mom[idx - n].X;
+        *M = mom[idx - n].M;
+    }
+}
+
+/*
+ * Full FP64 evaluation: out (4 doubles per body, tree order) = (a, phi) of
+ * every sink over its group's point and quadrupole lists, all cells'
+ * moments recomputed from x, m.  Returns 0, or -1 on an image code other
+ * than 13 (periodic lists are not covered).
+ */
+int orc_lists_eval64(long n, const double *x, const double *m, long ncells, const long *cfirst,
+                     const int *ccount, long ngroups, const long *gfirst, const int *gcount,
+                     const long *pptr, const unsigned *plist, const long *qptr,
+                     const unsigned *qlist, double eps2, double *out) {
+    orc_mom *mom = (orc_mom *)malloc(sizeof(orc_mom) * (size_t)(ncells > 0 ? ncells : 1));
+#pragma omp parallel for schedule(dynamic, 64)
+    for (long c = 0; c < ncells; c++) cell_moments(x, m, cfirst[c], ccount[c], &mom[c]);
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(| : bad)
+    for (long g = 0; g < ngroups; g++) {
+        for (int k = 0; k < gcount[g]; k++) {
+            long i = gfirst[g] + k;
+            double a[3] = {0, 0, 0}, phi = 0;
+            for (long e = pptr[g]; e < pptr[g + 1]; e++) {
+                if ((plist[e] >> 27) != 13u) { bad = 1; continue; }
+                const double *X; double M;
+                point_source(plist[e] & ORC_IDX_MASK, n, x, m, mom, &X, &M);
+                term64(x + 3 * i, X, M, NULL, 0, eps2, a, &phi);
+            }
+            if (qptr)
+                for (long e = qptr[g]; e < qptr[g + 1]; e++) {
+                    if ((qlist[e] >> 27) != 13u) { bad = 1; continue; }
+                    const orc_mom *c = &mom[qlist[e] & ORC_IDX_MASK];
+                    term64(x + 3 * i, c->X, c->M, c->Q, 1, eps2, a, &phi);
+                }
+            for (int d = 0; d < 3; d++) out[4 * i + d] = a[d];
+            out[4 * i + 3] = phi;
+        }
+    }
+    free(mom);
+    return bad ? -1 : 0;
+}
+
+/*
+ * The entries that depend on the selected bodies sel[0..nsel) (nsel <= 64):
+ * every (group, kind, position) whose list entry is a selected body or a
+ * cell containing one.  cparent: parent cell of each cell (-1 at a root).
+ * hits: 3 longs per hit (group, kind 0 = point / 1 = quadrupole, position),
+ * hmask: the selected bodies it depends on (bit s for sel[s]).  Returns the
+ * number of hits (filled when hits != NULL and cap allows), -1 for nsel > 64.
+ */
+long orc_fd_hits(long n, long ncells, const int *cparent, long ngroups, const long *pptr,
+                 const unsigned *plist, const long *qptr, const unsigned *qlist, int nsel,
+                 const long *sel, const long *body_leaf, long cap, long *hits,
+                 unsigned long long *hmask) {
+    if (nsel > 64)
+        return -1;
+    unsigned long long *mask = (unsigned long long *)calloc((size_t)(n + ncells), 8);
+    for (int s = 0; s < nsel; s++) {
+        unsigned long long bit = 1ull << s;
+        mask[sel[s]] |= bit;
+        for (long c = body_leaf[sel[s]]; c >= 0; c = cparent[c]) mask[n + c] |= bit;
+    }
+    long nh = 0;
+    for (long g = 0; g < ngroups; g++) {
+        for (int kind = 0; kind < 2; kind++) {
+            const long *ptr = kind ? qptr : pptr;
+            const unsigned *list = kind ? qlist : plist;
+            if (!ptr)
+                continue;
+            for (long e = ptr[g]; e < ptr[g + 1]; e++) {
+                long idx = (long)(list[e] & ORC_IDX_MASK) + (kind ? n : 0);
+                if (!mask[idx])
+                    continue;
+                if (hits && nh < cap) {
+                    hits[3 * nh] = g;
+                    hits[3 * nh + 1] = kind;
+                    hits[3 * nh + 2] = e;
+                    hmask[nh] = mask[idx];
+                }
+                nh++;
+            }
+        }
+    }
+    free(mask);
+    return nh;
+}
+
+/*
+ * The part of L = sum_i w_i.a_i + u_i phi_i (FP64, fixed lists) that depends
+ * on body j = sel[s]: every hit carrying bit s, over its group's sinks other
+ * than j, plus sink j against its own group's whole lists.  The other terms
+ * of L do not change when x_j or m_j does, so central differences of this
+ * partial sum are those of L.  Cell moments come from the bodies (x, m),
+ * so the caller perturbs x[3j + d] or m[j] and calls it twice.
+ */
+double orc_fd_partial_loss(int s, long j, long n, const double *x, const double *m, long ncells,
+                           const long *cfirst, const int *ccount, long ngroups,
+                           const long *gfirst, const int *gcount, const long *body_group,
+                           const long *pptr, const unsigned *plist, const long *qptr,
+                           const unsigned *qlist, long nhits, const long *hits,
+                           const unsigned long long *hmask, const double *w, const double *u,
+                           double eps2) {
+    const unsigned long long bit = 1ull << s;
+    double L = 0.0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : L)
+    for (long h = 0; h < nhits; h++) {
+        if (!(hmask[h] & bit))
+            continue;
+        long g = hits[3 * h], kind = hits[3 * h + 1], e = hits[3 * h + 2];
+        unsigned idx = (kind ? qlist[e] : plist[e]) & ORC_IDX_MASK;
+        orc_mom mo;
+        const double *X;
+        double M;
+        if (!kind && (long)idx < n) {
+            X = x + 3 * (long)idx;
+            M = m[idx];
+        } else {
+            long c = kind ? (long)idx : (long)idx - n;
+            cell_moments(x, m, cfirst[c], ccount[c], &mo);
+            X = mo.X;
+            M = mo.M;
+        }
+        for (int k = 0; k < gcount[g]; k++) {
+            long i = gfirst[g] + k;
+            if (i == j)
+                continue;
+            double a[3] = {0, 0, 0}, phi = 0;
+            term64(x + 3 * i, X, M, mo.Q, (int)kind, eps2, a, &phi);
+            L += w[3 * i] * a[0] + w[3 * i + 1] * a[1] + w[3 * i + 2] * a[2] + u[i] * phi;
+        }
+    }
+    /* sink j over its own lists */
+    long g = body_group[j];
+    double a[3] = {0, 0, 0}, phi = 0;
+    for (long e = pptr[g]; e < pptr[g + 1]; e++) {
+        unsigned idx = plist[e] & ORC_IDX_MASK;
+        if ((long)idx < n) {
+            term64(x + 3 * j, x + 3 * (long)idx, m[idx], NULL, 0, eps2, a, &phi);
+        } else {
+            orc_mom mo;
+            cell_moments(x, m, cfirst[idx - n], ccount[idx - n], &mo);
+            term64(x + 3 * j, mo.X, mo.M, NULL, 0, eps2, a, &phi);
+        }
+    }
+    if (qptr)
+        for (long e = qptr[g]; e < qptr[g + 1]; e++) {
+            orc_mom mo;
+            long c = qlist[e] & ORC_IDX_MASK;
+            cell_moments(x, m, cfirst[c], ccount[c], &mo);
+            term64(x + 3 * j, mo.X, mo.M, mo.Q, 1, eps2, a, &phi);
+        }
+    L += w[3 * j] * a[0] + w[3 * j + 1] * a[1] + w[3 * j + 2] * a[2] + u[j] * phi;
+    return L;
+}
+
+/*
+ * FP64 gradient of L = sum_i w_i.a_i + u_i phi_i for the Plummer-softened
+ * direct sum over all pairs (self excluded): dL/dx (3 per body), dL/dm.
+ * With d = x_i - x_j, rho^2 = |d|^2 + eps2, the pair adds to body i
+ * -(m_j)[rho^-3 w_i - 3 rho^-5 (w_i.d) d - u_i rho^-3 d] and the opposite to
+ * body j, and dL/dm_j -= rho^-3 w_i.d + u_i rho^-1 (sink i, source j).
+ */
+void orc_direct_grad(long n, const double *x, const double *m, const double *w, const double *u,
+                     double eps2, double *gx, double *gm) {
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long i = 0; i < n; i++) {
+        double g[3] = {0, 0, 0};
+        double gmi = 0;
+        for (long j = 0; j < n; j++) {
+            if (j == i)
+                continue;
+            /* sink i, source j */
+            double d[3] = {x[3 * i] - x[3 * j], x[3 * i + 1] - x[3 * j + 1], x[3 * i + 2] - x[3 * j + 2]};
+            double rho2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + eps2;
+            double ri = 1.0 / sqrt(rho2), ri3 = ri * ri * ri, ri5 = ri3 * ri * ri;
+            double wd = w[3 * i] * d[0] + w[3 * i + 1] * d[1] + w[3 * i + 2] * d[2];
+            for (int k = 0; k < 3; k++)
+                g[k] -= m[j] * (ri3 * w[3 * i + k] - 3.0 * ri5 * wd * d[k] - u[i] * ri3 * d[k]);
+            /* sink j, source i: the same pair seen from j; dL/dm_i from sink j */
+            double dj[3] = {-d[0], -d[1], -d[2]};
+            double wdj = w[3 * j] * dj[0] + w[3 * j + 1] * dj[1] + w[3 * j + 2] * dj[2];
+            for (int k = 0; k < 3; k++)
+                g[k] += m[i] * (ri3 * w[3 * j + k] - 3.0 * ri5 * wdj * dj[k] - u[j] * ri3 * dj[k]);
+            gmi -= ri3 * wdj + u[j] * ri;
+        }
+        for (int k = 0; k < 3; k++) gx[3 * i + k] = g[k];
+        gm[i] = gmi;
     }
 }

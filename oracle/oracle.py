@@ -21,7 +21,8 @@ REF_SO = os.path.join(HERE, "_ref", "libnlnref.so")
 MONO_PLUMMER, QUAD_PLUMMER, HEXA_PLUMMER = 0, 1, 2
 MONO_MASKED, MONO_K1, QUAD_COM, HEXA_COM, MONO_BARE = 3, 4, 5, 6, 7
 QUAD_PLUMMER_P = 8
-KIND_SZ = {0: 4, 1: 13, 2: 29, 3: 4, 4: 4, 5: 13, 6: 29, 7: 4, 8: 13}
+QUAD_DIPOLE = 9      # do_gravdq_avx8: unsoftened quadrupole plus the dipole fields
+KIND_SZ = {0: 4, 1: 13, 2: 29, 3: 4, 4: 4, 5: 13, 6: 29, 7: 4, 8: 13, 9: 13}
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -59,9 +60,18 @@ def unpack_runs(zptr, zlist):
     return ptr, out
 
 
+# The reference's nln/ directory, where oracle/Makefile compiles the
+# reference's own CPU code from (NLN_REF_DIR overrides); absent on a machine
+# without the reference tree, where only the restatement is built.
+REF_NLN = os.environ.get("NLN_REF_DIR", "/root/reference/nln")
+
+
 def build():
-    """Compile the restatement (and the reference kernels when the reference tree is present)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    """Compile the restatement (and the reference's CPU code when the reference tree is present)."""
+    cmd = ["make", "-s", "-C", HERE]
+    if os.path.exists(os.path.join(REF_NLN, "do_grav_avx8.c")):
+        cmd.append(f"REF_NLN={REF_NLN}")
+    subprocess.run(cmd, check=True)
 
 
 def orc():
@@ -109,6 +119,7 @@ def ref():
         lib.ref_segments_k1.argtypes = [_f32p, ctypes.c_int, ctypes.c_float, _u32p, ctypes.c_int,
                                         ctypes.c_long, _f32p, ctypes.c_float, _f32p]
         lib.ref_segments_k1.restype = ctypes.c_long
+        lib.ref_ewald_batch.argtypes = [_f64p, ctypes.c_long, ctypes.c_double, _f64p, _f64p]
         _ref = lib
     return _ref
 
@@ -165,6 +176,16 @@ def ewald(x, L):
     f = np.zeros_like(x)
     phi = np.zeros(len(x))
     orc().orc_ewald_batch(x, len(x), float(L), f, phi)
+    return f, phi
+
+
+def ref_ewald(x, L):
+    """ewald() of nln/ewald.c, compiled unmodified into oracle/_ref: (f, phi)
+    at displacements x (n, 3) = source - sink."""
+    x = np.ascontiguousarray(np.atleast_2d(x), np.float64)
+    f = np.zeros_like(x)
+    phi = np.zeros(len(x))
+    ref().ref_ewald_batch(x, len(x), float(L), f, phi)
     return f, phi
 
 

@@ -29,6 +29,8 @@ void do_grav_sK1_avx8(const vsf *, const vsf *, const float *, float *, float *,
                       const float *, int *);
 void do_gravq_avx8(const vsf *, const vsf *, const float *, float *, float *, float *,
                    const float *, int *);
+void do_gravdq_avx8(const vsf *, const vsf *, const float *, float *, float *, float *,
+                    const float *, int *);
 void do_gravh_avx8(const vsf *, const vsf *, const float *, float *, float *, float *,
                    const float *, int *);
 void do_gravmm_sK1_avx8(const float *xyz, const int stride, const float pmass, const void *mm,
@@ -51,6 +53,7 @@ static ref_grav_f pick(int kind) {
     case 4: return do_grav_sK1_avx8;
     case 5: return do_gravq_avx8;
     case 6: return do_gravh_avx8;
+    case 9: return do_gravdq_avx8;
     default: return NULL;
     }
 }
@@ -134,4 +137,16 @@ long ref_segments_k1(const float *xyz, int stride, float pmass, const uint32_t *
     out[2] += acc[2];
     out[3] += phi;
     return ncut;
+}
+
+/* the reference's periodic Green's function (nln/ewald.c:13-64) */
+void ewald(double *x, double L, double *f, double *phi);
+
+/* ewald() of nln/ewald.c at n displacements x (3 doubles each), OpenMP. */
+void ref_ewald_batch(const double *x, long n, double L, double *f, double *phi) {
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; i++) {
+        double xi[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+        ewald(xi, L, f + 3 * i, phi + i);
+    }
 }

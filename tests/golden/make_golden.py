@@ -1,6 +1,7 @@
-"""Generate tests/golden/ref_kernels.npz: outputs of the reference's own AVX
-kernels (nln/do_grav_avx8.c, nln/pgrav_vec.c compiled unmodified into
-oracle/_ref by oracle/Makefile) on seeded list inputs.
+"""Generate tests/golden/ref_kernels.npz: outputs of the reference's own CPU
+code (the AVX kernels of nln/do_grav_avx8.c and nln/pgrav_vec.c, and ewald()
+of nln/ewald.c, compiled unmodified into oracle/_ref by oracle/Makefile) on
+seeded inputs.
 
 Run here, where the reference tree is present:  python tests/golden/make_golden.py
 The fixture travels with the repository; tests compare both the CPU
@@ -95,6 +96,29 @@ def main():
     accp = np.zeros(4, np.float32)
     O.ref().ref_pinteract(0, p, accp, 1, 4, f, nblk)
     out.update(pgrav_src=src, pgrav_sink=p, pgrav_ref=accp)
+    # (added after the cases above, from their own seeds, so earlier arrays keep their values)
+    # do_gravdq_avx8: quadrupole plus the dipole fields, the arithmetic of the CUDA
+    # pQ1_mnss / pQQ1 kernels behind grav_qnss_CUDA / grav_qns_CUDA
+    rng = np.random.default_rng(20261204)
+    rec = make_records(rng, O.QUAD_COM, 203)
+    rec[:, 5:8] = rng.normal(0.0, 0.1, (203, 3)) * rec[:, :1]
+    f, nblk = O.pack_aosoa(rec)
+    sinks = rng.normal(0.0, 0.3, (16, 3)).astype(np.float32)
+    res = np.zeros((16, 4), np.float32)
+    for i, s in enumerate(sinks):
+        res[i] = O.ref_list_eval(O.QUAD_DIPOLE, f, nblk, s, 0.0)
+    k = O.QUAD_DIPOLE
+    out.update({f"k{k}_records": rec, f"k{k}_sinks": sinks, f"k{k}_e": np.float32(0.0),
+                f"k{k}_ref": res})
+    # ewald() of nln/ewald.c (compiled unmodified with the stand-in 2hot headers of
+    # oracle/ref_stubs) at seeded displacements, box sides 1 and 3
+    rng = np.random.default_rng(20261205)
+    for tag, L in (("1", 1.0), ("3", 3.0)):
+        x = np.concatenate([rng.uniform(-0.5 * L, 0.5 * L, (200, 3)),
+                            rng.uniform(-2.0 * L, 2.0 * L, (50, 3)),
+                            rng.normal(0.0, 1e-3 * L, (6, 3))])
+        fe, pe = O.ref_ewald(x, L)
+        out.update({f"ewald{tag}_x": x, f"ewald{tag}_f": fe, f"ewald{tag}_phi": pe})
     np.savez_compressed(os.path.join(HERE, "ref_kernels.npz"), **out)
     print("wrote", os.path.join(HERE, "ref_kernels.npz"))
 

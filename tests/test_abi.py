@@ -49,3 +49,53 @@ def test_reference_names_kept():
            "grav_mns_CUDA", "grav_mnss_CUDA", "grav_qns_CUDA", "grav_qnss_CUDA"]
     names = declared("gravcuda.h")
     assert all(r in names for r in ref)
+
+
+def _compile_with_reference_header(tmp_path, our_header_text, first="ours"):
+    """Compile one C unit that declares every entry point twice: from
+    include/gravcuda.h and from the reference's nln/gravcuda.h with CUDA
+    defined (the prototypes nln/mac.c is built against).  A conflicting
+    prototype is a compile error.  Returns the compiler's result."""
+    import subprocess
+    from oracle import oracle as O
+    inc = tmp_path / "inc"
+    inc.mkdir(exist_ok=True)
+    (inc / "gravcuda.h").write_text(our_header_text)
+    (inc / "nlnlists.h").write_text(open(os.path.join(REPO, "include", "nlnlists.h")).read())
+    ours = '#include "gravcuda.h"\n'
+    theirs = f'#define CUDA 1\n#include "{O.REF_NLN}/gravcuda.h"\n'
+    src = tmp_path / "both.c"
+    src.write_text("#include <stdint.h>\n"
+                   f'#include "{O.REF_NLN}/segment.h"\n'
+                   "#define SEGMENT_DEFINED 1\n" +
+                   (ours + theirs if first == "ours" else theirs + ours) +
+                   "int main(void) { return 0; }\n")
+    return subprocess.run(["gcc", "-std=gnu99", "-Werror", "-fsyntax-only", "-I", str(inc),
+                           str(src)], capture_output=True, text=True)
+
+
+def _reference_header_present():
+    from oracle import oracle as O
+    return os.path.exists(os.path.join(O.REF_NLN, "gravcuda.h"))
+
+
+@pytest.mark.skipif(not _reference_header_present(), reason="reference tree absent")
+@pytest.mark.parametrize("first", ["ours", "reference"])
+def test_prototypes_agree_with_reference_header(tmp_path, first):
+    """Signatures, not just names: every Part 1 prototype of include/gravcuda.h
+    must be compatible with nln/gravcuda.h:13-69 (both orders of inclusion)."""
+    text = open(os.path.join(REPO, "include", "gravcuda.h")).read()
+    r = _compile_with_reference_header(tmp_path, text, first)
+    assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.skipif(not _reference_header_present(), reason="reference tree absent")
+def test_prototype_drift_is_caught(tmp_path):
+    """The check above fails on a drifted signature (planted in a temporary
+    copy of the header, never in the product)."""
+    text = open(os.path.join(REPO, "include", "gravcuda.h")).read()
+    drifted = text.replace("const int source_n, const int sz, const float e, int *ncut,",
+                           "const int source_n, const int sz, const double e, int *ncut,", 1)
+    assert drifted != text
+    r = _compile_with_reference_header(tmp_path, drifted)
+    assert r.returncode != 0 and "grav_mn_CUDA" in r.stderr

@@ -119,3 +119,105 @@ def test_error_paths_return_status(gc):
         d.mn("pMp", 0, 8, f, 7, 4, 0.0)   # source_n not a multiple of 8
     d.terminate()
     assert L.gravcuda_status() == 0
+
+
+def _qsz_records(golden):
+    rec = golden[f"k{O.QUAD_DIPOLE}_records"]    # m x y z R qx qy qz qxx qxy qyy qxz qyz
+    assert np.abs(rec[:, 5:8]).max() > 0           # the dipole fields are exercised
+    return rec
+
+
+def test_grav_qnss_matches_reference_fixture(gc, golden):
+    """grav_qnss_CUDA ("pQ1_qnss", live at nln/mac.c:467; reference kernel
+    nln/pgrav.cu:293-368) on the committed outputs of do_gravdq_avx8, the
+    same arithmetic: every sink against the whole buffer."""
+    rec = _qsz_records(golden)
+    f, nblk = O.pack_aosoa(rec)
+    sinks = golden[f"k{O.QUAD_DIPOLE}_sinks"]
+    d = gc.DropIn(gc.body_table(sinks, 1.0))
+    seg = np.tile(np.array([[0, nblk * 8]], np.uint32), (len(sinks), 1))
+    d.qnss(0, len(sinks), seg, f, nblk * 8)
+    got = d.terminate()
+    ref = golden[f"k{O.QUAD_DIPOLE}_ref"]
+    assert rms_rel(got[:, :3], ref[:, :3]) < RMS_TOL
+    assert rms_rel(got[:, 3:], ref[:, 3:]) < RMS_TOL
+
+
+def test_grav_qnss_runs_match_oracle(gc, golden):
+    """Per-sink runs as nln/mac.c:395-425 queues them (each sink its own run
+    of 8-record blocks of one shared buffer, empty runs included), at a
+    nonzero sink base, against the oracle's do_gravdq restatement and, when
+    built, the compiled reference on the same runs."""
+    rng = np.random.default_rng(3)
+    rec = _qsz_records(golden)
+    f, nblk = O.pack_aosoa(rec)
+    nsink, base = 40, 7
+    sinks = rng.normal(0.0, 0.3, (base + nsink, 3)).astype(np.float32)
+    b0 = rng.integers(0, nblk, nsink)
+    nb = np.minimum(rng.integers(0, 8, nsink), nblk - b0)
+    nb[3] = 0
+    seg = np.stack([b0 * 8, nb * 8], 1).astype(np.uint32)
+    d = gc.DropIn(gc.body_table(sinks, 1.0))
+    d.qnss(base, nsink, seg, f, nblk * 8)
+    got = d.terminate()[base:]
+    for i in range(nsink):
+        sub = O.aligned_f32(int(nb[i]) * 8 * 13)
+        sub[:] = f[b0[i] * 8 * 13:(b0[i] + nb[i]) * 8 * 13]
+        want = O.list_eval(O.QUAD_DIPOLE, sub, int(nb[i]), sinks[base + i], 0.0)
+        if nb[i] == 0:
+            assert np.all(got[i] == 0)
+            continue
+        assert np.linalg.norm(got[i, :3] - want[:3]) <= 1e-5 * np.linalg.norm(want[:3])
+        assert abs(got[i, 3] - want[3]) <= 1e-5 * abs(want[3])
+        if O.ref_available():
+            r = O.ref_list_eval(O.QUAD_DIPOLE, sub, int(nb[i]), sinks[base + i], 0.0)
+            assert np.linalg.norm(got[i, :3] - r[:3]) <= 2e-5 * np.linalg.norm(r[:3])
+
+
+def test_grav_qns_matches_oracle(gc, golden):
+    """grav_qns_CUDA ("pQQ1", nln/pgrav.cu:1149-1200) on a hexacell table
+    registered by WalkInitSrcCUDA (nln/physics.h:140-157 with DIPOLE: 40
+    floats per cell, mass 0, pos 1..3, bmax 5, dipole 12..14, quadrupole
+    15..19) and index lists with repeats, against do_gravdq's restatement on
+    the same cells packed as a QSZ list."""
+    rng = np.random.default_rng(5)
+    rec = _qsz_records(golden)
+    nc = len(rec)
+    qtab = np.zeros((nc, 40), np.float32)
+    qtab[:, 0] = rec[:, 0]
+    qtab[:, 1:4] = rec[:, 1:4]
+    qtab[:, 4] = 9.0      # rcrit_m: not read
+    qtab[:, 5] = rec[:, 4]
+    qtab[:, 12:15] = rec[:, 5:8]
+    qtab[:, 15:20] = rec[:, 8:13]
+    qtab[:, 20:] = 7.0    # higher moments and bookkeeping: not read
+    nsink = 50
+    sinks = rng.normal(0.0, 0.3, (nsink, 3)).astype(np.float32)
+    d = gc.DropIn(gc.body_table(sinks, 1.0))
+    d.init_src(qtab)
+    lists = [rng.integers(0, nc, int(k)) for k in (100, 37, 1)]
+    spans = [(0, 20), (20, 25), (45, 5)]
+    for (b, m), sl in zip(spans, lists):
+        d.qns(b, m, sl)
+    got = d.terminate()
+    d.terminate_src()
+    for (b, m), sl in zip(spans, lists):
+        f, nblk = O.pack_aosoa(rec[sl])
+        for i in range(b, b + m):
+            want = O.list_eval(O.QUAD_DIPOLE, f, nblk, sinks[i], 0.0)
+            assert np.linalg.norm(got[i, :3] - want[:3]) <= 1e-5 * np.linalg.norm(want[:3])
+            assert abs(got[i, 3] - want[3]) <= 1e-5 * abs(want[3])
+
+
+def test_grav_qns_rejects_bad_indices(gc, golden):
+    rec = _qsz_records(golden)
+    qtab = np.zeros((len(rec), 40), np.float32)
+    qtab[:, 0] = rec[:, 0]
+    qtab[:, 1:4] = rec[:, 1:4]
+    qtab[:, 5] = rec[:, 4]
+    d = gc.DropIn(gc.body_table(np.zeros((4, 3), np.float32), 1.0))
+    d.init_src(qtab)
+    d.qns(0, 4, np.array([0, len(rec) + 5], np.int32))   # one entry past the table
+    with pytest.raises(gc.GravError):
+        d.terminate()
+    d.terminate_src()

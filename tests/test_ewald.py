@@ -165,3 +165,103 @@ def test_direct_ewald_oracle_softening_limit():
     # momentum: sum_i m_i a_i over all sinks vanishes
     a, _ = O.direct_ewald(pos, m, 1.0, 0.0, np.arange(40))
     assert np.abs((m[:, None] * a).sum(0)).max() < 1e-10
+
+
+def test_restatement_matches_reference_golden(golden):
+    """orc_ewald against the committed outputs of the reference's ewald()
+    (tests/golden/make_golden.py; runs without the reference tree)."""
+    for tag, L in (("1", 1.0), ("3", 3.0)):
+        f, p = O.ewald(golden[f"ewald{tag}_x"], L)
+        f0, p0 = golden[f"ewald{tag}_f"], golden[f"ewald{tag}_phi"]
+        assert np.abs(f - f0).max() <= 1e-12 * np.abs(f0).max()
+        assert np.abs(p - p0).max() <= 1e-12 * np.abs(p0).max()
+
+
+# ---- pinned to the reference's own ewald() (nln/ewald.c:13-64, compiled
+# unmodified into oracle/_ref by oracle/Makefile with stand-in 2hot headers)
+needs_ref = pytest.mark.skipif(not O.ref_available(),
+                               reason="oracle/_ref (the reference's compiled CPU code) is not built")
+
+
+def _displacements(L, n=12000, seed=11):
+    rng = np.random.default_rng(seed)
+    x = np.concatenate([
+        rng.uniform(-0.5 * L, 0.5 * L, (n - 2000, 3)),     # minimum-image cube
+        rng.uniform(-2.0 * L, 2.0 * L, (1000, 3)),          # other images
+        rng.normal(0.0, 1e-4 * L, (500, 3)),                # near the lattice site
+        np.eye(3)[rng.integers(0, 3, 500)] * rng.uniform(-L, L, (500, 1))])  # on the axes
+    x[0] = 0.0                                              # the x == 0 rule
+    return x
+
+
+@needs_ref
+@pytest.mark.parametrize("L", [1.0, 3.0])
+def test_restatement_matches_reference_ewald(L):
+    """orc_ewald against the reference's ewald() at 12,000 displacements:
+    relative agreement 1e-12 (the two evaluate the same sums in the same
+    order, so they agree exactly)."""
+    x = _displacements(L)
+    f0, p0 = O.ref_ewald(x, L)
+    f1, p1 = O.ewald(x, L)
+    assert np.all(np.isfinite(f0)) and np.all(np.isfinite(p0))
+    assert np.abs(f1 - f0).max() <= 1e-12 * np.abs(f0).max()
+    assert np.abs(p1 - p0).max() <= 1e-12 * np.abs(p0).max()
+    assert np.array_equal(f1, f0) and np.array_equal(p1, p0)
+
+
+@needs_ref
+@pytest.mark.parametrize("L", [1.0, 3.0])
+def test_table_values_match_reference_ewald(host, L):
+    """The FP64 table's C = phi + 1/r and gradient (csrc/host/ewald_table.cpp,
+    analytic derivatives of the same Ewald sum) against the reference's
+    ewald() at 10,000 displacements in the table's reach cube: C within
+    1e-12 / L, gradient within 1e-11 / L^2 (the force itself is up to
+    ~800 / L^2 there)."""
+    rng = np.random.default_rng(3)
+    y = rng.uniform(-0.625 * L, 0.625 * L, (10000, 3))
+    f, p = O.ref_ewald(y, L)
+    r = np.linalg.norm(y, axis=1)
+    o = np.array([ev(host, yy, L)[:4] for yy in y])
+    assert np.abs(o[:, 0] - (p + 1.0 / r)).max() < 1e-12 / L
+    assert np.abs(o[:, 1:4] - (f - y / r[:, None] ** 3)).max() < 1e-11 / L ** 2
+
+
+@needs_ref
+def test_table_interpolation_bound_against_reference(host):
+    """The device lookup (csrc/ewald.cuh ew_lookup: fourth-order Taylor
+    expansion about the nearest node of the 32^3 table over [0, 0.625 L]^3),
+    emulated here in FP64, against the reference's ewald() at 4,000 random
+    displacements: C within 1e-7 / L and its gradient within 3e-5 / L^2
+    (largest gradient 7 / L^2).  In FP32 on the device C's rounding adds
+    about 1e-6 / L."""
+    import math
+    n, L, reach = 32, 1.0, 0.625
+    tab = np.zeros(n ** 3 * NQ)
+    assert host.nln_ewald_table(L, n, reach, tab.ctypes.data) == 0
+    tab = tab.reshape(n, n, n, NQ)
+    h = reach * L / (n - 1)
+
+    def idx(a):  # multi-index offset of include/nlnlists.h
+        s = sum(a)
+        return s * (s + 1) * (s + 2) // 6 + (a[1] + a[2]) * (a[1] + a[2] + 1) // 2 + a[2]
+
+    rng = np.random.default_rng(5)
+    y = rng.uniform(-reach * L, reach * L, (4000, 3))
+    sg = np.where(y < 0, -1.0, 1.0)
+    a = np.abs(y)
+    ijk = np.minimum(np.rint(a / h).astype(int), n - 1)
+    d = a - ijk * h
+    V = tab[ijk[:, 0], ijk[:, 1], ijk[:, 2]]
+    terms = [b for b in itertools.product(range(5), repeat=3) if sum(b) <= 4]
+    out = np.zeros((len(y), 4))
+    for col, al in enumerate([(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1)]):
+        acc = np.zeros(len(y))
+        for b in terms:
+            if sum(al) + sum(b) <= 4:
+                w = np.prod([d[:, k] ** b[k] / math.factorial(b[k]) for k in range(3)], axis=0)
+                acc += V[:, idx(tuple(al[k] + b[k] for k in range(3)))] * w
+        out[:, col] = acc * np.prod([sg[:, k] ** al[k] for k in range(3)], axis=0)
+    f, p = O.ref_ewald(y, L)
+    r = np.linalg.norm(y, axis=1)
+    assert np.abs(out[:, 0] - (p + 1.0 / r)).max() < 1e-7 / L
+    assert np.abs(out[:, 1:4] - (f - y / r[:, None] ** 3)).max() < 3e-5 / L ** 2

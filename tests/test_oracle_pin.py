@@ -8,7 +8,7 @@ import pytest
 from oracle import oracle as O
 
 KINDS = [O.MONO_PLUMMER, O.QUAD_PLUMMER, O.HEXA_PLUMMER, O.MONO_MASKED, O.MONO_K1, O.QUAD_COM,
-         O.HEXA_COM]
+         O.HEXA_COM, O.QUAD_DIPOLE]
 
 
 def rel(a, b):
@@ -95,10 +95,11 @@ def test_restatement_matches_compiled_reference(kind, seed):
     if sz > 4:
         rec[:, 1:4] += np.sign(rec[:, 1:4]) * 1.0
         rec[:, 4] = rng.uniform(0.01, 0.2, n)
-        rec[:, 5:8] = 0.0
+        # dipole fields: zero about the centre of mass, except for do_gravdq's records
+        rec[:, 5:8] = 0.0 if kind != O.QUAD_DIPOLE else rng.normal(0.0, 0.1, (n, 3)) * rec[:, :1]
     f, nblk = O.pack_aosoa(rec)
     e = {O.MONO_PLUMMER: 1e-3, O.QUAD_PLUMMER: 1e-3, O.HEXA_PLUMMER: 1e-3, O.MONO_MASKED: 0.3,
-         O.MONO_K1: 2.0, O.QUAD_COM: 0.0, O.HEXA_COM: 0.0}[kind]
+         O.MONO_K1: 2.0, O.QUAD_COM: 0.0, O.HEXA_COM: 0.0, O.QUAD_DIPOLE: 0.0}[kind]
     for s in rng.uniform(-0.5, 0.5, (8, 3)).astype(np.float32):
         a = O.list_eval(kind, f, nblk, s, e)
         b = O.ref_list_eval(kind, f, nblk, s, e)
