@@ -48,7 +48,7 @@ struct Item {
     int64_t begin, end;
 };
 
-// One group's correction moments as k_ewald_side stores them (EwMoments).
+// One group's correction moments as k_ewald_moments stores them (EwMoments).
 struct EwStored {
     double lo[10];
     float hi[25];
@@ -82,7 +82,13 @@ struct DevProblem {
     EwTab ew;
     float ew_self;             // C(0) - pi/(alpha^2 L^3): the self term ewald() leaves out
     float ew_trace;            // trace of the Hessian of C: -4 pi / L^3
-    EwStored *ewm;             // per-group moments from k_ewald_side, or null: k_finish computes them
+    EwStored *ewm;             // per-group moments from k_ewald_moments
+    // FP64 centres of the cells for the point table's monopole records (the
+    // mixed form re-centres them like every other source): a pre-staged cell
+    // table (centre x, y in floats 0-3, z in floats 10-11 of each record of
+    // cstride float4s), or null, where the FP32 point record is used
+    const float4 *cstage;
+    int cstride;
 };
 
 template <int KIND, bool PAIRED = false>
@@ -614,6 +620,7 @@ __global__ void __launch_bounds__(256) k_points(DevProblem P) {
     float *mine = tile + (lane >> 1) * 8 + (lane & 1);
     const uint32_t *list = P.list[KP];
     const uint32_t ntab = (uint32_t)P.ntab[KP];
+    const uint32_t nb = ntab - (uint32_t)P.ncells;
     const bool periodic = P.box > 0;
     const float2 e2 = make_float2(P.eps2, P.eps2);
     while (true) {
@@ -643,9 +650,15 @@ __global__ void __launch_bounds__(256) k_points(DevProblem P) {
             const int64_t k = item.begin + (int64_t)t * TILE + lane;
             return (t < ntile && k < item.end) ? __ldg(list + k) : kNone;
         };
-        auto record = [&](uint32_t &e) -> float4 {
+        // a record's position (FP64: a cell monopole's centre from the staged
+        // cell table in the mixed form) and mass
+        struct Rec {
+            double x, y, z;
+            float m;
+        };
+        auto record = [&](uint32_t &e) -> Rec {
             if (e == kNone)
-                return make_float4(0.f, 0.f, 0.f, 0.f);
+                return Rec{0.0, 0.0, 0.0, 0.f};
             uint32_t idx = e & NLN_IDX_MASK;
             // entries are checked at upload, except in the pipelined end-to-end call
             if (idx >= ntab || (e >> NLN_IDX_BITS) > 26u) {
@@ -653,13 +666,21 @@ __global__ void __launch_bounds__(256) k_points(DevProblem P) {
                 idx = 0;
                 e = NLN_SHIFT_NONE << NLN_IDX_BITS;
             }
-            return __ldg(P.points + idx);
+            const float4 p = __ldg(P.points + idx);
+            if (!PLAIN && P.cstage && idx >= nb) {
+                const float4 *cs = P.cstage + (size_t)(idx - nb) * P.cstride;
+                const float4 a = __ldg(cs), b = __ldg(cs + 2);
+                return Rec{__hiloint2double(__float_as_int(a.y), __float_as_int(a.x)),
+                           __hiloint2double(__float_as_int(a.w), __float_as_int(a.z)),
+                           __hiloint2double(__float_as_int(b.w), __float_as_int(b.z)), p.w};
+            }
+            return Rec{(double)p.x, (double)p.y, (double)p.z, p.w};
         };
         uint32_t e_cur = entry(0);
-        float4 r_cur = record(e_cur);
+        Rec r_cur = record(e_cur);
         uint32_t e_nxt = entry(1);
         for (int t = 0; t < ntile; t++) {
-            const float4 r_nxt = record(e_nxt);  // consumed next tile
+            const Rec r_nxt = record(e_nxt);  // consumed next tile
             const uint32_t e_nn = entry(t + 2);
             const int nt = (int)min((int64_t)TILE, nent - (int64_t)t * TILE);
             // an absent record: massless and far from every sink
@@ -668,10 +689,10 @@ __global__ void __launch_bounds__(256) k_points(DevProblem P) {
                 double sxs = 0.0, sys = 0.0, szs = 0.0;
                 if (periodic)
                     decode_shift(e_cur >> NLN_IDX_BITS, P.box, sxs, sys, szs);
-                npx = (float)(c[0] - ((double)r_cur.x + sxs));
-                npy = (float)(c[1] - ((double)r_cur.y + sys));
-                npz = (float)(c[2] - ((double)r_cur.z + szs));
-                m = r_cur.w;
+                npx = (float)(c[0] - (r_cur.x + sxs));
+                npy = (float)(c[1] - (r_cur.y + sys));
+                npz = (float)(c[2] - (r_cur.z + szs));
+                m = r_cur.m;
             }
             __syncwarp();  // the previous tile is no longer read
             mine[0] = npx;
@@ -716,13 +737,196 @@ __global__ void __launch_bounds__(256) k_points(DevProblem P) {
     }
 }
 
-// Periodic correction moments of group g (ewald.cuh) over its correction
-// list, lanes striding it.  Bodies count as masses; a cell adds its
+// Periodic correction moments (ewald.cuh) of groups gbegin..ngroups-1, one
+// warp per group from a queue (counter 3), lanes striding the group's
+// correction list, stored per group for k_finish.  Bodies count as masses; a
+// cell adds its traceless second to fourth moments (the list's cells
+// include coarse ones standing for whole subtrees, and cells a tenth of the
+// box wide near the half-box, where C varies on the scale of the cell), and
+// its second-moment trace B2/3 against the constant Laplacian of C.
+//
+// The loads are what bound this loop: each entry needs its table node
+// (224 B) and its cell record (128 B) from scattered addresses, and the node
+// depends on the record's centre.  So every lane runs a three-deep pipeline
+// of its own entries: list word three tiles ahead, the source's FP64 centre
+// (a plain load) two tiles ahead, and one tile ahead a per-lane cp.async of
+// the node and the record into this warp's shared-memory stage, laid out
+// chunk-major ([chunk][lane] float4) so that the compute's reads are
+// conflict-free.  Each lane reads only what it copied itself.
+constexpr int kEwNodeChunks = 14;  // 56 floats: C and its derivatives of orders 0..5
+constexpr int kEwRecChunks = 7;    // floats 4..31 of an order-4 cell record (nln_hcell); the
+                                   // centre in floats 0..5 comes with the pipeline's registers
+struct EwStage {
+    float4 node[kEwNodeChunks][32];
+    float4 rec[kEwRecChunks][32];
+};
+constexpr int kEwWarpBytes = 2 * (int)sizeof(EwStage);  // two stages per warp: 21,504 B
+
+__global__ void __launch_bounds__(128) k_ewald_moments(DevProblem P) {
+    extern __shared__ __align__(16) unsigned char ewsm[];
+    const int lane = threadIdx.x & 31;
+    EwStage *stg = reinterpret_cast<EwStage *>(ewsm + (size_t)(threadIdx.x >> 5) * kEwWarpBytes);
+    const uint32_t ntab = (uint32_t)P.ntab[0];
+    const uint32_t nb = ntab - (uint32_t)P.ncells;
+    constexpr uint32_t kNone = 0xffffffffu;
+    // one source of the pipeline: list word (kNone: no entry in this lane)
+    // and its position (FP64) with, for a body, its mass
+    struct Src {
+        uint32_t e;
+        double x, y, z;
+        float m;
+    };
+    for (;;) {
+        int it = 0;
+        if (lane == 0)
+            it = atomicAdd(&P.counters[3], 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        const int64_t g = P.gbegin + it;
+        if (g >= P.ngroups)
+            break;
+        const nln_group G = P.groups[g];
+        const double c[3] = {G.cen[0], G.cen[1], G.cen[2]};
+        const int64_t cb = P.cptr[g], ce = P.cptr[g + 1];
+        const int ntile = (int)((ce - cb + 31) / 32);
+        // the list word is checked where it is used, a tile after its load
+        auto entry = [&](int t) -> uint32_t {
+            const int64_t k = cb + (int64_t)t * 32 + lane;
+            return (t < ntile && k < ce) ? __ldg(P.clist + k) : kNone;
+        };
+        auto source = [&](uint32_t e) -> Src {
+            Src r{kNone, 0.0, 0.0, 0.0, 0.f};
+            if (e == kNone)
+                return r;
+            const uint32_t idx = e & NLN_IDX_MASK;
+            if (idx >= ntab || (e >> NLN_IDX_BITS) > 26u) {  // as in k_batch
+                atomicOr(P.err, GC_DEV_BAD_INDEX);
+                return r;
+            }
+            r.e = e;
+            if (idx < nb) {
+                const float4 p = __ldg(P.points + idx);
+                r.x = p.x;
+                r.y = p.y;
+                r.z = p.z;
+                r.m = p.w;
+            } else {
+                const double *cen = P.hcells[idx - nb].cen;
+                r.x = __ldg(cen);
+                r.y = __ldg(cen + 1);
+                r.z = __ldg(cen + 2);
+            }
+            return r;
+        };
+        auto node_of = [&](const Src &q) -> EwNode {
+            double sx, sy, sz;
+            decode_shift(q.e >> NLN_IDX_BITS, P.box, sx, sy, sz);
+            return ew_node(P.ew, (float)(q.x + sx - c[0]), (float)(q.y + sy - c[1]),
+                           (float)(q.z + sz - c[2]));
+        };
+        auto issue = [&](const Src &q, EwStage &S) {
+            if (q.e == kNone)
+                return;
+            const uint32_t idx = q.e & NLN_IDX_MASK;
+            const float4 *node =
+                reinterpret_cast<const float4 *>(P.ew.t + (size_t)node_of(q).node * ew::kNode);
+#pragma unroll
+            for (int k = 0; k < kEwNodeChunks; k++) cp_async16(&S.node[k][lane], node + k);
+            if (idx >= nb) {
+                const float4 *rec = reinterpret_cast<const float4 *>(P.hcells + (idx - nb)) + 1;
+#pragma unroll
+                for (int k = 0; k < kEwRecChunks; k++) cp_async16(&S.rec[k][lane], rec + k);
+            }
+        };
+        EwMoments M;
+        M.zero();
+        Src s0 = source(entry(0));
+        issue(s0, stg[0]);
+        cp_async_commit();
+        Src s1 = source(entry(1));
+        uint32_t e2 = entry(2);
+        for (int t = 0; t < ntile; t++) {
+            if (t + 1 < ntile)
+                issue(s1, stg[(t + 1) & 1]);
+            cp_async_commit();
+            const Src s2 = source(e2);  // consumed by the next tile's issue
+            e2 = entry(t + 3);
+            cp_async_wait<1>();  // this lane's copies for tile t have landed
+            if (s0.e != kNone) {
+                const EwStage &S = stg[t & 1];
+                const EwNode N = node_of(s0);
+                // orders 0..4 (35 values) for the expansion; order 5 is read
+                // after it, so the two are never in registers together
+                float V[36];
+#pragma unroll
+                for (int k = 0; k < 9; k++) {
+                    const float4 v = S.node[k][lane];
+                    V[4 * k] = v.x;
+                    V[4 * k + 1] = v.y;
+                    V[4 * k + 2] = v.z;
+                    V[4 * k + 3] = v.w;
+                }
+                float o[ew::kNQ4], f5[21];
+                ew_expand<false>(V, N, o, nullptr);
+                if ((s0.e & NLN_IDX_MASK) < nb) {
+                    ew_add_mass(M, s0.m, o);
+                } else {
+                    float V5[24];  // node floats 32..55; order 5 starts at 35
+#pragma unroll
+                    for (int k = 8; k < kEwNodeChunks; k++) {
+                        const float4 v = S.node[k][lane];
+                        V5[4 * (k - 8)] = v.x;
+                        V5[4 * (k - 8) + 1] = v.y;
+                        V5[4 * (k - 8) + 2] = v.z;
+                        V5[4 * (k - 8) + 3] = v.w;
+                    }
+                    ew_fifth(V5 + 3, N, f5);
+                    float r[32];
+#pragma unroll
+                    for (int k = 0; k < kEwRecChunks; k++) {
+                        const float4 v = S.rec[k][lane];
+                        r[4 * (k + 1)] = v.x;
+                        r[4 * (k + 1) + 1] = v.y;
+                        r[4 * (k + 1) + 2] = v.z;
+                        r[4 * (k + 1) + 3] = v.w;
+                    }
+                    // nln_hcell floats: mass 6, R 7, q2 8..12, q3 13..19, q4 20..28, B2 29
+                    const float R = r[7];
+                    ew_add_mass(M, r[6], o);
+                    float Sm[15];
+                    ew_quad(R, r + 8, Sm);
+                    ew_fold<2, 3>(M, Sm, o, f5);
+                    ew_oct(R, r + 13, Sm);
+                    ew_fold<3, 2>(M, Sm, o, f5);
+                    ew_hex(R, r + 20, Sm);
+                    ew_fold<4, 1>(M, Sm, o, f5);
+                    M.add(0, r[29] * (1.f / 6.f) * P.ew_trace);
+                }
+            }
+            s0 = s1;
+            s1 = s2;
+        }
+        cp_async_wait<0>();
+        M.warp_sum();
+        if (lane == 0) {
+            EwStored &E = P.ewm[g];
+#pragma unroll
+            for (int q = 0; q < 10; q++) E.lo[q] = M.lo[q];
+#pragma unroll
+            for (int q = 0; q < 25; q++) E.hi[q] = M.hi[q];
+        }
+    }
+}
+
+// The same correction moments of group g by a plain loop over the list,
+// lanes striding it, every load on demand: no shared memory and fewer
+// registers than k_ewald_moments, which suits a kernel that shares the SMs
+// with the list kernels (the side stream).  The arithmetic and its order are
+// k_ewald_moments', so the two store identical moments.  Bodies count as masses; a cell adds its
 // traceless second to fourth moments (the list's cells include coarse
 // ones standing for whole subtrees, and cells a tenth of the box wide near
 // the half-box, where C varies on the scale of the cell), and its
 // second-moment trace B2/3 against the constant Laplacian of C.
-__device__ __forceinline__ void ewald_moments(const DevProblem &P, int64_t g, const double *c,
+__device__ __forceinline__ void ewald_moments_loop(const DevProblem &P, int64_t g, const double *c,
                                               int lane, EwMoments &M) {
     M.zero();
     float o[ew::kNQ4], f5[21];
@@ -760,9 +964,10 @@ __device__ __forceinline__ void ewald_moments(const DevProblem &P, int64_t g, co
     M.warp_sum();
 }
 
-// The correction moments of groups gbegin..ngroups-1, stored per group for
-// k_finish: one warp per group from a queue (counter 3), run on a side
-// stream beside the list kernels, which it does not depend on.
+// The correction moments of groups gbegin..ngroups-1 by ewald_moments_loop,
+// stored per group for k_finish: one warp per group from a queue (counter
+// 3), run on a side stream beside the list kernels, which it does not
+// depend on.
 __global__ void __launch_bounds__(64) k_ewald_side(DevProblem P) {
     const int lane = threadIdx.x & 31;
     for (;;) {
@@ -776,7 +981,7 @@ __global__ void __launch_bounds__(64) k_ewald_side(DevProblem P) {
         const nln_group G = P.groups[g];
         const double c[3] = {G.cen[0], G.cen[1], G.cen[2]};
         EwMoments M;
-        ewald_moments(P, g, c, lane, M);
+        ewald_moments_loop(P, g, c, lane, M);
         if (lane == 0) {
             EwStored &E = P.ewm[g];
 #pragma unroll
@@ -807,15 +1012,11 @@ __global__ void k_finish(DevProblem P) {
     if (P.ewald) {
         const double c[3] = {G.cen[0], G.cen[1], G.cen[2]};
         EwMoments M;
-        if (P.ewm) {
-            const EwStored &E = P.ewm[g];
+        const EwStored &E = P.ewm[g];  // k_ewald_moments
 #pragma unroll
-            for (int q = 0; q < 10; q++) M.lo[q] = E.lo[q];
+        for (int q = 0; q < 10; q++) M.lo[q] = E.lo[q];
 #pragma unroll
-            for (int q = 0; q < 25; q++) M.hi[q] = E.hi[q];
-        } else {
-            ewald_moments(P, g, c, lane, M);
-        }
+        for (int q = 0; q < 25; q++) M.hi[q] = E.hi[q];
         if (lane < G.count) {
             const float4 p = P.points[G.first + lane];
             double phi, ax, ay, az;
@@ -858,8 +1059,8 @@ struct grav_plan {
     float4 *qstage = nullptr, *hstage = nullptr;  // pre-staged cell tables (k_stage_cells)
     grav_step_state *step = nullptr;  // tree links, refit scratch and the step graph
     grav_adjoint_state *adj = nullptr;  // adjoint scratch
-    // periodic: the side stream of k_ewald_side, its fork/join events and
-    // the per-group moments it stores
+    // periodic: the side stream of k_ewald_moments, its fork/join events and
+    // the per-group correction moments
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
     EwStored *ewm = nullptr;
@@ -1471,6 +1672,8 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
         }
         pl->staged = true;
     }
+    d.cstage = pl->qstage ? pl->qstage : pl->hstage;
+    d.cstride = pl->qstage ? 4 : 8;
     rc |= encode_rows(&pl->tmap[KP], d.points, (uint64_t)np, 16);
     if (pl->qstage)
         rc |= encode_rows(&pl->tmap[KQ], pl->qstage, (uint64_t)hp->ncells, sizeof(nln_qcell));
@@ -1547,40 +1750,67 @@ int launch_kind(grav_plan *pl, const DevProblem &dp, cudaStream_t st) {
     return 0;
 }
 
-// Blocks per SM of k_ewald_side (0: the moments are computed in k_finish).
-// Automatic: 2 blocks (the best of 1-6 on the 128^3 and 256^3 boxes) when
-// the correction list is short beside the order-4 lists, else 0.  The side
-// kernel shares the SMs with the list kernels: it pays only while it ends
-// well within them.  Measured on one B200: correction entries at 1.2 % of
-// the order-4 interactions (256^3, MAC 1.5e-6) gain 1.2 %; where the
-// moments take half the order-4 kernel's time (128^3, MAC 1e-4) the side
-// stream loses 8 %.  The threshold below sits between.
-int side_blocks(const grav_plan *pl) {
-    if (!pl->dp.ewald || !pl->side || !pl->ewm || pl->tune.ewald_side < 0)
+// k_ewald_moments: `warps` warps per block, each with two 11 KiB stages,
+// blocks_per_sm x SM count blocks (0: as many as fit), at most one warp per
+// group; over dp's groups, on stream s.
+int launch_moments(grav_plan *pl, const DevProblem &dp, cudaStream_t s, int per_sm, int warps) {
+    const int64_t n = dp.ngroups - dp.gbegin;
+    if (n <= 0)
         return 0;
-    if (pl->tune.ewald_side > 0)
-        return pl->tune.ewald_side;
-    return pl->ewald_entries < 0.015 * (double)pl->counts[3] ? 2 : 0;
+    const size_t smem = (size_t)warps * kEwWarpBytes;
+    GC_CHECK(cudaFuncSetAttribute(k_ewald_moments, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  4 * kEwWarpBytes));
+    if (per_sm <= 0) {
+        int fit = 0;
+        GC_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_ewald_moments, warps * 32,
+                                                               smem));
+        per_sm = std::max(1, fit);
+    }
+    DevProblem d = dp;
+    d.ewm = pl->ewm;
+    const unsigned blocks = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>((n + warps - 1) / warps, (int64_t)per_sm * pl->nsm));
+    k_ewald_moments<<<blocks, warps * 32, smem, s>>>(d);
+    GC_CHECK(cudaGetLastError());
+    pl->launches++;
+    return 0;
 }
 
-// Fork: k_ewald_side over dp's groups on the side stream, after the work
+// Placement of the periodic correction moments: ewald_side > 0 runs them on
+// a side stream beside the list kernels (k_ewald_side) in that many two-warp
+// blocks per SM, sharing the SMs with them; ewald_side = -k runs them
+// on the evaluation's stream between the list kernels and the finish pass,
+// with the SMs to themselves, in blocks of k warps (k = 1, 2 or 4) as many
+// as fit.  Automatic (0): the evaluation's stream, two-warp blocks.
+int main_moments_warps(const grav_plan *pl) {
+    const int k = -pl->tune.ewald_side;
+    return (k == 1 || k == 2 || k == 4) ? k : 2;
+}
+
+int side_blocks(const grav_plan *pl) {
+    if (!pl->dp.ewald || !pl->side || !pl->ewm || pl->tune.ewald_side <= 0)
+        return 0;
+    return pl->tune.ewald_side;
+}
+
+// Fork: k_ewald_moments over dp's groups on the side stream, after the work
 // already on st; returns whether it forked (join with side_join).
 int side_fork(grav_plan *pl, const DevProblem &dp, cudaStream_t st, bool &forked) {
     forked = false;
     const int per_sm = side_blocks(pl);
-    const int64_t n = dp.ngroups - dp.gbegin;
-    if (per_sm <= 0 || n <= 0)
+    if (per_sm <= 0 || dp.ngroups - dp.gbegin <= 0)
         return 0;
     GC_CHECK(cudaEventRecord(pl->fork, st));
     GC_CHECK(cudaStreamWaitEvent(pl->side, pl->fork, 0));
     DevProblem d = dp;
     d.ewm = pl->ewm;
+    const int64_t n = dp.ngroups - dp.gbegin;
     const unsigned blocks =
         (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 1) / 2, (int64_t)per_sm * pl->nsm));
     k_ewald_side<<<blocks, 64, 0, pl->side>>>(d);
     GC_CHECK(cudaGetLastError());
-    GC_CHECK(cudaEventRecord(pl->join, pl->side));
     pl->launches++;
+    GC_CHECK(cudaEventRecord(pl->join, pl->side));
     forked = true;
     return 0;
 }
@@ -1590,9 +1820,12 @@ int side_join(grav_plan *pl, cudaStream_t st) {
     return 0;
 }
 
-// Two warps per block: at ~160 registers a thread, small blocks let more
-// warps stay resident, which this latency-bound kernel needs.
-int launch_finish(grav_plan *pl, const DevProblem &dp, cudaStream_t st) {
+// The finish pass, after the correction moments when they did not run on
+// the side stream (forked).
+int launch_finish(grav_plan *pl, const DevProblem &dp, cudaStream_t st, bool forked) {
+    if (dp.ewald && !forked)
+        if (int rc = launch_moments(pl, dp, st, 0, main_moments_warps(pl)))
+            return rc;
     const int wpb = 2;
     const int64_t n = dp.ngroups - dp.gbegin;
     if (n <= 0)
@@ -1633,12 +1866,11 @@ extern "C" int grav_groups_eval_CUDA(grav_plan *pl, void *stream) {
     if (int rc = mark(3))
         return rc;
     DevProblem df = pl->dp;
-    if (forked) {
+    df.ewm = pl->ewm;
+    if (forked)
         if (int rc = side_join(pl, st))
             return rc;
-        df.ewm = pl->ewm;
-    }
-    if (int rc = launch_finish(pl, df, st))
+    if (int rc = launch_finish(pl, df, st, forked))
         return rc;
     return mark(4);
 }
@@ -1850,12 +2082,11 @@ int eval_range(grav_plan *pl, size_t c, cudaStream_t st) {
         rc = launch_kind<KQ>(pl, dp, st);
     if (!rc)
         rc = launch_kind<KP>(pl, dp, st);
-    if (!rc && forked) {
+    dp.ewm = pl->ewm;
+    if (!rc && forked)
         rc = side_join(pl, st);
-        dp.ewm = pl->ewm;
-    }
     if (!rc)
-        rc = launch_finish(pl, dp, st);
+        rc = launch_finish(pl, dp, st, forked);
     return rc;
 }
 }  // namespace

@@ -108,6 +108,22 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return false;
 }
 
+// Per-thread asynchronous 16-byte copy global -> shared (cp.async, cached in
+// L2 only), grouped by commit_group and completed by wait_group.  Not the
+// bulk (TMA) path: each thread copies the bytes it will read itself.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+// Wait until at most N of this thread's committed groups are still in flight.
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Single MUFU reciprocal square root (approximate, flush-to-zero); the
 // reference uses an 11-bit rsqrtps refined by one Newton step
 // (nln/do_grav_avx8.c:2188-2201), which this matches in accuracy.

@@ -63,31 +63,56 @@ __device__ __forceinline__ void ew_monomials(float dx, float dy, float dz, float
                     mono[ew::idx(bx, by, bz)] = px[bx] * py[by] * pz[bz];
 }
 
-// C and its derivatives of orders 0..4 at y (35 floats, multi-index layout);
-// with WANT5 also the fifth derivatives at the nearest node (21 floats, f5).
-template <bool WANT5>
-__device__ __forceinline__ void ew_lookup(const EwTab &E, float yx, float yy, float yz, float *o,
-                                          float *f5) {
-    const float sx = yx < 0.f ? -1.f : 1.f, sy = yy < 0.f ? -1.f : 1.f, sz = yz < 0.f ? -1.f : 1.f;
+// The table node nearest |y| (the positive octant; C is even in each axis),
+// the offsets of |y| from it and the octant signs of y.
+struct EwNode {
+    int node;              // node number: (i n + j) n + k
+    float dx, dy, dz;      // |y| - node position
+    float sx, sy, sz;      // signs of y's components
+};
+
+__device__ __forceinline__ EwNode ew_node(const EwTab &E, float yx, float yy, float yz) {
+    EwNode r;
+    r.sx = yx < 0.f ? -1.f : 1.f;
+    r.sy = yy < 0.f ? -1.f : 1.f;
+    r.sz = yz < 0.f ? -1.f : 1.f;
     const float ax = fabsf(yx), ay = fabsf(yy), az = fabsf(yz);
     const int nm = E.n - 1;
     const int i = min(__float2int_rn(ax * E.inv_h), nm);
     const int j = min(__float2int_rn(ay * E.inv_h), nm);
     const int k = min(__float2int_rn(az * E.inv_h), nm);
-    const float dx = ax - i * E.h, dy = ay - j * E.h, dz = az - k * E.h;
-    const float4 *p =
-        reinterpret_cast<const float4 *>(E.t + (((size_t)i * E.n + j) * E.n + k) * ew::kNode);
-    float V[WANT5 ? 56 : 36];
+    r.dx = ax - i * E.h;
+    r.dy = ay - j * E.h;
+    r.dz = az - k * E.h;
+    r.node = (i * E.n + j) * E.n + k;
+    return r;
+}
+
+// The fifth derivatives at the node (21 floats, f5), octant signs applied,
+// from the node's order-5 values V5 = V[35..55].
+__device__ __forceinline__ void ew_fifth(const float *V5, const EwNode &N, float *f5) {
 #pragma unroll
-    for (int q = 0; q < (WANT5 ? 14 : 9); q++) {
-        const float4 v = __ldg(p + q);
-        V[4 * q] = v.x;
-        V[4 * q + 1] = v.y;
-        V[4 * q + 2] = v.z;
-        V[4 * q + 3] = v.w;
-    }
+    for (int a0 = 0; a0 <= 5; a0++)
+#pragma unroll
+        for (int a1 = 0; a1 <= 5; a1++) {
+            if (a0 + a1 > 5)
+                continue;
+            const int a2 = 5 - a0 - a1;
+            const float sg = ((a0 & 1) ? N.sx : 1.f) * ((a1 & 1) ? N.sy : 1.f) *
+                             ((a2 & 1) ? N.sz : 1.f);
+            const int q = ew::idx(a0, a1, a2) - ew::base(5);
+            f5[q] = sg * V5[q];
+        }
+}
+
+// C and its derivatives of orders 0..4 at the point (35 floats, multi-index
+// layout) from the node's values V (orders 0..4 in V[0..34], and 5 in
+// V[35..55] when WANT5); with WANT5 also the fifth derivatives at the node
+// (21 floats, f5).
+template <bool WANT5>
+__device__ __forceinline__ void ew_expand(const float *V, const EwNode &N, float *o, float *f5) {
     float mono[35];
-    ew_monomials(dx, dy, dz, mono);
+    ew_monomials(N.dx, N.dy, N.dz, mono);
     // o[alpha] = sum_{|beta| <= 4 - |alpha|} V[alpha + beta] d^beta / beta!, then the octant
     // sign.  Every loop has constant bounds (guards fold after unrolling), so
     // the arrays stay in registers.
@@ -109,21 +134,32 @@ __device__ __forceinline__ void ew_lookup(const EwTab &E, float yx, float yy, fl
                             if (a0 + a1 + a2 + b0 + b1 + b2 <= 4)
                                 acc = fmaf(V[ew::idx(a0 + b0, a1 + b1, a2 + b2)],
                                            mono[ew::idx(b0, b1, b2)], acc);
-                const float sg = ((a0 & 1) ? sx : 1.f) * ((a1 & 1) ? sy : 1.f) * ((a2 & 1) ? sz : 1.f);
+                const float sg = ((a0 & 1) ? N.sx : 1.f) * ((a1 & 1) ? N.sy : 1.f) *
+                                 ((a2 & 1) ? N.sz : 1.f);
                 o[ew::idx(a0, a1, a2)] = sg * acc;
             }
-    if (WANT5) {
+    if (WANT5)
+        ew_fifth(V + ew::base(5), N, f5);
+}
+
+// C and its derivatives at y by a fourth-order Taylor expansion about the
+// nearest node of the table (ew_node + ew_expand on the node read from global
+// memory).
+template <bool WANT5>
+__device__ __forceinline__ void ew_lookup(const EwTab &E, float yx, float yy, float yz, float *o,
+                                          float *f5) {
+    const EwNode N = ew_node(E, yx, yy, yz);
+    const float4 *p = reinterpret_cast<const float4 *>(E.t + (size_t)N.node * ew::kNode);
+    float V[WANT5 ? 56 : 36];
 #pragma unroll
-        for (int a0 = 0; a0 <= 5; a0++)
-#pragma unroll
-            for (int a1 = 0; a1 <= 5; a1++) {
-                if (a0 + a1 > 5)
-                    continue;
-                const int a2 = 5 - a0 - a1;
-                const float sg = ((a0 & 1) ? sx : 1.f) * ((a1 & 1) ? sy : 1.f) * ((a2 & 1) ? sz : 1.f);
-                f5[ew::idx(a0, a1, a2) - ew::base(5)] = sg * V[ew::idx(a0, a1, a2)];
-            }
+    for (int q = 0; q < (WANT5 ? 14 : 9); q++) {
+        const float4 v = __ldg(p + q);
+        V[4 * q] = v.x;
+        V[4 * q + 1] = v.y;
+        V[4 * q + 2] = v.z;
+        V[4 * q + 3] = v.w;
     }
+    ew_expand<WANT5>(V, N, o, f5);
 }
 
 // Group correction moments: orders 0..2 in FP64 (the net field is a small

@@ -8,12 +8,32 @@ Gaussian random field with P(k) ~ k^-2.5 (rms 0.5 grid spacing), Plummer
 softening 1/50 of the spacing, order-4 moments plus the Ewald correction,
 force error measured against an FP64 Ewald-summed direct sum on 8192 sinks.
 
+After the timed region the same run measures, untimed, one block per
+configuration of the benchmark set (--configs; all by default):
+  plummer64k  Plummer N = 65,536, order 2: batched and drop-in GPU results
+              against the reference's own AVX kernels on the full lists, and
+              against the FP64 direct sum on every sink
+  box128      periodic 128^3, order 4 + Ewald: mixed-precision against plain
+              FP32 kernels, accuracy on 4096 sinks and time
+  batch1024   1024 isolated systems of uneven N in one launch per list kind,
+              autotuned tile shapes, graph-captured KDK step
+  adjoint     Plummer N = 2^20: adjoint/forward time, FP64 central
+              differences at 64 coordinates and 16 masses, the FP64
+              direct-sum gradient on an N = 8192 system, and 16 leapfrog KDK
+              steps checkpointed every 4, checked against FP64 differences
+  kdk256      32 graph-captured KDK steps of the 256^3 box with energy drift
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload box256|box128|plummer64k]
+                    [--workload box256|box128|plummer64k|batch1024] [--configs all|none|a,b]
 
 Under torchrun (N > 1) every rank evaluates its own replica of the workload
 (the force evaluation does not shard across GPUs here): value is the sum of
-interactions over ranks divided by the slowest rank's time.
+interactions over ranks divided by the slowest rank's time.  The
+configuration blocks run on rank 0 only.
+
+The CPU legs (cpu_baseline, and the per-configuration checks against the
+reference's own kernels and the FP64 checkers) call oracle/, the parity
+checker; nothing measured on the GPU goes through it.
 """
 import argparse
 import json
@@ -36,27 +56,60 @@ UNIT = "interactions/s"
 # (reference count 26-27, nln/grav.c:56-75), 66 quadrupole
 # (nln/do_grav_avx8.c:378), 217 order 4 (nln/do_grav_avx8.c:45)
 FLOPS = np.array([23, 23, 66, 217], np.float64)
-# DRAM bytes (read + write) per interaction of each list kernel, from the ncu
-# capture of the 128^3 case (profiles/k_batch_box128_full.md); a launch's
+# DRAM bytes (read + write) per interaction of each list kernel, from one ncu
+# capture of the kernels on the periodic 128^3 box (MAC 1e-4); a launch's
 # traffic is this times its interactions (traffic grows with list entries)
 DRAM_BYTES_PER_INTERACTION = {"hexa": 0.2007, "quad": 0.193, "point": 0.164}
+ALL_CONFIGS = ("plummer64k", "box128", "batch1024", "adjoint", "kdk256")
 
 WORKLOADS = {
-    # configs[4]: N = 2^24 periodic box, order 4 + Ewald (the metric's N)
+    # N = 2^24 periodic box, order 4 + Ewald (the metric's N)
     # (MAC tolerance chosen for <= 1e-4 rms relative force error)
     "box256": dict(kind="box", n1d=256, rms_disp=0.5, p2cut=7, p4cut=20, ewald=True,
                    tol=1.5e-6, sample=8192),
-    # configs[1]: 128^3 periodic box, order 4 + Ewald
+    # 128^3 periodic box, order 4 + Ewald
     "box128": dict(kind="box", n1d=128, rms_disp=0.25, p2cut=7, p4cut=20, ewald=True,
                    tol=2.5e-6, sample=4096),
-    # configs[0]: Plummer sphere N = 65536, order 2
+    # Plummer sphere N = 65536, order 2
     "plummer64k": dict(kind="plummer", n=65536, eps=0.01, p2cut=7, p4cut=0, ewald=False,
                        tol=2e-5, sample=8192),
-    # configs[2]: 1024 independent isolated systems, N log-uniform in [512, 65536],
+    # 1024 independent isolated systems, N log-uniform in [512, 65536],
     # half Plummer half Hernquist (a = 1), eps = 0.01 a, order 4, one launch per kind
     "batch1024": dict(kind="batch", nsys=1024, nmin=512, nmax=65536, eps=0.01, p2cut=7,
                       p4cut=20, ewald=False, tol=1e-5, sample=2048),
 }
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def rel_rms(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    e = np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)
+    return float(np.sqrt(np.mean(e * e))), float(e.max())
+
+
+def time_evals(plan, stream, reps):
+    """Mean device milliseconds of `reps` evaluations (CUDA events on the stream)."""
+    import torch
+    plan.eval(stream.cuda_stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(reps):
+        plan.eval(stream.cuda_stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
 
 
 def log(*a):
@@ -241,9 +294,9 @@ def dropin_rate(tree, eps2, max_groups=2048, seed=1, max_bytes=1 << 30):
 
 
 def kdk_run(w, pos, m, eps2, box, tol, nsteps, dt, rebuild):
-    """configs[4]'s time-stepping leg: nsteps KDK steps (Integrate of
-    nln/integrate.c) from rest, graph-captured device steps between host
-    rebuilds; energies per step."""
+    """The large periodic box's time-stepping leg: nsteps KDK steps
+    (Integrate of nln/integrate.c) from rest, graph-captured device steps
+    between host rebuilds; energies per step."""
     from pgrav import step as S
     st = S.Stepper(pos, np.zeros_like(pos), m, eps2, box=box, ewald=w["ewald"] and box > 0,
                    rebuild=rebuild, graph=True,
@@ -266,41 +319,357 @@ def kdk_run(w, pos, m, eps2, box, tol, nsteps, dt, rebuild):
             "ke_last": float(h[-1]["ke"]), "pe_first": float(pe[0]), "pe_last": float(pe[-1])}
 
 
-def adjoint_timing(reps=5):
-    """configs[3]'s cost ratio: Plummer N = 2^20 (order 2), forward
-    evaluation against grav_plan_adjoint_CUDA on the same lists, CUDA events."""
+# ---------------------------------------------------------------- configuration legs
+def config_plummer64k(args, stream):
+    """Plummer N = 65,536, G = 1, M = 1, a = 1, eps = 0.01, order 2 (p4cut 0),
+    MAC tol 2e-5.  GPU: the batched kernels and the drop-in (grav_mn_CUDA
+    per group, pMp/pQp) on the host walk's lists.  CPU leg: the reference's
+    own do_gravp_avx8/do_gravpq_avx8 over the same full lists (the parity
+    check, bar 1e-5 relative rms), and the FP64 direct sum on every sink."""
     import torch
+    from oracle import oracle as O
     from pgrav import gravcuda as gc, host, ics
-    n = 1 << 20
+    w = WORKLOADS["plummer64k"]
+    pos, m = ics.plummer(w["n"], seed=123)
+    eps2 = w["eps"] ** 2
+    t = host.Tree(pos, m, leaf_max=16, group_max=32, p2cut=w["p2cut"], p4cut=0, tol=w["tol"],
+                  emit_aosoa=True)
+    res = {"workload": "Plummer N=65536, eps 0.01, order 2, MAC tol 2e-5", "n_bodies": int(t.n),
+           "groups": int(t.ngroups),
+           "interactions_per_sink": [round(float(x) / t.n, 1) for x in t.counts]}
+    inter = float(t.counts.sum())
+    # the reference quadrupole kernels' potential sign (-1) for the parity check
+    plan_r = gc.Plan(t, eps2, quad_phi_sign=-1.0)
+    ms = time_evals(plan_r, stream, 20)
+    got_r = plan_r.download()
+    plan_r.free()
+    plan = gc.Plan(t, eps2)
+    plan.eval()
+    got = plan.download()
+    plan.free()
+    res["batched"] = {"ms": ms, "value": inter / (ms * 1e-3), "unit": UNIT}
+    # drop-in: one grav_mn_CUDA per group and kind, as nln/mac.c issues them
+    bt = gc.body_table(t.sorted_pos, t.points[:t.n, 3])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    d = gc.DropIn(bt)
+    for k, (routine, sz) in enumerate((("pMp", 4), ("pQp", 13))):
+        ptr, data = t.aosoa[k]
+        for g in range(t.ngroups):
+            b0, b1 = int(ptr[g]), int(ptr[g + 1])
+            if b1 > b0:
+                d.mn(routine, int(t.groups["first"][g]), int(t.groups["count"][g]),
+                     data[b0 * sz * 8:b1 * sz * 8], (b1 - b0) * 8, sz, eps2)
+    got_d = d.terminate()
+    el = time.perf_counter() - t0
+    res["dropin"] = {"s": el, "value": inter / el, "unit": UNIT,
+                     "timing": "wall clock, WalkInitSinkCUDA .. WalkTerminateSinkCUDA from Python"}
+    # CPU leg: the reference's own kernels over the full lists, all host threads
+    if O.ref_available():
+        t0 = time.perf_counter()
+        ref = O.tree_eval(t, eps2, quad_kind=O.QUAD_PLUMMER, reference=True)
+        el = time.perf_counter() - t0
+        b_rms, b_max = rel_rms(got_r[:, :3], ref[:, :3])
+        d_rms, d_max = rel_rms(got_d[:, :3], ref[:, :3])
+        pb = float(np.sqrt(np.mean((got_r[:, 3] - ref[:, 3]) ** 2) / np.mean(ref[:, 3] ** 2)))
+        pd = float(np.sqrt(np.mean((got_d[:, 3] - ref[:, 3]) ** 2) / np.mean(ref[:, 3] ** 2)))
+        res["vs_reference_kernels"] = {
+            "kernels": "do_gravp_avx8 + do_gravpq_avx8 (nln/do_grav_avx8.c, compiled unmodified)",
+            "cpu_s": el, "cpu_value": inter / el, "cores": os.cpu_count(), "cpu_model": cpu_model(),
+            "batched_rms_rel_acc": b_rms, "batched_max_rel_acc": b_max, "batched_rms_phi": pb,
+            "dropin_rms_rel_acc": d_rms, "dropin_max_rel_acc": d_max, "dropin_rms_phi": pd,
+            "bar_rms": 1e-5, "meets_target": bool(b_rms <= 1e-5 and d_rms <= 1e-5 and
+                                                  pb <= 1e-5 and pd <= 1e-5)}
+    ref64 = gc.direct_fp64(t.points[:t.n], np.arange(t.n), eps2)
+    a_rms, a_max = rel_rms(got[:, :3], ref64[:, :3])
+    res["vs_fp64_direct"] = {"sinks": int(t.n), "rms_rel_force_err": a_rms,
+                             "max_rel_force_err": a_max,
+                             "rms_phi_err": float(np.sqrt(np.mean((got[:, 3] - ref64[:, 3]) ** 2) /
+                                                          np.mean(ref64[:, 3] ** 2)))}
+    return res
+
+
+def config_box128(args, stream):
+    """Periodic 128^3 box (GRF, P(k) ~ k^-2.5, rms displacement 0.25
+    spacing), eps = spacing/50, order 4 + Ewald (FP64-built table): the
+    mixed-precision kernels (FP32 offsets from FP64 group centres,
+    compensated sums) against the plain FP32 kernels (absolute FP32
+    coordinates, plain sums) on the same lists; errors against the FP64
+    Ewald-summed direct sum on 4096 random sinks."""
+    from pgrav import gravcuda as gc, host, ics
+    w = WORKLOADS["box128"]
+    pos, m = ics.grf_box(w["n1d"], seed=123, slope=-2.5, rms_disp=w["rms_disp"])
+    eps2 = (1.0 / w["n1d"] / 50.0) ** 2
+    t = host.Tree(pos, m, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=w["tol"], box=1.0)
+    inter = float(t.counts.sum())
+    samp = np.sort(np.random.default_rng(7).choice(t.n, 4096, replace=False))
+    ref = gc.direct_fp64(t.points[:t.n], samp, eps2, box=1.0)
+    res = {"workload": f"periodic 128^3, order 4 + Ewald, MAC tol {w['tol']}",
+           "n_bodies": int(t.n), "groups": int(t.ngroups),
+           "interactions_per_sink": [round(float(x) / t.n, 1) for x in t.counts], "sinks": 4096}
+    for name, plain in (("mixed", False), ("plain_fp32", True)):
+        plan = gc.Plan(t, eps2, ewald=True, plain=plain)
+        ms = time_evals(plan, stream, 10)
+        out = plan.download()
+        plan.free()
+        e_rms, e_max = rel_rms(out[samp, :3], ref[:, :3])
+        pe = float(np.sqrt(np.mean((out[samp, 3] - ref[:, 3]) ** 2) / np.mean(ref[:, 3] ** 2)))
+        res[name] = {"ms": ms, "value": inter / (ms * 1e-3), "unit": UNIT,
+                     "rms_rel_force_err": e_rms, "max_rel_force_err": e_max, "rms_phi_err": pe,
+                     "meets_target": bool(e_rms <= 1e-4)}
+    res["plain_over_mixed_time"] = res["plain_fp32"]["ms"] / res["mixed"]["ms"]
+    res["plain_over_mixed_rms_err"] = (res["plain_fp32"]["rms_rel_force_err"] /
+                                       res["mixed"]["rms_rel_force_err"])
+    return res
+
+
+def config_batch1024(args, stream):
+    """1024 isolated systems, N log-uniform in [512, 65536], half Plummer half
+    Hernquist (a = 1), eps = 0.01 a, order 4, FP32: one persistent launch per
+    list kind from one length-sorted queue, tile shapes from the autotuner,
+    and the graph-captured KDK step (evaluate, integrate, refit)."""
+    import torch
+    from pgrav import autotune as AT, gravcuda as gc
+    w = WORKLOADS["batch1024"]
+    t0 = time.perf_counter()
+    systems, _, eps2, _ = make_problem(w)
+    tree = build_tree(w, systems, None, 0.0, w["tol"])
+    setup = time.perf_counter() - t0
+    plan = gc.Plan(tree, eps2)
+    ta = time.perf_counter()
+    best, trials = AT.autotune(plan)
+    search = time.perf_counter() - ta
+    ms = time_evals(plan, stream, 10)
+    inter = float(plan.counts().sum())
+    out = plan.download()
+    rng = np.random.default_rng(7)
+    offs = tree.body_offsets
+    pick = rng.choice(len(offs) - 1, 8, replace=False)
+    got, refs = [], []
+    for sidx in pick:
+        lo, hi = int(offs[sidx]), int(offs[sidx + 1])
+        ss = np.sort(rng.choice(hi - lo, min(hi - lo, w["sample"] // 8), replace=False))
+        refs.append(gc.direct_fp64(tree.points[lo:hi], ss, eps2))
+        got.append(out[lo + ss])
+    e_rms, e_max = rel_rms(np.concatenate(got)[:, :3], np.concatenate(refs)[:, :3])
+    plan.set_tree(tree)
+    vel = torch.zeros((tree.n, 4), dtype=torch.float32, device="cuda")
+    prm = torch.tensor([1e-3, 5e-4, 0.0], dtype=torch.float64, device="cuda")
+    en = torch.zeros(2, dtype=torch.float64, device="cuda")
+    with torch.cuda.stream(stream):
+        plan.step(vel.data_ptr(), prm.data_ptr(), en.data_ptr(), stream.cuda_stream, graph=True)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(10):
+            plan.step(vel.data_ptr(), prm.data_ptr(), en.data_ptr(), stream.cuda_stream,
+                      graph=True)
+        b.record(stream)
+    torch.cuda.synchronize()
+    res = {"workload": "1024 isolated systems, N log-uniform in [512, 65536], Plummer/Hernquist, "
+                       "order 4, MAC tol 1e-5",
+           "systems": int(len(offs) - 1), "n_bodies": int(tree.n), "groups": int(tree.ngroups),
+           "host_build_s": setup, "ms": ms, "value": inter / (ms * 1e-3), "unit": UNIT,
+           "launches_per_eval": plan.launches(),
+           "tuning": {"chosen": {"warps_per_block": best.warps_per_block,
+                                 "blocks_per_sm": best.blocks_per_sm,
+                                 "chunks": [best.chunk_p, best.chunk_q, best.chunk_h]},
+                      "trials": len(trials), "search_s": search,
+                      "auto_ms": trials[0]["ms"], "best_ms": min(x["ms"] for x in trials)},
+           "graph_kdk_step_ms": a.elapsed_time(b) / 10,
+           "rms_rel_force_err": e_rms, "max_rel_force_err": e_max,
+           "accuracy_sinks": int(sum(len(r) for r in refs)),
+           "oracle": "each system's own FP64 direct sum (8 random systems)",
+           "meets_target": bool(e_rms <= 1e-4)}
+    plan.free()
+    return res
+
+
+def _fp64_leapfrog_loss(x0, v0, m, eps2, dt, nsteps, trees, checkers, target):
+    """L = sum (x_final + v_final) . target of FP64 KDK steps (kick dt/2,
+    drift dt, kick dt/2, two force evaluations per step as the autograd
+    leapfrog takes them) on the lists of `trees` (one per force evaluation),
+    every cell's moments recomputed in FP64 from the current bodies."""
+    x, v = x0.copy(), v0.copy()
+    k = 0
+
+    def acc(xx):
+        nonlocal k
+        t, chk = trees[k], checkers[k]
+        k += 1
+        o = chk.eval(xx[t.order], m[t.order], eps2)
+        a = np.empty_like(xx)
+        a[t.order] = o[:, :3]
+        return a
+
+    for _ in range(nsteps):
+        v = v + 0.5 * dt * acc(x)
+        x = x + dt * v
+        v = v + 0.5 * dt * acc(x)
+    return float((x * target).sum() + (v * target).sum())
+
+
+def config_adjoint(args, stream):
+    """Plummer N = 2^20, order 2, eps 0.01, MAC tol 1e-5; L = sum_i w_i.a_i +
+    u_i phi_i with w, u ~ N(0, 1) (seed 0).  GPU: forward and adjoint times
+    (CUDA events, same lists).  CPU checks: FP64 central differences (h =
+    1e-6) of an FP64 evaluation of the same lists at 64 position
+    coordinates and 16 masses (only the terms that depend on the perturbed
+    body are re-evaluated; the rest cancel), the FP64 direct-sum gradient on
+    a separate N = 8192 Plummer system, and 16 leapfrog KDK steps (dt = 1e-3)
+    checkpointed every 4 against the unsegmented backward and against FP64
+    differences through the same steps."""
+    import torch
+    from oracle import oracle as O
+    from pgrav import autograd as AG, gravcuda as gc, host, ics
+    n, eps2, tol = 1 << 20, 1e-4, 1e-5
     pos, m = ics.plummer(n, seed=123)
-    tol = 1e-5
     t = host.Tree(pos, m, leaf_max=16, group_max=32, p2cut=7, p4cut=0, tol=tol)
-    plan = gc.Plan(t, 0.01 ** 2)
+    plan = gc.Plan(t, eps2)
     plan.set_tree(t)
     rng = np.random.default_rng(0)
-    wu = torch.from_numpy(rng.normal(size=(n, 4)).astype(np.float32)).cuda()
+    wu_h = rng.normal(size=(n, 4)).astype(np.float32)
+    wu = torch.from_numpy(wu_h).cuda()
     grad = torch.empty((n, 4), dtype=torch.float32, device="cuda")
-    st = torch.cuda.Stream()
     for _ in range(3):
-        plan.eval(st.cuda_stream)
-        plan.adjoint(wu.data_ptr(), grad.data_ptr(), st.cuda_stream)
-    res = {}
-    for name, fn in (("forward", lambda: plan.eval(st.cuda_stream)),
-                     ("adjoint", lambda: plan.adjoint(wu.data_ptr(), grad.data_ptr(), st.cuda_stream))):
+        plan.eval(stream.cuda_stream)
+        plan.adjoint(wu.data_ptr(), grad.data_ptr(), stream.cuda_stream)
+    tm = {}
+    for name, fn in (("forward", lambda: plan.eval(stream.cuda_stream)),
+                     ("adjoint", lambda: plan.adjoint(wu.data_ptr(), grad.data_ptr(),
+                                                      stream.cuda_stream))):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
-        a.record(st)
-        for _ in range(reps):
+        a.record(stream)
+        for _ in range(5):
             fn()
-        b.record(st)
+        b.record(stream)
         torch.cuda.synchronize()
-        res[name] = a.elapsed_time(b) / reps
-    c = plan.counts()
+        tm[name] = a.elapsed_time(b) / 5
+    plan.eval(stream.cuda_stream)
+    plan.adjoint(wu.data_ptr(), grad.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    g = grad.cpu().numpy().astype(np.float64)
+    counts = plan.counts()
     plan.free()
-    return {"workload": "Plummer N=2^20, order 2, eps 0.01, tol 1e-5", "n_bodies": n,
-            "interactions_per_sink": [round(float(x) / n, 1) for x in c],
-            "forward_ms": res["forward"], "adjoint_ms": res["adjoint"],
-            "adjoint_over_forward": res["adjoint"] / res["forward"]}
+    res = {"workload": "Plummer N=2^20, order 2, eps 0.01, MAC tol 1e-5", "n_bodies": n,
+           "interactions_per_sink": [round(float(x) / n, 1) for x in counts],
+           "forward_ms": tm["forward"], "adjoint_ms": tm["adjoint"],
+           "adjoint_over_forward": tm["adjoint"] / tm["forward"], "target_ratio": 2.5,
+           "meets_target": bool(tm["adjoint"] / tm["forward"] <= 2.5)}
+    # FP64 central differences at 64 coordinates and 16 masses
+    t0 = time.perf_counter()
+    chk = O.ListsFP64(t)
+    sel = rng.choice(n, 64, replace=False)
+    chk.select(sel)
+    x = t.sorted_pos.astype(np.float64)
+    mm = t.points[:n, 3].astype(np.float64)
+    wv, uv = wu_h[:, :3].astype(np.float64), wu_h[:, 3].astype(np.float64)
+    coords = [(s, int(rng.integers(3))) for s in range(64)]
+    fdx = chk.fd_grad(x, mm, wv, uv, eps2, coords, h=1e-6)
+    fdm = chk.fd_grad(x, mm, wv, uv, eps2, [(s, 3) for s in range(16)], h=1e-6, mass_rel=True)
+    adx = np.array([g[sel[s], c] for s, c in coords])
+    adm = g[sel[:16], 3]
+    sx, sm = float(np.sqrt(np.mean(g[:, :3] ** 2))), float(np.sqrt(np.mean(g[:, 3] ** 2)))
+    ex, em = float(np.abs(adx - fdx).max() / sx), float(np.abs(adm - fdm).max() / sm)
+    res["fd"] = {"h": 1e-6, "coordinates": 64, "masses": 16, "cpu_s": time.perf_counter() - t0,
+                 "max_err_over_grad_rms_x": ex, "max_err_over_grad_rms_m": em,
+                 "rms_rel_err_x": float(np.sqrt(np.mean((adx - fdx) ** 2) / np.mean(fdx ** 2))),
+                 "bar": 1e-3, "meets_target": bool(ex <= 1e-3 and em <= 1e-3),
+                 "oracle": "FP64 evaluation of the same lists, cell moments from the bodies"}
+    del chk, t
+    # FP64 direct-sum gradient on an N = 8192 Plummer system
+    n2 = 8192
+    p2, m2 = ics.plummer(n2, seed=32)
+    w2 = rng.normal(size=(n2, 3)).astype(np.float32)
+    u2 = rng.normal(size=n2).astype(np.float32)
+    pt = torch.tensor(p2, device="cuda", requires_grad=True)
+    mt = torch.tensor(m2, device="cuda", requires_grad=True)
+    a2, f2 = AG.gravity(pt, mt, eps2, tol=1e-6, p2cut=7, p4cut=0)
+    ((torch.tensor(w2, device="cuda") * a2).sum() +
+     (torch.tensor(u2, device="cuda") * f2).sum()).backward()
+    gx, gm = O.direct_grad(p2, m2, w2, u2, eps2)
+    exd = np.linalg.norm(pt.grad.cpu().numpy() - gx, axis=1) / np.sqrt(np.mean((gx ** 2).sum(1)))
+    emd = np.abs(mt.grad.cpu().numpy() - gm) / np.sqrt(np.mean(gm ** 2))
+    res["vs_direct_gradient"] = {"n_bodies": n2, "mac_tol": 1e-6,
+                                 "rms_rel_err_x": float(np.sqrt(np.mean(exd ** 2))),
+                                 "rms_rel_err_m": float(np.sqrt(np.mean(emd ** 2))),
+                                 "bar": 1e-3,
+                                 "meets_target": bool(np.sqrt(np.mean(exd ** 2)) <= 1e-3 and
+                                                      np.sqrt(np.mean(emd ** 2)) <= 1e-3)}
+    res["leapfrog"] = leapfrog_check(args)
+    return res
+
+
+def leapfrog_check(args, n=4096, nsteps=16, every=4, dt=1e-3, ncoords=4):
+    """16 KDK steps through the autograd leapfrog, checkpointed every 4,
+    against the unsegmented backward and against FP64 central differences
+    through the same steps on the same lists (one tree per force
+    evaluation, built from the base trajectory)."""
+    import torch
+    from oracle import oracle as O
+    from pgrav import autograd as AG, host, ics
+    eps2, kw = 1e-4, dict(tol=1e-4, p2cut=7, p4cut=0, leaf_max=16, group_max=32)
+    pos, m = ics.plummer(n, seed=33)
+    rng = np.random.default_rng(9)
+    vel = rng.normal(0, 0.2, (n, 3)).astype(np.float32)
+    target = rng.normal(size=(n, 3))
+    tgt = torch.tensor(target, dtype=torch.float32, device="cuda")
+    grads, walls = [], []
+    for ck in (every, 0):
+        x0 = torch.tensor(pos, device="cuda", requires_grad=True)
+        v0 = torch.tensor(vel, device="cuda", requires_grad=True)
+        mm = torch.tensor(m, device="cuda", requires_grad=True)
+        t0 = time.perf_counter()
+        x, v = AG.leapfrog(x0, v0, mm, eps2, dt, nsteps, checkpoint_every=ck, **kw)
+        ((x * tgt).sum() + (v * tgt).sum()).backward()
+        torch.cuda.synchronize()
+        walls.append(time.perf_counter() - t0)
+        grads.append(x0.grad.cpu().numpy().astype(np.float64))
+    same = float(np.abs(grads[0] - grads[1]).max() / np.abs(grads[1]).max())
+    # FP64 differences: the base trajectory's trees, then +-h trajectories on them
+    x, v = pos.astype(np.float64), vel.astype(np.float64)
+    m64 = m.astype(np.float64)
+    trees, checkers = [], []
+
+    def acc(xx):
+        t = host.Tree(xx.astype(np.float32), m, **kw)
+        c = O.ListsFP64(t)
+        trees.append(t)
+        checkers.append(c)
+        o = c.eval(xx[t.order], m64[t.order], eps2)
+        a = np.empty_like(xx)
+        a[t.order] = o[:, :3]
+        return a
+
+    for _ in range(nsteps):
+        v = v + 0.5 * dt * acc(x)
+        x = x + dt * v
+        v = v + 0.5 * dt * acc(x)
+    h = 1e-6
+    picks = [(int(b), int(c)) for b, c in zip(rng.choice(n, ncoords, replace=False),
+                                                rng.integers(0, 3, ncoords))]
+    fd, ad = [], []
+    for b, c in picks:
+        xp, xm = pos.astype(np.float64), pos.astype(np.float64)
+        xp[b, c] += h
+        xm[b, c] -= h
+        lp = _fp64_leapfrog_loss(xp, vel.astype(np.float64), m64, eps2, dt, nsteps, trees,
+                                 checkers, target)
+        lm = _fp64_leapfrog_loss(xm, vel.astype(np.float64), m64, eps2, dt, nsteps, trees,
+                                 checkers, target)
+        fd.append((lp - lm) / (2 * h))
+        ad.append(grads[0][b, c])
+    fd, ad = np.array(fd), np.array(ad)
+    err = float(np.abs(ad - fd).max() / np.abs(fd).max())
+    return {"n_bodies": n, "steps": nsteps, "dt": dt, "checkpoint_every": every,
+            "mac_tol": kw["tol"], "loss": "sum (x_final + v_final) . T, T ~ N(0, 1)",
+            "wall_s_checkpointed": walls[0], "wall_s_plain": walls[1],
+            "checkpointed_vs_plain_max_rel": same, "fd_coordinates": ncoords, "fd_h": h,
+            "fd_max_rel_err": err, "bar": 1e-3,
+            "meets_target": bool(same <= 1e-5 and err <= 1e-3),
+            "note": "host tree rebuilt at every force evaluation (as the autograd function "
+                    "does), which bounds the size timed here"}
 
 
 def run_reference(args, w, rank, world):
@@ -314,7 +683,7 @@ def run_reference(args, w, rank, world):
         return 0
     pos, m, eps2, box = make_problem(w)
     tree = build_tree(w, pos, m, box, args.tol or w["tol"])
-    rates = []
+    rates, secs = [], []
     for _ in range(args.warmup):
         cpu_reference_rate(tree, eps2, seconds=1.0)
     per_step = max(2.0, 60.0 / max(1, args.steps))
@@ -322,14 +691,18 @@ def run_reference(args, w, rank, world):
     for _ in range(args.steps):
         info = cpu_reference_rate(tree, eps2, seconds=per_step)
         rates.append(info[0])
+        secs.append(info[1])
     value = float(np.mean(rates))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": float(tree.counts.sum() / value * 1e3),
+            # each step is a bounded sample of the evaluation (see cpu_baseline.sample):
+            # the wall time of that sample, not of a whole evaluation
+            "ms_per_step": float(np.mean(secs) * 1e3),
+            "full_evaluation_ms_at_this_rate": float(tree.counts.sum() / value * 1e3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded)", "config": config_of(args, w, tree, box),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": info[2],
-                             "kind": "reference", "sample": info[3]},
+                             "cpu_model": cpu_model(), "kind": "reference", "sample": info[3]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -372,18 +745,21 @@ def main():
     ap.add_argument("--dropin-groups", type=int, default=2048,
                     help="also time the plain FP32 drop-in path on this many sample groups "
                          "(0: skip)")
-    ap.add_argument("--kdk-steps", type=int, default=0,
-                    help="also run this many graph-captured KDK steps (energy drift)")
+    ap.add_argument("--kdk-steps", type=int, default=32,
+                    help="graph-captured KDK steps of the kdk256 configuration (energy drift)")
     ap.add_argument("--kdk-dt", type=float, default=0.01)
     ap.add_argument("--kdk-rebuild", type=int, default=8)
     ap.add_argument("--autotune", action="store_true",
                     help="pick the tile shapes with the autotuner first (always for batch1024)")
-    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
-                    help="skip timing the adjoint against the forward (Plummer 2^20, order 2)")
-    ap.add_argument("--adjoint", dest="adjoint", action="store_true",
-                    help="time the adjoint against the forward (the default)")
-    ap.set_defaults(adjoint=True)
+    ap.add_argument("--configs", default="all",
+                    help="configuration blocks measured after the timed region: all, none, or a "
+                         "comma list of " + ",".join(ALL_CONFIGS))
     args = ap.parse_args()
+    configs = (list(ALL_CONFIGS) if args.configs == "all" else
+               [] if args.configs == "none" else [c for c in args.configs.split(",") if c])
+    unknown = [c for c in configs if c not in ALL_CONFIGS]
+    if unknown:
+        ap.error(f"unknown configuration(s) {unknown}")
     w = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -461,10 +837,14 @@ def main():
     inter = float(counts.sum())
     value = inter * world / (ms_max * 1e-3)
 
-    # ---- roofline of the dominant kernel (FP32 CUDA-core pipe)
+    # ---- roofline of the dominant kernel (FP32 CUDA-core pipe): the peak is
+    # measured here (FMA microkernel, grav_fp32_peak_CUDA), after the timed region
     peaks, peak_src = measured_peaks()
     sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
-    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s
+    derived = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s at the nominal clock
+    with ClockSampler(local) as pclk:
+        fp32_peak = gc.fp32_peak()
+    peak_clocks = pclk.summary()
     kflops = {"hexa": counts[3] * FLOPS[3], "quad": counts[2] * FLOPS[2],
               "point": (counts[0] + counts[1]) * FLOPS[0]}
     dom = max(("hexa", "quad", "point"), key=lambda k: kms[k])
@@ -474,12 +854,17 @@ def main():
                 "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                 "traffic": float(DRAM_BYTES_PER_INTERACTION[dom] * (
                     counts[3] if dom == "hexa" else counts[2] if dom == "quad" else counts[0] + counts[1])),
-                "traffic_note": "bytes per launch: ncu dram bytes per interaction of the 128^3 "
-                                "capture (profiles/k_batch_box128_full.md) times this launch's "
+                "traffic_note": "bytes per launch: DRAM bytes per interaction of one ncu capture "
+                                "of this kernel on the periodic 128^3 box times this launch's "
                                 "interactions",
-                "peak_source": (f"148 SMs x 128 FP32 lanes x 2 x {sm_mhz:.0f} MHz "
-                                f"(sm_max_mhz of {peak_src} MEASURED_PEAKS.json; it holds no "
-                                f"FP32 CUDA-core figure)"),
+                "peak_source": ("measured in this run: FP32 FMA microkernel "
+                                "(grav_fp32_peak_CUDA, 8 independent chains per thread, 2048 "
+                                "threads per SM, best of 5 launches, CUDA events)"),
+                "peak_clocks": peak_clocks,
+                "peak_derived": derived,
+                "peak_derived_source": (f"148 SMs x 128 FP32 lanes x 2 x {sm_mhz:.0f} MHz "
+                                        f"(sm_max_mhz of {peak_src} MEASURED_PEAKS.json)"),
+                "frac_of_derived": achieved / derived,
                 "kernel_ms": {k: round(v, 4) for k, v in kms.items()},
                 "step_tflops": total_tflops, "step_frac": total_tflops / fp32_peak}
 
@@ -589,23 +974,38 @@ def main():
     if rank == 0 and args.cpu_seconds > 0:
         info = cpu_reference_rate(tree, eps2, seconds=args.cpu_seconds)
         if info:
-            cpu = {"value": info[0], "unit": UNIT, "cores": info[2], "kind": "reference",
-                   "sample": info[3]}
+            cpu = {"value": info[0], "unit": UNIT, "cores": info[2], "cpu_model": cpu_model(),
+                   "kind": "reference", "sample": info[3]}
 
     cfg = config_of(args, w, tree, box)
-    kdk = None
-    if args.kdk_steps > 0:
-        # the time-stepping leg builds its own trees: release this step's
-        # host lists and pinned copies (and torch's cache of pinned blocks) first
-        host = out = tree = None
-        import gc as pygc
-        pygc.collect()
-        empty_host = getattr(torch._C, "_host_emptyCache", None)
-        if empty_host:
-            empty_host()
-        kdk = kdk_run(w, pos, m, eps2, box, args.tol or w["tol"], args.kdk_steps, args.kdk_dt,
-                      args.kdk_rebuild)
-    adj = adjoint_timing() if args.adjoint and rank == 0 else None
+    # the configuration legs build their own trees: release this step's host
+    # lists and pinned copies (and torch's cache of pinned blocks) first
+    host = out = tree = None
+    import gc as pygc
+    pygc.collect()
+    empty_host = getattr(torch._C, "_host_emptyCache", None)
+    if empty_host:
+        empty_host()
+    blocks = {}
+    if rank == 0:
+        for name in configs:
+            log(f"[bench] configuration {name}")
+            tc = time.perf_counter()
+            try:
+                if name == "kdk256":
+                    if w["kind"] != "box":
+                        continue
+                    blocks[name] = kdk_run(w, pos, m, eps2, box, args.tol or w["tol"],
+                                           args.kdk_steps, args.kdk_dt, args.kdk_rebuild)
+                else:
+                    fn = {"plummer64k": config_plummer64k, "box128": config_box128,
+                          "batch1024": config_batch1024, "adjoint": config_adjoint}[name]
+                    blocks[name] = fn(args, stream)
+            except Exception as exc:  # one failing leg must not hide the others
+                blocks[name] = {"error": f"{type(exc).__name__}: {exc}"}
+            blocks.setdefault(name, {})["leg_wall_s"] = time.perf_counter() - tc
+            pygc.collect()
+            torch.cuda.empty_cache()
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -622,10 +1022,8 @@ def main():
             line["tuning"] = tuning
         if batch_kdk:
             line["batch_kdk"] = batch_kdk
-        if kdk:
-            line["kdk"] = kdk
-        if adj:
-            line["adjoint"] = adj
+        if blocks:
+            line["configs"] = blocks
         print(json.dumps(line))
     if world > 1:
         dist.barrier()

@@ -203,11 +203,12 @@ typedef struct grav_tuning {
     int chunk_h;                /* max order-4 cells per work item */
     int blocks_per_sm;          /* persistent grid = blocks_per_sm x SM count (0: as many as fit) */
     int ewald_n;                /* Ewald table nodes per axis (0: 32) */
-    int ewald_side;             /* periodic: the Ewald correction moments run on a side stream
-                                   beside the list kernels with this many 2-warp blocks per SM
-                                   (-1: inside the finish pass, after them; 0: automatic, 2
-                                   when the correction list is under 1.5 % of the order-4
-                                   interactions, else -1) */
+    int ewald_side;             /* periodic: where the Ewald correction moments run.  > 0: on a
+                                   side stream beside the list kernels, in this many two-warp
+                                   blocks per SM; -k (k = 1, 2, 4): on the evaluation's stream
+                                   between the list kernels and the finish pass, with the SMs to
+                                   themselves, in blocks of k warps; 0: automatic (-2).  The
+                                   results are the same either way. */
 } grav_tuning;
 
 /*

@@ -698,10 +698,12 @@ double orc_fd_partial_loss(int s, long j, long n, const double *x, const double 
 
 /*
  * FP64 gradient of L = sum_i w_i.a_i + u_i phi_i for the Plummer-softened
- * direct sum over all pairs (self excluded): dL/dx (3 per body), dL/dm.
- * With d = x_i - x_j, rho^2 = |d|^2 + eps2, the pair adds to body i
- * -(m_j)[rho^-3 w_i - 3 rho^-5 (w_i.d) d - u_i rho^-3 d] and the opposite to
- * body j, and dL/dm_j -= rho^-3 w_i.d + u_i rho^-1 (sink i, source j).
+ * direct sum over all pairs, the self pair included as the tree's lists
+ * include it (it adds -m_i / eps to phi_i and nothing to a_i): dL/dx (3 per
+ * body), dL/dm.  With d = x_i - x_j, rho^2 = |d|^2 + eps2, the pair adds to
+ * body i -(m_j)[rho^-3 w_i - 3 rho^-5 (w_i.d) d - u_i rho^-3 d] and the
+ * opposite to body j, and dL/dm_j -= rho^-3 w_i.d + u_i rho^-1 (sink i,
+ * source j); the self pair adds -u_i / eps to dL/dm_i.
  */
 void orc_direct_grad(long n, const double *x, const double *m, const double *w, const double *u,
                      double eps2, double *gx, double *gm) {
@@ -726,6 +728,8 @@ void orc_direct_grad(long n, const double *x, const double *m, const double *w, 
                 g[k] += m[i] * (ri3 * w[3 * j + k] - 3.0 * ri5 * wdj * dj[k] - u[j] * ri3 * dj[k]);
             gmi -= ri3 * wdj + u[j] * ri;
         }
+        if (eps2 > 0.0)
+            gmi -= u[i] / sqrt(eps2);
         for (int k = 0; k < 3; k++) gx[3 * i + k] = g[k];
         gm[i] = gmi;
     }

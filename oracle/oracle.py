@@ -96,6 +96,21 @@ def orc():
                                          ctypes.c_double, _i64p, ctypes.c_long, _f64p, _f64p]
         lib.orc_groups_eval.argtypes = [ctypes.c_int, _f32p, ctypes.c_int, _i64p, _i64p, _i64p,
                                         _i32p, ctypes.c_long, _f32p, ctypes.c_float, _f64p]
+        L_, vp = ctypes.c_long, ctypes.c_void_p
+        lib.orc_lists_eval64.argtypes = [L_, _f64p, _f64p, L_, _i64p, _i32p, L_, _i64p, _i32p,
+                                         _i64p, _u32p, vp, vp, ctypes.c_double, _f64p]
+        lib.orc_lists_eval64.restype = ctypes.c_int
+        lib.orc_fd_hits.argtypes = [L_, L_, _i32p, L_, _i64p, _u32p, vp, vp, ctypes.c_int, _i64p,
+                                    _i64p, L_, vp, vp]
+        lib.orc_fd_hits.restype = L_
+        lib.orc_fd_partial_loss.argtypes = [ctypes.c_int, L_, L_, _f64p, _f64p, L_, _i64p, _i32p,
+                                            L_, _i64p, _i32p, _i64p, _i64p, _u32p, vp, vp, L_,
+                                            _i64p, np.ctypeslib.ndpointer(np.uint64,
+                                                                         flags="C_CONTIGUOUS"),
+                                            _f64p, _f64p, ctypes.c_double]
+        lib.orc_fd_partial_loss.restype = ctypes.c_double
+        lib.orc_direct_grad.argtypes = [L_, _f64p, _f64p, _f64p, _f64p, ctypes.c_double, _f64p,
+                                        _f64p]
         _orc = lib
     return _orc
 
@@ -226,3 +241,119 @@ def tree_eval(tree, eps2, quad_kind=QUAD_PLUMMER_P, hexa_kind=HEXA_PLUMMER, mono
             orc().orc_groups_eval(kind, d, KIND_SZ[kind], bf, bc, sf, sc, len(sf), pos, eps2,
                                   out.ravel())
     return out
+
+
+# ---------------------------------------------------------------- FP64 list checks
+class ListsFP64:
+    """FP64 evaluation of a walked isolated tree's batched index lists with
+    every cell's moments recomputed from the bodies (orc_lists_eval64), and
+    central differences of L = sum w.a + u phi restricted to the terms that
+    depend on one body (orc_fd_hits / orc_fd_partial_loss): the checker of
+    the hand-written adjoint.  Point and quadrupole lists only."""
+
+    def __init__(self, tree):
+        self.t = t = tree
+        if len(t.hlist):
+            raise ValueError("order-4 lists are not covered by the FP64 list checker")
+        self.n, self.nc, self.ng = int(t.n), int(t.ncells), int(t.ngroups)
+        first, count = t.cell_ranges()
+        child, nchild, _ = t.cell_links()
+        self.cfirst = np.ascontiguousarray(first, np.int64)
+        self.ccount = np.ascontiguousarray(count, np.int32)
+        parent = np.full(self.nc, -1, np.int32)
+        inner = np.nonzero(child >= 0)[0]
+        parent[np.concatenate([np.arange(child[c], child[c] + nchild[c]) for c in inner])
+               if len(inner) else np.zeros(0, np.int64)] = np.repeat(inner, nchild[inner])
+        self.parent = parent
+        leaves = np.nonzero(child < 0)[0]
+        leaf = np.full(self.n, -1, np.int64)
+        for c in leaves:
+            leaf[first[c]:first[c] + count[c]] = c
+        self.leaf = leaf
+        self.gfirst = np.ascontiguousarray(t.groups["first"], np.int64)
+        self.gcount = np.ascontiguousarray(t.groups["count"], np.int32)
+        self.bgroup = np.repeat(np.arange(self.ng, dtype=np.int64), self.gcount)
+        self.pptr = np.ascontiguousarray(t.ptr[0], np.int64)
+        self.plist = np.ascontiguousarray(t.plist, np.uint32)
+        self.has_q = len(t.qlist) > 0
+        self.qptr = np.ascontiguousarray(t.ptr[1], np.int64)
+        self.qlist = np.ascontiguousarray(t.qlist if self.has_q else np.zeros(1, np.uint32))
+
+    def _q(self):
+        return (self.qptr.ctypes.data, self.qlist.ctypes.data) if self.has_q else (None, None)
+
+    def eval(self, x, m, eps2):
+        """(n, 4) FP64 (ax, ay, az, phi), tree order, positions x (n, 3) and masses m."""
+        x = np.ascontiguousarray(x, np.float64)
+        m = np.ascontiguousarray(m, np.float64)
+        out = np.zeros((self.n, 4))
+        qp, ql = self._q()
+        rc = orc().orc_lists_eval64(self.n, x.ravel(), m, self.nc, self.cfirst, self.ccount,
+                                    self.ng, self.gfirst, self.gcount, self.pptr, self.plist,
+                                    qp, ql, float(eps2), out.ravel())
+        if rc:
+            raise ValueError("periodic image codes are not covered")
+        return out
+
+    def select(self, bodies):
+        """Prepare central differences for up to 64 bodies (tree order)."""
+        self.sel = np.ascontiguousarray(bodies, np.int64)
+        qp, ql = self._q()
+        args = (self.n, self.nc, self.parent, self.ng, self.pptr, self.plist, qp, ql,
+                len(self.sel), self.sel, self.leaf)
+        nh = orc().orc_fd_hits(*args, 0, None, None)
+        if nh < 0:
+            raise ValueError("at most 64 selected bodies")
+        self.hits = np.zeros(3 * max(nh, 1), np.int64)
+        self.hmask = np.zeros(max(nh, 1), np.uint64)
+        orc().orc_fd_hits(*args, nh, self.hits.ctypes.data, self.hmask.ctypes.data)
+        self.nhits = nh
+
+    def partial_loss(self, s, x, m, w, u, eps2):
+        """The part of L that depends on selected body s (index into select()'s list)."""
+        qp, ql = self._q()
+        return orc().orc_fd_partial_loss(
+            int(s), int(self.sel[s]), self.n, np.ascontiguousarray(x, np.float64).ravel(),
+            np.ascontiguousarray(m, np.float64), self.nc, self.cfirst, self.ccount, self.ng,
+            self.gfirst, self.gcount, self.bgroup, self.pptr, self.plist, qp, ql, self.nhits,
+            self.hits, self.hmask, np.ascontiguousarray(w, np.float64).ravel(),
+            np.ascontiguousarray(u, np.float64), float(eps2))
+
+    def fd_grad(self, x, m, w, u, eps2, coords, h=1e-6, mass_rel=False):
+        """Central differences of L for (selected body s, component c) pairs;
+        c = 3 means the mass (relative step h m when mass_rel)."""
+        x = np.array(x, np.float64)
+        m = np.array(m, np.float64)
+        out = []
+        for s, c in coords:
+            j = int(self.sel[s])
+            if c < 3:
+                x0 = x[j, c]
+                x[j, c] = x0 + h
+                lp = self.partial_loss(s, x, m, w, u, eps2)
+                x[j, c] = x0 - h
+                lm = self.partial_loss(s, x, m, w, u, eps2)
+                x[j, c] = x0
+                out.append((lp - lm) / (2 * h))
+            else:
+                m0 = m[j]
+                hh = h * m0 if mass_rel else h
+                m[j] = m0 + hh
+                lp = self.partial_loss(s, x, m, w, u, eps2)
+                m[j] = m0 - hh
+                lm = self.partial_loss(s, x, m, w, u, eps2)
+                m[j] = m0
+                out.append((lp - lm) / (2 * hh))
+        return np.array(out)
+
+
+def direct_grad(x, m, w, u, eps2):
+    """FP64 dL/dx (n, 3) and dL/dm (n,) of L = sum w.a + u phi for the
+    Plummer-softened direct sum (orc_direct_grad)."""
+    x = np.ascontiguousarray(x, np.float64)
+    m = np.ascontiguousarray(m, np.float64)
+    gx = np.zeros_like(x)
+    gm = np.zeros(len(m))
+    orc().orc_direct_grad(len(m), x.ravel(), m, np.ascontiguousarray(w, np.float64).ravel(),
+                          np.ascontiguousarray(u, np.float64), float(eps2), gx.ravel(), gm)
+    return gx, gm

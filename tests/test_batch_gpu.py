@@ -252,3 +252,41 @@ def test_ewald_moments_on_side_stream_match_finish_pass(gc):
         outs.append(plan.download())
         plan.free()
     assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+
+
+@pytest.mark.parametrize("order", [2, 4])
+def test_plain_fp32_kernels_match_oracle(gc, order):
+    """precision = 1 (plain FP32: absolute coordinates, plain sums) on the same
+    lists: a Plummer sphere about the origin, where absolute FP32
+    coordinates lose nothing, matches the oracle like the mixed form."""
+    t = make_tree("plummer", 20000, leaf_max=16, group_max=32, p2cut=7,
+                  p4cut=20 if order == 4 else 0, tol=1e-3)
+    eps2 = 0.01 ** 2
+    plan = gc.Plan(t, eps2, plain=True)
+    plan.eval()
+    got = plan.download()
+    plan.free()
+    want = O.tree_eval(t, eps2)
+    assert rms_rel(got[:, :3], want[:, :3]) < RMS_TOL
+    assert rms_rel(got[:, 3:], want[:, 3:]) < RMS_TOL
+
+
+def test_plain_fp32_loses_accuracy_far_from_the_origin(gc):
+    """The same sphere moved to (1e4, 1e4, 1e4), order 2: plain FP32 rounds
+    every cell centre to an absolute FP32 coordinate (ulp 1e-3 there), the
+    mixed form keeps FP32 offsets from FP64 group centres.  Reference: the
+    FP64 evaluation of the same lists from the same (FP32) bodies."""
+    from pgrav import host, ics
+    pos, m = ics.plummer(20000, seed=11)
+    pos = pos + np.float32(1.0e4)
+    t = host.Tree(pos, m, leaf_max=16, group_max=32, p2cut=7, p4cut=0, tol=1e-3)
+    eps2 = 0.01 ** 2
+    want = O.ListsFP64(t).eval(t.sorted_pos, t.points[:t.n, 3], eps2)
+    errs = {}
+    for plain in (False, True):
+        plan = gc.Plan(t, eps2, plain=plain)
+        plan.eval()
+        errs[plain] = rms_rel(plan.download()[:, :3], want[:, :3])
+        plan.free()
+    assert errs[False] < 1e-5, errs
+    assert errs[True] > 10 * errs[False], errs
