@@ -30,6 +30,7 @@
 #include <numeric>
 #include <vector>
 
+#include "build.cuh"
 #include "common.cuh"
 #include "gravcuda.h"
 #include "ewald.cuh"
@@ -1053,7 +1054,9 @@ struct grav_plan {
     CUtensorMap tmap[3];    // row-gather views of the point, quadrupole and order-4 tables
     int timing = 0;         // record events around each kernel of an evaluation
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-    std::vector<int64_t> lists_ptr[3];  // host copies of the P, Q, H list offsets (queue rebuilds)
+    std::vector<int64_t> lists_ptr[4];  // host copies of the P, Q, H (queue rebuilds) and
+                                        // correction list offsets
+    int64_t *order = nullptr;           // device-built plans: tree position -> input index
     bool staged = false;                // the Q/H tensor maps view pre-staged tables
     bool plain = false;                 // plain FP32 kernels (grav_problem.precision = 1)
     float4 *qstage = nullptr, *hstage = nullptr;  // pre-staged cell tables (k_stage_cells)
@@ -1249,6 +1252,7 @@ namespace {
 // lists while the kernels evaluate the previous range, and the kernels'
 // own index checks stand in for the upload-time list check.
 thread_local double t_phase[5];  // grav_groups_CUDA_phases
+thread_local double t_build = 0, t_build_phase[6] = {0, 0, 0, 0, 0, 0};  // grav_plan_build_phases
 
 // The end-to-end call's device buffers come from a pool per device that
 // keeps freed memory reserved (until grav_groups_release_CUDA): mapping and
@@ -1283,8 +1287,11 @@ int e2e_pool(cudaMemPool_t *out) {
     return 0;
 }
 
+// adopt: a tree built on the device (gpu_tree_build) whose tables and lists
+// the plan takes over instead of copying; hp then holds its host copies of
+// the groups and offsets and device pointers to everything else.
 int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **plan_out,
-                int nchunks) {
+                int nchunks, const DevTree *adopt = nullptr) {
     *plan_out = nullptr;
     const double t_start = now_s();
     if (!hp || hp->nbodies <= 0 || hp->ngroups <= 0 || !hp->points || !hp->groups ||
@@ -1301,16 +1308,27 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
     cudaDeviceGetAttribute(&pl->nsm, cudaDevAttrMultiProcessorCount, dev);
     pl->hp = *hp;
     pl->plain = hp->precision == 1;
+    if (adopt) {
+        // the plan owns every buffer of the device-built tree from here on,
+        // failures included (grav_plan_free releases them)
+        void *own[] = {adopt->points, adopt->qcells, adopt->hcells, adopt->groups,
+                       adopt->list[0], adopt->list[1], adopt->list[2], adopt->list[3],
+                       adopt->order};
+        for (void *q : own)
+            if (q)
+                pl->allocs.push_back(q);
+        pl->order = adopt->order;
+    }
     pl->tune = tuning ? *tuning : default_tuning();
     const int64_t ng = hp->ngroups, nb = hp->nbodies, np = hp->nbodies + hp->ncells;
     const bool deferred = nchunks > 0;
     if (deferred && hp->lists_in_host) {
-        delete pl;
+        grav_plan_free(pl);
         return gc::set_status(-1, "upload: deferred lists and lists_in_host exclude each other");
     }
     if (deferred) {
         if (int e = e2e_pool(&pl->pool)) {
-            delete pl;
+            grav_plan_free(pl);
             return e;
         }
     }
@@ -1329,7 +1347,7 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
     if (hp->pptr[0] != 0 || (hp->qptr && hp->qptr[0] != 0) || (hp->hptr && hp->hptr[0] != 0))
         bad_group |= 1;
     if (bad_group) {
-        delete pl;
+        grav_plan_free(pl);
         return gc::set_status(-1, "a group has 0 or more than 32 sinks, lies outside the bodies, "
                                   "or has list offsets that decrease or do not start at 0");
     }
@@ -1339,14 +1357,14 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
     const int64_t *eptr = hp->pptr;
     if ((hp->qptr && hp->qptr[ng] && (!hp->qcells || hp->ncells <= 0)) ||
         (hp->hptr && hp->hptr[ng] && (!hp->hcells || hp->ncells <= 0))) {
-        delete pl;
+        grav_plan_free(pl);
         return gc::set_status(-1, "a cell list without its cell table");
     }
     const bool want_ewald = hp->box > 0 && hp->ewald;
     if (want_ewald) {
         if (!hp->cptr || (!hp->clist && !(deferred && hp->zlist[3])) ||
             (hp->ncells > 0 && !hp->hcells)) {
-            delete pl;
+            grav_plan_free(pl);
             return gc::set_status(-1, "the Ewald correction needs the correction list and the "
                                       "order-4 cell table");
         }
@@ -1356,7 +1374,7 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
             if (hp->cptr[g + 1] < hp->cptr[g])
                 bad |= 1;
         if (bad || hp->cptr[0] != 0) {
-            delete pl;
+            grav_plan_free(pl);
             return gc::set_status(-1, "bad correction list offsets");
         }
     }
@@ -1376,13 +1394,13 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
                         bad |= 1;
             }
             if (bad) {
-                delete pl;
+                grav_plan_free(pl);
                 return gc::set_status(-1, "bad run-packed list offsets (kind %d)", k);
             }
             packed[k] = true;
         }
         if (!hp->plist && !packed[0]) {
-            delete pl;
+            grav_plan_free(pl);
             return gc::set_status(-1, "grav_groups_CUDA: no point list");
         }
     }
@@ -1394,18 +1412,28 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
     DevProblem &d = pl->dp;
     int rc = 0;
     float4 *pts = nullptr;
-    rc |= dev_copy(pl, deferred, reinterpret_cast<const float4 *>(hp->points), (size_t)np, &pts);
-    d.points = pts;
     nln_qcell *qc = nullptr;
     nln_hcell *hc = nullptr;
-    if (hp->qptr && hp->qptr[ng])
-        rc |= dev_copy(pl, deferred, hp->qcells, (size_t)hp->ncells, &qc);
-    if ((hp->hptr && hp->hptr[ng]) || (want_ewald && hp->ncells > 0))
-        rc |= dev_copy(pl, deferred, hp->hcells, (size_t)hp->ncells, &hc);
+    nln_group *gr = nullptr;
+    const bool want_q = hp->qptr && hp->qptr[ng];
+    const bool want_h = (hp->hptr && hp->hptr[ng]) || (want_ewald && hp->ncells > 0);
+    if (adopt) {
+        pts = adopt->points;
+        qc = want_q ? adopt->qcells : nullptr;
+        hc = want_h ? adopt->hcells : nullptr;
+        gr = adopt->groups;
+    } else {
+        rc |= dev_copy(pl, deferred, reinterpret_cast<const float4 *>(hp->points), (size_t)np,
+                       &pts);
+        if (want_q)
+            rc |= dev_copy(pl, deferred, hp->qcells, (size_t)hp->ncells, &qc);
+        if (want_h)
+            rc |= dev_copy(pl, deferred, hp->hcells, (size_t)hp->ncells, &hc);
+        rc |= dev_copy(pl, deferred, hp->groups, (size_t)ng, &gr);
+    }
+    d.points = pts;
     d.qcells = qc;
     d.hcells = hc;
-    nln_group *gr = nullptr;
-    rc |= dev_copy(pl, deferred, hp->groups, (size_t)ng, &gr);
     d.groups = gr;
     if (pl->tune.warps_per_block < 1 || pl->tune.warps_per_block > 8)
         pl->tune.warps_per_block = 8;
@@ -1419,8 +1447,8 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
     // work items, created group by group (slot order), then sorted per kind by cost
     std::vector<Item> items[3];
     std::vector<int64_t> gslot;
-    const int64_t *ptrs[3] = {eptr, hp->qptr, hp->hptr};
-    for (int k = 0; k < 3; k++)
+    const int64_t *ptrs[4] = {eptr, hp->qptr, hp->hptr, want_ewald ? hp->cptr : nullptr};
+    for (int k = 0; k < 4; k++)
         if (ptrs[k])
             pl->lists_ptr[k].assign(ptrs[k], ptrs[k] + ng + 1);
     if (deferred) {
@@ -1505,6 +1533,10 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
             pl->zptr_dev[k] = zp;
             pl->lptr_dev[k] = lp;
         }
+    } else if (adopt) {
+        l0 = adopt->list[0];
+        l1 = hp->qptr ? adopt->list[1] : nullptr;
+        l2 = hp->hptr ? adopt->list[2] : nullptr;
     } else if (hp->lists_in_host) {
         // the kernels read the lists in place from page-locked host memory
         const uint32_t *m0 = mapped_host(hp->plist);
@@ -1560,6 +1592,8 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
             }
         } else if (deferred) {
             cl = all_clist;
+        } else if (adopt) {
+            cl = adopt->list[3];
         } else {
             rc |= dev_copy(pl, hp->clist, (size_t)std::max<int64_t>(1, hp->cptr[ng]), &cl);
         }
@@ -1617,7 +1651,10 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
         return rc;
     }
     cudaMemset(err, 0, sizeof(unsigned));
-    if (hp->lists_in_host || deferred) {
+    if (adopt) {
+        // lists from the device builder, which sized and checked them itself
+        for (int k = 0; k < 4; k++) pl->counts[k] = adopt->counts[k];
+    } else if (hp->lists_in_host || deferred) {
         // entries are checked by the kernels as they read them (bad ones set
         // the error word); the point list's body/cell split is not counted
         int64_t tot = 0;
@@ -2005,6 +2042,108 @@ extern "C" void grav_plan_free(grav_plan *pl) {
     if (pl->join)
         cudaEventDestroy(pl->join);
     delete pl;
+}
+
+extern "C" int grav_plan_build_CUDA(const nln_params *params, const float *bodies, int64_t n,
+                                    double eps2, float quad_phi_sign, int ewald,
+                                    const grav_tuning *tuning, grav_plan **plan) {
+    if (!params || !bodies || !plan || n <= 0)
+        return gc::set_status(-1, "grav_plan_build_CUDA: bad arguments");
+    *plan = nullptr;
+    if (((uintptr_t)bodies & 15u) != 0)
+        return gc::set_status(-1, "grav_plan_build_CUDA: bodies must be 16-byte aligned");
+    DevTree T;
+    const double t0 = now_s();
+    if (int rc = gpu_tree_build(*params, reinterpret_cast<const float4 *>(bodies), n, 0, T)) {
+        dev_tree_free(T);
+        return rc;
+    }
+    grav_problem hp{};
+    hp.nbodies = T.n;
+    hp.ncells = T.ncells;
+    hp.ngroups = T.ngroups;
+    hp.points = reinterpret_cast<const float *>(T.points);
+    hp.qcells = T.qcells;
+    hp.hcells = T.hcells;
+    hp.groups = T.groups_h.data();
+    hp.pptr = T.ptr_h[0].data();
+    hp.qptr = T.ptr_h[1].data();
+    hp.hptr = T.ptr_h[2].data();
+    hp.plist = T.list[0];
+    hp.qlist = T.list[1];
+    hp.hlist = T.list[2];
+    hp.eps2 = eps2;
+    hp.box = params->box;
+    hp.quad_phi_sign = quad_phi_sign;
+    hp.ewald = params->box > 0 && ewald;
+    hp.cptr = T.ptr_h[3].data();
+    hp.clist = T.list[3];
+    // the tree's links (for the device refit and the adjoint) come back first:
+    // the plan takes the device buffers over
+    const int64_t nc = T.ncells;
+    std::vector<int64_t> first(nc);
+    std::vector<int32_t> count(nc), child(nc), nchild(nc), level(nc);
+    cudaError_t e = cudaMemcpy(first.data(), T.cell_first, nc * 8, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(count.data(), T.cell_count, nc * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(child.data(), T.cell_child, nc * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(nchild.data(), T.cell_nchild, nc * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(level.data(), T.cell_level, nc * 4, cudaMemcpyDeviceToHost);
+    void *links[] = {T.cell_first, T.cell_count, T.cell_child, T.cell_nchild, T.cell_level};
+    for (void *q : links) cudaFree(q);
+    T.cell_first = nullptr;
+    T.cell_count = T.cell_child = T.cell_nchild = T.cell_level = nullptr;
+    if (e != cudaSuccess) {
+        dev_tree_free(T);
+        return gc::cuda_status(e, "grav_plan_build_CUDA: tree links");
+    }
+    grav_plan *pl = nullptr;
+    if (int rc = upload_impl(&hp, tuning, &pl, 0, &T))
+        return rc;  // upload_impl took the buffers over and released them
+    if (int rc = grav_plan_set_tree_CUDA(pl, first.data(), count.data(), child.data(),
+                                         nchild.data(), level.data())) {
+        grav_plan_free(pl);
+        return rc;
+    }
+    t_build = now_s() - t0;
+    for (int k = 0; k < 6; k++) t_build_phase[k] = T.seconds[k];
+    *plan = pl;
+    return 0;
+}
+
+extern "C" const int64_t *grav_plan_order(const grav_plan *pl) { return pl ? pl->order : nullptr; }
+
+extern "C" void grav_plan_build_phases(double seconds[7]) {
+    for (int k = 0; k < 6; k++) seconds[k] = t_build_phase[k];
+    seconds[6] = t_build;
+}
+
+extern "C" int grav_plan_problem(const grav_plan *pl, grav_problem *out) {
+    if (!pl || !out)
+        return gc::set_status(-1, "grav_plan_problem: bad arguments");
+    *out = pl->hp;
+    const DevProblem &d = pl->dp;
+    out->points = reinterpret_cast<const float *>(d.points);
+    out->qcells = d.qcells;
+    out->hcells = d.hcells;
+    out->groups = d.groups;
+    out->plist = d.list[0];
+    out->qlist = d.list[1];
+    out->hlist = d.list[2];
+    out->clist = d.clist;
+    auto host = [&](int k) { return pl->lists_ptr[k].empty() ? nullptr : pl->lists_ptr[k].data(); };
+    out->pptr = host(0);
+    out->qptr = host(1);
+    out->hptr = host(2);
+    out->cptr = host(3);
+    for (int k = 0; k < 4; k++) {
+        out->zptr[k] = nullptr;
+        out->zlist[k] = nullptr;
+    }
+    return 0;
 }
 
 namespace {

@@ -17,6 +17,8 @@
 
 #include <omp.h>
 
+#include "tree_math.h"
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -54,28 +56,6 @@ inline uint64_t spread3(uint32_t v) {
 }
 
 constexpr int KEY_LEVELS = 21;
-
-// Newton iteration on a polynomial sum_k a[k] r^k, started at x1 and stopped
-// when the step is below xacc; returns x1 when it does not converge in 30
-// steps (the behaviour of rtnewt, nln/cofm.c:602-624, with rcrit_poly's
-// Horner evaluation, nln/cofm.c:577-596).
-double newton_root(const double *a, int n, double x1, double xacc) {
-    double r = x1;
-    for (int it = 0; it < 30; it++) {
-        double p = a[n], dp = 0.0;
-        for (int k = n; k > 0; k--) {
-            dp = dp * r + p;
-            p = p * r + a[k - 1];
-        }
-        if (!std::isfinite(p) || !std::isfinite(dp) || dp == 0.0)
-            return x1;
-        double dx = p / dp;
-        r -= dx;
-        if (std::fabs(dx) < xacc)
-            return r;
-    }
-    return x1;
-}
 
 }  // namespace
 
@@ -118,6 +98,7 @@ struct nln_tree {
     ListBuf clist;  // periodic correction list
     std::vector<int64_t> zptr[4];  // run-packed lists (nln_tree_pack)
     ListBuf zlist[4];
+    std::vector<nln_wcell> wcells;  // what the walk reads of each cell (built by nln_tree_walk)
     std::vector<int64_t> aptr[3];
     std::vector<float> adata[3];
     int64_t counts[4] = {0, 0, 0, 0};
@@ -207,8 +188,32 @@ static void build_cells(nln_tree *t, const std::vector<uint64_t> &keys) {
     }
 }
 
+// The canonical order of every per-cell FP64 sum over a cell's bodies, which
+// the GPU tree builder reproduces exactly: bodies in blocks of 64 summed in
+// order, those partials in blocks of 64 summed in order, then those summed
+// in order.  term(k, acc) adds body k's K terms into acc.
+constexpr int kSumBlock = 64;
+
+template <int K, typename Term>
+static void canon_sum(int32_t count, Term term, double out[K]) {
+    for (int q = 0; q < K; q++) out[q] = 0.0;
+    const int32_t nb0 = (count + kSumBlock - 1) / kSumBlock;
+    const int32_t nb1 = (nb0 + kSumBlock - 1) / kSumBlock;
+    for (int32_t b1 = 0; b1 < nb1; b1++) {
+        double p1[K] = {};
+        for (int32_t b0 = b1 * kSumBlock; b0 < std::min(nb0, (b1 + 1) * kSumBlock); b0++) {
+            double p0[K] = {};
+            for (int32_t k = b0 * kSumBlock; k < std::min(count, (b0 + 1) * kSumBlock); k++)
+                term(k, p0);
+            for (int q = 0; q < K; q++) p1[q] += p0[q];
+        }
+        for (int q = 0; q < K; q++) out[q] += p1[q];
+    }
+}
+
 // FP64 moments about the centre of mass, directly from the bodies of each
-// cell, then the traceless R^-l normalisation of nln/cofm.c:398-420,486-562.
+// cell (canon_sum order), then the traceless R^-l normalisation of
+// nln/cofm.c:398-420,486-562.
 static void compute_moments(nln_tree *t) {
     const int64_t nc = (int64_t)t->cells.size();
     t->qc.assign(nc, nln_qcell{});
@@ -223,170 +228,53 @@ static void compute_moments(nln_tree *t) {
         Cell &c = t->cells[ci];
         const float *P = t->spos.data() + 3 * c.first;
         const float *M = t->smass.data() + c.first;
-        double m = 0, s[3] = {0, 0, 0};
-        for (int32_t k = 0; k < c.count; k++) {
-            m += M[k];
-            for (int d = 0; d < 3; d++) s[d] += M[k] * ((double)P[3 * k + d] - c.gc[d]);
-        }
-        for (int d = 0; d < 3; d++) c.cen[d] = c.gc[d] + (m > 0 ? s[d] / m : 0.0);
+        double s1[4];
+        canon_sum<4>(c.count, [&](int32_t k, double *a) { nln_mass_terms(P + 3 * k, M[k], c.gc, a); },
+                     s1);
+        const double m = s1[0];
+        for (int d = 0; d < 3; d++) c.cen[d] = c.gc[d] + (m > 0 ? s1[1 + d] / m : 0.0);
         c.mass = m;
-        // raw moments about cen
-        double x2 = 0, xy = 0, xz = 0, y2 = 0, yz = 0, z2 = 0;
-        double x3 = 0, x2y = 0, x2z = 0, xy2 = 0, xyz = 0, xz2 = 0, y3 = 0, y2z = 0, yz2 = 0,
-               z3 = 0;
-        double x4 = 0, x3y = 0, x3z = 0, x2y2 = 0, x2yz = 0, x2z2 = 0, xy3 = 0, xy2z = 0,
-               xyz2 = 0, xz3 = 0, y4 = 0, y3z = 0, y2z2 = 0, yz3 = 0, z4 = 0;
-        double r2s = 0, r4s = 0, r6s = 0, bmax2 = 0;
-        for (int32_t k = 0; k < c.count; k++) {
-            const double w = M[k];
-            const double x = (double)P[3 * k] - c.cen[0];
-            const double y = (double)P[3 * k + 1] - c.cen[1];
-            const double z = (double)P[3 * k + 2] - c.cen[2];
-            const double xx = x * x, yy = y * y, zz = z * z, r2 = xx + yy + zz;
-            bmax2 = std::max(bmax2, r2);
-            r2s += w * r2;
-            r4s += w * r2 * r2;
-            r6s += w * r2 * r2 * r2;
-            x2 += w * xx; xy += w * x * y; xz += w * x * z;
-            y2 += w * yy; yz += w * y * z; z2 += w * zz;
-            x3 += w * xx * x; x2y += w * xx * y; x2z += w * xx * z;
-            xy2 += w * x * yy; xyz += w * x * y * z; xz2 += w * x * zz;
-            y3 += w * yy * y; y2z += w * yy * z; yz2 += w * y * zz; z3 += w * zz * z;
-            x4 += w * xx * xx; x3y += w * xx * x * y; x3z += w * xx * x * z;
-            x2y2 += w * xx * yy; x2yz += w * xx * y * z; x2z2 += w * xx * zz;
-            xy3 += w * x * yy * y; xy2z += w * x * yy * z; xyz2 += w * x * y * zz;
-            xz3 += w * x * zz * z; y4 += w * yy * yy; y3z += w * yy * y * z;
-            y2z2 += w * yy * zz; yz3 += w * y * zz * z; z4 += w * zz * zz;
-        }
+        // raw moments about cen (layout of nln_moment_terms) and the largest r^2
+        double mo[NLN_NMOM];
+        double bmax2 = 0;
+        canon_sum<NLN_NMOM>(c.count, [&](int32_t k, double *a) {
+            bmax2 = std::max(bmax2, nln_moment_terms(P + 3 * k, M[k], c.cen, a));
+        }, mo);
         c.bmax = std::sqrt(bmax2);
-        c.B2 = r2s;
-        c.B4 = r4s;
-        c.B6 = r6s;
-        const double ri = c.bmax > 0 ? 1.0 / c.bmax : 0.0;
-        // point-table monopole of the cell
-        float *pt = &t->points[4 * (t->n + ci)];
-        for (int d = 0; d < 3; d++) pt[d] = (float)c.cen[d];
-        pt[3] = (float)m;
-        // quadrupole, nln/cofm.c:398-420
-        double tq = (x2 + y2 + z2) / 3.0;
-        double q2[5] = {(x2 - tq) * ri * ri, xy * ri * ri, (y2 - tq) * ri * ri, xz * ri * ri,
-                        yz * ri * ri};
-        // octupole, nln/cofm.c:507-522
-        double tx = (x3 + xy2 + xz2) / 5.0, ty = (x2y + y3 + yz2) / 5.0,
-               tz = (x2z + y2z + z3) / 5.0;
-        double r3 = ri * ri * ri;
-        double q3[7] = {(x3 - 3.0 * tx) * r3, (x2y - ty) * r3, (xy2 - tx) * r3,
-                        (y3 - 3.0 * ty) * r3, (x2z - tz) * r3, xyz * r3,
-                        (y2z - tz) * r3};
-        // hexadecapole, nln/cofm.c:523-558
-        double txx = (x4 + x2y2 + x2z2) / 7.0, txy = (x3y + xy3 + xyz2) / 7.0,
-               txz = (x3z + xy2z + xz3) / 7.0, tyy = (x2y2 + y4 + y2z2) / 7.0,
-               tyz = (x2yz + y3z + yz3) / 7.0, tzz = (x2z2 + y2z2 + z4) / 7.0;
-        double tt = 0.1 * (txx + tyy + tzz);
-        double r4 = r3 * ri;
-        double q4[9] = {(x4 - 6.0 * (txx - tt)) * r4, (x3y - 3.0 * txy) * r4,
-                        (x2y2 - (txx + tyy - 2.0 * tt)) * r4, (xy3 - 3.0 * txy) * r4,
-                        (y4 - 6.0 * (tyy - tt)) * r4, (x3z - 3.0 * txz) * r4,
-                        (x2yz - tyz) * r4, (xy2z - txz) * r4, (y3z - 3.0 * tyz) * r4};
-        nln_qcell &q = t->qc[ci];
-        nln_hcell &h = t->hc[ci];
-        for (int d = 0; d < 3; d++) q.cen[d] = h.cen[d] = c.cen[d];
-        q.mass = h.mass = (float)m;
-        q.R = h.R = (float)c.bmax;
-        q.B2 = h.B2 = (float)c.B2;
-        q.qxx = (float)q2[0];
-        q.qxy = (float)q2[1];
-        q.qyy = (float)q2[2];
-        q.qxz = (float)q2[3];
-        q.qyz = (float)q2[4];
-        for (int k = 0; k < 5; k++) h.q2[k] = (float)q2[k];
-        for (int k = 0; k < 7; k++) h.q3[k] = (float)q3[k];
-        for (int k = 0; k < 9; k++) h.q4[k] = (float)q4[k];
+        c.B2 = mo[31];
+        c.B4 = mo[32];
+        c.B6 = mo[33];
+        nln_cell_tables(c.cen, m, c.bmax, mo, &t->points[4 * (t->n + ci)], &t->qc[ci], &t->hc[ci]);
     }
 }
 
-// AREL critical radii, nln/cofm.c:276-565 (stol_max at its default;
-// ptol = tol / (1 + ptol_boost bmax / bmax0), bmax0 half the root cube).  A relative tolerance of 0 switches that
-// criterion off (the reference would divide by zero, cofm.c:322-335).
+// The MAC parameters of a tree (nln_cell_rcrit, nln_walk_group).
+static nln_mac mac_of(const nln_tree *t) {
+    nln_mac P;
+    P.tol = t->p.tol;
+    P.rel_tol = t->p.rel_tol;
+    P.rel_tol0 = t->p.rel_tol0;
+    P.ptol_boost = t->p.ptol_boost;
+    P.bmax0 = 0.5 * t->side;  // mac->bmax0 = r0, cofm.c:66
+    P.p2cut = t->p.p2cut;
+    P.p4cut = t->p.p4cut;
+    P.box = t->p.box;
+    P.ewald_theta = t->p.ewald_theta;
+    return P;
+}
+
+// AREL critical radii of every cell (nln_cell_rcrit).
 static void compute_rcrit(nln_tree *t) {
-    const double rel = t->p.rel_tol, rel0 = t->p.rel_tol0;
-    const double boost = t->p.ptol_boost, bmax0 = 0.5 * t->side;  // mac->bmax0 = r0, cofm.c:66
-    const int p2 = t->p.p2cut, p4 = t->p.p4cut;
+    const nln_mac P = mac_of(t);
     const int64_t nc = (int64_t)t->cells.size();
 #pragma omp parallel for schedule(dynamic, 256)
     for (int64_t ci = 0; ci < nc; ci++) {
         Cell &c = t->cells[ci];
-        c.rc_m = c.rc_q = c.rc_h = 0.0;
-        if (c.B2 <= 0.0 || c.mass <= 0.0 || c.bmax <= 0.0)
-            continue;  // coincident bodies: every expansion is exact
-        const double b = c.bmax, m = c.mass, B2 = c.B2;
-        // larger cells get a tighter tolerance with ptol_boost (cofm.c:302)
-        const double ptol = t->p.tol / (1.0 + (boost > 0 && bmax0 > 0 ? boost * b / bmax0 : 0.0));
-        const double B3 = B2 * std::sqrt(B2 / m);  // lower bound, cofm.c:314
-        double a[10];
-        // monopole
-        double bh = 0.5 * b;
-        double rmax = bh + std::sqrt(bh * bh + std::sqrt(3.0 * B2 / ptol));
-        a[0] = 2 * B3; a[1] = -3 * B2; a[2] = 0; a[3] = ptol * b * b; a[4] = -2 * ptol * b;
-        a[5] = ptol;
-        double r_abs = newton_root(a, 5, rmax, 0.01 * rmax) + 0.01 * rmax;
-        double r_rel0 = 0.0, r_rel = INFINITY;
-        if (rel0 > 0) {
-            rmax = b + std::sqrt(3.0 / rel0 * B2 / m);
-            a[0] = 2 * B3; a[1] = -3 * B2 + rel0 * b * b * m; a[2] = -2 * rel0 * b * m;
-            a[3] = rel0 * m;
-            r_rel0 = newton_root(a, 3, rmax, 0.01 * rmax) + 0.01 * rmax;
-        }
-        if (rel > 0) {
-            rmax = b + std::sqrt(3.0 / rel * B2 / m);
-            a[0] = 2 * B3; a[1] = -3 * B2 + rel * b * b * m; a[2] = -2 * rel * b * m;
-            a[3] = rel * m;
-            r_rel = newton_root(a, 3, rmax, 0.01 * rmax) + 0.01 * rmax;
-        }
-        c.rc_m = std::max(std::min(r_abs, r_rel), r_rel0);
-        const double m_abs = r_abs, m_rel0 = r_rel0, m_rel = r_rel;
-        // quadrupole, cofm.c:442-485
-        if (p2 && c.count >= p2) {
-            const double B3q = b * B2, B4 = c.B4;  // upper bound, cofm.c:433
-            a[0] = 3 * B4; a[1] = -4 * B3q; a[2] = 0; a[3] = 0; a[4] = ptol * b * b;
-            a[5] = -2 * ptol * b; a[6] = ptol;
-            r_abs = newton_root(a, 6, m_abs, 0.01 * m_abs) + 0.01 * m_abs;
-            r_rel0 = 0.0;
-            r_rel = INFINITY;
-            if (rel0 > 0) {
-                a[0] = 3 * B4; a[1] = -4 * B3q; a[2] = rel0 * b * b * m; a[3] = -2 * rel0 * b * m;
-                a[4] = rel0 * m;
-                r_rel0 = newton_root(a, 4, m_rel0, 0.01 * m_rel0) + 0.01 * m_rel0;
-            }
-            if (rel > 0 && std::isfinite(m_rel)) {
-                a[0] = 3 * B4; a[1] = -4 * B3q; a[2] = rel * b * b * m; a[3] = -2 * rel * b * m;
-                a[4] = rel * m;
-                r_rel = newton_root(a, 4, m_rel, 0.01 * m_rel) + 0.01 * m_rel;
-            }
-            c.rc_q = std::max(std::min(r_abs, r_rel), r_rel0);
-        }
-        // order 4, cofm.c:489-505
-        if (p4 && c.count >= p4) {
-            const double B5 = b * c.B4, B6 = c.B6;
-            std::fill(a, a + 10, 0.0);
-            a[0] = 5 * B6; a[1] = -6 * B5; a[6] = ptol * b * b; a[7] = -2 * ptol * b; a[8] = ptol;
-            r_abs = newton_root(a, 8, m_abs, 0.001 * m_abs) + 0.001 * m_abs;
-            r_rel0 = 0.0;
-            r_rel = INFINITY;
-            if (rel0 > 0) {
-                std::fill(a, a + 10, 0.0);
-                a[0] = 5 * B6; a[1] = -6 * B5; a[4] = rel0 * b * b * m; a[5] = -2 * rel0 * b * m;
-                a[6] = rel0 * m;
-                r_rel0 = newton_root(a, 6, m_rel0, 0.001 * m_rel0) + 0.001 * m_rel0;
-            }
-            if (rel > 0 && std::isfinite(m_rel)) {
-                std::fill(a, a + 10, 0.0);
-                a[0] = 5 * B6; a[1] = -6 * B5; a[4] = rel * b * b * m; a[5] = -2 * rel * b * m;
-                a[6] = rel * m;
-                r_rel = newton_root(a, 6, m_rel, 0.001 * m_rel) + 0.001 * m_rel;
-            }
-            c.rc_h = std::max(std::min(r_abs, r_rel), r_rel0);
-        }
+        double rc[3];
+        nln_cell_rcrit(P, c.count, c.mass, c.bmax, c.B2, c.B4, c.B6, rc);
+        c.rc_m = rc[0];
+        c.rc_q = rc[1];
+        c.rc_h = rc[2];
     }
 }
 
@@ -429,6 +317,15 @@ static void collect_groups(nln_tree *t) {
         for (auto it = big.rbegin(); it != big.rend(); ++it) stack.push_back(*it);
     }
     std::sort(runs.begin(), runs.end(), [](const Run &a, const Run &b) { return a.first < b.first; });
+    // a leaf that cannot split further (coincident bodies at the deepest key
+    // level) can hold more than gmax bodies: its run becomes consecutive
+    // groups of gmax, the last one the remainder
+    std::vector<Run> pieces;
+    pieces.reserve(runs.size());
+    for (const Run &r : runs)
+        for (int32_t k = 0; k < r.count; k += gmax)
+            pieces.push_back(Run{r.first + k, std::min<int32_t>(gmax, r.count - k)});
+    runs.swap(pieces);
     t->groups.resize(runs.size());
 #pragma omp parallel for schedule(static)
     for (size_t g = 0; g < runs.size(); g++) {
@@ -560,128 +457,32 @@ struct GroupLists {
     int64_t nb = 0, nm = 0;
 };
 
-inline uint16_t shift_code(const int s[3]) {
-    return (uint16_t)((s[0] + 1) * 9 + (s[1] + 1) * 3 + (s[2] + 1));
-}
+// Host emitter of nln_walk_group: the group's lists as vectors.
+struct HostEmit {
+    GroupLists &L;
+    void p(uint32_t e, bool body) {
+        L.p.push_back(e);
+        if (body)
+            L.nb++;
+        else
+            L.nm++;
+    }
+    void q(uint32_t e) { L.q.push_back(e); }
+    void h(uint32_t e) { L.h.push_back(e); }
+    void c(uint32_t e) { L.c.push_back(e); }
+};
 
 }  // namespace
 
-// Distance from y to the nearest nonzero lattice vector of the periodic cube.
-// For y in the minimum-image cube (|y_k| <= L/2) that vector is a single
-// step along one axis: a step along two axes i, j is no nearer since
-// L^2 - 2 L |y_j| >= 0.  So the six axis steps suffice.
-static double lattice_gap(const double y[3], double box) {
-    double D2 = INFINITY;
-    for (int k = 0; k < 3; k++)
-        for (int a = -1; a <= 1; a += 2) {
-            const double dx = y[0] - (k == 0 ? a * box : 0.0), dy = y[1] - (k == 1 ? a * box : 0.0),
-                         dz = y[2] - (k == 2 ? a * box : 0.0);
-            D2 = std::min(D2, dx * dx + dy * dy + dz * dz);
-        }
-    return std::sqrt(D2);
-}
-
-// The walk of one sink group (nln/mac.c:1703-1840 semantics: a cell is
-// taken at the lowest order whose critical radius it clears, else opened;
-// a leaf that cannot be taken expands to its bodies).
-//
-// Periodic boxes also get the group's correction list.  The correction
-// needs every source in the same image as its Newtonian entry, but only
-// near the half-box does that image depend on the walk: a cell whose
-// bodies all lie strictly inside the group centre's minimum-image cube
-// (|y|_inf + bmax < L/2) has every descendant entry in that same image.
-// Such a cell enters the correction list whole, in place of its subtree's
-// entries, once bmax + group radius <= ewald_theta x its distance to the
-// correction's nearest singularity (the group's own image at a lattice
-// vector); everywhere else the correction list repeats the Newtonian
-// entries.  Stack entries carry that "covered" flag in bit 0.
+// One group's walk (nln_walk_group over the tree's walk records).
 static void walk_group(const nln_tree *t, const nln_group &G, GroupLists &L,
                        std::vector<int32_t> &stack) {
-    const double box = t->p.box;
-    const double theta = t->p.ewald_theta;
-    const int p2 = t->p.p2cut, p4 = t->p.p4cut;
-    const uint32_t nb = (uint32_t)t->n;
-    int64_t covered = 0;
-    stack.clear();
-    stack.push_back(0);
-    while (!stack.empty()) {
-        const int32_t top = stack.back();
-        stack.pop_back();
-        const int32_t ci = top >> 1;
-        bool ccov = (top & 1) != 0;
-        const Cell &c = t->cells[ci];
-        double y[3];
-        int s[3] = {0, 0, 0};
-        for (int d = 0; d < 3; d++) {
-            y[d] = c.cen[d] - G.cen[d];
-            if (box > 0) {
-                s[d] = -(int)std::nearbyint(y[d] / box);
-                y[d] += s[d] * box;
-            }
-        }
-        const double dist = std::sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
-        // Periodic: the cell is taken whole in the image nearest the group
-        // centre.  Every sink-body displacement it implies must stay inside
-        // the domain of the Ewald correction, |y_k| <= NLN_EWALD_REACH * box,
-        // where the correction is smooth; otherwise the cell is opened.
-        bool inside = true;
-        const uint16_t sc = shift_code(s);
-        if (box > 0) {
-            const double ym = std::max(std::fabs(y[0]), std::max(std::fabs(y[1]), std::fabs(y[2])));
-            inside = ym + c.bmax + G.radius <= NLN_EWALD_REACH * box;
-            if (!ccov && theta > 0 && c.count > 0 && ym + c.bmax < 0.5 * box * (1.0 - 1e-9) &&
-                c.bmax + G.radius <= theta * lattice_gap(y, box)) {
-                L.c.push_back((nb + (uint32_t)ci) | ((uint32_t)sc << NLN_IDX_BITS));
-                ccov = true;
-            }
-        }
-        const bool emit_c = box > 0 && !ccov;
-        const double dd = dist - G.radius;
-        if (inside && c.count > 0) {
-            const bool take = dd > c.rc_m + c.bmax || (p2 && c.count >= p2 && dd > c.rc_q + c.bmax) ||
-                              (p4 && c.count >= p4 && dd > c.rc_h + c.bmax);
-            if (take) {
-                if (dd > c.rc_m + c.bmax) {
-                    L.p.push_back((nb + (uint32_t)ci) | ((uint32_t)sc << NLN_IDX_BITS));
-                    L.nm++;
-                } else if (p2 && c.count >= p2 && dd > c.rc_q + c.bmax) {
-                    L.q.push_back((uint32_t)ci | ((uint32_t)sc << NLN_IDX_BITS));
-                } else {
-                    L.h.push_back((uint32_t)ci | ((uint32_t)sc << NLN_IDX_BITS));
-                }
-                if (emit_c)
-                    L.c.push_back((nb + (uint32_t)ci) | ((uint32_t)sc << NLN_IDX_BITS));
-                covered += c.count;
-                continue;
-            }
-        }
-        if (c.child >= 0) {
-            for (int k = c.nchild - 1; k >= 0; k--)
-                stack.push_back(((c.child + k) << 1) | (ccov ? 1 : 0));
-            continue;
-        }
-        // leaf: expand to bodies (nln/mac.c:1817-1832)
-        for (int32_t k = 0; k < c.count; k++) {
-            uint32_t e;
-            if (inside || box <= 0) {
-                e = (uint32_t)(c.first + k) | ((uint32_t)sc << NLN_IDX_BITS);
-            } else {
-                // a leaf reaching out of the correction's domain: each body its own image
-                const float *x = &t->spos[3 * (c.first + k)];
-                int sb[3];
-                for (int d = 0; d < 3; d++) sb[d] = -(int)std::nearbyint((x[d] - G.cen[d]) / box);
-                e = (uint32_t)(c.first + k) | ((uint32_t)shift_code(sb) << NLN_IDX_BITS);
-            }
-            L.p.push_back(e);
-            if (emit_c)
-                L.c.push_back(e);
-        }
-        L.nb += c.count;
-        covered += c.count;
-    }
-    if (covered != t->n) {
-        std::fprintf(stderr, "nln_tree_walk: group at %lld covers %lld of %lld bodies\n",
-                     (long long)G.first, (long long)covered, (long long)t->n);
+    HostEmit em{L};
+    const int rc = nln_walk_group(t->wcells.data(), t->spos.data(), t->n, G, mac_of(t),
+                                  stack.data(), (int)stack.size(), em);
+    if (rc) {
+        std::fprintf(stderr, "nln_tree_walk: group at %lld: %s\n", (long long)G.first,
+                     rc == -1 ? "does not cover every body exactly once" : "walk stack overflow");
         std::abort();
     }
 }
@@ -752,6 +553,23 @@ extern "C" int nln_tree_walk(nln_tree *t) {
     }
     omp_set_num_threads(nthreads_of(t->p));
     const int64_t ng = (int64_t)t->groups.size();
+    const int64_t ncell = (int64_t)t->cells.size();
+    t->wcells.resize(ncell);
+#pragma omp parallel for schedule(static)
+    for (int64_t ci = 0; ci < ncell; ci++) {
+        const Cell &c = t->cells[ci];
+        nln_wcell &w = t->wcells[ci];
+        for (int d = 0; d < 3; d++) w.cen[d] = c.cen[d];
+        w.bmax = c.bmax;
+        w.rc[0] = c.rc_m;
+        w.rc[1] = c.rc_q;
+        w.rc[2] = c.rc_h;
+        w.first = c.first;
+        w.count = c.count;
+        w.child = c.child;
+        w.nchild = c.nchild;
+        w.pad = 0;
+    }
     // Groups are walked in chunks.  Each chunk's lists are packed into one
     // exact-size segment per kind, and its per-group vectors are reused by
     // the next chunk, so the host holds about one copy of the lists (plus
@@ -770,8 +588,7 @@ extern "C" int nln_tree_walk(nln_tree *t) {
         const int64_t c1 = std::min(ng, c0 + chunk);
 #pragma omp parallel
         {
-            std::vector<int32_t> stack;
-            stack.reserve(1024);
+            std::vector<int32_t> stack(NLN_WALK_STACK);
 #pragma omp for schedule(dynamic, 8)
             for (int64_t g = c0; g < c1; g++) {
                 GroupLists &L = GL[g - c0];

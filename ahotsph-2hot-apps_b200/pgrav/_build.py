@@ -61,24 +61,42 @@ def cuda_headers():
 def build_host(force=False):
     os.makedirs(LIBDIR, exist_ok=True)
     srcs = host_sources()
-    deps = srcs + [os.path.join(INCLUDE, "nlnhost.h")]
+    deps = srcs + [os.path.join(INCLUDE, "nlnhost.h"), os.path.join(CSRC, "host", "tree_math.h")]
     if force or _newer(HOST_SO, deps):
-        _run([_cxx(), "-O3", "-mavx2", "-mfma", "-fPIC", "-fopenmp", "-std=c++17", "-shared",
-              "-I", INCLUDE, "-o", HOST_SO] + srcs)
+        # no contraction into FMAs: the tree arithmetic (csrc/host/tree_math.h) must round
+        # exactly as the GPU builder's does
+        _run([_cxx(), "-O3", "-mavx2", "-mfma", "-ffp-contract=off", "-fPIC", "-fopenmp",
+              "-std=c++17", "-shared", "-I", INCLUDE, "-o", HOST_SO] + srcs)
     return HOST_SO
+
+
+# Sources compiled on their own with these extra flags: the GPU tree builder
+# must not contract a * b + c into fused multiply-adds, so that its
+# arithmetic rounds exactly as the host builder's (csrc/host/tree_math.h).
+SEPARATE = {"build.cu": ["-fmad=false"]}
 
 
 def build_cuda(force=False, verbose_ptxas=False):
     os.makedirs(LIBDIR, exist_ok=True)
     srcs = cuda_sources()
-    deps = srcs + cuda_headers() + [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE)]
+    deps = srcs + cuda_headers() + [os.path.join(CSRC, "host", f)
+                                    for f in os.listdir(os.path.join(CSRC, "host"))] + \
+        [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE)]
     if force or _newer(CUDA_SO, deps):
-        cmd = [_nvcc()] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-shared",
-                                  "-Xcompiler", "-fPIC,-fopenmp", "-ccbin", _cxx(),
-                                  "-I", INCLUDE, "-I", CSRC, "-o", CUDA_SO]
+        base = [_nvcc()] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler",
+                                   "-fPIC,-fopenmp", "-ccbin", _cxx(), "-I", INCLUDE, "-I", CSRC]
         if verbose_ptxas:
-            cmd += ["-Xptxas", "-v"]
-        _run(cmd + srcs + ["-lcudart", "-lgomp"])
+            base += ["-Xptxas", "-v"]
+        objs = []
+        for src in srcs:
+            flags = SEPARATE.get(os.path.basename(src))
+            if flags is None:
+                continue
+            obj = os.path.join(LIBDIR, os.path.basename(src) + ".o")
+            _run(base + flags + ["-c", "-o", obj, src])
+            objs.append(obj)
+        rest = [x for x in srcs if os.path.basename(x) not in SEPARATE]
+        _run(base + ["-shared", "-o", CUDA_SO] + rest + objs + ["-lcudart", "-lgomp"])
     return CUDA_SO
 
 

@@ -28,6 +28,7 @@ EXPORTS = [
     "grav_plan_bodies", "grav_plan_integrate_CUDA", "grav_plan_step_CUDA",
     "grav_plan_adjoint_CUDA", "grav_plan_retune_CUDA", "grav_plan_get_tuning",
     "grav_groups_CUDA_phases", "grav_groups_release_CUDA", "grav_fp32_peak_CUDA",
+    "grav_plan_build_CUDA", "grav_plan_order", "grav_plan_build_phases", "grav_plan_problem",
 ]
 
 
@@ -105,6 +106,9 @@ def lib(record_errors=True):
             "grav_plan_adjoint_CUDA": ([vp, vp, vp, vp], i32),
             "grav_plan_retune_CUDA": ([vp, vp], i32), "grav_plan_get_tuning": ([vp, vp], i32),
             "grav_fp32_peak_CUDA": ([vp], i32),
+            "grav_plan_build_CUDA": ([vp, vp, i64, f64, f32, i32, vp, vp], i32),
+            "grav_plan_order": ([vp], vp), "grav_plan_build_phases": ([vp], None),
+            "grav_plan_problem": ([vp, vp], i32),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -130,8 +134,89 @@ def _p(a):
     return None if a is None else a.ctypes.data
 
 
+def d2h(ptr, dtype, count):
+    """A host copy of `count` items of `dtype` at device pointer `ptr`."""
+    from cuda.bindings import runtime as rt
+    out = np.empty(count, dtype=dtype)
+    if count:
+        err, = rt.cudaMemcpy(out.ctypes.data, ptr, out.nbytes,
+                             rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)
+        if int(err) != 0:
+            raise GravError(f"cudaMemcpy D2H failed: {err}")
+    return out
+
+
+def _host_array(ptr, dtype, count):
+    if not ptr or count == 0:
+        return np.zeros(0, dtype)
+    return np.ctypeslib.as_array((ctypes.c_char * (np.dtype(dtype).itemsize * count)).from_address(
+        ptr)).view(dtype).copy()
+
+
 class Plan:
-    """A device-resident batched problem (grav_groups_upload_CUDA)."""
+    """A device-resident batched problem (grav_groups_upload_CUDA, or built on
+    the GPU by Plan.build)."""
+
+    @classmethod
+    def build(cls, pos, mass, eps2, box=0.0, ewald=False, quad_phi_sign=1.0, tuning=None,
+              leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-3, rel_tol=0.0, rel_tol0=0.0,
+              ewald_theta=0.2, ptol_boost=0.0, bodies=None):
+        """The tree, moments, critical radii, sink groups and lists built on
+        the GPU (grav_plan_build_CUDA) from positions (n, 3) and masses (n,),
+        or from `bodies`, a CUDA float32 tensor (n, 4) of (x, y, z, m); the
+        parameters are host.Tree's, and the result is bit-identical to a plan
+        uploaded from host.Tree on the same bodies.  Results come in tree
+        order: plan.order() maps tree positions to input indices."""
+        import torch
+        from .host import Params
+        if bodies is None:
+            pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+            n = len(pos)
+            b = np.empty((n, 4), np.float32)
+            b[:, :3] = pos
+            b[:, 3] = np.broadcast_to(np.asarray(mass, np.float32), (n,))
+            bodies = torch.from_numpy(b).cuda()
+        n = int(bodies.shape[0])
+        params = Params(leaf_max, group_max, p2cut, p4cut, tol, rel_tol, rel_tol0, float(box), 0, 0,
+                        ewald_theta, ptol_boost)
+        tun = None
+        if tuning is not None:
+            tun = Tuning(*tuning) if not isinstance(tuning, Tuning) else tuning
+        h = ctypes.c_void_p()
+        check(lib().grav_plan_build_CUDA(ctypes.byref(params), bodies.data_ptr(), n, float(eps2),
+                                         float(quad_phi_sign), int(bool(ewald)),
+                                         ctypes.byref(tun) if tun is not None else None,
+                                         ctypes.byref(h)))
+        self = cls.__new__(cls)
+        self.tree = None
+        self.ewald = bool(ewald)
+        self._keep = [params]
+        self._h = h
+        self.n = n
+        return self
+
+    def order(self):
+        """Tree position -> input index (device-built plans), numpy int64."""
+        ptr = lib().grav_plan_order(self._h)
+        if not ptr:
+            raise GravError("the plan was not built on the device")
+        return d2h(ptr, np.int64, self.n)
+
+    def problem(self):
+        """Host copies of the plan's tables and lists (grav_plan_problem):
+        dict with points, qcells, hcells, groups, ptr (4 offset arrays) and
+        lists (P, Q, H, correction)."""
+        p = Problem()
+        check(lib().grav_plan_problem(self._h, ctypes.byref(p)))
+        n, nc, ng = p.nbodies, p.ncells, p.ngroups
+        ptr = [_host_array(x, np.int64, ng + 1) for x in (p.pptr, p.qptr, p.hptr, p.cptr)]
+        lists = [d2h(x, np.uint32, int(q[-1]) if len(q) else 0) if x else np.zeros(0, np.uint32)
+                 for x, q in zip((p.plist, p.qlist, p.hlist, p.clist), ptr)]
+        return {"points": d2h(p.points, np.float32, 4 * (n + nc)).reshape(-1, 4),
+                "qcells": d2h(p.qcells, QCELL_DTYPE, nc) if p.qcells else None,
+                "hcells": d2h(p.hcells, HCELL_DTYPE, nc) if p.hcells else None,
+                "groups": d2h(p.groups, GROUP_DTYPE, ng), "ptr": ptr, "lists": lists,
+                "ncells": nc}
 
     def __init__(self, tree, eps2, quad_phi_sign=1.0, ewald=False, tuning=None, plain=False):
         """plain: the plain FP32 kernels (absolute coordinates, plain sums)
@@ -456,6 +541,15 @@ def groups_eval_problem(pp, eps2, box, ewald=False):
     pp.problem.ewald = int(bool(ewald))
     check(lib().grav_groups_CUDA(ctypes.byref(pp.problem), pp.out.ctypes.data))
     return pp.out
+
+
+def build_phases():
+    """Seconds of this thread's last GPU tree build: sort, cells, moments and
+    tables, sink groups, walk, and the whole grav_plan_build_CUDA call."""
+    out = np.zeros(7, np.float64)
+    lib().grav_plan_build_phases(out.ctypes.data)
+    return dict(zip(("sort", "cells", "moments", "groups", "walk", "other", "total"),
+                    out.tolist()))
 
 
 def groups_phases():

@@ -31,6 +31,7 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "nlnhost.h"
 #include "nlnlists.h"
 
 #ifdef __cplusplus
@@ -242,6 +243,37 @@ int grav_plan_set_timing(grav_plan *plan, int on);
 /* Milliseconds of the last evaluation's kernels: order-4, quadrupole, point, finish (synchronising). */
 int grav_plan_kernel_ms(grav_plan *plan, float ms[4]);
 void grav_plan_free(grav_plan *plan);
+
+/*
+ * ---- the tree and lists built on the GPU ----
+ * grav_plan_build_CUDA: build the tree, FP64 moments, critical radii, sink
+ * groups and interaction lists of n bodies on the device and return a plan
+ * that evaluates them, ready for grav_groups_eval_CUDA, the time step and
+ * the adjoint (the tree links are set).  params are nlnhost.h's (emit_aosoa
+ * and nthreads are ignored); bodies: device, n x float4 (x, y, z, m) in any
+ * order, 16-byte aligned, not kept.  Bodies in [0, box)^3 when params->box >
+ * 0.  The tables and lists are bit-identical to nln_tree_build +
+ * nln_tree_walk on the same bodies (both builders share their arithmetic
+ * and sum in the same order without fused multiply-adds), so a plan built
+ * either way evaluates to the same forces.  Synchronises the device.
+ * grav_plan_order: device int64 per body, tree position -> input index
+ * (results are in tree order); NULL for plans uploaded from the host.
+ * grav_plan_build_phases: seconds of this thread's last build: sort, cells,
+ * moments and tables, sink groups, walk (both passes), plus the whole call.
+ */
+int grav_plan_build_CUDA(const nln_params *params, const float *bodies, int64_t n, double eps2,
+                         float quad_phi_sign, int ewald, const grav_tuning *tuning,
+                         grav_plan **plan);
+const int64_t *grav_plan_order(const grav_plan *plan);
+void grav_plan_build_phases(double seconds[7]);
+
+/*
+ * The plan's problem as it evaluates it: sizes and parameters, device
+ * pointers to its tables and lists (points, qcells, hcells, groups, plist,
+ * qlist, hlist, clist; NULL where absent) and host pointers to the list
+ * offsets (pptr, qptr, hptr, cptr), valid until grav_plan_free.
+ */
+int grav_plan_problem(const grav_plan *plan, grav_problem *out);
 
 /*
  * One-call end-to-end form: upload, evaluate, download, free.  acc_phi:

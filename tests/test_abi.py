@@ -60,8 +60,10 @@ def _compile_with_reference_header(tmp_path, our_header_text, first="ours"):
     from oracle import oracle as O
     inc = tmp_path / "inc"
     inc.mkdir(exist_ok=True)
+    for name in os.listdir(os.path.join(REPO, "include")):
+        if name.endswith(".h") and name != "gravcuda.h":
+            (inc / name).write_text(open(os.path.join(REPO, "include", name)).read())
     (inc / "gravcuda.h").write_text(our_header_text)
-    (inc / "nlnlists.h").write_text(open(os.path.join(REPO, "include", "nlnlists.h")).read())
     ours = '#include "gravcuda.h"\n'
     theirs = f'#define CUDA 1\n#include "{O.REF_NLN}/gravcuda.h"\n'
     src = tmp_path / "both.c"

@@ -137,3 +137,17 @@ def test_unpack_rejects_malformed_runs():
         O.unpack_runs([0, 1, 3], np.array([e, run(2), e], np.uint32))
     with pytest.raises(AssertionError, match="follows a run word"):
         O.unpack_runs([0, 3], np.array([e, run(2), run(1)], np.uint32))
+
+
+def test_coincident_bodies_split_into_small_groups():
+    """A leaf of coincident bodies cannot split: its run becomes consecutive
+    groups of at most group_max sinks, and the walk still covers every body."""
+    from pgrav import host
+    rng = np.random.default_rng(5)
+    pos = np.concatenate([rng.normal(0, 1, (3000, 3)), np.zeros((300, 3))]).astype(np.float32)
+    m = np.full(len(pos), 1.0 / len(pos), np.float32)
+    t = host.Tree(pos, m, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-4)
+    assert t.groups["count"].max() <= 32
+    assert t.groups["count"].sum() == t.n
+    first = t.groups["first"]
+    assert np.array_equal(first[1:], first[:-1] + t.groups["count"][:-1])
