@@ -1253,6 +1253,7 @@ namespace {
 // own index checks stand in for the upload-time list check.
 thread_local double t_phase[5];  // grav_groups_CUDA_phases
 thread_local double t_build = 0, t_build_phase[6] = {0, 0, 0, 0, 0, 0};  // grav_plan_build_phases
+thread_local double t_phase_be[4] = {0, 0, 0, 0};  // grav_build_eval_phases
 
 // The end-to-end call's device buffers come from a pool per device that
 // keeps freed memory reserved (until grav_groups_release_CUDA): mapping and
@@ -1309,6 +1310,7 @@ int upload_impl(const grav_problem *hp, const grav_tuning *tuning, grav_plan **p
     pl->hp = *hp;
     pl->plain = hp->precision == 1;
     if (adopt) {
+        pl->pool = adopt->pool;  // freed the way they were allocated
         // the plan owns every buffer of the device-built tree from here on,
         // failures included (grav_plan_free releases them)
         void *own[] = {adopt->points, adopt->qcells, adopt->hcells, adopt->groups,
@@ -1816,18 +1818,25 @@ int launch_moments(grav_plan *pl, const DevProblem &dp, cudaStream_t s, int per_
 // Placement of the periodic correction moments: ewald_side > 0 runs them on
 // a side stream beside the list kernels (k_ewald_side) in that many two-warp
 // blocks per SM, sharing the SMs with them; ewald_side = -k runs them
-// on the evaluation's stream between the list kernels and the finish pass,
-// with the SMs to themselves, in blocks of k warps (k = 1, 2 or 4) as many
-// as fit.  Automatic (0): the evaluation's stream, two-warp blocks.
+// (k_ewald_moments) on the evaluation's stream between the list kernels and
+// the finish pass, with the SMs to themselves, in blocks of k warps (k = 1,
+// 2 or 4) as many as fit.  Automatic (0): the side stream with 2 blocks per
+// SM while the correction list is short beside the order-4 lists, else the
+// evaluation's stream with two-warp blocks.  Measured on one B200: at 256^3
+// (MAC 1.5e-6; correction entries 1.2 % of the order-4 interactions) the
+// side stream takes 813 ms a step against 825 ms; where the moments take
+// half the order-4 kernel's time (128^3, MAC 1e-4) the side stream loses.
 int main_moments_warps(const grav_plan *pl) {
     const int k = -pl->tune.ewald_side;
     return (k == 1 || k == 2 || k == 4) ? k : 2;
 }
 
 int side_blocks(const grav_plan *pl) {
-    if (!pl->dp.ewald || !pl->side || !pl->ewm || pl->tune.ewald_side <= 0)
+    if (!pl->dp.ewald || !pl->side || !pl->ewm || pl->tune.ewald_side < 0)
         return 0;
-    return pl->tune.ewald_side;
+    if (pl->tune.ewald_side > 0)
+        return pl->tune.ewald_side;
+    return pl->ewald_entries < 0.015 * (double)pl->counts[3] ? 2 : 0;
 }
 
 // Fork: k_ewald_moments over dp's groups on the side stream, after the work
@@ -2044,18 +2053,19 @@ extern "C" void grav_plan_free(grav_plan *pl) {
     delete pl;
 }
 
-extern "C" int grav_plan_build_CUDA(const nln_params *params, const float *bodies, int64_t n,
-                                    double eps2, float quad_phi_sign, int ewald,
-                                    const grav_tuning *tuning, grav_plan **plan) {
-    if (!params || !bodies || !plan || n <= 0)
-        return gc::set_status(-1, "grav_plan_build_CUDA: bad arguments");
+namespace {
+// The device build and the plan that adopts it; buffers from the device's
+// pool (grav_groups_release_CUDA returns the memory it keeps reserved).
+int build_plan(const nln_params *params, const float4 *bodies, int64_t n, double eps2,
+               float quad_phi_sign, int ewald, const grav_tuning *tuning, grav_plan **plan) {
     *plan = nullptr;
-    if (((uintptr_t)bodies & 15u) != 0)
-        return gc::set_status(-1, "grav_plan_build_CUDA: bodies must be 16-byte aligned");
+    cudaMemPool_t pool = nullptr;
+    if (int rc = e2e_pool(&pool))
+        return rc;
     DevTree T;
     const double t0 = now_s();
-    if (int rc = gpu_tree_build(*params, reinterpret_cast<const float4 *>(bodies), n, 0, T)) {
-        dev_tree_free(T);
+    if (int rc = gpu_tree_build(*params, bodies, n, 0, T, pool)) {
+        dev_tree_free(T, pool);
         return rc;
     }
     grav_problem hp{};
@@ -2093,11 +2103,11 @@ extern "C" int grav_plan_build_CUDA(const nln_params *params, const float *bodie
     if (e == cudaSuccess)
         e = cudaMemcpy(level.data(), T.cell_level, nc * 4, cudaMemcpyDeviceToHost);
     void *links[] = {T.cell_first, T.cell_count, T.cell_child, T.cell_nchild, T.cell_level};
-    for (void *q : links) cudaFree(q);
+    for (void *q : links) cudaFreeAsync(q, 0);
     T.cell_first = nullptr;
     T.cell_count = T.cell_child = T.cell_nchild = T.cell_level = nullptr;
     if (e != cudaSuccess) {
-        dev_tree_free(T);
+        dev_tree_free(T, pool);
         return gc::cuda_status(e, "grav_plan_build_CUDA: tree links");
     }
     grav_plan *pl = nullptr;
@@ -2112,6 +2122,90 @@ extern "C" int grav_plan_build_CUDA(const nln_params *params, const float *bodie
     for (int k = 0; k < 6; k++) t_build_phase[k] = T.seconds[k];
     *plan = pl;
     return 0;
+}
+
+// out[order[i]] = in[i]: results from tree order back to the input order.
+__global__ void k_unorder(const float4 *__restrict__ in, const int64_t *__restrict__ order,
+                          int64_t n, float4 *out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const int64_t j = order[i];
+        if (j >= 0 && j < n)
+            out[j] = in[i];
+    }
+}
+}  // namespace
+
+extern "C" int grav_plan_build_CUDA(const nln_params *params, const float *bodies, int64_t n,
+                                    double eps2, float quad_phi_sign, int ewald,
+                                    const grav_tuning *tuning, grav_plan **plan) {
+    if (!params || !bodies || !plan || n <= 0)
+        return gc::set_status(-1, "grav_plan_build_CUDA: bad arguments");
+    *plan = nullptr;
+    if (((uintptr_t)bodies & 15u) != 0)
+        return gc::set_status(-1, "grav_plan_build_CUDA: bodies must be 16-byte aligned");
+    return build_plan(params, reinterpret_cast<const float4 *>(bodies), n, eps2, quad_phi_sign,
+                      ewald, tuning, plan);
+}
+
+extern "C" int grav_build_eval_CUDA(const nln_params *params, const float *bodies, int64_t n,
+                                    double eps2, float quad_phi_sign, int ewald,
+                                    float *acc_phi) {
+    if (!params || !bodies || !acc_phi || n <= 0)
+        return gc::set_status(-1, "grav_build_eval_CUDA: bad arguments");
+    const double t_start = now_s();
+    cudaMemPool_t pool = nullptr;
+    if (int rc = e2e_pool(&pool))
+        return rc;
+    float4 *dev = nullptr, *out = nullptr;
+    const size_t bytes = (size_t)n * sizeof(float4);
+    GC_CHECK(cudaMallocFromPoolAsync((void **)&dev, bytes, pool, 0));
+    cudaError_t e = cudaMallocFromPoolAsync((void **)&out, bytes, pool, 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dev, bodies, bytes, cudaMemcpyHostToDevice, 0);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(dev, 0);
+        if (out)
+            cudaFreeAsync(out, 0);
+        return gc::cuda_status(e, "grav_build_eval_CUDA: bodies");
+    }
+    const double t_h2d = now_s();
+    grav_plan *pl = nullptr;
+    int rc = build_plan(params, dev, n, eps2, quad_phi_sign, ewald, nullptr, &pl);
+    const double t_built = now_s();
+    if (!rc)
+        rc = grav_groups_eval_CUDA(pl, nullptr);
+    if (!rc) {
+        k_unorder<<<(unsigned)((n + 255) / 256), 256>>>(pl->dp.out, pl->order, n, out);
+        e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = cudaMemcpy(acc_phi, out, bytes, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess)
+            rc = gc::cuda_status(e, "grav_build_eval_CUDA: results");
+    }
+    const double t_eval = now_s();
+    if (!rc) {
+        unsigned h = 0;
+        e = cudaMemcpy(&h, pl->dp.err, sizeof(h), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess)
+            rc = gc::cuda_status(e, "grav_build_eval_CUDA: error word");
+        else if (h)
+            rc = gc::set_status(-2, "grav_build_eval_CUDA: device error word 0x%x", h);
+    }
+    if (pl)
+        grav_plan_free(pl);
+    cudaFreeAsync(dev, 0);
+    cudaFreeAsync(out, 0);
+    cudaStreamSynchronize(0);
+    t_phase_be[0] = t_h2d - t_start;
+    t_phase_be[1] = t_built - t_h2d;
+    t_phase_be[2] = t_eval - t_built;
+    t_phase_be[3] = now_s() - t_eval;
+    return rc;
+}
+
+extern "C" void grav_build_eval_phases(double seconds[4]) {
+    for (int k = 0; k < 4; k++) seconds[k] = t_phase_be[k];
 }
 
 extern "C" const int64_t *grav_plan_order(const grav_plan *pl) { return pl ? pl->order : nullptr; }

@@ -56,16 +56,27 @@ unsigned grid_of(int64_t n, int threads = kThreads) {
     return (unsigned)std::max<int64_t>(1, (n + threads - 1) / threads);
 }
 
-// device buffers freed at the end of the build unless released to the caller
+// device buffers freed at the end of the build unless released to the
+// caller; from a memory pool (stream-ordered on st) when one is given
 struct Bufs {
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t st = nullptr;
     std::vector<void *> held;
     ~Bufs() {
-        for (void *p : held) cudaFree(p);
+        for (void *p : held) free_one(p);
+    }
+    void free_one(void *p) {
+        if (pool)
+            cudaFreeAsync(p, st);
+        else
+            cudaFree(p);
     }
     template <typename T>
     cudaError_t get(T **p, size_t n) {
         *p = nullptr;
-        cudaError_t e = cudaMalloc((void **)p, std::max<size_t>(1, n) * sizeof(T));
+        const size_t bytes = std::max<size_t>(1, n) * sizeof(T);
+        cudaError_t e = pool ? cudaMallocFromPoolAsync((void **)p, bytes, pool, st)
+                             : cudaMalloc((void **)p, bytes);
         if (e == cudaSuccess)
             held.push_back(*p);
         return e;
@@ -80,7 +91,7 @@ struct Bufs {
     void drop(T *p) {
         auto it = std::find(held.begin(), held.end(), (void *)p);
         if (it != held.end()) {
-            cudaFree(*it);
+            free_one(*it);
             held.erase(it);
         }
     }
@@ -562,18 +573,22 @@ int exclusive_scan(Bufs &B, const T *in, T *out, int64_t n, cudaStream_t st) {
 
 }  // namespace
 
-void dev_tree_free(DevTree &t) {
+void dev_tree_free(DevTree &t, cudaMemPool_t pool) {
     void *ps[] = {t.points, t.qcells, t.hcells, t.groups, t.list[0], t.list[1], t.list[2],
                   t.list[3], t.order, t.cell_first, t.cell_count, t.cell_child, t.cell_nchild,
                   t.cell_level};
     for (void *p : ps)
-        if (p)
-            cudaFree(p);
+        if (p) {
+            if (pool)
+                cudaFreeAsync(p, 0);
+            else
+                cudaFree(p);
+        }
     t = DevTree{};
 }
 
 int gpu_tree_build(const nln_params &p, const float4 *bodies, int64_t n, cudaStream_t st,
-                   DevTree &out) {
+                   DevTree &out, cudaMemPool_t pool) {
     out = DevTree{};
     if (!bodies || n <= 0)
         return gc::set_status(-1, "GPU tree build: no bodies");
@@ -584,6 +599,9 @@ int gpu_tree_build(const nln_params &p, const float4 *bodies, int64_t n, cudaStr
     if (n + 1 >= (int64_t)NLN_IDX_MASK || n >= (int64_t)INT32_MAX)
         return gc::set_status(-1, "GPU tree build: too many bodies for 27-bit list indices");
     Bufs B;
+    B.pool = pool;
+    B.st = st;
+    out.pool = pool;
     double t0 = now_s();
     // ---- bounding cube (the host arithmetic of nln_tree_build)
     const unsigned bb = 592;

@@ -30,6 +30,7 @@ struct DevTree {
     std::vector<nln_group> groups_h;
     std::vector<int64_t> ptr_h[4];  // ngroups + 1 list offsets per kind
     double seconds[6] = {0, 0, 0, 0, 0, 0};  // sort, cells, moments, groups, walk, copy-back
+    cudaMemPool_t pool = nullptr;   // the pool the buffers came from (cudaFreeAsync them)
 };
 
 // Build the tree, moments, critical radii, sink groups and interaction
@@ -37,6 +38,9 @@ struct DevTree {
 // semantics and arithmetic of nlnhost.h's nln_tree_build + nln_tree_walk
 // (bit-identical results); enqueued on st and synchronised.  Returns 0, -1
 // for bad arguments or positions (message recorded), or a CUDA status.
+// pool: when set, every device buffer comes from it (stream-ordered on st)
+// and is returned to it; the tree's buffers must then be freed with
+// cudaFreeAsync.
 int gpu_tree_build(const nln_params &p, const float4 *bodies, int64_t n, cudaStream_t st,
-                   DevTree &out);
-void dev_tree_free(DevTree &t);
+                   DevTree &out, cudaMemPool_t pool = nullptr);
+void dev_tree_free(DevTree &t, cudaMemPool_t pool = nullptr);

@@ -2,20 +2,19 @@
 hand-written adjoint (grav_plan_adjoint_CUDA), and a leapfrog integrator
 that backpropagates through KDK steps with step-level checkpointing.
 
-The forward builds the tree and the interaction lists on the host from the
-current positions and evaluates them on the GPU; the backward rebuilds the
-same (deterministic) tree from the saved inputs, holds those lists fixed
+The forward builds the tree and the interaction lists on the GPU from the
+current positions (grav_plan_build_CUDA) and evaluates them; the backward
+rebuilds the same (deterministic) tree from the saved inputs, holds those lists fixed
 (the tree is piecewise constant in the positions) and returns dL/dx and
 dL/dm for any loss whose gradient with respect to the outputs
 (accelerations, potentials) autograd supplies.  Only the inputs are saved,
 so checkpointed segments keep no device tables alive.  Isolated systems
 with monopole and quadrupole cells (p4cut = 0).
 """
-import numpy as np
 import torch
 
 from . import gravcuda as gc
-from . import host
+from .step import memcpy_d2d
 
 
 class TreeGravity(torch.autograd.Function):
@@ -23,12 +22,15 @@ class TreeGravity(torch.autograd.Function):
 
     @staticmethod
     def _plan(pos, mass, eps2, kw):
-        p = pos.detach().to("cpu", torch.float32).numpy()
-        m = mass.detach().to("cpu", torch.float32).numpy()
-        tree = host.Tree(p, m, **kw)
-        plan = gc.Plan(tree, float(eps2))
-        plan.set_tree(tree)
-        return tree, plan
+        """The plan built on the GPU and tree position -> input index (device)."""
+        n = pos.shape[0]
+        bodies = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+        bodies[:, :3] = pos.detach().to("cuda", torch.float32)
+        bodies[:, 3] = mass.detach().to("cuda", torch.float32)
+        torch.cuda.synchronize()
+        plan = gc.Plan.build(None, None, float(eps2), bodies=bodies, **kw)
+        order = torch.from_numpy(plan.order()).cuda()
+        return order, plan
 
     @staticmethod
     def forward(ctx, pos, mass, eps2, tree_kw):
@@ -36,11 +38,13 @@ class TreeGravity(torch.autograd.Function):
         kw.setdefault("p4cut", 0)
         if kw["p4cut"]:
             raise ValueError("the adjoint covers monopole and quadrupole cells (p4cut = 0)")
-        tree, plan = TreeGravity._plan(pos, mass, eps2, kw)
+        order, plan = TreeGravity._plan(pos, mass, eps2, kw)
         plan.eval()
-        out_t = torch.from_numpy(plan.download())
+        n = pos.shape[0]
+        out_t = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        memcpy_d2d(out_t.data_ptr(), plan.output_ptr(), n * 16)
         plan.free()
-        order = torch.from_numpy(tree.order)
         out = torch.empty_like(out_t)
         out[order] = out_t
         ctx.save_for_backward(pos, mass)
@@ -51,19 +55,18 @@ class TreeGravity(torch.autograd.Function):
     @staticmethod
     def backward(ctx, gacc, gphi):
         pos, mass = ctx.saved_tensors
-        tree, plan = TreeGravity._plan(pos, mass, ctx.eps2, ctx.kw)
-        n = tree.n
-        order = torch.from_numpy(tree.order)
-        wu = torch.zeros((n, 4), dtype=torch.float32)
+        order, plan = TreeGravity._plan(pos, mass, ctx.eps2, ctx.kw)
+        n = pos.shape[0]
+        wu = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
         if gacc is not None:
-            wu[:, :3] = gacc.detach().to("cpu", torch.float32)[order]
+            wu[:, :3] = gacc.detach().to("cuda", torch.float32)[order]
         if gphi is not None:
-            wu[:, 3] = gphi.detach().to("cpu", torch.float32)[order]
-        wu = wu.cuda()
+            wu[:, 3] = gphi.detach().to("cuda", torch.float32)[order]
         grad_t = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
         plan.adjoint(wu.data_ptr(), grad_t.data_ptr(), torch.cuda.current_stream().cuda_stream)
         grad = torch.empty_like(grad_t)
-        grad[order.cuda()] = grad_t
+        grad[order] = grad_t
         torch.cuda.current_stream().synchronize()
         plan.free()
         dev = gacc.device if gacc is not None else gphi.device

@@ -38,7 +38,7 @@ def _scaled(base, s):
 
 
 def autotune(plan, reps=3, shapes=((8, 0), (4, 0), (8, 1), (8, 2), (4, 2), (4, 4)),
-             scales=(0.25, 0.5, 1.0, 2.0, 4.0), sides=(-1, -2, -4, 2, 4), cache=None, key=None):
+             scales=(0.25, 0.5, 1.0, 2.0, 4.0), sides=(-2, -4, 2, 3), cache=None, key=None):
     """Tune `plan` in place.  Returns (best gc.Tuning, list of trials).  With
     `cache` (a JSON file path) and `key`, a stored result is applied without
     a search, and a new one is stored."""

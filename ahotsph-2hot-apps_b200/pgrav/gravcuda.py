@@ -29,6 +29,7 @@ EXPORTS = [
     "grav_plan_adjoint_CUDA", "grav_plan_retune_CUDA", "grav_plan_get_tuning",
     "grav_groups_CUDA_phases", "grav_groups_release_CUDA", "grav_fp32_peak_CUDA",
     "grav_plan_build_CUDA", "grav_plan_order", "grav_plan_build_phases", "grav_plan_problem",
+    "grav_build_eval_CUDA", "grav_build_eval_phases",
 ]
 
 
@@ -109,6 +110,8 @@ def lib(record_errors=True):
             "grav_plan_build_CUDA": ([vp, vp, i64, f64, f32, i32, vp, vp], i32),
             "grav_plan_order": ([vp], vp), "grav_plan_build_phases": ([vp], None),
             "grav_plan_problem": ([vp, vp], i32),
+            "grav_build_eval_CUDA": ([vp, vp, i64, f64, f32, i32, vp], i32),
+            "grav_build_eval_phases": ([vp], None),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -541,6 +544,30 @@ def groups_eval_problem(pp, eps2, box, ewald=False):
     pp.problem.ewald = int(bool(ewald))
     check(lib().grav_groups_CUDA(ctypes.byref(pp.problem), pp.out.ctypes.data))
     return pp.out
+
+
+def build_eval(bodies, eps2, box=0.0, ewald=False, quad_phi_sign=1.0, out=None, leaf_max=16,
+               group_max=32, p2cut=7, p4cut=20, tol=1e-3, rel_tol=0.0, rel_tol0=0.0,
+               ewald_theta=0.2, ptol_boost=0.0):
+    """grav_build_eval_CUDA: host bodies (n, 4) float32 (x, y, z, m) to host
+    (ax, ay, az, phi) (n, 4) in the same order: copy, GPU tree build,
+    evaluation and copy back in one call.  out: an (n, 4) float32 array to
+    fill (page-locked memory copies fastest)."""
+    from .host import Params
+    b = np.ascontiguousarray(bodies, np.float32).reshape(-1, 4)
+    n = len(b)
+    out = np.empty((n, 4), np.float32) if out is None else out
+    params = Params(leaf_max, group_max, p2cut, p4cut, tol, rel_tol, rel_tol0, float(box), 0, 0,
+                    ewald_theta, ptol_boost)
+    check(lib().grav_build_eval_CUDA(ctypes.byref(params), b.ctypes.data, n, float(eps2),
+                                     float(quad_phi_sign), int(bool(ewald)), out.ctypes.data))
+    return out
+
+
+def build_eval_phases():
+    out = np.zeros(4, np.float64)
+    lib().grav_build_eval_phases(out.ctypes.data)
+    return dict(zip(("h2d", "build", "eval_d2h", "release"), out.tolist()))
 
 
 def build_phases():

@@ -1,10 +1,12 @@
 """Time stepping on the device: the KDK integrator of nln/integrate.c:16-59
 (Integrate) around the batched force evaluation.
 
-The host builds the tree and the interaction lists every ``rebuild``
-steps.  Between rebuilds every step runs on the GPU as evaluate, integrate
-(kick by dtv, drift by dt) and refit of the cell tables, optionally replayed
-from one captured CUDA graph (grav_plan_step_CUDA).  Velocities lag the
+The tree and the interaction lists are rebuilt every ``rebuild`` steps,
+on the GPU from the bodies already there (grav_plan_build_CUDA; gpu_build,
+the default) or on the host (nlnhost.h, bit-identical lists).  Between
+rebuilds every step runs on the GPU as evaluate, integrate (kick by dtv,
+drift by dt) and refit of the cell tables, optionally replayed from one
+captured CUDA graph (grav_plan_step_CUDA).  Velocities lag the
 positions by half a step after the first kick (dtv = dt/2 once, then dt),
 and the energies of each step are those of Integrate: KE of the velocity
 synchronised to the positions' time, PE = 1/2 sum m phi (G = 1).
@@ -29,6 +31,13 @@ def memcpy_d2h(dst_array, src_ptr):
     return dst_array
 
 
+def memcpy_d2d(dst_ptr, src_ptr, nbytes):
+    rt = _rt()
+    err, = rt.cudaMemcpy(dst_ptr, src_ptr, nbytes, rt.cudaMemcpyKind.cudaMemcpyDeviceToDevice)
+    if int(err) != 0:
+        raise gc.GravError(f"cudaMemcpy D2D failed: {err}")
+
+
 def memcpy_h2d(dst_ptr, src_array):
     rt = _rt()
     src = np.ascontiguousarray(src_array)
@@ -48,7 +57,7 @@ class Stepper:
     """
 
     def __init__(self, pos, vel, mass, eps2, box=0.0, ewald=None, rebuild=8, graph=True,
-                 tree_kw=None):
+                 tree_kw=None, gpu_build=True):
         import torch
         self.torch = torch
         self.pos = np.array(pos, np.float32).reshape(-1, 3)
@@ -61,6 +70,9 @@ class Stepper:
         self.rebuild = max(1, int(rebuild))
         self.graph = bool(graph)
         self.tree_kw = dict(tree_kw or {})
+        self.gpu_build = bool(gpu_build)
+        self.orig = None  # GPU rebuilds: tree position -> original body index (device int64)
+        self.build_s = []  # seconds of every rebuild
         self.tpos = 0.0
         self.tvel = 0.0
         self.nsteps = 0
@@ -74,8 +86,52 @@ class Stepper:
         self.tree = None
         self._build()
 
-    # -- host rebuild: tree and lists from the current positions
+    # -- rebuild: tree and lists from the current positions
     def _build(self):
+        import time
+        t0 = time.perf_counter()
+        if self.gpu_build:
+            self._build_gpu()
+        else:
+            self._build_host()
+        self.torch.cuda.synchronize()
+        self.build_s.append(time.perf_counter() - t0)
+
+    # On the GPU: the bodies and velocities stay on the device.  They go to
+    # the builder in the original order, as the host rebuild hands them over
+    # (the key sort breaks ties by input index), so both rebuilds make the
+    # same tree; then into the new tree's order.
+    def _build_gpu(self):
+        torch = self.torch
+        n = self.n
+        if self.plan is None:
+            bodies = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+            bodies[:, :3] = torch.from_numpy(self.pos).cuda()
+            bodies[:, 3] = torch.from_numpy(self.mass).cuda()
+            vel = torch.from_numpy(self.vel).cuda()
+        else:
+            torch.cuda.synchronize()
+            tree_bodies = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+            memcpy_d2d(tree_bodies.data_ptr(), self.plan.bodies_ptr(), n * 16)
+            bodies = torch.empty_like(tree_bodies)
+            bodies[self.orig] = tree_bodies
+            vel = torch.empty((n, 3), dtype=torch.float32, device="cuda")
+            vel[self.orig] = self.dvel[:, :3]
+            self.plan.free()
+            self.plan = None
+        if self.box > 0:
+            x = torch.remainder(bodies[:, :3], self.box)
+            x[x >= self.box] = 0.0
+            bodies[:, :3] = x
+        self.plan = gc.Plan.build(None, None, self.eps2, box=self.box, ewald=self.ewald,
+                                  bodies=bodies, **self.tree_kw)
+        order = torch.from_numpy(self.plan.order()).cuda()
+        self.dvel = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+        self.dvel[:, :3] = vel[order]
+        self.orig = order
+
+    # On the host: tree and lists from the host copy of the positions.
+    def _build_host(self):
         torch = self.torch
         if self.plan is not None:
             self._pull()
@@ -96,7 +152,7 @@ class Stepper:
     def _pull(self):
         self.torch.cuda.synchronize()
         body = memcpy_d2h(np.empty((self.n, 4), np.float32), self.plan.bodies_ptr())
-        order = self.tree.order
+        order = self.orig.cpu().numpy() if self.gpu_build else self.tree.order
         self.pos[order] = body[:, :3]
         self.vel[order] = self.dvel.cpu().numpy()[:, :3]
 

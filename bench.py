@@ -306,12 +306,16 @@ def kdk_run(w, pos, m, eps2, box, tol, nsteps, dt, rebuild):
     st.run(nsteps, dt)
     wall = time.perf_counter() - t0
     h = st.history
+    builds = list(st.build_s)
     st.free()
     e = np.array([r["e"] for r in h])
     pe = np.array([r["pe"] for r in h])
     ms = np.array([r["ms"] for r in h])
     steady = ms[[k for k in range(len(ms)) if k % rebuild != 0]] if len(ms) > 1 else ms
     return {"steps": nsteps, "dt": dt, "rebuild_every": rebuild, "graph": True,
+            "rebuilds": "tree, moments, critical radii, groups and lists rebuilt on the GPU "
+                        "from the bodies on the device (grav_plan_build_CUDA)",
+            "rebuild_s": builds,
             "device_ms_per_step_median": float(np.median(steady)),
             "device_ms_first_step_after_rebuild_median": float(np.median(ms[::rebuild])),
             "wall_s": wall, "energy_first": float(e[0]), "energy_last": float(e[-1]),
@@ -598,7 +602,41 @@ def config_adjoint(args, stream):
                                  "meets_target": bool(np.sqrt(np.mean(exd ** 2)) <= 1e-3 and
                                                       np.sqrt(np.mean(emd ** 2)) <= 1e-3)}
     res["leapfrog"] = leapfrog_check(args)
+    res["leapfrog_2p20"] = leapfrog_time(n, eps2, tol)
     return res
+
+
+def leapfrog_time(n, eps2, tol, nsteps=16, every=4, dt=1e-3):
+    """Forward and backward through 16 leapfrog KDK steps (dt = 1e-3) of the
+    Plummer N = n system, checkpointed every 4 steps; every force
+    evaluation builds its tree on the GPU (as the autograd function does)."""
+    import torch
+    from pgrav import autograd as AG, ics
+    pos, m = ics.plummer(n, seed=123)
+    rng = np.random.default_rng(11)
+    vel = rng.normal(0, 0.2, (n, 3)).astype(np.float32)
+    tgt = torch.tensor(rng.normal(size=(n, 3)), dtype=torch.float32, device="cuda")
+    kw = dict(tol=tol, p2cut=7, p4cut=0, leaf_max=16, group_max=32)
+    x0 = torch.tensor(pos, device="cuda", requires_grad=True)
+    v0 = torch.tensor(vel, device="cuda", requires_grad=True)
+    mm = torch.tensor(m, device="cuda", requires_grad=True)
+    torch.cuda.reset_peak_memory_stats()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    x, v = AG.leapfrog(x0, v0, mm, eps2, dt, nsteps, checkpoint_every=every, **kw)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    ((x * tgt).sum() + (v * tgt).sum()).backward()
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    g = x0.grad
+    return {"n_bodies": n, "steps": nsteps, "dt": dt, "checkpoint_every": every, "mac_tol": tol,
+            "forward_s": t1 - t0, "backward_s": t2 - t1,
+            "force_evaluations": 2 * nsteps * 3,
+            "peak_torch_memory_gb": torch.cuda.max_memory_allocated() / 1e9,
+            "grad_finite": bool(torch.isfinite(g).all().item()),
+            "note": "wall clock; each force evaluation (forward, recomputation, backward) builds "
+                    "its tree and lists on the GPU"}
 
 
 def leapfrog_check(args, n=4096, nsteps=16, every=4, dt=1e-3, ncoords=4):
@@ -668,8 +706,8 @@ def leapfrog_check(args, n=4096, nsteps=16, every=4, dt=1e-3, ncoords=4):
             "checkpointed_vs_plain_max_rel": same, "fd_coordinates": ncoords, "fd_h": h,
             "fd_max_rel_err": err, "bar": 1e-3,
             "meets_target": bool(same <= 1e-5 and err <= 1e-3),
-            "note": "host tree rebuilt at every force evaluation (as the autograd function "
-                    "does), which bounds the size timed here"}
+            "note": "the FP64 differences rebuild the base trajectory's trees on the host "
+                    "(nlnhost.h, bit-identical to the GPU builder's the autograd function uses)"}
 
 
 def run_reference(args, w, rank, world):
@@ -734,7 +772,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="box256", choices=list(WORKLOADS))
     ap.add_argument("--tol", type=float, default=0.0)
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=3,
+                    help="end-to-end calls from positions (GPU tree build + evaluation)")
+    ap.add_argument("--e2e-lists-steps", type=int, default=2,
+                    help="end-to-end calls from lists built on the host (their transport)")
     ap.add_argument("--e2e-plain-lists", action="store_true",
                     help="end-to-end leg: copy the plain lists instead of the run-packed ones")
     ap.add_argument("--e2e-lists-in-host", action="store_true",
@@ -901,6 +942,7 @@ def main():
                "target_rms": 1e-4, "meets_target": bool(np.sqrt(np.mean(e * e)) <= 1e-4),
                "oracle": "FP64 direct sum" + (" with Ewald images" if box > 0 else "")}
     launches = plan.launches()
+    out_plan = plan.download() if rank == 0 else None
     batch_kdk = None
     if w["kind"] == "batch" and rank == 0:
         # the graph-captured KDK step of the batch (evaluate, integrate, refit)
@@ -923,11 +965,46 @@ def main():
                      "systems": int(len(tree.body_offsets) - 1)}
     plan.free()   # the end-to-end leg uploads its own copy
 
-    # ---- end to end through the C ABI with host buffers (pinned)
+    # ---- end to end: positions in host memory to forces in host memory in one
+    # call (grav_build_eval_CUDA): bodies to the device, tree, moments, critical
+    # radii, sink groups and lists built there, evaluation, results back in the
+    # bodies' order
     e2e = None
+    if args.e2e_steps > 0 and w["kind"] != "batch":
+        import torch as _t
+        nb = len(pos)
+        bbuf = _t.empty((nb, 4), dtype=_t.float32, pin_memory=True).numpy()
+        bbuf[:, :3] = pos
+        bbuf[:, 3] = m
+        obuf = _t.empty((nb, 4), dtype=_t.float32, pin_memory=True).numpy()
+        kw = dict(leaf_max=16, group_max=32, p2cut=w["p2cut"], p4cut=w["p4cut"],
+                  tol=args.tol or w["tol"])
+        ew = w["ewald"] and box > 0
+        gc.build_eval(bbuf, eps2, box=box, ewald=ew, out=obuf, **kw)  # warm-up
+        walls, phases = [], []
+        for _ in range(args.e2e_steps):
+            ta = time.perf_counter()
+            gc.build_eval(bbuf, eps2, box=box, ewald=ew, out=obuf, **kw)
+            walls.append(time.perf_counter() - ta)
+            phases.append(gc.build_eval_phases())
+        e2e_s = float(np.median(walls))
+        mid = int(np.argsort(walls)[len(walls) // 2])
+        same = bool(out_plan is not None and np.array_equal(obuf[tree.order], out_plan))
+        e2e = {"value": inter * world / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(bbuf.nbytes), "d2h_bytes_per_step": int(obuf.nbytes),
+               "ms_per_step": e2e_s * 1e3, "steps": args.e2e_steps,
+               "timing": "wall clock around grav_build_eval_CUDA: bodies (page-locked) to the "
+                         "device, tree + moments + critical radii + groups + MAC walk on the GPU, "
+                         "evaluation, (ax, ay, az, phi) back in the input order",
+               "walls_s": walls, "phases_s": phases[mid],
+               "equals_plan_output": same}
+        gc.lib().grav_groups_release_CUDA()
+
+    # ---- end to end from lists built on the host: the lists' transport
+    e2e_lists = None
     host = out = None
     pack_s = None
-    if args.e2e_steps > 0:
+    if args.e2e_lists_steps > 0:
         packed = not (args.e2e_plain_lists or args.e2e_lists_in_host)
         if packed:
             tp = time.perf_counter()
@@ -938,7 +1015,7 @@ def main():
         torch.cuda.synchronize()
         gc.groups_eval_problem(host, eps2, box, ewald=w["ewald"] and box > 0)  # warm-up
         walls, phases = [], []
-        for _ in range(args.e2e_steps):
+        for _ in range(args.e2e_lists_steps):
             ta = time.perf_counter()
             gc.groups_eval_problem(host, eps2, box, ewald=w["ewald"] and box > 0)
             torch.cuda.synchronize()
@@ -946,9 +1023,9 @@ def main():
             phases.append(gc.groups_phases())
         e2e_s = float(np.median(walls))
         mid = int(np.argsort(walls)[len(walls) // 2])
-        e2e = {"value": inter * world / e2e_s, "unit": UNIT,
+        e2e_lists = {"value": inter * world / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(host.h2d_bytes), "d2h_bytes_per_step": int(out.nbytes),
-               "ms_per_step": e2e_s * 1e3, "steps": args.e2e_steps,
+               "ms_per_step": e2e_s * 1e3, "steps": args.e2e_lists_steps,
                "timing": "wall clock around grav_groups_CUDA (upload, evaluate, download)",
                "walls_s": walls, "phases_s": phases[mid],
                "lists": ("read by the kernels in place from page-locked host memory over PCIe "
@@ -1013,7 +1090,8 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32 (FP64 centres, compensated sums)", "data": "synthetic (seeded)",
                 "config": cfg, "gpu_launches": launches * args.steps,
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "e2e_lists": e2e_lists,
+                "clocks": clocks,
                 "accuracy": acc,
                 "host_setup_s": {"ics": t1 - t0, "tree_walk": t2 - t1, "upload": t3 - t2}}
         if dropin:

@@ -208,8 +208,9 @@ typedef struct grav_tuning {
                                    side stream beside the list kernels, in this many two-warp
                                    blocks per SM; -k (k = 1, 2, 4): on the evaluation's stream
                                    between the list kernels and the finish pass, with the SMs to
-                                   themselves, in blocks of k warps; 0: automatic (-2).  The
-                                   results are the same either way. */
+                                   themselves, in blocks of k warps; 0: automatic (2 while the
+                                   correction list is under 1.5 % of the order-4 interactions,
+                                   else -2).  The results are the same either way. */
 } grav_tuning;
 
 /*
@@ -266,6 +267,20 @@ int grav_plan_build_CUDA(const nln_params *params, const float *bodies, int64_t 
                          grav_plan **plan);
 const int64_t *grav_plan_order(const grav_plan *plan);
 void grav_plan_build_phases(double seconds[7]);
+
+/*
+ * One call from positions to forces: copy the bodies (host, n x float4
+ * (x, y, z, m), any order; page-locked memory copies fastest) to the
+ * device, build the tree and lists there (grav_plan_build_CUDA), evaluate,
+ * and copy (ax, ay, az, phi) per body back to acc_phi (host, n x float4) in
+ * the bodies' own order.  Device buffers come from the memory pool of
+ * grav_groups_CUDA (kept reserved until grav_groups_release_CUDA).
+ * grav_build_eval_phases: seconds of this thread's last call: bodies to the
+ * device, build, evaluation and results back, release.
+ */
+int grav_build_eval_CUDA(const nln_params *params, const float *bodies, int64_t n, double eps2,
+                         float quad_phi_sign, int ewald, float *acc_phi);
+void grav_build_eval_phases(double seconds[4]);
 
 /*
  * The plan's problem as it evaluates it: sizes and parameters, device

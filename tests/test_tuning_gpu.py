@@ -33,8 +33,8 @@ def test_retune_keeps_results_and_autotune_picks_a_shape():
 
 def test_autotune_places_the_ewald_moments_of_a_periodic_plan():
     """For a periodic plan the autotuner also tries the Ewald moments on the
-    side stream and in the finish pass; whatever it picks, the forces are
-    those of the default shape."""
+    side stream and on the evaluation's stream; whatever it picks, the
+    forces are those of the default shape."""
     from pgrav import autotune as AT, gravcuda as gc, host, ics
     pos, m = ics.grf_box(20, seed=52, rms_disp=0.3)
     t = host.Tree(pos, m, tol=1e-4, box=1.0, p2cut=7, p4cut=20)
@@ -42,8 +42,9 @@ def test_autotune_places_the_ewald_moments_of_a_periodic_plan():
     plan.eval()
     ref = plan.download()
     best, trials = AT.autotune(plan, reps=1, shapes=((8, 0), (4, 0)), scales=(0.5, 1.0))
-    assert sorted({tr["ewald_side"] for tr in trials}) == [-1, 0, 2]
-    assert best.ewald_side in (-1, 0, 2)
+    tried = {tr["ewald_side"] for tr in trials}
+    assert 0 in tried and any(x < 0 for x in tried) and any(x > 0 for x in tried), tried
+    assert best.ewald_side in tried
     plan.eval()
     e = _rel(plan.download()[:, :3], ref[:, :3])
     assert e.max() < 1e-6, e.max()
