@@ -773,9 +773,9 @@ def main():
     ap.add_argument("--workload", default="box256", choices=list(WORKLOADS))
     ap.add_argument("--tol", type=float, default=0.0)
     ap.add_argument("--e2e-steps", type=int, default=3,
+                    help="end-to-end calls from lists built on the host (grav_groups_CUDA)")
+    ap.add_argument("--e2e-pos-steps", type=int, default=3,
                     help="end-to-end calls from positions (GPU tree build + evaluation)")
-    ap.add_argument("--e2e-lists-steps", type=int, default=2,
-                    help="end-to-end calls from lists built on the host (their transport)")
     ap.add_argument("--e2e-plain-lists", action="store_true",
                     help="end-to-end leg: copy the plain lists instead of the run-packed ones")
     ap.add_argument("--e2e-lists-in-host", action="store_true",
@@ -965,12 +965,13 @@ def main():
                      "systems": int(len(tree.body_offsets) - 1)}
     plan.free()   # the end-to-end leg uploads its own copy
 
-    # ---- end to end: positions in host memory to forces in host memory in one
-    # call (grav_build_eval_CUDA): bodies to the device, tree, moments, critical
-    # radii, sink groups and lists built there, evaluation, results back in the
-    # bodies' order
-    e2e = None
-    if args.e2e_steps > 0 and w["kind"] != "batch":
+    # ---- end to end from positions: positions in host memory to forces in host
+    # memory in one call (grav_build_eval_CUDA): bodies to the device, tree,
+    # moments, critical radii, sink groups and lists built there, evaluation,
+    # results back in the bodies' order.  The reference arm has no comparable
+    # leg: it times its kernels on lists its host walk built.
+    e2e_pos = None
+    if args.e2e_pos_steps > 0 and w["kind"] != "batch":
         import torch as _t
         nb = len(pos)
         bbuf = _t.empty((nb, 4), dtype=_t.float32, pin_memory=True).numpy()
@@ -982,7 +983,7 @@ def main():
         ew = w["ewald"] and box > 0
         gc.build_eval(bbuf, eps2, box=box, ewald=ew, out=obuf, **kw)  # warm-up
         walls, phases = [], []
-        for _ in range(args.e2e_steps):
+        for _ in range(args.e2e_pos_steps):
             ta = time.perf_counter()
             gc.build_eval(bbuf, eps2, box=box, ewald=ew, out=obuf, **kw)
             walls.append(time.perf_counter() - ta)
@@ -990,9 +991,9 @@ def main():
         e2e_s = float(np.median(walls))
         mid = int(np.argsort(walls)[len(walls) // 2])
         same = bool(out_plan is not None and np.array_equal(obuf[tree.order], out_plan))
-        e2e = {"value": inter * world / e2e_s, "unit": UNIT,
+        e2e_pos = {"value": inter * world / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(bbuf.nbytes), "d2h_bytes_per_step": int(obuf.nbytes),
-               "ms_per_step": e2e_s * 1e3, "steps": args.e2e_steps,
+               "ms_per_step": e2e_s * 1e3, "steps": args.e2e_pos_steps,
                "timing": "wall clock around grav_build_eval_CUDA: bodies (page-locked) to the "
                          "device, tree + moments + critical radii + groups + MAC walk on the GPU, "
                          "evaluation, (ax, ay, az, phi) back in the input order",
@@ -1000,11 +1001,13 @@ def main():
                "equals_plan_output": same}
         gc.lib().grav_groups_release_CUDA()
 
-    # ---- end to end from lists built on the host: the lists' transport
-    e2e_lists = None
+    # ---- end to end through the drop-in boundary: lists built by the host walk
+    # (as the reference's walk builds them) in page-locked host memory, forces
+    # back in host memory, one grav_groups_CUDA call per step
+    e2e = None
     host = out = None
     pack_s = None
-    if args.e2e_lists_steps > 0:
+    if args.e2e_steps > 0:
         packed = not (args.e2e_plain_lists or args.e2e_lists_in_host)
         if packed:
             tp = time.perf_counter()
@@ -1015,7 +1018,7 @@ def main():
         torch.cuda.synchronize()
         gc.groups_eval_problem(host, eps2, box, ewald=w["ewald"] and box > 0)  # warm-up
         walls, phases = [], []
-        for _ in range(args.e2e_lists_steps):
+        for _ in range(args.e2e_steps):
             ta = time.perf_counter()
             gc.groups_eval_problem(host, eps2, box, ewald=w["ewald"] and box > 0)
             torch.cuda.synchronize()
@@ -1023,9 +1026,9 @@ def main():
             phases.append(gc.groups_phases())
         e2e_s = float(np.median(walls))
         mid = int(np.argsort(walls)[len(walls) // 2])
-        e2e_lists = {"value": inter * world / e2e_s, "unit": UNIT,
+        e2e = {"value": inter * world / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(host.h2d_bytes), "d2h_bytes_per_step": int(out.nbytes),
-               "ms_per_step": e2e_s * 1e3, "steps": args.e2e_lists_steps,
+               "ms_per_step": e2e_s * 1e3, "steps": args.e2e_steps,
                "timing": "wall clock around grav_groups_CUDA (upload, evaluate, download)",
                "walls_s": walls, "phases_s": phases[mid],
                "lists": ("read by the kernels in place from page-locked host memory over PCIe "
@@ -1090,7 +1093,8 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32 (FP64 centres, compensated sums)", "data": "synthetic (seeded)",
                 "config": cfg, "gpu_launches": launches * args.steps,
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "e2e_lists": e2e_lists,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "e2e_from_positions": e2e_pos,
                 "clocks": clocks,
                 "accuracy": acc,
                 "host_setup_s": {"ics": t1 - t0, "tree_walk": t2 - t1, "upload": t3 - t2}}
