@@ -16,6 +16,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -329,11 +330,19 @@ __global__ void k_quad_index(const float *__restrict__ pos, float4 *accp, int m,
 }
 
 // ------------------------------------------------------------ state
+// A queue slot: its stream, a device list buffer, and two page-locked
+// staging buffers used in turn; the copy out of each staging buffer records
+// an event, so reusing a staging buffer waits only for the copy that last
+// read it (two calls back), never for the slot's kernels.
 struct Slot {
     bool inuse = false;
     cudaStream_t stream = nullptr;
     size_t cap = 0;
-    void *host = nullptr;
+    void *host = nullptr;      // the staging buffer of the current call
+    void *hbuf[2] = {nullptr, nullptr};
+    cudaEvent_t copied[2] = {nullptr, nullptr};
+    bool pending[2] = {false, false};
+    int turn = 0;
     void *dev = nullptr;
 };
 
@@ -365,26 +374,62 @@ int ensure_init() {
     return 0;
 }
 
+// Make slot q ready for a call of `bytes`: staging buffer s.host free to
+// write (the copy that last read it has completed), device buffer large
+// enough.  The device buffer is only rewritten by copies on the slot's own
+// stream, which run after the kernels queued before them.
 int slot_reserve(int q, size_t bytes) {
     if (q < 0 || q >= NQ)
         return gc::set_status(-1, "queue slot %d out of range", q);
     Slot &s = S.q[q];
     if (s.cap < bytes) {
         GC_CHECK(cudaStreamSynchronize(s.stream));
-        if (s.host)
-            GC_CHECK(cudaFreeHost(s.host));
+        for (int k = 0; k < 2; k++) {
+            if (s.hbuf[k])
+                GC_CHECK(cudaFreeHost(s.hbuf[k]));
+            s.hbuf[k] = nullptr;
+            s.pending[k] = false;
+            if (!s.copied[k])
+                GC_CHECK(cudaEventCreateWithFlags(&s.copied[k], cudaEventDisableTiming));
+        }
         if (s.dev)
             GC_CHECK(cudaFree(s.dev));
         size_t cap = 1 << 20;
         while (cap < bytes) cap <<= 1;
-        GC_CHECK(cudaMallocHost(&s.host, cap));
+        for (int k = 0; k < 2; k++) GC_CHECK(cudaMallocHost(&s.hbuf[k], cap));
         GC_CHECK(cudaMalloc(&s.dev, cap));
         s.cap = cap;
-    } else {
-        // the pinned buffer may still feed a previous copy
-        GC_CHECK(cudaStreamSynchronize(s.stream));
     }
+    s.turn ^= 1;
+    if (s.pending[s.turn])
+        GC_CHECK(cudaEventSynchronize(s.copied[s.turn]));
+    s.host = s.hbuf[s.turn];
     return 0;
+}
+
+// After the call's copy out of s.host is queued: mark the staging buffer busy.
+int slot_copied(Slot &s) {
+    GC_CHECK(cudaEventRecord(s.copied[s.turn], s.stream));
+    s.pending[s.turn] = true;
+    return 0;
+}
+
+// Copy a list into page-locked staging memory; large lists with several
+// host threads (a single thread's memcpy would bound the call).
+void stage_copy(void *dst, const void *src, size_t bytes) {
+    constexpr size_t kPar = 256u << 10;
+    if (bytes < kPar) {
+        memcpy(dst, src, bytes);
+        return;
+    }
+    const int nt = std::min<int>(8, (int)(bytes / kPar) + 1);
+    const size_t per = (bytes / nt + 63) / 64 * 64;
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int t = 0; t < nt; t++) {
+        const size_t a = (size_t)t * per, b = std::min(bytes, a + per);
+        if (a < b)
+            memcpy((char *)dst + a, (const char *)src + a, b - a);
+    }
 }
 
 int check_device_error(const char *what) {
@@ -411,7 +456,12 @@ int launch_list(cudaStream_t st, const float *pos, float4 *acc, int m, const flo
     int gy = (nblk + bpc - 1) / bpc;
     size_t smem = (size_t)2 * TBLK * sz * 8 * 4 + (size_t)TSRC * REC * 4 + 16;
     auto kern = k_list<ORDER, SOFT>;
-    GC_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // the largest dynamic shared memory set for this kernel so far (once per size)
+    static int smem_set = 0;
+    if ((int)smem > smem_set) {
+        GC_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        smem_set = (int)smem;
+    }
     kern<<<dim3(gx, gy), threads, smem, st>>>(pos, acc, m, f, nblk, sz, bpc, e, qsh, S.derr);
     GC_CHECK(cudaGetLastError());
     return 0;
@@ -473,8 +523,10 @@ int grav_mn_impl(const char *routine, const float *p, int n, int stride, const f
     if (int rc = slot_reserve(q, bytes))
         return rc;
     Slot &s = S.q[q];
-    memcpy(s.host, f, bytes);
+    stage_copy(s.host, f, bytes);
     GC_CHECK(cudaMemcpyAsync(s.dev, s.host, bytes, cudaMemcpyHostToDevice, s.stream));
+    if (int rc = slot_copied(s))
+        return rc;
     s.inuse = true;
     return dispatch_list(*r, s.stream, S.devpos + 3 * first, S.devaccp + first, n,
                          (const float *)s.dev, source_n / 8, sz, e);
@@ -503,8 +555,12 @@ extern "C" void CUDA_Finalize(void) {
             cudaStreamSynchronize(s.stream);
             cudaStreamDestroy(s.stream);
         }
-        if (s.host)
-            cudaFreeHost(s.host);
+        for (int k = 0; k < 2; k++) {
+            if (s.hbuf[k])
+                cudaFreeHost(s.hbuf[k]);
+            if (s.copied[k])
+                cudaEventDestroy(s.copied[k]);
+        }
         if (s.dev)
             cudaFree(s.dev);
         s = Slot{};
@@ -521,8 +577,12 @@ extern "C" int vecwidthCUDA(void) { return SPT; }
 extern "C" int qallocCUDA(int *inuse) {
     if (ensure_init())
         return -1;
+    // slots are handed out round-robin; without the busy count the search
+    // stops at the first free slot (one stream query per busy slot passed)
+    static int next = 0;
     int busy = 0, free_slot = -1;
-    for (int i = 0; i < NQ; i++) {
+    for (int k = 0; k < NQ; k++) {
+        const int i = (next + k) % NQ;
         Slot &s = S.q[i];
         if (s.inuse) {
             cudaError_t e = cudaStreamQuery(s.stream);
@@ -535,11 +595,16 @@ extern "C" int qallocCUDA(int *inuse) {
         }
         if (s.inuse)
             busy++;
-        else if (free_slot < 0)
+        else if (free_slot < 0) {
             free_slot = i;
+            if (!inuse)
+                break;
+        }
     }
     if (inuse)
         *inuse = busy;
+    if (free_slot >= 0)
+        next = (free_slot + 1) % NQ;
     return free_slot;
 }
 
@@ -690,6 +755,8 @@ static int runs_launch(int sink_base, int m, const uint16_t *ss_index, const seg
         if (ss_index[i] >= ss_len)
             return gc::set_status(-1, "ss_index[%d] = %d >= ss_len %d", i, ss_index[i], ss_len);
     GC_CHECK(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, s.stream));
+    if (int rc = slot_copied(s))
+        return rc;
     s.inuse = true;
     int threads = 128;
     k_runs_k1<<<(m + threads - 1) / threads, threads, 0, s.stream>>>(
@@ -755,6 +822,8 @@ extern "C" void grav_qns_CUDA(const char *routine, const int base, const int m,
         gc::set_status(-1, "grav_qns_CUDA: copy failed");
         return;
     }
+    if (slot_copied(s))
+        return;
     s.inuse = true;
     k_quad_index<<<(m + 127) / 128, 128, 0, s.stream>>>(S.devpos + 3 * (size_t)base,
                                                         S.devaccp + base, m, (const int *)s.dev,
@@ -792,6 +861,8 @@ extern "C" void grav_qnss_CUDA(const char *routine, const int base, const int m,
         gc::set_status(-1, "grav_qnss_CUDA: copy failed");
         return;
     }
+    if (slot_copied(s))
+        return;
     s.inuse = true;
     k_quad_runs<<<(m + 127) / 128, 128, 0, s.stream>>>(
         S.devpos + 3 * (size_t)base, S.devaccp + base, m, (const segment *)s.dev,

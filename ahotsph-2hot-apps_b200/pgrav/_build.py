@@ -100,9 +100,25 @@ def build_cuda(force=False, verbose_ptxas=False):
     return CUDA_SO
 
 
+DRIVE_SO = os.path.join(LIBDIR, "libmacdrive.so")
+
+
+def build_drive(force=False):
+    """lib/libmacdrive.so: a C caller of the drop-in ABI as nln/mac.c drives it
+    (timing without an interpreter in the loop), linked to libgravcuda.so."""
+    cuda = build_cuda(force)
+    src = os.path.join(CSRC, "drive", "mac_drive.c")
+    if force or _newer(DRIVE_SO, [src, cuda, os.path.join(INCLUDE, "gravcuda.h")]):
+        cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
+        _run([cc, "-O2", "-fPIC", "-shared", "-std=gnu99", "-I", INCLUDE, "-o", DRIVE_SO, src,
+              "-L", LIBDIR, "-lgravcuda", "-Wl,-rpath,$ORIGIN"])
+    return DRIVE_SO
+
+
 def build_all(force=False):
     build_host(force)
     build_cuda(force)
+    build_drive(force)
 
 
 if __name__ == "__main__":

@@ -458,6 +458,41 @@ def fp32_peak():
     return out.value
 
 
+_drive = None
+
+
+def drive_mn(dropin, first, count, packs, e):
+    """Time the drop-in call sequence of nln/mac.c from C (lib/libmacdrive.so):
+    for every group g and list kind, one grav_mn_CUDA on a slot from
+    qallocCUDA, then WalkTerminateSinkCUDA; returns the wall-clock seconds.
+    dropin: a DropIn (its body table is registered); first, count: sinks of
+    each group in that table; packs: (routine, sz, blk_ptr, data) per kind,
+    blk_ptr with one entry per group plus one."""
+    global _drive
+    if _drive is None:
+        lib()
+        _drive = ctypes.CDLL(_build.build_drive())
+        _drive.mac_drive_mn.restype = ctypes.c_double
+        _drive.mac_drive_mn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64,
+                                        ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float]
+    first = np.ascontiguousarray(first, np.int64)
+    count = np.ascontiguousarray(count, np.int32)
+    k = len(packs)
+    names = (ctypes.c_char_p * k)(*[r.encode() for r, _, _, _ in packs])
+    sz = (ctypes.c_int * k)(*[int(z) for _, z, _, _ in packs])
+    datas = [np.ascontiguousarray(d, np.float32) for _, _, _, d in packs]
+    ptrs = [np.ascontiguousarray(b, np.int64) for _, _, b, _ in packs]
+    data_p = (ctypes.c_void_p * k)(*[d.ctypes.data for d in datas])
+    ptr_p = (ctypes.c_void_p * k)(*[b.ctypes.data for b in ptrs])
+    secs = _drive.mac_drive_mn(dropin.btab.ctypes.data, BODY_STRIDE, len(dropin.btab), len(first),
+                               first.ctypes.data, count.ctypes.data, k, names, sz, data_p, ptr_p,
+                               float(e))
+    check()
+    return secs
+
+
 def direct_fp64(points, sinks, eps2, box=0.0):
     """FP64 direct sum on the GPU at sample sinks (grav_direct_fp64_CUDA):
     (nsink, 4) doubles (ax, ay, az, phi); Ewald-summed when box > 0."""

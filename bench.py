@@ -258,8 +258,10 @@ def dropin_rate(tree, eps2, max_groups=2048, seed=1, max_bytes=1 << 30):
     """The plain FP32 drop-in path (gravcuda.h Part 1 as nln/mac.c drives it:
     WalkInitSinkCUDA, one grav_mn_CUDA per group and list kind on the
     reference AoSoA lists with absolute FP32 coordinates, then
-    WalkTerminateSinkCUDA) over a random sample of the same groups; wall
-    clock, Newtonian list terms: (interactions/s, seconds, sample)."""
+    WalkTerminateSinkCUDA) over a random sample of the same groups, the
+    calls issued from C (lib/libmacdrive.so), the sampled groups' sinks in a
+    body table of their own; wall clock from the first call to the results,
+    Newtonian list terms: (interactions/s, seconds, sample)."""
     from pgrav import gravcuda as gc
     rng = np.random.default_rng(seed)
     per_group = sum(float(tree.ptr[k][-1]) / tree.ngroups * sz * 4 for k, sz in ((0, 4), (1, 13), (2, 29)))
@@ -274,23 +276,19 @@ def dropin_rate(tree, eps2, max_groups=2048, seed=1, max_bytes=1 << 30):
         bp, data = tree.aosoa_subset(gids, kind)
         packs.append((routine, sz, bp, data))
         inter += int(((ptr[gids + 1] - ptr[gids]) * tree.groups["count"][gids]).sum())
-    bt = gc.body_table(tree.sorted_pos, tree.points[:tree.n, 3])
     first = tree.groups["first"][gids].astype(np.int64)
-    count = tree.groups["count"][gids].astype(np.int64)
-    import torch
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    d = gc.DropIn(bt)
-    for routine, sz, bp, data in packs:
-        for s in range(ng):
-            b0, b1 = int(bp[s]), int(bp[s + 1])
-            if b1 > b0:
-                d.mn(routine, int(first[s]), int(count[s]), data[b0 * sz * 8:b1 * sz * 8],
-                     (b1 - b0) * 8, sz, eps2)
-    d.terminate()
-    el = time.perf_counter() - t0
+    count = tree.groups["count"][gids].astype(np.int32)
+    idx = np.concatenate([np.arange(f, f + c) for f, c in zip(first, count)])
+    local_first = np.concatenate([[0], np.cumsum(count)[:-1]]).astype(np.int64)
+    bt = gc.body_table(tree.sorted_pos[idx], tree.points[idx, 3])
+    secs = []
+    for _ in range(3):  # the first pass sizes the slots' buffers
+        d = gc.DropIn(bt.copy())
+        secs.append(gc.drive_mn(d, local_first, count, packs, eps2))
+    el = min(secs[1:])
     return (inter / el, el, f"{ng} random sink groups ({int(count.sum())} sinks, {inter} "
-            f"interactions), one grav_mn_CUDA per group and kind (pMp/pQp/pHp)")
+            f"interactions), one grav_mn_CUDA per group and kind (pMp/pQp/pHp) issued from C "
+            f"(best of 2 passes after one)")
 
 
 def kdk_run(w, pos, m, eps2, box, tol, nsteps, dt, rebuild):
@@ -352,22 +350,22 @@ def config_plummer64k(args, stream):
     got = plan.download()
     plan.free()
     res["batched"] = {"ms": ms, "value": inter / (ms * 1e-3), "unit": UNIT}
-    # drop-in: one grav_mn_CUDA per group and kind, as nln/mac.c issues them
+    # drop-in: one grav_mn_CUDA per group and kind, as nln/mac.c issues them (from C)
     bt = gc.body_table(t.sorted_pos, t.points[:t.n, 3])
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    d = gc.DropIn(bt)
-    for k, (routine, sz) in enumerate((("pMp", 4), ("pQp", 13))):
-        ptr, data = t.aosoa[k]
-        for g in range(t.ngroups):
-            b0, b1 = int(ptr[g]), int(ptr[g + 1])
-            if b1 > b0:
-                d.mn(routine, int(t.groups["first"][g]), int(t.groups["count"][g]),
-                     data[b0 * sz * 8:b1 * sz * 8], (b1 - b0) * 8, sz, eps2)
-    got_d = d.terminate()
-    el = time.perf_counter() - t0
+    packs = [(routine, sz, t.aosoa[k][0], t.aosoa[k][1])
+             for k, (routine, sz) in enumerate((("pMp", 4), ("pQp", 13)))]
+    first = np.ascontiguousarray(t.groups["first"], np.int64)
+    count = np.ascontiguousarray(t.groups["count"], np.int32)
+    secs = []
+    for _ in range(3):  # the first pass sizes the slots' buffers
+        d = gc.DropIn(bt.copy())
+        secs.append(gc.drive_mn(d, first, count, packs, eps2))
+    got_d = d.btab[:, 7:11].copy()
+    el = min(secs[1:])
     res["dropin"] = {"s": el, "value": inter / el, "unit": UNIT,
-                     "timing": "wall clock, WalkInitSinkCUDA .. WalkTerminateSinkCUDA from Python"}
+                     "timing": "wall clock of the calls issued from C (lib/libmacdrive.so), first "
+                               "grav_mn_CUDA to the end of WalkTerminateSinkCUDA, best of 2 "
+                               "passes after one"}
     # CPU leg: the reference's own kernels over the full lists, all host threads
     if O.ref_available():
         t0 = time.perf_counter()
