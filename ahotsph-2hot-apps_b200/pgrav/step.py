@@ -189,6 +189,37 @@ class Stepper:
     def run(self, nsteps, dt):
         return [self.step(dt) for _ in range(nsteps)]
 
+    def save(self, path):
+        """A checkpoint: the bodies (original order, ident = original index)
+        and the step state in an SDF file with the reference's header keys
+        (nln/output.c:217-330) plus this run's parameters."""
+        from . import sdf
+        pos, vel = self.state()
+        sdf.write(path, pos, vel, self.mass, header={
+            "version": (sdf.INT, 2), "version_2HOT": (sdf.INT, 2), "npart": (sdf.INT64, self.n),
+            "iter": (sdf.INT, self.nsteps), "do_periodic": (sdf.INT, int(self.box > 0)),
+            "tpos": (sdf.DOUBLE, self.tpos), "tvel": (sdf.DOUBLE, self.tvel),
+            "tacc": (sdf.DOUBLE, self.tpos), "R0": (sdf.FLOAT, 0.5 * self.box),
+            "L0": (sdf.FLOAT, self.box), "Gnewt": (sdf.DOUBLE, 1.0),
+            "eps2": (sdf.DOUBLE, self.eps2), "ewald": (sdf.INT, int(self.ewald)),
+            "rebuild": (sdf.INT, self.rebuild)})
+
+    @classmethod
+    def load(cls, path, graph=True, tree_kw=None, gpu_build=True):
+        """Resume from a checkpoint written by save(): the same bodies, step
+        count and times, so the run continues as the saved one would have."""
+        from . import sdf
+        h, b = sdf.read(path)
+        order = np.argsort(b["ident"], kind="stable")
+        st = cls(b["pos"][order], b["vel"][order], b["mass"][order], h["eps2"],
+                 box=float(h.get("L0", 0.0)) if h.get("do_periodic") else 0.0,
+                 ewald=bool(h.get("ewald", 0)), rebuild=h.get("rebuild", 8), graph=graph,
+                 tree_kw=tree_kw, gpu_build=gpu_build)
+        st.nsteps = int(h["iter"])
+        st.tpos = float(h["tpos"])
+        st.tvel = float(h["tvel"])
+        return st
+
     def free(self):
         if self.plan is not None:
             self.plan.free()

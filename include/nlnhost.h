@@ -169,6 +169,38 @@ void nln_ewald_eval(double L, const double *y, double *out);
 /* The same on an n^3 grid over [0, reach*L]^3 (node (i,j,k) at (i,j,k)*reach*L/(n-1)). */
 int nln_ewald_table(double L, int n, double reach, double *out);
 
+/*
+ * ---- snapshots and checkpoints in the SDF format ----
+ * The reference writes bodies as outbody records (nln/physics.h:49-58:
+ * mass, x y z, vx vy vz, with SAVE_ACC also ax ay az phi, int64 ident;
+ * packed) with the descriptor OUTBODYDESC (nln/physics.h:62-110) and header
+ * scalars (version, npart, iter, tpos, tvel, ..., nln/output.c:217-330)
+ * into an SDF file: an ASCII header of C-like declarations ending
+ * "# SDF-EOH", then the little-endian records.  nln_sdf_write writes one
+ * (acc_phi: NULL for the plain record, else 4 floats per body (ax, ay, az,
+ * phi)); header entries are (key, type, value) with the NLN_SDF_* types.
+ * nln_sdf_read reads one back: its header entries, the record count, and
+ * the bodies (nln_sdf_bodies; any output pointer may be NULL).  Errors:
+ * -1 / NULL with a message in nln_sdf_error().
+ */
+#define NLN_SDF_INT 0
+#define NLN_SDF_INT64 1
+#define NLN_SDF_FLOAT 2
+#define NLN_SDF_DOUBLE 3
+typedef struct nln_sdf nln_sdf;
+int nln_sdf_write(const char *path, int64_t n, const float *mass, const float *pos,
+                  const float *vel, const float *acc_phi, const int64_t *ident, int nkeys,
+                  const char *const *keys, const int *types, const double *values);
+nln_sdf *nln_sdf_read(const char *path);
+int64_t nln_sdf_count(const nln_sdf *s);
+int nln_sdf_has_acc(const nln_sdf *s);
+int nln_sdf_nkeys(const nln_sdf *s);
+const char *nln_sdf_key(const nln_sdf *s, int k, int *type, double *value);
+int nln_sdf_bodies(const nln_sdf *s, float *mass, float *pos, float *vel, float *acc_phi,
+                   int64_t *ident);
+void nln_sdf_free(nln_sdf *s);
+const char *nln_sdf_error(void);
+
 #ifdef __cplusplus
 }
 #endif
