@@ -207,7 +207,9 @@ class Stepper:
     @classmethod
     def load(cls, path, graph=True, tree_kw=None, gpu_build=True):
         """Resume from a checkpoint written by save(): the same bodies, step
-        count and times, so the run continues as the saved one would have."""
+        count and times.  The tree is built from the saved bodies, so a
+        checkpoint taken on a rebuild step (a multiple of `rebuild`) continues
+        exactly as the saved run would have."""
         from . import sdf
         h, b = sdf.read(path)
         order = np.argsort(b["ident"], kind="stable")

@@ -156,10 +156,11 @@ def test_kdk_periodic_box_runs_and_wraps(mods):
 
 
 def test_checkpoint_and_resume_continue_the_run(tmp_path):
-    """8 KDK steps straight through against 3 steps, an SDF checkpoint
-    (Stepper.save), a resumed stepper (Stepper.load) and 5 more steps: the
-    same positions and velocities bit for bit (rebuilds fall on the same
-    steps and see the same bodies in the same order)."""
+    """8 KDK steps straight through against 4 steps, an SDF checkpoint
+    (Stepper.save) at that rebuild boundary, a resumed stepper
+    (Stepper.load, which builds its tree from the saved bodies as the
+    straight run rebuilds from the same bodies) and 4 more steps: the same
+    positions and velocities bit for bit."""
     from pgrav import ics, step as S
     pos, m = ics.plummer(3000, seed=21)
     vel = np.random.default_rng(2).normal(0, 0.1, pos.shape).astype(np.float32)
@@ -169,13 +170,13 @@ def test_checkpoint_and_resume_continue_the_run(tmp_path):
     want = a.state()
     a.free()
     b = S.Stepper(pos, vel, m, 1e-4, rebuild=4, graph=True, tree_kw=kw)
-    b.run(3, 1e-3)
+    b.run(4, 1e-3)
     path = tmp_path / "ck.sdf"
     b.save(path)
     b.free()
     c = S.Stepper.load(path, graph=True, tree_kw=kw)
-    assert c.nsteps == 3
-    c.run(5, 1e-3)
+    assert c.nsteps == 4
+    c.run(4, 1e-3)
     got = c.state()
     c.free()
     assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
