@@ -8,8 +8,9 @@ rebuilds the same (deterministic) tree from the saved inputs, holds those lists 
 (the tree is piecewise constant in the positions) and returns dL/dx and
 dL/dm for any loss whose gradient with respect to the outputs
 (accelerations, potentials) autograd supplies.  Only the inputs are saved,
-so checkpointed segments keep no device tables alive.  Isolated systems
-with monopole and quadrupole cells (p4cut = 0).
+so checkpointed segments keep no device tables alive.  Every list kind is
+covered: bodies, monopole, quadrupole and order-4 cells, and in periodic
+boxes (box > 0, ewald=True) the image shifts and the Ewald correction.
 """
 import torch
 
@@ -35,9 +36,6 @@ class TreeGravity(torch.autograd.Function):
     @staticmethod
     def forward(ctx, pos, mass, eps2, tree_kw):
         kw = dict(tree_kw or {})
-        kw.setdefault("p4cut", 0)
-        if kw["p4cut"]:
-            raise ValueError("the adjoint covers monopole and quadrupole cells (p4cut = 0)")
         order, plan = TreeGravity._plan(pos, mass, eps2, kw)
         plan.eval()
         n = pos.shape[0]
@@ -82,13 +80,17 @@ def leapfrog(pos, vel, mass, eps2, dt, nsteps, checkpoint_every=0, **tree_kw):
     """KDK leapfrog (kick dt/2, drift dt, kick dt/2 per step) through the
     differentiable force; with checkpoint_every = k the steps run in segments
     of k under torch.utils.checkpoint, so only segment boundaries are stored
-    and each segment's forces are recomputed in the backward pass."""
+    and each segment's forces are recomputed in the backward pass.  In a
+    periodic box (tree_kw box > 0) drifted positions wrap into [0, box)."""
     from torch.utils.checkpoint import checkpoint
+    box = float(tree_kw.get("box", 0.0) or 0.0)
 
     def one(x, v):
         a, _ = gravity(x, mass, eps2, **tree_kw)
         v = v + 0.5 * dt * a
         x = x + dt * v
+        if box > 0:
+            x = torch.remainder(x, box)
         a, _ = gravity(x, mass, eps2, **tree_kw)
         v = v + 0.5 * dt * a
         return x, v

@@ -471,232 +471,6 @@ void orc_groups_eval(int kind, const float *f, int sz, const long *blk_first,
 }
 
 /*
- * ---- FP64 evaluation of fixed batched index lists (the adjoint's checker) ----
- *
- * The batched lists (include/nlnlists.h): bodies 0..n-1 in tree order, the
- * point table's records n + c are cell c's monopoles, quadrupole-list
- * entries are cells.  Isolated trees only (image code 13).  Every cell's
- * moments are taken in FP64 from its bodies: mass M, centre of mass X and
- * the traceless Q = -3 (S2 - tr(S2)/3 I), S2 = sum m (x - X)(x - X)^T, so
- * that a quadrupole cell adds phi += 1/2 rho^-5 d.Q.d and
- * a += 5/2 rho^-7 (d.Q.d) d - rho^-5 Q d to its monopole term (the physical
- * quadrupole potential, sign +1, of do_gravpq_avx8's arithmetic,
- * nln/do_grav_avx8.c:2090-2160 with the order-4 kernels' sign, :1846);
- * d = sink - source, rho^2 = |d|^2 + eps2.  Order-4 lists are not covered.
- */
-typedef struct {
-    double M, X[3], Q[6]; /* Q: xx xy xz yy yz zz */
-} orc_mom;
-
-static void cell_moments(const double *x, const double *m, long first, int count, orc_mom *o) {
-    double M = 0, s[3] = {0, 0, 0};
-    for (long b = first; b < first + count; b++) {
-        M += m[b];
-        for (int d = 0; d < 3; d++) s[d] += m[b] * x[3 * b + d];
-    }
-    o->M = M;
-    for (int d = 0; d < 3; d++) o->X[d] = M > 0 ? s[d] / M : 0.0;
-    double S[6] = {0, 0, 0, 0, 0, 0};
-    for (long b = first; b < first + count; b++) {
-        double y0 = x[3 * b] - o->X[0], y1 = x[3 * b + 1] - o->X[1], y2 = x[3 * b + 2] - o->X[2];
-        S[0] += m[b] * y0 * y0; S[1] += m[b] * y0 * y1; S[2] += m[b] * y0 * y2;
-        S[3] += m[b] * y1 * y1; S[4] += m[b] * y1 * y2; S[5] += m[b] * y2 * y2;
-    }
-    double tr = (S[0] + S[3] + S[5]) / 3.0;
-    o->Q[0] = -3.0 * (S[0] - tr); o->Q[1] = -3.0 * S[1]; o->Q[2] = -3.0 * S[2];
-    o->Q[3] = -3.0 * (S[3] - tr); o->Q[4] = -3.0 * S[4]; o->Q[5] = -3.0 * (S[5] - tr);
-}
-
-/* One sink at s against a point (quad = 0) or a quadrupole cell (quad = 1). */
-static void term64(const double *s, const double *X, double M, const double *Q, int quad,
-                   double eps2, double *a, double *phi) {
-    double d0 = s[0] - X[0], d1 = s[1] - X[1], d2 = s[2] - X[2];
-    double rho2 = d0 * d0 + d1 * d1 + d2 * d2 + eps2;
-    double ri = 1.0 / sqrt(rho2), ri2 = ri * ri, ri3 = ri * ri2;
-    *phi -= M * ri;
-    a[0] -= M * d0 * ri3;
-    a[1] -= M * d1 * ri3;
-    a[2] -= M * d2 * ri3;
-    if (!quad)
-        return;
-    double q0 = Q[0] * d0 + Q[1] * d1 + Q[2] * d2;
-    double q1 = Q[1] * d0 + Q[3] * d1 + Q[4] * d2;
-    double q2 = Q[2] * d0 + Q[4] * d1 + Q[5] * d2;
-    double P2 = d0 * q0 + d1 * q1 + d2 * q2;
-    double ri5 = ri3 * ri2, ri7 = ri5 * ri2;
-    *phi += 0.5 * ri5 * P2;
-    a[0] += 2.5 * ri7 * P2 * d0 - ri5 * q0;
-    a[1] += 2.5 * ri7 * P2 * d1 - ri5 * q1;
-    a[2] += 2.5 * ri7 * P2 * d2 - ri5 * q2;
-}
-
-#define ORC_IDX_MASK ((1u << 27) - 1u)
-
-/* (X, M, Q) of point-table record idx (body, or cell monopole) from mom[]. */
-static void point_source(unsigned idx, long n, const double *x, const double *m, const orc_mom *mom,
-                         const double **X, double *M) {
-    if ((long)idx < n) {
-        *X = x + 3 * (long)idx;
-        *M = m[idx];
-    } else {
-        *X = mom[idx - n].X;
-        *M = mom[idx - n].M;
-    }
-}
-
-/*
- * Full FP64 evaluation: out (4 doubles per body, tree order) = (a, phi) of
- * every sink over its group's point and quadrupole lists, all cells'
- * moments recomputed from x, m.  Returns 0, or -1 on an image code other
- * than 13 (periodic lists are not covered).
- */
-int orc_lists_eval64(long n, const double *x, const double *m, long ncells, const long *cfirst,
-                     const int *ccount, long ngroups, const long *gfirst, const int *gcount,
-                     const long *pptr, const unsigned *plist, const long *qptr,
-                     const unsigned *qlist, double eps2, double *out) {
-    orc_mom *mom = (orc_mom *)malloc(sizeof(orc_mom) * (size_t)(ncells > 0 ? ncells : 1));
-#pragma omp parallel for schedule(dynamic, 64)
-    for (long c = 0; c < ncells; c++) cell_moments(x, m, cfirst[c], ccount[c], &mom[c]);
-    int bad = 0;
-#pragma omp parallel for schedule(dynamic, 16) reduction(| : bad)
-    for (long g = 0; g < ngroups; g++) {
-        for (int k = 0; k < gcount[g]; k++) {
-            long i = gfirst[g] + k;
-            double a[3] = {0, 0, 0}, phi = 0;
-            for (long e = pptr[g]; e < pptr[g + 1]; e++) {
-                if ((plist[e] >> 27) != 13u) { bad = 1; continue; }
-                const double *X; double M;
-                point_source(plist[e] & ORC_IDX_MASK, n, x, m, mom, &X, &M);
-                term64(x + 3 * i, X, M, NULL, 0, eps2, a, &phi);
-            }
-            if (qptr)
-                for (long e = qptr[g]; e < qptr[g + 1]; e++) {
-                    if ((qlist[e] >> 27) != 13u) { bad = 1; continue; }
-                    const orc_mom *c = &mom[qlist[e] & ORC_IDX_MASK];
-                    term64(x + 3 * i, c->X, c->M, c->Q, 1, eps2, a, &phi);
-                }
-            for (int d = 0; d < 3; d++) out[4 * i + d] = a[d];
-            out[4 * i + 3] = phi;
-        }
-    }
-    free(mom);
-    return bad ? -1 : 0;
-}
-
-/*
- * The entries that depend on the selected bodies sel[0..nsel) (nsel <= 64):
- * every (group, kind, position) whose list entry is a selected body or a
- * cell containing one.  cparent: parent cell of each cell (-1 at a root).
- * hits: 3 longs per hit (group, kind 0 = point / 1 = quadrupole, position),
- * hmask: the selected bodies it depends on (bit s for sel[s]).  Returns the
- * number of hits (filled when hits != NULL and cap allows), -1 for nsel > 64.
- */
-long orc_fd_hits(long n, long ncells, const int *cparent, long ngroups, const long *pptr,
-                 const unsigned *plist, const long *qptr, const unsigned *qlist, int nsel,
-                 const long *sel, const long *body_leaf, long cap, long *hits,
-                 unsigned long long *hmask) {
-    if (nsel > 64)
-        return -1;
-    unsigned long long *mask = (unsigned long long *)calloc((size_t)(n + ncells), 8);
-    for (int s = 0; s < nsel; s++) {
-        unsigned long long bit = 1ull << s;
-        mask[sel[s]] |= bit;
-        for (long c = body_leaf[sel[s]]; c >= 0; c = cparent[c]) mask[n + c] |= bit;
-    }
-    long nh = 0;
-    for (long g = 0; g < ngroups; g++) {
-        for (int kind = 0; kind < 2; kind++) {
-            const long *ptr = kind ? qptr : pptr;
-            const unsigned *list = kind ? qlist : plist;
-            if (!ptr)
-                continue;
-            for (long e = ptr[g]; e < ptr[g + 1]; e++) {
-                long idx = (long)(list[e] & ORC_IDX_MASK) + (kind ? n : 0);
-                if (!mask[idx])
-                    continue;
-                if (hits && nh < cap) {
-                    hits[3 * nh] = g;
-                    hits[3 * nh + 1] = kind;
-                    hits[3 * nh + 2] = e;
-                    hmask[nh] = mask[idx];
-                }
-                nh++;
-            }
-        }
-    }
-    free(mask);
-    return nh;
-}
-
-/*
- * The part of L = sum_i w_i.a_i + u_i phi_i (FP64, fixed lists) that depends
- * on body j = sel[s]: every hit carrying bit s, over its group's sinks other
- * than j, plus sink j against its own group's whole lists.  The other terms
- * of L do not change when x_j or m_j does, so central differences of this
- * partial sum are those of L.  Cell moments come from the bodies (x, m),
- * so the caller perturbs x[3j + d] or m[j] and calls it twice.
- */
-double orc_fd_partial_loss(int s, long j, long n, const double *x, const double *m, long ncells,
-                           const long *cfirst, const int *ccount, long ngroups,
-                           const long *gfirst, const int *gcount, const long *body_group,
-                           const long *pptr, const unsigned *plist, const long *qptr,
-                           const unsigned *qlist, long nhits, const long *hits,
-                           const unsigned long long *hmask, const double *w, const double *u,
-                           double eps2) {
-    const unsigned long long bit = 1ull << s;
-    double L = 0.0;
-#pragma omp parallel for schedule(dynamic, 256) reduction(+ : L)
-    for (long h = 0; h < nhits; h++) {
-        if (!(hmask[h] & bit))
-            continue;
-        long g = hits[3 * h], kind = hits[3 * h + 1], e = hits[3 * h + 2];
-        unsigned idx = (kind ? qlist[e] : plist[e]) & ORC_IDX_MASK;
-        orc_mom mo;
-        const double *X;
-        double M;
-        if (!kind && (long)idx < n) {
-            X = x + 3 * (long)idx;
-            M = m[idx];
-        } else {
-            long c = kind ? (long)idx : (long)idx - n;
-            cell_moments(x, m, cfirst[c], ccount[c], &mo);
-            X = mo.X;
-            M = mo.M;
-        }
-        for (int k = 0; k < gcount[g]; k++) {
-            long i = gfirst[g] + k;
-            if (i == j)
-                continue;
-            double a[3] = {0, 0, 0}, phi = 0;
-            term64(x + 3 * i, X, M, mo.Q, (int)kind, eps2, a, &phi);
-            L += w[3 * i] * a[0] + w[3 * i + 1] * a[1] + w[3 * i + 2] * a[2] + u[i] * phi;
-        }
-    }
-    /* sink j over its own lists */
-    long g = body_group[j];
-    double a[3] = {0, 0, 0}, phi = 0;
-    for (long e = pptr[g]; e < pptr[g + 1]; e++) {
-        unsigned idx = plist[e] & ORC_IDX_MASK;
-        if ((long)idx < n) {
-            term64(x + 3 * j, x + 3 * (long)idx, m[idx], NULL, 0, eps2, a, &phi);
-        } else {
-            orc_mom mo;
-            cell_moments(x, m, cfirst[idx - n], ccount[idx - n], &mo);
-            term64(x + 3 * j, mo.X, mo.M, NULL, 0, eps2, a, &phi);
-        }
-    }
-    if (qptr)
-        for (long e = qptr[g]; e < qptr[g + 1]; e++) {
-            orc_mom mo;
-            long c = qlist[e] & ORC_IDX_MASK;
-            cell_moments(x, m, cfirst[c], ccount[c], &mo);
-            term64(x + 3 * j, mo.X, mo.M, mo.Q, 1, eps2, a, &phi);
-        }
-    L += w[3 * j] * a[0] + w[3 * j + 1] * a[1] + w[3 * j + 2] * a[2] + u[j] * phi;
-    return L;
-}
-
-/*
  * FP64 gradient of L = sum_i w_i.a_i + u_i phi_i for the Plummer-softened
  * direct sum over all pairs, the self pair included as the tree's lists
  * include it (it adds -m_i / eps to phi_i and nothing to a_i): dL/dx (3 per
@@ -733,4 +507,420 @@ void orc_direct_grad(long n, const double *x, const double *m, const double *w, 
         for (int k = 0; k < 3; k++) gx[3 * i + k] = g[k];
         gm[i] = gmi;
     }
+}
+
+/*
+ * ---- FP64 evaluation of fixed lists of every kind, periodic boxes included ----
+ *
+ * The general form of orc_lists_eval64: point (kind 0), quadrupole (1) and
+ * order-4 (2) lists and the periodic correction list (3), with the image
+ * shift of every entry.  Cells' moments come from their bodies in FP64:
+ * mass M, centre of mass X and the symmetric trace-free (STF) parts A_l of
+ * the raw moments sum m y^l (y = x - X), l = 2, 3, 4, held as full tensors
+ * of 3^l entries.  A cell of order L adds to its monopole term the exact
+ * harmonic terms of the Taylor series of 1/|d - y| (d = sink - source),
+ *     phi_l = -g_l <A_l, d^l> rho^-(2l+1),   g_l = (2l-1)!! / l!,
+ *     a_l   = g_l (l A_l.d^(l-1) rho^-(2l+1) - (2l+1) <A_l, d^l> rho^-(2l+3) d),
+ * with the Plummer rho^2 = |d|^2 + eps2 of the list kernels (nln/cofm.c
+ * normalises the same STF moments by R^l, :398-420, 486-562; the order-4
+ * kernel do_gravph_avx8, nln/do_grav_avx8.c:1779-1904, evaluates these
+ * terms in its own variables).  Correction-list entries (point-table
+ * records: a body, or a cell n + c standing for all of its bodies) add, for
+ * every body b of the entry, m_b C(y) to phi and m_b grad C(y) to a, with
+ * y = x_b + shift - x_sink and C(y) = Phi(y) + 1/|y| the periodic Green's
+ * function of orc_ewald less the nearest-image Newtonian term (C(0) its
+ * limit); every sink then adds -m_i (C(0) - pi/(alpha^2 L^3)), the self
+ * term the Ewald sum leaves out.  This is the exact sum the list kernels'
+ * cell moments and Taylor series approximate.
+ */
+#define ORC_IDX_MASK ((1u << 27) - 1u)
+
+typedef struct {
+    double M, X[3];
+    double A[3][81]; /* A_2, A_3, A_4 as full tensors, index i1*3^(l-1) + ... + il */
+} orc_momx;
+
+static const int orc_pow3[5] = {1, 3, 9, 27, 81};
+
+/* STF part of the full symmetric tensor T of order l (2..4) into A. */
+static void stf_project(int l, const double *T, double *A) {
+    if (l == 2) {
+        double tr = (T[0] + T[4] + T[8]) / 3.0;
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) A[3 * i + j] = T[3 * i + j] - (i == j ? tr : 0.0);
+    } else if (l == 3) {
+        double t[3];
+        for (int k = 0; k < 3; k++) t[k] = T[9 * k + 0] + T[9 * k + 4] + T[9 * k + 8];
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++)
+                for (int k = 0; k < 3; k++)
+                    A[9 * i + 3 * j + k] = T[9 * i + 3 * j + k] -
+                                           ((i == j ? t[k] : 0.0) + (i == k ? t[j] : 0.0) +
+                                            (j == k ? t[i] : 0.0)) / 5.0;
+    } else {
+        double t2[9], tt = 0.0;
+        for (int k = 0; k < 3; k++)
+            for (int q = 0; q < 3; q++)
+                t2[3 * k + q] = T[27 * k + 9 * q + 0] + T[27 * k + 9 * q + 4] + T[27 * k + 9 * q + 8];
+        tt = t2[0] + t2[4] + t2[8];
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++)
+                for (int k = 0; k < 3; k++)
+                    for (int q = 0; q < 3; q++) {
+                        double s6 = (i == j ? t2[3 * k + q] : 0.0) + (i == k ? t2[3 * j + q] : 0.0) +
+                                    (i == q ? t2[3 * j + k] : 0.0) + (j == k ? t2[3 * i + q] : 0.0) +
+                                    (j == q ? t2[3 * i + k] : 0.0) + (k == q ? t2[3 * i + j] : 0.0);
+                        double s3 = (i == j && k == q ? 1.0 : 0.0) + (i == k && j == q ? 1.0 : 0.0) +
+                                    (i == q && j == k ? 1.0 : 0.0);
+                        A[27 * i + 9 * j + 3 * k + q] =
+                            T[27 * i + 9 * j + 3 * k + q] - s6 / 7.0 + s3 * tt / 35.0;
+                    }
+    }
+}
+
+static void cell_momx(const double *x, const double *m, long first, int count, orc_momx *o) {
+    double M = 0, s[3] = {0, 0, 0};
+    for (long b = first; b < first + count; b++) {
+        M += m[b];
+        for (int d = 0; d < 3; d++) s[d] += m[b] * x[3 * b + d];
+    }
+    o->M = M;
+    for (int d = 0; d < 3; d++) o->X[d] = M > 0 ? s[d] / M : 0.0;
+    double T[81];
+    for (int l = 2; l <= 4; l++) {
+        memset(T, 0, sizeof(T));
+        for (long b = first; b < first + count; b++) {
+            double y[3] = {x[3 * b] - o->X[0], x[3 * b + 1] - o->X[1], x[3 * b + 2] - o->X[2]};
+            for (int t = 0; t < orc_pow3[l]; t++) {
+                double p = m[b];
+                for (int k = 0, r = t; k < l; k++, r /= 3) p *= y[r % 3];
+                T[t] += p;
+            }
+        }
+        stf_project(l, T, o->A[l - 2]);
+    }
+}
+
+/* Monopole plus orders 2..order of a cell at X (M, A) on a sink at s. */
+static void termx(const double *s, const double *X, double M, const orc_momx *c, int order,
+                  double eps2, double *a, double *phi) {
+    const double d[3] = {s[0] - X[0], s[1] - X[1], s[2] - X[2]};
+    const double rho2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + eps2;
+    const double ri = 1.0 / sqrt(rho2), ri2 = ri * ri;
+    *phi -= M * ri;
+    for (int k = 0; k < 3; k++) a[k] -= M * d[k] * ri * ri2;
+    static const double g[5] = {0, 0, 1.5, 2.5, 4.375};
+    for (int l = 2; l <= order; l++) {
+        const double *A = c->A[l - 2];
+        double P = 0.0, E[3] = {0, 0, 0};
+        for (int t = 0; t < orc_pow3[l]; t++) {
+            /* t = i1 * 3^(l-1) + rest: E_i1 takes the rest's monomial */
+            double mono = 1.0;
+            int r = t;
+            for (int k = 0; k < l - 1; k++, r /= 3) mono *= d[r % 3];
+            const int i1 = r % 3;
+            E[i1] += A[t] * mono;
+            P += A[t] * mono * d[i1];
+        }
+        const int n = 2 * l + 1;
+        const double rn = pow(ri, n), rn2 = rn * ri2;
+        *phi -= g[l] * P * rn;
+        for (int k = 0; k < 3; k++) a[k] += g[l] * (l * E[k] * rn - n * P * rn2 * d[k]);
+    }
+}
+
+static void decode_shift64(unsigned code, double box, double *sh) {
+    sh[0] = ((int)(code / 9) - 1) * box;
+    sh[1] = ((int)(code / 3 % 3) - 1) * box;
+    sh[2] = ((int)(code % 3) - 1) * box;
+}
+
+/* C(0) = lim_{y->0} Phi(y) + 1/|y| of orc_ewald's sum (the n = 0 real-space
+   term erfc(alpha r)/r - 1/r tends to -2 alpha/sqrt(pi)). */
+double orc_ewald_c0(double L) {
+    const int N = 4;
+    double alpha = 2.0 / L;
+    double phi = M_PI / (alpha * alpha * L * L * L) + 2.0 * alpha / sqrt(M_PI);
+    double a2 = -M_PI * M_PI / (alpha * alpha * L * L), a5 = 1.0 / (M_PI * L);
+    for (int i = -N; i <= N; i++)
+        for (int j = -N; j <= N; j++)
+            for (int k = -N; k <= N; k++) {
+                double r = L * sqrt((double)(i * i + j * j + k * k));
+                if (r == 0.0 || r > 4.0 * L)
+                    continue;
+                phi -= erfc(alpha * r) / r;
+            }
+    for (int i = -N; i <= N; i++)
+        for (int j = -N; j <= N; j++)
+            for (int k = -N; k <= N; k++) {
+                double hh = (double)(i * i + j * j + k * k);
+                if (hh > 16 || hh == 0)
+                    continue;
+                phi -= a5 * exp(a2 * hh) / hh;
+            }
+    return phi;
+}
+
+/* One body of mass mb at y (source + shift - sink) through the correction C. */
+static void corr_body(const double *y, double mb, double L, double c0, double *a, double *phi) {
+    if (y[0] == 0.0 && y[1] == 0.0 && y[2] == 0.0) {
+        *phi += mb * c0;
+        return;
+    }
+    double f[3], p;
+    orc_ewald(y, L, f, &p);
+    const double r2 = y[0] * y[0] + y[1] * y[1] + y[2] * y[2], r = sqrt(r2);
+    *phi += mb * (p + 1.0 / r);
+    for (int k = 0; k < 3; k++) a[k] += mb * (f[k] - y[k] / (r2 * r));
+}
+
+/* Lists of one group, as the arrays of the general evaluators. */
+typedef struct {
+    long n, ncells;
+    const double *x, *m;
+    const long *cfirst;
+    const int *ccount;
+    const long *ptr[4];
+    const unsigned *list[4];
+    double eps2, box;
+    int ewald;
+    double c0, self;
+} orc_lx;
+
+/* (a, phi) of sink i over group g's lists; moms: every cell's moments. */
+static void sink_lists(const orc_lx *P, const orc_momx *moms, long g, long i, double *a,
+                       double *phi) {
+    const double *s = P->x + 3 * i;
+    for (int kind = 0; kind < 3; kind++) {
+        if (!P->ptr[kind])
+            continue;
+        for (long e = P->ptr[kind][g]; e < P->ptr[kind][g + 1]; e++) {
+            const unsigned ent = P->list[kind][e], idx = ent & ORC_IDX_MASK;
+            double sh[3], X[3];
+            decode_shift64(ent >> 27, P->box, sh);
+            if (kind == 0 && (long)idx < P->n) {
+                for (int k = 0; k < 3; k++) X[k] = P->x[3 * (long)idx + k] + sh[k];
+                termx(s, X, P->m[idx], NULL, 0, P->eps2, a, phi);
+            } else {
+                const orc_momx *c = &moms[kind == 0 ? (long)idx - P->n : (long)idx];
+                for (int k = 0; k < 3; k++) X[k] = c->X[k] + sh[k];
+                termx(s, X, c->M, c, kind == 0 ? 0 : kind == 1 ? 2 : 4, P->eps2, a, phi);
+            }
+        }
+    }
+    if (P->ewald && P->ptr[3]) {
+        for (long e = P->ptr[3][g]; e < P->ptr[3][g + 1]; e++) {
+            const unsigned ent = P->list[3][e], idx = ent & ORC_IDX_MASK;
+            double sh[3];
+            decode_shift64(ent >> 27, P->box, sh);
+            long b0 = idx, b1 = (long)idx + 1;
+            if ((long)idx >= P->n) {
+                b0 = P->cfirst[idx - P->n];
+                b1 = b0 + P->ccount[idx - P->n];
+            }
+            for (long b = b0; b < b1; b++) {
+                double y[3];
+                for (int k = 0; k < 3; k++) y[k] = P->x[3 * b + k] + sh[k] - s[k];
+                corr_body(y, P->m[b], P->box, P->c0, a, phi);
+            }
+        }
+        *phi -= P->m[i] * P->self;
+    }
+}
+
+static void lx_init(orc_lx *P, long n, const double *x, const double *m, long ncells,
+                    const long *cfirst, const int *ccount, const long *const *ptr,
+                    const unsigned *const *list, double eps2, double box, int ewald) {
+    P->n = n;
+    P->ncells = ncells;
+    P->x = x;
+    P->m = m;
+    P->cfirst = cfirst;
+    P->ccount = ccount;
+    for (int k = 0; k < 4; k++) {
+        P->ptr[k] = ptr[k];
+        P->list[k] = list[k];
+    }
+    P->eps2 = eps2;
+    P->box = box;
+    P->ewald = ewald && box > 0.0;
+    P->c0 = P->ewald ? orc_ewald_c0(box) : 0.0;
+    P->self = P->ewald ? P->c0 - M_PI / (4.0 / (box * box) * box * box * box) : 0.0;
+}
+
+/*
+ * out (4 doubles per body, tree order) = (a, phi) of every sink over its
+ * group's lists of every kind (ptr[k] / list[k] NULL for a kind without
+ * lists; k = 0 P, 1 Q, 2 H, 3 correction, the last only with ewald and
+ * box > 0).
+ */
+void orc_lists_eval64x(long n, const double *x, const double *m, long ncells, const long *cfirst,
+                       const int *ccount, long ngroups, const long *gfirst, const int *gcount,
+                       const long *const *ptr, const unsigned *const *list, double eps2,
+                       double box, int ewald, double *out) {
+    orc_lx P;
+    lx_init(&P, n, x, m, ncells, cfirst, ccount, ptr, list, eps2, box, ewald);
+    orc_momx *mom = (orc_momx *)malloc(sizeof(orc_momx) * (size_t)(ncells > 0 ? ncells : 1));
+#pragma omp parallel for schedule(dynamic, 64)
+    for (long c = 0; c < ncells; c++) cell_momx(x, m, cfirst[c], ccount[c], &mom[c]);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long g = 0; g < ngroups; g++) {
+        for (int k = 0; k < gcount[g]; k++) {
+            long i = gfirst[g] + k;
+            double a[3] = {0, 0, 0}, phi = 0;
+            sink_lists(&P, mom, g, i, a, &phi);
+            for (int d = 0; d < 3; d++) out[4 * i + d] = a[d];
+            out[4 * i + 3] = phi;
+        }
+    }
+    free(mom);
+}
+
+/*
+ * The entries of every kind that depend on the selected bodies sel[0..nsel)
+ * (nsel <= 64), as orc_fd_hits: 3 longs per hit (group, kind 0..3,
+ * position) and the mask of the selected bodies it depends on.  Point and
+ * correction entries are point-table records (bodies, cells n + c);
+ * quadrupole and order-4 entries are cells.
+ */
+long orc_fd_hits_x(long n, long ncells, const int *cparent, long ngroups, const long *const *ptr,
+                   const unsigned *const *list, int nsel, const long *sel, const long *body_leaf,
+                   long cap, long *hits, unsigned long long *hmask) {
+    if (nsel > 64)
+        return -1;
+    unsigned long long *mask = (unsigned long long *)calloc((size_t)(n + ncells), 8);
+    for (int s = 0; s < nsel; s++) {
+        unsigned long long bit = 1ull << s;
+        mask[sel[s]] |= bit;
+        for (long c = body_leaf[sel[s]]; c >= 0; c = cparent[c]) mask[n + c] |= bit;
+    }
+    long nh = 0;
+    for (long g = 0; g < ngroups; g++) {
+        for (int kind = 0; kind < 4; kind++) {
+            if (!ptr[kind])
+                continue;
+            for (long e = ptr[kind][g]; e < ptr[kind][g + 1]; e++) {
+                long idx = (long)(list[kind][e] & ORC_IDX_MASK) + (kind == 1 || kind == 2 ? n : 0);
+                if (!mask[idx])
+                    continue;
+                if (hits && nh < cap) {
+                    hits[3 * nh] = g;
+                    hits[3 * nh + 1] = kind;
+                    hits[3 * nh + 2] = e;
+                    hmask[nh] = mask[idx];
+                }
+                nh++;
+            }
+        }
+    }
+    free(mask);
+    return nh;
+}
+
+/*
+ * The part of L = sum_i w_i.a_i + u_i phi_i (orc_lists_eval64x's sums,
+ * fixed lists) that depends on body j = sel[s], as orc_fd_partial_loss:
+ * every hit carrying bit s over its group's sinks other than j (for a
+ * correction entry only body j's own term, the entry's other bodies being
+ * constant), plus sink j over its own group's whole lists.
+ */
+double orc_fd_partial_loss_x(int s, long j, long n, const double *x, const double *m, long ncells,
+                             const long *cfirst, const int *ccount, long ngroups,
+                             const long *gfirst, const int *gcount, const long *body_group,
+                             const long *const *ptr, const unsigned *const *list, long nhits,
+                             const long *hits, const unsigned long long *hmask, const double *w,
+                             const double *u, double eps2, double box, int ewald) {
+    orc_lx P;
+    lx_init(&P, n, x, m, ncells, cfirst, ccount, ptr, list, eps2, box, ewald);
+    const unsigned long long bit = 1ull << s;
+    double L = 0.0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : L)
+    for (long h = 0; h < nhits; h++) {
+        if (!(hmask[h] & bit))
+            continue;
+        const long g = hits[3 * h], kind = hits[3 * h + 1], e = hits[3 * h + 2];
+        const unsigned ent = list[kind][e], idx = ent & ORC_IDX_MASK;
+        double sh[3];
+        decode_shift64(ent >> 27, box, sh);
+        orc_momx mo;
+        double X[3], M = 0.0;
+        int order = 0, corr = kind == 3;
+        if (corr) {
+            if (!P.ewald)
+                continue;
+            for (int k = 0; k < 3; k++) X[k] = x[3 * j + k] + sh[k];
+            M = m[j];
+        } else if (kind == 0 && (long)idx < n) {
+            for (int k = 0; k < 3; k++) X[k] = x[3 * (long)idx + k] + sh[k];
+            M = m[idx];
+        } else {
+            const long c = kind == 0 ? (long)idx - n : (long)idx;
+            cell_momx(x, m, cfirst[c], ccount[c], &mo);
+            for (int k = 0; k < 3; k++) X[k] = mo.X[k] + sh[k];
+            M = mo.M;
+            order = kind == 0 ? 0 : kind == 1 ? 2 : 4;
+        }
+        for (int k = 0; k < gcount[g]; k++) {
+            long i = gfirst[g] + k;
+            if (i == j)
+                continue;
+            double a[3] = {0, 0, 0}, phi = 0;
+            if (corr) {
+                double y[3] = {X[0] - x[3 * i], X[1] - x[3 * i + 1], X[2] - x[3 * i + 2]};
+                corr_body(y, M, box, P.c0, a, &phi);
+            } else {
+                termx(x + 3 * i, X, M, &mo, order, eps2, a, &phi);
+            }
+            L += w[3 * i] * a[0] + w[3 * i + 1] * a[1] + w[3 * i + 2] * a[2] + u[i] * phi;
+        }
+    }
+    /* sink j over its own lists, cells' moments from the bodies */
+    const long g = body_group[j];
+    double a[3] = {0, 0, 0}, phi = 0;
+    orc_momx *moms = (orc_momx *)calloc((size_t)(ncells > 0 ? ncells : 1), sizeof(orc_momx));
+    char *done = (char *)calloc((size_t)(ncells > 0 ? ncells : 1), 1);
+    for (int kind = 0; kind < 3; kind++) {
+        if (!ptr[kind])
+            continue;
+        for (long e = ptr[kind][g]; e < ptr[kind][g + 1]; e++) {
+            const unsigned idx = list[kind][e] & ORC_IDX_MASK;
+            if (kind == 0 && (long)idx < n)
+                continue;
+            const long c = kind == 0 ? (long)idx - n : (long)idx;
+            if (!done[c]) {
+                cell_momx(x, m, cfirst[c], ccount[c], &moms[c]);
+                done[c] = 1;
+            }
+        }
+    }
+    orc_lx Q = P;
+    Q.ewald = 0;
+    sink_lists(&Q, moms, g, j, a, &phi);
+    if (P.ewald && ptr[3]) {
+        double lc = 0.0;
+        const long e0 = ptr[3][g], e1 = ptr[3][g + 1];
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : lc)
+        for (long e = e0; e < e1; e++) {
+            const unsigned ent = list[3][e], idx = ent & ORC_IDX_MASK;
+            double sh[3];
+            decode_shift64(ent >> 27, box, sh);
+            long b0 = idx, b1 = (long)idx + 1;
+            if ((long)idx >= n) {
+                b0 = cfirst[idx - n];
+                b1 = b0 + ccount[idx - n];
+            }
+            double ae[3] = {0, 0, 0}, pe = 0.0;
+            for (long b = b0; b < b1; b++) {
+                double y[3];
+                for (int k = 0; k < 3; k++) y[k] = x[3 * b + k] + sh[k] - x[3 * j + k];
+                corr_body(y, m[b], box, P.c0, ae, &pe);
+            }
+            lc += w[3 * j] * ae[0] + w[3 * j + 1] * ae[1] + w[3 * j + 2] * ae[2] + u[j] * pe;
+        }
+        L += lc - u[j] * m[j] * P.self;
+    }
+    free(moms);
+    free(done);
+    L += w[3 * j] * a[0] + w[3 * j + 1] * a[1] + w[3 * j + 2] * a[2] + u[j] * phi;
+    return L;
 }

@@ -97,18 +97,20 @@ def orc():
         lib.orc_groups_eval.argtypes = [ctypes.c_int, _f32p, ctypes.c_int, _i64p, _i64p, _i64p,
                                         _i32p, ctypes.c_long, _f32p, ctypes.c_float, _f64p]
         L_, vp = ctypes.c_long, ctypes.c_void_p
-        lib.orc_lists_eval64.argtypes = [L_, _f64p, _f64p, L_, _i64p, _i32p, L_, _i64p, _i32p,
-                                         _i64p, _u32p, vp, vp, ctypes.c_double, _f64p]
-        lib.orc_lists_eval64.restype = ctypes.c_int
-        lib.orc_fd_hits.argtypes = [L_, L_, _i32p, L_, _i64p, _u32p, vp, vp, ctypes.c_int, _i64p,
-                                    _i64p, L_, vp, vp]
-        lib.orc_fd_hits.restype = L_
-        lib.orc_fd_partial_loss.argtypes = [ctypes.c_int, L_, L_, _f64p, _f64p, L_, _i64p, _i32p,
-                                            L_, _i64p, _i32p, _i64p, _i64p, _u32p, vp, vp, L_,
-                                            _i64p, np.ctypeslib.ndpointer(np.uint64,
-                                                                         flags="C_CONTIGUOUS"),
-                                            _f64p, _f64p, ctypes.c_double]
-        lib.orc_fd_partial_loss.restype = ctypes.c_double
+        pp = ctypes.POINTER(ctypes.c_void_p)
+        lib.orc_lists_eval64x.argtypes = [L_, _f64p, _f64p, L_, _i64p, _i32p, L_, _i64p, _i32p,
+                                          pp, pp, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                          _f64p]
+        lib.orc_fd_hits_x.argtypes = [L_, L_, _i32p, L_, pp, pp, ctypes.c_int, _i64p, _i64p, L_,
+                                      vp, vp]
+        lib.orc_fd_hits_x.restype = L_
+        lib.orc_fd_partial_loss_x.argtypes = [
+            ctypes.c_int, L_, L_, _f64p, _f64p, L_, _i64p, _i32p, L_, _i64p, _i32p, _i64p, pp,
+            pp, L_, _i64p, np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS"), _f64p, _f64p,
+            ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        lib.orc_fd_partial_loss_x.restype = ctypes.c_double
+        lib.orc_ewald_c0.argtypes = [ctypes.c_double]
+        lib.orc_ewald_c0.restype = ctypes.c_double
         lib.orc_direct_grad.argtypes = [L_, _f64p, _f64p, _f64p, _f64p, ctypes.c_double, _f64p,
                                         _f64p]
         _orc = lib
@@ -245,17 +247,18 @@ def tree_eval(tree, eps2, quad_kind=QUAD_PLUMMER_P, hexa_kind=HEXA_PLUMMER, mono
 
 # ---------------------------------------------------------------- FP64 list checks
 class ListsFP64:
-    """FP64 evaluation of a walked isolated tree's batched index lists with
-    every cell's moments recomputed from the bodies (orc_lists_eval64), and
-    central differences of L = sum w.a + u phi restricted to the terms that
-    depend on one body (orc_fd_hits / orc_fd_partial_loss): the checker of
-    the hand-written adjoint.  Point and quadrupole lists only."""
+    """FP64 evaluation of a walked tree's batched index lists of every kind
+    (points, quadrupole and order-4 cells, the periodic correction list,
+    image shifts) with every cell's moments recomputed from the bodies
+    (orc_lists_eval64x), and central differences of L = sum w.a + u phi
+    restricted to the terms that depend on one body (orc_fd_hits_x /
+    orc_fd_partial_loss_x): the checker of the hand-written adjoint.
+    ewald: apply the correction list (periodic trees that carry one)."""
 
-    def __init__(self, tree):
+    def __init__(self, tree, ewald=True):
         self.t = t = tree
-        if len(t.hlist):
-            raise ValueError("order-4 lists are not covered by the FP64 list checker")
         self.n, self.nc, self.ng = int(t.n), int(t.ncells), int(t.ngroups)
+        self.box = float(getattr(t, "box", 0.0) or 0.0)
         first, count = t.cell_ranges()
         child, nchild, _ = t.cell_links()
         self.cfirst = np.ascontiguousarray(first, np.int64)
@@ -273,51 +276,55 @@ class ListsFP64:
         self.gfirst = np.ascontiguousarray(t.groups["first"], np.int64)
         self.gcount = np.ascontiguousarray(t.groups["count"], np.int32)
         self.bgroup = np.repeat(np.arange(self.ng, dtype=np.int64), self.gcount)
-        self.pptr = np.ascontiguousarray(t.ptr[0], np.int64)
-        self.plist = np.ascontiguousarray(t.plist, np.uint32)
-        self.has_q = len(t.qlist) > 0
-        self.qptr = np.ascontiguousarray(t.ptr[1], np.int64)
-        self.qlist = np.ascontiguousarray(t.qlist if self.has_q else np.zeros(1, np.uint32))
-
-    def _q(self):
-        return (self.qptr.ctypes.data, self.qlist.ctypes.data) if self.has_q else (None, None)
+        lists = [t.plist, t.qlist, t.hlist, getattr(t, "clist", np.zeros(0, np.uint32))]
+        self._keep = []
+        ptrs, datas = [], []
+        for k in range(4):
+            has = len(lists[k]) > 0 and (k < 3 or (ewald and self.box > 0))
+            if has:
+                pk = np.ascontiguousarray(t.ptr[k], np.int64)
+                lk = np.ascontiguousarray(lists[k], np.uint32)
+                self._keep += [pk, lk]
+                ptrs.append(pk.ctypes.data)
+                datas.append(lk.ctypes.data)
+            else:
+                ptrs.append(None)
+                datas.append(None)
+        self.ewald = int(ptrs[3] is not None)
+        self.ptrs = (ctypes.c_void_p * 4)(*ptrs)
+        self.lists = (ctypes.c_void_p * 4)(*datas)
 
     def eval(self, x, m, eps2):
         """(n, 4) FP64 (ax, ay, az, phi), tree order, positions x (n, 3) and masses m."""
         x = np.ascontiguousarray(x, np.float64)
         m = np.ascontiguousarray(m, np.float64)
         out = np.zeros((self.n, 4))
-        qp, ql = self._q()
-        rc = orc().orc_lists_eval64(self.n, x.ravel(), m, self.nc, self.cfirst, self.ccount,
-                                    self.ng, self.gfirst, self.gcount, self.pptr, self.plist,
-                                    qp, ql, float(eps2), out.ravel())
-        if rc:
-            raise ValueError("periodic image codes are not covered")
+        orc().orc_lists_eval64x(self.n, x.ravel(), m, self.nc, self.cfirst, self.ccount, self.ng,
+                                self.gfirst, self.gcount, self.ptrs, self.lists, float(eps2),
+                                self.box, self.ewald, out.ravel())
         return out
 
     def select(self, bodies):
         """Prepare central differences for up to 64 bodies (tree order)."""
         self.sel = np.ascontiguousarray(bodies, np.int64)
-        qp, ql = self._q()
-        args = (self.n, self.nc, self.parent, self.ng, self.pptr, self.plist, qp, ql,
-                len(self.sel), self.sel, self.leaf)
-        nh = orc().orc_fd_hits(*args, 0, None, None)
+        args = (self.n, self.nc, self.parent, self.ng, self.ptrs, self.lists, len(self.sel),
+                self.sel, self.leaf)
+        nh = orc().orc_fd_hits_x(*args, 0, None, None)
         if nh < 0:
             raise ValueError("at most 64 selected bodies")
         self.hits = np.zeros(3 * max(nh, 1), np.int64)
         self.hmask = np.zeros(max(nh, 1), np.uint64)
-        orc().orc_fd_hits(*args, nh, self.hits.ctypes.data, self.hmask.ctypes.data)
+        orc().orc_fd_hits_x(*args, nh, self.hits.ctypes.data, self.hmask.ctypes.data)
         self.nhits = nh
 
     def partial_loss(self, s, x, m, w, u, eps2):
         """The part of L that depends on selected body s (index into select()'s list)."""
-        qp, ql = self._q()
-        return orc().orc_fd_partial_loss(
+        return orc().orc_fd_partial_loss_x(
             int(s), int(self.sel[s]), self.n, np.ascontiguousarray(x, np.float64).ravel(),
             np.ascontiguousarray(m, np.float64), self.nc, self.cfirst, self.ccount, self.ng,
-            self.gfirst, self.gcount, self.bgroup, self.pptr, self.plist, qp, ql, self.nhits,
-            self.hits, self.hmask, np.ascontiguousarray(w, np.float64).ravel(),
-            np.ascontiguousarray(u, np.float64), float(eps2))
+            self.gfirst, self.gcount, self.bgroup, self.ptrs, self.lists, self.nhits, self.hits,
+            self.hmask, np.ascontiguousarray(w, np.float64).ravel(),
+            np.ascontiguousarray(u, np.float64), float(eps2), self.box, self.ewald)
 
     def fd_grad(self, x, m, w, u, eps2, coords, h=1e-6, mass_rel=False):
         """Central differences of L for (selected body s, component c) pairs;
@@ -345,6 +352,11 @@ class ListsFP64:
                 m[j] = m0
                 out.append((lp - lm) / (2 * hh))
         return np.array(out)
+
+
+def ewald_c0(L):
+    """C(0) = lim Phi(y) + 1/|y| of the Ewald sum in a cube of side L."""
+    return orc().orc_ewald_c0(float(L))
 
 
 def direct_grad(x, m, w, u, eps2):

@@ -1,7 +1,8 @@
 """GPU: the hand-written adjoint (csrc/adjoint.cuh) against FP64 central
-differences of an FP64 evaluation of the same interaction lists, against
-the analytic FP64 direct-sum gradient, and through checkpointed leapfrog
-steps (pgrav/autograd.py)."""
+differences of an FP64 evaluation of the same interaction lists (point,
+quadrupole and order-4 cells; periodic boxes with image shifts and the
+Ewald correction), against the analytic FP64 direct-sum gradient, and
+through checkpointed leapfrog steps (pgrav/autograd.py)."""
 import numpy as np
 import pytest
 
@@ -102,6 +103,82 @@ def test_adjoint_matches_central_differences(monkeypatch):
     fdm = np.array(fdm)
     mscale = np.sqrt(np.mean(gm ** 2))
     assert np.abs(gm[mpicks] - fdm).max() < 2e-4 * mscale, (np.abs(gm[mpicks] - fdm).max() / mscale)
+
+
+def _adjoint_vs_oracle_fd(pos, m, eps2, tkw, nsel, seed, ewald=False):
+    """The GPU adjoint (through pgrav.autograd) at nsel bodies against FP64
+    central differences of the oracle's evaluation of the same lists
+    (ListsFP64, every cell's moments from the bodies).  Returns the largest
+    position and mass errors, each over the rms of that gradient, and the
+    FD values themselves."""
+    import torch
+    from oracle import oracle as O
+    from pgrav import autograd as AG, host
+    n = len(pos)
+    rng = np.random.default_rng(seed)
+    w = rng.normal(size=(n, 3))
+    u = rng.normal(size=n)
+    kw = dict(tkw)
+    if ewald:
+        kw["ewald"] = True
+    p = torch.tensor(pos, dtype=torch.float32, device="cuda", requires_grad=True)
+    mm = torch.tensor(m, dtype=torch.float32, device="cuda", requires_grad=True)
+    a, phi = AG.gravity(p, mm, eps2, **kw)
+    L = (torch.tensor(w, dtype=torch.float32, device="cuda") * a).sum() + \
+        (torch.tensor(u, dtype=torch.float32, device="cuda") * phi).sum()
+    L.backward()
+    gx = p.grad.cpu().numpy().astype(np.float64)
+    gm = mm.grad.cpu().numpy().astype(np.float64)
+    t = host.Tree(pos, m, **tkw)
+    o = np.asarray(t.order)
+    chk = O.ListsFP64(t, ewald=ewald)
+    sel = rng.choice(n, nsel, replace=False)     # tree positions
+    chk.select(sel)
+    xt = np.asarray(t.sorted_pos, np.float64)
+    mt = np.asarray(t.points[:n, 3], np.float64)
+    coords = [(s, c) for s in range(nsel) for c in (0, 1, 2, 3)]
+    fd = chk.fd_grad(xt, mt, w[o], u[o], eps2, coords, h=1e-6, mass_rel=True).reshape(nsel, 4)
+    ad = np.concatenate([gx[o[sel]], gm[o[sel]][:, None]], 1)
+    scale = np.array([np.sqrt(np.mean(gx ** 2))] * 3 + [np.sqrt(np.mean(gm ** 2))])
+    ex = np.abs(ad[:, :3] - fd[:, :3]).max() / scale[0]
+    em = np.abs(ad[:, 3] - fd[:, 3]).max() / scale[3]
+    return ex, em, dict(fd=fd, ad=ad, scale=scale, tree=t, sel=sel, w=w[o], u=u[o], x=xt, m=mt,
+                        coords=coords)
+
+
+def test_adjoint_order4_matches_central_differences():
+    """Order-4 cells (p4cut = 20): the trace-free moment duals, their chain
+    through the centre of mass, and the pair terms of orders 2..4."""
+    from pgrav import host, ics
+    pos, m = ics.plummer(4000, seed=34)
+    tkw = dict(tol=1e-3, p2cut=7, p4cut=20, leaf_max=8)
+    t = host.Tree(pos, m, **tkw)
+    assert t.counts[3] > 0.1 * t.counts.sum()   # order-4 interactions carry weight
+    ex, em, _ = _adjoint_vs_oracle_fd(pos, m, 1e-4, tkw, 16, 35)
+    assert ex < 2e-4 and em < 2e-4, (ex, em)
+
+
+def test_adjoint_periodic_matches_central_differences():
+    """A periodic 16^3 box with order-4 cells, image shifts and the Ewald
+    correction.  The oracle sums the correction exactly over each entry's
+    bodies; the kernels use cell moments and each group's Taylor series of
+    it, so the bar is that truncation (the correction itself moves the
+    gradient by far more)."""
+    from pgrav import ics
+    n1 = 16
+    pos, m = ics.grf_box(n1, seed=36)
+    eps2 = (1.0 / n1 / 50) ** 2
+    tkw = dict(tol=1e-5, p2cut=7, p4cut=20, leaf_max=8, group_max=16, box=1.0)
+    ex, em, r = _adjoint_vs_oracle_fd(pos, m, eps2, tkw, 8, 37, ewald=True)
+    assert ex < 3e-3 and em < 3e-3, (ex, em)
+    # the correction's share of the gradient is far above that bar
+    from oracle import oracle as O
+    chk0 = O.ListsFP64(r["tree"], ewald=False)
+    chk0.select(r["sel"])
+    fd0 = chk0.fd_grad(r["x"], r["m"], r["w"], r["u"], eps2, r["coords"], h=1e-6,
+                       mass_rel=True).reshape(-1, 4)
+    share = np.abs(r["fd"] - fd0).max(0) / r["scale"]
+    assert share[:3].max() > 10 * ex and share[3] > 10 * em, (share, ex, em)
 
 
 def direct_grad(x, m, eps2, w, u, block=512):
