@@ -1062,6 +1062,9 @@ extern "C" int grav_plan_adjoint_CUDA(grav_plan *pl, const float *wu, float *gra
     if (pl->plain)
         return gc::set_status(-1, "grav_plan_adjoint_CUDA: the mixed-precision form only "
                                   "(grav_problem.precision = 0)");
+    if (pl->dp.ewald && !pl->evaluated)
+        return gc::set_status(-1, "grav_plan_adjoint_CUDA: evaluate the plan first (the "
+                                  "periodic correction's adjoint reads its group moments)");
     cudaStream_t st = (cudaStream_t)stream;
     const int64_t nb = pl->hp.nbodies, nc = pl->hp.ncells, ng = pl->hp.ngroups;
     grav_step_state *S = pl->step;

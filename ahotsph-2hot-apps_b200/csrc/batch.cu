@@ -1059,6 +1059,9 @@ struct grav_plan {
     int64_t *order = nullptr;           // device-built plans: tree position -> input index
     bool staged = false;                // the Q/H tensor maps view pre-staged tables
     bool plain = false;                 // plain FP32 kernels (grav_problem.precision = 1)
+    int integrator = 0;                 // 0: Integrate, 1: CosmoIntegrate (step.cuh)
+    bool evaluated = false;             // grav_groups_eval_CUDA has been enqueued (the
+                                        // correction moments the adjoint reads are set)
     float4 *qstage = nullptr, *hstage = nullptr;  // pre-staged cell tables (k_stage_cells)
     grav_step_state *step = nullptr;  // tree links, refit scratch and the step graph
     grav_adjoint_state *adj = nullptr;  // adjoint scratch
@@ -1918,6 +1921,7 @@ extern "C" int grav_groups_eval_CUDA(grav_plan *pl, void *stream) {
             return rc;
     if (int rc = launch_finish(pl, df, st, forked))
         return rc;
+    pl->evaluated = true;
     return mark(4);
 }
 

@@ -227,28 +227,61 @@ __global__ void k_refit_tables(const double *__restrict__ raw, int64_t ncells, i
     }
 }
 
-// params = {dt, dtv, dtsync}; energy += {sum m vc.vc, sum m phi}
+// Integrate (nln/integrate.c:16-59), COSMO = false: params = {dt, dtv,
+// dtsync}; vc = v + dtsync a, v += dtv a, x += dt v.
+// CosmoIntegrate (nln/integrate.c:82-135), COSMO = true: params = {kick to
+// the positions' time, kick, drift, 1/a0, a1, 1/a0^2}; vc = v + p0 a,
+// v += p1 a, x = a1 (x / a0 + drift v) with the reference's three roundings
+// to FP32 (its output position is a float written three times), ke scaled
+// by 1/a0^2 per body.  Both accumulate energy += {sum m vc.vc, sum m phi};
+// positions and velocities are formed in FP64 without fused multiply-adds
+// and rounded to FP32, as the reference's double expressions stored to
+// floats.
+template <bool COSMO>
 __global__ void k_integrate(float4 *__restrict__ pts, const float4 *__restrict__ acc,
                             float4 *__restrict__ vel, int64_t n, const double *__restrict__ params,
                             double *__restrict__ energy) {
-    const double dt = params[0], dtv = params[1], dtsync = params[2];
+    double p[6];
+    if (COSMO) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) p[k] = params[k];
+    } else {
+        p[0] = params[2];  // dtsync
+        p[1] = params[1];  // dtv
+        p[2] = params[0];  // dt
+        p[3] = p[4] = p[5] = 1.0;
+    }
     double ke = 0.0, pe = 0.0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        float4 p = pts[i];
+        float4 x = pts[i];
         const float4 a = acc[i];
         float4 v = vel[i];
-        const double vx = v.x + dtsync * a.x, vy = v.y + dtsync * a.y, vz = v.z + dtsync * a.z;
-        ke += p.w * (vx * vx + vy * vy + vz * vz);
-        pe += (double)p.w * a.w;
-        v.x = (float)(v.x + dtv * a.x);
-        v.y = (float)(v.y + dtv * a.y);
-        v.z = (float)(v.z + dtv * a.z);
-        p.x = (float)(p.x + dt * v.x);
-        p.y = (float)(p.y + dt * v.y);
-        p.z = (float)(p.z + dt * v.z);
+        const double vx = __dadd_rn(v.x, __dmul_rn(p[0], a.x));
+        const double vy = __dadd_rn(v.y, __dmul_rn(p[0], a.y));
+        const double vz = __dadd_rn(v.z, __dmul_rn(p[0], a.z));
+        const double vv = __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz));
+        ke = __dadd_rn(ke, COSMO ? __dmul_rn(__dmul_rn((double)x.w, vv), p[5])
+                                 : __dmul_rn((double)x.w, vv));
+        pe = __dadd_rn(pe, __dmul_rn((double)x.w, (double)a.w));
+        v.x = (float)__dadd_rn(v.x, __dmul_rn(p[1], a.x));
+        v.y = (float)__dadd_rn(v.y, __dmul_rn(p[1], a.y));
+        v.z = (float)__dadd_rn(v.z, __dmul_rn(p[1], a.z));
+        if (COSMO) {
+            x.x = (float)__dmul_rn(p[3], x.x);
+            x.y = (float)__dmul_rn(p[3], x.y);
+            x.z = (float)__dmul_rn(p[3], x.z);
+        }
+        x.x = (float)__dadd_rn(x.x, __dmul_rn(p[2], v.x));
+        x.y = (float)__dadd_rn(x.y, __dmul_rn(p[2], v.y));
+        x.z = (float)__dadd_rn(x.z, __dmul_rn(p[2], v.z));
+        if (COSMO) {
+            x.x = (float)__dmul_rn(p[4], x.x);
+            x.y = (float)__dmul_rn(p[4], x.y);
+            x.z = (float)__dmul_rn(p[4], x.z);
+        }
         vel[i] = v;
-        pts[i] = p;
+        pts[i] = x;
     }
     for (int d = 16; d > 0; d >>= 1) {
         ke += __shfl_xor_sync(0xffffffffu, ke, d);
@@ -328,8 +361,12 @@ int integrate_enqueue(grav_plan *pl, float *vel, const double *params, double *e
                       cudaStream_t st) {
     const int64_t n = pl->hp.nbodies;
     const unsigned blocks = (unsigned)std::min<int64_t>((n + 255) / 256, (int64_t)pl->nsm * 8);
-    k_integrate<<<blocks, 256, 0, st>>>(const_cast<float4 *>(pl->dp.points), pl->dp.out,
-                                        reinterpret_cast<float4 *>(vel), n, params, energy);
+    if (pl->integrator == 1)
+        k_integrate<true><<<blocks, 256, 0, st>>>(const_cast<float4 *>(pl->dp.points), pl->dp.out,
+                                                  reinterpret_cast<float4 *>(vel), n, params, energy);
+    else
+        k_integrate<false><<<blocks, 256, 0, st>>>(const_cast<float4 *>(pl->dp.points), pl->dp.out,
+                                                   reinterpret_cast<float4 *>(vel), n, params, energy);
     GC_CHECK(cudaGetLastError());
     return 0;
 }
@@ -427,6 +464,15 @@ extern "C" int grav_plan_refit_CUDA(grav_plan *pl, void *stream) {
 
 extern "C" float *grav_plan_bodies(grav_plan *pl) {
     return pl ? const_cast<float *>(reinterpret_cast<const float *>(pl->dp.points)) : nullptr;
+}
+
+extern "C" int grav_plan_set_integrator_CUDA(grav_plan *pl, int kind) {
+    if (!pl || kind < 0 || kind > 1)
+        return gc::set_status(-1, "grav_plan_set_integrator_CUDA: bad arguments");
+    if (pl->integrator != kind && pl->step)
+        step_graph_reset(pl->step);
+    pl->integrator = kind;
+    return 0;
 }
 
 extern "C" int grav_plan_integrate_CUDA(grav_plan *pl, float *vel, const double *params,

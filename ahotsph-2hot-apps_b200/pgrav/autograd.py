@@ -54,6 +54,8 @@ class TreeGravity(torch.autograd.Function):
     def backward(ctx, gacc, gphi):
         pos, mass = ctx.saved_tensors
         order, plan = TreeGravity._plan(pos, mass, ctx.eps2, ctx.kw)
+        if ctx.kw.get("ewald"):
+            plan.eval()   # the correction's adjoint reads the evaluation's group moments
         n = pos.shape[0]
         wu = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
         if gacc is not None:

@@ -26,6 +26,7 @@ EXPORTS = [
     "grav_groups_CUDA", "grav_direct_fp64_CUDA", "grav_plan_set_timing", "grav_plan_kernel_ms",
     "grav_groups_eval_dev_CUDA", "grav_plan_set_tree_CUDA", "grav_plan_refit_CUDA",
     "grav_plan_bodies", "grav_plan_integrate_CUDA", "grav_plan_step_CUDA",
+    "grav_plan_set_integrator_CUDA",
     "grav_plan_adjoint_CUDA", "grav_plan_retune_CUDA", "grav_plan_get_tuning",
     "grav_groups_CUDA_phases", "grav_groups_release_CUDA", "grav_fp32_peak_CUDA",
     "grav_plan_build_CUDA", "grav_plan_order", "grav_plan_build_phases", "grav_plan_problem",
@@ -103,6 +104,7 @@ def lib(record_errors=True):
             "grav_plan_set_tree_CUDA": ([vp, vp, vp, vp, vp, vp], i32),
             "grav_plan_refit_CUDA": ([vp, vp], i32), "grav_plan_bodies": ([vp], vp),
             "grav_plan_integrate_CUDA": ([vp, vp, vp, vp, vp], i32),
+            "grav_plan_set_integrator_CUDA": ([vp, i32], i32),
             "grav_plan_step_CUDA": ([vp, vp, vp, vp, vp, i32], i32),
             "grav_plan_adjoint_CUDA": ([vp, vp, vp, vp], i32),
             "grav_plan_retune_CUDA": ([vp, vp], i32), "grav_plan_get_tuning": ([vp, vp], i32),
@@ -300,6 +302,11 @@ class Plan:
 
     def integrate(self, vel_ptr, params_ptr, energy_ptr, stream=None):
         check(lib().grav_plan_integrate_CUDA(self._h, vel_ptr, params_ptr, energy_ptr, stream))
+
+    def set_integrator(self, kind):
+        """0: Integrate (params {dt, dtv, dtsync}); 1: CosmoIntegrate (params of
+        nln_cosmo_kdk, 6 doubles) for later integrate and step calls."""
+        check(lib().grav_plan_set_integrator_CUDA(self._h, int(kind)))
 
     def retune(self, tuning):
         """New tile shapes (a Tuning or a tuple of its fields); rebuilds the queue only."""

@@ -54,10 +54,21 @@ class Stepper:
     run periodic (with the Ewald correction unless ewald=False).  tree_kw
     goes to host.Tree (tol, leaf_max, ...).  graph=True replays each step
     from a CUDA graph captured on the first step after every rebuild.
+
+    cosmo (a pgrav.cosmo.Cosmology) makes the run comoving: pos are
+    comoving positions (box the comoving side), vel the peculiar velocities
+    a dx/dt, eps2 the comoving softening, tstart the cosmic time of the
+    initial conditions, G = 1.  Steps use CosmoIntegrate's factors
+    (nln/integrate.c:82-135) on comoving coordinates: the canonical momentum
+    p = a^2 dx/dt takes kick(t0, t1) = int dt/a times the comoving
+    acceleration and the positions drift by int dt/a^2 (the reference applies
+    the same factors to physical positions, scaled by a0 and a1).  The energy
+    record is the physical peculiar kinetic energy and the physical potential
+    energy (phi / a).
     """
 
     def __init__(self, pos, vel, mass, eps2, box=0.0, ewald=None, rebuild=8, graph=True,
-                 tree_kw=None, gpu_build=True):
+                 tree_kw=None, gpu_build=True, cosmo=None, tstart=0.0):
         import torch
         self.torch = torch
         self.pos = np.array(pos, np.float32).reshape(-1, 3)
@@ -73,13 +84,16 @@ class Stepper:
         self.gpu_build = bool(gpu_build)
         self.orig = None  # GPU rebuilds: tree position -> original body index (device int64)
         self.build_s = []  # seconds of every rebuild
-        self.tpos = 0.0
-        self.tvel = 0.0
+        self.cosmo = cosmo
+        self.tpos = float(tstart)
+        self.tvel = float(tstart)
+        if cosmo is not None:
+            self.vel = (self.vel * np.float32(cosmo.a_at_t(tstart))).astype(np.float32)  # p = a u
         self.nsteps = 0
         self.history = []
         self.stream = torch.cuda.Stream()
         dev = torch.device("cuda")
-        self.params = torch.zeros(3, dtype=torch.float64, device=dev)
+        self.params = torch.zeros(6 if cosmo is not None else 3, dtype=torch.float64, device=dev)
         self.energy = torch.zeros(2, dtype=torch.float64, device=dev)
         self.dvel = None
         self.plan = None
@@ -94,6 +108,8 @@ class Stepper:
             self._build_gpu()
         else:
             self._build_host()
+        if self.cosmo is not None:
+            self.plan.set_integrator(1)
         self.torch.cuda.synchronize()
         self.build_s.append(time.perf_counter() - t0)
 
@@ -157,8 +173,11 @@ class Stepper:
         self.vel[order] = self.dvel.cpu().numpy()[:, :3]
 
     def state(self):
-        """(pos, vel) in the original order, current."""
+        """(pos, vel) in the original order, current (comoving runs: comoving
+        positions and the peculiar velocities a dx/dt at tvel)."""
         self._pull()
+        if self.cosmo is not None:
+            return self.pos.copy(), (self.vel / np.float32(self.cosmo.a_at_t(self.tvel))).astype(np.float32)
         return self.pos.copy(), self.vel.copy()
 
     def step(self, dt):
@@ -169,16 +188,25 @@ class Stepper:
         dtsync = self.tpos - self.tvel
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        if self.cosmo is not None:
+            f = self.cosmo.kdk(self.tpos, self.tvel, dt, dtv)
+            # comoving form: the acceleration is a0^2 times the physical one
+            coef = [f[0] * f[5], f[1] * f[5], f[2], 1.0, 1.0, f[5]]
+        else:
+            coef = [dt, dtv, dtsync]
         with torch.cuda.stream(self.stream):
-            self.params.copy_(torch.tensor([dt, dtv, dtsync], dtype=torch.float64))
+            self.params.copy_(torch.tensor(coef, dtype=torch.float64))
             e0.record(self.stream)
             self.plan.step(self.dvel.data_ptr(), self.params.data_ptr(), self.energy.data_ptr(),
                            self.stream.cuda_stream, graph=self.graph)
             e1.record(self.stream)
         self.stream.synchronize()
         ke, pe = self.energy.cpu().numpy()
-        rec = {"t": self.tpos, "ke": 0.5 * float(ke), "pe": 0.5 * float(pe),
+        pscale = 1.0 / self.cosmo.a_at_t(self.tpos) if self.cosmo is not None else 1.0
+        rec = {"t": self.tpos, "ke": 0.5 * float(ke), "pe": 0.5 * float(pe) * pscale,
                "ms": e0.elapsed_time(e1), "graph": self.graph}
+        if self.cosmo is not None:
+            rec["a"] = self.cosmo.a_at_t(self.tpos)
         rec["e"] = rec["ke"] + rec["pe"]
         self.history.append(rec)
         self.tpos += dt
@@ -202,7 +230,17 @@ class Stepper:
             "tacc": (sdf.DOUBLE, self.tpos), "R0": (sdf.FLOAT, 0.5 * self.box),
             "L0": (sdf.FLOAT, self.box), "Gnewt": (sdf.DOUBLE, 1.0),
             "eps2": (sdf.DOUBLE, self.eps2), "ewald": (sdf.INT, int(self.ewald)),
-            "rebuild": (sdf.INT, self.rebuild)})
+            "rebuild": (sdf.INT, self.rebuild), **self._cosmo_header()})
+
+    def _cosmo_header(self):
+        from . import sdf
+        if self.cosmo is None:
+            return {}
+        p = self.cosmo.params
+        h = {"cosmology": (sdf.INT, 1)}
+        for k in ("H0", "Omega_m", "Omega_r", "Omega_lambda", "Omega_de", "w0", "wa"):
+            h[k] = (sdf.DOUBLE, float(getattr(p, k)))
+        return h
 
     @classmethod
     def load(cls, path, graph=True, tree_kw=None, gpu_build=True):
@@ -213,10 +251,16 @@ class Stepper:
         from . import sdf
         h, b = sdf.read(path)
         order = np.argsort(b["ident"], kind="stable")
+        cosmo = None
+        if h.get("cosmology"):
+            from .cosmo import Cosmology
+            cosmo = Cosmology(**{k: float(h[k]) for k in ("H0", "Omega_m", "Omega_r",
+                                                          "Omega_lambda", "Omega_de", "w0", "wa")})
         st = cls(b["pos"][order], b["vel"][order], b["mass"][order], h["eps2"],
                  box=float(h.get("L0", 0.0)) if h.get("do_periodic") else 0.0,
                  ewald=bool(h.get("ewald", 0)), rebuild=h.get("rebuild", 8), graph=graph,
-                 tree_kw=tree_kw, gpu_build=gpu_build)
+                 tree_kw=tree_kw, gpu_build=gpu_build, cosmo=cosmo,
+                 tstart=float(h["tvel"]) if cosmo is not None else 0.0)
         st.nsteps = int(h["iter"])
         st.tpos = float(h["tpos"])
         st.tvel = float(h["tvel"])

@@ -359,6 +359,13 @@ int grav_fp32_peak_CUDA(double *tflops);
  * dtsync = tpos - tvel}; for each body ke += m |v + dtsync a|^2, pe += m phi
  * (added into energy, device, 2 doubles), then v += dtv a, x += dt v.
  * vel: device, float4 (vx, vy, vz, unused) per body, tree order.
+ * grav_plan_set_integrator_CUDA: kind 0 (default) is the Integrate above;
+ * kind 1 is CosmoIntegrate of nln/integrate.c:82-135: params (device, 6
+ * doubles) = {a0^2 kick(tvel, tpos), a0^2 kick(tvel, tvel + dtv),
+ * drift(tpos, tpos + dt), 1/a0, a(tpos + dt), 1/a0^2} (nlnhost.h
+ * nln_cosmo_kdk); ke += m |v + p0 a|^2 p5, pe += m phi, v += p1 a,
+ * x = p4 (p3 x + p2 v) with positions rounded to FP32 after each factor as
+ * the reference does.  It applies to later integrate and step calls.
  * grav_plan_step_CUDA: one step = zero energy, evaluate, integrate, refit.
  * With use_graph the step is captured once into a CUDA graph on `stream`
  * (a created stream, not the legacy default) and replayed by later calls
@@ -372,6 +379,7 @@ int grav_plan_refit_CUDA(grav_plan *plan, void *stream);
 float *grav_plan_bodies(grav_plan *plan);
 int grav_plan_integrate_CUDA(grav_plan *plan, float *vel, const double *params, double *energy,
                              void *stream);
+int grav_plan_set_integrator_CUDA(grav_plan *plan, int kind);
 int grav_plan_step_CUDA(grav_plan *plan, float *vel, const double *params, double *energy,
                         void *stream, int use_graph);
 
@@ -380,13 +388,18 @@ int grav_plan_step_CUDA(grav_plan *plan, float *vel, const double *params, doubl
  * For a loss L = sum_i w_i . a_i + u_i phi_i on the plan's last evaluation,
  * dL/dx and dL/dm of every body with the lists held fixed: the pair terms'
  * tidal-tensor-vector products on the sink and source sides, the mass and
- * quadrupole-moment adjoints of every listed cell, then the moments'
- * chain rule to the cell's bodies (centre of mass, second moment).  wu:
- * device float4 (wx, wy, wz, u) per body, tree order; grad: device float4
- * (dL/dx, dL/dy, dL/dz, dL/dm) per body, tree order.  Needs the tree links
- * (grav_plan_set_tree_CUDA); isolated problems with monopole and
- * quadrupole lists and quad_phi_sign = +1 (no order-4 cells, no periodic
- * images).  Enqueued on `stream`.
+ * trace-free moment adjoints (orders 2, 3, 4) of every listed cell, the
+ * periodic correction's adjoint through each group's Taylor moments and each
+ * correction entry's table lookup, then the moments' chain rule to the
+ * cell's bodies (centre of mass, trace-free moments, the second-moment
+ * trace).  wu: device float4 (wx, wy, wz, u) per body, tree order; grad:
+ * device float4 (dL/dx, dL/dy, dL/dz, dL/dm) per body, tree order.  Needs
+ * the tree links (grav_plan_set_tree_CUDA), the physical quadrupole
+ * potential (quad_phi_sign = +1), the mixed-precision form and, for the
+ * periodic correction, an evaluation enqueued before it (its group moments
+ * are read).  Every list kind and periodic image shift is covered; the
+ * correction's derivatives of order 6 (beyond its table) are dropped.
+ * Enqueued on `stream`.
  */
 int grav_plan_adjoint_CUDA(grav_plan *plan, const float *wu, float *grad, void *stream);
 

@@ -201,6 +201,39 @@ int nln_sdf_bodies(const nln_sdf *s, float *mass, float *pos, float *vel, float 
 void nln_sdf_free(nln_sdf *s);
 const char *nln_sdf_error(void);
 
+/*
+ * ---- background cosmology (the cosmological leapfrog's factors) ----
+ * The reference integrates comoving runs with CosmoIntegrate
+ * (nln/integrate.c:82-135), which takes a(t) and the integrals
+ * kick(t0, t1) = int dt / a and drift(t0, t1) = int dt / a^2 from the 2hot
+ * library's cosmology object.  nln_cosmo integrates the Friedmann equation
+ *   H^2 = H0^2 (Omega_r a^-4 + Omega_m a^-3 + Omega_k a^-2 + Omega_lambda
+ *               + Omega_de a^(-3(1+w0+wa)) exp(-3 wa (1-a))),
+ *   Omega_k = 1 - Omega_r - Omega_m - Omega_lambda - Omega_de,
+ * in the run's time unit (H0 in its inverse), t = 0 at a = 0.
+ * nln_cosmo_kdk: CosmoIntegrate's factors for a step from positions at tpos
+ * and velocities at tvel: out = {a0^2 kick(tvel, tpos), a0^2 kick(tvel,
+ * tvel + dtv), drift(tpos, tpos + dt), 1/a0, a(tpos + dt), 1/a0^2},
+ * a0 = a(tpos) -- the params of the cosmological integrator
+ * (grav_plan_set_integrator_CUDA).  nln_cosmo_new returns NULL for
+ * H0 <= 0 or no matter or radiation.
+ */
+typedef struct nln_cosmo_params {
+    double H0;
+    double Omega_m, Omega_r, Omega_lambda;
+    double Omega_de, w0, wa; /* a w0 + wa (1 - a) dark-energy fluid */
+} nln_cosmo_params;
+typedef struct nln_cosmo nln_cosmo;
+nln_cosmo *nln_cosmo_new(const nln_cosmo_params *params);
+void nln_cosmo_free(nln_cosmo *c);
+double nln_cosmo_hubble(const nln_cosmo *c, double a);
+double nln_cosmo_t_at_a(const nln_cosmo *c, double a);
+double nln_cosmo_a_at_t(const nln_cosmo *c, double t);
+double nln_cosmo_kick(const nln_cosmo *c, double t0, double t1);
+double nln_cosmo_drift(const nln_cosmo *c, double t0, double t1);
+void nln_cosmo_kdk(const nln_cosmo *c, double tpos, double tvel, double dt, double dtv,
+                   double out[6]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -924,3 +924,34 @@ double orc_fd_partial_loss_x(int s, long j, long n, const double *x, const doubl
     L += w[3 * j] * a[0] + w[3 * j + 1] * a[1] + w[3 * j + 2] * a[2] + u[j] * phi;
     return L;
 }
+
+/*
+ * CosmoIntegrate of nln/integrate.c:82-135 on n bodies held as float4
+ * records: pos (x, y, z, m), vel (vx, vy, vz, -), acc (ax, ay, az, phi).
+ * f: the step's six factors {a0^2 kick(tvel, tpos), a0^2 kick(tvel,
+ * tvel + dtv), drift(tpos, tpos + dt), 1/a0, a(tpos + dt), 1/a0^2} of the
+ * cosmology (the integrals are the caller's).  As the reference: the
+ * centred velocity in FP64 for the energies, the new velocity stored to
+ * float, the position converted to comoving, drifted and converted back,
+ * each stored to float; ke += m |vc|^2 / a0^2, pe += m phi (the reference
+ * halves both when it returns them).
+ */
+void orc_cosmo_integrate(long n, float *pos, float *vel, const float *acc, const double *f,
+                         double *ke, double *pe) {
+    double k = 0.0, p = 0.0;
+    const double a0 = 1.0 / f[3];
+    for (long i = 0; i < n; i++) {
+        float *x = pos + 4 * i, *v = vel + 4 * i;
+        const float *a = acc + 4 * i;
+        double vc[3];
+        for (int d = 0; d < 3; d++) vc[d] = v[d] + f[0] * a[d];
+        k += x[3] * (vc[0] * vc[0] + vc[1] * vc[1] + vc[2] * vc[2]) / (a0 * a0);
+        p += x[3] * a[3];
+        for (int d = 0; d < 3; d++) v[d] = (float)(v[d] + f[1] * a[d]);
+        for (int d = 0; d < 3; d++) x[d] = (float)(f[3] * x[d]);
+        for (int d = 0; d < 3; d++) x[d] = (float)(x[d] + f[2] * v[d]);
+        for (int d = 0; d < 3; d++) x[d] = (float)(f[4] * x[d]);
+    }
+    *ke = k;
+    *pe = p;
+}

@@ -109,6 +109,8 @@ def orc():
             pp, L_, _i64p, np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS"), _f64p, _f64p,
             ctypes.c_double, ctypes.c_double, ctypes.c_int]
         lib.orc_fd_partial_loss_x.restype = ctypes.c_double
+        lib.orc_cosmo_integrate.argtypes = [L_, _f32p, _f32p, _f32p, _f64p, ctypes.c_void_p,
+                                             ctypes.c_void_p]
         lib.orc_ewald_c0.argtypes = [ctypes.c_double]
         lib.orc_ewald_c0.restype = ctypes.c_double
         lib.orc_direct_grad.argtypes = [L_, _f64p, _f64p, _f64p, _f64p, ctypes.c_double, _f64p,
@@ -352,6 +354,19 @@ class ListsFP64:
                 m[j] = m0
                 out.append((lp - lm) / (2 * hh))
         return np.array(out)
+
+
+def cosmo_integrate(pos4, vel4, acc4, factors):
+    """CosmoIntegrate (orc_cosmo_integrate) on copies of float32 (n, 4)
+    arrays: returns (pos4, vel4, ke, pe)."""
+    pos = np.ascontiguousarray(pos4, np.float32).copy()
+    vel = np.ascontiguousarray(vel4, np.float32).copy()
+    acc = np.ascontiguousarray(acc4, np.float32)
+    ke, pe = ctypes.c_double(), ctypes.c_double()
+    orc().orc_cosmo_integrate(len(pos), pos.ravel(), vel.ravel(), acc.ravel(),
+                              np.ascontiguousarray(factors, np.float64), ctypes.byref(ke),
+                              ctypes.byref(pe))
+    return pos, vel, ke.value, pe.value
 
 
 def ewald_c0(L):

@@ -105,12 +105,12 @@ def test_adjoint_matches_central_differences(monkeypatch):
     assert np.abs(gm[mpicks] - fdm).max() < 2e-4 * mscale, (np.abs(gm[mpicks] - fdm).max() / mscale)
 
 
-def _adjoint_vs_oracle_fd(pos, m, eps2, tkw, nsel, seed, ewald=False):
+def _adjoint_vs_oracle_fd(pos, m, eps2, tkw, nsel, seed, ewald=False, pool=None):
     """The GPU adjoint (through pgrav.autograd) at nsel bodies against FP64
     central differences of the oracle's evaluation of the same lists
     (ListsFP64, every cell's moments from the bodies).  Returns the largest
     position and mass errors, each over the rms of that gradient, and the
-    FD values themselves."""
+    FD values themselves.  pool: tree positions to draw the bodies from."""
     import torch
     from oracle import oracle as O
     from pgrav import autograd as AG, host
@@ -132,7 +132,7 @@ def _adjoint_vs_oracle_fd(pos, m, eps2, tkw, nsel, seed, ewald=False):
     t = host.Tree(pos, m, **tkw)
     o = np.asarray(t.order)
     chk = O.ListsFP64(t, ewald=ewald)
-    sel = rng.choice(n, nsel, replace=False)     # tree positions
+    sel = rng.choice(n if pool is None else pool, nsel, replace=False)     # tree positions
     chk.select(sel)
     xt = np.asarray(t.sorted_pos, np.float64)
     mt = np.asarray(t.points[:n, 3], np.float64)
@@ -151,10 +151,14 @@ def test_adjoint_order4_matches_central_differences():
     through the centre of mass, and the pair terms of orders 2..4."""
     from pgrav import host, ics
     pos, m = ics.plummer(4000, seed=34)
-    tkw = dict(tol=1e-3, p2cut=7, p4cut=20, leaf_max=8)
+    tkw = dict(tol=1e-3, p2cut=4, p4cut=8, leaf_max=8)
     t = host.Tree(pos, m, **tkw)
-    assert t.counts[3] > 0.1 * t.counts.sum()   # order-4 interactions carry weight
-    ex, em, _ = _adjoint_vs_oracle_fd(pos, m, 1e-4, tkw, 16, 35)
+    # bodies of cells on order-4 lists, whose moments' chain the check covers
+    hc = np.unique(np.asarray(t.hlist) & ((1 << 27) - 1))
+    first, count = t.cell_ranges()
+    pool = np.unique(np.concatenate([np.arange(first[c], first[c] + count[c]) for c in hc]))
+    assert len(hc) > 50 and len(pool) > 500
+    ex, em, _ = _adjoint_vs_oracle_fd(pos, m, 1e-4, tkw, 16, 35, pool=pool)
     assert ex < 2e-4 and em < 2e-4, (ex, em)
 
 
@@ -168,7 +172,7 @@ def test_adjoint_periodic_matches_central_differences():
     n1 = 16
     pos, m = ics.grf_box(n1, seed=36)
     eps2 = (1.0 / n1 / 50) ** 2
-    tkw = dict(tol=1e-5, p2cut=7, p4cut=20, leaf_max=8, group_max=16, box=1.0)
+    tkw = dict(tol=1e-4, p2cut=4, p4cut=8, leaf_max=8, group_max=16, box=1.0)
     ex, em, r = _adjoint_vs_oracle_fd(pos, m, eps2, tkw, 8, 37, ewald=True)
     assert ex < 3e-3 and em < 3e-3, (ex, em)
     # the correction's share of the gradient is far above that bar

@@ -180,3 +180,78 @@ def test_checkpoint_and_resume_continue_the_run(tmp_path):
     got = c.state()
     c.free()
     assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+
+
+def test_cosmo_integrate_matches_reference_restatement(mods):
+    """CosmoIntegrate on the device (grav_plan_set_integrator_CUDA kind 1)
+    against the oracle's restatement of nln/integrate.c:82-135 on the same
+    bodies, forces and factors: positions and velocities bit for bit."""
+    torch, gc, host, ics, step = mods
+    from oracle import oracle as O
+    from pgrav.cosmo import Cosmology
+    pos, m = ics.plummer(6000, seed=25)
+    t = host.Tree(pos, m, tol=1e-4)
+    plan = gc.Plan(t, 1e-4)
+    plan.eval()
+    f = plan.download()
+    x0 = step.memcpy_d2h(np.empty((t.n, 4), np.float32), plan.bodies_ptr())
+    rng = np.random.default_rng(6)
+    v = rng.normal(0, 0.3, (t.n, 4)).astype(np.float32)
+    v[:, 3] = 0
+    c = Cosmology(H0=0.0511365, Omega_m=0.3, Omega_lambda=0.7)
+    tpos, dt = c.t_at_a(0.25), 0.05 * c.t_at_a(0.25)
+    tvel = tpos - 0.5 * dt
+    fac = c.kdk(tpos, tvel, dt, tpos + 0.5 * dt - tvel)
+    dvel = torch.from_numpy(v.copy()).cuda()
+    params = torch.tensor(fac, dtype=torch.float64, device="cuda")
+    energy = torch.zeros(2, dtype=torch.float64, device="cuda")
+    plan.set_integrator(1)
+    plan.integrate(dvel.data_ptr(), params.data_ptr(), energy.data_ptr())
+    torch.cuda.synchronize()
+    x1 = step.memcpy_d2h(np.empty((t.n, 4), np.float32), plan.bodies_ptr())
+    plan.free()
+    rx, rv, ke, pe = O.cosmo_integrate(x0, v, f.astype(np.float32), fac)
+    np.testing.assert_array_equal(x1[:, :3], rx[:, :3])
+    np.testing.assert_array_equal(dvel.cpu().numpy()[:, :3], rv[:, :3])
+    got = energy.cpu().numpy()
+    assert got[0] == pytest.approx(ke, rel=1e-12) and got[1] == pytest.approx(pe, rel=1e-12)
+
+
+def test_zeldovich_plane_wave_grows_linearly(mods):
+    """A comoving run (Stepper with a Cosmology) of an Einstein-de Sitter box:
+    sheets displaced by a plane wave follow the Zel'dovich solution, exact in
+    one dimension before shell crossing -- the displacement grows as a from
+    a = 0.1 to 0.2 (periodic forces with the Ewald correction, kicks and
+    drifts of the cosmological leapfrog)."""
+    torch, gc, host, ics, step = mods
+    from pgrav.cosmo import Cosmology
+    n1 = 16
+    g = (np.arange(n1) + 0.5) / n1
+    q = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    n = len(q)
+    m = np.full(n, 1.0 / n)
+    c = Cosmology(H0=np.sqrt(8 * np.pi / 3), Omega_m=1.0)   # G rho_bar = 1 in a unit box
+    a0, a1 = 0.1, 0.2
+    A = 0.4 / (2 * np.pi * a1)                               # k A a1 = 0.4: no shell crossing
+    psi = np.zeros_like(q)
+    psi[:, 0] = A * np.sin(2 * np.pi * q[:, 0])
+    x = np.mod(q + a0 * psi, 1.0)
+    u = a0 * a0 * c.hubble(a0) * psi                         # a dx/dt of the growing mode
+    t0, t1 = c.t_at_a(a0), c.t_at_a(a1)
+    st = step.Stepper(x, u, m, (0.05 / n1) ** 2, box=1.0, rebuild=4, graph=True,
+                      tree_kw=dict(tol=1e-6, p2cut=7, p4cut=20), cosmo=c, tstart=t0)
+    nst = 40
+    st.run(nst, (t1 - t0) / nst)
+    assert st.tpos == pytest.approx(t1, rel=1e-12)
+    xe, ue = st.state()
+    st.free()
+    d = np.mod(xe - q + 0.5, 1.0) - 0.5
+    s = np.sin(2 * np.pi * q[:, 0])
+    amp = 2 * np.mean(d[:, 0] * s)
+    assert amp == pytest.approx(a1 * A, rel=2e-3), (amp, a1 * A)
+    assert np.abs(d[:, 0] - amp * s).max() < 1e-2 * a1 * A
+    assert np.abs(d[:, 1:]).max() < 1e-3 * a1 * A
+    # peculiar velocities at tvel (half a step behind) follow a^2 H psi
+    at = c.a_at_t(st.tvel)
+    np.testing.assert_allclose(ue[:, 0], at * at * c.hubble(at) * psi[:, 0] / 1.0, rtol=0,
+                               atol=5e-3 * np.abs(at * at * c.hubble(at) * psi[:, 0]).max())
