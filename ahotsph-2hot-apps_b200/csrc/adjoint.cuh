@@ -41,6 +41,10 @@
 // of mass).  k_adjoint_cells forms PG_l and Xbar' once per cell,
 // k_adjoint_bodies walks every body's ancestors.
 //
+// A body's pair with itself (in its own group's point list, d = 0) adds
+// +t and -t to the same body and is left out of the position adjoint; its
+// mass term (-u/eps) stays.
+//
 // Work layout: one warp per work item (group, list kind, slice), as the
 // forward's queues.  Points and quadrupoles: each lane holds two sinks as
 // an f32x2 pair and one record of a 32-record tile; records and their
@@ -188,7 +192,11 @@ __global__ void __launch_bounds__(256) k_adjoint_points(AdjProblem P) {
                     const float dx = sx_ + nx, dy = sy_ + ny, dz = sz_ + nz;
                     const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, e2.x)));
                     const float ri = rsqrt_fast(r2), ri2 = ri * ri;
-                    const float mr3 = m * ri * ri2;
+                    // a body against itself (d = 0: offsets of one point, exact negatives)
+                    // adds t on both sides of the same body; leave it out, since the
+                    // two FP32 sums would not cancel it exactly (t = m w / eps^3)
+                    const bool self = dx == 0.f && dy == 0.f && dz == 0.f;
+                    const float mr3 = self ? 0.f : m * ri * ri2;
                     const float wd = fmaf(wx_, dx, fmaf(wy_, dy, wz_ * dz));
                     const float in = fmaf(-3.f * ri2, wd, -u_);
                     const float ex = fmaf(in, dx, wx_), ey = fmaf(in, dy, wy_), ez = fmaf(in, dz, wz_);

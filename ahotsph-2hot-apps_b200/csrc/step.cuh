@@ -236,7 +236,7 @@ __global__ void k_refit_tables(const double *__restrict__ raw, int64_t ncells, i
 // by 1/a0^2 per body.  Both accumulate energy += {sum m vc.vc, sum m phi};
 // positions and velocities are formed in FP64 without fused multiply-adds
 // and rounded to FP32, as the reference's double expressions stored to
-// floats.
+// floats; m phi is a float product (both operands are floats there).
 template <bool COSMO>
 __global__ void k_integrate(float4 *__restrict__ pts, const float4 *__restrict__ acc,
                             float4 *__restrict__ vel, int64_t n, const double *__restrict__ params,
@@ -263,7 +263,7 @@ __global__ void k_integrate(float4 *__restrict__ pts, const float4 *__restrict__
         const double vv = __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz));
         ke = __dadd_rn(ke, COSMO ? __dmul_rn(__dmul_rn((double)x.w, vv), p[5])
                                  : __dmul_rn((double)x.w, vv));
-        pe = __dadd_rn(pe, __dmul_rn((double)x.w, (double)a.w));
+        pe = __dadd_rn(pe, (double)__fmul_rn(x.w, a.w));  // a float product, as the reference's
         v.x = (float)__dadd_rn(v.x, __dmul_rn(p[1], a.x));
         v.y = (float)__dadd_rn(v.y, __dmul_rn(p[1], a.y));
         v.z = (float)__dadd_rn(v.z, __dmul_rn(p[1], a.z));

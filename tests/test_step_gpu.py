@@ -222,12 +222,14 @@ def test_zeldovich_plane_wave_grows_linearly(mods):
     sheets displaced by a plane wave follow the Zel'dovich solution, exact in
     one dimension before shell crossing -- the displacement grows as a from
     a = 0.1 to 0.2 (periodic forces with the Ewald correction, kicks and
-    drifts of the cosmological leapfrog)."""
+    drifts of the cosmological leapfrog).  16 sheets of 48 x 48 bodies: the
+    in-sheet spacing stays well below the closest sheets' separation, where
+    a sheet's field is uniform to 1e-5."""
     torch, gc, host, ics, step = mods
     from pgrav.cosmo import Cosmology
-    n1 = 16
-    g = (np.arange(n1) + 0.5) / n1
-    q = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    ns, nt = 16, 48
+    gs, gt = (np.arange(ns) + 0.5) / ns, (np.arange(nt) + 0.5) / nt
+    q = np.stack(np.meshgrid(gs, gt, gt, indexing="ij"), -1).reshape(-1, 3)
     n = len(q)
     m = np.full(n, 1.0 / n)
     c = Cosmology(H0=np.sqrt(8 * np.pi / 3), Omega_m=1.0)   # G rho_bar = 1 in a unit box
@@ -238,7 +240,7 @@ def test_zeldovich_plane_wave_grows_linearly(mods):
     x = np.mod(q + a0 * psi, 1.0)
     u = a0 * a0 * c.hubble(a0) * psi                         # a dx/dt of the growing mode
     t0, t1 = c.t_at_a(a0), c.t_at_a(a1)
-    st = step.Stepper(x, u, m, (0.05 / n1) ** 2, box=1.0, rebuild=4, graph=True,
+    st = step.Stepper(x, u, m, (0.05 / nt) ** 2, box=1.0, rebuild=4, graph=True,
                       tree_kw=dict(tol=1e-6, p2cut=7, p4cut=20), cosmo=c, tstart=t0)
     nst = 40
     st.run(nst, (t1 - t0) / nst)
@@ -248,10 +250,10 @@ def test_zeldovich_plane_wave_grows_linearly(mods):
     d = np.mod(xe - q + 0.5, 1.0) - 0.5
     s = np.sin(2 * np.pi * q[:, 0])
     amp = 2 * np.mean(d[:, 0] * s)
-    assert amp == pytest.approx(a1 * A, rel=2e-3), (amp, a1 * A)
-    assert np.abs(d[:, 0] - amp * s).max() < 1e-2 * a1 * A
+    assert amp == pytest.approx(a1 * A, rel=1e-3), (amp, a1 * A)
+    assert np.abs(d[:, 0] - a1 * A * s).max() < 2e-3 * a1 * A
     assert np.abs(d[:, 1:]).max() < 1e-3 * a1 * A
     # peculiar velocities at tvel (half a step behind) follow a^2 H psi
     at = c.a_at_t(st.tvel)
-    np.testing.assert_allclose(ue[:, 0], at * at * c.hubble(at) * psi[:, 0] / 1.0, rtol=0,
-                               atol=5e-3 * np.abs(at * at * c.hubble(at) * psi[:, 0]).max())
+    want = at * at * c.hubble(at) * psi[:, 0]
+    assert np.abs(ue[:, 0] - want).max() < 2e-3 * np.abs(want).max()
