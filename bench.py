@@ -601,7 +601,51 @@ def config_adjoint(args, stream):
                                                       np.sqrt(np.mean(emd ** 2)) <= 1e-3)}
     res["leapfrog"] = leapfrog_check(args)
     res["leapfrog_2p20"] = leapfrog_time(n, eps2, tol)
+    res["headline_adjoint"] = headline_adjoint(stream)
     return res
+
+
+def headline_adjoint(stream, reps=2):
+    """The adjoint of the headline workload (the 256^3 periodic box, order 4
+    + Ewald, tree and lists built on the GPU): forward and adjoint times
+    with CUDA events on the same plan (the adjoint reads the evaluation's
+    correction moments).  Its correctness is pinned in
+    tests/test_adjoint_gpu.py against FP64 differences of the oracle on
+    periodic order-4 lists with the correction."""
+    import torch
+    from pgrav import gravcuda as gc
+    w = WORKLOADS["box256"]
+    pos, m, eps2, box = make_problem(w)
+    n = len(m)
+    bodies = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    bodies[:, :3] = torch.from_numpy(np.asarray(pos, np.float32)).cuda()
+    bodies[:, 3] = torch.from_numpy(np.asarray(m, np.float32)).cuda()
+    del pos
+    plan = gc.Plan.build(None, None, eps2, bodies=bodies, box=box, ewald=True, leaf_max=16,
+                         group_max=32, p2cut=w["p2cut"], p4cut=w["p4cut"], tol=w["tol"])
+    del bodies
+    g = torch.Generator(device="cuda").manual_seed(0)
+    wu = torch.randn((n, 4), device="cuda", generator=g)
+    grad = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    plan.eval(stream.cuda_stream)
+    plan.adjoint(wu.data_ptr(), grad.data_ptr(), stream.cuda_stream)
+    tm = {}
+    for name, fn in (("forward", lambda: plan.eval(stream.cuda_stream)),
+                     ("adjoint", lambda: plan.adjoint(wu.data_ptr(), grad.data_ptr(),
+                                                      stream.cuda_stream))):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        tm[name] = a.elapsed_time(b) / reps
+    finite = bool(torch.isfinite(grad).all().item())
+    plan.free()
+    return {"workload": "periodic 256^3 box, order 4 + Ewald (the headline), lists built on the GPU",
+            "n_bodies": n, "forward_ms": tm["forward"], "adjoint_ms": tm["adjoint"],
+            "adjoint_over_forward": tm["adjoint"] / tm["forward"], "grad_finite": finite}
 
 
 def leapfrog_time(n, eps2, tol, nsteps=16, every=4, dt=1e-3):
