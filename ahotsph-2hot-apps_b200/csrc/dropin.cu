@@ -9,7 +9,11 @@
 //    every thread of the block as broadcasts;
 //  * a long list is split across blocks (grid.y) and each thread holds
 //    SPT sinks, so one call fills more than a handful of SMs;
-//  * results are accumulated with one float4 atomic per sink per block.
+//  * results are accumulated with one float4 atomic per sink per block;
+//  * grav_mn_CUDA returns once the list is copied out of the caller's
+//    memory into page-locked staging; a submitter thread issues the copy to
+//    the device and the launch, so the caller's next list copy overlaps the
+//    CUDA calls of this one.
 #include <cuda_runtime.h>
 #include <stdarg.h>
 #include <stdio.h>
@@ -17,8 +21,12 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -341,9 +349,32 @@ struct Slot {
     void *host = nullptr;      // the staging buffer of the current call
     void *hbuf[2] = {nullptr, nullptr};
     cudaEvent_t copied[2] = {nullptr, nullptr};
-    bool pending[2] = {false, false};
+    // staging buffer states: 0 free, 1 filled and waiting for the submitter,
+    // 2 its copy to the device issued (copied[k] recorded)
+    std::atomic<int> bstate[2] = {{0}, {0}};
+    std::atomic<int> queued{0};  // jobs of this slot not yet issued
+    // recorded by the submitter after each launch; kpending = 1 until the
+    // submitter has seen it complete (then qallocCUDA needs no stream query)
+    cudaEvent_t kdone = nullptr;
+    std::atomic<int> kpending{0};
     int turn = 0;
     void *dev = nullptr;
+    void reset() {
+        kdone = nullptr;
+        kpending.store(0);
+        inuse = false;
+        stream = nullptr;
+        cap = 0;
+        host = nullptr;
+        for (int k = 0; k < 2; k++) {
+            hbuf[k] = nullptr;
+            copied[k] = nullptr;
+            bstate[k].store(0);
+        }
+        queued.store(0);
+        turn = 0;
+        dev = nullptr;
+    }
 };
 
 struct State {
@@ -360,6 +391,21 @@ struct State {
     int nsm = 148;
 };
 State S;
+// The entry points that use the slots run one at a time (nln/mac.c calls
+// them from one thread; this makes concurrent callers safe too).
+std::recursive_mutex g_call_mu;
+
+// Seconds spent per phase of the drop-in calls since the last
+// WalkInitSinkCUDA (gravcuda_dropin_phases): copies into staging, waits for
+// a free staging buffer, waits for room in the submitter's queue, the
+// submitter's CUDA calls, the drain at WalkTerminateSinkCUDA; and the calls.
+std::atomic<int64_t> g_phase_ns[5] = {{0}, {0}, {0}, {0}, {0}};
+std::atomic<int64_t> g_phase_calls{0};
+inline int64_t now_ns() {
+    return std::chrono::duration_cast<std::chrono::nanoseconds>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
 
 int ensure_init() {
     if (S.init)
@@ -368,27 +414,46 @@ int ensure_init() {
     GC_CHECK(cudaMalloc(&S.derr, sizeof(unsigned)));
     GC_CHECK(cudaMemset(S.derr, 0, sizeof(unsigned)));
     cudaDeviceGetAttribute(&S.nsm, cudaDevAttrMultiProcessorCount, 0);
-    for (int i = 0; i < NQ; i++)
+    for (int i = 0; i < NQ; i++) {
         GC_CHECK(cudaStreamCreateWithFlags(&S.q[i].stream, cudaStreamNonBlocking));
+        GC_CHECK(cudaEventCreateWithFlags(&S.q[i].kdone, cudaEventDisableTiming));
+    }
     S.init = true;
     return 0;
 }
 
+// Wait, with a bound, until `done` holds; false when the bound ran out.
+template <typename F>
+bool wait_until(F done, double seconds = 120.0) {
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int spin = 0; !done(); spin++) {
+        if (spin < 4096)
+            continue;
+        std::this_thread::yield();
+        if ((spin & 1023) == 0 &&
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > seconds)
+            return false;
+    }
+    return true;
+}
+
 // Make slot q ready for a call of `bytes`: staging buffer s.host free to
-// write (the copy that last read it has completed), device buffer large
-// enough.  The device buffer is only rewritten by copies on the slot's own
-// stream, which run after the kernels queued before them.
+// write (the copy that last read it has been issued and has completed),
+// device buffer large enough.  The device buffer is only rewritten by copies
+// on the slot's own stream, which run after the kernels queued before them.
 int slot_reserve(int q, size_t bytes) {
     if (q < 0 || q >= NQ)
         return gc::set_status(-1, "queue slot %d out of range", q);
     Slot &s = S.q[q];
     if (s.cap < bytes) {
+        if (!wait_until([&] { return s.queued.load(std::memory_order_acquire) == 0; }))
+            return gc::set_status(-1, "queue slot %d: the submitter did not drain", q);
         GC_CHECK(cudaStreamSynchronize(s.stream));
         for (int k = 0; k < 2; k++) {
             if (s.hbuf[k])
                 GC_CHECK(cudaFreeHost(s.hbuf[k]));
             s.hbuf[k] = nullptr;
-            s.pending[k] = false;
+            s.bstate[k].store(0);
             if (!s.copied[k])
                 GC_CHECK(cudaEventCreateWithFlags(&s.copied[k], cudaEventDisableTiming));
         }
@@ -401,35 +466,133 @@ int slot_reserve(int q, size_t bytes) {
         s.cap = cap;
     }
     s.turn ^= 1;
-    if (s.pending[s.turn])
+    std::atomic<int> &st = s.bstate[s.turn];
+    const int64_t t0 = now_ns();
+    if (!wait_until([&] { return st.load(std::memory_order_acquire) != 1; }))
+        return gc::set_status(-1, "queue slot %d: the submitter did not issue", q);
+    if (st.load(std::memory_order_acquire) == 2) {
         GC_CHECK(cudaEventSynchronize(s.copied[s.turn]));
+        st.store(0, std::memory_order_relaxed);
+    }
+    g_phase_ns[1] += now_ns() - t0;
     s.host = s.hbuf[s.turn];
     return 0;
 }
 
-// After the call's copy out of s.host is queued: mark the staging buffer busy.
+// The synchronous form (the body-run and index-list entry points): issue
+// the copy from the calling thread after every queued job of the slot.
 int slot_copied(Slot &s) {
     GC_CHECK(cudaEventRecord(s.copied[s.turn], s.stream));
-    s.pending[s.turn] = true;
+    s.bstate[s.turn].store(2, std::memory_order_release);
     return 0;
 }
 
-// Copy a list into page-locked staging memory; large lists with several
-// host threads (a single thread's memcpy would bound the call).
-void stage_copy(void *dst, const void *src, size_t bytes) {
-    constexpr size_t kPar = 256u << 10;
-    if (bytes < kPar) {
-        memcpy(dst, src, bytes);
-        return;
-    }
-    const int nt = std::min<int>(8, (int)(bytes / kPar) + 1);
-    const size_t per = (bytes / nt + 63) / 64 * 64;
-#pragma omp parallel for num_threads(nt) schedule(static)
-    for (int t = 0; t < nt; t++) {
-        const size_t a = (size_t)t * per, b = std::min(bytes, a + per);
+int slot_quiet(int q) {
+    if (!wait_until([&] { return S.q[q].queued.load(std::memory_order_acquire) == 0; }))
+        return gc::set_status(-1, "queue slot %d: the submitter did not drain", q);
+    return 0;
+}
+
+// Copying lists into page-locked staging memory.  One thread's memcpy of
+// lists just built elsewhere runs at about 15 GB/s on the GPU's host; the
+// copy is split between the calling thread and a few persistent workers
+// that spin briefly between calls and then sleep (a parallel region per
+// call costs more than the copy it splits).
+struct CopyPool {
+    static constexpr int kWorkers = 4;
+    static constexpr size_t kPart = 64u << 10;  // below this a list is copied by one thread
+    std::thread th[kWorkers];
+    bool started = false;
+    std::atomic<uint64_t> gen{0};
+    std::atomic<int> remaining{0};
+    std::atomic<int> sleepers{0};
+    std::atomic<bool> stop{false};
+    std::mutex mu;
+    std::condition_variable cv;
+    char *dst = nullptr;
+    const char *src = nullptr;
+    size_t bytes = 0, per = 0;
+    int parts = 0;
+
+    void part(int k) {
+        const size_t a = (size_t)k * per, b = std::min(bytes, a + per);
         if (a < b)
-            memcpy((char *)dst + a, (const char *)src + a, b - a);
+            memcpy(dst + a, src + a, b - a);
     }
+    void worker(int w) {
+        uint64_t seen = 0;
+        while (true) {
+            uint64_t g = gen.load(std::memory_order_acquire);
+            for (int spin = 0; g == seen && spin < 20000 && !stop.load(); spin++)
+                g = gen.load(std::memory_order_acquire);
+            if (g == seen) {
+                std::unique_lock<std::mutex> lk(mu);
+                sleepers++;
+                cv.wait_for(lk, std::chrono::milliseconds(20), [&] {
+                    return stop.load() || gen.load(std::memory_order_acquire) != seen;
+                });
+                sleepers--;
+                if (stop.load())
+                    return;
+                continue;
+            }
+            seen = g;
+            if (w + 1 < parts) {
+                part(w + 1);
+                remaining.fetch_sub(1, std::memory_order_release);
+            }
+        }
+    }
+    void copy(void *d, const void *sr, size_t n) {
+        const int np = (int)std::min<size_t>(kWorkers + 1, n / kPart + 1);
+        if (np <= 1) {
+            memcpy(d, sr, n);
+            return;
+        }
+        if (!started) {
+            for (int w = 0; w < kWorkers; w++) th[w] = std::thread([this, w] { worker(w); });
+            started = true;
+            atexit([] { shutdown_pool(); });
+        }
+        dst = (char *)d;
+        src = (const char *)sr;
+        bytes = n;
+        parts = np;
+        per = (n / np + 63) / 64 * 64;
+        remaining.store(np - 1, std::memory_order_relaxed);
+        gen.fetch_add(1, std::memory_order_release);
+        if (sleepers.load()) {
+            std::lock_guard<std::mutex> lk(mu);
+            cv.notify_all();
+        }
+        part(0);
+        // the workers' parts, with a bound; past it the whole list is copied
+        // here (the same bytes, so a late worker's writes change nothing)
+        if (!wait_until([&] { return remaining.load(std::memory_order_acquire) == 0; }, 10.0))
+            memcpy(d, sr, n);
+    }
+    static void shutdown_pool();
+};
+CopyPool *g_pool = nullptr;
+
+void CopyPool::shutdown_pool() {
+    if (!g_pool || !g_pool->started)
+        return;
+    {
+        std::lock_guard<std::mutex> lk(g_pool->mu);
+        g_pool->stop.store(true);
+    }
+    g_pool->cv.notify_all();
+    for (auto &t : g_pool->th)
+        if (t.joinable())
+            t.join();
+    g_pool->started = false;
+}
+
+void stage_copy(void *dst, const void *src, size_t bytes) {
+    if (!g_pool)
+        g_pool = new CopyPool();
+    g_pool->copy(dst, src, bytes);
 }
 
 int check_device_error(const char *what) {
@@ -496,8 +659,168 @@ int dispatch_list(const Routine &r, cudaStream_t st, const float *pos, float4 *a
     return gc::set_status(-1, "no kernel for routine %s", r.name);
 }
 
+// ---- deferred issue: the submitter thread ----
+// grav_mn_CUDA copies its list into a slot's staging buffer and queues a
+// job; one submitter thread takes the jobs in order and issues, on the
+// slot's stream, the copy to the device, the event that frees the staging
+// buffer, and the launch.  Errors there set the status as in the calling
+// thread (abort in the default error mode), and drain_all returns them.
+struct Job {
+    const Routine *r;
+    int q, turn, n, nblk, sz;
+    int64_t first;
+    size_t bytes;
+    float e;
+};
+
+struct Submitter {
+    static constexpr int kCap = 256;
+    Job ring[kCap];
+    std::atomic<uint64_t> head{0}, tail{0};  // next job to push / to issue
+    std::atomic<bool> sleeping{false}, stop{false};
+    std::atomic<int> err{0};
+    std::mutex mu;
+    std::condition_variable cv;
+    std::thread th;
+    bool started = false;
+    // staging buffers whose copies were issued, oldest first: polled while
+    // the queue is empty and marked free when their copy has completed, so
+    // the caller rarely waits on an event
+    std::pair<int, int> issued[kCap];
+    uint64_t issued_head = 0, issued_tail = 0;
+
+    void poll_slots() {
+        for (int q = 0; q < NQ; q++) {
+            Slot &s = S.q[q];
+            if (s.kpending.load(std::memory_order_acquire) == 1 &&
+                s.queued.load(std::memory_order_acquire) == 0 &&
+                cudaEventQuery(s.kdone) == cudaSuccess)
+                s.kpending.store(0, std::memory_order_release);
+        }
+    }
+    void poll_issued() {
+        while (issued_tail != issued_head) {
+            const auto [q, k] = issued[issued_tail % kCap];
+            Slot &s = S.q[q];
+            if (s.bstate[k].load(std::memory_order_acquire) != 2) {  // taken over by the caller
+                issued_tail++;
+                continue;
+            }
+            if (cudaEventQuery(s.copied[k]) != cudaSuccess)
+                return;
+            int two = 2;
+            s.bstate[k].compare_exchange_strong(two, 0, std::memory_order_acq_rel);
+            issued_tail++;
+        }
+    }
+
+    void issue(const Job &j) {
+        const int64_t t0 = now_ns();
+        Slot &s = S.q[j.q];
+        cudaError_t e = cudaMemcpyAsync(s.dev, s.hbuf[j.turn], j.bytes, cudaMemcpyHostToDevice,
+                                        s.stream);
+        if (e == cudaSuccess)
+            e = cudaEventRecord(s.copied[j.turn], s.stream);
+        s.bstate[j.turn].store(2, std::memory_order_release);
+        if (issued_head - issued_tail < (uint64_t)kCap)
+            issued[issued_head++ % kCap] = {j.q, j.turn};
+        int rc = e == cudaSuccess ? 0 : gc::cuda_status(e, "grav_mn_CUDA: list copy");
+        if (!rc)
+            rc = dispatch_list(*j.r, s.stream, S.devpos + 3 * j.first, S.devaccp + j.first, j.n,
+                               (const float *)s.dev, j.nblk, j.sz, j.e);
+        if (!rc && cudaEventRecord(s.kdone, s.stream) == cudaSuccess)
+            s.kpending.store(1, std::memory_order_release);
+        if (rc) {
+            int zero = 0;
+            err.compare_exchange_strong(zero, rc);
+        }
+        g_phase_ns[3] += now_ns() - t0;
+        s.queued.fetch_sub(1, std::memory_order_release);
+    }
+    void run() {
+        while (true) {
+            const uint64_t t = tail.load(std::memory_order_relaxed);
+            if (t == head.load(std::memory_order_acquire)) {
+                poll_issued();
+                poll_slots();
+                bool got = false;
+                for (int spin = 0; spin < 20000 && !got; spin++)
+                    got = t != head.load(std::memory_order_acquire);
+                if (!got) {
+                    std::unique_lock<std::mutex> lk(mu);
+                    sleeping.store(true);
+                    cv.wait_for(lk, std::chrono::milliseconds(50), [&] {
+                        return stop.load() || t != head.load(std::memory_order_acquire);
+                    });
+                    sleeping.store(false);
+                }
+                if (stop.load() && t == head.load(std::memory_order_acquire))
+                    return;
+                continue;
+            }
+            issue(ring[t % kCap]);
+            tail.store(t + 1, std::memory_order_release);
+        }
+    }
+    int push(const Job &j) {
+        if (!started) {
+            th = std::thread([this] { run(); });
+            started = true;
+            atexit([] { shutdown_submitter(); });
+        }
+        const uint64_t h = head.load(std::memory_order_relaxed);
+        const int64_t t0 = now_ns();
+        if (!wait_until([&] { return h - tail.load(std::memory_order_acquire) < (uint64_t)kCap; }))
+            return gc::set_status(-1, "grav_mn_CUDA: the submitter stopped taking jobs");
+        g_phase_ns[2] += now_ns() - t0;
+        ring[h % kCap] = j;
+        S.q[j.q].queued.fetch_add(1, std::memory_order_release);
+        head.store(h + 1, std::memory_order_release);
+        if (sleeping.load()) {
+            std::lock_guard<std::mutex> lk(mu);
+            cv.notify_one();
+        }
+        return 0;
+    }
+    int drain() {
+        const int64_t t0 = now_ns();
+        struct Add {
+            int64_t t0;
+            ~Add() { g_phase_ns[4] += now_ns() - t0; }
+        } add{t0};
+        if (!wait_until([&] {
+                return tail.load(std::memory_order_acquire) == head.load(std::memory_order_acquire);
+            }))
+            return gc::set_status(-1, "grav_mn_CUDA: the submitter did not drain");
+        return err.exchange(0);
+    }
+    static void shutdown_submitter();
+};
+Submitter *g_sub = nullptr;
+
+void Submitter::shutdown_submitter() {
+    if (!g_sub || !g_sub->started)
+        return;
+    g_sub->drain();
+    {
+        std::lock_guard<std::mutex> lk(g_sub->mu);
+        g_sub->stop.store(true);
+    }
+    g_sub->cv.notify_one();
+    if (g_sub->th.joinable())
+        g_sub->th.join();
+    g_sub->started = false;
+}
+
+Submitter &submitter() {
+    if (!g_sub)
+        g_sub = new Submitter();
+    return *g_sub;
+}
+
 int grav_mn_impl(const char *routine, const float *p, int n, int stride, const float *f,
                  int source_n, int sz, float e, int q) {
+    std::lock_guard<std::recursive_mutex> call_lock(g_call_mu);
     if (ensure_init())
         return gc::g_status;
     const Routine *r = nullptr;
@@ -523,13 +846,13 @@ int grav_mn_impl(const char *routine, const float *p, int n, int stride, const f
     if (int rc = slot_reserve(q, bytes))
         return rc;
     Slot &s = S.q[q];
+    const int64_t t0 = now_ns();
     stage_copy(s.host, f, bytes);
-    GC_CHECK(cudaMemcpyAsync(s.dev, s.host, bytes, cudaMemcpyHostToDevice, s.stream));
-    if (int rc = slot_copied(s))
-        return rc;
+    g_phase_ns[0] += now_ns() - t0;
+    g_phase_calls++;
+    s.bstate[s.turn].store(1, std::memory_order_release);
     s.inuse = true;
-    return dispatch_list(*r, s.stream, S.devpos + 3 * first, S.devaccp + first, n,
-                         (const float *)s.dev, source_n / 8, sz, e);
+    return submitter().push(Job{r, q, s.turn, n, source_n / 8, sz, first, bytes, e});
 }
 
 }  // namespace
@@ -546,7 +869,9 @@ extern "C" void CUDA_Init(void *device_prop) {
 }
 
 extern "C" void CUDA_Finalize(void) {
+    std::lock_guard<std::recursive_mutex> call_lock(g_call_mu);
     grav_groups_release_CUDA();
+    Submitter::shutdown_submitter();
     if (!S.init)
         return;
     for (int i = 0; i < NQ; i++) {
@@ -561,20 +886,36 @@ extern "C" void CUDA_Finalize(void) {
             if (s.copied[k])
                 cudaEventDestroy(s.copied[k]);
         }
+        if (s.kdone)
+            cudaEventDestroy(s.kdone);
         if (s.dev)
             cudaFree(s.dev);
-        s = Slot{};
+        s.reset();
     }
     cudaFree(S.devpos);
     cudaFree(S.devaccp);
     cudaFree(S.qdev);
     cudaFree(S.derr);
-    S = State{};
+    S.init = false;
+    S.Btab = nullptr;
+    S.bstride = 0;
+    S.nobj = 0;
+    S.devpos = nullptr;
+    S.devaccp = nullptr;
+    S.qdev = nullptr;
+    S.ncells = 0;
+    S.derr = nullptr;
 }
 
 extern "C" int vecwidthCUDA(void) { return SPT; }
 
+extern "C" void gravcuda_dropin_phases(double out[6]) {
+    for (int k = 0; k < 5; k++) out[k] = 1e-9 * (double)g_phase_ns[k].load();
+    out[5] = (double)g_phase_calls.load();
+}
+
 extern "C" int qallocCUDA(int *inuse) {
+    std::lock_guard<std::recursive_mutex> call_lock(g_call_mu);
     if (ensure_init())
         return -1;
     // slots are handed out round-robin; without the busy count the search
@@ -584,11 +925,15 @@ extern "C" int qallocCUDA(int *inuse) {
     for (int k = 0; k < NQ; k++) {
         const int i = (next + k) % NQ;
         Slot &s = S.q[i];
-        if (s.inuse) {
+        if (s.inuse && s.queued.load(std::memory_order_acquire) == 0 &&
+            s.kpending.load(std::memory_order_acquire) == 0 && g_sub && g_sub->started)
+            s.inuse = false;  // the submitter saw its last launch complete
+        if (s.inuse && s.queued.load(std::memory_order_acquire) == 0) {
             cudaError_t e = cudaStreamQuery(s.stream);
-            if (e == cudaSuccess)
+            if (e == cudaSuccess) {
                 s.inuse = false;
-            else if (e != cudaErrorNotReady) {
+                s.kpending.store(0, std::memory_order_release);
+            } else if (e != cudaErrorNotReady) {
                 gc::cuda_status(e, "cudaStreamQuery");
                 return -1;
             }
@@ -609,6 +954,7 @@ extern "C" int qallocCUDA(int *inuse) {
 }
 
 extern "C" void WalkInitSrcCUDA(float *qtab, int stride, int64_t nobj) {
+    std::lock_guard<std::recursive_mutex> call_lock(g_call_mu);
     if (ensure_init())
         return;
     if (!qtab || stride < 20 || nobj <= 0) {
@@ -636,15 +982,23 @@ extern "C" void WalkInitSrcCUDA(float *qtab, int stride, int64_t nobj) {
 }
 
 extern "C" void WalkTerminateSrcCUDA(void) {
+    std::lock_guard<std::recursive_mutex> call_lock(g_call_mu);
     if (S.qdev)
         cudaFree(S.qdev);
     S.qdev = nullptr;
     S.ncells = 0;
 }
 
+static int drain_all();
+
 extern "C" void WalkInitSinkCUDA(float *btab, int stride, int64_t nobj) {
+    std::lock_guard<std::recursive_mutex> call_lock(g_call_mu);
     if (ensure_init())
         return;
+    if (drain_all())  // queued lists of an earlier walk still read the old tables
+        return;
+    for (auto &x : g_phase_ns) x = 0;
+    g_phase_calls = 0;
     if (!btab || stride < 4 || nobj <= 0) {
         gc::set_status(-1, "WalkInitSinkCUDA: bad table");
         return;
@@ -669,6 +1023,9 @@ extern "C" void WalkInitSinkCUDA(float *btab, int stride, int64_t nobj) {
 }
 
 static int drain_all() {
+    if (g_sub && g_sub->started)
+        if (int rc = g_sub->drain())
+            return rc;
     for (int i = 0; i < NQ; i++) {
         if (S.q[i].stream)
             GC_CHECK(cudaStreamSynchronize(S.q[i].stream));
@@ -678,6 +1035,7 @@ static int drain_all() {
 }
 
 extern "C" int gravcuda_peek_accumulators(float *out, int64_t first, int64_t count) {
+    std::lock_guard<std::recursive_mutex> call_lock(g_call_mu);
     if (!S.devaccp || first < 0 || first + count > S.nobj)
         return gc::set_status(-1, "gravcuda_peek_accumulators: range outside the sink table");
     if (int rc = drain_all())
@@ -687,6 +1045,7 @@ extern "C" int gravcuda_peek_accumulators(float *out, int64_t first, int64_t cou
 }
 
 extern "C" void WalkTerminateSinkCUDA(float *btab, int stride, int64_t nobj) {
+    std::lock_guard<std::recursive_mutex> call_lock(g_call_mu);
     if (!S.devaccp) {
         gc::set_status(-1, "WalkTerminateSinkCUDA before WalkInitSinkCUDA");
         return;
@@ -725,6 +1084,7 @@ extern "C" void grav_mn_CUDA(const char *routine, const float *p, float *accp, c
 static int runs_launch(int sink_base, int m, const uint16_t *ss_index, const segment *ss_seg,
                        int ss_len, const segment *seg, int seg_len, int source_base,
                        const int *source_n, float mmass, float e, int q) {
+    std::lock_guard<std::recursive_mutex> call_lock(g_call_mu);
     if (ensure_init())
         return gc::g_status;
     if (!S.devpos)
@@ -741,6 +1101,8 @@ static int runs_launch(int sink_base, int m, const uint16_t *ss_index, const seg
     size_t o_cnt = al(o_gs + n_gs), n_cnt = source_n ? (size_t)ss_len * 4 : 0;
     size_t o_seg = al(o_cnt + n_cnt), n_seg = (size_t)seg_len * sizeof(segment);
     size_t total = o_seg + n_seg;
+    if (int rc = slot_quiet(q))
+        return rc;
     if (int rc = slot_reserve(q, total))
         return rc;
     Slot &s = S.q[q];
@@ -758,6 +1120,7 @@ static int runs_launch(int sink_base, int m, const uint16_t *ss_index, const seg
     if (int rc = slot_copied(s))
         return rc;
     s.inuse = true;
+    s.kpending.store(2, std::memory_order_release);  // launched here: query the stream
     int threads = 128;
     k_runs_k1<<<(m + threads - 1) / threads, threads, 0, s.stream>>>(
         S.devpos + 3 * (size_t)sink_base, S.devaccp + sink_base, m,
@@ -797,6 +1160,7 @@ extern "C" void grav_mnss_CUDA(const char *routine, const int sink_base, const i
 
 extern "C" void grav_qns_CUDA(const char *routine, const int base, const int m,
                               const int *source_list, const int source_n, int q) {
+    std::lock_guard<std::recursive_mutex> call_lock(g_call_mu);
     if (ensure_init())
         return;
     if (!routine || strcmp(routine, "pQQ1") != 0) {
@@ -814,7 +1178,7 @@ extern "C" void grav_qns_CUDA(const char *routine, const int base, const int m,
     if (m == 0 || source_n == 0)
         return;
     size_t bytes = (size_t)source_n * sizeof(int);
-    if (slot_reserve(q, bytes))
+    if (slot_quiet(q) || slot_reserve(q, bytes))
         return;
     Slot &s = S.q[q];
     memcpy(s.host, source_list, bytes);
@@ -825,6 +1189,7 @@ extern "C" void grav_qns_CUDA(const char *routine, const int base, const int m,
     if (slot_copied(s))
         return;
     s.inuse = true;
+    s.kpending.store(2, std::memory_order_release);  // launched here: query the stream
     k_quad_index<<<(m + 127) / 128, 128, 0, s.stream>>>(S.devpos + 3 * (size_t)base,
                                                         S.devaccp + base, m, (const int *)s.dev,
                                                         source_n, S.qdev, (int)S.ncells, S.derr);
@@ -836,6 +1201,7 @@ extern "C" void grav_qns_CUDA(const char *routine, const int base, const int m,
 extern "C" void grav_qnss_CUDA(const char *routine, const int base, const int m,
                                const segment *seg, const float *source, const int source_n,
                                int q) {
+    std::lock_guard<std::recursive_mutex> call_lock(g_call_mu);
     if (ensure_init())
         return;
     if (!routine || strcmp(routine, "pQ1_qnss") != 0) {
@@ -851,7 +1217,7 @@ extern "C" void grav_qnss_CUDA(const char *routine, const int base, const int m,
     auto al = [](size_t x) { return (x + 127) & ~(size_t)127; };
     size_t n_seg = (size_t)m * sizeof(segment);
     size_t o_src = al(n_seg), n_src = (size_t)source_n * 13 * sizeof(float);
-    if (slot_reserve(q, o_src + n_src))
+    if (slot_quiet(q) || slot_reserve(q, o_src + n_src))
         return;
     Slot &s = S.q[q];
     memcpy(s.host, seg, n_seg);
@@ -864,6 +1230,7 @@ extern "C" void grav_qnss_CUDA(const char *routine, const int base, const int m,
     if (slot_copied(s))
         return;
     s.inuse = true;
+    s.kpending.store(2, std::memory_order_release);  // launched here: query the stream
     k_quad_runs<<<(m + 127) / 128, 128, 0, s.stream>>>(
         S.devpos + 3 * (size_t)base, S.devaccp + base, m, (const segment *)s.dev,
         (const float *)((char *)s.dev + o_src), source_n, S.derr);

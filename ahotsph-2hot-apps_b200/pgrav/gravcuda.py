@@ -26,7 +26,7 @@ EXPORTS = [
     "grav_groups_CUDA", "grav_direct_fp64_CUDA", "grav_plan_set_timing", "grav_plan_kernel_ms",
     "grav_groups_eval_dev_CUDA", "grav_plan_set_tree_CUDA", "grav_plan_refit_CUDA",
     "grav_plan_bodies", "grav_plan_integrate_CUDA", "grav_plan_step_CUDA",
-    "grav_plan_set_integrator_CUDA",
+    "grav_plan_set_integrator_CUDA", "gravcuda_dropin_phases",
     "grav_plan_adjoint_CUDA", "grav_plan_retune_CUDA", "grav_plan_get_tuning",
     "grav_groups_CUDA_phases", "grav_groups_release_CUDA", "grav_fp32_peak_CUDA",
     "grav_plan_build_CUDA", "grav_plan_order", "grav_plan_build_phases", "grav_plan_problem",
@@ -105,6 +105,7 @@ def lib(record_errors=True):
             "grav_plan_refit_CUDA": ([vp, vp], i32), "grav_plan_bodies": ([vp], vp),
             "grav_plan_integrate_CUDA": ([vp, vp, vp, vp, vp], i32),
             "grav_plan_set_integrator_CUDA": ([vp, i32], i32),
+            "gravcuda_dropin_phases": ([vp], None),
             "grav_plan_step_CUDA": ([vp, vp, vp, vp, vp, i32], i32),
             "grav_plan_adjoint_CUDA": ([vp, vp, vp, vp], i32),
             "grav_plan_retune_CUDA": ([vp, vp], i32), "grav_plan_get_tuning": ([vp, vp], i32),
@@ -498,6 +499,15 @@ def drive_mn(dropin, first, count, packs, e):
                                float(e))
     check()
     return secs
+
+
+def dropin_phases():
+    """gravcuda_dropin_phases: seconds of staging copies, staging waits, queue
+    waits, the submitter's CUDA calls and the final drain, and the call count."""
+    out = (ctypes.c_double * 6)()
+    lib().gravcuda_dropin_phases(out)
+    return {"staging_copy_s": out[0], "staging_wait_s": out[1], "queue_wait_s": out[2],
+            "submitter_s": out[3], "drain_s": out[4], "calls": int(out[5])}
 
 
 def direct_fp64(points, sinks, eps2, box=0.0):

@@ -147,6 +147,17 @@ int grav_mn_status_CUDA(const char *routine, const float *p, const int n, const 
 int gravcuda_peek_accumulators(float *out, int64_t first, int64_t count);
 
 /*
+ * Where the drop-in calls' time went since the last WalkInitSinkCUDA, in
+ * seconds: [0] copying lists out of the caller's memory into page-locked
+ * staging, [1] waiting for a free staging buffer, [2] waiting for room in
+ * the submitter's queue (grav_mn_CUDA returns after the staging copy; a
+ * submitter thread issues the device copy and the launch), [3] the
+ * submitter's CUDA calls, [4] the drain at WalkTerminateSinkCUDA; [5] the
+ * number of grav_mn_CUDA calls.
+ */
+void gravcuda_dropin_phases(double out[6]);
+
+/*
  * ---- batched index-list evaluation ----
  * A step's problem: bodies in tree order and cell monopoles in one point
  * table, quadrupole and order-4 cell tables, sink groups, and per-group
