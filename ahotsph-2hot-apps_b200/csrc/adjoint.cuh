@@ -55,6 +55,7 @@
 // (k_adjoint_hexa).  Record sums are flushed with FP64 atomics once per
 // tile, sink sums once per item.
 #pragma once
+#include <type_traits>
 
 namespace {
 
@@ -170,7 +171,7 @@ __global__ void __launch_bounds__(256) k_adjoint_points(AdjProblem P) {
             const float4 p_next = record(e_next);
             const uint32_t e_after = entry(b0 + 2 * kAdjTile);
             // this lane's record, negated position relative to the centre
-            const uint32_t idx = e_cur & NLN_IDX_MASK;
+            const uint32_t idx = e_cur & NLN_IDX_MASK, e_prev_code = e_cur >> NLN_IDX_BITS;
             float nx = -1.0e3f, ny = -1.0e3f, nz = -1.0e3f, m = 0.f;  // massless and far: adds 0
             const bool live = lane < nt && e_cur != 0xffffffffu;
             if (live) {
@@ -182,40 +183,52 @@ __global__ void __launch_bounds__(256) k_adjoint_points(AdjProblem P) {
             e_next = e_after;
             p_cur = p_next;
             float ax = 0.f, ay = 0.f, az = 0.f, am = 0.f;  // the record's sums of t, w.d/r^3 + u/r
+            // A body against itself (d = 0: offsets of one point, exact
+            // negatives) adds t on both sides of the same body; it is left
+            // out, since the two FP32 sums would not cancel it exactly
+            // (t = m w / eps^3).  Only tiles holding one of the group's own
+            // bodies can meet it: those run the loop with the check.
+            const bool own = live && (e_prev_code == NLN_SHIFT_NONE) &&
+                             idx - (uint32_t)G.first < (uint32_t)G.count;
+            auto steps = [&](auto self_c) {
+                constexpr bool SELF = decltype(self_c)::value;
 #pragma unroll 4
-            for (int k = 0; k < 16; k++) {
+                for (int k = 0; k < 16; k++) {
 #pragma unroll
-                for (int hh = 0; hh < 2; hh++) {
-                    const float sx_ = hh ? Sx.y : Sx.x, sy_ = hh ? Sy.y : Sy.x, sz_ = hh ? Sz.y : Sz.x;
-                    const float wx_ = hh ? Wx.y : Wx.x, wy_ = hh ? Wy.y : Wy.x, wz_ = hh ? Wz.y : Wz.x;
-                    const float u_ = hh ? U.y : U.x;
-                    const float dx = sx_ + nx, dy = sy_ + ny, dz = sz_ + nz;
-                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, e2.x)));
-                    const float ri = rsqrt_fast(r2), ri2 = ri * ri;
-                    // a body against itself (d = 0: offsets of one point, exact negatives)
-                    // adds t on both sides of the same body; leave it out, since the
-                    // two FP32 sums would not cancel it exactly (t = m w / eps^3)
-                    const bool self = dx == 0.f && dy == 0.f && dz == 0.f;
-                    const float mr3 = self ? 0.f : m * ri * ri2;
-                    const float wd = fmaf(wx_, dx, fmaf(wy_, dy, wz_ * dz));
-                    const float in = fmaf(-3.f * ri2, wd, -u_);
-                    const float ex = fmaf(in, dx, wx_), ey = fmaf(in, dy, wy_), ez = fmaf(in, dz, wz_);
-                    const float tx = mr3 * ex, ty = mr3 * ey, tz = mr3 * ez;
-                    if (hh) { Gx.y += tx; Gy.y += ty; Gz.y += tz; } else { Gx.x += tx; Gy.x += ty; Gz.x += tz; }
-                    ax += tx;
-                    ay += ty;
-                    az += tz;
-                    am = fmaf(ri, fmaf(wd, ri2, u_), am);
+                    for (int hh = 0; hh < 2; hh++) {
+                        const float sx_ = hh ? Sx.y : Sx.x, sy_ = hh ? Sy.y : Sy.x, sz_ = hh ? Sz.y : Sz.x;
+                        const float wx_ = hh ? Wx.y : Wx.x, wy_ = hh ? Wy.y : Wy.x, wz_ = hh ? Wz.y : Wz.x;
+                        const float u_ = hh ? U.y : U.x;
+                        const float dx = sx_ + nx, dy = sy_ + ny, dz = sz_ + nz;
+                        const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, e2.x)));
+                        const float ri = rsqrt_fast(r2), ri2 = ri * ri;
+                        float mr3 = m * ri * ri2;
+                        if (SELF && dx == 0.f && dy == 0.f && dz == 0.f)
+                            mr3 = 0.f;
+                        const float wd = fmaf(wx_, dx, fmaf(wy_, dy, wz_ * dz));
+                        const float in = fmaf(-3.f * ri2, wd, -u_);
+                        const float ex = fmaf(in, dx, wx_), ey = fmaf(in, dy, wy_), ez = fmaf(in, dz, wz_);
+                        const float tx = mr3 * ex, ty = mr3 * ey, tz = mr3 * ez;
+                        if (hh) { Gx.y += tx; Gy.y += ty; Gz.y += tz; } else { Gx.x += tx; Gy.x += ty; Gz.x += tz; }
+                        ax += tx;
+                        ay += ty;
+                        az += tz;
+                        am = fmaf(ri, fmaf(wd, ri2, u_), am);
+                    }
+                    nx = __shfl_sync(FULL, nx, next);
+                    ny = __shfl_sync(FULL, ny, next);
+                    nz = __shfl_sync(FULL, nz, next);
+                    m = __shfl_sync(FULL, m, next);
+                    ax = __shfl_sync(FULL, ax, next);
+                    ay = __shfl_sync(FULL, ay, next);
+                    az = __shfl_sync(FULL, az, next);
+                    am = __shfl_sync(FULL, am, next);
                 }
-                nx = __shfl_sync(FULL, nx, next);
-                ny = __shfl_sync(FULL, ny, next);
-                nz = __shfl_sync(FULL, nz, next);
-                m = __shfl_sync(FULL, m, next);
-                ax = __shfl_sync(FULL, ax, next);
-                ay = __shfl_sync(FULL, ay, next);
-                az = __shfl_sync(FULL, az, next);
-                am = __shfl_sync(FULL, am, next);
-            }
+            };
+            if (__any_sync(FULL, own))
+                steps(std::true_type{});
+            else
+                steps(std::false_type{});
             if (live) {
                 if (idx < nb) {
                     double *g = P.gbody + (size_t)idx * 4;

@@ -578,7 +578,10 @@ static void stf_project(int l, const double *T, double *A) {
     }
 }
 
-static void cell_momx(const double *x, const double *m, long first, int count, orc_momx *o) {
+/* Mass, centre of mass and the trace-free moments up to order `order`
+   (0 or 1: none; 2: A_2; 4: A_2..A_4) of a cell's bodies. */
+static void cell_momx_upto(const double *x, const double *m, long first, int count, int order,
+                           orc_momx *o) {
     double M = 0, s[3] = {0, 0, 0};
     for (long b = first; b < first + count; b++) {
         M += m[b];
@@ -587,7 +590,7 @@ static void cell_momx(const double *x, const double *m, long first, int count, o
     o->M = M;
     for (int d = 0; d < 3; d++) o->X[d] = M > 0 ? s[d] / M : 0.0;
     double T[81];
-    for (int l = 2; l <= 4; l++) {
+    for (int l = 2; l <= order; l++) {
         memset(T, 0, sizeof(T));
         for (long b = first; b < first + count; b++) {
             double y[3] = {x[3 * b] - o->X[0], x[3 * b + 1] - o->X[1], x[3 * b + 2] - o->X[2]};
@@ -599,6 +602,10 @@ static void cell_momx(const double *x, const double *m, long first, int count, o
         }
         stf_project(l, T, o->A[l - 2]);
     }
+}
+
+static void cell_momx(const double *x, const double *m, long first, int count, orc_momx *o) {
+    cell_momx_upto(x, m, first, count, 4, o);
 }
 
 /* Monopole plus orders 2..order of a cell at X (M, A) on a sink at s. */
@@ -855,10 +862,10 @@ double orc_fd_partial_loss_x(int s, long j, long n, const double *x, const doubl
             M = m[idx];
         } else {
             const long c = kind == 0 ? (long)idx - n : (long)idx;
-            cell_momx(x, m, cfirst[c], ccount[c], &mo);
+            order = kind == 0 ? 0 : kind == 1 ? 2 : 4;
+            cell_momx_upto(x, m, cfirst[c], ccount[c], order, &mo);
             for (int k = 0; k < 3; k++) X[k] = mo.X[k] + sh[k];
             M = mo.M;
-            order = kind == 0 ? 0 : kind == 1 ? 2 : 4;
         }
         for (int k = 0; k < gcount[g]; k++) {
             long i = gfirst[g] + k;
@@ -887,9 +894,10 @@ double orc_fd_partial_loss_x(int s, long j, long n, const double *x, const doubl
             if (kind == 0 && (long)idx < n)
                 continue;
             const long c = kind == 0 ? (long)idx - n : (long)idx;
-            if (!done[c]) {
-                cell_momx(x, m, cfirst[c], ccount[c], &moms[c]);
-                done[c] = 1;
+            const int need = kind == 0 ? 1 : kind == 1 ? 2 : 4;
+            if (done[c] < need) {
+                cell_momx_upto(x, m, cfirst[c], ccount[c], need, &moms[c]);
+                done[c] = (char)need;
             }
         }
     }
