@@ -693,33 +693,39 @@ __global__ void k_adjoint_ewald_groups(AdjProblem P) {
             pz[k] = pz[k - 1] * (-u[2]) / k;
         }
         double a[3] = {0, 0, 0}, H[6] = {0, 0, 0, 0, 0, 0};
+        // every multi-index (a0, a1, a2) of order <= 4 (constant bounds, so
+        // the loops unroll fully and the arrays stay in registers)
 #pragma unroll
-        for (int L = 0; L <= 4; L++) {
+        for (int a0 = 0; a0 <= 4; a0++)
 #pragma unroll
-            for (int p2 = 0; p2 < mi_n(L); p2++) {
-                const int a0 = L - mi_s(p2), a1 = mi_a1(p2), a2 = mi_a2(p2);
-                const int q = ew::base(L) + p2;
-                const double W = px[a0] * py[a1] * pz[a2];
-                mb[q] += uu * W;
-                if (L <= 3) {
-                    // the accelerations' and the Mbar's w terms at order L + 1
+            for (int a1 = 0; a1 <= 4; a1++)
 #pragma unroll
-                    for (int k = 0; k < 3; k++) {
-                        const int qk = ew::base(L + 1) + mi_up(p2, k);
-                        a[k] += M[qk] * W;
-                        mb[qk] += w[k] * W;
+                for (int a2 = 0; a2 <= 4; a2++) {
+                    const int L = a0 + a1 + a2;
+                    if (L > 4)
+                        continue;
+                    const int q = ew::idx(a0, a1, a2);
+                    const double W = px[a0] * py[a1] * pz[a2];
+                    mb[q] += uu * W;
+                    if (L <= 3) {
+                        // the accelerations' and the Mbar's w terms at order L + 1
+#pragma unroll
+                        for (int k = 0; k < 3; k++) {
+                            const int qk = ew::idx(a0 + (k == 0), a1 + (k == 1), a2 + (k == 2));
+                            a[k] += M[qk] * W;
+                            mb[qk] += w[k] * W;
+                        }
+                    }
+                    if (L <= 2) {
+#pragma unroll
+                        for (int k = 0; k < 3; k++)
+#pragma unroll
+                            for (int l = k; l < 3; l++)
+                                H[mi_pair(k, l)] +=
+                                    M[ew::idx(a0 + (k == 0) + (l == 0), a1 + (k == 1) + (l == 1),
+                                              a2 + (k == 2) + (l == 2))] * W;
                     }
                 }
-                if (L <= 2) {
-#pragma unroll
-                    for (int k = 0; k < 3; k++)
-#pragma unroll
-                        for (int l = k; l < 3; l++)
-                            H[mi_pair(k, l)] +=
-                                M[ew::base(L + 2) + mi_up(mi_up(p2, k), l)] * W;
-                }
-            }
-        }
         double t[3];
 #pragma unroll
         for (int k = 0; k < 3; k++)
@@ -759,50 +765,67 @@ __device__ __forceinline__ void ew_adj_moment(const float *Mb, const float *o, c
                                               double *g) {
     constexpr float ik = 1.f / (float)fact(K);
 #pragma unroll
-    for (int pb = 0; pb < mi_n(K); pb++) {
-        float acc = 0.f;
+    for (int b0 = 0; b0 <= K; b0++)
 #pragma unroll
-        for (int La = 0; La <= SMAX; La++)
+        for (int b1 = 0; b1 <= K; b1++) {
+            if (b0 + b1 > K)
+                continue;
+            const int b2 = K - b0 - b1;
+            float acc = 0.f;
 #pragma unroll
-            for (int pa = 0; pa < mi_n(La); pa++) {
-                const int q = ew::base(La + K) + mi_loc(mi_a1(pa) + mi_a1(pb), mi_a2(pa) + mi_a2(pb));
-                acc = fmaf(Mb[ew::base(La) + pa], ew_D(o, f5, q), acc);
-            }
-        atomicAdd(g + pb, (double)(acc * ik));
-    }
+            for (int a0 = 0; a0 <= SMAX; a0++)
+#pragma unroll
+                for (int a1 = 0; a1 <= SMAX; a1++)
+#pragma unroll
+                    for (int a2 = 0; a2 <= SMAX; a2++) {
+                        if (a0 + a1 + a2 > SMAX)
+                            continue;
+                        acc = fmaf(Mb[ew::idx(a0, a1, a2)],
+                                   ew_D(o, f5, ew::idx(a0 + b0, a1 + b1, a2 + b2)), acc);
+                    }
+            atomicAdd(g + (ew::idx(b0, b1, b2) - ew::base(K)), (double)(acc * ik));
+        }
 }
 
 // N[g] += sum_{|b| = K} S[b] / b! Mbar[g - b] for |g| <= 4
 template <int K>
 __device__ __forceinline__ void ew_adj_conv(const float *S, const float *Mb, float *N) {
 #pragma unroll
-    for (int Lg = K; Lg <= 4; Lg++)
+    for (int b0 = 0; b0 <= K; b0++)
 #pragma unroll
-        for (int pg = 0; pg < mi_n(Lg); pg++) {
-            float acc = N[ew::base(Lg) + pg];
+        for (int b1 = 0; b1 <= K; b1++) {
+            if (b0 + b1 > K)
+                continue;
+            const int b2 = K - b0 - b1;
+            const float sb = S[ew::idx(b0, b1, b2) - ew::base(K)] *
+                             (ew::ifact(b0) * ew::ifact(b1) * ew::ifact(b2));
 #pragma unroll
-            for (int pb = 0; pb < mi_n(K); pb++) {
-                const int a1 = mi_a1(pg) - mi_a1(pb), a2 = mi_a2(pg) - mi_a2(pb);
-                const int a0 = (Lg - mi_s(pg)) - (K - mi_s(pb));
-                if (a0 < 0 || a1 < 0 || a2 < 0)
-                    continue;
-                const float ib = 1.f / (float)(fact(K - mi_s(pb)) * fact(mi_a1(pb)) * fact(mi_a2(pb)));
-                acc = fmaf(S[pb] * ib, Mb[ew::base(Lg - K) + mi_loc(a1, a2)], acc);
-            }
-            N[ew::base(Lg) + pg] = acc;
+            for (int a0 = 0; a0 <= 4 - K; a0++)
+#pragma unroll
+                for (int a1 = 0; a1 <= 4 - K; a1++)
+#pragma unroll
+                    for (int a2 = 0; a2 <= 4 - K; a2++) {
+                        if (a0 + a1 + a2 > 4 - K)
+                            continue;
+                        const int q = ew::idx(a0 + b0, a1 + b1, a2 + b2);
+                        N[q] = fmaf(sb, Mb[ew::idx(a0, a1, a2)], N[q]);
+                    }
         }
 }
 
 __global__ void __launch_bounds__(64) k_adjoint_ewald_entries(AdjProblem P) {
     const int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
+    __shared__ float mb_s[2][36];  // the group's Mbar, read by every lane alike
+    float *Mb = mb_s[threadIdx.x >> 5];
+    if (g < P.ngroups) {
+        for (int q = lane; q < 35; q += 32) Mb[q] = (float)P.mbar[g * 35 + q];
+    }
+    __syncwarp();
     if (g >= P.ngroups)
         return;
     const nln_group G = P.groups[g];
     const double c[3] = {G.cen[0], G.cen[1], G.cen[2]};
-    float Mb[35];
-#pragma unroll
-    for (int q = 0; q < 35; q++) Mb[q] = (float)P.mbar[g * 35 + q];
     const uint32_t nb = (uint32_t)P.nbodies;
     for (int64_t k = P.cptr[g] + lane; k < P.cptr[g + 1]; k += 32) {
         const uint32_t ent = P.clist[k];
@@ -852,12 +875,18 @@ __global__ void __launch_bounds__(64) k_adjoint_ewald_entries(AdjProblem P) {
         }
         float dX[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-        for (int L = 0; L <= 4; L++)
+        for (int a0 = 0; a0 <= 4; a0++)
 #pragma unroll
-            for (int p = 0; p < mi_n(L); p++)
+            for (int a1 = 0; a1 <= 4; a1++)
 #pragma unroll
-                for (int l = 0; l < 3; l++)
-                    dX[l] = fmaf(N[ew::base(L) + p], ew_D(o, f5, ew::base(L + 1) + mi_up(p, l)), dX[l]);
+                for (int a2 = 0; a2 <= 4; a2++) {
+                    if (a0 + a1 + a2 > 4)
+                        continue;
+                    const float nq = N[ew::idx(a0, a1, a2)];
+                    dX[0] = fmaf(nq, ew_D(o, f5, ew::idx(a0 + 1, a1, a2)), dX[0]);
+                    dX[1] = fmaf(nq, ew_D(o, f5, ew::idx(a0, a1 + 1, a2)), dX[1]);
+                    dX[2] = fmaf(nq, ew_D(o, f5, ew::idx(a0, a1, a2 + 1)), dX[2]);
+                }
         double *gt = h ? P.gcell + (size_t)(idx - nb) * kCellAdj : P.gbody + (size_t)idx * 4;
         if (h) {
             atomicAdd(gt + 0, (double)dm);

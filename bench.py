@@ -61,12 +61,17 @@ FLOPS = np.array([23, 23, 66, 217], np.float64)
 # traffic is this times its interactions (traffic grows with list entries)
 DRAM_BYTES_PER_INTERACTION = {"hexa": 0.2007, "quad": 0.193, "point": 0.164}
 ALL_CONFIGS = ("plummer64k", "box128", "batch1024", "adjoint", "kdk256")
+# blocks that run only when named: the periodic adjoint alone (--adjoint-workload)
+EXTRA_CONFIGS = ("adjoint_periodic",)
 
 WORKLOADS = {
     # N = 2^24 periodic box, order 4 + Ewald (the metric's N)
     # (MAC tolerance chosen for <= 1e-4 rms relative force error)
     "box256": dict(kind="box", n1d=256, rms_disp=0.5, p2cut=7, p4cut=20, ewald=True,
                    tol=1.5e-6, sample=8192),
+    # 64^3 periodic box, order 4 + Ewald (small cases for profiling)
+    "box64": dict(kind="box", n1d=64, rms_disp=0.25, p2cut=7, p4cut=20, ewald=True,
+                  tol=2.5e-6, sample=2048),
     # 128^3 periodic box, order 4 + Ewald
     "box128": dict(kind="box", n1d=128, rms_disp=0.25, p2cut=7, p4cut=20, ewald=True,
                    tol=2.5e-6, sample=4096),
@@ -601,20 +606,20 @@ def config_adjoint(args, stream):
                                                       np.sqrt(np.mean(emd ** 2)) <= 1e-3)}
     res["leapfrog"] = leapfrog_check(args)
     res["leapfrog_2p20"] = leapfrog_time(n, eps2, tol)
-    res["headline_adjoint"] = headline_adjoint(stream)
+    res["headline_adjoint"] = headline_adjoint(stream, args.adjoint_workload)
     return res
 
 
-def headline_adjoint(stream, reps=2):
-    """The adjoint of the headline workload (the 256^3 periodic box, order 4
-    + Ewald, tree and lists built on the GPU): forward and adjoint times
-    with CUDA events on the same plan (the adjoint reads the evaluation's
-    correction moments).  Its correctness is pinned in
+def headline_adjoint(stream, workload="box256", reps=2):
+    """The adjoint of a periodic workload (the headline 256^3 box by default,
+    order 4 + Ewald, tree and lists built on the GPU): forward and adjoint
+    times with CUDA events on the same plan (the adjoint reads the
+    evaluation's correction moments).  Its correctness is pinned in
     tests/test_adjoint_gpu.py against FP64 differences of the oracle on
     periodic order-4 lists with the correction."""
     import torch
     from pgrav import gravcuda as gc
-    w = WORKLOADS["box256"]
+    w = WORKLOADS[workload]
     pos, m, eps2, box = make_problem(w)
     n = len(m)
     bodies = torch.empty((n, 4), dtype=torch.float32, device="cuda")
@@ -643,7 +648,7 @@ def headline_adjoint(stream, reps=2):
         tm[name] = a.elapsed_time(b) / reps
     finite = bool(torch.isfinite(grad).all().item())
     plan.free()
-    return {"workload": "periodic 256^3 box, order 4 + Ewald (the headline), lists built on the GPU",
+    return {"workload": f"periodic {w['n1d']}^3 box, order 4 + Ewald, lists built on the GPU",
             "n_bodies": n, "forward_ms": tm["forward"], "adjoint_ms": tm["adjoint"],
             "adjoint_over_forward": tm["adjoint"] / tm["forward"], "grad_finite": finite}
 
@@ -836,11 +841,14 @@ def main():
                     help="pick the tile shapes with the autotuner first (always for batch1024)")
     ap.add_argument("--configs", default="all",
                     help="configuration blocks measured after the timed region: all, none, or a "
-                         "comma list of " + ",".join(ALL_CONFIGS))
+                         "comma list of " + ",".join(ALL_CONFIGS + EXTRA_CONFIGS))
+    ap.add_argument("--adjoint-workload", default="box256",
+                    choices=[k for k, v in WORKLOADS.items() if v["kind"] == "box"],
+                    help="the periodic workload of the adjoint blocks' forward/adjoint timing")
     args = ap.parse_args()
     configs = (list(ALL_CONFIGS) if args.configs == "all" else
                [] if args.configs == "none" else [c for c in args.configs.split(",") if c])
-    unknown = [c for c in configs if c not in ALL_CONFIGS]
+    unknown = [c for c in configs if c not in ALL_CONFIGS + EXTRA_CONFIGS]
     if unknown:
         ap.error(f"unknown configuration(s) {unknown}")
     w = WORKLOADS[args.workload]
@@ -1121,7 +1129,9 @@ def main():
                                            args.kdk_steps, args.kdk_dt, args.kdk_rebuild)
                 else:
                     fn = {"plummer64k": config_plummer64k, "box128": config_box128,
-                          "batch1024": config_batch1024, "adjoint": config_adjoint}[name]
+                          "batch1024": config_batch1024, "adjoint": config_adjoint,
+                          "adjoint_periodic": lambda a, st: headline_adjoint(
+                              st, a.adjoint_workload)}[name]
                     blocks[name] = fn(args, stream)
             except Exception as exc:  # one failing leg must not hide the others
                 blocks[name] = {"error": f"{type(exc).__name__}: {exc}"}
