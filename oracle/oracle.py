@@ -139,8 +139,27 @@ def ref():
                                         ctypes.c_long, _f32p, ctypes.c_float, _f32p]
         lib.ref_segments_k1.restype = ctypes.c_long
         lib.ref_ewald_batch.argtypes = [_f64p, ctypes.c_long, ctypes.c_double, _f64p, _f64p]
+        if hasattr(lib, "ref_periodic_le"):
+            lib.ref_periodic_le.argtypes = [ctypes.c_long, _f32p, _f32p, ctypes.c_double,
+                                            ctypes.c_int, ctypes.c_double, _i64p, ctypes.c_long,
+                                            _f64p, _f64p]
         _ref = lib
     return _ref
+
+
+def ref_periodic_le(pos, mass, L, eps2, sinks, nimage=2):
+    """The reference's periodic scheme (ref_harness.c ref_periodic_le): the
+    direct sum over the (2 nimage + 1)^3 images of the box plus the compiled
+    FixCubeEwaldLE far field (nln/ewald_le2.c), for a box of side L centred
+    on the origin; (acc (nsink, 3), phi (nsink,)) in FP64, G = 1."""
+    pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    mass = np.ascontiguousarray(mass, np.float32)
+    sinks = np.ascontiguousarray(sinks, np.int64)
+    acc = np.zeros((len(sinks), 3))
+    phi = np.zeros(len(sinks))
+    ref().ref_periodic_le(len(mass), pos.ravel(), mass, float(L), int(nimage), float(eps2), sinks,
+                          len(sinks), acc.ravel(), phi)
+    return acc, phi
 
 
 def aligned_f32(n, align=64):

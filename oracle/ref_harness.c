@@ -8,6 +8,7 @@
  * over a list suffix, mac.c:549-676) so that tests and the CPU baseline can
  * run them over many sinks and many lists.
  */
+#include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -149,4 +150,80 @@ void ref_ewald_batch(const double *x, long n, double L, double *f, double *phi) 
         double xi[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
         ewald(xi, L, f + 3 * i, phi + i);
     }
+}
+
+/*
+ * The reference's own periodic scheme, for comparison
+ * with other periodic evaluations: n bodies in a cube of side L centred on
+ * the origin (positions in [-L/2, L/2)), G = 1.
+ *   - every body in each of the (2 nimage + 1)^3 images of the box
+ *     (SetGravOffset, nln/mac.c:91-111) summed directly in FP64 with the
+ *     Plummer softening eps2 on every pair, the sink's own body in its own
+ *     image included as the lists include it (phi -= m/eps, no force):
+ *     the limit the reference's tree walk over those images approximates;
+ *   - then FixCubeEwaldLE (nln/main.c:1811-1859) with subtract_background
+ *     = 0: the lattice beyond those images from the compiled
+ *     nln/ewald_le2.c (calculate_cartesian_moments, ewald_background,
+ *     ewald_le), scaled by L G rho and L^2 G rho as there.
+ * acc: 3 doubles per sink, phi: one, for the bodies sinks[0..nsink).
+ */
+typedef struct {
+    float mass;
+    float pos[3];
+} le_body; /* the layout of oracle/ref_stubs/physics.h's body */
+void calculate_cartesian_moments(le_body *btab, int nobj, double L, float *Q, int msb);
+void ewald_background(const float xx[3], float mass, double phicorr, double acc[3], double *phi);
+void ewald_le(const float xx[3], double acc[3], double *phi, float *Q, int nimage);
+
+void ref_periodic_le(long n, const float *pos, const float *mass, double L, int nimage,
+                     double eps2, const long *sinks, long nsink, double *acc, double *phi) {
+    le_body *bt = (le_body *)malloc(sizeof(le_body) * (size_t)n);
+    double mtot = 0.0;
+    for (long i = 0; i < n; i++) {
+        bt[i].mass = mass[i];
+        for (int d = 0; d < 3; d++) bt[i].pos[d] = pos[3 * i + d];
+        mtot += mass[i];
+    }
+    static float Q[1716];
+    calculate_cartesian_moments(bt, (int)n, L, Q, 0);
+    const double grho = mtot / (L * L * L);
+    double phicorr = 0.0;
+    for (int i = -nimage; i <= nimage; i++)
+        for (int j = -nimage; j <= nimage; j++)
+            for (int k = -nimage; k <= nimage; k++)
+                if (i || j || k)
+                    phicorr += 1.0 / sqrt((double)(i * i + j * j + k * k));
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long s = 0; s < nsink; s++) {
+        const long i = sinks[s];
+        double a[3] = {0, 0, 0}, p = 0.0;
+        for (int ii = -nimage; ii <= nimage; ii++)
+            for (int jj = -nimage; jj <= nimage; jj++)
+                for (int kk = -nimage; kk <= nimage; kk++) {
+                    const double off[3] = {ii * L, jj * L, kk * L};
+                    for (long j = 0; j < n; j++) {
+                        double d[3];
+                        for (int c = 0; c < 3; c++)
+                            d[c] = (double)pos[3 * j + c] + off[c] - (double)pos[3 * i + c];
+                        const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + eps2;
+                        if (r2 <= 0.0)
+                            continue;
+                        const double ri = 1.0 / sqrt(r2), mr3 = mass[j] * ri * ri * ri;
+                        p -= mass[j] * ri;
+                        for (int c = 0; c < 3; c++) a[c] += mr3 * d[c];
+                    }
+                }
+        float r[3];
+        double f[3], ph;
+        for (int c = 0; c < 3; c++) r[c] = (float)(pos[3 * i + c] / L);
+        ewald_background(r, mass[i], phicorr, f, &ph);
+        for (int c = 0; c < 3; c++) a[c] += f[c] * L * grho;
+        p += ph * L * L * grho;
+        ewald_le(r, f, &ph, Q, nimage);
+        for (int c = 0; c < 3; c++) a[c] += f[c] * L * grho;
+        p += ph * L * L * grho;
+        for (int c = 0; c < 3; c++) acc[3 * s + c] = a[c];
+        phi[s] = p;
+    }
+    free(bt);
 }

@@ -265,3 +265,25 @@ def test_table_interpolation_bound_against_reference(host):
     r = np.linalg.norm(y, axis=1)
     assert np.abs(out[:, 0] - (p + 1.0 / r)).max() < 1e-7 / L
     assert np.abs(out[:, 1:4] - (f - y / r[:, None] ** 3)).max() < 3e-5 / L ** 2
+
+
+@needs_ref
+def test_reference_periodic_scheme_matches_ewald_sum():
+    """The reference's own periodic scheme -- every body in the 125 images of
+    the box (SetGravOffset, nln/mac.c:91-111) plus FixCubeEwaldLE's order-8
+    local expansion of the rest (nln/main.c:1811-1859, the compiled
+    nln/ewald_le2.c) -- against the Ewald-summed direct sum (the oracle of
+    nln/grav_n2.c) on a 16^3 clustered box: the same forces within the
+    expansion's truncation, potentials up to one constant (the two schemes'
+    conventions for the mean and the self images)."""
+    from pgrav import ics
+    pos, m = ics.grf_box(16, seed=7)
+    eps2 = (1 / 16 / 50) ** 2
+    pc = (pos.astype(np.float64) - 0.5).astype(np.float32)   # the reference centres its box
+    samp = np.arange(0, len(m), 16)
+    acc, phi = O.ref_periodic_le(pc, m, 1.0, eps2, samp)
+    a2, p2 = O.direct_ewald(pc.astype(np.float64), m.astype(np.float64), 1.0, eps2, samp)
+    e = np.linalg.norm(acc - a2, axis=1) / np.sqrt(np.mean((a2 ** 2).sum(1)))
+    assert np.sqrt(np.mean(e ** 2)) < 3e-5 and e.max() < 1e-4, (np.sqrt(np.mean(e ** 2)), e.max())
+    d = phi - p2
+    assert d.std() < 1e-6 * np.sqrt(np.mean(p2 ** 2)), d.std()

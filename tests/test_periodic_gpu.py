@@ -101,3 +101,31 @@ def test_batched_ewald_small_box_large_groups(gc):
     samp = np.random.default_rng(1).choice(t.n, 256, replace=False)
     ref = gc.direct_fp64(t.points[:t.n], samp, eps2, box=1.0)
     assert rel_rms(got[samp, :3], ref[:, :3]) < 2e-3
+
+
+@pytest.mark.skipif(not __import__("oracle.oracle", fromlist=["x"]).ref_available(),
+                    reason="oracle/_ref (the reference's compiled CPU code) is not built")
+def test_batched_matches_reference_periodic_scheme(gc):
+    """The periodic evaluation (each source in the image nearest the group,
+    the rest of the lattice from the Ewald table) against the reference's own
+    periodic scheme on the same bodies: every body in the 125 images of the
+    box plus FixCubeEwaldLE's order-8 local expansion (nln/mac.c:91-111,
+    nln/main.c:1811-1859, the compiled nln/ewald_le2.c).  64^3 clustered box,
+    order 4, MAC 2e-6: forces within the 1e-4 bar, potentials up to one
+    constant (the schemes' conventions for the mean and the self images)."""
+    from oracle import oracle as O
+    from pgrav import host, ics
+    n1 = 64
+    pos, m = ics.grf_box(n1, seed=9)
+    eps2 = (1.0 / n1 / 50) ** 2
+    t = host.Tree(pos, m, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=2e-6, box=1.0)
+    plan = gc.Plan(t, eps2, ewald=True)
+    plan.eval()
+    got = plan.download()
+    plan.free()
+    samp = np.sort(np.random.default_rng(2).choice(t.n, 256, replace=False))
+    xt = (t.points[:t.n, :3].astype(np.float64) - 0.5).astype(np.float32)  # centred, as there
+    acc, phi = O.ref_periodic_le(xt, t.points[:t.n, 3], 1.0, eps2, samp)
+    assert rel_rms(got[samp, :3], acc) <= 1e-4, rel_rms(got[samp, :3], acc)
+    d = got[samp, 3] - phi
+    assert d.std() < 1e-4 * np.sqrt(np.mean(phi ** 2)), d.std()
