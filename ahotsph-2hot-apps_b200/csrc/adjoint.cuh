@@ -88,6 +88,7 @@ struct AdjProblem {
     float ew_self, ew_trace;
     const EwStored *ewm;     // the forward's per-group moments
     double *mbar;            // 35 per group: dL/dM[alpha]
+    double *gstf;            // kStfIndep per cell: the correction's trace-free moment duals
 };
 
 // Offset of the record at image code `code` relative to the group centre c,
@@ -659,6 +660,92 @@ __global__ void __launch_bounds__(32 * kAdjHexaWarps) k_adjoint_hexa(AdjProblem 
     }
 }
 
+// STF projection (in place) of a symmetric tensor of order L held by its
+// components (the multi-index layout): subtract the trace parts.
+template <typename T>
+__device__ __forceinline__ void stf2(T *G) {
+    const T tr = (G[mi_pair(0, 0)] + G[mi_pair(1, 1)] + G[mi_pair(2, 2)]) / (T)3;
+    G[mi_pair(0, 0)] -= tr;
+    G[mi_pair(1, 1)] -= tr;
+    G[mi_pair(2, 2)] -= tr;
+}
+
+// the component of order L of the sorted index tuple (i1 <= i2 <= ...)
+__host__ __device__ constexpr int tup3(int i, int j, int k) {
+    return mi_loc((i == 1) + (j == 1) + (k == 1), (i == 2) + (j == 2) + (k == 2));
+}
+__host__ __device__ constexpr int tup4(int i, int j, int k, int l) {
+    return mi_loc((i == 1) + (j == 1) + (k == 1) + (l == 1), (i == 2) + (j == 2) + (k == 2) + (l == 2));
+}
+
+template <typename T>
+__device__ __forceinline__ void stf3(T *G) {
+    T t[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) t[k] = G[tup3(k, 0, 0)] + G[tup3(k, 1, 1)] + G[tup3(k, 2, 2)];
+    T o[10];
+#pragma unroll
+    for (int p = 0; p < 10; p++) {
+        // the tuple of component p
+        const int a0 = 3 - mi_s(p), a1 = mi_a1(p);
+        const int i[3] = {0 < a0 ? 0 : (0 < a0 + a1 ? 1 : 2), 1 < a0 ? 0 : (1 < a0 + a1 ? 1 : 2),
+                          2 < a0 ? 0 : (2 < a0 + a1 ? 1 : 2)};
+        T s = 0;
+        if (i[0] == i[1]) s += t[i[2]];
+        if (i[0] == i[2]) s += t[i[1]];
+        if (i[1] == i[2]) s += t[i[0]];
+        o[p] = G[p] - s / (T)5;
+    }
+#pragma unroll
+    for (int p = 0; p < 10; p++) G[p] = o[p];
+}
+
+template <typename T>
+__device__ __forceinline__ void stf4(T *G) {
+    T T2[6];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int q = k; q < 3; q++)
+            T2[mi_pair(k, q)] = G[tup4(k, q, 0, 0)] + G[tup4(k, q, 1, 1)] + G[tup4(k, q, 2, 2)];
+    const T tt = T2[mi_pair(0, 0)] + T2[mi_pair(1, 1)] + T2[mi_pair(2, 2)];
+    T o[15];
+#pragma unroll
+    for (int p = 0; p < 15; p++) {
+        const int a0 = 4 - mi_s(p), a1 = mi_a1(p);
+        int i[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) i[r] = r < a0 ? 0 : (r < a0 + a1 ? 1 : 2);
+        T s6 = 0, s3 = 0;
+        // the six pairs (r, q) and the indices left over
+        const int pr[6][4] = {{0, 1, 2, 3}, {0, 2, 1, 3}, {0, 3, 1, 2},
+                              {1, 2, 0, 3}, {1, 3, 0, 2}, {2, 3, 0, 1}};
+#pragma unroll
+        for (int e = 0; e < 6; e++)
+            if (i[pr[e][0]] == i[pr[e][1]])
+                s6 += T2[mi_pair(i[pr[e][2]] < i[pr[e][3]] ? i[pr[e][2]] : i[pr[e][3]],
+                                 i[pr[e][2]] < i[pr[e][3]] ? i[pr[e][3]] : i[pr[e][2]])];
+        if (i[0] == i[1] && i[2] == i[3]) s3 += 1;
+        if (i[0] == i[2] && i[1] == i[3]) s3 += 1;
+        if (i[0] == i[3] && i[1] == i[2]) s3 += 1;
+        o[p] = G[p] - s6 / (T)7 + s3 * tt / (T)35;
+    }
+#pragma unroll
+    for (int p = 0; p < 15; p++) G[p] = o[p];
+}
+
+// A trace-free tensor of order L is fixed by its 2L + 1 components with at
+// most one z index (a2 <= 1); the rest follow from A[a0,a1,a2] =
+// -A[a0+2,a1,a2-2] - A[a0,a1+2,a2-2], in layout order.
+template <int L>
+__device__ __forceinline__ void stf_fill(double *A) {
+#pragma unroll
+    for (int p = 0; p < mi_n(L); p++)
+        if (mi_a2(p) >= 2)
+            A[p] = -A[mi_loc(mi_a1(p), mi_a2(p) - 2)] - A[mi_loc(mi_a1(p) + 2, mi_a2(p) - 2)];
+}
+constexpr int kStfIndep = 5 + 7 + 9;  // doubles per cell of the correction's moment duals
+
 // Periodic correction, sink side: one warp per group, a lane per sink.
 // Mbar[alpha] = sum_i u_i (-u_i)^alpha/alpha! + sum_k w_ik (-u_i)^(alpha-e_k)/(alpha-e_k)!
 // (|alpha - e_k| <= 3, the terms the accelerations use), and each sink's
@@ -762,7 +849,7 @@ __device__ __forceinline__ float ew_D(const float *o, const float *f5, int q) {
 
 template <int K, int SMAX>
 __device__ __forceinline__ void ew_adj_moment(const float *Mb, const float *o, const float *f5,
-                                              double *g) {
+                                              float *G) {
     constexpr float ik = 1.f / (float)fact(K);
 #pragma unroll
     for (int b0 = 0; b0 <= K; b0++)
@@ -783,8 +870,25 @@ __device__ __forceinline__ void ew_adj_moment(const float *Mb, const float *o, c
                         acc = fmaf(Mb[ew::idx(a0, a1, a2)],
                                    ew_D(o, f5, ew::idx(a0 + b0, a1 + b1, a2 + b2)), acc);
                     }
-            atomicAdd(g + (ew::idx(b0, b1, b2) - ew::base(K)), (double)(acc * ik));
+            G[ew::idx(b0, b1, b2) - ew::base(K)] = acc * ik;
         }
+}
+
+// The trace-free part of a moment dual of order K, added to the cell's
+// independent components (a2 <= 1): 2K + 1 atomics instead of (K+1)(K+2)/2.
+template <int K>
+__device__ __forceinline__ void add_indep(float *G, double *dst) {
+    if (K == 2)
+        stf2(G);
+    else if (K == 3)
+        stf3(G);
+    else
+        stf4(G);
+    int k = 0;
+#pragma unroll
+    for (int p = 0; p < mi_n(K); p++)
+        if (mi_a2(p) <= 1)
+            atomicAdd(dst + k++, (double)G[p]);
 }
 
 // N[g] += sum_{|b| = K} S[b] / b! Mbar[g - b] for |g| <= 4
@@ -862,15 +966,20 @@ __global__ void __launch_bounds__(64) k_adjoint_ewald_entries(AdjProblem P) {
         if (h) {
             float S[15];
             double *gc = P.gcell + (size_t)(idx - nb) * kCellAdj;
+            double *gi = P.gstf + (size_t)(idx - nb) * kStfIndep;
+            float G[15];
             ew_quad(h->R, h->q2, S);
             ew_adj_conv<2>(S, Mb, N);
-            ew_adj_moment<2, 3>(Mb, o, f5, gc + kAdjG2);
+            ew_adj_moment<2, 3>(Mb, o, f5, G);
+            add_indep<2>(G, gi);
             ew_oct(h->R, h->q3, S);
             ew_adj_conv<3>(S, Mb, N);
-            ew_adj_moment<3, 2>(Mb, o, f5, gc + kAdjG3);
+            ew_adj_moment<3, 2>(Mb, o, f5, G);
+            add_indep<3>(G, gi + 5);
             ew_hex(h->R, h->q4, S);
             ew_adj_conv<4>(S, Mb, N);
-            ew_adj_moment<4, 1>(Mb, o, f5, gc + kAdjG4);
+            ew_adj_moment<4, 1>(Mb, o, f5, G);
+            add_indep<4>(G, gi + 12);
             atomicAdd(gc + kAdjB2, (double)(Mb[0] * (1.f / 6.f) * P.ew_trace));
         }
         float dX[3] = {0.f, 0.f, 0.f};
@@ -902,95 +1011,49 @@ __global__ void __launch_bounds__(64) k_adjoint_ewald_entries(AdjProblem P) {
     }
 }
 
-// STF projection (in place) of a symmetric tensor of order L held by its
-// components (the multi-index layout): subtract the trace parts.
-__device__ __forceinline__ void stf2(double *G) {
-    const double tr = (G[mi_pair(0, 0)] + G[mi_pair(1, 1)] + G[mi_pair(2, 2)]) / 3.0;
-    G[mi_pair(0, 0)] -= tr;
-    G[mi_pair(1, 1)] -= tr;
-    G[mi_pair(2, 2)] -= tr;
-}
-
-// the component of order L of the sorted index tuple (i1 <= i2 <= ...)
-__host__ __device__ constexpr int tup3(int i, int j, int k) {
-    return mi_loc((i == 1) + (j == 1) + (k == 1), (i == 2) + (j == 2) + (k == 2));
-}
-__host__ __device__ constexpr int tup4(int i, int j, int k, int l) {
-    return mi_loc((i == 1) + (j == 1) + (k == 1) + (l == 1), (i == 2) + (j == 2) + (k == 2) + (l == 2));
-}
-
-__device__ __forceinline__ void stf3(double *G) {
-    double t[3];
-#pragma unroll
-    for (int k = 0; k < 3; k++) t[k] = G[tup3(k, 0, 0)] + G[tup3(k, 1, 1)] + G[tup3(k, 2, 2)];
-    double o[10];
-#pragma unroll
-    for (int p = 0; p < 10; p++) {
-        // the tuple of component p
-        const int a0 = 3 - mi_s(p), a1 = mi_a1(p);
-        const int i[3] = {0 < a0 ? 0 : (0 < a0 + a1 ? 1 : 2), 1 < a0 ? 0 : (1 < a0 + a1 ? 1 : 2),
-                          2 < a0 ? 0 : (2 < a0 + a1 ? 1 : 2)};
-        double s = 0.0;
-        if (i[0] == i[1]) s += t[i[2]];
-        if (i[0] == i[2]) s += t[i[1]];
-        if (i[1] == i[2]) s += t[i[0]];
-        o[p] = G[p] - s / 5.0;
-    }
-#pragma unroll
-    for (int p = 0; p < 10; p++) G[p] = o[p];
-}
-
-__device__ __forceinline__ void stf4(double *G) {
-    double T2[6];
-#pragma unroll
-    for (int k = 0; k < 3; k++)
-#pragma unroll
-        for (int q = k; q < 3; q++)
-            T2[mi_pair(k, q)] = G[tup4(k, q, 0, 0)] + G[tup4(k, q, 1, 1)] + G[tup4(k, q, 2, 2)];
-    const double tt = T2[mi_pair(0, 0)] + T2[mi_pair(1, 1)] + T2[mi_pair(2, 2)];
-    double o[15];
-#pragma unroll
-    for (int p = 0; p < 15; p++) {
-        const int a0 = 4 - mi_s(p), a1 = mi_a1(p);
-        int i[4];
-#pragma unroll
-        for (int r = 0; r < 4; r++) i[r] = r < a0 ? 0 : (r < a0 + a1 ? 1 : 2);
-        double s6 = 0.0, s3 = 0.0;
-        // the six pairs (r, q) and the indices left over
-        const int pr[6][4] = {{0, 1, 2, 3}, {0, 2, 1, 3}, {0, 3, 1, 2},
-                              {1, 2, 0, 3}, {1, 3, 0, 2}, {2, 3, 0, 1}};
-#pragma unroll
-        for (int e = 0; e < 6; e++)
-            if (i[pr[e][0]] == i[pr[e][1]])
-                s6 += T2[mi_pair(i[pr[e][2]] < i[pr[e][3]] ? i[pr[e][2]] : i[pr[e][3]],
-                                 i[pr[e][2]] < i[pr[e][3]] ? i[pr[e][3]] : i[pr[e][2]])];
-        if (i[0] == i[1] && i[2] == i[3]) s3 += 1.0;
-        if (i[0] == i[2] && i[1] == i[3]) s3 += 1.0;
-        if (i[0] == i[3] && i[1] == i[2]) s3 += 1.0;
-        o[p] = G[p] - s6 / 7.0 + s3 * tt / 35.0;
-    }
-#pragma unroll
-    for (int p = 0; p < 15; p++) G[p] = o[p];
-}
-
 // Per cell with a non-zero adjoint: project the moment duals onto their
 // trace-free parts and fold the moments' dependence on the centre of mass
 // into Xbar (Xbar' = Xbar - 3 PG_3.A_2 - 4 PG_4.A_3); flag marks the cells
 // the bodies' pass visits.
-__global__ void k_adjoint_cells(double *__restrict__ gcell, const nln_hcell *__restrict__ hc,
-                                int64_t nc, int *__restrict__ flag) {
+__global__ void k_adjoint_cells(double *__restrict__ gcell, const double *__restrict__ gstf,
+                                const nln_hcell *__restrict__ hc, int64_t nc,
+                                int *__restrict__ flag) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc)
         return;
     double *G = gcell + (size_t)c * kCellAdj;
     bool any = false;
     for (int q = 0; q < kCellAdj; q++) any |= G[q] != 0.0;
-    flag[c] = any;
-    if (!any)
+    const double *I = gstf ? gstf + (size_t)c * kStfIndep : nullptr;
+    bool anyi = false;
+    if (I)
+        for (int q = 0; q < kStfIndep; q++) anyi |= I[q] != 0.0;
+    flag[c] = any || anyi;
+    if (!any && !anyi)
         return;
     stf2(G + kAdjG2);
     stf3(G + kAdjG3);
     stf4(G + kAdjG4);
+    if (anyi) {
+        // the correction's duals, already trace-free, from their independent parts
+        double A2[6], A3[10], A4[15];
+        int k = 0;
+#pragma unroll
+        for (int p = 0; p < 6; p++) A2[p] = mi_a2(p) <= 1 ? I[k++] : 0.0;
+#pragma unroll
+        for (int p = 0; p < 10; p++) A3[p] = mi_a2(p) <= 1 ? I[k++] : 0.0;
+#pragma unroll
+        for (int p = 0; p < 15; p++) A4[p] = mi_a2(p) <= 1 ? I[k++] : 0.0;
+        stf_fill<2>(A2);
+        stf_fill<3>(A3);
+        stf_fill<4>(A4);
+#pragma unroll
+        for (int p = 0; p < 6; p++) G[kAdjG2 + p] += A2[p];
+#pragma unroll
+        for (int p = 0; p < 10; p++) G[kAdjG3 + p] += A3[p];
+#pragma unroll
+        for (int p = 0; p < 15; p++) G[kAdjG4 + p] += A4[p];
+    }
     if (hc) {
         float A2[6], A3[10];
         const nln_hcell &h = hc[c];
@@ -1086,10 +1149,10 @@ __global__ void k_adjoint_bodies(const float4 *__restrict__ pts, const int32_t *
 struct grav_adjoint_state {
     int32_t *leaf = nullptr, *parent = nullptr;
     int *flag = nullptr;
-    double *gbody = nullptr, *gcell = nullptr, *mbar = nullptr;
+    double *gbody = nullptr, *gcell = nullptr, *mbar = nullptr, *gstf = nullptr;
     ~grav_adjoint_state() {
         for (void *p : {(void *)leaf, (void *)parent, (void *)flag, (void *)gbody, (void *)gcell,
-                        (void *)mbar})
+                        (void *)mbar, (void *)gstf})
             if (p)
                 cudaFree(p);
     }
@@ -1157,6 +1220,8 @@ extern "C" int grav_plan_adjoint_CUDA(grav_plan *pl, const float *wu, float *gra
             e = cudaMalloc((void **)&A->gcell, nc * kCellAdj * sizeof(double));
         if (e == cudaSuccess && pl->dp.ewald)
             e = cudaMalloc((void **)&A->mbar, ng * 35 * sizeof(double));
+        if (e == cudaSuccess && pl->dp.ewald)
+            e = cudaMalloc((void **)&A->gstf, nc * kStfIndep * sizeof(double));
         if (e != cudaSuccess) {
             delete A;
             return gc::cuda_status(e, "grav_plan_adjoint_CUDA: scratch");
@@ -1166,6 +1231,8 @@ extern "C" int grav_plan_adjoint_CUDA(grav_plan *pl, const float *wu, float *gra
     grav_adjoint_state *A = pl->adj;
     GC_CHECK(cudaMemsetAsync(A->gbody, 0, nb * 4 * sizeof(double), st));
     GC_CHECK(cudaMemsetAsync(A->gcell, 0, nc * kCellAdj * sizeof(double), st));
+    if (A->gstf)
+        GC_CHECK(cudaMemsetAsync(A->gstf, 0, nc * kStfIndep * sizeof(double), st));
     GC_CHECK(cudaMemsetAsync(pl->dp.counters, 0, 4 * sizeof(int), st));
     AdjProblem P{};
     P.points = pl->dp.points;
@@ -1196,6 +1263,7 @@ extern "C" int grav_plan_adjoint_CUDA(grav_plan *pl, const float *wu, float *gra
     P.ew_trace = pl->dp.ew_trace;
     P.ewm = pl->ewm;
     P.mbar = A->mbar;
+    P.gstf = A->gstf;
     const unsigned blocks = (unsigned)pl->nsm * 4;
     if (P.nitems[KP] > 0)
         k_adjoint_points<<<blocks, 256, 0, st>>>(P);
@@ -1210,8 +1278,8 @@ extern "C" int grav_plan_adjoint_CUDA(grav_plan *pl, const float *wu, float *gra
         GC_CHECK(cudaGetLastError());
     }
     if (nc > 0)
-        k_adjoint_cells<<<(unsigned)((nc + 127) / 128), 128, 0, st>>>(A->gcell, pl->dp.hcells, nc,
-                                                                       A->flag);
+        k_adjoint_cells<<<(unsigned)((nc + 127) / 128), 128, 0, st>>>(A->gcell, A->gstf,
+                                                                       pl->dp.hcells, nc, A->flag);
     k_adjoint_bodies<<<(unsigned)((nb + 127) / 128), 128, 0, st>>>(
         pl->dp.points, A->leaf, A->parent, pl->dp.qcells, pl->dp.hcells, A->gcell, A->flag,
         A->gbody, nb, reinterpret_cast<float4 *>(grad));

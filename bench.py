@@ -69,7 +69,10 @@ WORKLOADS = {
     # (MAC tolerance chosen for <= 1e-4 rms relative force error)
     "box256": dict(kind="box", n1d=256, rms_disp=0.5, p2cut=7, p4cut=20, ewald=True,
                    tol=1.5e-6, sample=8192),
-    # 64^3 periodic box, order 4 + Ewald (small cases for profiling)
+    # 32^3 and 64^3 periodic boxes, order 4 + Ewald (small cases: the
+    # periodic adjoint's check, profiling)
+    "box32": dict(kind="box", n1d=32, rms_disp=0.25, p2cut=7, p4cut=20, ewald=True,
+                  tol=2.5e-6, sample=1024),
     "box64": dict(kind="box", n1d=64, rms_disp=0.25, p2cut=7, p4cut=20, ewald=True,
                   tol=2.5e-6, sample=2048),
     # 128^3 periodic box, order 4 + Ewald
@@ -630,6 +633,62 @@ def config_adjoint(args, stream):
     res["leapfrog"] = leapfrog_check(args)
     res["leapfrog_2p20"] = leapfrog_time(n, eps2, tol)
     res["headline_adjoint"] = headline_adjoint(stream, args.adjoint_workload)
+    res["periodic_32"] = periodic_adjoint_check(stream)
+    return res
+
+
+def periodic_adjoint_check(stream, nsel=3, seed=37):
+    """The adjoint of the periodic 32^3 box (order 4 + Ewald, lists built on
+    the GPU): its time against the evaluation's, and FP64 central
+    differences (h = 1e-6) of the oracle's evaluation of the same lists at
+    nsel bodies (positions and masses), the correction summed exactly over
+    each entry's bodies.  The bar is the correction's truncation (the
+    kernels use cell moments and each group's Taylor series of it)."""
+    import torch
+    from oracle import oracle as O
+    from pgrav import gravcuda as gc, host
+    w = WORKLOADS["box32"]
+    pos, m, eps2, box = make_problem(w)
+    n = len(m)
+    kw = dict(leaf_max=16, group_max=32, p2cut=w["p2cut"], p4cut=w["p4cut"], tol=w["tol"])
+    res = headline_adjoint(stream, "box32")
+    rng = np.random.default_rng(seed)
+    wu_h = rng.normal(size=(n, 4)).astype(np.float32)
+    b = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    b[:, :3] = torch.from_numpy(np.asarray(pos, np.float32)).cuda()
+    b[:, 3] = torch.from_numpy(np.asarray(m, np.float32)).cuda()
+    plan = gc.Plan.build(None, None, eps2, bodies=b, box=box, ewald=True, **kw)
+    order = plan.order()
+    wu = torch.from_numpy(wu_h[order]).cuda()
+    grad = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    plan.eval(stream.cuda_stream)
+    plan.adjoint(wu.data_ptr(), grad.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    g = grad.cpu().numpy().astype(np.float64)   # tree order
+    plan.free()
+    t0 = time.perf_counter()
+    t = host.Tree(pos, m, box=box, **kw)
+    assert np.array_equal(np.asarray(t.order), order)
+    chk = O.ListsFP64(t, ewald=True)
+    sel = rng.choice(n, nsel, replace=False)
+    chk.select(sel)
+    x = np.asarray(t.sorted_pos, np.float64)
+    mm = np.asarray(t.points[:n, 3], np.float64)
+    wt = wu_h[order].astype(np.float64)
+    coords = [(s, c) for s in range(nsel) for c in (0, 1, 2, 3)]
+    fd = chk.fd_grad(x, mm, wt[:, :3], wt[:, 3], eps2, coords, h=1e-6,
+                     mass_rel=True).reshape(nsel, 4)
+    ad = g[sel]
+    sx, sm = float(np.sqrt(np.mean(g[:, :3] ** 2))), float(np.sqrt(np.mean(g[:, 3] ** 2)))
+    ex = float(np.abs(ad[:, :3] - fd[:, :3]).max() / sx)
+    em = float(np.abs(ad[:, 3] - fd[:, 3]).max() / sm)
+    res["fd"] = {"h": 1e-6, "bodies": nsel, "coordinates": 4 * nsel, "cpu_s": time.perf_counter() - t0,
+                 "max_err_over_grad_rms_x": ex, "max_err_over_grad_rms_m": em, "bar": 5e-3,
+                 "meets_target": bool(ex <= 5e-3 and em <= 5e-3),
+                 "oracle": "FP64 evaluation of the same lists (image shifts, order-4 cells), the "
+                           "correction summed exactly over each entry's bodies"}
+    res["target_ratio"] = 2.5
+    res["meets_target"] = bool(res["adjoint_over_forward"] <= 2.5 and res["fd"]["meets_target"])
     return res
 
 
