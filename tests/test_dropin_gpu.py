@@ -221,3 +221,28 @@ def test_grav_qns_rejects_bad_indices(gc, golden):
     with pytest.raises(gc.GravError):
         d.terminate()
     d.terminate_src()
+
+
+def test_dropin_phases_are_counted():
+    """gravcuda_dropin_phases after a walk of drop-in calls: every call
+    counted, the staging copies and the submitter's CUDA calls timed."""
+    import numpy as np
+    from pgrav import gravcuda as gc, host, ics
+    pos, m = ics.plummer(4000, seed=5)
+    t = host.Tree(pos, m, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-4,
+                  emit_aosoa=True)
+    gids = np.arange(min(64, t.ngroups))
+    packs = []
+    ncalls = 0
+    for kind, routine, sz in ((0, "pMp", 4), (1, "pQp", 13), (2, "pHp", 29)):
+        bp, data = t.aosoa_subset(gids, kind)
+        packs.append((routine, sz, bp, data))
+        ncalls += int((np.diff(bp) > 0).sum())
+    first = t.groups["first"][gids].astype(np.int64)
+    count = t.groups["count"][gids].astype(np.int32)
+    bt = gc.body_table(t.sorted_pos, t.points[:t.n, 3])
+    d = gc.DropIn(bt)
+    secs = gc.drive_mn(d, first, count, packs, 1e-4)
+    ph = gc.dropin_phases()
+    assert secs > 0 and ph["calls"] == ncalls, (ph, ncalls)
+    assert ph["staging_copy_s"] > 0 and ph["submitter_s"] > 0

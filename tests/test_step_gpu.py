@@ -257,3 +257,38 @@ def test_zeldovich_plane_wave_grows_linearly(mods):
     at = c.a_at_t(st.tvel)
     want = at * at * c.hubble(at) * psi[:, 0]
     assert np.abs(ue[:, 0] - want).max() < 2e-3 * np.abs(want).max()
+
+
+def test_cosmological_checkpoint_and_resume(tmp_path):
+    """A comoving run checkpointed at a rebuild boundary (Stepper.save keeps
+    the cosmology and the step times in the SDF header) and resumed
+    (Stepper.load) continues the straight run: the peculiar velocities are
+    stored as a dx/dt, so the canonical momenta come back to FP32 rounding."""
+    from pgrav import ics, step as S
+    from pgrav.cosmo import Cosmology
+    pos, m = ics.grf_box(16, seed=22)
+    c = Cosmology(H0=np.sqrt(8 * np.pi / 3), Omega_m=0.3, Omega_lambda=0.7)
+    t0 = c.t_at_a(0.2)
+    dt = 0.02 * t0
+    vel = np.random.default_rng(3).normal(0, 0.01, pos.shape).astype(np.float32)
+    kw = dict(leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-5)
+    mk = lambda: S.Stepper(pos, vel, m, (1 / 16 / 50) ** 2, box=1.0, rebuild=4, graph=True,
+                           tree_kw=kw, cosmo=c, tstart=t0)
+    a = mk()
+    a.run(8, dt)
+    want = a.state()
+    a.free()
+    b = mk()
+    b.run(4, dt)
+    path = tmp_path / "cosmo.sdf"
+    b.save(path)
+    b.free()
+    r = S.Stepper.load(path, graph=True, tree_kw=kw)
+    assert r.cosmo is not None and r.nsteps == 4
+    assert r.cosmo.params.Omega_lambda == pytest.approx(0.7)
+    r.run(4, dt)
+    got = r.state()
+    r.free()
+    dx = np.abs(np.mod(got[0] - want[0] + 0.5, 1.0) - 0.5)
+    assert dx.max() < 1e-6, dx.max()
+    assert np.abs(got[1] - want[1]).max() < 1e-5 * np.abs(want[1]).max()
