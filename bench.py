@@ -839,6 +839,20 @@ def leapfrog_check(args, n=4096, nsteps=16, every=4, dt=1e-3, ncoords=4):
                     "(nlnhost.h, bit-identical to the GPU builder's the autograd function uses)"}
 
 
+def job_rate(ms_local, inter_local, world, device="cpu"):
+    """Whole-job figures of `world` replicas, one per GPU, each evaluating the
+    same workload: the step time is the slowest rank's (an all-reduce MAX
+    over the process group when world > 1) and the interactions are every
+    rank's.  Returns (ms_max, interactions per second)."""
+    import torch
+    ms_t = torch.tensor([float(ms_local)], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    return ms_max, inter_local * world / (ms_max * 1e-3)
+
+
 def run_reference(args, w, rank, world):
     """--impl reference: the reference's CPU kernels on the host cores."""
     if rank != 0:
@@ -1002,13 +1016,9 @@ def main():
     ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
     kms = plan.kernel_ms()
     clocks = clk.summary()
-    ms_t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
     counts = plan.counts().astype(np.float64)
     inter = float(counts.sum())
-    value = inter * world / (ms_max * 1e-3)
+    ms_max, value = job_rate(ms, inter, world, "cuda")
 
     # ---- roofline of the dominant kernel (FP32 CUDA-core pipe): the peak is
     # measured here (FMA microkernel, grav_fp32_peak_CUDA), after the timed region
