@@ -369,8 +369,10 @@ __device__ __forceinline__ void relay_pairs(const unsigned char *stage, uint32_t
 #pragma unroll
         for (int k = 4; k < 10; k++) g[k] = f[k];
         if (KIND == KH) {
-            g[10] = -f[21];
-            g[11] = -f[25];
+            // h_z's xxz and yyz coefficients with -Xxxyy folded in (its
+            // z z-trace terms): -(Xxxxx + Xxxyy), -(Xyyyy + Xxxyy)
+            g[10] = -(f[21] + f[23]);
+            g[11] = -(f[25] + f[23]);
 #pragma unroll
             for (int k = 12; k < 19; k++) g[k] = -f[k];
             g[19] = f[19];
@@ -378,7 +380,7 @@ __device__ __forceinline__ void relay_pairs(const unsigned char *stage, uint32_t
 #pragma unroll
             for (int k = 21; k < 30; k++) g[k] = f[k];
             g[30] = -f[30];
-            g[31] = -f[23];
+            g[31] = 0.f;
         }
     } else {
 #pragma unroll

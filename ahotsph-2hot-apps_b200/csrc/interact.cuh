@@ -233,9 +233,10 @@ __device__ __forceinline__ void mono2_plummer(float2 npx, float2 npy, float2 npz
 // Two order-4 records against one sink with the paired FP32 instructions,
 // on a pair-interleaved tile: field f of records a (.x) and b (.y) sits at
 // floats 2f, 2f+1 of the pair.  Fields: 0-2 position (group-centred), 3
-// mass, 4-9 Q as in the staged record, 10 -Xxxxx, 11 -Xyyyy, 12-18 -O (the
-// octupole negated), 19-20 the octupole sums (not negated), 21-29 X, 30 -XS,
-// 31 -Xxxyy.  Working in v = source - sink = -d with those signs folded in
+// mass, 4-9 Q as in the staged record, 10 -(Xxxxx + Xxxyy), 11 -(Xyyyy +
+// Xxxyy) (h_z's xxz and yyz coefficients, the traceless moment's zz-pair
+// components folded in), 12-18 -O (the octupole negated), 19-20 the
+// octupole sums (not negated), 21-29 X, 30 -XS, 31 unused.  Working in v = source - sink = -d with those signs folded in
 // leaves no negation in the loop:
 //   e'(v) = -O:vv (so v.e' = d.e), h(v) = -h(d), U = Q.v + r^-2 (e' + r^-2 h),
 //   a   = v (m/r^3 - r^-2 (5/2 eq_2.d + 7/3 eq_3.d + 9/4 eq_4.d)) + r^-5 U,
@@ -319,17 +320,16 @@ __device__ __forceinline__ void hexa2_plummer(const float *__restrict__ pr, floa
     w = q[14];
     const float2 X7 = f2(w.x, w.y), X8 = f2(w.z, w.w);  // Xxyyz Xyyyz
     w = q[15];
-    const float2 nXS = f2(w.x, w.y), nX2 = f2(w.z, w.w);
+    const float2 nXS = f2(w.x, w.y);
     w = q[5];
-    const float2 nX0 = f2(w.x, w.y), nX4 = f2(w.z, w.w);
+    const float2 nX02 = f2(w.x, w.y), nX42 = f2(w.z, w.w);
     const float2 xxy = __fmul2_rn(vy, xx), xyy = __fmul2_rn(vx, yy), xyz = __fmul2_rn(xy, vz);
     const float2 h0 = __ffma2_rn(X0, xxx, __ffma2_rn(X3, yyy, __ffma2_rn(X1, xxy, __ffma2_rn(X5, xxz,
                       __ffma2_rn(X2, xyy, __ffma2_rn(X6, xyz, __fmul2_rn(X7, yyz)))))));
     const float2 h1 = __ffma2_rn(X3, xyy, __ffma2_rn(X1, xxx, __ffma2_rn(X4, yyy, __ffma2_rn(X8, yyz,
                       __ffma2_rn(X2, xxy, __ffma2_rn(X6, xxz, __fmul2_rn(X7, xyz)))))));
-    const float2 h2 = __ffma2_rn(nX0, xxz, __ffma2_rn(nXS, xyz, __ffma2_rn(nX4, yyz, __ffma2_rn(X5, xxx,
-                      __ffma2_rn(X8, yyy, __ffma2_rn(nX2, __fadd2_rn(xxz, yyz), __ffma2_rn(X6, xxy,
-                      __fmul2_rn(X7, xyy))))))));
+    const float2 h2 = __ffma2_rn(nX02, xxz, __ffma2_rn(nXS, xyz, __ffma2_rn(nX42, yyz, __ffma2_rn(X5, xxx,
+                      __ffma2_rn(X8, yyy, __ffma2_rn(X6, xxy, __fmul2_rn(X7, xyy)))))));
     const float2 d4 = __ffma2_rn(vx, h0, __ffma2_rn(vy, h1, __fmul2_rn(vz, h2)));
     // sums of the orders
     const float2 ri7 = __fmul2_rn(ri5, ri2), ri9 = __fmul2_rn(ri7, ri2);
