@@ -443,11 +443,10 @@ int grav_plan_adjoint_CUDA(grav_plan *plan, const float *wu, float *grad, void *
  * host threads, other streams) race on it and must be serialised by the
  * caller.  The first call on each device (with that device current) looks
  * up the scratch's address with cudaGetSymbolAddress, reads the device's SM
- * count and sets kernel attributes; make it before any stream capture.  The
- * call enqueues on `stream` (cudaStream_t as void*; NULL = legacy default)
- * and waits for that stream before it returns, on success and on every
- * error after its first enqueue, so no work of a returned call still uses
- * the scratch.  It returns 0, -1 for a rejected problem, or -2 when a
+ * count and sets kernel attributes.  The call enqueues on `stream`
+ * (cudaStream_t as void*; NULL = legacy default) and waits for that stream
+ * before it returns, on success and on every error after its first
+ * enqueue, so no work of a returned call still uses the scratch.  It returns 0, -1 for a rejected problem, or -2 when a
  * kernel flagged an error (a bad group, list offset or entry, a lost copy).
  *
  * Precondition the call cannot check: grav_problem carries no list lengths,
