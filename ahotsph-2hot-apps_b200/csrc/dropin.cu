@@ -498,8 +498,11 @@ int slot_quiet(int q) {
 // copy is split between the calling thread and a few persistent workers
 // that spin briefly between calls and then sleep (a parallel region per
 // call costs more than the copy it splits).
+#ifndef GRAV_COPY_WORKERS
+#define GRAV_COPY_WORKERS 4
+#endif
 struct CopyPool {
-    static constexpr int kWorkers = 4;
+    static constexpr int kWorkers = GRAV_COPY_WORKERS;
     static constexpr size_t kPart = 64u << 10;  // below this a list is copied by one thread
     std::thread th[kWorkers];
     bool started = false;
@@ -537,10 +540,13 @@ struct CopyPool {
                 continue;
             }
             seen = g;
-            if (w + 1 < parts) {
+            if (w + 1 < parts)
                 part(w + 1);
-                remaining.fetch_sub(1, std::memory_order_release);
-            }
+            // every worker acknowledges every generation, with or without a
+            // part: the caller publishes the next copy only after all have,
+            // so no worker can read one copy's generation and another's
+            // fields (parts, pointers)
+            remaining.fetch_sub(1, std::memory_order_release);
         }
     }
     void copy(void *d, const void *sr, size_t n) {
@@ -559,15 +565,16 @@ struct CopyPool {
         bytes = n;
         parts = np;
         per = (n / np + 63) / 64 * 64;
-        remaining.store(np - 1, std::memory_order_relaxed);
+        remaining.store(kWorkers, std::memory_order_relaxed);
         gen.fetch_add(1, std::memory_order_release);
         if (sleepers.load()) {
             std::lock_guard<std::mutex> lk(mu);
             cv.notify_all();
         }
         part(0);
-        // the workers' parts, with a bound; past it the whole list is copied
-        // here (the same bytes, so a late worker's writes change nothing)
+        // the workers' parts and acknowledgements, with a bound; past it the
+        // whole list is copied here (the same bytes, so a late worker's
+        // writes change nothing)
         if (!wait_until([&] { return remaining.load(std::memory_order_acquire) == 0; }, 10.0))
             memcpy(d, sr, n);
     }
