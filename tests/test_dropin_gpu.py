@@ -246,3 +246,48 @@ def test_dropin_phases_are_counted():
     ph = gc.dropin_phases()
     assert secs > 0 and ph["calls"] == ncalls, (ph, ncalls)
     assert ph["staging_copy_s"] > 0 and ph["submitter_s"] > 0
+
+
+def test_c_driven_calls_with_split_copies_match_oracle():
+    """The mac.c call sequence issued from C (lib/libmacdrive.so) on lists
+    long enough that the staging copy is split between the calling thread
+    and the copy workers (>= 64 KB parts), calls of every kind and size
+    back to back: every group's sinks against the oracle on the same AoSoA
+    lists.  A copy that returned before all of its parts were written would
+    hand a stale list to the device."""
+    from pgrav import gravcuda as gc, host, ics
+    pos, m = ics.grf_box(32, seed=11, rms_disp=0.3)
+    t = host.Tree(pos, m, leaf_max=16, group_max=32, p2cut=7, p4cut=20, tol=1e-5, box=1.0)
+    lens = sum(np.diff(t.ptr[k]) for k in range(3))
+    gids = np.sort(np.argsort(lens)[-40:])
+    eps2 = (1.0 / 32 / 50) ** 2
+    packs = []
+    for kind, routine, sz in ((0, "pMp", 4), (1, "pQp", 13), (2, "pHp", 29)):
+        bp, data = t.aosoa_subset(gids, kind)
+        packs.append((routine, sz, bp, data))
+    big = max(int(np.diff(bp).max()) * sz * 8 * 4 for _, sz, bp, _ in packs)
+    assert big >= 2 * (64 << 10), big          # the copy is split
+    first = t.groups["first"][gids].astype(np.int64)
+    count = t.groups["count"][gids].astype(np.int32)
+    bt = gc.body_table(t.sorted_pos, t.points[:t.n, 3])
+    gots = []
+    for _ in range(3):                           # later passes reuse the staging buffers
+        d = gc.DropIn(bt.copy())
+        gc.drive_mn(d, first, count, packs, eps2)   # ends with WalkTerminateSinkCUDA
+        gots.append(d.btab[:, 7:11].copy())
+    kinds = {"pMp": O.MONO_PLUMMER, "pQp": O.QUAD_PLUMMER, "pHp": O.HEXA_PLUMMER}
+    want = np.zeros((t.n, 4))
+    for routine, sz, bp, data in packs:
+        for j, g in enumerate(gids):
+            nblk = int(bp[j + 1] - bp[j])
+            if nblk == 0:
+                continue
+            f = O.aligned_f32(nblk * sz * 8)
+            f[:] = data[bp[j] * sz * 8:bp[j + 1] * sz * 8]
+            f0, c = int(first[j]), int(count[j])
+            for s in range(f0, f0 + c):
+                want[s] += O.list_eval(kinds[routine], f, nblk, t.sorted_pos[s], eps2)
+    rows = np.concatenate([np.arange(f0, f0 + c) for f0, c in zip(first, count)])
+    for got in gots:
+        assert rms_rel(got[rows, :3], want[rows, :3]) < RMS_TOL
+        assert rms_rel(got[rows, 3:], want[rows, 3:]) < RMS_TOL
