@@ -506,6 +506,7 @@ struct CopyPool {
     static constexpr size_t kPart = 64u << 10;  // below this a list is copied by one thread
     std::thread th[kWorkers];
     bool started = false;
+    bool retired = false;
     std::atomic<uint64_t> gen{0};
     std::atomic<int> remaining{0};
     std::atomic<int> sleepers{0};
@@ -549,11 +550,15 @@ struct CopyPool {
             remaining.fetch_sub(1, std::memory_order_release);
         }
     }
-    void copy(void *d, const void *sr, size_t n) {
+    // 0, or -1 when the workers did not acknowledge within the bound: the
+    // copy is then complete (done here) but a late worker may still write
+    // into d, so the pool retires (later copies run on the calling thread
+    // alone and publish no generation) and the call reports the failure.
+    int copy(void *d, const void *sr, size_t n) {
         const int np = (int)std::min<size_t>(kWorkers + 1, n / kPart + 1);
-        if (np <= 1) {
+        if (np <= 1 || retired) {
             memcpy(d, sr, n);
-            return;
+            return 0;
         }
         if (!started) {
             for (int w = 0; w < kWorkers; w++) th[w] = std::thread([this, w] { worker(w); });
@@ -572,11 +577,13 @@ struct CopyPool {
             cv.notify_all();
         }
         part(0);
-        // the workers' parts and acknowledgements, with a bound; past it the
-        // whole list is copied here (the same bytes, so a late worker's
-        // writes change nothing)
-        if (!wait_until([&] { return remaining.load(std::memory_order_acquire) == 0; }, 10.0))
+        // the workers' parts and acknowledgements, with a bound
+        if (!wait_until([&] { return remaining.load(std::memory_order_acquire) == 0; }, 10.0)) {
             memcpy(d, sr, n);
+            retired = true;
+            return -1;
+        }
+        return 0;
     }
     static void shutdown_pool();
 };
@@ -596,10 +603,13 @@ void CopyPool::shutdown_pool() {
     g_pool->started = false;
 }
 
-void stage_copy(void *dst, const void *src, size_t bytes) {
+int stage_copy(void *dst, const void *src, size_t bytes) {
     if (!g_pool)
         g_pool = new CopyPool();
-    g_pool->copy(dst, src, bytes);
+    if (g_pool->copy(dst, src, bytes))
+        return gc::set_status(-1, "staging copy: the copy workers did not finish within 10 s "
+                                  "(copies continue on the calling thread)");
+    return 0;
 }
 
 int check_device_error(const char *what) {
@@ -854,8 +864,10 @@ int grav_mn_impl(const char *routine, const float *p, int n, int stride, const f
         return rc;
     Slot &s = S.q[q];
     const int64_t t0 = now_ns();
-    stage_copy(s.host, f, bytes);
+    const int copied = stage_copy(s.host, f, bytes);
     g_phase_ns[0] += now_ns() - t0;
+    if (copied)
+        return copied;
     g_phase_calls++;
     s.bstate[s.turn].store(1, std::memory_order_release);
     s.inuse = true;
