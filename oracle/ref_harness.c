@@ -153,7 +153,8 @@ void ref_ewald_batch(const double *x, long n, double L, double *f, double *phi) 
 }
 
 /*
- * The reference's own periodic scheme, for comparison
+ * The reference's own periodic scheme (images in the walk plus the
+ * order-8 local expansion of FixCubeEwaldLE), for comparison
  * with other periodic evaluations: n bodies in a cube of side L centred on
  * the origin (positions in [-L/2, L/2)), G = 1.
  *   - every body in each of the (2 nimage + 1)^3 images of the box
