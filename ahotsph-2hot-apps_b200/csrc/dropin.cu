@@ -15,6 +15,7 @@
 //    the device and the launch, so the caller's next list copy overlaps the
 //    CUDA calls of this one.
 #include <cuda_runtime.h>
+#include <immintrin.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -493,6 +494,36 @@ int slot_quiet(int q) {
     return 0;
 }
 
+// Streaming copy into page-locked memory: non-temporal 32-byte stores
+// write the destination without reading it into the caches first, which a
+// plain memcpy of a few hundred KB does (glibc streams only far larger
+// copies).  The fence makes the stores visible before the copy is reported
+// done, to other threads and to the device copy that reads the buffer.
+__attribute__((target("avx2"))) void stream_copy_avx2(char *d, const char *s, size_t n) {
+    size_t i = 0;
+    for (; i + 128 <= n; i += 128) {
+        const __m256i x0 = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(s + i));
+        const __m256i x1 = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(s + i + 32));
+        const __m256i x2 = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(s + i + 64));
+        const __m256i x3 = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(s + i + 96));
+        _mm256_stream_si256(reinterpret_cast<__m256i *>(d + i), x0);
+        _mm256_stream_si256(reinterpret_cast<__m256i *>(d + i + 32), x1);
+        _mm256_stream_si256(reinterpret_cast<__m256i *>(d + i + 64), x2);
+        _mm256_stream_si256(reinterpret_cast<__m256i *>(d + i + 96), x3);
+    }
+    if (i < n)
+        memcpy(d + i, s + i, n - i);
+    _mm_sfence();
+}
+
+void copy_bytes(char *d, const char *s, size_t n) {
+    static const bool avx2 = __builtin_cpu_supports("avx2");
+    if (avx2 && n >= 4096 && ((uintptr_t)d & 31) == 0)
+        stream_copy_avx2(d, s, n);
+    else
+        memcpy(d, s, n);
+}
+
 // Copying lists into page-locked staging memory.  One thread's memcpy of
 // lists just built elsewhere runs at about 15 GB/s on the GPU's host; the
 // copy is split between the calling thread and a few persistent workers
@@ -521,7 +552,7 @@ struct CopyPool {
     void part(int k) {
         const size_t a = (size_t)k * per, b = std::min(bytes, a + per);
         if (a < b)
-            memcpy(dst + a, src + a, b - a);
+            copy_bytes(dst + a, src + a, b - a);
     }
     void worker(int w) {
         uint64_t seen = 0;
@@ -557,7 +588,7 @@ struct CopyPool {
     int copy(void *d, const void *sr, size_t n) {
         const int np = (int)std::min<size_t>(kWorkers + 1, n / kPart + 1);
         if (np <= 1 || retired) {
-            memcpy(d, sr, n);
+            copy_bytes((char *)d, (const char *)sr, n);
             return 0;
         }
         if (!started) {
