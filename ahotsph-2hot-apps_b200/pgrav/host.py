@@ -93,6 +93,16 @@ class _Handle:
             pass
 
 
+def cubic_acc(r, a):
+    """Acceleration at r (3,) from the uniform cube of half-side a and unit
+    density centred on the origin, G = 1 (nln_cubic_acc): the near-zone field
+    a background-subtracting walk adds back per sink, scaled by -rho0."""
+    rr = (ctypes.c_double * 3)(*[float(v) for v in np.asarray(r, np.float64).reshape(3)])
+    out = (ctypes.c_double * 3)()
+    lib().nln_cubic_acc(rr, ctypes.c_double(float(a)), out)
+    return np.array(out[:])
+
+
 def _view(ptr, dtype, count, owner=None):
     """A zero-copy array over library memory; the buffer keeps `owner` (the
     tree's handle) alive as long as the array exists."""

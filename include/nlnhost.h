@@ -170,6 +170,15 @@ void nln_ewald_eval(double L, const double *y, double *out);
 int nln_ewald_table(double L, int n, double reach, double *out);
 
 /*
+ * Acceleration at r (relative to the cube's centre) from a cube of half-side
+ * a and unit density, G = 1, pointing toward the cube: the field that the
+ * reference's background subtraction adds back per sink for its near zone,
+ * scaled by -rho0 (cubic_acc, nln/ewald_le2.c:773-1033; nln/mac.c:688-706).
+ * FP64, valid inside and outside the cube.
+ */
+void nln_cubic_acc(const double r[3], double a, double acc[3]);
+
+/*
  * ---- snapshots and checkpoints in the SDF format ----
  * The reference writes bodies as outbody records (nln/physics.h:49-58:
  * mass, x y z, vx vy vz, with SAVE_ACC also ax ay az phi, int64 ident;

@@ -139,6 +139,8 @@ def ref():
                                         ctypes.c_long, _f32p, ctypes.c_float, _f32p]
         lib.ref_segments_k1.restype = ctypes.c_long
         lib.ref_ewald_batch.argtypes = [_f64p, ctypes.c_long, ctypes.c_double, _f64p, _f64p]
+        if hasattr(lib, "cubic_acc"):
+            lib.cubic_acc.argtypes = [_f32p, ctypes.c_float, _f32p]
         if hasattr(lib, "ref_periodic_le"):
             lib.ref_periodic_le.argtypes = [ctypes.c_long, _f32p, _f32p, ctypes.c_double,
                                             ctypes.c_int, ctypes.c_double, _i64p, ctypes.c_long,
@@ -160,6 +162,16 @@ def ref_periodic_le(pos, mass, L, eps2, sinks, nimage=2):
     ref().ref_periodic_le(len(mass), pos.ravel(), mass, float(L), int(nimage), float(eps2), sinks,
                           len(sinks), acc.ravel(), phi)
     return acc, phi
+
+
+def ref_cubic_acc(r, a):
+    """The reference's cubic_acc (nln/ewald_le2.c:773-1033, compiled
+    unmodified): acceleration at r from the cube of half-side a and unit
+    density centred on the origin (float)."""
+    rr = np.ascontiguousarray(r, np.float32).reshape(3)
+    out = np.zeros(3, np.float32)
+    ref().cubic_acc(rr, float(a), out)
+    return out
 
 
 def aligned_f32(n, align=64):

@@ -291,3 +291,31 @@ def test_c_driven_calls_with_split_copies_match_oracle():
     for got in gots:
         assert rms_rel(got[rows, :3], want[rows, :3]) < RMS_TOL
         assert rms_rel(got[rows, 3:], want[rows, 3:]) < RMS_TOL
+
+
+def test_background_subtracted_monopoles(gc, golden):
+    """A background-subtracting walk (nln/mac.c DLRcritMACsb) hands the
+    drop-in ordinary pMp lists whose extra entries are negative-mass
+    monopoles: the uniform cubes of opened cells and of single bodies
+    (mac.c:1662-1690, 1695-1708).  grav_mn_CUDA evaluates them as it does
+    every entry; against the oracle and, on the real-mass part, the
+    reference fixture."""
+    rec = np.asarray(golden["k0_records"], np.float32)
+    sinks = golden["k0_sinks"]
+    e = float(golden["k0_e"])
+    rng = np.random.default_rng(9)
+    anti = np.zeros((57, 4), np.float32)
+    anti[:, :3] = rng.uniform(-1.5, 1.5, (57, 3))
+    anti[:, 3] = -float(rec[:, 3].mean()) * rng.uniform(0.2, 1.0, 57)   # -rho0 x cube volume
+    both = np.concatenate([rec, anti])
+    f, nblk = O.pack_aosoa(both)
+    d = gc.DropIn(gc.body_table(sinks, 1.0))
+    d.mn("pMp", 0, len(sinks), f, nblk * 8, 4, e)
+    got = d.terminate()
+    want = np.array([O.list_eval(O.MONO_PLUMMER, f, nblk, s, e) for s in sinks])
+    assert rms_rel(got[:, :3], want[:, :3]) < RMS_TOL
+    assert rms_rel(got[:, 3:], want[:, 3:]) < RMS_TOL
+    # the anti-masses alone are what separates it from the reference fixture
+    fa, na = O.pack_aosoa(anti)
+    wanta = np.array([O.list_eval(O.MONO_PLUMMER, fa, na, s, e) for s in sinks])
+    assert rms_rel(got - wanta, golden["k0_ref"]) < RMS_TOL
