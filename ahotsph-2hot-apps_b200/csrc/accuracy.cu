@@ -209,24 +209,44 @@ extern "C" int grav_direct_fp64_CUDA(const float *points, int64_t n, const int64
 // (a, b runtime values, so nothing folds), one FMA (2 flops) per chain per
 // step, in a grid of blocks_per_sm x SM count blocks of 256 threads.  The
 // chains are independent, so the FMA pipes, not the latency, bound it.
+// Both forms are timed, scalar fmaf and the paired __ffma2_rn that the
+// interaction kernels issue (kChains pairs, twice the FMAs per step), and
+// the larger rate is the peak.
 namespace {
 constexpr int kChains = 8;
 constexpr int kPeakThreads = 256;
 
+template <bool PAIRED>
 __global__ void __launch_bounds__(kPeakThreads) k_fma_peak(float *out, int iters, float a,
                                                            float b) {
-    float x[kChains];
-#pragma unroll
-    for (int k = 0; k < kChains; k++) x[k] = (float)(threadIdx.x + k) * 1e-3f;
-    for (int i = 0; i < iters; i++) {
-#pragma unroll
-        for (int u = 0; u < 16; u++)
-#pragma unroll
-            for (int k = 0; k < kChains; k++) x[k] = fmaf(x[k], a, b);
-    }
     float s = 0.f;
+    if constexpr (PAIRED) {
+        float2 x[kChains];
+        const float2 a2 = make_float2(a, a), b2 = make_float2(b, b);
 #pragma unroll
-    for (int k = 0; k < kChains; k++) s += x[k];
+        for (int k = 0; k < kChains; k++)
+            x[k] = make_float2((float)(threadIdx.x + k) * 1e-3f, (float)k * 1e-3f);
+        for (int i = 0; i < iters; i++) {
+#pragma unroll
+            for (int u = 0; u < 16; u++)
+#pragma unroll
+                for (int k = 0; k < kChains; k++) x[k] = __ffma2_rn(x[k], a2, b2);
+        }
+#pragma unroll
+        for (int k = 0; k < kChains; k++) s += x[k].x + x[k].y;
+    } else {
+        float x[kChains];
+#pragma unroll
+        for (int k = 0; k < kChains; k++) x[k] = (float)(threadIdx.x + k) * 1e-3f;
+        for (int i = 0; i < iters; i++) {
+#pragma unroll
+            for (int u = 0; u < 16; u++)
+#pragma unroll
+                for (int k = 0; k < kChains; k++) x[k] = fmaf(x[k], a, b);
+        }
+#pragma unroll
+        for (int k = 0; k < kChains; k++) s += x[k];
+    }
     if (s == -1.2345f)  // never true for these inputs; keeps the chains live
         out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
@@ -247,23 +267,28 @@ extern "C" int grav_fp32_peak_CUDA(double *tflops) {
     if (e == cudaSuccess)
         e = cudaEventCreate(&e1);
     double best = 0.0;
-    for (int rep = 0; rep < 6 && e == cudaSuccess; rep++) {
-        e = cudaEventRecord(e0, 0);
-        if (e == cudaSuccess) {
-            k_fma_peak<<<blocks, kPeakThreads>>>(out, iters, 0.999f, 1e-4f);
-            e = cudaGetLastError();
+    for (int paired = 0; paired < 2; paired++)
+        for (int rep = 0; rep < 6 && e == cudaSuccess; rep++) {
+            e = cudaEventRecord(e0, 0);
+            if (e == cudaSuccess) {
+                if (paired)
+                    k_fma_peak<true><<<blocks, kPeakThreads>>>(out, iters / 2, 0.999f, 1e-4f);
+                else
+                    k_fma_peak<false><<<blocks, kPeakThreads>>>(out, iters, 0.999f, 1e-4f);
+                e = cudaGetLastError();
+            }
+            if (e == cudaSuccess)
+                e = cudaEventRecord(e1, 0);
+            if (e == cudaSuccess)
+                e = cudaEventSynchronize(e1);
+            float ms = 0.f;
+            if (e == cudaSuccess)
+                e = cudaEventElapsedTime(&ms, e0, e1);
+            // a paired step is 2 FMAs per chain; it runs half the steps
+            const double flops = 2.0 * kChains * 16.0 * iters * (double)blocks * kPeakThreads;
+            if (e == cudaSuccess && rep > 0 && ms > 0.f)  // the first launch warms up
+                best = std::max(best, flops / (ms * 1e-3) / 1e12);
         }
-        if (e == cudaSuccess)
-            e = cudaEventRecord(e1, 0);
-        if (e == cudaSuccess)
-            e = cudaEventSynchronize(e1);
-        float ms = 0.f;
-        if (e == cudaSuccess)
-            e = cudaEventElapsedTime(&ms, e0, e1);
-        const double flops = 2.0 * kChains * 16.0 * iters * (double)blocks * kPeakThreads;
-        if (e == cudaSuccess && rep > 0 && ms > 0.f)  // the first launch warms up
-            best = std::max(best, flops / (ms * 1e-3) / 1e12);
-    }
     if (e0)
         cudaEventDestroy(e0);
     if (e1)

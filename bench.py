@@ -1042,7 +1042,8 @@ def main():
                                 "interactions",
                 "peak_source": ("measured in this run: FP32 FMA microkernel "
                                 "(grav_fp32_peak_CUDA, 8 independent chains per thread, 2048 "
-                                "threads per SM, best of 5 launches, CUDA events)"),
+                                "threads per SM, scalar and paired f32x2 FMAs, the larger of "
+                                "their best of 5 launches, CUDA events)"),
                 "peak_clocks": peak_clocks,
                 "peak_derived": derived,
                 "peak_derived_source": (f"148 SMs x 128 FP32 lanes x 2 x {sm_mhz:.0f} MHz "

@@ -344,8 +344,9 @@ int grav_direct_fp64_CUDA(const float *points, int64_t n, const int64_t *sinks, 
 
 /*
  * The FP32 CUDA-core peak of the current device, measured: a grid of
- * independent FMA chains (8 per thread, 2048 threads per SM) timed with CUDA
- * events, best of five launches after one warm-up, in TFLOP/s (2 flops per
+ * independent FMA chains (8 per thread, 2048 threads per SM), once as scalar
+ * FMAs and once as paired f32x2 FMAs, timed with CUDA events, best of five
+ * launches after one warm-up each, the larger rate in TFLOP/s (2 flops per
  * FMA).  The roofline denominator of the interaction kernels; about
  * 74 TFLOP/s on a B200 at 1965 MHz (148 SMs x 128 lanes x 2 flops x clock).
  */
