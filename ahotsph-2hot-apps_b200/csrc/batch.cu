@@ -2059,6 +2059,10 @@ extern "C" void grav_plan_free(grav_plan *pl) {
     delete pl;
 }
 
+// step.cuh: the plan's step state adopts a device-built tree's links
+int set_tree_adopt(grav_plan *pl, int64_t *cell_first, int32_t *cell_count, int32_t *cell_child,
+                   int32_t *cell_nchild, const int32_t *cell_level, cudaMemPool_t pool);
+
 namespace {
 // The device build and the plan that adopts it; buffers from the device's
 // pool (grav_groups_release_CUDA returns the memory it keeps reserved).
@@ -2094,35 +2098,25 @@ int build_plan(const nln_params *params, const float4 *bodies, int64_t n, double
     hp.ewald = params->box > 0 && ewald;
     hp.cptr = T.ptr_h[3].data();
     hp.clist = T.list[3];
-    // the tree's links (for the device refit and the adjoint) come back first:
-    // the plan takes the device buffers over
-    const int64_t nc = T.ncells;
-    std::vector<int64_t> first(nc);
-    std::vector<int32_t> count(nc), child(nc), nchild(nc), level(nc);
-    cudaError_t e = cudaMemcpy(first.data(), T.cell_first, nc * 8, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess)
-        e = cudaMemcpy(count.data(), T.cell_count, nc * 4, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess)
-        e = cudaMemcpy(child.data(), T.cell_child, nc * 4, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess)
-        e = cudaMemcpy(nchild.data(), T.cell_nchild, nc * 4, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess)
-        e = cudaMemcpy(level.data(), T.cell_level, nc * 4, cudaMemcpyDeviceToHost);
-    void *links[] = {T.cell_first, T.cell_count, T.cell_child, T.cell_nchild, T.cell_level};
-    for (void *q : links) cudaFreeAsync(q, 0);
+    // the tree's links (for the device refit and the adjoint) stay on the
+    // device: the plan's step state adopts them
+    int64_t *cfirst = T.cell_first;
+    int32_t *ccount = T.cell_count, *cchild = T.cell_child, *cnchild = T.cell_nchild,
+            *clevel = T.cell_level;
     T.cell_first = nullptr;
     T.cell_count = T.cell_child = T.cell_nchild = T.cell_level = nullptr;
-    if (e != cudaSuccess) {
-        dev_tree_free(T, pool);
-        return gc::cuda_status(e, "grav_plan_build_CUDA: tree links");
-    }
     grav_plan *pl = nullptr;
-    if (int rc = upload_impl(&hp, tuning, &pl, 0, &T))
-        return rc;  // upload_impl took the buffers over and released them
-    if (int rc = grav_plan_set_tree_CUDA(pl, first.data(), count.data(), child.data(),
-                                         nchild.data(), level.data())) {
+    if (int rc = upload_impl(&hp, tuning, &pl, 0, &T)) {
+        for (void *q : {(void *)cfirst, (void *)ccount, (void *)cchild, (void *)cnchild,
+                        (void *)clevel})
+            cudaFreeAsync(q, 0);
+        return rc;  // upload_impl took the tree's other buffers over and released them
+    }
+    const int rc_links = set_tree_adopt(pl, cfirst, ccount, cchild, cnchild, clevel, pool);
+    cudaFreeAsync(clevel, 0);
+    if (rc_links) {
         grav_plan_free(pl);
-        return rc;
+        return rc_links;
     }
     t_build = now_s() - t0;
     for (int k = 0; k < 6; k++) t_build_phase[k] = T.seconds[k];

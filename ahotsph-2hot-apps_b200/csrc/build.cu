@@ -916,6 +916,8 @@ int gpu_tree_build(const nln_params &p, const float4 *bodies, int64_t n, cudaStr
     if (hbad)
         return gc::set_status(-1, "GPU tree build: a group's walk did not cover every body "
                                   "exactly once, or overflowed its stack");
+    const double t_count = now_s() - t0;
+    t0 = now_s();
     for (int k = 0; k < 4; k++) out.ptr_h[k].assign(ng + 1, 0);
     for (int64_t g = 0; g < ng; g++) {
         // a group's lists cover every body once: no kind can exceed the point table
@@ -938,6 +940,8 @@ int gpu_tree_build(const nln_params &p, const float4 *bodies, int64_t n, cudaStr
         BC(cudaMemcpyAsync(dptr[k], out.ptr_h[k].data(), (ng + 1) * sizeof(int64_t),
                            cudaMemcpyHostToDevice, st));
     }
+    out.seconds[5] = now_s() - t0;  // offsets and list allocation
+    t0 = now_s();
     BC(cudaMemsetAsync(flag, 0, sizeof(unsigned), st));
     k_walk_fill<<<grid_of(ng, 128), 128, 0, st>>>(wc, spos, n, out.groups, ng, P, dptr[0], dptr[1],
                                               dptr[2], dptr[3], out.list[0], out.list[1],
@@ -948,7 +952,7 @@ int gpu_tree_build(const nln_params &p, const float4 *bodies, int64_t n, cudaStr
     if (hbad)
         return gc::set_status(-1, "GPU tree build: the filling walk differs from the counting "
                                   "walk (0x%x)", hbad);
-    out.seconds[4] = now_s() - t0;
+    out.seconds[4] = t_count + (now_s() - t0);
     // ---- the tree links, handed on
     out.cell_first = C.first;
     out.cell_count = C.count;

@@ -29,7 +29,7 @@ struct DevTree {
     int64_t counts[4] = {0, 0, 0, 0};  // interactions: body, monopole cell, quadrupole, order 4
     std::vector<nln_group> groups_h;
     std::vector<int64_t> ptr_h[4];  // ngroups + 1 list offsets per kind
-    double seconds[6] = {0, 0, 0, 0, 0, 0};  // sort, cells, moments, groups, walk, copy-back
+    double seconds[6] = {0, 0, 0, 0, 0, 0};  // sort, cells, moments, groups, walk passes, lists
     cudaMemPool_t pool = nullptr;   // the pool the buffers came from (cudaFreeAsync them)
 };
 

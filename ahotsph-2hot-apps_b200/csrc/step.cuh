@@ -312,6 +312,7 @@ __global__ void k_integrate(float4 *__restrict__ pts, const float4 *__restrict__
 
 // Per-plan state of the time step (owned by the plan, freed with it).
 struct grav_step_state {
+    cudaMemPool_t pool = nullptr;  // the device buffers came from this pool (adopted links)
     int64_t ncells = 0;
     int64_t *cfirst = nullptr;
     int32_t *ccount = nullptr, *cchild = nullptr, *cnchild = nullptr, *order = nullptr;
@@ -330,8 +331,12 @@ struct grav_step_state {
             cudaGraphDestroy(graph);
         for (void *p : {(void *)cfirst, (void *)ccount, (void *)cchild, (void *)cnchild,
                         (void *)order, (void *)raw})
-            if (p)
-                cudaFree(p);
+            if (p) {
+                if (pool)
+                    cudaFreeAsync(p, 0);
+                else
+                    cudaFree(p);
+            }
     }
 };
 
@@ -392,6 +397,66 @@ void step_graph_reset(grav_step_state *S) {
         cudaGraphDestroy(S->graph);
     S->exec = nullptr;
     S->graph = nullptr;
+}
+
+// The tree links of a plan whose tree was built on the device: the
+// builder's device arrays are adopted as they are (no round trip through the
+// host), and the per-cell FP64 scratch comes from the same pool.  The
+// builder makes cells level by level, so each depth is one index range and
+// the deepest-first order is those ranges in reverse; only the depths are
+// read back, to find the ranges.  The adopted arrays belong to the plan
+// from here on, also when this fails.
+int set_tree_adopt(grav_plan *pl, int64_t *cell_first, int32_t *cell_count, int32_t *cell_child,
+                   int32_t *cell_nchild, const int32_t *cell_level, cudaMemPool_t pool) {
+    const int64_t nc = pl->hp.ncells;
+    auto *S = new grav_step_state();
+    S->pool = pool;
+    S->ncells = nc;
+    S->cfirst = cell_first;
+    S->ccount = cell_count;
+    S->cchild = cell_child;
+    S->cnchild = cell_nchild;
+    std::vector<int32_t> level((size_t)std::max<int64_t>(nc, 1));
+    cudaError_t e = nc > 0 ? cudaMemcpy(level.data(), cell_level, nc * sizeof(int32_t),
+                                        cudaMemcpyDeviceToHost)
+                           : cudaSuccess;
+    if (e != cudaSuccess || nc <= 0) {
+        delete S;
+        return e != cudaSuccess ? gc::cuda_status(e, "grav_plan_build_CUDA: tree depths")
+                                : gc::set_status(-1, "grav_plan_build_CUDA: the plan has no cells");
+    }
+    std::vector<int64_t> start;  // start[l]: first cell of depth l
+    for (int64_t c = 0; c < nc; c++) {
+        if (level[c] < 0 || (c > 0 && level[c] < level[c - 1]) || level[c] > (int32_t)start.size()) {
+            delete S;
+            return gc::set_status(-1, "grav_plan_build_CUDA: cells not in depth order at %lld",
+                                  (long long)c);
+        }
+        if (level[c] == (int32_t)start.size())
+            start.push_back(c);
+    }
+    start.push_back(nc);
+    std::vector<int32_t> order;
+    order.reserve(nc);
+    S->level_ptr.assign(1, 0);
+    for (int64_t l = (int64_t)start.size() - 2; l >= 0; l--) {
+        for (int64_t c = start[l]; c < start[l + 1]; c++) order.push_back((int32_t)c);
+        S->level_ptr.push_back((int64_t)order.size());
+    }
+    e = cudaMallocFromPoolAsync((void **)&S->order, nc * sizeof(int32_t), pool, 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(S->order, order.data(), nc * sizeof(int32_t), cudaMemcpyHostToDevice, 0);
+    if (e == cudaSuccess)
+        e = cudaMallocFromPoolAsync((void **)&S->raw, (size_t)nc * kRaw * sizeof(double), pool, 0);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(0);  // `order` is read before the host vector goes
+    if (e != cudaSuccess) {
+        delete S;
+        return gc::cuda_status(e, "grav_plan_build_CUDA: tree links");
+    }
+    delete pl->step;
+    pl->step = S;
+    return 0;
 }
 
 extern "C" int grav_plan_set_tree_CUDA(grav_plan *pl, const int64_t *cell_first,

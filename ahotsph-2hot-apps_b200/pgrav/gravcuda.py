@@ -203,10 +203,15 @@ class Plan:
 
     def order(self):
         """Tree position -> input index (device-built plans), numpy int64."""
+        return d2h(self.order_ptr(), np.int64, self.n)
+
+    def order_ptr(self):
+        """Device pointer to the plan's int64 tree position -> input index
+        (device-built plans)."""
         ptr = lib().grav_plan_order(self._h)
         if not ptr:
             raise GravError("the plan was not built on the device")
-        return d2h(ptr, np.int64, self.n)
+        return ptr
 
     def problem(self):
         """Host copies of the plan's tables and lists (grav_plan_problem):
@@ -624,10 +629,12 @@ def build_eval_phases():
 
 def build_phases():
     """Seconds of this thread's last GPU tree build: sort, cells, moments and
-    tables, sink groups, walk, and the whole grav_plan_build_CUDA call."""
+    tables, sink groups, the two walk passes (count and fill), the list
+    offsets and allocations between them, and the whole
+    grav_plan_build_CUDA call."""
     out = np.zeros(7, np.float64)
     lib().grav_plan_build_phases(out.ctypes.data)
-    return dict(zip(("sort", "cells", "moments", "groups", "walk", "other", "total"),
+    return dict(zip(("sort", "cells", "moments", "groups", "walk", "lists", "total"),
                     out.tolist()))
 
 

@@ -84,6 +84,7 @@ class Stepper:
         self.gpu_build = bool(gpu_build)
         self.orig = None  # GPU rebuilds: tree position -> original body index (device int64)
         self.build_s = []  # seconds of every rebuild
+        self.build_phases = []  # GPU rebuilds: gravcuda.build_phases() of each
         self.cosmo = cosmo
         self.tpos = float(tstart)
         self.tvel = float(tstart)
@@ -112,6 +113,9 @@ class Stepper:
             self.plan.set_integrator(1)
         self.torch.cuda.synchronize()
         self.build_s.append(time.perf_counter() - t0)
+        if self.gpu_build:
+            from . import gravcuda
+            self.build_phases.append(gravcuda.build_phases())
 
     # On the GPU: the bodies and velocities stay on the device.  They go to
     # the builder in the original order, as the host rebuild hands them over
@@ -141,7 +145,8 @@ class Stepper:
             bodies[:, :3] = x
         self.plan = gc.Plan.build(None, None, self.eps2, box=self.box, ewald=self.ewald,
                                   bodies=bodies, **self.tree_kw)
-        order = torch.from_numpy(self.plan.order()).cuda()
+        order = torch.empty(n, dtype=torch.int64, device="cuda")
+        memcpy_d2d(order.data_ptr(), self.plan.order_ptr(), n * 8)
         self.dvel = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
         self.dvel[:, :3] = vel[order]
         self.orig = order

@@ -313,6 +313,7 @@ def kdk_run(w, pos, m, eps2, box, tol, nsteps, dt, rebuild):
     wall = time.perf_counter() - t0
     h = st.history
     builds = list(st.build_s)
+    build_phases = [{k: round(v, 4) for k, v in ph.items()} for ph in st.build_phases]
     st.free()
     e = np.array([r["e"] for r in h])
     pe = np.array([r["pe"] for r in h])
@@ -322,6 +323,7 @@ def kdk_run(w, pos, m, eps2, box, tol, nsteps, dt, rebuild):
             "rebuilds": "tree, moments, critical radii, groups and lists rebuilt on the GPU "
                         "from the bodies on the device (grav_plan_build_CUDA)",
             "rebuild_s": builds,
+            "rebuild_phases_s": build_phases,
             "device_ms_per_step_median": float(np.median(steady)),
             "device_ms_first_step_after_rebuild_median": float(np.median(ms[::rebuild])),
             "wall_s": wall, "energy_first": float(e[0]), "energy_last": float(e[-1]),

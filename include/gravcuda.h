@@ -271,7 +271,8 @@ void grav_plan_free(grav_plan *plan);
  * grav_plan_order: device int64 per body, tree position -> input index
  * (results are in tree order); NULL for plans uploaded from the host.
  * grav_plan_build_phases: seconds of this thread's last build: sort, cells,
- * moments and tables, sink groups, walk (both passes), plus the whole call.
+ * moments and tables, sink groups, walk (both passes), the list offsets and
+ * allocations between the passes, plus the whole call.
  */
 int grav_plan_build_CUDA(const nln_params *params, const float *bodies, int64_t n, double eps2,
                          float quad_phi_sign, int ewald, const grav_tuning *tuning,
