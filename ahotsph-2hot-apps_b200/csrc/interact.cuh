@@ -268,7 +268,8 @@ __device__ __forceinline__ void hexa2_plummer(const float *__restrict__ pr, floa
     const float2 r2 = __ffma2_rn(vx, vx, __ffma2_rn(vy, vy, __ffma2_rn(vz, vz, eps2)));
     const float2 ri = f2(rsqrt_fast(r2.x), rsqrt_fast(r2.y));
     const float2 ri2 = __fmul2_rn(ri, ri);
-    const float2 mri3 = __fmul2_rn(__fmul2_rn(m, ri), ri2);
+    const float2 ri3 = __fmul2_rn(ri, ri2);  // shared by the monopole and the higher orders
+    const float2 mri3 = __fmul2_rn(m, ri3);
     A.nphi = __ffma2_rn(m, ri, A.nphi);
     // quadrupole
     w = q[2];
@@ -281,7 +282,7 @@ __device__ __forceinline__ void hexa2_plummer(const float *__restrict__ pr, floa
     float2 Uy = __ffma2_rn(Qxy, vx, __ffma2_rn(Qyy, vy, __fmul2_rn(Qyz, vz)));
     float2 Uz = __ffma2_rn(Qxz, vx, __ffma2_rn(Qyz, vy, __fmul2_rn(Qzz, vz)));
     const float2 vQv = __ffma2_rn(vx, Ux, __ffma2_rn(vy, Uy, __fmul2_rn(vz, Uz)));
-    const float2 ri5 = __fmul2_rn(__fmul2_rn(ri, ri2), ri2);
+    const float2 ri5 = __fmul2_rn(ri3, ri2);
     const float2 eqd2 = __fmul2_rn(ri5, vQv);
     // monomials of v (hexa_vec's, with -zz in place of zz)
     const float2 third = splat2(1.0f / 3.0f);
@@ -358,7 +359,8 @@ __device__ __forceinline__ void quad2_plummer(const float *__restrict__ pr, floa
     const float2 r2 = __ffma2_rn(vx, vx, __ffma2_rn(vy, vy, __ffma2_rn(vz, vz, eps2)));
     const float2 ri = f2(rsqrt_fast(r2.x), rsqrt_fast(r2.y));
     const float2 ri2 = __fmul2_rn(ri, ri);
-    const float2 mri3 = __fmul2_rn(__fmul2_rn(m, ri), ri2);
+    const float2 ri3 = __fmul2_rn(ri, ri2);  // shared by the monopole and quadrupole terms
+    const float2 mri3 = __fmul2_rn(m, ri3);
     w = q[2];
     const float2 Qxx = f2(w.x, w.y), Qxy = f2(w.z, w.w);
     w = q[3];
@@ -369,7 +371,7 @@ __device__ __forceinline__ void quad2_plummer(const float *__restrict__ pr, floa
     const float2 Uy = __ffma2_rn(Qxy, vx, __ffma2_rn(Qyy, vy, __fmul2_rn(Qyz, vz)));
     const float2 Uz = __ffma2_rn(Qxz, vx, __ffma2_rn(Qyz, vy, __fmul2_rn(Qzz, vz)));
     const float2 vQv = __ffma2_rn(vx, Ux, __ffma2_rn(vy, Uy, __fmul2_rn(vz, Uz)));
-    const float2 ri5 = __fmul2_rn(__fmul2_rn(ri, ri2), ri2);
+    const float2 ri5 = __fmul2_rn(ri3, ri2);
     const float2 eqd2 = __fmul2_rn(ri5, vQv);
     A.nphi = __ffma2_rn(nqsh, eqd2, __ffma2_rn(m, ri, A.nphi));
     const float2 Kn = __ffma2_rn(__fmul2_rn(splat2(-2.5f), ri2), eqd2, mri3);
