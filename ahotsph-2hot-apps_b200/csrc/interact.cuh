@@ -325,12 +325,14 @@ __device__ __forceinline__ void hexa2_plummer(const float *__restrict__ pr, floa
     w = q[5];
     const float2 nX02 = f2(w.x, w.y), nX42 = f2(w.z, w.w);
     const float2 xxy = __fmul2_rn(vy, xx), xyy = __fmul2_rn(vx, yy), xyz = __fmul2_rn(xy, vz);
+    // each chain starts from xyz, the monomial ready first (two operations
+    // from v; the others take four)
     const float2 h0 = __ffma2_rn(X0, xxx, __ffma2_rn(X3, yyy, __ffma2_rn(X1, xxy, __ffma2_rn(X5, xxz,
-                      __ffma2_rn(X2, xyy, __ffma2_rn(X6, xyz, __fmul2_rn(X7, yyz)))))));
+                      __ffma2_rn(X2, xyy, __ffma2_rn(X7, yyz, __fmul2_rn(X6, xyz)))))));
     const float2 h1 = __ffma2_rn(X3, xyy, __ffma2_rn(X1, xxx, __ffma2_rn(X4, yyy, __ffma2_rn(X8, yyz,
                       __ffma2_rn(X2, xxy, __ffma2_rn(X6, xxz, __fmul2_rn(X7, xyz)))))));
-    const float2 h2 = __ffma2_rn(nX02, xxz, __ffma2_rn(nXS, xyz, __ffma2_rn(nX42, yyz, __ffma2_rn(X5, xxx,
-                      __ffma2_rn(X8, yyy, __ffma2_rn(X6, xxy, __fmul2_rn(X7, xyy)))))));
+    const float2 h2 = __ffma2_rn(nX02, xxz, __ffma2_rn(nX42, yyz, __ffma2_rn(X5, xxx, __ffma2_rn(X8, yyy,
+                      __ffma2_rn(X6, xxy, __ffma2_rn(X7, xyy, __fmul2_rn(nXS, xyz)))))));
     const float2 d4 = __ffma2_rn(vx, h0, __ffma2_rn(vy, h1, __fmul2_rn(vz, h2)));
     // sums of the orders
     const float2 ri7 = __fmul2_rn(ri5, ri2), ri9 = __fmul2_rn(ri7, ri2);
