@@ -902,8 +902,9 @@ __global__ void __launch_bounds__(128) k_ewald_moments(DevProblem P) {
                     ew_fold<3, 2>(M, Sm, o, f5);
                     ew_hex(R, r + 20, Sm);
                     ew_fold<4, 1>(M, Sm, o, f5);
-                    M.add(0, r[29] * (1.f / 6.f) * P.ew_trace);
+                    M.add(0, __fmul_rn(__fmul_rn(r[29], 1.f / 6.f), P.ew_trace));
                 }
+                M.end_entry();
             }
             s0 = s1;
             s1 = s2;
@@ -961,8 +962,9 @@ __device__ __forceinline__ void ewald_moments_loop(const DevProblem &P, int64_t 
             ew_fold<3, 2>(M, S, o, f5);
             ew_hex(h.R, h.q4, S);
             ew_fold<4, 1>(M, S, o, f5);
-            M.add(0, h.B2 * (1.f / 6.f) * P.ew_trace);
+            M.add(0, __fmul_rn(__fmul_rn(h.B2, 1.f / 6.f), P.ew_trace));
         }
+        M.end_entry();
     }
     M.warp_sum();
 }

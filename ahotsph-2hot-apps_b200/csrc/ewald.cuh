@@ -164,21 +164,36 @@ __device__ __forceinline__ void ew_lookup(const EwTab &E, float yx, float yy, fl
 
 // Group correction moments: orders 0..2 in FP64 (the net field is a small
 // difference of O(1)-per-mass terms summed over thousands of entries), the
-// u^2 and u^3 terms (orders 3, 4) in FP32.
+// u^2 and u^3 terms (orders 3, 4) in FP32.  One entry's terms of orders
+// 0..2 (its mass and up to four folds) are first summed in FP32 (`cur`),
+// which carries their own FP32 rounding anyway, and reach the FP64 sums once
+// per entry (end_entry): one FP64 add per component and entry, not five.
 struct EwMoments {
     double lo[10];
     float hi[25];
+    float cur[10];
     __device__ __forceinline__ void zero() {
 #pragma unroll
         for (int q = 0; q < 10; q++) lo[q] = 0.0;
 #pragma unroll
         for (int q = 0; q < 25; q++) hi[q] = 0.f;
+#pragma unroll
+        for (int q = 0; q < 10; q++) cur[q] = 0.f;
     }
+    // rounded adds (never contracted with the product that forms v), so
+    // every kernel that sums moments stores the same bits
     __device__ __forceinline__ void add(int q, float v) {
         if (q < 10)
-            lo[q] += (double)v;
+            cur[q] = __fadd_rn(cur[q], v);
         else
-            hi[q - 10] += v;
+            hi[q - 10] = __fadd_rn(hi[q - 10], v);
+    }
+    __device__ __forceinline__ void end_entry() {
+#pragma unroll
+        for (int q = 0; q < 10; q++) {
+            lo[q] += (double)cur[q];
+            cur[q] = 0.f;
+        }
     }
     __device__ __forceinline__ double get(int q) const { return q < 10 ? lo[q] : (double)hi[q - 10]; }
     __device__ __forceinline__ void warp_sum() {
@@ -225,7 +240,7 @@ __device__ __forceinline__ void ew_fold(EwMoments &M, const float *S, const floa
 // A source of mass m at the looked-up point: M_s += m D^alpha C.
 __device__ __forceinline__ void ew_add_mass(EwMoments &M, float m, const float *o) {
 #pragma unroll
-    for (int q = 0; q < ew::kNQ4; q++) M.add(q, m * o[q]);
+    for (int q = 0; q < ew::kNQ4; q++) M.add(q, __fmul_rn(m, o[q]));
 }
 
 // Traceless second moment (multi-index layout xx xy xz yy yz zz) from the
